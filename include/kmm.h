@@ -1,0 +1,245 @@
+/*
+ * kmm.h -- C ABI of the B200 Kim-Moin-Moser channel timestep.
+ *
+ * This is the drop-in boundary between the reference's Fortran host program
+ * (FFTW_DNS/code/src/dns/main_dns.f90, which keeps its time loop, its
+ * subroutine names and dns.config) and the GPU implementation of the hot path:
+ * solvers.f90 (Chebyshev-tau solvers, influence matrix, vcw3dp), derivatives.f90
+ * (Chebyshev / Fourier derivatives), helpers.f90 (norm, xyzfft, polymer coupling)
+ * and part_track.f90 (tracer integrator).
+ *
+ * Conventions
+ *  - Every entry point returns an int status (KMM_OK == 0).  The reference
+ *    `stop`s on the same conditions (CFL > 1, solvers.f90:3510-3514; particle
+ *    interpolation index < 1, part_track.f90:580-590; grid mismatch,
+ *    main_dns.f90:961-970); the Fortran shim calls `stop` on nonzero.
+ *  - Arrays cross the boundary as plain host pointers in the reference's own
+ *    Fortran layout (column major, y fastest):
+ *        spectral field   complex(8) (nyp,nz,nxh)   -> interleaved re/im doubles
+ *        3/2 physical     real(8)    (nyp,mz,mx)
+ *        wall rows        complex(8) (nz,nxh)
+ *        mean modes       real(8)    (nyp)
+ *        particles        real(8)    (npart)
+ *        initial fields   real(8)    (nyp,nz,nx)
+ *        imatrix          integer(4) (nyp,mz,mx)
+ *    The context owns one device mirror per field; kmm_upload / kmm_download move
+ *    a whole field between the host array and its mirror.  Routines operate on
+ *    the mirrors named by kmm_field ids, so the state stays resident in HBM and
+ *    the host syncs only at restart / output cadence.
+ *  - One host thread per context.  Calls are asynchronous on the context's
+ *    stream except kmm_download, kmm_sync and status reads.
+ *  - Grid sizes are run-time values (the reference has them as compile-time
+ *    parameters in grid_size.f90:1-47).
+ */
+#ifndef KMM_H
+#define KMM_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KMM_ABI_VERSION 1
+
+/* ---- status codes -------------------------------------------------------- */
+enum kmm_status {
+    KMM_OK = 0,
+    KMM_ERR_ARG = 1,          /* bad argument, unknown field, size mismatch        */
+    KMM_ERR_CUDA = 2,         /* CUDA runtime error (message in kmm_last_error)     */
+    KMM_ERR_CFL = 3,          /* max CFL > 1        (solvers.f90:3510-3514)         */
+    KMM_ERR_NAN = 4,          /* non-finite value in the state                      */
+    KMM_ERR_INTERP = 5,       /* particle cell index out of range (part_track.f90:580-590) */
+    KMM_ERR_TIMEOUT = 6,      /* a bounded device-side wait gave up                 */
+    KMM_ERR_NOMEM = 7,        /* device allocation failed                           */
+    KMM_ERR_UNSUPPORTED = 8   /* option not available in this build                 */
+};
+
+/* ---- run parameters -------------------------------------------------------
+ * One member per value `setstuff` reads from dns.config (main_dns.f90:934-1068),
+ * in file order, plus the module switches the reference selects at compile time
+ * (-DSCALAR / -DPOLYMER, Makefile:9-10) and a few variants that have no
+ * counterpart in the reference (each defaults to the reference behaviour).    */
+typedef struct kmm_params {
+    int    nsteps, iprnfrq;
+    double dt, gain, ugain, theta;
+    int    ny, nz, nx;              /* NY1, NZ1, NX1 (grid_size.f90:2)               */
+    int    bftail;
+    double yl, zl, xl, re, xstart, uinf;
+    int    kwall, perturbtime;
+    double r_tau, gravity;
+    int    irstrt, crstrt, print3d, geomtype, particle_flag, flow_select;
+    int    itarget, ipeter, ipolyflag, scl_flag;
+    int    npart, new_part;
+    double ratio, ap, c_mu;
+    int    cd_switch;
+    double zlmax, tpoly, alpha_poly, diffpoly, c11z, c22z, c33z, qbeta;
+    double diff, deltat, sigmax, sigmay, sigmaz;
+    int    src_start, src_stop, scltarg;
+    int    cadence;
+    double spts;
+    /* modules (-DSCALAR, -DPOLYMER) */
+    int    scalar_on, polymer_on;
+    /* variants (0 = reference behaviour) */
+    int    scalar_bc;      /* 0: zero-flux walls (main_dns.f90:350-353); 1: scalar = 0 at both walls */
+    double scalar_q;       /* uniform volumetric scalar source added to -u.grad(c); 0: none           */
+    int    tracer_scheme;  /* 0: explicit Euler (part_track.f90:416-421); 1: Williamson RK3           */
+    int    precision;      /* 0: FP64 drop-in; 1: mixed (FP32 transforms / products, FP64 solves)     */
+} kmm_params;
+
+/* ---- field ids -------------------------------------------------------------
+ * Names follow the reference's variable names in main_dns.f90:23-100.       */
+enum kmm_field {
+    /* spectral complex(8) (nyp,nz,nxh) */
+    KMM_U = 0, KMM_V, KMM_W, KMM_OMX, KMM_OMY, KMM_OMZ,
+    KMM_FN, KMM_FNM1, KMM_GN, KMM_GNM1,
+    KMM_U11, KMM_U12, KMM_U13, KMM_U21, KMM_U22, KMM_U23, KMM_U31, KMM_U32, KMM_U33,
+    KMM_LU, KMM_LV, KMM_LW,
+    KMM_GF1, KMM_GF2,
+    KMM_WRKC, KMM_WRK1,
+    KMM_SCALAR, KMM_SCLX, KMM_SCLY, KMM_SCLZ, KMM_SCN, KMM_SCNM1,
+    KMM_C11, KMM_C12, KMM_C13, KMM_C21, KMM_C22, KMM_C23, KMM_C31, KMM_C32, KMM_C33,
+    KMM_C11N, KMM_C12N, KMM_C13N, KMM_C22N, KMM_C23N, KMM_C33N,
+    KMM_C11NM1, KMM_C12NM1, KMM_C13NM1, KMM_C22NM1, KMM_C23NM1, KMM_C33NM1,
+    KMM_STR11N, KMM_STR12N, KMM_STR13N, KMM_STR22N, KMM_STR23N, KMM_STR33N,
+    KMM_STR11NM1, KMM_STR12NM1, KMM_STR13NM1, KMM_STR22NM1, KMM_STR23NM1, KMM_STR33NM1,
+    KMM_QP11, KMM_QP12, KMM_QP13, KMM_QP22, KMM_QP23, KMM_QP33,
+    KMM_T1, KMM_T2, KMM_T3,
+    /* dcIJK = d(c_IJ)/dx_K, derivatives.f90:148-254 */
+    KMM_DC111, KMM_DC112, KMM_DC113, KMM_DC121, KMM_DC122, KMM_DC123, KMM_DC131, KMM_DC132, KMM_DC133,
+    KMM_DC211, KMM_DC212, KMM_DC213, KMM_DC221, KMM_DC222, KMM_DC223, KMM_DC231, KMM_DC232, KMM_DC233,
+    KMM_DC311, KMM_DC312, KMM_DC313, KMM_DC321, KMM_DC322, KMM_DC323, KMM_DC331, KMM_DC332, KMM_DC333,
+    KMM_CSOURCE,
+    KMM_NSPECTRAL,
+
+    /* real(8) (nyp) */
+    KMM_U0 = 200, KMM_W0, KMM_H1N, KMM_H1NM1, KMM_H3N, KMM_H3NM1, KMM_UXMEAN,
+    KMM_NMEAN_END,
+
+    /* complex(8) (nz,nxh) */
+    KMM_BCTOP = 300, KMM_BCBOT, KMM_DNV1B, KMM_DNV1T, KMM_DNV2B, KMM_DNV2T, KMM_DENOM, KMM_C1, KMM_C2,
+    KMM_NWALL_END,
+
+    /* real(8) (nyp,mz,mx), 3/2-rule physical grid */
+    KMM_FXINTG = 400, KMM_FYINTG, KMM_FZINTG, KMM_UP3D, KMM_VP3D, KMM_WP3D, KMM_SWIRL3D,
+    KMM_NPHYS_END,
+
+    /* integer(4) (nyp,mz,mx) */
+    KMM_IMATRIX = 500,
+
+    /* real(8) (npart) */
+    KMM_XPART = 600, KMM_YPART, KMM_ZPART, KMM_UPART, KMM_VPART, KMM_WPART, KMM_SWIRLPART,
+    KMM_NPART_END,
+
+    /* real(8) (nyp,nz,nx): initial physical fields (COMMON /init/, main_dns.f90:98) */
+    KMM_INITU = 700, KMM_INITV, KMM_INITW, KMM_INITSCL,
+    KMM_NINIT_END
+};
+
+/* run diagnostics gathered by the last vcw3dp / step (host copy after kmm_stats) */
+typedef struct kmm_stats {
+    double cflmax;       /* max over the 3/2 grid of (|u|/dx+|v|/dy+|w|/dz) dt (solvers.f90:2985-2986) */
+    double umax;         /* max |u| on the 3/2 grid                                                  */
+    int    it;           /* COMMON /itime/ it after the call                                         */
+    int    status;       /* last nonzero status raised on the device (0 if none)                     */
+} kmm_stats;
+
+typedef struct kmm_ctx kmm_ctx;
+
+/* ---- context ------------------------------------------------------------- */
+/* Replaces setstuff + setbcs (main_dns.f90:829-1418): wavenumbers, Chebyshev
+ * weights c(i), ycoord/seght, dy/deta, BC coefficients by flow_select, the
+ * mean pressure gradient of init_flow.f90:117 and the force-spreading matrix of
+ * forcepre (main_dns.f90:1551-1558).  `device` is the CUDA ordinal.          */
+int  kmm_ctx_create(const kmm_params *params, int device, kmm_ctx **out);
+int  kmm_ctx_destroy(kmm_ctx *ctx);
+const char *kmm_last_error(const kmm_ctx *ctx);
+int  kmm_abi_version(void);
+
+/* element count and element size (bytes) of a field, 0 elements if unknown */
+int  kmm_field_size(const kmm_ctx *ctx, int field, size_t *nelem, int *elem_bytes);
+/* whole-field copies between a host array in reference layout and its mirror */
+int  kmm_upload(kmm_ctx *ctx, int field, const void *host, size_t bytes);
+int  kmm_download(kmm_ctx *ctx, int field, void *host, size_t bytes);
+/* copy one mirror into another (the reference's n -> n-1 history copies) */
+int  kmm_copy(kmm_ctx *ctx, int dst, int src);
+int  kmm_zero(kmm_ctx *ctx, int field);
+/* COMMON /itime/ it */
+int  kmm_set_it(kmm_ctx *ctx, int it);
+int  kmm_sync(kmm_ctx *ctx);
+int  kmm_get_stats(kmm_ctx *ctx, kmm_stats *out);
+
+/* ---- derivatives (derivatives.f90) --------------------------------------- */
+/* cderiv(f,df), derivatives.f90:258-314 */
+int  kmm_cderiv(kmm_ctx *ctx, int f, int df);
+/* c{0,1,2}der{b,t}w(wrkc,wrk1,iy), derivatives.f90:318-653:
+ * order 0/1/2, wall 0 = bottom (y=-1, "b"), 1 = top (y=+1, "t"); writes row iy (1-based) of `out` */
+int  kmm_wallderiv(kmm_ctx *ctx, int f, int order, int wall, int out, int iy);
+/* gradv, derivatives.f90:6-86 (u,v,w -> u11..u33, Lu, Lv, Lw) */
+int  kmm_gradv(kmm_ctx *ctx);
+/* gradscl, derivatives.f90:90-144 */
+int  kmm_gradscl(kmm_ctx *ctx);
+/* derivscji, derivatives.f90:148-254 */
+int  kmm_derivscji(kmm_ctx *ctx);
+
+/* ---- solvers (solvers.f90) ----------------------------------------------- */
+/* gfcn twice + common denominator: solvers.f90:5-172, main_dns.f90:151-161 */
+int  kmm_gfcn(kmm_ctx *ctx);
+/* phirhs(v,wrkc,wrk1,fn,fnm1,bcbot,bctop,var), solvers.f90:555-676; zeroes KMM_BCTOP/KMM_BCBOT */
+int  kmm_phirhs(kmm_ctx *ctx, int v, int fn, int fnm1, double var);
+/* the kx loop around solve(u,x,g,dyde,bctop,bcbot,ib,a,wrkc), solvers.f90:174-553,
+ * main_dns.f90:393-407; BC rows from KMM_BCTOP / KMM_BCBOT                  */
+int  kmm_solve(kmm_ctx *ctx, int u, double g, int ib);
+/* the kx loop around penta(u,x,g,dyde,ib,at,bt,gtop,ab,bb,gbot,a,wrkc), solvers.f90:680-1061,
+ * main_dns.f90:479-484; gtop/gbot from KMM_BCTOP / KMM_BCBOT               */
+int  kmm_penta(kmm_ctx *ctx, int u, double g, int ib, double at, double bt, double ab, double bb);
+/* uzero(u0,h1,h1l,uflag), solvers.f90:1065-1493 (uflag 1: u0,h1n,h1nm1; 3: w0,h3n,h3nm1) */
+int  kmm_uzero(kmm_ctx *ctx, int uflag);
+/* phi = d2v/dy2 - k^2 v in place, main_dns.f90:363-375 */
+int  kmm_phi_from_v(kmm_ctx *ctx);
+/* influence-matrix combination v += c1 gf1 + c2 gf2, main_dns.f90:426-466 */
+int  kmm_influence(kmm_ctx *ctx);
+/* veloc(u,v,w,u0,w0,omy,wrkc), solvers.f90:1576-1659 */
+int  kmm_veloc(kmm_ctx *ctx);
+/* vort(u,v,w,omx,omz), solvers.f90:1663-1722 */
+int  kmm_vort(kmm_ctx *ctx);
+/* nonlin(fn,omz,gn,wrkc,wrk1), solvers.f90:1497-1572 */
+int  kmm_nonlin(kmm_ctx *ctx);
+/* vcw3dp(...), solvers.f90:1726-3538: dealiased u x omega (+ scalar, polymer,
+ * immersed-boundary, mean-pressure-gradient terms) into fn, gn, omz (+ scn,
+ * c_n, str_n, qp); CFL check; tracer update when npart > 0.  Returns
+ * KMM_ERR_CFL when max CFL > 1, as the reference stops.                     */
+int  kmm_vcw3dp(kmm_ctx *ctx);
+
+/* ---- helpers (helpers.f90) ----------------------------------------------- */
+/* norm(a), helpers.f90:91-158 */
+int  kmm_norm(kmm_ctx *ctx, int f);
+/* xyzfft(a,b,-1), helpers.f90:6-87: physical (nyp,nz,nx) field `src` (KMM_INIT*) -> spectral `dst` */
+int  kmm_xyzfft(kmm_ctx *ctx, int dst, int src);
+/* polyNL, helpers.f90:610-674 (into KMM_T1.. scratch named by the reference's cNL arrays) */
+int  kmm_polynl(kmm_ctx *ctx);
+/* polyforce(qp..,t1,t2,t3), helpers.f90:498-560 */
+int  kmm_polyforce(kmm_ctx *ctx);
+/* subforce(gn,fn,omz,t1,t2,t3), helpers.f90:564-606 */
+int  kmm_subforce(kmm_ctx *ctx);
+
+/* ---- main-program blocks (main_dns.f90) --------------------------------- */
+/* spectral smoothing of the nonlinear terms, main_dns.f90:710-745 */
+int  kmm_filter(kmm_ctx *ctx);
+/* initial(...) with irstrt = 0, main_dns.f90:1602-2231 (initial fields from KMM_INITU/V/W) */
+int  kmm_initial(kmm_ctx *ctx);
+/* one iteration of the time loop body, main_dns.f90:198-811, fused */
+int  kmm_step(kmm_ctx *ctx);
+/* `n` iterations (stops early with the status of a failing step) */
+int  kmm_run(kmm_ctx *ctx, int n);
+
+/* ---- particles (part_track.f90) ----------------------------------------- */
+/* tracer_update(u,v,w), part_track.f90:360-433, from KMM_UP3D/VP3D/WP3D */
+int  kmm_tracer_update(kmm_ctx *ctx);
+/* init_part's velocity interpolation, part_track.f90:229-292 */
+int  kmm_init_part(kmm_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KMM_H */
