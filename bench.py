@@ -1,0 +1,350 @@
+"""Benchmark of the B200 KMM channel timestep (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl kmm|reference] [--config cfg2]
+
+Workload (default, the configuration the headline metric is quoted on): the Re_tau = 180 channel on
+128 x 129 x 128 (Lx = 4 pi, Lz = 4 pi/3, dt = 0.005), log-law mean profile + 10 % rms divergence-
+free noise (seed 1), passive scalar (Sc = 1, uniform source, Dirichlet walls) and 100,000 tracers
+(seed 2, RK3), FP64.  A "step" is one iteration of the reference's time loop (main_dns.f90:198-811).
+Inputs are synthetic and seeded.  The working set (~0.8 GB) is far larger than L2 (126 MB), so no
+L2 flush is inserted between steps.
+
+--impl kmm (default): value = steps/s of the device-resident run (CUDA events on the library's
+    stream, max over ranks); e2e = the same steps through the C ABI with the restart state held on
+    the host: every step uploads the prognostic state from pinned memory, steps, and downloads it.
+--impl reference: the CPU restatement of the reference (oracle/, OpenMP over all host cores) on a
+    bounded sample of the same workload (rank 0 only).
+Multi-GPU: replicas only (the reference's ensemble is independent runs); each rank runs its own
+    channel on its GPU, value = total steps of all ranks / max elapsed time.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "timesteps/s at 128x129x128: FP64 drop-in vs mixed-prec; ensemble steps/s"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d, "measured"
+    except Exception:
+        return PEAKS_FALLBACK, "fallback"
+
+
+def make_config(name, precision=0):
+    from polymer_dns_b200 import abi
+    if name == "cfg1":
+        re = 1400.0
+        p = abi.default_params(nx=32, ny=32, nz=32, dt=0.01, re=re, r_tau=math.sqrt(3 * re), xl=4 * math.pi,
+                               zl=2 * math.pi, precision=precision)
+        init = dict(profile="laminar", amp=0.05, kmax=4, seed=0)
+        desc = "cfg1 32x33x32 laminar+perturbation, 100-step case"
+    elif name in ("cfg2", "cfg3"):
+        re, r_tau = 2800.0, 180.0
+        kw = dict(nx=128, ny=128, nz=128, dt=0.005, re=re, r_tau=r_tau, xl=4 * math.pi, zl=4 * math.pi / 3,
+                  scalar_on=1, diff=1.0, scalar_bc=1, scalar_q=1.0, npart=100000, ap=1e-3, tracer_scheme=1,
+                  precision=precision)
+        desc = "Re_tau=180 channel 128x129x128, scalar (Sc=1, uniform source, Dirichlet walls), 100k RK3 tracers"
+        if name == "cfg3":
+            kw.update(polymer_on=1, zlmax=30.0, tpoly=20.0, qbeta=0.9, diffpoly=1000.0, gain=-400.0, ugain=-40.0)
+            desc += ", FENE-P (Wi=20, beta=0.9, L^2=900), IB cylinder r=0.25 at (pi,0)"
+        p = abi.default_params(**kw)
+        init = dict(profile="loglaw", amp=0.1, kmax=8, seed=1)
+    else:
+        raise SystemExit("unknown config %s" % name)
+    return p, init, desc
+
+
+def build_inputs(p, init, name):
+    from polymer_dns_b200 import inputs
+    f = inputs.channel_initial(p.nx, p.ny, p.nz, p.xl, p.yl, p.zl, p.re, p.r_tau, init["profile"], init["amp"],
+                               init["kmax"], init["seed"])
+    extra = {}
+    if p.scalar_on:
+        extra["INITSCL"] = np.zeros_like(f[0])
+    if p.npart > 0:
+        x, y, z = inputs.uniform_particles(p.npart, p.xl, p.yl, p.zl, p.ap, 2)
+        extra.update(XPART=x, YPART=y, ZPART=z)
+    if name == "cfg3":
+        extra["IMATRIX"] = inputs.cylinder_imatrix(p.nx, p.ny, p.nz, p.xl, p.yl, math.pi, 0.0, 0.25)
+    return f, extra
+
+
+def load(ctx, f, extra, setter):
+    setter("INITU", f[0])
+    setter("INITV", f[1])
+    setter("INITW", f[2])
+    for k, v in extra.items():
+        setter(k, v)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# per-stage algorithmic bytes per launch (each operand read or written once)
+def stage_bytes(p, nin, nout):
+    nyp, nz, nxh, mx, mz = p.ny + 1, p.nz, p.nx // 2, 3 * p.nx // 2, 3 * p.nz // 2
+    spec = nyp * nz * nxh * 16
+    q = nyp * mz * nxh * 16
+    phys = nyp * mz * mx * 8
+    return {
+        "dct_fwd": 2 * nin * spec,
+        "zfft_bwd": nin * (spec + q),
+        "xphys": nin * q + nout * phys + 3 * phys,
+        "xfwd": nout * (phys + q),
+        "zfft_fwd": nout * (q + spec),
+        "dct_bwd": 2 * nout * spec,
+    }
+
+
+def fused_model_bytes(p):
+    """Fused-minimum bytes per step (field passes x 16 B): velocity 28, scalar +13, polymer +108,
+    tracers 264 B/particle, IB 52 B per solid cell."""
+    nyp, nz, nxh = p.ny + 1, p.nz, p.nx // 2
+    P = nyp * nz * nxh
+    passes = 28 + (13 if p.scalar_on else 0) + (108 if p.polymer_on else 0)
+    return passes * 16 * P + 264 * p.npart
+
+
+def run_kmm(a, rank, world, local_rank):
+    import torch
+    from polymer_dns_b200 import runtime
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    p, init, desc = make_config(a.config, a.precision)
+    f, extra = build_inputs(p, init, a.config)
+    ctx = runtime.KmmContext(p, device=local_rank)
+    load(ctx, f, extra, ctx.upload)
+    ctx.initial()
+    for _ in range(a.warmup):
+        ctx.step()
+    ctx.call("sync")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        ctx.call("sync")
+
+    # device-resident timed region
+    barrier()
+    launches0 = ctx.launch_count()
+    ctx.set_timing(1)
+    with ClockSampler(local_rank) as clk:
+        ctx.event_record(0)
+        for _ in range(a.steps):
+            ctx.step()
+        ctx.event_record(1)
+        ms = ctx.event_elapsed(0, 1)
+    barrier()
+    launches = ctx.launch_count() - launches0
+    stages = ctx.stage_times()
+    ctx.set_timing(0)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / a.steps
+    value = world * a.steps / (ms / 1e3)
+
+    # end-to-end through the C ABI with the restart state on the host (pinned buffers)
+    state = ["V", "FN", "FNM1", "OMY", "GN", "GNM1", "U0", "H1N", "H1NM1", "W0", "H3N", "H3NM1"]
+    if p.scalar_on:
+        state += ["SCALAR", "SCN", "SCNM1"]
+    if p.npart:
+        state += ["XPART", "YPART", "ZPART", "UPART", "VPART", "WPART"]
+    host = {}
+    for n in state:
+        arr = ctx.download(n)
+        buf = torch.empty(arr.nbytes, dtype=torch.uint8, pin_memory=True)
+        buf.numpy()[:] = np.frombuffer(arr.tobytes(order="F"), dtype=np.uint8)
+        host[n] = buf
+    nbytes = sum(int(b.numel()) for b in host.values())
+    e2e_steps = max(2, min(a.steps, 10))
+    barrier()
+    ctx.event_record(2)
+    for _ in range(e2e_steps):
+        for n, b in host.items():
+            ctx.upload_ptr(n, b.data_ptr(), int(b.numel()))
+        ctx.step()
+        for n, b in host.items():
+            ctx.download_ptr(n, b.data_ptr(), int(b.numel()))
+    ctx.event_record(3)
+    e2e_ms = ctx.event_elapsed(2, 3)
+    barrier()
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * e2e_steps / (e2e_ms / 1e3)
+
+    result = None
+    if rank == 0:
+        peaks, peaks_kind = load_peaks()
+        nin = 6 + (4 if p.scalar_on else 0) + (45 if p.polymer_on else 0)
+        nout = 3 + (1 if p.scalar_on else 0) + (18 if p.polymer_on else 0)
+        sb = stage_bytes(p, nin, nout)
+        vc_stages = {k: v for k, v in stages.items() if k in sb and v[1] > 0}
+        dom = max(vc_stages, key=lambda k: vc_stages[k][0]) if vc_stages else None
+        total_stage_ms = sum(v[0] for v in stages.values())
+        roof = None
+        if dom:
+            avg_ms = vc_stages[dom][0] / vc_stages[dom][1]
+            ach = sb[dom] / (avg_ms / 1e3) / 1e9
+            peak = float(peaks.get("hbm_gbs", 6650.0))
+            roof = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 1), "peak": peak,
+                    "peak_kind": peaks_kind, "unit": "GB/s", "frac": round(ach / peak, 4),
+                    "avg_launch_ms": round(avg_ms, 4), "algorithmic_bytes_per_launch": sb[dom],
+                    "traffic": None}
+        model = fused_model_bytes(p)
+        result = {
+            "metric": METRIC, "value": round(value, 3), "unit": "timesteps/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if p.precision == 0 else "mixed",
+            "data": "synthetic (seeded log-law + noise, uniform tracers)",
+            "config": {"workload": desc, "grid": [p.nx, p.ny + 1, p.nz], "dt": p.dt, "npart": p.npart,
+                       "precision": "fp64 drop-in" if p.precision == 0 else "mixed",
+                       "parallelism": "replicas x%d" % world,
+                       "l2": "inputs larger than L2 (state ~%d MB), no flush" % int(model / 1e6),
+                       "grid_point_steps_per_s": round(value * p.nx * (p.ny + 1) * p.nz, 1),
+                       "fused_model_bytes_per_step": model,
+                       "step_frac_of_hbm": round(model / (ms_per_step / 1e3) / 1e9 / float(peaks.get("hbm_gbs", 6650.0)), 4),
+                       "stage_ms_per_step": {k: round(v[0] / max(1, a.steps), 4) for k, v in stages.items()},
+                       "stage_share": {k: round(v[0] / total_stage_ms, 4) for k, v in stages.items()} if total_stage_ms else {}},
+            "roofline": roof,
+            "e2e": {"value": round(e2e_value, 3), "unit": "timesteps/s", "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes, "steps": e2e_steps},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        if not a.no_cpu_baseline and world == 1:
+            result["cpu_baseline"] = cpu_baseline(a.config, a.cpu_steps)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def cpu_baseline(config, nsteps):
+    """The oracle (C restatement of the reference, OpenMP) on the host cores: a bounded sample."""
+    from oracle import pyoracle
+    p, init, desc = make_config(config)
+    f, extra = build_inputs(p, init, config)
+    o = pyoracle.Oracle(p)
+    load(o, f, extra, o.set)
+    o.initial()
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        o.step()
+    dt = time.perf_counter() - t0
+    o.close()
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": round(nsteps / dt, 5), "unit": "timesteps/s", "cores": cores, "kind": "port",
+            "sample": "%d steps of the same workload after initial (%.1f s)" % (nsteps, dt)}
+
+
+def run_reference(a, rank, world):
+    if rank != 0:
+        return None
+    p, init, desc = make_config(a.config)
+    steps = max(1, min(a.steps, a.cpu_steps))
+    cb = cpu_baseline(a.config, steps)
+    return {"metric": METRIC, "value": cb["value"], "unit": "timesteps/s", "n_gpus": world, "steps": steps,
+            "warmup": 0, "ms_per_step": round(1e3 / cb["value"], 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": desc, "grid": [p.nx, p.ny + 1, p.nz], "npart": p.npart},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="kmm", choices=["kmm", "reference"])
+    ap.add_argument("--config", default="cfg2", choices=["cfg1", "cfg2", "cfg3"])
+    ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    if a.warmup < 3:
+        a.warmup = 3
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if a.impl == "reference":
+        res = run_reference(a, rank, world)
+    else:
+        res = run_kmm(a, rank, world, local_rank)
+    if rank == 0 and res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -239,6 +239,29 @@ int  kmm_tracer_update(kmm_ctx *ctx);
 /* init_part's velocity interpolation, part_track.f90:229-292 */
 int  kmm_init_part(kmm_ctx *ctx);
 
+/* ---- instrumentation (no counterpart in the reference, whose only profiling is the
+ * cadence timer of main_dns.f90:797-809) --------------------------------------- */
+enum kmm_stage {
+    KMM_STAGE_COLUMN = 0,   /* linear stage of the step before vcw3dp (main_dns.f90:203-606)   */
+    KMM_STAGE_DCT_FWD,      /* vcw3dp: Chebyshev -> physical y                                  */
+    KMM_STAGE_ZFFT_BWD,     /* vcw3dp: zero-pad + inverse z transform                           */
+    KMM_STAGE_XPHYS,        /* vcw3dp: inverse x transform + pointwise terms                    */
+    KMM_STAGE_XFWD,         /* vcw3dp: forward x transform                                      */
+    KMM_STAGE_ZFFT_FWD,     /* vcw3dp: forward z transform + truncation                         */
+    KMM_STAGE_DCT_BWD,      /* vcw3dp: physical -> Chebyshev y                                  */
+    KMM_STAGE_POST,         /* after vcw3dp: norms, polymer force, filter, nonlin (607-771)     */
+    KMM_NSTAGES
+};
+/* record CUDA events around each stage (on = 1) until the next kmm_get_stage_times */
+int  kmm_set_timing(kmm_ctx *ctx, int on);
+/* summed milliseconds and record counts per kmm_stage since the last call */
+int  kmm_get_stage_times(kmm_ctx *ctx, double *ms, int *count, int nstages);
+/* number of kernel launches the context has issued so far */
+long long kmm_launch_count(const kmm_ctx *ctx);
+/* CUDA events on the context's stream: record into slot (0..15), elapsed ms between two slots */
+int  kmm_event_record(kmm_ctx *ctx, int slot);
+int  kmm_event_elapsed(kmm_ctx *ctx, int slot_a, int slot_b, double *ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1576,6 +1576,12 @@ int orc_vcw3dp(orc_ctx *c)
         for (int m = 0; m < 6; ++m) { out_ids[nout] = q[m]; out_slot[nout++] = O_QP11 + m; }
     }
 
+    /* resolve (and allocate) every field before the parallel regions */
+    cplx *inp[P_NIN], *outp[O_NOUT];
+    for (int f = 0; f < nin; ++f) inp[f] = SF(c, in_ids[f]);
+    for (int f = 0; f < nout; ++f) outp[f] = SF(c, out_ids[f]);
+    (void)RF(c, KMM_UXMEAN);
+    for (int f = KMM_XPART; f < KMM_NPART_END; ++f) (void)orc_field(c, f);
     /* scale by c(i)/2 and DCT-I along y (REDFT00), solvers.f90:2241-2546 */
     cplx **yin = calloc((size_t)nin, sizeof(cplx *));
     for (int f = 0; f < nin; ++f) yin[f] = malloc(sizeof(cplx) * nspec);
@@ -1588,7 +1594,7 @@ int orc_vcw3dp(orc_ctx *c)
 #pragma omp for collapse(2)
         for (int f = 0; f < nin; ++f)
             for (int col = 0; col < nz * nxh; ++col) {
-                const cplx *src = SF(c, in_ids[f]) + (size_t)col * nyp;
+                const cplx *src = inp[f] + (size_t)col * nyp;
                 for (int i = 0; i < nyp; ++i) {
                     double fac = c->c[i] / 2.0;
                     x[i] = creal(src[i]) * fac + I * (cimag(src[i]) * fac);
@@ -1803,7 +1809,7 @@ int orc_vcw3dp(orc_ctx *c)
         for (int f = 0; f < nout; ++f)
             for (int col = 0; col < nz * nxh; ++col) {
                 dct1_c(&c->py2, yout[f] + (size_t)col * nyp, o, w1, w2);
-                cplx *dst = SF(c, out_ids[f]) + (size_t)col * nyp;
+                cplx *dst = outp[f] + (size_t)col * nyp;
                 for (int i = 0; i < nyp; ++i) dst[i] = (creal(o[i]) + I * cimag(o[i])) / (double)ny;
                 dst[0] = dst[0] / 2.0;
                 dst[nyp - 1] = dst[nyp - 1] / 2.0;

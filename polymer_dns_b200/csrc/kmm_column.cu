@@ -1,0 +1,1076 @@
+// kmm_column.cu -- per-(kx,kz)-column routines of solvers.f90 / derivatives.f90 / helpers.f90.
+//
+// Spectral fields are complex(8) (nyp,nz,nxh), y fastest: column col = k*nz + j holds the nyp
+// Chebyshev coefficients of wavenumber pair (kx = wavx(k), kz = wavz(j)) contiguously, so a tile
+// of TILE consecutive columns is one contiguous block of TILE*nyp double2 -> fully coalesced
+// loads and stores.  The y recurrences (Chebyshev derivative, tau eliminations) run with one
+// thread per column on the tile in shared memory, in the reference's own operation order.
+// This file is compiled with -fmad=false so those recurrences round like the reference's
+// separate multiply / add sequence.
+#include <math.h>
+
+#include "kmm_internal.cuh"
+
+#define TILE 16
+#define TPB 128
+
+static inline size_t tile_smem(int nyp, int nbuf) { return sizeof(double2) * (size_t)TILE * nyp * nbuf; }
+
+__device__ __forceinline__ void tile_load(double2 *s, const double2 *__restrict__ g, int col0, int ncol, int nyp) {
+    const size_t n = (size_t)ncol * nyp;
+    const double2 *src = g + (size_t)col0 * nyp;
+    for (size_t e = threadIdx.x; e < n; e += blockDim.x) s[e] = src[e];
+}
+
+__device__ __forceinline__ void tile_store(double2 *__restrict__ g, const double2 *s, int col0, int ncol, int nyp) {
+    const size_t n = (size_t)ncol * nyp;
+    double2 *dst = g + (size_t)col0 * nyp;
+    for (size_t e = threadIdx.x; e < n; e += blockDim.x) dst[e] = s[e];
+}
+
+// ---------------------------------------------------------------------------
+// cderiv(f,df), derivatives.f90:258-314: two independent parity chains per column
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TPB) k_cderiv(const double2 *__restrict__ f, double2 *__restrict__ df, int ncols,
+                                                int nyp, double dyde) {
+    extern __shared__ double2 sm[];
+    double2 *sf = sm, *sd = sm + (size_t)TILE * nyp;
+    const int col0 = blockIdx.x * TILE;
+    const int ncol = min(TILE, ncols - col0);
+    tile_load(sf, f, col0, ncol, nyp);
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < 2 * ncol) {
+        const int cl = t >> 1, par = t & 1;
+        const double2 *F = sf + (size_t)cl * nyp;
+        double2 *D = sd + (size_t)cl * nyp;
+        const int ny = nyp - 1;
+        double2 acc;
+        int idx;
+        if (par == (ny & 1)) {          // chain through index ny: D[ny] = 0
+            acc = make_double2(0.0, 0.0);
+            D[ny] = acc;
+            idx = ny - 2;
+        } else {                        // chain through ny-1: D[ny-1] = 2 ny F[ny] dyde
+            double s = 2.0 * (double)ny;
+            acc = make_double2(s * F[ny].x * dyde, s * F[ny].y * dyde);
+            D[ny - 1] = acc;
+            idx = ny - 3;
+        }
+        for (; idx >= 0; idx -= 2) {    // D[idx] = D[idx+2] + 2 (idx+1) F[idx+1] dyde
+            double s = 2.0 * (double)(idx + 1);
+            double2 fv = F[idx + 1];
+            acc = make_double2(acc.x + s * fv.x * dyde, acc.y + s * fv.y * dyde);
+            D[idx] = acc;
+        }
+        if (par == 0) D[0] = make_double2(0.5 * D[0].x, 0.5 * D[0].y);
+    }
+    __syncthreads();
+    tile_store(df, sd, col0, ncol, nyp);
+}
+
+int kmm_internal_cderiv(kmm_ctx *ctx, const double2 *f, double2 *df) {
+    const int ncols = ctx->nz * ctx->nxh;
+    const size_t sm = tile_smem(ctx->nyp, 2);
+    static bool attr = false;
+    if (!attr) {
+        CK(cudaFuncSetAttribute(k_cderiv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(TILE * KMM_MAX_NYP * 2 * sizeof(double2))));
+        attr = true;
+    }
+    k_cderiv<<<(ncols + TILE - 1) / TILE, TPB, sm, ctx->stream>>>(f, df, ncols, ctx->nyp, ctx->dyde);
+    CKL();
+    return KMM_OK;
+}
+
+extern "C" int kmm_cderiv(kmm_ctx *ctx, int f, int df) {
+    if (!ctx || f == df) return KMM_ERR_ARG;
+    double2 *a = SPEC(ctx, f), *b = SPEC(ctx, df);
+    if (!a || !b || f >= KMM_NSPECTRAL || df >= KMM_NSPECTRAL) return KMM_ERR_ARG;
+    return kmm_internal_cderiv(ctx, a, b);
+}
+
+// ---------------------------------------------------------------------------
+// c{0,1,2}der{b,t}w, derivatives.f90:318-653: one warp per column, then the
+// partial sums are folded in the reference's index order by lane 0.
+// ---------------------------------------------------------------------------
+__global__ void k_wallderiv(const double2 *__restrict__ f, double2 *__restrict__ out, int ncols, int nyp, int order,
+                            int wall, int iy, double dyde) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= ncols) return;
+    const double2 *F = f + (size_t)warp * nyp;
+    // each lane accumulates a contiguous chunk in ascending order; chunks are then added in order
+    const int chunk = (nyp + 31) / 32;
+    const int i0 = lane * chunk, i1 = min(nyp, i0 + chunk);
+    double2 acc = make_double2(0.0, 0.0);
+    for (int i = i0; i < i1; ++i) {
+        double rp = (double)i;
+        double sgn = 1.0;
+        if (wall == 0) sgn = (order == 0) ? ((i & 1) ? -1.0 : 1.0) : ((i & 1) ? 1.0 : -1.0);
+        double2 v = F[i];
+        double wgt;
+        if (order == 0) {
+            acc = make_double2(acc.x + sgn * v.x, acc.y + sgn * v.y);
+            continue;
+        } else if (order == 1) {
+            wgt = rp * rp * sgn;
+            acc = make_double2(acc.x + wgt * v.x * dyde, acc.y + wgt * v.y * dyde);
+        } else {
+            double rp2 = rp * rp;
+            wgt = (rp2 - 1.0) * rp2 * sgn;
+            acc = make_double2(acc.x + wgt * v.x * dyde * dyde / 3.0, acc.y + wgt * v.y * dyde * dyde / 3.0);
+        }
+    }
+    for (int off = 1; off < 32; off <<= 1) {
+        double ax = __shfl_down_sync(0xffffffffu, acc.x, off);
+        double ay = __shfl_down_sync(0xffffffffu, acc.y, off);
+        if ((lane & (2 * off - 1)) == 0) { acc.x += ax; acc.y += ay; }
+    }
+    if (lane == 0) out[(size_t)warp * nyp + (iy - 1)] = acc;
+}
+
+int kmm_internal_wallderiv(kmm_ctx *ctx, const double2 *f, int order, int wall, double2 *out, int iy) {
+    const int ncols = ctx->nz * ctx->nxh;
+    const int threads = 256;
+    const int blocks = (ncols * 32 + threads - 1) / threads;
+    k_wallderiv<<<blocks, threads, 0, ctx->stream>>>(f, out, ncols, ctx->nyp, order, wall, iy, ctx->dyde);
+    CKL();
+    return KMM_OK;
+}
+
+extern "C" int kmm_wallderiv(kmm_ctx *ctx, int f, int order, int wall, int out, int iy) {
+    if (!ctx || order < 0 || order > 2 || wall < 0 || wall > 1 || iy < 1 || iy > ctx->nyp) return KMM_ERR_ARG;
+    if (f >= KMM_NSPECTRAL || out >= KMM_NSPECTRAL) return KMM_ERR_ARG;
+    double2 *a = SPEC(ctx, f), *b = SPEC(ctx, out);
+    if (!a || !b) return KMM_ERR_NOMEM;
+    return kmm_internal_wallderiv(ctx, a, order, wall, b, iy);
+}
+
+// ---------------------------------------------------------------------------
+// norm(a), helpers.f90:91-158
+// ---------------------------------------------------------------------------
+__global__ void k_norm(double2 *a, int nyp, int nz, int nxh, int nzh) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int npair = nyp * (nz / 2);      // j = 1..nz/2 (0-based j = 0 handles the (0,0) mode)
+    if (t < npair) {
+        const int i = t % nyp, j = t / nyp;  // 0-based j in [0, nz/2)
+        if (j == 0) {
+            double2 v = a[i];
+            a[i] = make_double2(v.x, 0.0);
+        } else {
+            const int jp = nz - j;           // 0-based partner of j (1-based nz+2-j)
+            double2 x = a[(size_t)j * nyp + i], y = a[(size_t)jp * nyp + i];
+            double2 m = make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
+            a[(size_t)j * nyp + i] = m;
+            a[(size_t)jp * nyp + i] = make_double2(m.x, -m.y);
+        }
+    } else {
+        const int u = t - npair;
+        if (u < nyp * nxh) {
+            const int i = u % nyp, k = u / nyp;
+            a[((size_t)k * nz + nzh) * nyp + i] = make_double2(0.0, 0.0);
+        }
+    }
+}
+
+int kmm_internal_norm(kmm_ctx *ctx, double2 *a) {
+    const int n = ctx->nyp * (ctx->nz / 2) + ctx->nyp * ctx->nxh;
+    k_norm<<<(n + 255) / 256, 256, 0, ctx->stream>>>(a, ctx->nyp, ctx->nz, ctx->nxh, ctx->nzh);
+    CKL();
+    return KMM_OK;
+}
+
+extern "C" int kmm_norm(kmm_ctx *ctx, int f) {
+    if (!ctx || f < 0 || f >= KMM_NSPECTRAL) return KMM_ERR_ARG;
+    double2 *a = SPEC(ctx, f);
+    if (!a) return KMM_ERR_NOMEM;
+    return kmm_internal_norm(ctx, a);
+}
+
+// ---------------------------------------------------------------------------
+// tau solvers.  Matrix rows of evnc / oddc (solvers.f90:324-383), recomputed on the fly:
+//   even (ip=0) row i, j = 2i;  odd (ip=1) row i, j = 2i+1:
+//   a1 = wn rj1, a2 = -dyde^2 - wn rj2, a3 = wn rj3 with the end-row overrides.
+// ---------------------------------------------------------------------------
+struct TauRow { double a1, a2, a3; };
+
+__device__ __forceinline__ TauRow tau_row(int i, int par, double wn, double dyde, int nyh, int nyhm) {
+    TauRow r;
+    const int j = par == 0 ? 2 * i : 2 * i + 1;
+    const double rj1 = 1.0 / (double)(4 * j * (j - 1));
+    const double rj2 = 1.0 / (double)(2 * (j * j - 1));
+    const double rj3 = 1.0 / (double)(4 * j * (j + 1));
+    r.a1 = wn * rj1;
+    r.a2 = -1.0 * dyde * dyde - wn * rj2;
+    r.a3 = wn * rj3;
+    if (par == 0) {
+        if (i == 1) r.a1 = 2.0 * r.a1;
+        if (i == nyhm) r.a3 = 0.0;
+        if (i == nyh) { r.a2 = -1.0 * dyde * dyde; r.a3 = 0.0; }
+    } else {
+        if (i == nyhm - 1) r.a3 = 0.0;
+        if (i == nyhm) { r.a2 = -1.0 * dyde * dyde; r.a3 = 0.0; }
+    }
+    return r;
+}
+
+// RHS rows 2..nrank of evns/pntevns (par 0) or odds/pntodds (par 1), written in place at the
+// parity positions W(i) = col[2(i-1)+par]; c0 = c(0) Chebyshev weight (2).
+__device__ __forceinline__ void tau_rhs_inplace(double2 *col, int par, int ny, int nyh, int nyhm, double c0) {
+#define POS(i) (2 * ((i) - 1) + par)
+    if (par == 0) {
+        // rows i = 2..nyhm use s(j-2), s(j), s(j+2), j = 2i-2 (solvers.f90:387-448)
+        double2 sm2 = col[0], s0 = col[2];
+        for (int i = 2; i <= nyhm; ++i) {
+            const int j = 2 * i - 2;
+            double2 sp2 = col[j + 2];
+            const double rj1 = 1.0 / (double)(4 * j * (j - 1));
+            const double rj2 = 1.0 / (double)(2 * (j * j - 1));
+            const double rj3 = 1.0 / (double)(4 * j * (j + 1));
+            const double cm = (j - 2 == 0) ? c0 : 1.0;
+            double2 w;
+            w.x = -cm * sm2.x * rj1 + s0.x * rj2 - sp2.x * rj3;
+            w.y = -cm * sm2.y * rj1 + s0.y * rj2 - sp2.y * rj3;
+            col[POS(i)] = w;
+            sm2 = s0;
+            s0 = sp2;
+        }
+        {   // row nyh: j = ny-2
+            const int j = ny - 2;
+            const double rj1 = 1.0 / (double)(4 * j * (j - 1));
+            const double rj2 = 1.0 / (double)(2 * (j * j - 1));
+            double2 w;
+            w.x = -sm2.x * rj1 + s0.x * rj2;
+            w.y = -sm2.y * rj1 + s0.y * rj2;
+            col[POS(nyh)] = w;
+        }
+        {   // row nyhp: j = ny, s(ny-2) is the current s0
+            const int j = ny;
+            const double rj1 = 1.0 / (double)(4 * j * (j - 1));
+            col[POS(nyh + 1)] = make_double2(-s0.x * rj1, -s0.y * rj1);
+        }
+    } else {
+        // rows i = 2..nyhm-1, j = 2i-1 (solvers.f90:450-496)
+        double2 sm2 = col[1], s0 = col[3];
+        for (int i = 2; i <= nyhm - 1; ++i) {
+            const int j = 2 * i - 1;
+            double2 sp2 = col[j + 2];
+            const double rj1 = 1.0 / (double)(4 * j * (j - 1));
+            const double rj2 = 1.0 / (double)(2 * (j * j - 1));
+            const double rj3 = 1.0 / (double)(4 * j * (j + 1));
+            double2 w;
+            w.x = -sm2.x * rj1 + s0.x * rj2 - sp2.x * rj3;
+            w.y = -sm2.y * rj1 + s0.y * rj2 - sp2.y * rj3;
+            col[POS(i)] = w;
+            sm2 = s0;
+            s0 = sp2;
+        }
+        {   // row nyhm: j = ny-3
+            const int j = ny - 3;
+            const double rj1 = 1.0 / (double)(4 * j * (j - 1));
+            const double rj2 = 1.0 / (double)(2 * (j * j - 1));
+            double2 w;
+            w.x = -sm2.x * rj1 + s0.x * rj2;
+            w.y = -sm2.y * rj1 + s0.y * rj2;
+            col[POS(nyhm)] = w;
+        }
+        {   // row nyh: j = ny-1, s(ny-3) is the current s0
+            const int j = ny - 1;
+            const double rj1 = 1.0 / (double)(4 * j * (j - 1));
+            col[POS(nyh)] = make_double2(-s0.x * rj1, -s0.y * rj1);
+        }
+    }
+#undef POS
+}
+
+// eqsolve(a,t,wrk,nrank), solvers.f90:500-553, in place at parity positions; d: local scratch
+__device__ __forceinline__ double tau_t(int q, int par, int ib, double dyde) {
+    if (ib == 0) return 1.0;                               // dircbc
+    const int m2 = par == 0 ? 2 * (q - 1) : 2 * (q - 1) + 1; // neumbc
+    return dyde * (double)(m2 * m2);
+}
+
+__device__ void eqsolve_inplace(double2 *col, int par, int nrank, double wn, double dyde, int nyh, int nyhm, int ib,
+                                double *d) {
+#define W(i) col[2 * ((i) - 1) + par]
+    const int m = nrank - 1, mm1 = m - 1;
+    d[m] = tau_row(m, par, wn, dyde, nyh, nyhm).a2;
+    for (int i = mm1; i >= 1; --i) {
+        TauRow ri = tau_row(i, par, wn, dyde, nyh, nyhm);
+        TauRow rn = tau_row(i + 1, par, wn, dyde, nyh, nyhm);
+        d[i] = ri.a2 - ri.a3 * rn.a1 / d[i + 1];
+        double2 w1 = W(i + 1), w2 = W(i + 2);
+        W(i + 1) = make_double2(w1.x - ri.a3 * w2.x / d[i + 1], w1.y - ri.a3 * w2.y / d[i + 1]);
+    }
+    TauRow rm = tau_row(m, par, wn, dyde, nyh, nyhm);
+    const double tn = tau_t(nrank, par, ib, dyde);
+    double f = tau_t(m, par, ib, dyde) - tn * rm.a1 / d[m];
+    double2 w1 = W(1), wn_ = W(nrank);
+    w1 = make_double2(w1.x - tn * wn_.x / d[m], w1.y - tn * wn_.y / d[m]);
+    for (int i = mm1; i >= 1; --i) {
+        TauRow ri = tau_row(i, par, wn, dyde, nyh, nyhm);
+        double2 wi = W(i + 1);
+        w1 = make_double2(w1.x - f * wi.x / d[i], w1.y - f * wi.y / d[i]);
+        f = tau_t(i, par, ib, dyde) - f * ri.a1 / d[i];
+    }
+    w1 = make_double2(w1.x / f, w1.y / f);
+    W(1) = w1;
+    double2 prev = w1;
+    for (int i = 2; i <= nrank; ++i) {
+        TauRow rp = tau_row(i - 1, par, wn, dyde, nyh, nyhm);
+        double2 wi = W(i);
+        prev = make_double2((wi.x - rp.a1 * prev.x) / d[i - 1], (wi.y - rp.a1 * prev.y) / d[i - 1]);
+        W(i) = prev;
+    }
+#undef W
+}
+
+// solve(u,x,g,dyde,bctop,bcbot,ib,a,wrkc), solvers.f90:174-283 for every (kx,kz) column
+__global__ void __launch_bounds__(TPB) k_solve(double2 *__restrict__ u, const double2 *__restrict__ bct,
+                                               const double2 *__restrict__ bcb, const double *__restrict__ wavx,
+                                               const double *__restrict__ wavz, int ncols, int nz, int nyp, double g,
+                                               int ib, double dyde, double c0) {
+    extern __shared__ double2 sm[];
+    const int col0 = blockIdx.x * TILE;
+    const int ncol = min(TILE, ncols - col0);
+    tile_load(sm, u, col0, ncol, nyp);
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < ncol) {
+        const int ny = nyp - 1, nyh = ny / 2, nyhm = nyh - 1, nyhp = nyh + 1;
+        const int colg = col0 + t;
+        const int j = colg % nz, k = colg / nz;
+        double2 *col = sm + (size_t)t * nyp;
+        double wn = wavz[j] * wavz[j] + wavx[k] * wavx[k] + g;
+        bool kzero = false;
+        if (ib != 0 && wn <= 1.0e-20) { kzero = true; wn = 1.0; }
+        double *d = (double *)(sm + (size_t)TILE * nyp) + (size_t)t * (nyhp + 1);
+        const double2 bt = bct[colg], bb = bcb[colg];
+        for (int par = 0; par < 2; ++par) {
+            const int nrank = par == 0 ? nyhp : nyh;
+            tau_rhs_inplace(col, par, ny, nyh, nyhm, c0);
+            // BC row: evns / odds
+            double2 w1;
+            if ((ib == 0) == (par == 0)) w1 = make_double2(0.5 * (bt.x + bb.x), 0.5 * (bt.y + bb.y));
+            else w1 = make_double2(0.5 * (bt.x - bb.x), 0.5 * (bt.y - bb.y));
+            col[par] = w1;
+            eqsolve_inplace(col, par, nrank, wn, dyde, nyh, nyhm, ib, d);
+        }
+        if (kzero)
+            for (int i = 0; i < nyp; ++i) col[i] = make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    tile_store(u, sm, col0, ncol, nyp);
+}
+
+int kmm_internal_solve(kmm_ctx *ctx, double2 *u, double g, int ib, const double2 *bct, const double2 *bcb) {
+    const int ncols = ctx->nz * ctx->nxh;
+    static bool attr = false;
+    if (!attr) {
+        CK(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(TILE * KMM_MAX_NYP * (sizeof(double2) + sizeof(double)))));
+        attr = true;
+    }
+    const size_t smem = tile_smem(ctx->nyp, 1) + sizeof(double) * TILE * (size_t)(ctx->nyhp + 1);
+    k_solve<<<(ncols + TILE - 1) / TILE, TPB, smem, ctx->stream>>>(
+        u, bct, bcb, ctx->d_wavx, ctx->d_wavz, ncols, ctx->nz, ctx->nyp, g, ib, ctx->dyde, ctx->h_c[0]);
+    CKL();
+    return KMM_OK;
+}
+
+extern "C" int kmm_solve(kmm_ctx *ctx, int u, double g, int ib) {
+    if (!ctx || u < 0 || u >= KMM_NSPECTRAL) return KMM_ERR_ARG;
+    double2 *a = SPEC(ctx, u), *bt = SPEC(ctx, KMM_BCTOP), *bb = SPEC(ctx, KMM_BCBOT);
+    if (!a || !bt || !bb) return KMM_ERR_NOMEM;
+    return kmm_internal_solve(ctx, a, g, ib, bt, bb);
+}
+
+// penta: mixedbc + pntevns/pntodds + pntsolve + fillt, solvers.f90:680-1061
+__global__ void __launch_bounds__(TPB) k_penta(double2 *__restrict__ u, const double2 *__restrict__ gtop,
+                                               const double2 *__restrict__ gbot, const double *__restrict__ wavx,
+                                               const double *__restrict__ wavz, int ncols, int nz, int nyp, double g,
+                                               int ib, double at, double bt, double ab, double bb, double dyde,
+                                               double c0) {
+    extern __shared__ double2 sm[];
+    const int col0 = blockIdx.x * TILE;
+    const int ncol = min(TILE, ncols - col0);
+    tile_load(sm, u, col0, ncol, nyp);
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < ncol) {
+        const int ny = nyp - 1, nyh = ny / 2, nyhm = nyh - 1, nyhp = nyh + 1;
+        const int colg = col0 + t;
+        const int j = colg % nz, k = colg / nz;
+        double2 *col = sm + (size_t)t * nyp;   // gs(i,ip) lives at the parity positions of the column
+        double wn = wavz[j] * wavz[j] + wavx[k] * wavx[k] + g;
+        bool kzero = false;
+        if (ib != 0 && wn <= 1.0e-20) { kzero = true; wn = 1.0; }
+        double *dsb = (double *)(sm + (size_t)TILE * nyp) + (size_t)t * 2 * (nyhp + 1);
+        double *ds[2] = {dsb, dsb + (nyhp + 1)};
+        double f[2][2];
+        double2 s[2];
+        s[0] = gtop[colg];
+        s[1] = gbot[colg];
+        for (int par = 0; par < 2; ++par) {
+            const int ip = par + 1;
+            const int n = par == 0 ? nyhp : nyh, m = n - 1, mm1 = m - 1;
+            tau_rhs_inplace(col, par, ny, nyh, nyhm, c0);
+#define GS(i) col[2 * ((i) - 1) + par]
+            double *D = ds[par];
+            D[m] = tau_row(m, par, wn, dyde, nyh, nyhm).a2;
+            for (int i = mm1; i >= 1; --i) {
+                TauRow ri = tau_row(i, par, wn, dyde, nyh, nyhm);
+                TauRow rn = tau_row(i + 1, par, wn, dyde, nyh, nyhm);
+                D[i] = ri.a2 - ri.a3 * rn.a1 / D[i + 1];
+                double2 g1 = GS(i + 1), g2 = GS(i + 2);
+                GS(i + 1) = make_double2(g1.x - ri.a3 * g2.x / D[i + 1], g1.y - ri.a3 * g2.y / D[i + 1]);
+            }
+            // ipass 1 eliminates into the bottom row (js = 2, tb), ipass 2 into the top row (js = 1, tt)
+            for (int ipass = 1; ipass <= 2; ++ipass) {
+                const int js = ipass == 1 ? 2 : 1;
+                // fillt: t(q) = t{b,t}(2q-1) (even) or t{b,t}(2q) (odd); mixedbc: tt(jj) = at + dyde bt (jj-1)^2,
+                // tb(jj) = (ab + dyde bb (jj-1)^2) (-1)^(jj-1)
+#define TVAL(q) ([&](int qq) -> double {                                         \
+                    int jj = par == 0 ? 2 * qq - 1 : 2 * qq;                    \
+                    int j1 = jj - 1;                                            \
+                    if (ipass == 2) return at + dyde * bt * (double)(j1 * j1);   \
+                    double v = ab + dyde * bb * (double)(j1 * j1);               \
+                    return (jj % 2 == 0) ? -v : v;                              \
+                }(q))
+                TauRow rm = tau_row(m, par, wn, dyde, nyh, nyhm);
+                double ff = TVAL(m) - TVAL(n) * rm.a1 / D[m];
+                double2 gn = GS(n);
+                double tn = TVAL(n);
+                double2 ss = s[js - 1];
+                ss = make_double2(ss.x - tn * gn.x / D[m], ss.y - tn * gn.y / D[m]);
+                for (int i = mm1; i >= 1; --i) {
+                    TauRow ri = tau_row(i, par, wn, dyde, nyh, nyhm);
+                    double2 gi = GS(i + 1);
+                    ss = make_double2(ss.x - ff * gi.x / D[i], ss.y - ff * gi.y / D[i]);
+                    ff = TVAL(i) - ff * ri.a1 / D[i];
+                }
+                s[js - 1] = ss;
+                f[js - 1][par] = ff;
+#undef TVAL
+            }
+#undef GS
+        }
+        // 2x2 system for the first even / odd unknowns, then both back substitutions
+        const double det = f[0][0] * f[1][1] - f[1][0] * f[0][1];
+        double2 x0 = make_double2((s[0].x * f[1][1] - s[1].x * f[0][1]) / det, (s[0].y * f[1][1] - s[1].y * f[0][1]) / det);
+        double2 x1 = make_double2((s[1].x * f[0][0] - s[0].x * f[1][0]) / det, (s[1].y * f[0][0] - s[0].y * f[1][0]) / det);
+        col[0] = x0;
+        col[1] = x1;
+        {
+            double2 prev = x0;
+            for (int i = 2; i <= nyhp; ++i) {   // even: wrk(2i-1)
+                TauRow rp = tau_row(i - 1, 0, wn, dyde, nyh, nyhm);
+                double2 gi = col[2 * (i - 1)];
+                prev = make_double2((gi.x - rp.a1 * prev.x) / ds[0][i - 1], (gi.y - rp.a1 * prev.y) / ds[0][i - 1]);
+                col[2 * (i - 1)] = prev;
+            }
+            prev = x1;
+            for (int i = 2; i <= nyh; ++i) {    // odd: wrk(2i)
+                TauRow rp = tau_row(i - 1, 1, wn, dyde, nyh, nyhm);
+                double2 gi = col[2 * (i - 1) + 1];
+                prev = make_double2((gi.x - rp.a1 * prev.x) / ds[1][i - 1], (gi.y - rp.a1 * prev.y) / ds[1][i - 1]);
+                col[2 * (i - 1) + 1] = prev;
+            }
+        }
+        if (kzero)
+            for (int i = 0; i < nyp; ++i) col[i] = make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    tile_store(u, sm, col0, ncol, nyp);
+}
+
+int kmm_internal_penta(kmm_ctx *ctx, double2 *u, double g, int ib, double at, double bt, double ab, double bb,
+                       const double2 *gt, const double2 *gb) {
+    const int ncols = ctx->nz * ctx->nxh;
+    static bool attr = false;
+    if (!attr) {
+        CK(cudaFuncSetAttribute(k_penta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(TILE * KMM_MAX_NYP * (sizeof(double2) + sizeof(double)))));
+        attr = true;
+    }
+    const size_t smem = tile_smem(ctx->nyp, 1) + sizeof(double) * TILE * 2 * (size_t)(ctx->nyhp + 1);
+    k_penta<<<(ncols + TILE - 1) / TILE, TPB, smem, ctx->stream>>>(
+        u, gt, gb, ctx->d_wavx, ctx->d_wavz, ncols, ctx->nz, ctx->nyp, g, ib, at, bt, ab, bb, ctx->dyde, ctx->h_c[0]);
+    CKL();
+    return KMM_OK;
+}
+
+extern "C" int kmm_penta(kmm_ctx *ctx, int u, double g, int ib, double at, double bt, double ab, double bb) {
+    if (!ctx || u < 0 || u >= KMM_NSPECTRAL) return KMM_ERR_ARG;
+    double2 *a = SPEC(ctx, u), *gt = SPEC(ctx, KMM_BCTOP), *gb = SPEC(ctx, KMM_BCBOT);
+    if (!a || !gt || !gb) return KMM_ERR_NOMEM;
+    return kmm_internal_penta(ctx, a, g, ib, at, bt, ab, bb, gt, gb);
+}
+
+// ---------------------------------------------------------------------------
+// uzero / psolve1d / p1d*, solvers.f90:1065-1493 (one thread: the (0,0) mode only)
+// ---------------------------------------------------------------------------
+__device__ void cderiv1d_dev(const double *f, double *df, int nyp, double dyde) {
+    const int ny = nyp - 1;
+    df[nyp - 1] = 0.0;
+    df[ny - 1] = 2.0 * (double)ny * f[nyp - 1] * dyde;
+    for (int i = ny - 1; i >= 1; --i) df[i - 1] = df[i + 1] + 2.0 * (double)i * f[i] * dyde;
+    df[0] = 0.5 * df[0];
+}
+
+__global__ void k_uzero(double *u0, const double *h1, const double *h1l, int nyp, double re, double dt, double th,
+                        double dyde, double at, double bt, double gtop, double ab, double bb, double gbot, double c0,
+                        double wz0, double *scratch) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int ny = nyp - 1, nyh = ny / 2, nyhm = nyh - 1, nyhp = nyh + 1;
+    const int L = KMM_MAX_NYP;
+    double *wrk1 = scratch, *t = scratch + L, *out = scratch + 2 * L;
+    double *cs[2] = {scratch + 3 * L, scratch + 4 * L}, *ds[2] = {scratch + 5 * L, scratch + 6 * L};
+    double *gs[2] = {scratch + 7 * L, scratch + 8 * L};
+    for (int i = 0; i < nyp; ++i) wrk1[i] = -re * u0[i] / (dt * th) - re * (3.0 * h1[i] - h1l[i]) / (2.0 * th);
+    if (th > 0.99) {
+        for (int i = 0; i < nyp; ++i) u0[i] = wrk1[i];
+    } else {
+        cderiv1d_dev(u0, t, nyp, dyde);
+        cderiv1d_dev(t, u0, nyp, dyde);
+        for (int i = 0; i < nyp; ++i) u0[i] = wrk1[i] - (1.0 - th) * u0[i] / th;
+    }
+    const double g = re / (th * dt);
+    // psolve1d, solvers.f90:1180-1245 with mixedbc1d (minus sign in tb, solvers.f90:1249-1269)
+    const double wn = wz0 * wz0 + 0.0 + g;
+    double f[2][2], s[2];
+    double *wrk = wrk1;   // reuse
+    s[0] = gtop;
+    s[1] = gbot;
+    for (int par = 0; par < 2; ++par) {
+        const int n = par == 0 ? nyhp : nyh, m = n - 1, mm1 = m - 1;
+        // RHS rows (p1devns / p1dodds)
+        for (int q = 0; q < nyp; ++q) wrk[q] = 0.0;
+        if (par == 0) {
+            for (int i = 2; i <= nyhm; ++i) {
+                int j = 2 * i - 2;
+                double rj1 = 1.0 / (double)(4 * j * (j - 1)), rj2 = 1.0 / (double)(2 * (j * j - 1)), rj3 = 1.0 / (double)(4 * j * (j + 1));
+                double cm = (j - 2 == 0) ? c0 : 1.0;
+                wrk[i - 1] = -cm * u0[j - 2] * rj1 + u0[j] * rj2 - u0[j + 2] * rj3;
+            }
+            int j = ny - 2;
+            double rj1 = 1.0 / (double)(4 * j * (j - 1)), rj2 = 1.0 / (double)(2 * (j * j - 1));
+            wrk[nyh - 1] = -u0[j - 2] * rj1 + u0[j] * rj2;
+            j = ny;
+            rj1 = 1.0 / (double)(4 * j * (j - 1));
+            wrk[nyhp - 1] = -u0[j - 2] * rj1;
+        } else {
+            for (int i = 2; i <= nyhm - 1; ++i) {
+                int j = 2 * i - 1;
+                double rj1 = 1.0 / (double)(4 * j * (j - 1)), rj2 = 1.0 / (double)(2 * (j * j - 1)), rj3 = 1.0 / (double)(4 * j * (j + 1));
+                wrk[i - 1] = -u0[j - 2] * rj1 + u0[j] * rj2 - u0[j + 2] * rj3;
+            }
+            int j = ny - 3;
+            double rj1 = 1.0 / (double)(4 * j * (j - 1)), rj2 = 1.0 / (double)(2 * (j * j - 1));
+            wrk[nyhm - 1] = -u0[j - 2] * rj1 + u0[j] * rj2;
+            j = ny - 1;
+            rj1 = 1.0 / (double)(4 * j * (j - 1));
+            wrk[nyh - 1] = -u0[j - 2] * rj1;
+        }
+        // p1dsolve
+        for (int i = 1; i <= m; ++i) { gs[par][i] = wrk[i - 1]; cs[par][i] = tau_row(i, par, wn, dyde, nyh, nyhm).a1; }
+        ds[par][m] = tau_row(m, par, wn, dyde, nyh, nyhm).a2;
+        gs[par][n] = wrk[n - 1];
+        for (int i = mm1; i >= 1; --i) {
+            TauRow ri = tau_row(i, par, wn, dyde, nyh, nyhm);
+            ds[par][i] = ri.a2 - ri.a3 * cs[par][i + 1] / ds[par][i + 1];
+            gs[par][i + 1] = gs[par][i + 1] - ri.a3 * gs[par][i + 2] / ds[par][i + 1];
+        }
+        for (int ipass = 1; ipass <= 2; ++ipass) {
+            const int js = ipass == 1 ? 2 : 1;
+            for (int q = 1; q <= n; ++q) {
+                int jj = par == 0 ? 2 * q - 1 : 2 * q, j1 = jj - 1;
+                double v = ipass == 2 ? at + dyde * bt * (double)(j1 * j1) : ab - dyde * bb * (double)(j1 * j1);
+                if (ipass == 1 && jj % 2 == 0) v = -v;
+                t[q - 1] = v;
+            }
+            double ff = t[m - 1] - t[n - 1] * cs[par][m] / ds[par][m];
+            double ss = s[js - 1] - t[n - 1] * gs[par][n] / ds[par][m];
+            for (int i = mm1; i >= 1; --i) {
+                ss = ss - ff * gs[par][i + 1] / ds[par][i];
+                ff = t[i - 1] - ff * cs[par][i] / ds[par][i];
+            }
+            s[js - 1] = ss;
+            f[js - 1][par] = ff;
+        }
+    }
+    const double det = f[0][0] * f[1][1] - f[1][0] * f[0][1];
+    out[0] = (s[0] * f[1][1] - s[1] * f[0][1]) / det;
+    out[1] = (s[1] * f[0][0] - s[0] * f[1][0]) / det;
+    for (int i = 2; i <= nyhp; ++i) {
+        int ii = 2 * i - 1;
+        out[ii - 1] = (gs[0][i] - cs[0][i - 1] * out[ii - 3]) / ds[0][i - 1];
+    }
+    for (int i = 2; i <= nyh; ++i) {
+        int ii = 2 * i;
+        out[ii - 1] = (gs[1][i] - cs[1][i - 1] * out[ii - 3]) / ds[1][i - 1];
+    }
+    for (int i = 0; i < nyp; ++i) u0[i] = out[i];
+}
+
+extern "C" int kmm_uzero(kmm_ctx *ctx, int uflag) {
+    if (!ctx || (uflag != 1 && uflag != 3)) return KMM_ERR_ARG;
+    double *u0 = REAL(ctx, uflag == 1 ? KMM_U0 : KMM_W0);
+    double *h1 = REAL(ctx, uflag == 1 ? KMM_H1N : KMM_H3N);
+    double *h1l = REAL(ctx, uflag == 1 ? KMM_H1NM1 : KMM_H3NM1);
+    if (!u0 || !h1 || !h1l) return KMM_ERR_NOMEM;
+    // uflag 3 passes btu, as the reference does (solvers.f90:1173)
+    if (uflag == 1)
+        k_uzero<<<1, 1, 0, ctx->stream>>>(u0, h1, h1l, ctx->nyp, ctx->re, ctx->dt, ctx->theta, ctx->dyde, ctx->atu,
+                                          ctx->btu, ctx->gtu, ctx->abu, ctx->bbu, ctx->gbu, ctx->h_c[0], ctx->h_wavz[0], ctx->d_scratch);
+    else
+        k_uzero<<<1, 1, 0, ctx->stream>>>(u0, h1, h1l, ctx->nyp, ctx->re, ctx->dt, ctx->theta, ctx->dyde, ctx->atw,
+                                          ctx->btu, ctx->gtw, ctx->abw, ctx->bbw, ctx->gbw, ctx->h_c[0], ctx->h_wavz[0], ctx->d_scratch);
+    CKL();
+    return KMM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// pointwise spectral kernels
+// ---------------------------------------------------------------------------
+#define GRID_LOOP(n) for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < (n); idx += (size_t)gridDim.x * blockDim.x)
+#define DECOMP()                              \
+    const int i = (int)(idx % nyp);           \
+    const size_t jk = idx / nyp;              \
+    const int j = (int)(jk % nz);             \
+    const int k = (int)(jk / nz);             \
+    (void)i; (void)j; (void)k;
+
+// phirhs first part, solvers.f90:633-664: wrkc = -re var/(dt th) v - re var/(2 th)(3 fn - fnm1) [+ (1-th) w2 v/th]
+__global__ void k_phirhs_a(double2 *__restrict__ v, const double2 *__restrict__ fn, const double2 *__restrict__ fnm1,
+                           double2 *__restrict__ wrkc, const double *__restrict__ wavx, const double *__restrict__ wavz,
+                           size_t n, int nyp, int nz, double re, double var, double dt, double th) {
+    const double a = -re * var / (dt * th), b = re * var / (2.0 * th);
+    GRID_LOOP(n) {
+        DECOMP();
+        double2 vv = v[idx], f = fn[idx], fm = fnm1[idx];
+        double2 w;
+        w.x = a * vv.x - b * (3.0 * f.x - fm.x);
+        w.y = a * vv.y - b * (3.0 * f.y - fm.y);
+        if (th > 0.99) { vv = w; v[idx] = w; }
+        const double w2 = wavz[j] * wavz[j] + wavx[k] * wavx[k];
+        const double c = (1.0 - th) * w2;
+        w.x = w.x + c * vv.x / th;
+        w.y = w.y + c * vv.y / th;
+        wrkc[idx] = w;
+    }
+}
+
+// phirhs last part, solvers.f90:668-675: v = wrkc - (1-th) v''/th
+__global__ void k_phirhs_b(double2 *__restrict__ v, const double2 *__restrict__ wrkc, size_t n, double th) {
+    GRID_LOOP(n) {
+        double2 w = wrkc[idx], d = v[idx];
+        v[idx] = make_double2(w.x - (1.0 - th) * d.x / th, w.y - (1.0 - th) * d.y / th);
+    }
+}
+
+__global__ void k_zero_wall(double2 *a, double2 *b, size_t n) {
+    GRID_LOOP(n) { a[idx] = make_double2(0.0, 0.0); b[idx] = make_double2(0.0, 0.0); }
+}
+
+extern "C" int kmm_phirhs(kmm_ctx *ctx, int v, int fn, int fnm1, double var) {
+    if (!ctx || v >= KMM_NSPECTRAL || fn >= KMM_NSPECTRAL || fnm1 >= KMM_NSPECTRAL) return KMM_ERR_ARG;
+    double2 *V = SPEC(ctx, v), *F = SPEC(ctx, fn), *FM = SPEC(ctx, fnm1);
+    if (!V || !F || !FM) return KMM_ERR_NOMEM;
+    return kmm_internal_phirhs(ctx, V, F, FM, var);
+}
+
+int kmm_internal_phirhs(kmm_ctx *ctx, double2 *V, const double2 *F, const double2 *FM, double var) {
+    double2 *bt = SPEC(ctx, KMM_BCTOP), *bb = SPEC(ctx, KMM_BCBOT);
+    if (!bt || !bb) return KMM_ERR_NOMEM;
+    const size_t nw = (size_t)ctx->nz * ctx->nxh, n = ctx->nspec;
+    k_zero_wall<<<kmm_blocks(nw, 256), 256, 0, ctx->stream>>>(bt, bb, nw);
+    CKL();
+    double2 *wrkc = ctx->wrk[0], *wrk1 = ctx->wrk[1];
+    k_phirhs_a<<<kmm_blocks(n, 256), 256, 0, ctx->stream>>>(V, F, FM, wrkc, ctx->d_wavx, ctx->d_wavz, n, ctx->nyp,
+                                                            ctx->nz, ctx->re, var, ctx->dt, ctx->theta);
+    CKL();
+    RET(kmm_internal_cderiv(ctx, V, wrk1));
+    RET(kmm_internal_cderiv(ctx, wrk1, V));
+    k_phirhs_b<<<kmm_blocks(n, 256), 256, 0, ctx->stream>>>(V, wrkc, n, ctx->theta);
+    CKL();
+    return KMM_OK;
+}
+
+// main_dns.f90:363-375
+__global__ void k_phi(double2 *__restrict__ v, const double2 *__restrict__ d2, const double *__restrict__ wavx,
+                      const double *__restrict__ wavz, size_t n, int nyp, int nz) {
+    GRID_LOOP(n) {
+        DECOMP();
+        const double wn2 = wavx[k] * wavx[k] + wavz[j] * wavz[j];
+        double2 a = d2[idx], b = v[idx];
+        v[idx] = make_double2(a.x - wn2 * b.x, a.y - wn2 * b.y);
+    }
+}
+
+extern "C" int kmm_phi_from_v(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    double2 *v = SPEC(ctx, KMM_V);
+    if (!v) return KMM_ERR_NOMEM;
+    RET(kmm_internal_cderiv(ctx, v, ctx->wrk[1]));
+    RET(kmm_internal_cderiv(ctx, ctx->wrk[1], ctx->wrk[0]));
+    k_phi<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(v, ctx->wrk[0], ctx->d_wavx, ctx->d_wavz, ctx->nspec,
+                                                                ctx->nyp, ctx->nz);
+    CKL();
+    return KMM_OK;
+}
+
+// influence-matrix combination, main_dns.f90:456-466
+__global__ void k_influence(double2 *__restrict__ v, const double2 *__restrict__ wrkc, const double2 *__restrict__ gf1,
+                            const double2 *__restrict__ gf2, const double2 *__restrict__ d1b,
+                            const double2 *__restrict__ d1t, const double2 *__restrict__ d2b,
+                            const double2 *__restrict__ d2t, const double2 *__restrict__ den, double2 *c1o,
+                            double2 *c2o, int ncols, int nyp, int iyb, int iyt) {
+    const int col = blockIdx.x;
+    if (col >= ncols) return;
+    const double2 wb = wrkc[(size_t)col * nyp + iyb - 1], wt = wrkc[(size_t)col * nyp + iyt - 1];
+    const double2 c1 = cdiv(csub(cmul(wb, d2t[col]), cmul(wt, d2b[col])), den[col]);
+    const double2 c2 = cdiv(csub(cmul(wt, d1b[col]), cmul(wb, d1t[col])), den[col]);
+    if (threadIdx.x == 0) { c1o[col] = c1; c2o[col] = c2; }
+    for (int i = threadIdx.x; i < nyp; i += blockDim.x) {
+        size_t x = (size_t)col * nyp + i;
+        double2 a = cmul(c1, gf1[x]), b = cmul(c2, gf2[x]);
+        double2 vv = v[x];
+        v[x] = make_double2(vv.x + a.x + b.x, vv.y + a.y + b.y);
+    }
+}
+
+extern "C" int kmm_influence(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    double2 *v = SPEC(ctx, KMM_V), *wrkc = ctx->wrk[2], *wrk1 = ctx->wrk[3];
+    const int iyb = 2, iyt = 4;
+    if (ctx->nb == 1) {
+        RET(kmm_internal_wallderiv(ctx, v, 1, 0, wrkc, iyb));
+        if (ctx->nt == 1) { RET(kmm_internal_wallderiv(ctx, v, 1, 1, wrkc, iyt)); }
+        else { RET(kmm_internal_cderiv(ctx, v, wrk1)); RET(kmm_internal_wallderiv(ctx, wrk1, 1, 1, wrkc, iyt)); }
+    } else {
+        RET(kmm_internal_cderiv(ctx, v, wrk1));
+        RET(kmm_internal_wallderiv(ctx, wrk1, 1, 0, wrkc, iyb));
+        if (ctx->nt == 1) { RET(kmm_internal_wallderiv(ctx, v, 1, 1, wrkc, iyt)); }
+        else { RET(kmm_internal_cderiv(ctx, v, wrk1)); RET(kmm_internal_wallderiv(ctx, wrk1, 1, 1, wrkc, iyt)); }
+    }
+    const int ncols = ctx->nz * ctx->nxh;
+    k_influence<<<ncols, 128, 0, ctx->stream>>>(v, wrkc, SPEC(ctx, KMM_GF1), SPEC(ctx, KMM_GF2), SPEC(ctx, KMM_DNV1B),
+                                               SPEC(ctx, KMM_DNV1T), SPEC(ctx, KMM_DNV2B), SPEC(ctx, KMM_DNV2T),
+                                               SPEC(ctx, KMM_DENOM), SPEC(ctx, KMM_C1), SPEC(ctx, KMM_C2), ncols,
+                                               ctx->nyp, iyb, iyt);
+    CKL();
+    return KMM_OK;
+}
+
+// veloc, solvers.f90:1576-1659 (wrkc = dv/dy)
+__global__ void k_veloc(double2 *__restrict__ u, double2 *__restrict__ v, double2 *__restrict__ w,
+                        const double2 *__restrict__ dv, const double2 *__restrict__ omy, const double *__restrict__ u0,
+                        const double *__restrict__ w0, const double *__restrict__ wavx, const double *__restrict__ wavz,
+                        size_t n, int nyp, int nz) {
+    GRID_LOOP(n) {
+        DECOMP();
+        const double2 d = dv[idx], o = omy[idx];
+        if (k > 0) {
+            const double w2 = wavx[k] * wavx[k] + wavz[j] * wavz[j];
+            // u = -(-i kx dv + i kz om)/w2 ; w = -(-i kz dv - i kx om)/w2
+            double2 a = cimul(d, -wavx[k]), b = cimul(o, wavz[j]);
+            double2 s = cadd(a, b);
+            u[idx] = make_double2(-s.x / w2, -s.y / w2);
+            double2 c = cimul(d, -wavz[j]), e = cimul(o, wavx[k]);
+            double2 t = csub(c, e);
+            w[idx] = make_double2(-t.x / w2, -t.y / w2);
+        } else if (j > 0) {
+            const double w2 = wavz[j] * wavz[j];
+            double2 b = cimul(o, wavz[j]);
+            u[idx] = make_double2(-b.x / w2, -b.y / w2);
+            double2 c = cimul(d, -wavz[j]);
+            w[idx] = make_double2(-c.x / w2, -c.y / w2);
+        } else {
+            u[idx] = make_double2(u0[i], 0.0);
+            v[idx] = make_double2(0.0, 0.0);
+            w[idx] = make_double2(w0[i], 0.0);
+        }
+    }
+}
+
+extern "C" int kmm_veloc(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    double2 *u = SPEC(ctx, KMM_U), *v = SPEC(ctx, KMM_V), *w = SPEC(ctx, KMM_W), *omy = SPEC(ctx, KMM_OMY);
+    double *u0 = REAL(ctx, KMM_U0), *w0 = REAL(ctx, KMM_W0);
+    if (!u || !v || !w || !omy || !u0 || !w0) return KMM_ERR_NOMEM;
+    RET(kmm_internal_cderiv(ctx, v, ctx->wrk[0]));
+    k_veloc<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(u, v, w, ctx->wrk[0], omy, u0, w0, ctx->d_wavx,
+                                                                  ctx->d_wavz, ctx->nspec, ctx->nyp, ctx->nz);
+    CKL();
+    return KMM_OK;
+}
+
+// vort, solvers.f90:1663-1722: omz = i kx v - du/dy; omx = dw/dy - i kz v
+__global__ void k_vort(const double2 *__restrict__ v, double2 *__restrict__ omx, double2 *__restrict__ omz,
+                       const double *__restrict__ wavx, const double *__restrict__ wavz, size_t n, int nyp, int nz) {
+    GRID_LOOP(n) {
+        DECOMP();
+        const double2 vv = v[idx];
+        omz[idx] = csub(cimul(vv, wavx[k]), omz[idx]);
+        omx[idx] = csub(omx[idx], cimul(vv, wavz[j]));
+    }
+}
+
+extern "C" int kmm_vort(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    double2 *u = SPEC(ctx, KMM_U), *v = SPEC(ctx, KMM_V), *w = SPEC(ctx, KMM_W);
+    double2 *omx = SPEC(ctx, KMM_OMX), *omz = SPEC(ctx, KMM_OMZ);
+    if (!u || !v || !w || !omx || !omz) return KMM_ERR_NOMEM;
+    RET(kmm_internal_cderiv(ctx, u, omz));
+    RET(kmm_internal_cderiv(ctx, w, omx));
+    k_vort<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(v, omx, omz, ctx->d_wavx, ctx->d_wavz, ctx->nspec,
+                                                                 ctx->nyp, ctx->nz);
+    CKL();
+    return KMM_OK;
+}
+
+// gradv, derivatives.f90:6-86
+__global__ void k_gradv(const double2 *__restrict__ u, const double2 *__restrict__ v, const double2 *__restrict__ w,
+                        double2 *u11, double2 *u21, double2 *u31, double2 *u13, double2 *u23, double2 *u33,
+                        double2 *Lu, double2 *Lv, double2 *Lw, const double2 *__restrict__ d2u,
+                        const double2 *__restrict__ d2v, const double2 *__restrict__ d2w,
+                        const double *__restrict__ wavx, const double *__restrict__ wavz, size_t n, int nyp, int nz) {
+    GRID_LOOP(n) {
+        DECOMP();
+        const double kx = wavx[k], kz = wavz[j];
+        const double wn2 = kx * kx + kz * kz;
+        const double2 a = u[idx], b = v[idx], c = w[idx];
+        u11[idx] = cimul(a, kx);
+        u21[idx] = cimul(b, kx);
+        u31[idx] = cimul(c, kx);
+        u13[idx] = cimul(a, kz);
+        u23[idx] = cimul(b, kz);
+        u33[idx] = cimul(c, kz);
+        double2 p = d2u[idx], q = d2v[idx], r = d2w[idx];
+        Lu[idx] = make_double2(p.x - wn2 * a.x, p.y - wn2 * a.y);
+        Lv[idx] = make_double2(q.x - wn2 * b.x, q.y - wn2 * b.y);
+        Lw[idx] = make_double2(r.x - wn2 * c.x, r.y - wn2 * c.y);
+    }
+}
+
+extern "C" int kmm_gradv(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    double2 *u = SPEC(ctx, KMM_U), *v = SPEC(ctx, KMM_V), *w = SPEC(ctx, KMM_W);
+    double2 *u12 = SPEC(ctx, KMM_U12), *u22 = SPEC(ctx, KMM_U22), *u32 = SPEC(ctx, KMM_U32);
+    RET(kmm_internal_cderiv(ctx, u, u12));
+    RET(kmm_internal_cderiv(ctx, v, u22));
+    RET(kmm_internal_cderiv(ctx, w, u32));
+    RET(kmm_internal_cderiv(ctx, u12, ctx->wrk[0]));
+    RET(kmm_internal_cderiv(ctx, u22, ctx->wrk[1]));
+    RET(kmm_internal_cderiv(ctx, u32, ctx->wrk[2]));
+    k_gradv<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(
+        u, v, w, SPEC(ctx, KMM_U11), SPEC(ctx, KMM_U21), SPEC(ctx, KMM_U31), SPEC(ctx, KMM_U13), SPEC(ctx, KMM_U23),
+        SPEC(ctx, KMM_U33), SPEC(ctx, KMM_LU), SPEC(ctx, KMM_LV), SPEC(ctx, KMM_LW), ctx->wrk[0], ctx->wrk[1],
+        ctx->wrk[2], ctx->d_wavx, ctx->d_wavz, ctx->nspec, ctx->nyp, ctx->nz);
+    CKL();
+    return KMM_OK;
+}
+
+// i kx a -> dx, i kz a -> dz (gradscl / derivscji x,z parts)
+__global__ void k_dxdz(const double2 *__restrict__ a, double2 *__restrict__ dx, double2 *__restrict__ dz,
+                       const double *__restrict__ wavx, const double *__restrict__ wavz, size_t n, int nyp, int nz) {
+    GRID_LOOP(n) {
+        DECOMP();
+        const double2 v = a[idx];
+        dx[idx] = cimul(v, wavx[k]);
+        dz[idx] = cimul(v, wavz[j]);
+    }
+}
+
+extern "C" int kmm_gradscl(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    double2 *s = SPEC(ctx, KMM_SCALAR);
+    RET(kmm_internal_cderiv(ctx, s, SPEC(ctx, KMM_SCLY)));
+    k_dxdz<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(s, SPEC(ctx, KMM_SCLX), SPEC(ctx, KMM_SCLZ),
+                                                                 ctx->d_wavx, ctx->d_wavz, ctx->nspec, ctx->nyp, ctx->nz);
+    CKL();
+    return KMM_OK;
+}
+
+extern "C" int kmm_derivscji(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    for (int ij = 0; ij < 9; ++ij) {
+        double2 *cf = SPEC(ctx, KMM_C11 + ij);
+        RET(kmm_internal_cderiv(ctx, cf, SPEC(ctx, KMM_DC111 + 3 * ij + 1)));
+        k_dxdz<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(cf, SPEC(ctx, KMM_DC111 + 3 * ij),
+                                                                     SPEC(ctx, KMM_DC111 + 3 * ij + 2), ctx->d_wavx,
+                                                                     ctx->d_wavz, ctx->nspec, ctx->nyp, ctx->nz);
+        CKL();
+    }
+    return KMM_OK;
+}
+
+// nonlin, solvers.f90:1497-1572
+__global__ void k_nonlin_a(const double2 *__restrict__ omz, const double2 *__restrict__ gn, double2 *__restrict__ wrkc,
+                           const double *__restrict__ wavx, const double *__restrict__ wavz, size_t n, int nyp, int nz) {
+    GRID_LOOP(n) {
+        DECOMP();
+        const double2 o = omz[idx], g = gn[idx];
+        double2 s = make_double2(wavz[j] * o.x + wavx[k] * g.x, wavz[j] * o.y + wavx[k] * g.y);
+        wrkc[idx] = make_double2(-s.y, s.x);
+    }
+}
+
+__global__ void k_nonlin_b(double2 *__restrict__ fn, double2 *__restrict__ gn, const double2 *__restrict__ omz,
+                           const double2 *__restrict__ d, const double *__restrict__ wavx,
+                           const double *__restrict__ wavz, size_t n, int nyp, int nz) {
+    GRID_LOOP(n) {
+        DECOMP();
+        const double w2 = -wavx[k] * wavx[k] - wavz[j] * wavz[j];
+        double2 f = fn[idx], dd = d[idx];
+        fn[idx] = make_double2(w2 * f.x - dd.x, w2 * f.y - dd.y);
+        const double2 g = gn[idx], o = omz[idx];
+        double2 s = make_double2(wavz[j] * g.x - wavx[k] * o.x, wavz[j] * g.y - wavx[k] * o.y);
+        gn[idx] = make_double2(-s.y, s.x);
+    }
+}
+
+extern "C" int kmm_nonlin(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    double2 *fn = SPEC(ctx, KMM_FN), *gn = SPEC(ctx, KMM_GN), *omz = SPEC(ctx, KMM_OMZ);
+    k_nonlin_a<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(omz, gn, ctx->wrk[0], ctx->d_wavx, ctx->d_wavz,
+                                                                     ctx->nspec, ctx->nyp, ctx->nz);
+    CKL();
+    RET(kmm_internal_cderiv(ctx, ctx->wrk[0], ctx->wrk[1]));
+    k_nonlin_b<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(fn, gn, omz, ctx->wrk[1], ctx->d_wavx,
+                                                                     ctx->d_wavz, ctx->nspec, ctx->nyp, ctx->nz);
+    CKL();
+    return KMM_OK;
+}
+
+// spectral smoothing, main_dns.f90:710-745 (factors precomputed per column / per y with the
+// reference's formulas; exp of an argument evaluated identically on every call)
+struct PtrList16 { double2 *p[16]; };
+
+__global__ void k_filter(PtrList16 ptrs, int nptr, size_t n, int nyp, int nz, int nzh, int ny) {
+    GRID_LOOP(n) {
+        DECOMP();
+        const int j1 = j + 1;
+        const int jj = (j1 > nzh) ? nz - j1 + 1 : j1 - 1;
+        const double zr = (double)jj / (double)nzh, yr = (double)i / (double)ny;
+        double z2 = zr * zr, z4 = z2 * z2, z8 = z4 * z4;
+        double y2 = yr * yr, y4 = y2 * y2, y8 = y4 * y4;
+        const double zs = exp(-3.0 * (z8 * z2));
+        const double ys = exp(-3.0 * (y8 * y2));
+        for (int p = 0; p < nptr; ++p) {
+            double2 a = ptrs.p[p][idx];
+            a = make_double2(a.x * zs * ys, a.y * zs * ys);
+            ptrs.p[p][idx] = a;
+        }
+    }
+}
+
+extern "C" int kmm_filter(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    PtrList16 h;
+    int np = 0;
+    h.p[np++] = SPEC(ctx, KMM_OMZ);
+    h.p[np++] = SPEC(ctx, KMM_GN);
+    h.p[np++] = SPEC(ctx, KMM_FN);
+    if (ctx->p.scalar_on) h.p[np++] = SPEC(ctx, KMM_SCN);
+    if (ctx->p.polymer_on) {
+        for (int m = 0; m < 6; ++m) h.p[np++] = SPEC(ctx, KMM_C11N + m);
+        for (int m = 0; m < 6; ++m) h.p[np++] = SPEC(ctx, KMM_STR11N + m);
+    }
+    for (int q = 0; q < np; ++q)
+        if (!h.p[q]) return KMM_ERR_NOMEM;
+    k_filter<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(h, np, ctx->nspec, ctx->nyp, ctx->nz, ctx->nzh,
+                                                                   ctx->ny);
+    CKL();
+    return KMM_OK;
+}
+
+// polyNL, helpers.f90:610-674 -> scratch NL fields in ctx->wrk? (six fields: use T1..T3 + WRKC/WRK1 is not enough)
+__global__ void k_polynl(double2 *nl, const double2 *cn, const double2 *cnm1, const double2 *sn, const double2 *snm1,
+                         size_t n, double tinv) {
+    GRID_LOOP(n) {
+        double2 a = cn[idx], b = sn[idx], c = cnm1[idx], d = snm1[idx];
+        nl[idx] = make_double2(3.0 * (a.x - tinv * b.x) - (c.x - tinv * d.x), 3.0 * (a.y - tinv * b.y) - (c.y - tinv * d.y));
+    }
+}
+
+__global__ void k_polyforce(const double2 *s11, const double2 *s12, const double2 *s13, const double2 *s22,
+                            const double2 *s23, const double2 *s33, const double2 *w1, const double2 *w2,
+                            const double2 *w3, double2 *t1, double2 *t2, double2 *t3, const double *wavx,
+                            const double *wavz, size_t n, int nyp, int nz) {
+    GRID_LOOP(n) {
+        DECOMP();
+        const double kx = wavx[k], kz = wavz[j];
+        double2 a = cimul(make_double2(kx * s11[idx].x + kz * s13[idx].x, kx * s11[idx].y + kz * s13[idx].y), 1.0);
+        double2 b = cimul(make_double2(kx * s12[idx].x + kz * s23[idx].x, kx * s12[idx].y + kz * s23[idx].y), 1.0);
+        double2 c = cimul(make_double2(kx * s13[idx].x + kz * s33[idx].x, kx * s13[idx].y + kz * s33[idx].y), 1.0);
+        t1[idx] = cadd(a, w1[idx]);
+        t2[idx] = cadd(b, w2[idx]);
+        t3[idx] = cadd(c, w3[idx]);
+    }
+}
+
+extern "C" int kmm_polyforce(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    double2 *s11 = SPEC(ctx, KMM_QP11), *s12 = SPEC(ctx, KMM_QP12), *s13 = SPEC(ctx, KMM_QP13);
+    double2 *s22 = SPEC(ctx, KMM_QP22), *s23 = SPEC(ctx, KMM_QP23), *s33 = SPEC(ctx, KMM_QP33);
+    RET(kmm_internal_cderiv(ctx, s12, ctx->wrk[0]));
+    RET(kmm_internal_cderiv(ctx, s22, ctx->wrk[1]));
+    RET(kmm_internal_cderiv(ctx, s23, ctx->wrk[2]));
+    k_polyforce<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(
+        s11, s12, s13, s22, s23, s33, ctx->wrk[0], ctx->wrk[1], ctx->wrk[2], SPEC(ctx, KMM_T1), SPEC(ctx, KMM_T2),
+        SPEC(ctx, KMM_T3), ctx->d_wavx, ctx->d_wavz, ctx->nspec, ctx->nyp, ctx->nz);
+    CKL();
+    return KMM_OK;
+}
+
+__global__ void k_subforce(double2 *gn, double2 *fn, double2 *omz, const double2 *t1, const double2 *t2,
+                           const double2 *t3, size_t n) {
+    GRID_LOOP(n) {
+        gn[idx] = cadd(gn[idx], t1[idx]);
+        fn[idx] = cadd(fn[idx], t2[idx]);
+        omz[idx] = cadd(omz[idx], t3[idx]);
+    }
+}
+
+extern "C" int kmm_subforce(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    k_subforce<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(SPEC(ctx, KMM_GN), SPEC(ctx, KMM_FN),
+                                                                     SPEC(ctx, KMM_OMZ), SPEC(ctx, KMM_T1),
+                                                                     SPEC(ctx, KMM_T2), SPEC(ctx, KMM_T3), ctx->nspec);
+    CKL();
+    return KMM_OK;
+}
+
+// y <- a*x  (the 2.0*cNL argument of main_dns.f90:248-261)
+__global__ void k_scale_copy(double2 *y, const double2 *x, double a, size_t n) {
+    GRID_LOOP(n) { y[idx] = make_double2(a * x[idx].x, a * x[idx].y); }
+}
+
+int kmm_internal_axpy_spec(kmm_ctx *ctx, double2 *y, const double2 *x, double a) {
+    k_scale_copy<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(y, x, a, ctx->nspec);
+    CKL();
+    return KMM_OK;
+}
+
+// polyNL into six caller-provided buffers
+int kmm_internal_polynl(kmm_ctx *ctx, double2 *const *nl) {
+    const double tinv = 1.0 / ctx->p.tpoly;
+    for (int m = 0; m < 6; ++m) {
+        k_polynl<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(nl[m], SPEC(ctx, KMM_C11N + m),
+                                                                       SPEC(ctx, KMM_C11NM1 + m), SPEC(ctx, KMM_STR11N + m),
+                                                                       SPEC(ctx, KMM_STR11NM1 + m), ctx->nspec, tinv);
+        CKL();
+    }
+    return KMM_OK;
+}
+
+// a(0,0 mode, Chebyshev 0) = value, everything else 0 (xyzfft of a constant field)
+__global__ void k_constant_mode(double2 *a, size_t n, double value) {
+    GRID_LOOP(n) { a[idx] = make_double2(idx == 0 ? value : 0.0, 0.0); }
+}
+
+int kmm_internal_set_constant_mode(kmm_ctx *ctx, double2 *a, double value) {
+    k_constant_mode<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(a, ctx->nspec, value);
+    CKL();
+    return KMM_OK;
+}

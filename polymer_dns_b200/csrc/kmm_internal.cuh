@@ -1,0 +1,232 @@
+// kmm_internal.cuh -- shared definitions of the B200 KMM library (context, helpers, device FFT).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "../../include/kmm.h"
+
+#define KMM_MAXF 800
+#define KMM_MAX_FFT_FACTORS 16
+#define KMM_MAX_NYP 1025
+#define KMM_TIMER_RECORDS 4096
+
+// ---------------------------------------------------------------------------
+// error handling: every CUDA call goes through CK, which records the message
+// in the context and returns KMM_ERR_CUDA from the enclosing function.
+// ---------------------------------------------------------------------------
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e__ = (call);                                                             \
+        if (e__ != cudaSuccess) {                                                             \
+            kmm_set_error(ctx, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e__)); \
+            return KMM_ERR_CUDA;                                                              \
+        }                                                                                     \
+    } while (0)
+
+#define CKL()                                \
+    do {                                     \
+        CK(cudaGetLastError());              \
+        ctx->launches++;                     \
+    } while (0)
+#define RET(x) do { int r__ = (x); if (r__) return r__; } while (0)
+
+// FFT plan: n = product of fac[] (radices 4, 2, 3, 5); tw[m] = exp(-2 pi i m / n) in FP64
+struct DevPlan {
+    int n, nf;
+    int fac[KMM_MAX_FFT_FACTORS];
+    const double2 *tw;
+};
+
+struct kmm_ctx {
+    kmm_params p;
+    int device;
+    cudaStream_t stream;
+    // grid (grid_size.f90:1-47, run-time here)
+    int nx, ny, nz, nyp, nym, nxh, nyh, nzh, nyhp, nyhm, mx, mz;
+    size_t nspec;   // nyp*nz*nxh
+    size_t nphys;   // nyp*mz*mx
+    // COMMON /solver/, /flow/, /domain/ values (main_dns.f90:934-1165)
+    double re, dt, theta, gain, ugain, dyde, alpha, beta, dPdx, xl, yl, zl, uinf, pi;
+    double atu, btu, gtu, abu, bbu, gbu, atw, btw, gtw, abw, bbw, gbw;
+    int nt, nb;
+    double p1t, p1b, p2t, p2b;
+    int substep;
+    int it;
+    int kmaxsurf;
+    // host and device copies of wavenumbers, Chebyshev weights, grid
+    double *h_wavx, *h_wavz, *h_c, *h_ycoord, *h_seght;
+    double *d_wavx, *d_wavz, *d_c, *d_ycoord, *d_seght;
+    double h_fspread[10][10];
+    double *d_fspread;
+    // field mirrors
+    void *f[KMM_MAXF];
+    // scratch
+    double2 *wrk[6];            // spectral-size scratch
+    double2 *pl_in, *pl_out;     // y-physical spectral-xz planes (fields x nyp x nxh x nz)
+    double2 *q_in, *q_out;       // after the z transform (fields x nyp x mz x nxh)
+    size_t pl_in_fields, pl_out_fields;
+    double *d_cfl;               // nyp
+    int *d_status;               // device-raised status
+    double *d_umax;              // scratch for |u| max (per plane)
+    double *d_scratch;           // 9*KMM_MAX_NYP doubles for the (0,0)-mode solver
+    double *scsource;            // (nyp,mz,mx) scalar source (scl_flag = 2)
+    DevPlan py2, pmz, pmx, pnx, pnz;
+    double2 *tw_store[5];
+    kmm_stats stats;
+    char err[512];
+    // instrumentation: kernel launches issued, and CUDA-event stage timers (bench / profiling)
+    long long launches;
+    int timing_on;
+    int tm_n;
+    int tm_stage[KMM_TIMER_RECORDS];
+    cudaEvent_t tm_ev[2 * KMM_TIMER_RECORDS];
+    int tm_ev_ready;
+    cudaEvent_t user_ev[16];
+};
+
+void kmm_tic(kmm_ctx *ctx);
+void kmm_toc(kmm_ctx *ctx, int stage);
+
+void kmm_set_error(kmm_ctx *ctx, const char *fmt, ...);
+
+// field helpers (kmm_ctx.cu)
+int kmm_field_info(const kmm_ctx *ctx, int field, size_t *nelem, int *eb);
+void *kmm_field_ptr(kmm_ctx *ctx, int field);   // allocates (zeroed) on first use, NULL on failure
+static inline double2 *SPEC(kmm_ctx *ctx, int f) { return (double2 *)kmm_field_ptr(ctx, f); }
+static inline double *REAL(kmm_ctx *ctx, int f) { return (double *)kmm_field_ptr(ctx, f); }
+
+// internal entry points shared between translation units
+int kmm_internal_cderiv(kmm_ctx *ctx, const double2 *f, double2 *df);
+int kmm_internal_norm(kmm_ctx *ctx, double2 *a);
+int kmm_internal_wallderiv(kmm_ctx *ctx, const double2 *f, int order, int wall, double2 *out, int iy);
+int kmm_internal_solve(kmm_ctx *ctx, double2 *u, double g, int ib, const double2 *bct, const double2 *bcb);
+int kmm_internal_penta(kmm_ctx *ctx, double2 *u, double g, int ib, double at, double bt, double ab, double bb,
+                       const double2 *gt, const double2 *gb);
+int kmm_internal_axpy_spec(kmm_ctx *ctx, double2 *y, const double2 *x, double a);
+int kmm_internal_set_constant_mode(kmm_ctx *ctx, double2 *a, double value);
+int kmm_plan_init(kmm_ctx *ctx, DevPlan *p, int n, int slot);
+int kmm_ensure_plane_buffers(kmm_ctx *ctx, int nin, int nout);
+// (nyp,mz,mx) host array <-> internal [y][z][x] device array (one of host_src / host_dst is NULL)
+int kmm_phys_layout(kmm_ctx *ctx, int field, void *dev, const void *host_src, void *host_dst);
+int kmm_internal_polynl(kmm_ctx *ctx, double2 *const *nl);
+int kmm_internal_phirhs(kmm_ctx *ctx, double2 *V, const double2 *F, const double2 *FM, double var);
+
+// ---------------------------------------------------------------------------
+// complex helpers on double2
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ double2 cdivr(double2 a, double s) { return make_double2(a.x / s, a.y / s); }
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+// i*s*a for real s
+__host__ __device__ __forceinline__ double2 cimul(double2 a, double s) { return make_double2(-s * a.y, s * a.x); }
+// complex division as C99 does for finite operands (a/b)
+__host__ __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+    double den = b.x * b.x + b.y * b.y;
+    return make_double2((a.x * b.x + a.y * b.y) / den, (a.y * b.x - a.x * b.y) / den);
+}
+
+// ---------------------------------------------------------------------------
+// shared-memory Stockham FFT over a batch of sequences.
+//   a, b: two smem buffers; sequence s occupies [s*ld, s*ld + n).
+//   sign -1: exp(-2 pi i jk/n) (FFTW_FORWARD), +1: exp(+...) (FFTW_BACKWARD).
+//   All threads of the block must call it; returns the buffer holding the result.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void radix_dft(int R, double2 *v, int sign) {
+    if (R == 2) {
+        double2 a0 = v[0], a1 = v[1];
+        v[0] = cadd(a0, a1);
+        v[1] = csub(a0, a1);
+    } else if (R == 4) {
+        double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+        double2 b0 = cadd(v[1], v[3]);
+        double2 d = csub(v[1], v[3]);
+        double2 b1 = sign < 0 ? make_double2(d.y, -d.x) : make_double2(-d.y, d.x);  // sign*i*d
+        v[0] = cadd(a0, b0);
+        v[1] = cadd(a1, b1);
+        v[2] = csub(a0, b0);
+        v[3] = csub(a1, b1);
+    } else if (R == 3) {
+        const double s3 = 0.86602540378443864676 * (double)sign;
+        double2 t1 = cadd(v[1], v[2]);
+        double2 t2 = csub(v[0], cscale(t1, 0.5));
+        double2 d = csub(v[1], v[2]);
+        double2 t3 = make_double2(s3 * d.x, s3 * d.y);
+        double2 o0 = cadd(v[0], t1);
+        v[1] = make_double2(t2.x - t3.y, t2.y + t3.x);   // t2 + i t3
+        v[2] = make_double2(t2.x + t3.y, t2.y - t3.x);   // t2 - i t3
+        v[0] = o0;
+    } else {  // R == 5
+        const double c5a = 0.30901699437494742410, c5b = -0.80901699437494742410;
+        const double s5a = 0.95105651629515357212 * (double)sign, s5b = 0.58778525229247312917 * (double)sign;
+        double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+        double2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+        double2 o0 = cadd(v[0], cadd(t1, t2));
+        double2 r1 = cadd(v[0], cadd(cscale(t1, c5a), cscale(t2, c5b)));
+        double2 r2 = cadd(v[0], cadd(cscale(t1, c5b), cscale(t2, c5a)));
+        double2 m1 = cadd(cscale(t3, s5a), cscale(t4, s5b));
+        double2 m2 = csub(cscale(t3, s5b), cscale(t4, s5a));
+        double2 i1 = make_double2(-m1.y, m1.x), i2 = make_double2(-m2.y, m2.x);
+        v[0] = o0;
+        v[1] = cadd(r1, i1);
+        v[4] = csub(r1, i1);
+        v[2] = cadd(r2, i2);
+        v[3] = csub(r2, i2);
+    }
+}
+
+__device__ __forceinline__ double2 *fft_smem(const DevPlan &P, double2 *a, double2 *b, int nseq, int ld, int sign) {
+    const int n = P.n;
+    double2 *src = a, *dst = b;
+    int Ns = 1;
+    for (int f = 0; f < P.nf; ++f) {
+        const int R = P.fac[f];
+        const int nR = n / R;
+        const int tstep = n / (Ns * R);
+        const int total = nseq * nR;
+        for (int t = threadIdx.x; t < total; t += blockDim.x) {
+            const int s = t / nR, j = t - s * nR;
+            const int k = j % Ns;
+            const double2 *sp = src + (size_t)s * ld;
+            double2 *dp = dst + (size_t)s * ld;
+            double2 v[5];
+#pragma unroll
+            for (int r = 0; r < 5; ++r) {
+                if (r < R) {
+                    double2 x = sp[j + r * nR];
+                    if (r && k) {
+                        double2 w = __ldg(&P.tw[(r * k * tstep) % n]);
+                        if (sign > 0) w.y = -w.y;
+                        x = cmul(x, w);
+                    }
+                    v[r] = x;
+                }
+            }
+            radix_dft(R, v, sign);
+            const int idxD = (j / Ns) * Ns * R + k;
+#pragma unroll
+            for (int q = 0; q < 5; ++q)
+                if (q < R) dp[idxD + q * Ns] = v[q];
+        }
+        __syncthreads();
+        double2 *tmp = src;
+        src = dst;
+        dst = tmp;
+        Ns *= R;
+    }
+    return src;
+}
+
+static inline int kmm_blocks(size_t n, int threads) {
+    size_t b = (n + threads - 1) / threads;
+    if (b > 148 * 32) b = 148 * 32;
+    if (b < 1) b = 1;
+    return (int)b;
+}

@@ -1,0 +1,660 @@
+// kmm_plane.cu -- vcw3dp (solvers.f90:1726-3538): dealiased nonlinear terms on the 3/2 grid.
+//
+// Data flow per call (all FP64):
+//   1. k_dct_fwd : spectral columns (nyp,nz,nxh) * c(i)/2 -> DCT-I along y (REDFT00)
+//                  -> plane layout PL[f][y][kx][kz]                        (solvers.f90:2241-2546)
+//   2. k_zfft_bwd: zero-pad kz nz -> mz (modes j > nzh move to (mz-nz)+j), inverse c2c along z
+//                  -> Q[f][y][z][kx]                                        (solvers.f90:2578-2803)
+//   3. k_xphys   : per (y,z) row: Hermitian c2r along x (two fields per complex FFT),
+//                  pointwise u x omega, -u.grad(c), polymer source/stress, CFL, immersed
+//                  boundary forces and dPdx; physical outputs -> PO[o][y][z][x],
+//                  u,v,w -> 3/2-grid copies for the tracers                 (solvers.f90:2806-3139)
+//   4. k_spread  : 5x5 force spreading for the planes i <= kmaxsurf       (solvers.f90:3069-3108)
+//   5. k_xfwd    : r2c along x, keep kx < nxh                              (solvers.f90:3147-3177)
+//   6. k_zfft_fwd: c2c along z, truncate to nz, /(mx*mz) -> PL[o][y][kx][kz] (solvers.f90:3180-3273)
+//   7. k_dct_bwd : DCT-I along y, /ny, halve first and last coefficient    (solvers.f90:3279-3416)
+// The internal 3/2-grid layout is [y][z][x] (x fastest); kmm_upload / kmm_download convert the
+// reference's (nyp,mz,mx) arrays.
+#include <math.h>
+
+#include "kmm_internal.cuh"
+
+#define MAXIO 64
+
+struct FieldPtrs { const double2 *p[MAXIO]; };
+struct FieldPtrsW { double2 *p[MAXIO]; };
+
+// ---------------------------------------------------------------------------
+// 1. forward Chebyshev -> physical y (scaled by c(i)/2), columns -> plane layout
+// ---------------------------------------------------------------------------
+#define DCT_CB 8
+__global__ void __launch_bounds__(256) k_dct_fwd(FieldPtrs in, double2 *__restrict__ pl, DevPlan P, int nyp, int nz,
+                                                 int nxh, int ncols) {
+    extern __shared__ double2 sm[];
+    const int ny = nyp - 1, L = 2 * ny;
+    const int f = blockIdx.y;
+    const int col0 = blockIdx.x * DCT_CB;
+    const int ncb = min(DCT_CB, ncols - col0);
+    double2 *a = sm, *b = sm + (size_t)DCT_CB * L;
+    const double2 *src = in.p[f] + (size_t)col0 * nyp;
+    for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
+        const int c = e / nyp, i = e - c * nyp;
+        double2 v = src[e];
+        const double fac = (i == 0 || i == ny) ? 1.0 : 0.5;   // c(i)/2.0
+        v = make_double2(v.x * fac, v.y * fac);
+        a[c * L + i] = v;
+        if (i > 0 && i < ny) a[c * L + L - i] = v;
+    }
+    for (int e = threadIdx.x + ncb * L; e < DCT_CB * L; e += blockDim.x) a[e] = make_double2(0.0, 0.0);
+    __syncthreads();
+    double2 *r = fft_smem(P, a, b, DCT_CB, L, -1);
+    // PL[f][y][kx][kz]: col = kx*nz + kz
+    for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
+        const int y = e / ncb, c = e - y * ncb;
+        const int col = col0 + c;
+        const int kx = col / nz, kz = col - kx * nz;
+        pl[(((size_t)f * nyp + y) * nxh + kx) * nz + kz] = r[c * L + y];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 2. z: zero-pad + inverse c2c (FFTW_BACKWARD)
+// ---------------------------------------------------------------------------
+#define ZKB 16
+__global__ void __launch_bounds__(256) k_zfft_bwd(const double2 *__restrict__ pl, double2 *__restrict__ q, DevPlan P,
+                                                  int nyp, int nz, int nxh, int mz) {
+    extern __shared__ double2 sm[];
+    const int y = blockIdx.y, f = blockIdx.z;
+    const int kx0 = blockIdx.x * ZKB;
+    const int nk = min(ZKB, nxh - kx0);
+    const int nzh = nz / 2;
+    double2 *a = sm, *b = sm + (size_t)ZKB * mz;
+    for (int e = threadIdx.x; e < ZKB * mz; e += blockDim.x) a[e] = make_double2(0.0, 0.0);
+    __syncthreads();
+    const double2 *src = pl + (((size_t)f * nyp + y) * nxh + kx0) * nz;
+    for (int e = threadIdx.x; e < nk * nz; e += blockDim.x) {
+        const int c = e / nz, j = e - c * nz;
+        const int jj = (j < nzh) ? j : (mz - nz) + j;
+        a[c * mz + jj] = src[e];
+    }
+    __syncthreads();
+    double2 *r = fft_smem(P, a, b, ZKB, mz, +1);
+    double2 *dst = q + (((size_t)f * nyp + y) * mz) * nxh;
+    for (int e = threadIdx.x; e < nk * mz; e += blockDim.x) {
+        const int z = e / nk, c = e - z * nk;
+        dst[(size_t)z * nxh + kx0 + c] = r[c * mz + z];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3. x: c2r + pointwise physics
+// ---------------------------------------------------------------------------
+// input slots (order of the physical arrays used below)
+enum { S_U, S_V, S_W, S_WX, S_WY, S_WZ, S_U11, S_U12, S_U13, S_U21, S_U22, S_U23, S_U31, S_U32, S_U33,
+       S_SC, S_CX, S_CY, S_CZ, S_C11, S_DC111 = S_C11 + 9, S_NSLOT = S_DC111 + 27 };
+enum { O_H1, O_H2, O_H3, O_SC, O_C11N, O_STR11N = O_C11N + 6, O_QP11 = O_STR11N + 6, O_NSLOT = O_QP11 + 6 };
+
+struct PhysArgs {
+    int slot_of_in[S_NSLOT];    // index into the input list, -1 if not transformed
+    int slot_of_out[O_NSLOT];   // index into the output list, -1 if not produced
+    int nin, nout;
+    int scalar, polymer, ipeter, itarget, scl_flag, flow_select, it, perturbtime, save_uvw, ib_any;
+    double delxm, delzm, dt, dPdx, gain, ugain, zl2, qbeta, alpha_poly, re, tpoly, scalar_q;
+};
+
+__device__ __forceinline__ void atomic_max_pos(double *addr, double v) {
+    // max of non-negative doubles (NaN bit patterns compare larger and propagate)
+    atomicMax((unsigned long long *)addr, (unsigned long long)__double_as_longlong(v));
+}
+
+#define XZB 2
+__global__ void __launch_bounds__(256) k_xphys(const double2 *__restrict__ q, double *__restrict__ po,
+                                               double *__restrict__ drag, double *__restrict__ up3,
+                                               double *__restrict__ vp3, double *__restrict__ wp3,
+                                               const int *__restrict__ imatrix, double *__restrict__ fxi,
+                                               double *__restrict__ fyi, double *__restrict__ fzi,
+                                               const double *__restrict__ scsource, const double *__restrict__ seght,
+                                               double *__restrict__ cfl, double *__restrict__ umax, DevPlan P,
+                                               PhysArgs A, int nyp, int mz, int mx, int nxh) {
+    extern __shared__ double2 sm[];
+    const int y = blockIdx.y;
+    const int z0 = blockIdx.x * XZB;
+    const int nzr = min(XZB, mz - z0);
+    const int hx = mx / 2;
+    // smem: phys[nin][XZB][mx] doubles, then FFT scratch a,b [XZB][mx] double2
+    double *phys = (double *)sm;
+    double2 *fa = (double2 *)(phys + (size_t)A.nin * XZB * mx);
+    double2 *fb = fa + (size_t)XZB * mx;
+    for (int f = 0; f < A.nin; f += 2) {
+        const int g = f + 1 < A.nin ? f + 1 : -1;
+        // Hermitian extension of A + iB for each row
+        for (int e = threadIdx.x; e < XZB * mx; e += blockDim.x) {
+            const int r = e / mx, k = e - r * mx;
+            double2 v = make_double2(0.0, 0.0);
+            if (r < nzr) {
+                const int z = z0 + r;
+                int kk = k <= hx ? k : mx - k;      // source mode
+                double2 A_ = make_double2(0.0, 0.0), B_ = make_double2(0.0, 0.0);
+                if (kk < nxh) {
+                    A_ = q[(((size_t)f * nyp + y) * mz + z) * nxh + kk];
+                    if (g >= 0) B_ = q[(((size_t)g * nyp + y) * mz + z) * nxh + kk];
+                }
+                if (k == 0 || k == hx) { A_.y = 0.0; B_.y = 0.0; }   // c2r ignores Im of DC / Nyquist
+                if (k <= hx) v = make_double2(A_.x - B_.y, A_.y + B_.x);          // A + iB
+                else v = make_double2(A_.x + B_.y, -A_.y + B_.x);                 // conj(A) + i conj(B)
+            }
+            fa[e] = v;
+        }
+        __syncthreads();
+        double2 *r = fft_smem(P, fa, fb, XZB, mx, +1);
+        for (int e = threadIdx.x; e < XZB * mx; e += blockDim.x) {
+            const int rr = e / mx, k = e - rr * mx;
+            phys[((size_t)f * XZB + rr) * mx + k] = r[e].x;
+            if (g >= 0) phys[((size_t)g * XZB + rr) * mx + k] = r[e].y;
+        }
+        __syncthreads();
+    }
+    // pointwise terms, solvers.f90:2885-3063
+    double cmax = 0.0, umx = 0.0;
+    const double sg = seght[y];
+#define IN(s) phys[((size_t)A.slot_of_in[s] * XZB + rr) * mx + k]
+    for (int e = threadIdx.x; e < nzr * mx; e += blockDim.x) {
+        const int rr = e / mx, k = e - rr * mx;
+        const int z = z0 + rr;
+        const double up = IN(S_U), vp = IN(S_V), wp = IN(S_W);
+        const double wxp = IN(S_WX), wyp = IN(S_WY), wzp = IN(S_WZ);
+        double out[O_NSLOT];
+        out[O_H1] = vp * wzp - wp * wyp;
+        out[O_H2] = -up * wzp + wp * wxp;
+        out[O_H3] = up * wyp - vp * wxp;
+        if (A.scalar) out[O_SC] = -(up * IN(S_CX) + vp * IN(S_CY) + wp * IN(S_CZ));
+        if (A.polymer) {
+            double c[9], gu[9];
+#pragma unroll
+            for (int m = 0; m < 9; ++m) { c[m] = IN(S_C11 + m); gu[m] = IN(S_U11 + m); }
+            const double c11 = c[0], c12 = c[1], c13 = c[2], c21 = c[3], c22 = c[4], c23 = c[5], c31 = c[6], c32 = c[7], c33 = c[8];
+            const double u11 = gu[0], u12 = gu[1], u13 = gu[2], u21 = gu[3], u22 = gu[4], u23 = gu[5], u31 = gu[6], u32 = gu[7], u33 = gu[8];
+#define DC(ij, kk) IN(S_DC111 + 3 * (ij) + (kk))
+            out[O_C11N + 0] = c11 * u11 + c12 * u12 + c13 * u13 + c11 * u11 + c21 * u12 + c31 * u13 - (up * DC(0, 0) + vp * DC(0, 1) + wp * DC(0, 2));
+            out[O_C11N + 1] = c11 * u21 + c12 * u22 + c13 * u23 + c12 * u11 + c22 * u12 + c32 * u13 - (up * DC(1, 0) + vp * DC(1, 1) + wp * DC(1, 2));
+            out[O_C11N + 2] = c11 * u31 + c12 * u32 + c13 * u33 + c13 * u11 + c23 * u12 + c33 * u13 - (up * DC(2, 0) + vp * DC(2, 1) + wp * DC(2, 2));
+            out[O_C11N + 3] = c21 * u21 + c22 * u22 + c23 * u23 + c12 * u21 + c22 * u22 + c32 * u23 - (up * DC(4, 0) + vp * DC(4, 1) + wp * DC(4, 2));
+            out[O_C11N + 4] = c21 * u31 + c22 * u32 + c23 * u33 + c13 * u21 + c23 * u22 + c33 * u23 - (up * DC(5, 0) + vp * DC(5, 1) + wp * DC(5, 2));
+            out[O_C11N + 5] = c31 * u31 + c32 * u32 + c33 * u33 + c13 * u31 + c23 * u32 + c33 * u33 - (up * DC(8, 0) + vp * DC(8, 1) + wp * DC(8, 2));
+#undef DC
+            const double trp = c11 + c22 + c33;
+            const double s6[6] = {c11, c12, c13, c22, c23, c33};
+            const double pf = (A.zl2 - 3.0) / (A.zl2 - trp);
+#pragma unroll
+            for (int m = 0; m < 6; ++m) out[O_STR11N + m] = A.ipeter == 0 ? s6[m] : pf * s6[m];
+            out[O_STR11N + 0] -= 1.0;
+            out[O_STR11N + 3] -= 1.0;
+            out[O_STR11N + 5] -= 1.0;
+            double beta_poly = A.qbeta;
+            if (A.itarget == 1) {
+                const double sc = fabs(A.scalar ? IN(S_SC) : 0.0);
+                if (A.alpha_poly * sc < 18.0) beta_poly = exp(-A.alpha_poly * sc);
+            } else if (A.itarget == 2) {
+                const double sc = fabs(A.scalar ? IN(S_SC) : 0.0);
+                beta_poly = 1.0 / (A.alpha_poly * sc + 1.0);
+            }
+            const double zbeta1 = (1.0 - beta_poly) / (A.re * beta_poly * A.tpoly);
+#pragma unroll
+            for (int m = 0; m < 6; ++m) out[O_QP11 + m] = zbeta1 * out[O_STR11N + m];
+        }
+        const double cflcheck = (fabs(up) / A.delxm + fabs(vp) / sg + fabs(wp) / A.delzm) * A.dt;
+        cmax = fmax(cmax, cflcheck);
+        if (cflcheck != cflcheck) cmax = cflcheck;
+        umx = fmax(umx, fabs(up));
+        // immersed boundary (solvers.f90:2996-3059); fxintg etc. in [y][z][x] layout
+        const size_t g3 = ((size_t)y * mz + z) * mx + k;
+        double dx = 0.0, dy = 0.0, dz = 0.0;
+        if (A.ib_any) {
+            const int t = imatrix[g3];
+            if (t == 1 || (t == 4 && A.it <= A.perturbtime)) {
+                const double fx = fxi[g3] + up, fy = fyi[g3] + vp, fz = fzi[g3] + wp;
+                fxi[g3] = fx; fyi[g3] = fy; fzi[g3] = fz;
+                dx = (-A.ugain * up) - A.gain * fx;
+                dy = (-A.ugain * vp) - A.gain * fy;
+                dz = (-A.ugain * wp) - A.gain * fz;
+            } else if (t == 3) {
+                const double fz = fzi[g3] + wp;
+                fzi[g3] = fz;
+                dz = -A.ugain * wp - A.gain * fz;
+            } else if (t == 11) {
+                dx = 1.0;
+            } else if (t == 0 && A.flow_select == 1) {
+                out[O_H1] = out[O_H1] - A.dPdx;
+            }
+            drag[0 * (size_t)nyp * mz * mx + g3] = dx;
+            drag[1 * (size_t)nyp * mz * mx + g3] = dy;
+            drag[2 * (size_t)nyp * mz * mx + g3] = dz;
+        } else if (A.flow_select == 1) {
+            out[O_H1] = out[O_H1] - A.dPdx;
+        }
+        if (A.scalar) {
+            if (A.scl_flag >= 2) out[O_SC] = out[O_SC] + scsource[g3] / A.dt;
+            if (A.scalar_q != 0.0) out[O_SC] = out[O_SC] + A.scalar_q;
+        }
+        for (int o = 0; o < O_NSLOT; ++o) {
+            const int s = A.slot_of_out[o];
+            if (s >= 0) po[(size_t)s * nyp * mz * mx + g3] = out[o];
+        }
+        if (A.save_uvw) { up3[g3] = up; vp3[g3] = vp; wp3[g3] = wp; }
+    }
+#undef IN
+    // block reductions of the CFL number and |u| for this plane
+    __shared__ double red[2][32];
+    for (int off = 16; off; off >>= 1) {
+        double c2 = __shfl_down_sync(0xffffffffu, cmax, off);
+        double u2 = __shfl_down_sync(0xffffffffu, umx, off);
+        cmax = (c2 != c2) ? c2 : fmax(cmax, c2);
+        umx = fmax(umx, u2);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { red[0][w] = cmax; red[1][w] = umx; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q2 = 1; q2 < (int)(blockDim.x >> 5); ++q2) {
+            cmax = (red[0][q2] != red[0][q2]) ? red[0][q2] : fmax(cmax, red[0][q2]);
+            umx = fmax(umx, red[1][q2]);
+        }
+        atomic_max_pos(&cfl[y], cmax);
+        atomic_max_pos(&umax[y], umx);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 4. 5x5 force spreading with the reference's sequential-loop semantics (solvers.f90:3069-3108):
+//    the plane loop runs k (x) outer, j (z) inner and assigns vwx(j,k) before adding its own and
+//    its neighbours' spread; a contribution from source q to target t survives only if t was
+//    assigned no later than q, i.e. flat(t) <= flat(q) with flat = (j-1) + (k-1)*mz.  Targets
+//    are computed in the column-major plane without a j-range check (the reference's test
+//    `j .ge. 3 .or. j .le. mz-2` is always true), so j+jj outside 1..mz lands in the next or
+//    previous x column; targets outside the plane array are dropped.
+// ---------------------------------------------------------------------------
+__global__ void k_spread(double *__restrict__ po, const double *__restrict__ drag, const double *__restrict__ fspread,
+                         int nyp, int mz, int mx, int kmaxsurf, int o1, int o2, int o3) {
+    const size_t nplane = (size_t)mz * mx;
+    const int y = blockIdx.y;
+    if (y + 1 > kmaxsurf) return;
+    const size_t n3 = (size_t)nyp * nplane;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nplane; e += (size_t)gridDim.x * blockDim.x) {
+        // target t in reference flat order: t = jt + kt*mz (0-based)
+        const long t = (long)e;
+        double ax = 0.0, ay = 0.0, az = 0.0;
+        for (int ii = -2; ii <= 2; ++ii)
+            for (int jj = -2; jj <= 2; ++jj) {
+                const long s = t - jj;                 // = jq + X*mz with X = wrap(kq+ii) - 1
+                if (s < 0 || s >= (long)nplane) continue;
+                const int jq = (int)(s % mz);
+                const int X = (int)(s / mz);
+                int kq = X - ii;                        // 0-based source column before wrap
+                if (kq < 0) kq += mx;
+                if (kq >= mx) kq -= mx;
+                const long qflat = (long)jq + (long)kq * mz;
+                if (qflat < t) continue;                // overwritten by the later assignment of t
+                const double sw = fspread[(abs(ii)) * 10 + abs(jj)];
+                const size_t gq = ((size_t)y * mz + jq) * mx + kq;
+                ax += sw * drag[gq];
+                ay += sw * drag[n3 + gq];
+                az += sw * drag[2 * n3 + gq];
+            }
+        const int jt = (int)(t % mz), kt = (int)(t / mz);
+        const size_t gt = ((size_t)y * mz + jt) * mx + kt;
+        if (o1 >= 0) po[(size_t)o1 * n3 + gt] += ax;
+        if (o2 >= 0) po[(size_t)o2 * n3 + gt] += ay;
+        if (o3 >= 0) po[(size_t)o3 * n3 + gt] += az;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 5. x: r2c (two real rows per complex FFT), keep kx < nxh
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_xfwd(const double *__restrict__ po, double2 *__restrict__ q, DevPlan P,
+                                              int nout, int nyp, int mz, int mx, int nxh) {
+    extern __shared__ double2 sm[];
+    const int y = blockIdx.y;
+    const int z0 = blockIdx.x * XZB;
+    const int nzr = min(XZB, mz - z0);
+    double2 *fa = sm, *fb = sm + (size_t)XZB * mx;
+    const size_t n3 = (size_t)nyp * mz * mx;
+    for (int o = 0; o < nout; o += 2) {
+        const int g = o + 1 < nout ? o + 1 : -1;
+        for (int e = threadIdx.x; e < XZB * mx; e += blockDim.x) {
+            const int r = e / mx, k = e - r * mx;
+            double2 v = make_double2(0.0, 0.0);
+            if (r < nzr) {
+                const size_t g3 = ((size_t)y * mz + z0 + r) * mx + k;
+                v.x = po[(size_t)o * n3 + g3];
+                if (g >= 0) v.y = po[(size_t)g * n3 + g3];
+            }
+            fa[e] = v;
+        }
+        __syncthreads();
+        double2 *r = fft_smem(P, fa, fb, XZB, mx, -1);
+        for (int e = threadIdx.x; e < nzr * nxh; e += blockDim.x) {
+            const int rr = e / nxh, k = e - rr * nxh;
+            const double2 Z = r[rr * mx + k];
+            const double2 Zc = cconj(r[rr * mx + ((mx - k) % mx)]);
+            const double2 a = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
+            const size_t d = (((size_t)o * nyp + y) * mz + z0 + rr) * nxh + k;
+            q[d] = a;
+            if (g >= 0) {
+                const double2 dd = csub(Z, Zc);                 // -i/2 (Z - Zc)
+                q[(((size_t)g * nyp + y) * mz + z0 + rr) * nxh + k] = make_double2(0.5 * dd.y, -0.5 * dd.x);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 6. z: forward c2c, truncate to nz, /(mx*mz)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_zfft_fwd(const double2 *__restrict__ q, double2 *__restrict__ pl, DevPlan P,
+                                                  int nyp, int nz, int nxh, int mz, double scale) {
+    extern __shared__ double2 sm[];
+    const int y = blockIdx.y, f = blockIdx.z;
+    const int kx0 = blockIdx.x * ZKB;
+    const int nk = min(ZKB, nxh - kx0);
+    const int nzh = nz / 2;
+    double2 *a = sm, *b = sm + (size_t)ZKB * mz;
+    const double2 *src = q + (((size_t)f * nyp + y) * mz) * nxh;
+    for (int e = threadIdx.x; e < ZKB * mz; e += blockDim.x) {
+        const int z = e / ZKB, c = e - z * ZKB;
+        a[c * mz + z] = c < nk ? src[(size_t)z * nxh + kx0 + c] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    double2 *r = fft_smem(P, a, b, ZKB, mz, -1);
+    double2 *dst = pl + (((size_t)f * nyp + y) * nxh + kx0) * nz;
+    for (int e = threadIdx.x; e < nk * nz; e += blockDim.x) {
+        const int c = e / nz, j = e - c * nz;
+        const int jj = (j < nzh) ? j : (mz - nz) + j;
+        const double2 v = r[c * mz + jj];
+        dst[e] = make_double2(v.x / scale, v.y / scale);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 7. y: DCT-I back to Chebyshev coefficients, /ny, halve the end coefficients
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_dct_bwd(const double2 *__restrict__ pl, FieldPtrsW out, DevPlan P, int nyp,
+                                                 int nz, int nxh, int ncols) {
+    extern __shared__ double2 sm[];
+    const int ny = nyp - 1, L = 2 * ny;
+    const int f = blockIdx.y;
+    const int col0 = blockIdx.x * DCT_CB;
+    const int ncb = min(DCT_CB, ncols - col0);
+    double2 *a = sm, *b = sm + (size_t)DCT_CB * L;
+    for (int e = threadIdx.x; e < DCT_CB * L; e += blockDim.x) a[e] = make_double2(0.0, 0.0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
+        const int y = e / ncb, c = e - y * ncb;
+        const int col = col0 + c;
+        const int kx = col / nz, kz = col - kx * nz;
+        const double2 v = pl[(((size_t)f * nyp + y) * nxh + kx) * nz + kz];
+        a[c * L + y] = v;
+        if (y > 0 && y < ny) a[c * L + L - y] = v;
+    }
+    __syncthreads();
+    double2 *r = fft_smem(P, a, b, DCT_CB, L, -1);
+    double2 *dst = out.p[f] + (size_t)col0 * nyp;
+    for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
+        const int c = e / nyp, i = e - c * nyp;
+        double2 v = r[c * L + i];
+        v = make_double2(v.x / (double)ny, v.y / (double)ny);
+        if (i == 0 || i == ny) v = make_double2(v.x / 2.0, v.y / 2.0);
+        dst[e] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// physical scratch (outputs, drag) sized on demand
+// ---------------------------------------------------------------------------
+static double *g_po = NULL, *g_drag = NULL;
+static size_t g_po_n = 0, g_drag_n = 0;
+
+static int ensure_phys(kmm_ctx *ctx, int nout, bool need_drag) {
+    size_t n = ctx->nphys * (size_t)nout;
+    if (n > g_po_n) {
+        if (g_po) cudaFree(g_po);
+        g_po = NULL;
+        CK(cudaMalloc(&g_po, sizeof(double) * n));
+        g_po_n = n;
+    }
+    if (need_drag && 3 * ctx->nphys > g_drag_n) {
+        if (g_drag) cudaFree(g_drag);
+        g_drag = NULL;
+        CK(cudaMalloc(&g_drag, sizeof(double) * 3 * ctx->nphys));
+        g_drag_n = 3 * ctx->nphys;
+    }
+    return KMM_OK;
+}
+
+__global__ void k_kmaxsurf(const int *__restrict__ im, int *out, int nyp, int mz, int mx) {
+    const size_t n = (size_t)nyp * mz * mx;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int t = im[e];
+        if (t == 1 || t == 3 || t == 4) atomicMax(out, (int)(e % mx) + 1);   // 1-based x index k
+        if (!(t == 0 || t == 1 || t == 3 || t == 4 || t == 11)) atomicOr(out + 1, 1);
+    }
+}
+
+int kmm_update_kmaxsurf(kmm_ctx *ctx) {
+    if (ctx->kmaxsurf >= 0) return KMM_OK;
+    int *im = (int *)kmm_field_ptr(ctx, KMM_IMATRIX);
+    if (!im) return KMM_ERR_NOMEM;
+    int h[2] = {0, 0};
+    int *tmp = NULL;
+    CK(cudaMallocAsync((void **)&tmp, 2 * sizeof(int), ctx->stream));
+    CK(cudaMemsetAsync(tmp, 0, 2 * sizeof(int), ctx->stream));
+    k_kmaxsurf<<<kmm_blocks(ctx->nphys, 256), 256, 0, ctx->stream>>>(im, tmp, ctx->nyp, ctx->mz, ctx->mx);
+    CKL();
+    CK(cudaMemcpyAsync(h, tmp, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaFreeAsync(tmp, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h[1]) {
+        kmm_set_error(ctx, "imatrix holds a cell type other than 0, 1, 3, 4, 11 (buffer/suction/moving-wall types are not built)");
+        return KMM_ERR_UNSUPPORTED;
+    }
+    ctx->kmaxsurf = h[0];
+    return KMM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// driver
+// ---------------------------------------------------------------------------
+int kmm_tracers(kmm_ctx *ctx);   // kmm_tracer.cu
+
+static bool g_attr_done = false;
+
+extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    const int nyp = ctx->nyp, nz = ctx->nz, nxh = ctx->nxh, mx = ctx->mx, mz = ctx->mz;
+    const int ncols = nz * nxh;
+    const int it = ctx->it;
+    const bool scal = ctx->p.scalar_on != 0;
+    const bool poly = ctx->p.polymer_on && (it >= ctx->p.src_start - 1);
+    // the immersed-boundary branches run only when an imatrix was uploaded (all-fluid otherwise)
+    const bool ib_any = ctx->f[KMM_IMATRIX] != NULL;
+    if (ib_any) RET(kmm_update_kmaxsurf(ctx));
+
+    // inputs actually consumed by the physics (the reference also transforms u_ij and the
+    // Laplacian every step; those only feed output, swirl and the inertial-particle path)
+    PhysArgs A;
+    memset(&A, 0, sizeof(A));
+    for (int s = 0; s < S_NSLOT; ++s) A.slot_of_in[s] = -1;
+    for (int o = 0; o < O_NSLOT; ++o) A.slot_of_out[o] = -1;
+    FieldPtrs in;
+    FieldPtrsW outp;
+    int nin = 0, nout = 0;
+    auto add_in = [&](int slot, int fid) -> int {
+        double2 *p = SPEC(ctx, fid);
+        if (!p) return KMM_ERR_NOMEM;
+        A.slot_of_in[slot] = nin;
+        in.p[nin++] = p;
+        return KMM_OK;
+    };
+    auto add_out = [&](int slot, int fid) -> int {
+        double2 *p = SPEC(ctx, fid);
+        if (!p) return KMM_ERR_NOMEM;
+        A.slot_of_out[slot] = nout;
+        outp.p[nout++] = p;
+        return KMM_OK;
+    };
+    static const int fl[6] = {KMM_U, KMM_V, KMM_W, KMM_OMX, KMM_OMY, KMM_OMZ};
+    for (int m = 0; m < 6; ++m) RET(add_in(S_U + m, fl[m]));
+    if (scal) {
+        RET(add_in(S_SC, KMM_SCALAR));
+        RET(add_in(S_CX, KMM_SCLX));
+        RET(add_in(S_CY, KMM_SCLY));
+        RET(add_in(S_CZ, KMM_SCLZ));
+    }
+    if (poly) {
+        static const int gu[9] = {KMM_U11, KMM_U12, KMM_U13, KMM_U21, KMM_U22, KMM_U23, KMM_U31, KMM_U32, KMM_U33};
+        for (int m = 0; m < 9; ++m) RET(add_in(S_U11 + m, gu[m]));
+        for (int m = 0; m < 9; ++m) RET(add_in(S_C11 + m, KMM_C11 + m));
+        for (int m = 0; m < 27; ++m) RET(add_in(S_DC111 + m, KMM_DC111 + m));
+    }
+    RET(add_out(O_H1, KMM_GN));
+    RET(add_out(O_H2, KMM_FN));
+    // h3 is written into omz, an input: stage it in the output plane buffer and write it last
+    RET(add_out(O_H3, KMM_OMZ));
+    if (scal) RET(add_out(O_SC, KMM_SCN));
+    if (poly) {
+        for (int m = 0; m < 6; ++m) RET(add_out(O_C11N + m, KMM_C11N + m));
+        for (int m = 0; m < 6; ++m) RET(add_out(O_STR11N + m, KMM_STR11N + m));
+        static const int qq[6] = {KMM_QP11, KMM_QP12, KMM_QP13, KMM_QP22, KMM_QP23, KMM_QP33};
+        for (int m = 0; m < 6; ++m) RET(add_out(O_QP11 + m, qq[m]));
+    }
+    A.nin = nin;
+    A.nout = nout;
+    A.scalar = scal;
+    A.polymer = poly;
+    A.ipeter = ctx->p.ipeter;
+    A.itarget = ctx->p.itarget;
+    A.scl_flag = ctx->p.scl_flag;
+    A.flow_select = ctx->p.flow_select;
+    A.it = it;
+    A.perturbtime = ctx->p.perturbtime;
+    A.save_uvw = 1;
+    A.ib_any = ib_any;
+    A.delxm = ctx->xl / (double)mx;
+    A.delzm = ctx->zl / (double)mz;
+    A.dt = ctx->dt;
+    A.dPdx = ctx->dPdx;
+    A.gain = ctx->gain;
+    A.ugain = ctx->ugain;
+    A.zl2 = ctx->p.zlmax * ctx->p.zlmax;
+    A.qbeta = ctx->p.qbeta;
+    A.alpha_poly = ctx->p.alpha_poly;
+    A.re = ctx->re;
+    A.tpoly = ctx->p.tpoly;
+    A.scalar_q = ctx->p.scalar_q;
+
+    RET(kmm_ensure_plane_buffers(ctx, nin, nout));
+    RET(ensure_phys(ctx, nout, ib_any));
+    double *up3 = REAL(ctx, KMM_UP3D), *vp3 = REAL(ctx, KMM_VP3D), *wp3 = REAL(ctx, KMM_WP3D);
+    double *fxi = NULL, *fyi = NULL, *fzi = NULL;
+    int *im = NULL;
+    if (ib_any) {
+        fxi = REAL(ctx, KMM_FXINTG); fyi = REAL(ctx, KMM_FYINTG); fzi = REAL(ctx, KMM_FZINTG);
+        im = (int *)kmm_field_ptr(ctx, KMM_IMATRIX);
+    }
+    if (scal && ctx->p.scl_flag >= 2) {
+        if (!ctx->scsource) {
+            CK(cudaMalloc(&ctx->scsource, sizeof(double) * ctx->nphys));
+            CK(cudaMemsetAsync(ctx->scsource, 0, sizeof(double) * ctx->nphys, ctx->stream));
+        }
+        if (ctx->p.scl_flag == 2 && ctx->p.npart > 0) {
+            kmm_set_error(ctx, "scl_flag = 2 particle-Gaussian scalar source is not built on the GPU path");
+            return KMM_ERR_UNSUPPORTED;
+        }
+    }
+
+    if (!g_attr_done) {
+        CK(cudaFuncSetAttribute(k_dct_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        CK(cudaFuncSetAttribute(k_dct_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        CK(cudaFuncSetAttribute(k_zfft_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        CK(cudaFuncSetAttribute(k_zfft_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        CK(cudaFuncSetAttribute(k_xphys, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        CK(cudaFuncSetAttribute(k_xfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        g_attr_done = true;
+    }
+    const size_t sm_dct = sizeof(double2) * 2 * DCT_CB * 2 * ctx->ny;
+    const size_t sm_z = sizeof(double2) * 2 * ZKB * mz;
+    const size_t sm_x = sizeof(double) * (size_t)nin * XZB * mx + sizeof(double2) * 2 * XZB * mx;
+    const size_t sm_xf = sizeof(double2) * 2 * XZB * mx;
+    if (sm_x > 227 * 1024 || sm_dct > 227 * 1024 || sm_z > 227 * 1024) {
+        kmm_set_error(ctx, "vcw3dp shared-memory plan exceeds 227 KB (nin=%d, mx=%d)", nin, mx);
+        return KMM_ERR_UNSUPPORTED;
+    }
+    CK(cudaMemsetAsync(ctx->d_cfl, 0, sizeof(double) * nyp, ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_umax, 0, sizeof(double) * nyp, ctx->stream));
+
+    kmm_tic(ctx);
+    k_dct_fwd<<<dim3((ncols + DCT_CB - 1) / DCT_CB, nin), 256, sm_dct, ctx->stream>>>(in, ctx->pl_in, ctx->py2, nyp,
+                                                                                        nz, nxh, ncols);
+    CKL();
+    kmm_toc(ctx, KMM_STAGE_DCT_FWD);
+    kmm_tic(ctx);
+    k_zfft_bwd<<<dim3((nxh + ZKB - 1) / ZKB, nyp, nin), 256, sm_z, ctx->stream>>>(ctx->pl_in, ctx->q_in, ctx->pmz,
+                                                                                   nyp, nz, nxh, mz);
+    CKL();
+    kmm_toc(ctx, KMM_STAGE_ZFFT_BWD);
+    kmm_tic(ctx);
+    k_xphys<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_x, ctx->stream>>>(
+        ctx->q_in, g_po, g_drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl,
+        ctx->d_umax, ctx->pmx, A, nyp, mz, mx, nxh);
+    CKL();
+    kmm_toc(ctx, KMM_STAGE_XPHYS);
+    if (ib_any && ctx->kmaxsurf > 0) {
+        const int ksp = ctx->kmaxsurf < nyp ? ctx->kmaxsurf : nyp;
+        k_spread<<<dim3(kmm_blocks((size_t)mz * mx, 256) > 64 ? 64 : kmm_blocks((size_t)mz * mx, 256), ksp), 256, 0,
+                   ctx->stream>>>(g_po, g_drag, ctx->d_fspread, nyp, mz, mx, ctx->kmaxsurf, A.slot_of_out[O_H1],
+                                  A.slot_of_out[O_H2], A.slot_of_out[O_H3]);
+        CKL();
+    }
+    kmm_tic(ctx);
+    k_xfwd<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_xf, ctx->stream>>>(g_po, ctx->q_out, ctx->pmx, nout, nyp, mz,
+                                                                         mx, nxh);
+    CKL();
+    kmm_toc(ctx, KMM_STAGE_XFWD);
+    kmm_tic(ctx);
+    k_zfft_fwd<<<dim3((nxh + ZKB - 1) / ZKB, nyp, nout), 256, sm_z, ctx->stream>>>(ctx->q_out, ctx->pl_out, ctx->pmz,
+                                                                                    nyp, nz, nxh, mz,
+                                                                                    (double)mx * (double)mz);
+    CKL();
+    kmm_toc(ctx, KMM_STAGE_ZFFT_FWD);
+    kmm_tic(ctx);
+    k_dct_bwd<<<dim3((ncols + DCT_CB - 1) / DCT_CB, nout), 256, sm_dct, ctx->stream>>>(ctx->pl_out, outp, ctx->py2,
+                                                                                        nyp, nz, nxh, ncols);
+    CKL();
+    kmm_toc(ctx, KMM_STAGE_DCT_BWD);
+
+    // tracers (solvers.f90:3463-3476)
+    int st = KMM_OK;
+    if (ctx->p.npart > 0) {
+        st = kmm_tracers(ctx);
+        if (st != KMM_OK && st != KMM_ERR_INTERP) return st;
+    }
+    // CFL check (solvers.f90:3497-3514)
+    double h_cfl[KMM_MAX_NYP], h_um[KMM_MAX_NYP];
+    CK(cudaMemcpyAsync(h_cfl, ctx->d_cfl, sizeof(double) * nyp, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(h_um, ctx->d_umax, sizeof(double) * nyp, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    double cflmax = 0.0, umax = 0.0;
+    bool nan = false;
+    for (int i = 0; i < nyp; ++i) {
+        if (h_cfl[i] != h_cfl[i]) nan = true;
+        else if (h_cfl[i] > cflmax) cflmax = h_cfl[i];
+        if (h_um[i] > umax) umax = h_um[i];
+    }
+    ctx->stats.cflmax = nan ? NAN : cflmax;
+    ctx->stats.umax = umax;
+    if (st == KMM_OK && nan) st = KMM_ERR_NAN;
+    if (st == KMM_OK && cflmax > 1.0) st = KMM_ERR_CFL;
+    ctx->stats.status = st;
+    return st;
+}

@@ -1,0 +1,384 @@
+// kmm_step.cu -- host-side orchestration of the main program's blocks (main_dns.f90):
+// Green's functions (gfcn, solvers.f90:5-172), initial (main_dns.f90:1602-2231) and the body
+// of the time loop (main_dns.f90:198-811).  Every device call goes through the routine entry
+// points of the other translation units, in the reference's order.
+#include <math.h>
+
+#include "kmm_internal.cuh"
+
+// ---------------------------------------------------------------------------
+// gfcn: two Green's functions + wall derivatives + common denominator
+// ---------------------------------------------------------------------------
+__global__ void k_gfcn_bc(double2 *bct, double2 *bcb, int nz, int nxh, double pt, double pb) {
+    const int n = nz * nxh;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int j = e % nz, k = e / nz;
+        double2 t = make_double2(pt, pt), b = make_double2(pb, pb);
+        if (k == 0 && j >= nz / 2) { t.y = -t.y; b.y = -b.y; }   // conjg for j = nz/2+1..nz, kx = 0
+        if (e == 0) { t = make_double2(pt, 0.0); b = make_double2(pb, 0.0); }
+        bct[e] = t;
+        bcb[e] = b;
+    }
+}
+
+// (0,0) mode real + Hermitian symmetrisation of the kx = 0 plane (solvers.f90:118-139)
+__global__ void k_gfcn_sym(double2 *g, int nyp, int nz) {
+    const int n = nyp * (nz / 2);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int i = e % nyp, j = e / nyp;
+        if (j == 0) {
+            g[i].y = 0.0;
+        } else {
+            const int jp = nz - j;
+            double2 x = g[(size_t)j * nyp + i], y = g[(size_t)jp * nyp + i];
+            double2 m = make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
+            g[(size_t)j * nyp + i] = m;
+            g[(size_t)jp * nyp + i] = make_double2(m.x, -m.y);
+        }
+    }
+}
+
+__global__ void k_gather_row(const double2 *w, double2 *dnvb, double2 *dnvt, int ncols, int nyp) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncols; c += gridDim.x * blockDim.x) {
+        dnvb[c] = w[(size_t)c * nyp + 0];
+        dnvt[c] = w[(size_t)c * nyp + 1];
+    }
+}
+
+__global__ void k_denom(double2 *den, const double2 *d1t, const double2 *d2b, const double2 *d2t, const double2 *d1b,
+                        int n) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+        den[e] = csub(cmul(d1t[e], d2b[e]), cmul(d2t[e], d1b[e]));
+}
+
+static int gfcn1(kmm_ctx *ctx, int gf, int dnvbf, int dnvtf, double pb, double pt) {
+    double2 *g = SPEC(ctx, gf), *bct = SPEC(ctx, KMM_BCTOP), *bcb = SPEC(ctx, KMM_BCBOT);
+    double2 *dnvb = SPEC(ctx, dnvbf), *dnvt = SPEC(ctx, dnvtf);
+    if (!g || !bct || !bcb || !dnvb || !dnvt) return KMM_ERR_NOMEM;
+    const int nw = ctx->nz * ctx->nxh;
+    k_gfcn_bc<<<kmm_blocks(nw, 256), 256, 0, ctx->stream>>>(bct, bcb, ctx->nz, ctx->nxh, pt, pb);
+    CKL();
+    CK(cudaMemsetAsync(g, 0, sizeof(double2) * ctx->nspec, ctx->stream));
+    RET(kmm_internal_solve(ctx, g, ctx->re / (ctx->theta * ctx->dt), 0, bct, bcb));
+    CK(cudaMemsetAsync(bct, 0, sizeof(double2) * nw, ctx->stream));
+    CK(cudaMemsetAsync(bcb, 0, sizeof(double2) * nw, ctx->stream));
+    RET(kmm_internal_solve(ctx, g, 0.0, 0, bct, bcb));
+    k_gfcn_sym<<<kmm_blocks((size_t)ctx->nyp * ctx->nz / 2, 256), 256, 0, ctx->stream>>>(g, ctx->nyp, ctx->nz);
+    CKL();
+    double2 *wrkc = ctx->wrk[2], *wrk1 = ctx->wrk[3];
+    if (ctx->nb == 1) { RET(kmm_internal_wallderiv(ctx, g, 1, 0, wrkc, 1)); }
+    else { RET(kmm_internal_cderiv(ctx, g, wrk1)); RET(kmm_internal_wallderiv(ctx, wrk1, 1, 0, wrkc, 1)); }
+    if (ctx->nt == 1) { RET(kmm_internal_wallderiv(ctx, g, 1, 1, wrkc, 2)); }
+    else { RET(kmm_internal_cderiv(ctx, g, wrk1)); RET(kmm_internal_wallderiv(ctx, wrk1, 1, 1, wrkc, 2)); }
+    k_gather_row<<<kmm_blocks(nw, 256), 256, 0, ctx->stream>>>(wrkc, dnvb, dnvt, nw, ctx->nyp);
+    CKL();
+    return KMM_OK;
+}
+
+extern "C" int kmm_gfcn(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    RET(gfcn1(ctx, KMM_GF1, KMM_DNV1B, KMM_DNV1T, ctx->p1b, ctx->p1t));
+    RET(gfcn1(ctx, KMM_GF2, KMM_DNV2B, KMM_DNV2T, ctx->p2b, ctx->p2t));
+    const int nw = ctx->nz * ctx->nxh;
+    k_denom<<<kmm_blocks(nw, 256), 256, 0, ctx->stream>>>(SPEC(ctx, KMM_DENOM), SPEC(ctx, KMM_DNV1T),
+                                                          SPEC(ctx, KMM_DNV2B), SPEC(ctx, KMM_DNV2T),
+                                                          SPEC(ctx, KMM_DNV1B), nw);
+    CKL();
+    return KMM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// small spectral helpers used by initial / step
+// ---------------------------------------------------------------------------
+// omy = i kz u - i kx w; (0,0) mode zero (main_dns.f90:1954-1968)
+__global__ void k_init_omy(const double2 *u, const double2 *w, double2 *omy, const double *wavx, const double *wavz,
+                           size_t n, int nyp, int nz) {
+    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        const size_t jk = idx / nyp;
+        const int j = (int)(jk % nz), k = (int)(jk / nz);
+        double2 a = cimul(u[idx], wavz[j]), b = cimul(w[idx], wavx[k]);
+        omy[idx] = (j == 0 && k == 0) ? make_double2(0.0, 0.0) : csub(a, b);
+    }
+}
+
+// u0 = Re u(:,1,1), w0 = Re w(:,1,1); u(:,1,1) = u0, v(:,1,1) = 0, w(:,1,1) = w0 (main_dns.f90:1994-2005)
+__global__ void k_init_mean(double2 *u, double2 *v, double2 *w, double *u0, double *w0, int nyp) {
+    for (int i = threadIdx.x; i < nyp; i += blockDim.x) {
+        u0[i] = u[i].x;
+        w0[i] = w[i].x;
+        u[i] = make_double2(u0[i], 0.0);
+        v[i] = make_double2(0.0, 0.0);
+        w[i] = make_double2(w0[i], 0.0);
+    }
+}
+
+// h1n = Re gn(:,1,1), h3n = Re omz(:,1,1) (main_dns.f90:748-751)
+__global__ void k_hmean(const double2 *gn, const double2 *omz, double *h1n, double *h3n, int nyp) {
+    for (int i = threadIdx.x; i < nyp; i += blockDim.x) {
+        h1n[i] = gn[i].x;
+        h3n[i] = omz[i].x;
+    }
+}
+
+// omy(:,1,1) = 0 (main_dns.f90:494-502)
+__global__ void k_zero_mean(double2 *a, int nyp) {
+    for (int i = threadIdx.x; i < nyp; i += blockDim.x) a[i] = make_double2(0.0, 0.0);
+}
+
+__global__ void k_add(double2 *y, const double2 *x, size_t n) {
+    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x)
+        y[idx] = cadd(y[idx], x[idx]);
+}
+
+static int norm_ids(kmm_ctx *ctx, const int *ids, int n) {
+    for (int m = 0; m < n; ++m) {
+        double2 *a = SPEC(ctx, ids[m]);
+        if (!a) return KMM_ERR_NOMEM;
+        RET(kmm_internal_norm(ctx, a));
+    }
+    return KMM_OK;
+}
+
+static const int kPolyComp[6] = {KMM_C11, KMM_C12, KMM_C13, KMM_C22, KMM_C23, KMM_C33};
+static const int kQp[6] = {KMM_QP11, KMM_QP12, KMM_QP13, KMM_QP22, KMM_QP23, KMM_QP33};
+
+static int poly_norm_c(kmm_ctx *ctx) {
+    for (int m = 0; m < 9; ++m) RET(kmm_norm(ctx, KMM_C11 + m));
+    return KMM_OK;
+}
+
+static int poly_norm_dc(kmm_ctx *ctx) {
+    for (int m = 0; m < 27; ++m) RET(kmm_norm(ctx, KMM_DC111 + m));
+    return KMM_OK;
+}
+
+static int poly_norm_out(kmm_ctx *ctx) {
+    RET(poly_norm_c(ctx));
+    for (int m = 0; m < 6; ++m) RET(kmm_norm(ctx, KMM_C11N + m));
+    for (int m = 0; m < 6; ++m) RET(kmm_norm(ctx, KMM_STR11N + m));
+    return norm_ids(ctx, kQp, 6);
+}
+
+// constant conformation tensor: xyzfft of a constant keeps only Chebyshev mode 0 of the (0,0) mode
+static int poly_set_constant(kmm_ctx *ctx) {
+    const double cz[9] = {ctx->p.c11z, 0, 0, 0, ctx->p.c22z, 0, 0, 0, ctx->p.c33z};
+    for (int m = 0; m < 9; ++m) RET(kmm_internal_set_constant_mode(ctx, SPEC(ctx, KMM_C11 + m), cz[m]));
+    return KMM_OK;
+}
+
+static double2 *poly_scratch(kmm_ctx *ctx, int m) {
+    const int id = KMM_NSPECTRAL + m;   // private ids past the public spectral range
+    if (!ctx->f[id]) {
+        if (cudaMalloc(&ctx->f[id], sizeof(double2) * ctx->nspec) != cudaSuccess) return NULL;
+        cudaMemsetAsync(ctx->f[id], 0, sizeof(double2) * ctx->nspec, ctx->stream);
+    }
+    return (double2 *)ctx->f[id];
+}
+
+// ---------------------------------------------------------------------------
+// initial (irstrt = 0), after the setup's gfcn (main_dns.f90:151-161, 1602-2231)
+// ---------------------------------------------------------------------------
+extern "C" int kmm_initial(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    const size_t n = ctx->nspec;
+    RET(kmm_gfcn(ctx));
+    ctx->it = 0;
+    RET(kmm_xyzfft(ctx, KMM_U, KMM_INITU));
+    RET(kmm_xyzfft(ctx, KMM_V, KMM_INITV));
+    RET(kmm_xyzfft(ctx, KMM_W, KMM_INITW));
+    if (ctx->p.scalar_on) {
+        RET(kmm_xyzfft(ctx, KMM_SCALAR, KMM_INITSCL));
+        RET(kmm_zero(ctx, KMM_CSOURCE));
+    }
+    if (ctx->p.polymer_on) RET(poly_set_constant(ctx));
+    k_init_omy<<<kmm_blocks(n, 256), 256, 0, ctx->stream>>>(SPEC(ctx, KMM_U), SPEC(ctx, KMM_W), SPEC(ctx, KMM_OMY),
+                                                            ctx->d_wavx, ctx->d_wavz, n, ctx->nyp, ctx->nz);
+    CKL();
+    static const int l1[4] = {KMM_U, KMM_V, KMM_W, KMM_OMY};
+    RET(norm_ids(ctx, l1, 4));
+    if (ctx->p.scalar_on) { static const int l[2] = {KMM_SCALAR, KMM_CSOURCE}; RET(norm_ids(ctx, l, 2)); }
+    if (ctx->p.polymer_on) RET(poly_norm_c(ctx));
+    k_init_mean<<<1, 256, 0, ctx->stream>>>(SPEC(ctx, KMM_U), SPEC(ctx, KMM_V), SPEC(ctx, KMM_W), REAL(ctx, KMM_U0),
+                                           REAL(ctx, KMM_W0), ctx->nyp);
+    CKL();
+    RET(norm_ids(ctx, l1, 4));
+    RET(kmm_vort(ctx));
+    { static const int l[2] = {KMM_OMX, KMM_OMZ}; RET(norm_ids(ctx, l, 2)); }
+    if (ctx->p.scalar_on) {
+        RET(kmm_gradscl(ctx));
+        static const int l[3] = {KMM_SCLX, KMM_SCLY, KMM_SCLZ};
+        RET(norm_ids(ctx, l, 3));
+    }
+    RET(kmm_gradv(ctx));
+    { static const int l[12] = {KMM_U11, KMM_U12, KMM_U13, KMM_U21, KMM_U22, KMM_U23, KMM_U31, KMM_U32, KMM_U33,
+                                KMM_LU, KMM_LV, KMM_LW};
+      RET(norm_ids(ctx, l, 12)); }
+    if (ctx->p.polymer_on) {
+        RET(kmm_derivscji(ctx));
+        RET(poly_norm_c(ctx));
+        RET(poly_norm_dc(ctx));
+    }
+    int st = kmm_vcw3dp(ctx);
+    if (st != KMM_OK && st != KMM_ERR_CFL && st != KMM_ERR_INTERP && st != KMM_ERR_NAN) return st;
+    { static const int l[5] = {KMM_V, KMM_OMY, KMM_FN, KMM_GN, KMM_OMZ}; RET(norm_ids(ctx, l, 5)); }
+    if (ctx->p.polymer_on) {
+        RET(poly_norm_out(ctx));
+        if (ctx->it >= ctx->p.src_start) {
+            RET(kmm_polyforce(ctx));
+            static const int l[3] = {KMM_T1, KMM_T2, KMM_T3};
+            RET(norm_ids(ctx, l, 3));
+            RET(kmm_subforce(ctx));
+        }
+    }
+    if (ctx->p.scalar_on && ctx->p.src_start == 0) {
+        k_add<<<kmm_blocks(n, 256), 256, 0, ctx->stream>>>(SPEC(ctx, KMM_SCN), SPEC(ctx, KMM_CSOURCE), n);
+        CKL();
+    }
+    k_hmean<<<1, 256, 0, ctx->stream>>>(SPEC(ctx, KMM_GN), SPEC(ctx, KMM_OMZ), REAL(ctx, KMM_H1N), REAL(ctx, KMM_H3N),
+                                       ctx->nyp);
+    CKL();
+    RET(kmm_nonlin(ctx));
+    { static const int l[2] = {KMM_FN, KMM_GN}; RET(norm_ids(ctx, l, 2)); }
+    if (ctx->p.scalar_on) RET(kmm_norm(ctx, KMM_SCN));
+    RET(kmm_copy(ctx, KMM_FNM1, KMM_FN));
+    RET(kmm_copy(ctx, KMM_GNM1, KMM_GN));
+    if (ctx->p.scalar_on) RET(kmm_copy(ctx, KMM_SCNM1, KMM_SCN));
+    if (ctx->p.polymer_on)
+        for (int m = 0; m < 6; ++m) {
+            RET(kmm_copy(ctx, KMM_C11NM1 + m, KMM_C11N + m));
+            RET(kmm_copy(ctx, KMM_STR11NM1 + m, KMM_STR11N + m));
+        }
+    RET(kmm_copy(ctx, KMM_H1NM1, KMM_H1N));
+    RET(kmm_copy(ctx, KMM_H3NM1, KMM_H3N));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return st;
+}
+
+// ---------------------------------------------------------------------------
+// one iteration of the time loop, main_dns.f90:198-811
+// ---------------------------------------------------------------------------
+extern "C" int kmm_step(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    const double re = ctx->re, dt = ctx->dt, th = ctx->theta;
+    ctx->it += 1;
+    const int it = ctx->it;
+    kmm_tic(ctx);
+    if (ctx->p.polymer_on) {
+        if (it == ctx->p.src_start - 1 || (it == ctx->p.irstrt && ctx->p.crstrt == 0)) RET(poly_set_constant(ctx));
+        if (it >= ctx->p.src_start) {
+            double2 *nl[6];
+            for (int m = 0; m < 6; ++m) {
+                nl[m] = poly_scratch(ctx, m);
+                if (!nl[m]) return KMM_ERR_NOMEM;
+            }
+            RET(kmm_internal_polynl(ctx, nl));
+            double2 *nl2 = poly_scratch(ctx, 6);
+            if (!nl2) return KMM_ERR_NOMEM;
+            for (int m = 0; m < 6; ++m) {
+                RET(kmm_internal_axpy_spec(ctx, nl2, nl[m], 2.0));
+                RET(kmm_internal_phirhs(ctx, SPEC(ctx, kPolyComp[m]), nl[m], nl2, ctx->p.diffpoly));
+            }
+            for (int m = 0; m < 6; ++m) {
+                RET(kmm_copy(ctx, KMM_C11NM1 + m, KMM_C11N + m));
+                RET(kmm_copy(ctx, KMM_STR11NM1 + m, KMM_STR11N + m));
+            }
+            const double g = (re * ctx->p.diffpoly) / (dt * th);
+            RET(kmm_zero(ctx, KMM_BCTOP));
+            RET(kmm_zero(ctx, KMM_BCBOT));
+            for (int m = 0; m < 6; ++m) RET(kmm_penta(ctx, kPolyComp[m], g, 0, 0.0, 1.0, 0.0, 1.0));
+            RET(norm_ids(ctx, kPolyComp, 6));
+            RET(kmm_copy(ctx, KMM_C21, KMM_C12));
+            RET(kmm_copy(ctx, KMM_C31, KMM_C13));
+            RET(kmm_copy(ctx, KMM_C32, KMM_C23));
+        }
+    }
+    if (ctx->p.scalar_on) {
+        RET(kmm_phirhs(ctx, KMM_SCALAR, KMM_SCN, KMM_SCNM1, ctx->p.diff));
+        RET(kmm_copy(ctx, KMM_SCNM1, KMM_SCN));
+        const double g = (re * ctx->p.diff) / (dt * th);
+        RET(kmm_zero(ctx, KMM_BCTOP));   // bcscltop = bcsclbot = 0 (main_dns.f90:39)
+        RET(kmm_zero(ctx, KMM_BCBOT));
+        if (ctx->p.scalar_bc == 1) RET(kmm_penta(ctx, KMM_SCALAR, g, 0, 1.0, 0.0, 1.0, 0.0));
+        else RET(kmm_penta(ctx, KMM_SCALAR, g, 0, 0.0, 1.0, 0.0, 1.0));
+    }
+    RET(kmm_phi_from_v(ctx));
+    RET(kmm_phirhs(ctx, KMM_V, KMM_FN, KMM_FNM1, 1.0));
+    RET(kmm_copy(ctx, KMM_FNM1, KMM_FN));
+    RET(kmm_solve(ctx, KMM_V, re / (dt * th), 0));
+    RET(kmm_solve(ctx, KMM_V, 0.0, 0));
+    RET(kmm_phirhs(ctx, KMM_OMY, KMM_GN, KMM_GNM1, 1.0));
+    RET(kmm_copy(ctx, KMM_GNM1, KMM_GN));
+    RET(kmm_influence(ctx));
+    RET(kmm_penta(ctx, KMM_OMY, re / (dt * th), 0, ctx->atu, ctx->btu, ctx->abu, ctx->bbu));
+    RET(kmm_uzero(ctx, 1));
+    RET(kmm_uzero(ctx, 3));
+    k_zero_mean<<<1, 256, 0, ctx->stream>>>(SPEC(ctx, KMM_OMY), ctx->nyp);
+    CKL();
+    RET(kmm_copy(ctx, KMM_H1NM1, KMM_H1N));
+    RET(kmm_copy(ctx, KMM_H3NM1, KMM_H3N));
+    { static const int l[2] = {KMM_V, KMM_OMY}; RET(norm_ids(ctx, l, 2)); }
+    RET(kmm_veloc(ctx));
+    { static const int l[2] = {KMM_U, KMM_W}; RET(norm_ids(ctx, l, 2)); }
+    RET(kmm_vort(ctx));
+    { static const int l[2] = {KMM_OMX, KMM_OMZ}; RET(norm_ids(ctx, l, 2)); }
+    if (ctx->p.scalar_on) {
+        RET(kmm_norm(ctx, KMM_SCALAR));
+        RET(kmm_gradscl(ctx));
+        static const int l[3] = {KMM_SCLX, KMM_SCLY, KMM_SCLZ};
+        RET(norm_ids(ctx, l, 3));
+    }
+    if (ctx->p.polymer_on || ctx->p.particle_flag > 0) {
+        // the velocity gradient / Laplacian feed only the polymer terms and inertial particles
+        RET(kmm_gradv(ctx));
+        static const int l[12] = {KMM_U11, KMM_U12, KMM_U13, KMM_U21, KMM_U22, KMM_U23, KMM_U31, KMM_U32, KMM_U33,
+                                  KMM_LU, KMM_LV, KMM_LW};
+        RET(norm_ids(ctx, l, 12));
+    }
+    if (ctx->p.polymer_on) {
+        RET(kmm_derivscji(ctx));
+        RET(poly_norm_c(ctx));
+        RET(poly_norm_dc(ctx));
+    }
+    kmm_toc(ctx, KMM_STAGE_COLUMN);
+    int st = kmm_vcw3dp(ctx);
+    if (st != KMM_OK) return st;
+    kmm_tic(ctx);
+    { static const int l[5] = {KMM_V, KMM_OMY, KMM_FN, KMM_GN, KMM_OMZ}; RET(norm_ids(ctx, l, 5)); }
+    if (ctx->p.scalar_on) { static const int l[2] = {KMM_SCALAR, KMM_SCN}; RET(norm_ids(ctx, l, 2)); }
+    if (ctx->p.polymer_on) {
+        if (it >= ctx->p.src_start - 1) RET(poly_norm_out(ctx));
+        if (it >= ctx->p.src_start) {
+            RET(kmm_polyforce(ctx));
+            static const int l[3] = {KMM_T1, KMM_T2, KMM_T3};
+            RET(norm_ids(ctx, l, 3));
+            RET(kmm_subforce(ctx));
+        }
+    }
+    RET(kmm_filter(ctx));
+    k_hmean<<<1, 256, 0, ctx->stream>>>(SPEC(ctx, KMM_GN), SPEC(ctx, KMM_OMZ), REAL(ctx, KMM_H1N), REAL(ctx, KMM_H3N),
+                                       ctx->nyp);
+    CKL();
+    { static const int l[3] = {KMM_FN, KMM_GN, KMM_OMZ}; RET(norm_ids(ctx, l, 3)); }
+    RET(kmm_nonlin(ctx));
+    { static const int l[2] = {KMM_FN, KMM_GN}; RET(norm_ids(ctx, l, 2)); }
+    if (ctx->p.scalar_on) RET(kmm_norm(ctx, KMM_SCN));
+    kmm_toc(ctx, KMM_STAGE_POST);
+    return KMM_OK;
+}
+
+extern "C" int kmm_run(kmm_ctx *ctx, int n) {
+    if (!ctx || n < 0) return KMM_ERR_ARG;
+    for (int s = 0; s < n; ++s) RET(kmm_step(ctx));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return KMM_OK;
+}
+
+extern "C" int kmm_polynl(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    double2 *nl[6];
+    for (int m = 0; m < 6; ++m) {
+        nl[m] = poly_scratch(ctx, m);
+        if (!nl[m]) return KMM_ERR_NOMEM;
+    }
+    return kmm_internal_polynl(ctx, nl);
+}

@@ -1,0 +1,190 @@
+"""Python handle on libkmm_b200.so through its C ABI (include/kmm.h).
+
+This is the host-side mirror of the reference's Fortran calls: each method has
+the name of the reference subroutine it replaces and takes field names where the
+Fortran routine takes arrays.  There is no CPU fallback: if the CUDA library is
+missing or no GPU is visible, constructing a context raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libkmm_b200.so")
+_lib = None
+
+# name -> argtypes after the context pointer
+_ROUTINES = {
+    "cderiv": "ii", "wallderiv": "iiiii", "gradv": "", "gradscl": "", "derivscji": "", "gfcn": "",
+    "phirhs": "iiid", "solve": "idi", "penta": "ididddd", "uzero": "i", "phi_from_v": "", "influence": "",
+    "veloc": "", "vort": "", "nonlin": "", "vcw3dp": "", "norm": "i", "xyzfft": "ii", "polynl": "",
+    "polyforce": "", "subforce": "", "filter": "", "initial": "", "step": "", "run": "i",
+    "tracer_update": "", "init_part": "", "copy": "ii", "zero": "i", "set_it": "i", "sync": "",
+}
+_CT = {"i": ctypes.c_int, "d": ctypes.c_double}
+
+
+class KmmError(RuntimeError):
+    def __init__(self, status, where, message=""):
+        self.status = status
+        super().__init__("%s returned %s%s" % (where, abi.STATUS_NAMES.get(status, status),
+                                                (": " + message) if message else ""))
+
+
+def lib():
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libkmm_b200.so is missing: build it with `python -m polymer_dns_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        L.kmm_ctx_create.argtypes = [ctypes.POINTER(abi.KmmParams), ctypes.c_int, ctypes.POINTER(vp)]
+        L.kmm_ctx_create.restype = ctypes.c_int
+        L.kmm_ctx_destroy.argtypes = [vp]
+        L.kmm_ctx_destroy.restype = ctypes.c_int
+        L.kmm_last_error.argtypes = [vp]
+        L.kmm_last_error.restype = ctypes.c_char_p
+        L.kmm_abi_version.restype = ctypes.c_int
+        L.kmm_field_size.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)]
+        L.kmm_field_size.restype = ctypes.c_int
+        for fn in ("kmm_upload", "kmm_download"):
+            getattr(L, fn).argtypes = [vp, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]
+            getattr(L, fn).restype = ctypes.c_int
+        L.kmm_get_stats.argtypes = [vp, ctypes.POINTER(abi.KmmStats)]
+        L.kmm_get_stats.restype = ctypes.c_int
+        L.kmm_set_timing.argtypes = [vp, ctypes.c_int]
+        L.kmm_set_timing.restype = ctypes.c_int
+        L.kmm_get_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        L.kmm_get_stage_times.restype = ctypes.c_int
+        L.kmm_launch_count.argtypes = [vp]
+        L.kmm_launch_count.restype = ctypes.c_longlong
+        L.kmm_event_record.argtypes = [vp, ctypes.c_int]
+        L.kmm_event_record.restype = ctypes.c_int
+        L.kmm_event_elapsed.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.kmm_event_elapsed.restype = ctypes.c_int
+        for name, sig in _ROUTINES.items():
+            f = getattr(L, "kmm_" + name)
+            f.argtypes = [vp] + [_CT[c] for c in sig]
+            f.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    """Names the library must export (every entry point declared in include/kmm.h)."""
+    base = ["kmm_ctx_create", "kmm_ctx_destroy", "kmm_last_error", "kmm_abi_version", "kmm_field_size",
+            "kmm_upload", "kmm_download", "kmm_get_stats", "kmm_set_timing", "kmm_get_stage_times",
+            "kmm_launch_count", "kmm_event_record", "kmm_event_elapsed"]
+    return base + ["kmm_" + n for n in _ROUTINES]
+
+
+class KmmContext:
+    """A device context holding every field mirror of one channel run."""
+
+    def __init__(self, params, device=0):
+        self.params = params
+        self.L = lib()
+        self.h = ctypes.c_void_p()
+        st = self.L.kmm_ctx_create(ctypes.byref(params), int(device), ctypes.byref(self.h))
+        if st:
+            raise KmmError(st, "kmm_ctx_create")
+        self.nx, self.ny, self.nz, self.npart = params.nx, params.ny, params.nz, params.npart
+
+    def close(self):
+        if self.h:
+            self.L.kmm_ctx_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _id(self, f):
+        return abi.FIELD[f] if isinstance(f, str) else int(f)
+
+    def error(self):
+        m = self.L.kmm_last_error(self.h)
+        return m.decode() if m else ""
+
+    def _check(self, st, where, allow=()):
+        if st and st not in allow:
+            raise KmmError(st, where, self.error())
+        return st
+
+    def upload(self, f, arr):
+        fid = self._id(f)
+        _, dt = abi.field_kind(fid)
+        a = np.asarray(arr, dtype=np.dtype(dt))
+        a = np.asfortranarray(a.reshape(abi.field_shape(fid, self.nx, self.ny, self.nz, self.npart), order="F"))
+        self._check(self.L.kmm_upload(self.h, fid, a.ctypes.data, a.nbytes), "kmm_upload(%s)" % f)
+
+    def download(self, f):
+        fid = self._id(f)
+        _, dt = abi.field_kind(fid)
+        shape = abi.field_shape(fid, self.nx, self.ny, self.nz, self.npart)
+        a = np.empty(shape, dtype=np.dtype(dt), order="F")
+        self._check(self.L.kmm_download(self.h, fid, a.ctypes.data, a.nbytes), "kmm_download(%s)" % f)
+        return a
+
+    def call(self, name, *args, allow=()):
+        conv = [self._id(a) if isinstance(a, str) else a for a in args]
+        st = getattr(self.L, "kmm_" + name)(self.h, *conv)
+        return self._check(st, "kmm_" + name, allow)
+
+    def stats(self):
+        s = abi.KmmStats()
+        self._check(self.L.kmm_get_stats(self.h, ctypes.byref(s)), "kmm_get_stats")
+        return s
+
+    def set_timing(self, on):
+        self._check(self.L.kmm_set_timing(self.h, int(on)), "kmm_set_timing")
+
+    def stage_times(self):
+        n = 8
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_int * n)()
+        self._check(self.L.kmm_get_stage_times(self.h, ms, cnt, n), "kmm_get_stage_times")
+        names = ["column", "dct_fwd", "zfft_bwd", "xphys", "xfwd", "zfft_fwd", "dct_bwd", "post"]
+        return {names[i]: (ms[i], cnt[i]) for i in range(n)}
+
+    def launch_count(self):
+        return int(self.L.kmm_launch_count(self.h))
+
+    def event_record(self, slot):
+        self._check(self.L.kmm_event_record(self.h, slot), "kmm_event_record")
+
+    def event_elapsed(self, a, b):
+        ms = ctypes.c_double()
+        self._check(self.L.kmm_event_elapsed(self.h, a, b, ctypes.byref(ms)), "kmm_event_elapsed")
+        return ms.value
+
+    def upload_ptr(self, f, ptr, nbytes):
+        """Upload from a raw host pointer (e.g. pinned memory) in the reference layout."""
+        fid = self._id(f)
+        self._check(self.L.kmm_upload(self.h, fid, ctypes.c_void_p(ptr), nbytes), "kmm_upload(%s)" % f)
+
+    def download_ptr(self, f, ptr, nbytes):
+        fid = self._id(f)
+        self._check(self.L.kmm_download(self.h, fid, ctypes.c_void_p(ptr), nbytes), "kmm_download(%s)" % f)
+
+    # mirrors of the reference's main-program blocks
+    def initial(self):
+        return self.call("initial")
+
+    def step(self):
+        return self.call("step")
+
+    def run(self, n):
+        return self.call("run", n)

@@ -1,0 +1,297 @@
+"""GPU parity: every routine of the C ABI against the CPU oracle on the same seeded inputs.
+
+Tolerances (FP64 drop-in): per-routine results agree to <= 1e-12 relative (the column routines
+share the reference's operation order; transforms differ only in FFT rounding); whole runs agree
+to <= 1e-10 relative after 10 steps, the bar of the FP64 drop-in.  Relative error = max|a-b| /
+max|b| per field.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from polymer_dns_b200 import abi, inputs
+from tests import kmm_cases as kc
+
+pytestmark = pytest.mark.gpu
+
+ROUTINE_TOL = 1e-12
+RUN_TOL = 1e-10
+
+
+@pytest.fixture(scope="module")
+def rt():
+    from polymer_dns_b200 import build, runtime
+    build.build()
+    return runtime
+
+
+def _pair(rt, oracle_mod, p):
+    return rt.KmmContext(p), oracle_mod.Oracle(p)
+
+
+def _put(g, o, name, a):
+    g.upload(name, a)
+    o.set(name, a)
+
+
+def _cmp(g, o, name, tol=ROUTINE_TOL):
+    e = kc.rel_err(g.download(name), o.get(name))
+    assert e <= tol, "%s rel err %.3e > %.1e" % (name, e, tol)
+    return e
+
+
+GRIDS = [(16, 16, 12), (32, 32, 32), (24, 24, 16)]
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_cderiv_wallderiv_norm(rt, oracle_mod, grid):
+    p = kc.cfg_small(*grid)
+    g, o = _pair(rt, oracle_mod, p)
+    rng = np.random.default_rng(11)
+    a = kc.random_spectral(rng, p, hermitian=False)
+    _put(g, o, "WRKC", a)
+    g.call("cderiv", "WRKC", "WRK1")
+    o.call("cderiv", "WRKC", "WRK1")
+    assert np.array_equal(g.download("WRK1"), o.get("WRK1"))   # same operation order: bitwise
+    for order in (0, 1, 2):
+        for wall in (0, 1):
+            g.call("wallderiv", "WRKC", order, wall, "WRK1", 2 + order)
+            o.call("wallderiv", "WRKC", order, wall, "WRK1", 2 + order)
+    _cmp(g, o, "WRK1")
+    g.call("norm", "WRKC")
+    o.call("norm", "WRKC")
+    assert np.array_equal(g.download("WRKC"), o.get("WRKC"))
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_tau_solvers(rt, oracle_mod, grid):
+    p = kc.cfg_small(*grid)
+    g, o = _pair(rt, oracle_mod, p)
+    rng = np.random.default_rng(12)
+    for g_, ib in ((p.re / (p.dt * p.theta), 0), (0.0, 0), (1000.0, 1), (0.0, 1)):
+        a = kc.random_spectral(rng, p, hermitian=False)
+        bt = rng.standard_normal((p.nz, p.nx // 2)) + 1j * rng.standard_normal((p.nz, p.nx // 2))
+        bb = rng.standard_normal((p.nz, p.nx // 2)) + 1j * rng.standard_normal((p.nz, p.nx // 2))
+        for name, v in (("WRKC", a), ("BCTOP", bt), ("BCBOT", bb)):
+            _put(g, o, name, v)
+        g.call("solve", "WRKC", g_, ib)
+        o.call("solve", "WRKC", g_, ib)
+        _cmp(g, o, "WRKC")
+    for at, bt_, ab, bb_ in ((1.0, 0.0, 1.0, 0.0), (0.0, 1.0, 0.0, 1.0), (1.0, 0.3, 0.7, 0.5)):
+        a = kc.random_spectral(rng, p, hermitian=False)
+        _put(g, o, "WRKC", a)
+        gt = rng.standard_normal((p.nz, p.nx // 2)) + 1j * rng.standard_normal((p.nz, p.nx // 2))
+        _put(g, o, "BCTOP", gt)
+        _put(g, o, "BCBOT", -gt)
+        g.call("penta", "WRKC", 2800.0, 0, at, bt_, ab, bb_)
+        o.call("penta", "WRKC", 2800.0, 0, at, bt_, ab, bb_)
+        _cmp(g, o, "WRKC")
+
+
+def test_mean_mode_and_spectral_routines(rt, oracle_mod):
+    p = kc.cfg_small(16, 24, 16)
+    g, o = _pair(rt, oracle_mod, p)
+    rng = np.random.default_rng(13)
+    for name in ("V", "OMY", "FN", "FNM1", "GN", "GNM1", "OMZ", "U", "W"):
+        _put(g, o, name, kc.random_spectral(rng, p))
+    for name in ("U0", "W0", "H1N", "H1NM1", "H3N", "H3NM1"):
+        v = np.zeros(p.ny + 1)
+        v[:12] = rng.standard_normal(12)
+        _put(g, o, name, v)
+    for r in ("phi_from_v",):
+        g.call(r); o.call(r)
+    _cmp(g, o, "V")
+    g.call("phirhs", "V", "FN", "FNM1", 1.0)
+    o.call("phirhs", "V", "FN", "FNM1", 1.0)
+    _cmp(g, o, "V")
+    g.call("uzero", 1); o.call("uzero", 1)
+    g.call("uzero", 3); o.call("uzero", 3)
+    _cmp(g, o, "U0")
+    _cmp(g, o, "W0")
+    for r in ("veloc", "vort", "gradv", "nonlin"):
+        g.call(r)
+        o.call(r)
+    for name in ("U", "W", "OMX", "OMZ", "U11", "U12", "U33", "LU", "LW", "FN", "GN"):
+        _cmp(g, o, name)
+    g.call("filter"); o.call("filter")
+    for name in ("FN", "GN", "OMZ"):
+        _cmp(g, o, name)
+
+
+def test_gfcn_and_influence(rt, oracle_mod):
+    p = kc.cfg_small(16, 32, 16)
+    g, o = _pair(rt, oracle_mod, p)
+    g.call("gfcn")
+    o.call("gfcn")
+    for name in ("GF1", "GF2", "DNV1B", "DNV1T", "DNV2B", "DNV2T", "DENOM"):
+        _cmp(g, o, name)
+    rng = np.random.default_rng(14)
+    _put(g, o, "V", kc.random_spectral(rng, p))
+    g.call("influence")
+    o.call("influence")
+    _cmp(g, o, "V")
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_xyzfft(rt, oracle_mod, grid):
+    p = kc.cfg_small(*grid)
+    g, o = _pair(rt, oracle_mod, p)
+    iu, iv, iw = kc.initial_fields(p)
+    _put(g, o, "INITU", iu)
+    g.call("xyzfft", "U", "INITU")
+    o.call("xyzfft", "U", "INITU")
+    _cmp(g, o, "U")
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_vcw3dp_fluid(rt, oracle_mod, grid):
+    p = kc.cfg_small(*grid, dt=1e-5)
+    g, o = _pair(rt, oracle_mod, p)
+    rng = np.random.default_rng(15)
+    for name in ("U", "V", "W", "OMX", "OMY", "OMZ"):
+        _put(g, o, name, kc.random_spectral(rng, p))
+    assert g.call("vcw3dp") == 0
+    assert o.call("vcw3dp") == 0
+    for name in ("GN", "FN", "OMZ"):
+        _cmp(g, o, name)
+    _cmp(g, o, "UP3D")
+    assert abs(g.stats().cflmax - o.stats().cflmax) <= 1e-12 * o.stats().cflmax
+
+
+def test_vcw3dp_scalar_polymer_ib(rt, oracle_mod):
+    p = kc.cfg_small(16, 24, 16, dt=1e-5, scalar_on=1, polymer_on=1, scalar_q=0.3, zlmax=30.0, tpoly=20.0,
+                     qbeta=0.9, gain=-400.0, ugain=-40.0)
+    g, o = _pair(rt, oracle_mod, p)
+    rng = np.random.default_rng(16)
+    names = ["U", "V", "W", "OMX", "OMY", "OMZ", "U11", "U12", "U13", "U21", "U22", "U23", "U31", "U32", "U33",
+             "SCALAR", "SCLX", "SCLY", "SCLZ"] + ["C%d%d" % (i, j) for i in (1, 2, 3) for j in (1, 2, 3)] \
+        + ["DC%d%d%d" % (i, j, k) for i in (1, 2, 3) for j in (1, 2, 3) for k in (1, 2, 3)]
+    for name in names:
+        a = kc.random_spectral(rng, p) * 0.1
+        if name in ("C11", "C22", "C33"):
+            a[0, 0, 0] += 1.0
+        _put(g, o, name, a)
+    im = inputs.cylinder_imatrix(p.nx, p.ny, p.nz, p.xl, p.yl, xc=math.pi, yc=0.0, radius=0.25)
+    _put(g, o, "IMATRIX", im)
+    fx = rng.standard_normal(im.shape) * 0.01
+    _put(g, o, "FXINTG", np.asfortranarray(fx))
+    assert g.call("vcw3dp") == 0
+    assert o.call("vcw3dp") == 0
+    for name in ("GN", "FN", "OMZ", "SCN", "C11N", "C23N", "STR11N", "STR33N", "QP12", "QP33"):
+        _cmp(g, o, name)
+    for name in ("FXINTG", "FYINTG", "FZINTG"):
+        _cmp(g, o, name)
+
+
+def test_spreading_semantics(rt, oracle_mod):
+    """Solid cells inside the spreading planes (i <= kmaxsurf) exercise the 5x5 scatter order."""
+    p = kc.cfg_small(16, 16, 12, dt=1e-5, gain=-4.0, ugain=-2.0)
+    g, o = _pair(rt, oracle_mod, p)
+    rng = np.random.default_rng(17)
+    for name in ("U", "V", "W", "OMX", "OMY", "OMZ"):
+        _put(g, o, name, kc.random_spectral(rng, p))
+    mx, mz = 3 * p.nx // 2, 3 * p.nz // 2
+    im = np.zeros((p.ny + 1, mz, mx), np.int32, order="F")
+    im[1:6, :, 3:9] = 1                 # planes 2..6 (1-based), x columns 4..9 -> kmaxsurf = 9
+    im[2, 0:2, 0] = 3                   # z-edge cells next to the x seam
+    im[3, mz - 2:, mx - 1] = 1
+    _put(g, o, "IMATRIX", im)
+    assert g.call("vcw3dp") == 0
+    assert o.call("vcw3dp") == 0
+    for name in ("GN", "FN", "OMZ", "FXINTG", "FZINTG"):
+        _cmp(g, o, name)
+
+
+def test_tracers(rt, oracle_mod):
+    p = kc.cfg_small(16, 24, 16, npart=2000, ap=1e-3)
+    g, o = _pair(rt, oracle_mod, p)
+    rng = np.random.default_rng(18)
+    for name in ("U", "V", "W", "OMX", "OMY", "OMZ"):
+        _put(g, o, name, kc.random_spectral(rng, p) * 0.05)
+    x, y, z = inputs.uniform_particles(p.npart, p.xl, p.yl, p.zl, p.ap, 2)
+    for n, a in (("XPART", x), ("YPART", y), ("ZPART", z)):
+        _put(g, o, n, a)
+    for it in (0, 1, 2):
+        g.call("set_it", it)
+        o.call("set_it", it)
+        assert g.call("vcw3dp") == 0
+        assert o.call("vcw3dp") == 0
+    for n in ("XPART", "YPART", "ZPART", "UPART", "VPART", "WPART"):
+        _cmp(g, o, n)
+
+
+# ----------------------------------------------------------------------------- whole runs
+def _run_pair(rt, oracle_mod, p, nsteps, fields, scalar=None, imatrix=None, particles=None):
+    g, o = _pair(rt, oracle_mod, p)
+    for ctx in (g, o):
+        kc.load_initial(ctx, p, fields, scalar)
+        if imatrix is not None:
+            (ctx.upload if hasattr(ctx, "upload") else ctx.set)("IMATRIX", imatrix)
+        if particles is not None:
+            for n, a in zip(("XPART", "YPART", "ZPART"), particles):
+                (ctx.upload if hasattr(ctx, "upload") else ctx.set)(n, a)
+    assert g.initial() == 0
+    assert o.initial() == 0
+    for _ in range(nsteps):
+        assert g.step() == 0
+        assert o.step() == 0
+    return g, o
+
+
+@pytest.mark.parametrize("grid", [(32, 32, 32), (24, 32, 16)])
+def test_fp64_dropin_10_steps(rt, oracle_mod, grid):
+    """The plain drop-in bar: max relative field difference <= 1e-10 after 10 steps."""
+    p = kc.cfg_small(*grid)
+    g, o = _run_pair(rt, oracle_mod, p, 10, kc.initial_fields(p, amp=0.05, seed=0))
+    for name in kc.SPECTRAL_STATE[:6]:
+        _cmp(g, o, name, RUN_TOL)
+    for name in kc.MEAN_STATE:
+        _cmp(g, o, name, RUN_TOL)
+
+
+def test_dropin_scalar_tracers_10_steps(rt, oracle_mod):
+    p = kc.cfg_small(32, 32, 32, scalar_on=1, diff=1.0, scalar_bc=1, scalar_q=1.0, npart=1000, ap=1e-3,
+                     tracer_scheme=0)
+    fields = kc.initial_fields(p, amp=0.05, seed=1)
+    parts = inputs.uniform_particles(p.npart, p.xl, p.yl, p.zl, p.ap, 2)
+    g, o = _run_pair(rt, oracle_mod, p, 10, fields, scalar=np.zeros_like(fields[0]), particles=parts)
+    for name in ("V", "OMY", "FN", "GN", "SCALAR", "SCN"):
+        _cmp(g, o, name, RUN_TOL)
+    for name in ("XPART", "YPART", "ZPART"):
+        _cmp(g, o, name, RUN_TOL)
+
+
+def test_dropin_polymer_ib_10_steps(rt, oracle_mod):
+    p = kc.cfg_small(32, 32, 32, scalar_on=1, polymer_on=1, diff=1.0, scalar_bc=1, scalar_q=1.0,
+                     zlmax=30.0, tpoly=20.0, qbeta=0.9, diffpoly=1000.0, gain=-400.0, ugain=-40.0, dt=0.005)
+    fields = kc.initial_fields(p, amp=0.05, seed=1)
+    im = inputs.cylinder_imatrix(p.nx, p.ny, p.nz, p.xl, p.yl, xc=math.pi, yc=0.0, radius=0.25)
+    g, o = _run_pair(rt, oracle_mod, p, 10, fields, scalar=np.zeros_like(fields[0]), imatrix=im)
+    for name in ("V", "OMY", "FN", "GN", "SCALAR", "C11", "C12", "C22", "C33", "STR11N", "QP12"):
+        _cmp(g, o, name, RUN_TOL)
+
+
+def test_full_size_properties():
+    """128x129x128 (the Re_tau = 180 grid): continuity and the laminar steady state hold on the GPU."""
+    from polymer_dns_b200 import runtime
+    p = kc.cfg_small(128, 128, 128, dt=0.005, re=2800.0, xl=4 * math.pi, zl=4 * math.pi / 3)
+    with runtime.KmmContext(p) as g:
+        kc.load_initial(g, p, kc.initial_fields(p, amp=0.0))
+        assert g.initial() == 0
+        u0 = g.download("U0")
+        assert g.run(5) == 0
+        assert np.abs(g.download("U0") - u0).max() < 1e-12
+        assert np.abs(g.download("V")).max() < 1e-12
+    with runtime.KmmContext(p) as g:
+        kc.load_initial(g, p, kc.initial_fields(p, profile="loglaw", amp=0.1, kmax=8, seed=1))
+        assert g.initial() == 0
+        assert g.run(5) == 0
+        u, w = g.download("U"), g.download("W")
+        g.call("cderiv", "V", "WRKC")
+        dv = g.download("WRKC")
+        kx = np.arange(p.nx // 2) * 2 * math.pi / p.xl
+        kz = np.fft.fftfreq(p.nz, 1.0 / p.nz) * 2 * math.pi / p.zl
+        div = 1j * kx[None, None, :] * u + dv + 1j * kz[None, :, None] * w
+        assert np.abs(div).max() < 1e-11 * np.abs(u).max()
+        assert 0 < g.stats().cflmax < 1.0
