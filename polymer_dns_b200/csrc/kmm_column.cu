@@ -72,11 +72,7 @@ __global__ void __launch_bounds__(TPB) k_cderiv(const double2 *__restrict__ f, d
 int kmm_internal_cderiv(kmm_ctx *ctx, const double2 *f, double2 *df) {
     const int ncols = ctx->nz * ctx->nxh;
     const size_t sm = tile_smem(ctx->nyp, 2);
-    static bool attr = false;
-    if (!attr) {
-        CK(cudaFuncSetAttribute(k_cderiv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(TILE * KMM_MAX_NYP * 2 * sizeof(double2))));
-        attr = true;
-    }
+    RET(kmm_smem_attr(ctx, (const void *)k_cderiv, sm));
     k_cderiv<<<(ncols + TILE - 1) / TILE, TPB, sm, ctx->stream>>>(f, df, ncols, ctx->nyp, ctx->dyde);
     CKL();
     return KMM_OK;
@@ -365,12 +361,8 @@ __global__ void __launch_bounds__(TPB) k_solve(double2 *__restrict__ u, const do
 
 int kmm_internal_solve(kmm_ctx *ctx, double2 *u, double g, int ib, const double2 *bct, const double2 *bcb) {
     const int ncols = ctx->nz * ctx->nxh;
-    static bool attr = false;
-    if (!attr) {
-        CK(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(TILE * KMM_MAX_NYP * (sizeof(double2) + sizeof(double)))));
-        attr = true;
-    }
     const size_t smem = tile_smem(ctx->nyp, 1) + sizeof(double) * TILE * (size_t)(ctx->nyhp + 1);
+    RET(kmm_smem_attr(ctx, (const void *)k_solve, smem));
     k_solve<<<(ncols + TILE - 1) / TILE, TPB, smem, ctx->stream>>>(
         u, bct, bcb, ctx->d_wavx, ctx->d_wavz, ncols, ctx->nz, ctx->nyp, g, ib, ctx->dyde, ctx->h_c[0]);
     CKL();
@@ -486,12 +478,8 @@ __global__ void __launch_bounds__(TPB) k_penta(double2 *__restrict__ u, const do
 int kmm_internal_penta(kmm_ctx *ctx, double2 *u, double g, int ib, double at, double bt, double ab, double bb,
                        const double2 *gt, const double2 *gb) {
     const int ncols = ctx->nz * ctx->nxh;
-    static bool attr = false;
-    if (!attr) {
-        CK(cudaFuncSetAttribute(k_penta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(TILE * KMM_MAX_NYP * (sizeof(double2) + sizeof(double)))));
-        attr = true;
-    }
     const size_t smem = tile_smem(ctx->nyp, 1) + sizeof(double) * TILE * 2 * (size_t)(ctx->nyhp + 1);
+    RET(kmm_smem_attr(ctx, (const void *)k_penta, smem));
     k_penta<<<(ncols + TILE - 1) / TILE, TPB, smem, ctx->stream>>>(
         u, gt, gb, ctx->d_wavx, ctx->d_wavz, ncols, ctx->nz, ctx->nyp, g, ib, at, bt, ab, bb, ctx->dyde, ctx->h_c[0]);
     CKL();

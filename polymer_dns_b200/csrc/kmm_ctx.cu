@@ -388,3 +388,14 @@ extern "C" int kmm_event_elapsed(kmm_ctx *ctx, int a, int b, double *ms) {
     *ms = (double)t;
     return KMM_OK;
 }
+
+// raise a kernel's dynamic shared-memory limit to `bytes` (>48 KB needs the opt-in; max 227 KB)
+int kmm_smem_attr(kmm_ctx *ctx, const void *func, size_t bytes) {
+    if (bytes <= 48 * 1024) return KMM_OK;
+    if (bytes > 227 * 1024) {
+        kmm_set_error(ctx, "kernel needs %zu bytes of shared memory (> 227 KB)", bytes);
+        return KMM_ERR_UNSUPPORTED;
+    }
+    CK(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return KMM_OK;
+}

@@ -108,6 +108,7 @@ int kmm_internal_penta(kmm_ctx *ctx, double2 *u, double g, int ib, double at, do
 int kmm_internal_axpy_spec(kmm_ctx *ctx, double2 *y, const double2 *x, double a);
 int kmm_internal_set_constant_mode(kmm_ctx *ctx, double2 *a, double value);
 int kmm_plan_init(kmm_ctx *ctx, DevPlan *p, int n, int slot);
+int kmm_smem_attr(kmm_ctx *ctx, const void *func, size_t bytes);
 int kmm_ensure_plane_buffers(kmm_ctx *ctx, int nin, int nout);
 // (nyp,mz,mx) host array <-> internal [y][z][x] device array (one of host_src / host_dst is NULL)
 int kmm_phys_layout(kmm_ctx *ctx, int field, void *dev, const void *host_src, void *host_dst);

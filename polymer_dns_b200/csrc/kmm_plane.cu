@@ -467,7 +467,6 @@ int kmm_update_kmaxsurf(kmm_ctx *ctx) {
 // ---------------------------------------------------------------------------
 int kmm_tracers(kmm_ctx *ctx);   // kmm_tracer.cu
 
-static bool g_attr_done = false;
 
 extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     if (!ctx) return KMM_ERR_ARG;
@@ -573,23 +572,16 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         }
     }
 
-    if (!g_attr_done) {
-        CK(cudaFuncSetAttribute(k_dct_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-        CK(cudaFuncSetAttribute(k_dct_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-        CK(cudaFuncSetAttribute(k_zfft_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-        CK(cudaFuncSetAttribute(k_zfft_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-        CK(cudaFuncSetAttribute(k_xphys, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-        CK(cudaFuncSetAttribute(k_xfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-        g_attr_done = true;
-    }
     const size_t sm_dct = sizeof(double2) * 2 * DCT_CB * 2 * ctx->ny;
     const size_t sm_z = sizeof(double2) * 2 * ZKB * mz;
     const size_t sm_x = sizeof(double) * (size_t)nin * XZB * mx + sizeof(double2) * 2 * XZB * mx;
     const size_t sm_xf = sizeof(double2) * 2 * XZB * mx;
-    if (sm_x > 227 * 1024 || sm_dct > 227 * 1024 || sm_z > 227 * 1024) {
-        kmm_set_error(ctx, "vcw3dp shared-memory plan exceeds 227 KB (nin=%d, mx=%d)", nin, mx);
-        return KMM_ERR_UNSUPPORTED;
-    }
+    RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd, sm_dct));
+    RET(kmm_smem_attr(ctx, (const void *)k_dct_bwd, sm_dct));
+    RET(kmm_smem_attr(ctx, (const void *)k_zfft_bwd, sm_z));
+    RET(kmm_smem_attr(ctx, (const void *)k_zfft_fwd, sm_z));
+    RET(kmm_smem_attr(ctx, (const void *)k_xphys, sm_x));
+    RET(kmm_smem_attr(ctx, (const void *)k_xfwd, sm_xf));
     CK(cudaMemsetAsync(ctx->d_cfl, 0, sizeof(double) * nyp, ctx->stream));
     CK(cudaMemsetAsync(ctx->d_umax, 0, sizeof(double) * nyp, ctx->stream));
 

@@ -204,7 +204,7 @@ def test_spreading_semantics(rt, oracle_mod):
 
 
 def test_tracers(rt, oracle_mod):
-    p = kc.cfg_small(16, 24, 16, npart=2000, ap=1e-3)
+    p = kc.cfg_small(16, 24, 16, npart=2000, ap=1e-3, dt=1e-3)
     g, o = _pair(rt, oracle_mod, p)
     rng = np.random.default_rng(18)
     for name in ("U", "V", "W", "OMX", "OMY", "OMZ"):
