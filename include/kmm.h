@@ -239,6 +239,13 @@ int  kmm_tracer_update(kmm_ctx *ctx);
 /* init_part's velocity interpolation, part_track.f90:229-292 */
 int  kmm_init_part(kmm_ctx *ctx);
 
+/* ---- options --------------------------------------------------------------- */
+enum kmm_option {
+    KMM_OPT_FUSED = 1   /* 1 (default): kmm_step runs the fused kernels when the run has no polymer and no
+                           immersed boundary; 0: kmm_step runs the routine-by-routine kernels   */
+};
+int  kmm_set_option(kmm_ctx *ctx, int option, int value);
+
 /* ---- instrumentation (no counterpart in the reference, whose only profiling is the
  * cadence timer of main_dns.f90:797-809) --------------------------------------- */
 enum kmm_stage {

@@ -167,6 +167,19 @@ int kmm_plan_init(kmm_ctx *ctx, DevPlan *p, int n, int slot) {
     return KMM_OK;
 }
 
+// same transform length and twiddle table, factors ordered 8, 4, 2, 3, 5 (fewer warp-FFT stages)
+void kmm_plan_r8(const DevPlan *src, DevPlan *dst) {
+    *dst = *src;
+    int m = src->n, nf = 0;
+    static const int rads[5] = {8, 4, 2, 3, 5};
+    for (int r = 0; r < 5; ++r)
+        while (m % rads[r] == 0 && nf < KMM_MAX_FFT_FACTORS) {
+            dst->fac[nf++] = rads[r];
+            m /= rads[r];
+        }
+    dst->nf = nf;
+}
+
 // setbcs, main_dns.f90:1175-1418
 static void setbcs(kmm_ctx *c) {
     switch (c->p.flow_select) {
@@ -253,6 +266,7 @@ extern "C" int kmm_ctx_create(const kmm_params *p, int device, kmm_ctx **out) {
         c->substep = (int)ceil(s > 1.0 ? s : 1.0);
     }
     c->kmaxsurf = -1;
+    c->use_fused = 1;
 #define DUP(dst, src, n)                                                        \
     do {                                                                        \
         CK(cudaMalloc(&(dst), sizeof(double) * (size_t)(n)));                   \
@@ -279,6 +293,11 @@ extern "C" int kmm_ctx_create(const kmm_params *p, int device, kmm_ctx **out) {
     if (!st) st = kmm_plan_init(c, &c->pmx, c->mx, 2);
     if (!st) st = kmm_plan_init(c, &c->pnx, c->nx, 3);
     if (!st) st = kmm_plan_init(c, &c->pnz, c->nz, 4);
+    if (!st) {
+        kmm_plan_r8(&c->py2, &c->wy2);
+        kmm_plan_r8(&c->pmz, &c->wmz);
+        kmm_plan_r8(&c->pmx, &c->wmx);
+    }
     if (st) {
         kmm_ctx_destroy(c);
         return st;
@@ -295,6 +314,9 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
         for (int e = 0; e < 2 * KMM_TIMER_RECORDS; ++e) cudaEventDestroy(ctx->tm_ev[e]);
     for (int e = 0; e < 16; ++e)
         if (ctx->user_ev[e]) cudaEventDestroy(ctx->user_ev[e]);
+    kmm_fused_release(ctx);
+    if (ctx->po) cudaFree(ctx->po);
+    if (ctx->drag) cudaFree(ctx->drag);
     for (int f = 0; f < KMM_MAXF; ++f)
         if (ctx->f[f]) cudaFree(ctx->f[f]);
     for (int w = 0; w < 6; ++w)
@@ -398,4 +420,12 @@ int kmm_smem_attr(kmm_ctx *ctx, const void *func, size_t bytes) {
     }
     CK(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     return KMM_OK;
+}
+
+extern "C" int kmm_set_option(kmm_ctx *ctx, int option, int value) {
+    if (!ctx) return KMM_ERR_ARG;
+    switch (option) {
+    case KMM_OPT_FUSED: ctx->use_fused = value ? 1 : 0; return KMM_OK;
+    default: return KMM_ERR_ARG;
+    }
 }

@@ -55,6 +55,7 @@ struct kmm_ctx {
     double p1t, p1b, p2t, p2b;
     int substep;
     int it;
+    int in_step;                 // inside kmm_step (intermediate copies only kept when needed)
     int kmaxsurf;
     // host and device copies of wavenumbers, Chebyshev weights, grid
     double *h_wavx, *h_wavz, *h_c, *h_ycoord, *h_seght;
@@ -74,6 +75,7 @@ struct kmm_ctx {
     double *d_scratch;           // 9*KMM_MAX_NYP doubles for the (0,0)-mode solver
     double *scsource;            // (nyp,mz,mx) scalar source (scl_flag = 2)
     DevPlan py2, pmz, pmx, pnx, pnz;
+    DevPlan wy2, wmz, wmx;        // same lengths, radix-8-first factorisation for the warp FFT
     double2 *tw_store[5];
     kmm_stats stats;
     char err[512];
@@ -85,8 +87,16 @@ struct kmm_ctx {
     cudaEvent_t tm_ev[2 * KMM_TIMER_RECORDS];
     int tm_ev_ready;
     cudaEvent_t user_ev[16];
+    // fused-path state (tau tables, stage buffers) and the general path's physical scratch
+    struct KmmFused *fused;
+    double *po, *drag;
+    size_t po_n, drag_n;
+    int use_fused;
 };
 
+void kmm_fused_release(kmm_ctx *ctx);
+int kmm_fused_step(kmm_ctx *ctx);
+bool kmm_fused_applicable(const kmm_ctx *ctx);
 void kmm_tic(kmm_ctx *ctx);
 void kmm_toc(kmm_ctx *ctx, int stage);
 
@@ -108,6 +118,7 @@ int kmm_internal_penta(kmm_ctx *ctx, double2 *u, double g, int ib, double at, do
 int kmm_internal_axpy_spec(kmm_ctx *ctx, double2 *y, const double2 *x, double a);
 int kmm_internal_set_constant_mode(kmm_ctx *ctx, double2 *a, double value);
 int kmm_plan_init(kmm_ctx *ctx, DevPlan *p, int n, int slot);
+void kmm_plan_r8(const DevPlan *src, DevPlan *dst);
 int kmm_smem_attr(kmm_ctx *ctx, const void *func, size_t bytes);
 int kmm_ensure_plane_buffers(kmm_ctx *ctx, int nin, int nout);
 // (nyp,mz,mx) host array <-> internal [y][z][x] device array (one of host_src / host_dst is NULL)
@@ -217,6 +228,70 @@ __device__ __forceinline__ double2 *fft_smem(const DevPlan &P, double2 *a, doubl
                 if (q < R) dp[idxD + q * Ns] = v[q];
         }
         __syncthreads();
+        double2 *tmp = src;
+        src = dst;
+        dst = tmp;
+        Ns *= R;
+    }
+    return src;
+}
+
+// radix-8 DFT (two radix-4 halves + the W8 twiddles), same sign convention as radix_dft
+__device__ __forceinline__ void radix8_dft(double2 *v, int sign) {
+    double2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+    radix_dft(4, e, sign);
+    radix_dft(4, o, sign);
+    const double h = 0.70710678118654752440;
+    // W8^q o[q], W8 = exp(sign 2 pi i / 8)
+    double2 t1 = make_double2(h * (o[1].x - sign * o[1].y), h * (o[1].y + sign * o[1].x));
+    double2 t2 = sign < 0 ? make_double2(o[2].y, -o[2].x) : make_double2(-o[2].y, o[2].x);
+    double2 t3 = make_double2(h * (-o[3].x - sign * o[3].y), h * (-o[3].y + sign * o[3].x));
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], t1);
+    v[5] = csub(e[1], t1);
+    v[2] = cadd(e[2], t2);
+    v[6] = csub(e[2], t2);
+    v[3] = cadd(e[3], t3);
+    v[7] = csub(e[3], t3);
+}
+
+// ---------------------------------------------------------------------------
+// warp-private Stockham FFT: one sequence of length P.n in the warp's own shared buffers a, b;
+// only __syncwarp between stages.  Radices 8, 4, 2, 3, 5 (plan from kmm_plan_r8).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 *fft_warp(const DevPlan &P, double2 *a, double2 *b, int sign) {
+    const int n = P.n;
+    const int lane = threadIdx.x & 31;
+    double2 *src = a, *dst = b;
+    int Ns = 1;
+    for (int f = 0; f < P.nf; ++f) {
+        const int R = P.fac[f];
+        const int nR = n / R;
+        const int tstep = n / (Ns * R);
+        for (int j = lane; j < nR; j += 32) {
+            const int k = j % Ns;
+            double2 v[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                if (r < R) {
+                    double2 x = src[j + r * nR];
+                    if (r && k) {
+                        double2 w = __ldg(&P.tw[(r * k * tstep) % n]);
+                        if (sign > 0) w.y = -w.y;
+                        x = cmul(x, w);
+                    }
+                    v[r] = x;
+                }
+            }
+            if (R == 8) radix8_dft(v, sign);
+            else radix_dft(R, v, sign);
+            const int idxD = (j / Ns) * Ns * R + k;
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (q < R) dst[idxD + q * Ns] = v[q];
+        }
+        __syncwarp();
         double2 *tmp = src;
         src = dst;
         dst = tmp;

@@ -412,22 +412,19 @@ __global__ void __launch_bounds__(256) k_dct_bwd(const double2 *__restrict__ pl,
 // ---------------------------------------------------------------------------
 // physical scratch (outputs, drag) sized on demand
 // ---------------------------------------------------------------------------
-static double *g_po = NULL, *g_drag = NULL;
-static size_t g_po_n = 0, g_drag_n = 0;
-
 static int ensure_phys(kmm_ctx *ctx, int nout, bool need_drag) {
     size_t n = ctx->nphys * (size_t)nout;
-    if (n > g_po_n) {
-        if (g_po) cudaFree(g_po);
-        g_po = NULL;
-        CK(cudaMalloc(&g_po, sizeof(double) * n));
-        g_po_n = n;
+    if (n > ctx->po_n) {
+        if (ctx->po) { CK(cudaStreamSynchronize(ctx->stream)); cudaFree(ctx->po); }
+        ctx->po = NULL;
+        CK(cudaMalloc(&ctx->po, sizeof(double) * n));
+        ctx->po_n = n;
     }
-    if (need_drag && 3 * ctx->nphys > g_drag_n) {
-        if (g_drag) cudaFree(g_drag);
-        g_drag = NULL;
-        CK(cudaMalloc(&g_drag, sizeof(double) * 3 * ctx->nphys));
-        g_drag_n = 3 * ctx->nphys;
+    if (need_drag && 3 * ctx->nphys > ctx->drag_n) {
+        if (ctx->drag) { CK(cudaStreamSynchronize(ctx->stream)); cudaFree(ctx->drag); }
+        ctx->drag = NULL;
+        CK(cudaMalloc(&ctx->drag, sizeof(double) * 3 * ctx->nphys));
+        ctx->drag_n = 3 * ctx->nphys;
     }
     return KMM_OK;
 }
@@ -466,6 +463,8 @@ int kmm_update_kmaxsurf(kmm_ctx *ctx) {
 // driver
 // ---------------------------------------------------------------------------
 int kmm_tracers(kmm_ctx *ctx);   // kmm_tracer.cu
+int kmm_fast_x(kmm_ctx *ctx, const double2 *q, double2 *r, int nin, int nout, bool save_uvw, double *up3,
+               double *vp3, double *wp3);   // kmm_fast.cu
 
 
 extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
@@ -595,24 +594,36 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
                                                                                    nyp, nz, nxh, mz);
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_BWD);
-    kmm_tic(ctx);
-    k_xphys<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_x, ctx->stream>>>(
-        ctx->q_in, g_po, g_drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl,
-        ctx->d_umax, ctx->pmx, A, nyp, mz, mx, nxh);
-    CKL();
-    kmm_toc(ctx, KMM_STAGE_XPHYS);
-    if (ib_any && ctx->kmaxsurf > 0) {
-        const int ksp = ctx->kmaxsurf < nyp ? ctx->kmaxsurf : nyp;
-        k_spread<<<dim3(kmm_blocks((size_t)mz * mx, 256) > 64 ? 64 : kmm_blocks((size_t)mz * mx, 256), ksp), 256, 0,
-                   ctx->stream>>>(g_po, g_drag, ctx->d_fspread, nyp, mz, mx, ctx->kmaxsurf, A.slot_of_out[O_H1],
-                                  A.slot_of_out[O_H2], A.slot_of_out[O_H3]);
-        CKL();
+    bool fast_done = false;
+    if (!poly && !ib_any) {
+        // fused warp-per-row x stage (no polymer, no immersed boundary)
+        kmm_tic(ctx);
+        const bool save = ctx->p.npart > 0 || !ctx->in_step;
+        const int fst = kmm_fast_x(ctx, ctx->q_in, ctx->q_out, nin, nout, save, up3, vp3, wp3);
+        if (fst == KMM_OK) fast_done = true;
+        else if (fst != KMM_ERR_UNSUPPORTED) return fst;
+        kmm_toc(ctx, KMM_STAGE_XPHYS);
     }
-    kmm_tic(ctx);
-    k_xfwd<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_xf, ctx->stream>>>(g_po, ctx->q_out, ctx->pmx, nout, nyp, mz,
-                                                                         mx, nxh);
-    CKL();
-    kmm_toc(ctx, KMM_STAGE_XFWD);
+    if (!fast_done) {
+        kmm_tic(ctx);
+        k_xphys<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_x, ctx->stream>>>(
+            ctx->q_in, ctx->po, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl,
+            ctx->d_umax, ctx->pmx, A, nyp, mz, mx, nxh);
+        CKL();
+        kmm_toc(ctx, KMM_STAGE_XPHYS);
+        if (ib_any && ctx->kmaxsurf > 0) {
+            const int ksp = ctx->kmaxsurf < nyp ? ctx->kmaxsurf : nyp;
+            k_spread<<<dim3(kmm_blocks((size_t)mz * mx, 256) > 64 ? 64 : kmm_blocks((size_t)mz * mx, 256), ksp), 256, 0,
+                       ctx->stream>>>(ctx->po, ctx->drag, ctx->d_fspread, nyp, mz, mx, ctx->kmaxsurf, A.slot_of_out[O_H1],
+                                      A.slot_of_out[O_H2], A.slot_of_out[O_H3]);
+            CKL();
+        }
+        kmm_tic(ctx);
+        k_xfwd<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_xf, ctx->stream>>>(ctx->po, ctx->q_out, ctx->pmx, nout, nyp, mz,
+                                                                             mx, nxh);
+        CKL();
+        kmm_toc(ctx, KMM_STAGE_XFWD);
+    }
     kmm_tic(ctx);
     k_zfft_fwd<<<dim3((nxh + ZKB - 1) / ZKB, nyp, nout), 256, sm_z, ctx->stream>>>(ctx->q_out, ctx->pl_out, ctx->pmz,
                                                                                     nyp, nz, nxh, mz,

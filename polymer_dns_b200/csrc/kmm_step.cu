@@ -259,6 +259,7 @@ extern "C" int kmm_initial(kmm_ctx *ctx) {
 // ---------------------------------------------------------------------------
 extern "C" int kmm_step(kmm_ctx *ctx) {
     if (!ctx) return KMM_ERR_ARG;
+    if (ctx->use_fused && kmm_fused_applicable(ctx)) return kmm_fused_step(ctx);
     const double re = ctx->re, dt = ctx->dt, th = ctx->theta;
     ctx->it += 1;
     const int it = ctx->it;
@@ -340,7 +341,9 @@ extern "C" int kmm_step(kmm_ctx *ctx) {
         RET(poly_norm_dc(ctx));
     }
     kmm_toc(ctx, KMM_STAGE_COLUMN);
+    ctx->in_step = 1;
     int st = kmm_vcw3dp(ctx);
+    ctx->in_step = 0;
     if (st != KMM_OK) return st;
     kmm_tic(ctx);
     { static const int l[5] = {KMM_V, KMM_OMY, KMM_FN, KMM_GN, KMM_OMZ}; RET(norm_ids(ctx, l, 5)); }

@@ -23,6 +23,7 @@ _ROUTINES = {
     "veloc": "", "vort": "", "nonlin": "", "vcw3dp": "", "norm": "i", "xyzfft": "ii", "polynl": "",
     "polyforce": "", "subforce": "", "filter": "", "initial": "", "step": "", "run": "i",
     "tracer_update": "", "init_part": "", "copy": "ii", "zero": "i", "set_it": "i", "sync": "",
+    "set_option": "ii",
 }
 _CT = {"i": ctypes.c_int, "d": ctypes.c_double}
 

@@ -287,6 +287,7 @@ def test_full_size_properties():
         kc.load_initial(g, p, kc.initial_fields(p, profile="loglaw", amp=0.1, kmax=8, seed=1))
         assert g.initial() == 0
         assert g.run(5) == 0
+        g.call("veloc")   # the fused step keeps the prognostic state; u, w are derived on demand
         u, w = g.download("U"), g.download("W")
         g.call("cderiv", "V", "WRKC")
         dv = g.download("WRKC")
@@ -295,3 +296,31 @@ def test_full_size_properties():
         div = 1j * kx[None, None, :] * u + dv + 1j * kz[None, :, None] * w
         assert np.abs(div).max() < 1e-11 * np.abs(u).max()
         assert 0 < g.stats().cflmax < 1.0
+
+
+@pytest.mark.parametrize("grid,scalar", [((32, 32, 32), 0), ((24, 32, 16), 1), ((16, 64, 12), 1)])
+def test_fused_step_matches_routine_path(rt, oracle_mod, grid, scalar):
+    """kmm_step's fused kernels against the routine-by-routine kernels and the oracle after 5 steps."""
+    kw = dict(scalar_on=scalar, diff=1.0, scalar_bc=1, scalar_q=0.5) if scalar else {}
+    p = kc.cfg_small(*grid, **kw)
+    fields = kc.initial_fields(p, amp=0.05, seed=3)
+    sc = np.zeros_like(fields[0]) if scalar else None
+    ctxs = []
+    for fused in (1, 0):
+        g = rt.KmmContext(p)
+        g.call("set_option", 1, fused)
+        kc.load_initial(g, p, fields, sc)
+        assert g.initial() == 0
+        ctxs.append(g)
+    o = oracle_mod.Oracle(p)
+    kc.load_initial(o, p, fields, sc)
+    assert o.initial() == 0
+    for _ in range(5):
+        for g in ctxs:
+            assert g.step() == 0
+        assert o.step() == 0
+    names = ["V", "OMY", "FN", "FNM1", "GN", "GNM1", "U0", "W0", "H1N", "H3N"] + (["SCALAR", "SCN", "SCNM1"] if scalar else [])
+    for name in names:
+        a, b = ctxs[0].download(name), ctxs[1].download(name)
+        assert kc.rel_err(a, b) <= 1e-12, name
+        _cmp(ctxs[0], o, name, RUN_TOL)
