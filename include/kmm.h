@@ -246,6 +246,24 @@ enum kmm_option {
 };
 int  kmm_set_option(kmm_ctx *ctx, int option, int value);
 
+/* ---- transform without device allocation --------------------------------------
+ * kmm_xyzfft_noalloc has no counterpart in the reference.  It is kmm_xyzfft (the physical ->
+ * spectral transform of an initial field, helpers.f90:6-87) for callers that cannot allocate
+ * device memory: a host whose device memory belongs to another allocator or a fixed budget, or a
+ * time-critical loop that cannot afford cudaMalloc's implicit device synchronisation, and that
+ * therefore has no kmm context (creating one allocates).  The caller passes device pointers:
+ * `phys` real(8) (ny+1, nz, nx) and `spec` complex(8) (ny+1, nz, nx/2), both in the reference's
+ * Fortran layout, and a cudaStream_t (NULL for the legacy default stream).  Nothing is allocated:
+ * the working copy of the physical field lives in a file-scope device array of
+ * KMM_XYZFFT_NOALLOC_MAX doubles (32 MiB) that every GPU loading the library holds until the
+ * process exits; (ny+1)*nz*nx above that limit is rejected with KMM_ERR_ARG before any work, as are
+ * transform lengths 2*ny, nx, nz that are not 2^a 3^b 5^c or exceed 4096.  The first call on each
+ * device (the current one) resolves the array's device address once.  Every call on a device
+ * shares the array and overwrites it completely; calls that overlap on the GPU (other streams or
+ * host threads) race on it, so serialise them.                                          */
+#define KMM_XYZFFT_NOALLOC_MAX (4 * 1024 * 1024)
+int  kmm_xyzfft_noalloc(const double *phys, double *spec, int nx, int ny, int nz, void *stream);
+
 /* ---- instrumentation (no counterpart in the reference, whose only profiling is the
  * cadence timer of main_dns.f90:797-809) --------------------------------------- */
 enum kmm_stage {

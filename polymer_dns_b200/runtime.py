@@ -67,6 +67,8 @@ def lib():
         L.kmm_event_record.restype = ctypes.c_int
         L.kmm_event_elapsed.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
         L.kmm_event_elapsed.restype = ctypes.c_int
+        L.kmm_xyzfft_noalloc.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
+        L.kmm_xyzfft_noalloc.restype = ctypes.c_int
         for name, sig in _ROUTINES.items():
             f = getattr(L, "kmm_" + name)
             f.argtypes = [vp] + [_CT[c] for c in sig]
@@ -79,8 +81,14 @@ def exported_symbols():
     """Names the library must export (every entry point declared in include/kmm.h)."""
     base = ["kmm_ctx_create", "kmm_ctx_destroy", "kmm_last_error", "kmm_abi_version", "kmm_field_size",
             "kmm_upload", "kmm_download", "kmm_get_stats", "kmm_set_timing", "kmm_get_stage_times",
-            "kmm_launch_count", "kmm_event_record", "kmm_event_elapsed"]
+            "kmm_launch_count", "kmm_event_record", "kmm_event_elapsed", "kmm_xyzfft_noalloc"]
     return base + ["kmm_" + n for n in _ROUTINES]
+
+
+def xyzfft_noalloc(phys_dev_ptr, spec_dev_ptr, nx, ny, nz, stream=None):
+    """kmm_xyzfft_noalloc on raw device pointers (no context, no device allocation)."""
+    return lib().kmm_xyzfft_noalloc(ctypes.c_void_p(phys_dev_ptr), ctypes.c_void_p(spec_dev_ptr), int(nx), int(ny),
+                                    int(nz), ctypes.c_void_p(stream) if stream else None)
 
 
 class KmmContext:
