@@ -23,7 +23,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE
 # rounding like the reference's operation sequence
 PER_FILE = {"kmm_column.cu": ["-fmad=false"]}
 SOURCES = ["kmm_ctx.cu", "kmm_column.cu", "kmm_plane.cu", "kmm_fast.cu", "kmm_fused.cu", "kmm_tracer.cu", "kmm_step.cu", "kmm_noalloc.cu"]
-HEADERS = ["kmm_internal.cuh", "kmm_warpcol.cuh"]
+HEADERS = ["kmm_internal.cuh", "kmm_warpcol.cuh", "kmm_fft.cuh"]
 
 
 def nvcc():

@@ -9,7 +9,7 @@
 // outputs) whenever there is no polymer and no immersed boundary.
 #include <math.h>
 
-#include "kmm_internal.cuh"
+#include "kmm_fft.cuh"
 
 #define FX_WARPS 4
 #define FX_MAXF 10   // u v w wx wy wz [c cx cy cz]
@@ -20,13 +20,15 @@ struct FxArgs {
     double delxm, delzm, dt, dPdx, scalar_q;
 };
 
-template <int E>
+// MX > 0: the x length is the compile-time constant MX (specialised FFT); MX = 0: runtime plan
+template <int E, int MX>
 __global__ void __launch_bounds__(FX_WARPS * 32, 1) k_fx(const double2 *__restrict__ q, double2 *__restrict__ r,
                                                       double *__restrict__ up3, double *__restrict__ vp3,
                                                       double *__restrict__ wp3, const double *__restrict__ seght,
                                                       double *__restrict__ cfl, double *__restrict__ umax, DevPlan P,
-                                                      FxArgs A, int nyp, int mz, int mx, int nxh) {
+                                                      FxArgs A, int nyp, int mz, int mx_rt, int nxh) {
     extern __shared__ double2 sm[];
+    const int mx = MX > 0 ? MX : mx_rt;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y = blockIdx.y;
     const int z = blockIdx.x * FX_WARPS + warp;
@@ -55,7 +57,9 @@ __global__ void __launch_bounds__(FX_WARPS * 32, 1) k_fx(const double2 *__restri
                     a[k] = k <= hx ? make_double2(Av.x - Bv.y, Av.y + Bv.x) : make_double2(Av.x + Bv.y, -Av.y + Bv.x);
                 }
                 __syncwarp();
-                const double2 *res = fft_warp(P, a, b, +1);
+                const double2 *res;
+                if constexpr (MX > 0) res = fft_warp_ct<double2, MX, +1>(a, b, P.tw);
+                else res = fft_warp(P, a, b, +1);
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
                     const int x = lane + 32 * e;
@@ -112,12 +116,14 @@ __global__ void __launch_bounds__(FX_WARPS * 32, 1) k_fx(const double2 *__restri
                     if (x < mx) a[x] = make_double2(out[o][e], has_g && g < FX_MAXO ? out[g][e] : 0.0);
                 }
                 __syncwarp();
-                const double2 *res = fft_warp(P, a, b, -1);
+                const double2 *res;
+                if constexpr (MX > 0) res = fft_warp_ct<double2, MX, -1>(a, b, P.tw);
+                else res = fft_warp(P, a, b, -1);
                 double2 *ra = r + (((size_t)o * nyp + y) * mz + z) * nxh;
                 double2 *rb = r + (((size_t)g * nyp + y) * mz + z) * nxh;
                 for (int k = lane; k < nxh; k += 32) {
                     const double2 Z = res[k];
-                    const double2 Zc = cconj(res[(mx - k) % mx]);
+                    const double2 Zc = cconj(res[k == 0 ? 0 : mx - k]);
                     ra[k] = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
                     if (has_g) {
                         const double2 d = csub(Z, Zc);
@@ -160,23 +166,30 @@ int kmm_fast_x(kmm_ctx *ctx, const double2 *q, double2 *r, int nin, int nout, bo
     const size_t smem = sizeof(double2) * 2 * (size_t)mx * FX_WARPS;
     const dim3 grid((mz + FX_WARPS - 1) / FX_WARPS, ctx->nyp);
     const int E = (mx + 31) / 32;
-#define FX_LAUNCH(EE)                                                                                   \
+#define FX_LAUNCH(EE, MM)                                                                               \
     do {                                                                                                \
-        RET(kmm_smem_attr(ctx, (const void *)k_fx<EE>, smem));                                          \
-        k_fx<EE><<<grid, FX_WARPS * 32, smem, ctx->stream>>>(q, r, up3, vp3, wp3, ctx->d_seght, ctx->d_cfl, \
+        RET(kmm_smem_attr(ctx, (const void *)k_fx<EE, MM>, smem));                                      \
+        k_fx<EE, MM><<<grid, FX_WARPS * 32, smem, ctx->stream>>>(q, r, up3, vp3, wp3, ctx->d_seght, ctx->d_cfl, \
                                                             ctx->d_umax, ctx->wmx, A, ctx->nyp, mz, mx,   \
                                                             ctx->nxh);                                  \
         CKL();                                                                                          \
         return KMM_OK;                                                                                  \
     } while (0)
+    switch (mx) {   // specialised lengths: nx = 32, 64, 96, 128
+    case 48: FX_LAUNCH(2, 48);
+    case 96: FX_LAUNCH(3, 96);
+    case 144: FX_LAUNCH(5, 144);
+    case 192: FX_LAUNCH(6, 192);
+    default: break;
+    }
     switch (E) {
-    case 1: FX_LAUNCH(1);
-    case 2: FX_LAUNCH(2);
-    case 3: FX_LAUNCH(3);
-    case 5: FX_LAUNCH(5);
-    case 6: FX_LAUNCH(6);
-    case 9: FX_LAUNCH(9);
-    case 12: FX_LAUNCH(12);
+    case 1: FX_LAUNCH(1, 0);
+    case 2: FX_LAUNCH(2, 0);
+    case 3: FX_LAUNCH(3, 0);
+    case 5: FX_LAUNCH(5, 0);
+    case 6: FX_LAUNCH(6, 0);
+    case 9: FX_LAUNCH(9, 0);
+    case 12: FX_LAUNCH(12, 0);
     default: return KMM_ERR_UNSUPPORTED;
     }
 #undef FX_LAUNCH

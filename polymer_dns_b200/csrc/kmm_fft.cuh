@@ -1,0 +1,231 @@
+// kmm_fft.cuh -- warp-private Stockham FFTs specialised at compile time for one transform length.
+//
+// The runtime-plan FFT (fft_warp) spends most of its instructions on integer division, modulo and
+// radix dispatch.  Here the length N is a template argument: the radix sequence (8, 4, 2, 3, 5,
+// the order of kmm_plan_r8) and every stride are constants, the butterfly loop over j = lane +
+// 32 it has a fixed trip count, j % Ns and j / Ns become shifts for the power-of-two strides,
+// and the twiddle index r k tstep never reaches N, so it needs no modulo.  The arithmetic per
+// butterfly is the same as fft_warp's: twiddle multiply of inputs r >= 1, then the radix-R DFT.
+//
+// C is double2 or float2; the twiddle table holds exp(-2 pi i m / N), m = 0..N-1, in the same type.
+#pragma once
+
+#include "kmm_internal.cuh"
+
+namespace kct {
+
+__host__ __device__ constexpr int radix_at(int r) { return r == 0 ? 8 : r == 1 ? 4 : r == 2 ? 2 : r == 3 ? 3 : 5; }
+
+// number of factors of n over radices 8, 4, 2, 3, 5 (-1 when n has another prime factor)
+__host__ __device__ constexpr int nfac(int n) {
+    int c = 0;
+    for (int r = 0; r < 5; ++r)
+        while (n % radix_at(r) == 0) {
+            n /= radix_at(r);
+            ++c;
+        }
+    return n == 1 ? c : -1;
+}
+
+// f-th factor
+__host__ __device__ constexpr int fac(int n, int f) {
+    int c = 0;
+    for (int r = 0; r < 5; ++r)
+        while (n % radix_at(r) == 0) {
+            if (c == f) return radix_at(r);
+            n /= radix_at(r);
+            ++c;
+        }
+    return 1;
+}
+
+// product of the first f factors (the Stockham stride Ns of stage f)
+__host__ __device__ constexpr int stride(int n, int f) {
+    int p = 1;
+    for (int i = 0; i < f; ++i) p *= fac(n, i);
+    return p;
+}
+
+// ---- complex arithmetic on double2 / float2
+template <typename C>
+struct Real;
+template <>
+struct Real<double2> {
+    typedef double T;
+};
+template <>
+struct Real<float2> {
+    typedef float T;
+};
+
+template <typename C>
+__device__ __forceinline__ C mk(typename Real<C>::T x, typename Real<C>::T y) {
+    C c;
+    c.x = x;
+    c.y = y;
+    return c;
+}
+template <typename C>
+__device__ __forceinline__ C add(C a, C b) { return mk<C>(a.x + b.x, a.y + b.y); }
+template <typename C>
+__device__ __forceinline__ C sub(C a, C b) { return mk<C>(a.x - b.x, a.y - b.y); }
+template <typename C>
+__device__ __forceinline__ C mul(C a, C b) { return mk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+template <typename C>
+__device__ __forceinline__ C scl(C a, typename Real<C>::T s) { return mk<C>(a.x * s, a.y * s); }
+
+// radix-R DFTs, X_q = sum_r v_r exp(S 2 pi i r q / R); the same operation sequence as radix_dft /
+// radix8_dft of the runtime FFT
+template <typename C, int R, int S>
+struct Dft;
+
+template <typename C, int S>
+struct Dft<C, 2, S> {
+    static __device__ __forceinline__ void run(C *v) {
+        const C a0 = v[0], a1 = v[1];
+        v[0] = add(a0, a1);
+        v[1] = sub(a0, a1);
+    }
+};
+
+template <typename C, int S>
+struct Dft<C, 4, S> {
+    static __device__ __forceinline__ void run(C *v) {
+        const C a0 = add(v[0], v[2]), a1 = sub(v[0], v[2]);
+        const C b0 = add(v[1], v[3]);
+        const C d = sub(v[1], v[3]);
+        const C b1 = S < 0 ? mk<C>(d.y, -d.x) : mk<C>(-d.y, d.x);   // S i d
+        v[0] = add(a0, b0);
+        v[1] = add(a1, b1);
+        v[2] = sub(a0, b0);
+        v[3] = sub(a1, b1);
+    }
+};
+
+template <typename C, int S>
+struct Dft<C, 3, S> {
+    static __device__ __forceinline__ void run(C *v) {
+        typedef typename Real<C>::T T;
+        const T s3 = (T)0.86602540378443864676 * (T)S;
+        const C t1 = add(v[1], v[2]);
+        const C t2 = sub(v[0], scl(t1, (T)0.5));
+        const C d = sub(v[1], v[2]);
+        const C t3 = mk<C>(s3 * d.x, s3 * d.y);
+        const C o0 = add(v[0], t1);
+        v[1] = mk<C>(t2.x - t3.y, t2.y + t3.x);
+        v[2] = mk<C>(t2.x + t3.y, t2.y - t3.x);
+        v[0] = o0;
+    }
+};
+
+template <typename C, int S>
+struct Dft<C, 5, S> {
+    static __device__ __forceinline__ void run(C *v) {
+        typedef typename Real<C>::T T;
+        const T c5a = (T)0.30901699437494742410, c5b = (T)-0.80901699437494742410;
+        const T s5a = (T)0.95105651629515357212 * (T)S, s5b = (T)0.58778525229247312917 * (T)S;
+        const C t1 = add(v[1], v[4]), t2 = add(v[2], v[3]);
+        const C t3 = sub(v[1], v[4]), t4 = sub(v[2], v[3]);
+        const C o0 = add(v[0], add(t1, t2));
+        const C r1 = add(v[0], add(scl(t1, c5a), scl(t2, c5b)));
+        const C r2 = add(v[0], add(scl(t1, c5b), scl(t2, c5a)));
+        const C m1 = add(scl(t3, s5a), scl(t4, s5b));
+        const C m2 = sub(scl(t3, s5b), scl(t4, s5a));
+        const C i1 = mk<C>(-m1.y, m1.x), i2 = mk<C>(-m2.y, m2.x);
+        v[0] = o0;
+        v[1] = add(r1, i1);
+        v[4] = sub(r1, i1);
+        v[2] = add(r2, i2);
+        v[3] = sub(r2, i2);
+    }
+};
+
+template <typename C, int S>
+struct Dft<C, 8, S> {
+    static __device__ __forceinline__ void run(C *v) {
+        typedef typename Real<C>::T T;
+        C e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+        Dft<C, 4, S>::run(e);
+        Dft<C, 4, S>::run(o);
+        const T h = (T)0.70710678118654752440;
+        const C t1 = mk<C>(h * (o[1].x - (T)S * o[1].y), h * (o[1].y + (T)S * o[1].x));
+        const C t2 = S < 0 ? mk<C>(o[2].y, -o[2].x) : mk<C>(-o[2].y, o[2].x);
+        const C t3 = mk<C>(h * (-o[3].x - (T)S * o[3].y), h * (-o[3].y + (T)S * o[3].x));
+        v[0] = add(e[0], o[0]);
+        v[4] = sub(e[0], o[0]);
+        v[1] = add(e[1], t1);
+        v[5] = sub(e[1], t1);
+        v[2] = add(e[2], t2);
+        v[6] = sub(e[2], t2);
+        v[3] = add(e[3], t3);
+        v[7] = sub(e[3], t3);
+    }
+};
+
+// one Stockham stage: butterflies j = 0..N/R-1 of each of the NQ sequences (stored N apart)
+// spread over the 32 lanes
+template <typename C, int N, int F, int S, int NQ>
+__device__ __forceinline__ void stage(const C *__restrict__ src, C *__restrict__ dst, const C *__restrict__ tw,
+                                      int lane) {
+    constexpr int R = fac(N, F);
+    constexpr int NS = stride(N, F);
+    constexpr int NR = N / R;
+    constexpr int TSTEP = N / (NS * R);
+    constexpr int IT = (NQ * NR + 31) / 32;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int u = lane + 32 * it;
+        if ((NQ * NR) % 32 == 0 || u < NQ * NR) {
+            const int sq = NQ > 1 ? u / NR : 0;
+            const int j = NQ > 1 ? u - sq * NR : u;
+            const C *sp = src + sq * N;
+            C *dp = dst + sq * N;
+            const int k = j % NS;
+            C v[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                C x = sp[j + r * NR];
+                if (NS > 1 && r > 0 && k) {
+                    C w = __ldg(&tw[r * k * TSTEP]);
+                    if (S > 0) w.y = -w.y;
+                    x = mul(x, w);
+                }
+                v[r] = x;
+            }
+            Dft<C, R, S>::run(v);
+            const int idxD = (j - k) * R + k;
+#pragma unroll
+            for (int q = 0; q < R; ++q) dp[idxD + q * NS] = v[q];
+        }
+    }
+}
+
+template <typename C, int N, int F, int S, int NQ, bool END>
+struct Step;
+template <typename C, int N, int F, int S, int NQ>
+struct Step<C, N, F, S, NQ, true> {
+    static __device__ __forceinline__ C *go(C *src, C *, const C *, int) { return src; }
+};
+template <typename C, int N, int F, int S, int NQ>
+struct Step<C, N, F, S, NQ, false> {
+    static __device__ __forceinline__ C *go(C *src, C *dst, const C *tw, int lane) {
+        stage<C, N, F, S, NQ>(src, dst, tw, lane);
+        __syncwarp();
+        return Step<C, N, F + 1, S, NQ, (F + 1 >= nfac(N))>::go(dst, src, tw, lane);
+    }
+};
+}   // namespace kct
+
+// S = -1: exp(-2 pi i jk/N) (FFTW_FORWARD), +1: exp(+...) (FFTW_BACKWARD).  NQ sequences of
+// length N lie N apart in a; b is a scratch buffer of the same size (both private to the calling
+// warp); the input must be visible to the whole warp (__syncwarp after writing it).  Returns the
+// buffer holding the result.
+template <typename C, int N, int S, int NQ = 1>
+__device__ __forceinline__ C *fft_warp_ct(C *a, C *b, const C *tw) {
+    static_assert(kct::nfac(N) > 0, "transform length must be 2^a 3^b 5^c");
+    return kct::Step<C, N, 0, S, NQ, false>::go(a, b, tw, threadIdx.x & 31);
+}
+
+// the transform lengths with compiled instances (3/2-rule grids of nx, nz = 32, 64, 96, 128, 384
+// and the Chebyshev extensions 2 ny = 64, 128, 192, 256, 512)
+#define KMM_CT_LEN_LIST(X) X(48) X(64) X(96) X(128) X(144) X(192) X(256) X(512) X(576)

@@ -19,6 +19,7 @@
 // recurrences (eqsolve, pntsolve).
 #include <math.h>
 
+#include "kmm_fft.cuh"
 #include "kmm_warpcol.cuh"
 
 // ---------------------------------------------------------------------------
@@ -233,7 +234,7 @@ __device__ __forceinline__ void col_norm(Col<E> &x, double2 *xbuf, int kx, int j
 
 // DCT-I of one column through the warp FFT (even extension of length 2 ny):
 //   to_phys: scale by c(i)/2 first (solvers.f90:2241-2546);  !to_phys: /ny, halve the ends (3279-3416)
-template <int E>
+template <int E, int L0>
 __device__ __forceinline__ void col_dct(Col<E> &x, double2 *a, double2 *b, const DevPlan &P, int nyp, bool to_phys) {
     const int lane = threadIdx.x & 31;
     const int ny = nyp - 1, L = 2 * ny;
@@ -248,7 +249,9 @@ __device__ __forceinline__ void col_dct(Col<E> &x, double2 *a, double2 *b, const
         }
     }
     __syncwarp();
-    const double2 *r = fft_warp(P, a, b, -1);
+    const double2 *r;
+    if constexpr (L0 > 0) r = fft_warp_ct<double2, L0, -1>(a, b, P.tw);
+    else r = fft_warp(P, a, b, -1);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const int i = lane + 32 * e;
@@ -276,7 +279,8 @@ struct ColFwdArgs {
     double atu, btu, gtu, abu, bbu, gbu, atw, gtw, abw, bbw, gbw;
 };
 
-template <int E>
+// L0 > 0: 2 ny is the compile-time constant L0 (specialised DCT); L0 = 0: runtime plan
+template <int E, int L0>
 __global__ void __launch_bounds__(64) k_col_fwd(ColFwdArgs A, FusedTabs T, DevPlan P) {
     extern __shared__ double2 sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -455,27 +459,27 @@ __global__ void __launch_bounds__(64) k_col_fwd(ColFwdArgs A, FusedTabs T, DevPl
     col_store<E>(A.omy + off, om, nyp);
     // ---- y-physical outputs: u, v, w, omega_y, du/dy, dw/dy [, c, dc/dy]
     double2 *yp = A.yp;
-    col_dct<E>(v, fa, fb, P, nyp, true);
+    col_dct<E, L0>(v, fa, fb, P, nyp, true);
     col_store<E>(yp + 1 * ncols * nyp + off, v, nyp);
-    col_dct<E>(om, fa, fb, P, nyp, true);
+    col_dct<E, L0>(om, fa, fb, P, nyp, true);
     col_store<E>(yp + 3 * ncols * nyp + off, om, nyp);
     col_cderiv<E>(d1, u, nyp, A.dyde);
-    col_dct<E>(u, fa, fb, P, nyp, true);
+    col_dct<E, L0>(u, fa, fb, P, nyp, true);
     col_store<E>(yp + 0 * ncols * nyp + off, u, nyp);
-    col_dct<E>(d1, fa, fb, P, nyp, true);
+    col_dct<E, L0>(d1, fa, fb, P, nyp, true);
     col_store<E>(yp + 4 * ncols * nyp + off, d1, nyp);
     col_cderiv<E>(d1, w, nyp, A.dyde);
-    col_dct<E>(w, fa, fb, P, nyp, true);
+    col_dct<E, L0>(w, fa, fb, P, nyp, true);
     col_store<E>(yp + 2 * ncols * nyp + off, w, nyp);
-    col_dct<E>(d1, fa, fb, P, nyp, true);
+    col_dct<E, L0>(d1, fa, fb, P, nyp, true);
     col_store<E>(yp + 5 * ncols * nyp + off, d1, nyp);
     if (A.scalar) {
         col_norm<E>(s, xbuf, kx, j, A.nzh);
         col_store<E>(A.scal + off, s, nyp);
         col_cderiv<E>(d1, s, nyp, A.dyde);
-        col_dct<E>(s, fa, fb, P, nyp, true);
+        col_dct<E, L0>(s, fa, fb, P, nyp, true);
         col_store<E>(yp + 6 * ncols * nyp + off, s, nyp);
-        col_dct<E>(d1, fa, fb, P, nyp, true);
+        col_dct<E, L0>(d1, fa, fb, P, nyp, true);
         col_store<E>(yp + 7 * ncols * nyp + off, d1, nyp);
     }
 }
@@ -488,9 +492,12 @@ __global__ void __launch_bounds__(64) k_col_fwd(ColFwdArgs A, FusedTabs T, DevPl
 #define ZT_WARPS (ZT_KX * ZT_Y)
 
 // Q[g][y][z][kx], g = u v w wx wy wz [c cx cy cz], from the y-physical base fields
+// MZ > 0: compile-time z length (specialised FFT); MZ = 0: runtime plan
+template <int MZ>
 __global__ void __launch_bounds__(ZT_WARPS * 32) k_zb(const double2 *__restrict__ yp, double2 *__restrict__ q,
                                                       const double *__restrict__ wavx, const double *__restrict__ wavz,
-                                                      DevPlan P, int nout, int nyp, int nz, int nxh, int mz) {
+                                                      DevPlan P, int nout, int nyp, int nz, int nxh, int mz_rt) {
+    const int mz = MZ > 0 ? MZ : mz_rt;
     extern __shared__ double2 sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int kl = warp % ZT_KX, yl = warp / ZT_KX;
@@ -529,7 +536,9 @@ __global__ void __launch_bounds__(ZT_WARPS * 32) k_zb(const double2 *__restrict_
                 a[jj] = val;
             }
             __syncwarp();
-            const double2 *r = fft_warp(P, a, b, +1);
+            const double2 *r;
+            if constexpr (MZ > 0) r = fft_warp_ct<double2, MZ, +1>(a, b, P.tw);
+            else r = fft_warp(P, a, b, +1);
             for (int z = lane; z < mz; z += 32) stage[((size_t)yl * mz + z) * ZT_KX + kl] = r[z];
         }
         __syncthreads();
@@ -546,8 +555,10 @@ __global__ void __launch_bounds__(ZT_WARPS * 32) k_zb(const double2 *__restrict_
 }
 
 // y-physical outputs [o][ncols][nyp] from R[o][y][z][kx]
+template <int MZ>
 __global__ void __launch_bounds__(ZT_WARPS * 32) k_zf(const double2 *__restrict__ r, double2 *__restrict__ yo, DevPlan P,
-                                                      int nout, int nyp, int nz, int nxh, int mz, double scale) {
+                                                      int nout, int nyp, int nz, int nxh, int mz_rt, double scale) {
+    const int mz = MZ > 0 ? MZ : mz_rt;
     extern __shared__ double2 sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int kl = warp % ZT_KX, yl = warp / ZT_KX;
@@ -561,7 +572,9 @@ __global__ void __launch_bounds__(ZT_WARPS * 32) k_zf(const double2 *__restrict_
         if (act) {
             for (int z = lane; z < mz; z += 32) a[z] = __ldg(r + (((size_t)o * nyp + y) * mz + z) * nxh + kx);
             __syncwarp();
-            const double2 *res = fft_warp(P, a, b, -1);
+            const double2 *res;
+            if constexpr (MZ > 0) res = fft_warp_ct<double2, MZ, -1>(a, b, P.tw);
+            else res = fft_warp(P, a, b, -1);
             for (int kz = lane; kz < nz; kz += 32) {
                 const int jj = kz < nzh ? kz : (mz - nz) + kz;
                 const double2 v = res[jj];
@@ -591,7 +604,7 @@ struct ColBwdArgs {
     double dyde;
 };
 
-template <int E>
+template <int E, int L0>
 __global__ void __launch_bounds__(64) k_col_bwd(ColBwdArgs A, DevPlan P) {
     extern __shared__ double2 sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -607,11 +620,11 @@ __global__ void __launch_bounds__(64) k_col_bwd(ColBwdArgs A, DevPlan P) {
     const double kxv = A.wavx[kx], kzv = A.wavz[j];
     Col<E> h1, h2, h3;
     col_load<E>(h1, A.yo + 0 * ncols * nyp + off, nyp);
-    col_dct<E>(h1, fa, fb, P, nyp, false);
+    col_dct<E, L0>(h1, fa, fb, P, nyp, false);
     col_load<E>(h2, A.yo + 1 * ncols * nyp + off, nyp);
-    col_dct<E>(h2, fa, fb, P, nyp, false);
+    col_dct<E, L0>(h2, fa, fb, P, nyp, false);
     col_load<E>(h3, A.yo + 2 * ncols * nyp + off, nyp);
-    col_dct<E>(h3, fa, fb, P, nyp, false);
+    col_dct<E, L0>(h3, fa, fb, P, nyp, false);
     // norm(fn), norm(gn), norm(omz) after vcw3dp (main_dns.f90:620-624)
     col_norm<E>(h2, xbuf, kx, j, A.nzh);
     col_norm<E>(h1, xbuf, kx, j, A.nzh);
@@ -625,7 +638,7 @@ __global__ void __launch_bounds__(64) k_col_bwd(ColBwdArgs A, DevPlan P) {
     Col<E> sc;
     if (A.scalar) {
         col_load<E>(sc, A.yo + 3 * ncols * nyp + off, nyp);
-        col_dct<E>(sc, fa, fb, P, nyp, false);
+        col_dct<E, L0>(sc, fa, fb, P, nyp, false);
         col_norm<E>(sc, xbuf, kx, j, A.nzh);
     }
 #pragma unroll
@@ -722,14 +735,25 @@ int kmm_fused_step(kmm_ctx *ctx) {
     const size_t smc = sizeof(double2) * (64 * (size_t)E + 2 * 2 * 2 * (size_t)ctx->ny);
     const int nblk = (int)(ncols / 2);
     kmm_tic(ctx);
-#define COLF(EE)                                                                                      \
-    case EE:                                                                                          \
-        RET(kmm_smem_attr(ctx, (const void *)k_col_fwd<EE>, smc));                                    \
-        k_col_fwd<EE><<<nblk, 64, smc, ctx->stream>>>(F, FU->tabs, ctx->wy2);                           \
-        break;
-    switch (E) {
-        COLF(2) COLF(3) COLF(4) COLF(5) COLF(9)
-    default: return KMM_ERR_UNSUPPORTED;
+#define COLF(EE, LL)                                                                                  \
+    do {                                                                                              \
+        RET(kmm_smem_attr(ctx, (const void *)k_col_fwd<EE, LL>, smc));                                \
+        k_col_fwd<EE, LL><<<nblk, 64, smc, ctx->stream>>>(F, FU->tabs, ctx->wy2);                       \
+    } while (0)
+    switch (2 * ctx->ny) {   // specialised lengths: ny = 32, 64, 96, 128
+    case 64: COLF(2, 64); break;
+    case 128: COLF(3, 128); break;
+    case 192: COLF(4, 192); break;
+    case 256: COLF(5, 256); break;
+    default:
+        switch (E) {
+        case 2: COLF(2, 0); break;
+        case 3: COLF(3, 0); break;
+        case 4: COLF(4, 0); break;
+        case 5: COLF(5, 0); break;
+        case 9: COLF(9, 0); break;
+        default: return KMM_ERR_UNSUPPORTED;
+        }
     }
 #undef COLF
     CKL();
@@ -746,8 +770,20 @@ int kmm_fused_step(kmm_ctx *ctx) {
     const size_t smzf = sizeof(double2) * ((size_t)ZT_WARPS * 2 * mz + (size_t)ZT_KX * nz * ZT_Y);
     const dim3 gz((nxh + ZT_KX - 1) / ZT_KX, (nyp + ZT_Y - 1) / ZT_Y);
     kmm_tic(ctx);
-    RET(kmm_smem_attr(ctx, (const void *)k_zb, smz));
-    k_zb<<<gz, ZT_WARPS * 32, smz, ctx->stream>>>(g_yp, g_q, ctx->d_wavx, ctx->d_wavz, ctx->wmz, nq, nyp, nz, nxh, mz);
+#define ZB(MM)                                                                                        \
+    do {                                                                                              \
+        RET(kmm_smem_attr(ctx, (const void *)k_zb<MM>, smz));                                         \
+        k_zb<MM><<<gz, ZT_WARPS * 32, smz, ctx->stream>>>(g_yp, g_q, ctx->d_wavx, ctx->d_wavz, ctx->wmz, nq, nyp, nz, \
+                                                        nxh, mz);                                     \
+    } while (0)
+    switch (mz) {   // specialised lengths: nz = 32, 64, 96, 128
+    case 48: ZB(48); break;
+    case 96: ZB(96); break;
+    case 144: ZB(144); break;
+    case 192: ZB(192); break;
+    default: ZB(0); break;
+    }
+#undef ZB
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_BWD);
     // x transforms + products
@@ -758,9 +794,20 @@ int kmm_fused_step(kmm_ctx *ctx) {
     kmm_toc(ctx, KMM_STAGE_XPHYS);
     // z forward transforms
     kmm_tic(ctx);
-    RET(kmm_smem_attr(ctx, (const void *)k_zf, smzf));
-    k_zf<<<gz, ZT_WARPS * 32, smzf, ctx->stream>>>(g_r, g_yo, ctx->wmz, nout, nyp, nz, nxh, mz,
-                                                  (double)ctx->mx * (double)mz);
+#define ZF(MM)                                                                                        \
+    do {                                                                                              \
+        RET(kmm_smem_attr(ctx, (const void *)k_zf<MM>, smzf));                                        \
+        k_zf<MM><<<gz, ZT_WARPS * 32, smzf, ctx->stream>>>(g_r, g_yo, ctx->wmz, nout, nyp, nz, nxh, mz,  \
+                                                         (double)ctx->mx * (double)mz);               \
+    } while (0)
+    switch (mz) {
+    case 48: ZF(48); break;
+    case 96: ZF(96); break;
+    case 144: ZF(144); break;
+    case 192: ZF(192); break;
+    default: ZF(0); break;
+    }
+#undef ZF
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_FWD);
     // back to Chebyshev space, norm, filter, nonlin
@@ -770,14 +817,25 @@ int kmm_fused_step(kmm_ctx *ctx) {
     B.wavx = ctx->d_wavx; B.wavz = ctx->d_wavz; B.nz = nz; B.nxh = nxh; B.nyp = nyp; B.nzh = ctx->nzh;
     B.scalar = scalar; B.dyde = ctx->dyde;
     kmm_tic(ctx);
-#define COLB(EE)                                                                                      \
-    case EE:                                                                                          \
-        RET(kmm_smem_attr(ctx, (const void *)k_col_bwd<EE>, smc));                                    \
-        k_col_bwd<EE><<<nblk, 64, smc, ctx->stream>>>(B, ctx->wy2);                                    \
-        break;
-    switch (E) {
-        COLB(2) COLB(3) COLB(4) COLB(5) COLB(9)
-    default: return KMM_ERR_UNSUPPORTED;
+#define COLB(EE, LL)                                                                                  \
+    do {                                                                                              \
+        RET(kmm_smem_attr(ctx, (const void *)k_col_bwd<EE, LL>, smc));                                \
+        k_col_bwd<EE, LL><<<nblk, 64, smc, ctx->stream>>>(B, ctx->wy2);                                \
+    } while (0)
+    switch (2 * ctx->ny) {
+    case 64: COLB(2, 64); break;
+    case 128: COLB(3, 128); break;
+    case 192: COLB(4, 192); break;
+    case 256: COLB(5, 256); break;
+    default:
+        switch (E) {
+        case 2: COLB(2, 0); break;
+        case 3: COLB(3, 0); break;
+        case 4: COLB(4, 0); break;
+        case 5: COLB(5, 0); break;
+        case 9: COLB(9, 0); break;
+        default: return KMM_ERR_UNSUPPORTED;
+        }
     }
 #undef COLB
     CKL();
