@@ -241,8 +241,11 @@ int  kmm_init_part(kmm_ctx *ctx);
 
 /* ---- options --------------------------------------------------------------- */
 enum kmm_option {
-    KMM_OPT_FUSED = 1   /* 1 (default): kmm_step runs the fused kernels when the run has no polymer and no
+    KMM_OPT_FUSED = 1,  /* 1 (default): kmm_step runs the fused kernels when the run has no polymer and no
                            immersed boundary; 0: kmm_step runs the routine-by-routine kernels   */
+    KMM_OPT_COLUMN_BLOCKED = 2  /* 1 (default): the fused step's column kernels hold a column on 16
+                           lanes in blocks of ny/16 coefficients (ny = 32, 64, 96, 128);
+                           0: one warp per column, coefficient i on lane i mod 32           */
 };
 int  kmm_set_option(kmm_ctx *ctx, int option, int value);
 

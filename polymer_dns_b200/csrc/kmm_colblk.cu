@@ -1,0 +1,382 @@
+// kmm_colblk.cu -- the column stages of the fused step (kmm_fused.cu) in the blocked layout of
+// kmm_colblk.cuh: one warp per (kz, -kz) column pair, 16 lanes per column.  The sequence of
+// operations is that of k_col_fwd / k_col_bwd (main_dns.f90:325-544 and 606-771 with
+// solvers.f90:555-1722, 3279-3416); only the data layout and the scan structure differ.
+#include <math.h>
+
+#include "kmm_fft.cuh"
+#include "kmm_colblk.cuh"
+
+#define CB_WARPS 4   // column pairs per block
+
+// phirhs on one column (solvers.f90:633-675)
+template <int K>
+__device__ __forceinline__ void bphirhs(BCol<K> &x, const BCol<K> &fn, const BCol<K> &fnm1, double re, double var,
+                                        double dt, double th, double w2, double dyde, unsigned mask) {
+    const double a = -re * var / (dt * th), b = re * var / (2.0 * th);
+    const double c = (1.0 - th) * w2;
+    BCol<K> w;
+#pragma unroll
+    for (int m = 0; m <= K; ++m) {
+        double2 r;
+        r.x = a * x.v[m].x - b * (3.0 * fn.v[m].x - fnm1.v[m].x);
+        r.y = a * x.v[m].y - b * (3.0 * fn.v[m].y - fnm1.v[m].y);
+        if (th > 0.99) x.v[m] = r;
+        r.x = r.x + c * x.v[m].x / th;
+        r.y = r.y + c * x.v[m].y / th;
+        w.v[m] = r;
+    }
+    BCol<K> d1, d2;
+    bcderiv<K>(d1, x, dyde, mask);
+    bcderiv<K>(d2, d1, dyde, mask);
+#pragma unroll
+    for (int m = 0; m <= K; ++m)
+        x.v[m] = make_double2(w.v[m].x - (1.0 - th) * d2.v[m].x / th, w.v[m].y - (1.0 - th) * d2.v[m].y / th);
+}
+
+template <int K>
+__global__ void __launch_bounds__(CB_WARPS * 32) k_bcol_fwd(ColFwdArgs A, FusedTabs T, const double *__restrict__ rj,
+                                                            const double2 *__restrict__ tw) {
+    constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
+    constexpr unsigned FULL = 0xffffffffu;
+    extern __shared__ double2 sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, h = lane >> 4;
+    double2 *fa = sm + (size_t)warp * 4 * L, *fb = fa + 2 * L;
+    const int npair = A.nz / 2;
+    const int pr = blockIdx.x * CB_WARPS + warp;
+    if (pr >= A.nxh * npair) return;   // whole warps only: no block-wide barrier below
+    const int q = pr % npair, kx = pr / npair;
+    const int j = h == 0 ? q : (q == 0 ? A.nzh : A.nz - q);
+    const int col = kx * A.nz + j;
+    const size_t off = (size_t)col * NYP;
+    const double kxv = A.wavx[kx], kzv = A.wavz[j];
+    const double w2 = kzv * kzv + kxv * kxv;
+    const double g1 = A.re / (A.dt * A.th);
+    const bool mean = (kx == 0 && j == 0);
+    const size_t ncols = (size_t)A.nz * A.nxh;
+    const double2 zero = make_double2(0.0, 0.0);
+    BCol<K> d1;
+
+    // ---- passive scalar (main_dns.f90:325-359), finished first: norm, store, y-physical c, dc/dy
+    if (A.scalar) {
+        BCol<K> s;
+        bload<K>(s, A.scal + off);
+        {
+            BCol<K> n1, n0;
+            bload<K>(n1, A.scn + off);
+            bload<K>(n0, A.scnm1 + off);
+            bphirhs<K>(s, n1, n0, A.re, A.diff, A.dt, A.th, w2, A.dyde, FULL);
+        }
+        const TauTab ts = tab_at(T, TB_SCL, col, NYP);
+        bsolve_robin<K>(s, ts, zero, zero, w2 + T.g[TB_SCL], A.c0, rj, FULL);
+        bnorm<K>(s, kx, j, A.nzh);
+        bstore<K>(A.scal + off, s);
+        bcderiv<K>(d1, s, A.dyde, FULL);
+        bdct<K>(s, fa, fb, tw, true);
+        bstore<K>(A.yp + 6 * ncols * NYP + off, s);
+        bdct<K>(d1, fa, fb, tw, true);
+        bstore<K>(A.yp + 7 * ncols * NYP + off, d1);
+    }
+    // ---- wall-normal velocity: phi, phirhs, Helmholtz + Poisson (main_dns.f90:363-407)
+    BCol<K> v;
+    {
+        BCol<K> d2;
+        bload<K>(v, A.v + off);
+        bcderiv<K>(d1, v, A.dyde, FULL);
+        bcderiv<K>(d2, d1, A.dyde, FULL);
+#pragma unroll
+        for (int m = 0; m <= K; ++m) v.v[m] = make_double2(d2.v[m].x - w2 * v.v[m].x, d2.v[m].y - w2 * v.v[m].y);
+    }
+    {
+        BCol<K> f1, f0;
+        bload<K>(f1, A.fn + off);
+        bload<K>(f0, A.fnm1 + off);
+        bphirhs<K>(v, f1, f0, A.re, 1.0, A.dt, A.th, w2, A.dyde, FULL);
+    }
+    {
+        const TauTab tp = tab_at(T, TB_PHI, col, NYP);
+        bsolve_dirichlet<K>(v, tp, zero, zero, w2 + g1, A.c0, rj, FULL);
+        const TauTab tv = tab_at(T, TB_V, col, NYP);
+        bsolve_dirichlet<K>(v, tv, zero, zero, w2, A.c0, rj, FULL);
+    }
+    // ---- normal vorticity phirhs (main_dns.f90:411-422)
+    BCol<K> om;
+    bload<K>(om, A.omy + off);
+    {
+        BCol<K> g1c, g0c;
+        bload<K>(g1c, A.gn + off);
+        bload<K>(g0c, A.gnm1 + off);
+        bphirhs<K>(om, g1c, g0c, A.re, 1.0, A.dt, A.th, w2, A.dyde, FULL);
+    }
+    // ---- influence matrix (main_dns.f90:426-466)
+    {
+        double2 wb, wt;
+        if (A.nb == 1 && A.nt == 1) {
+            bwall1<K>(v, A.dyde, wb, wt, FULL);
+        } else {
+            BCol<K> dv;
+            bcderiv<K>(dv, v, A.dyde, FULL);
+            double2 b2, t2;
+            bwall1<K>(dv, A.dyde, b2, t2, FULL);
+            bwall1<K>(v, A.dyde, wb, wt, FULL);
+            if (A.nb == 2) wb = b2;
+            if (A.nt == 2) wt = t2;
+        }
+        const double2 c1 = cdiv(csub(cmul(wb, A.dnv2t[col]), cmul(wt, A.dnv2b[col])), A.denom[col]);
+        const double2 c2 = cdiv(csub(cmul(wt, A.dnv1b[col]), cmul(wb, A.dnv1t[col])), A.denom[col]);
+        BCol<K> gfa;
+        bload<K>(gfa, A.gf1 + off);
+#pragma unroll
+        for (int m = 0; m <= K; ++m) {
+            const double2 a = cmul(c1, gfa.v[m]);
+            v.v[m] = make_double2(v.v[m].x + a.x, v.v[m].y + a.y);
+        }
+        bload<K>(gfa, A.gf2 + off);
+#pragma unroll
+        for (int m = 0; m <= K; ++m) {
+            const double2 b = cmul(c2, gfa.v[m]);
+            v.v[m] = make_double2(v.v[m].x + b.x, v.v[m].y + b.y);
+        }
+    }
+    // ---- normal vorticity Robin solve (main_dns.f90:479-484)
+    {
+        const TauTab to = tab_at(T, TB_OMY, col, NYP);
+        bsolve_robin<K>(om, to, zero, zero, w2 + g1, A.c0, rj, FULL);
+    }
+    // ---- mean modes (main_dns.f90:489-502): uzero for u0 and w0 on the (0,0) column's half-warp
+    if (kx == 0 && q == 0) {
+        if (h == 0) {
+            constexpr unsigned HM = 0x0000ffffu;
+            const double th = A.th;
+            const int t = lane & 15;
+            for (int which = 0; which < 2; ++which) {
+                double *U = which == 0 ? A.u0 : A.w0;
+                const double *H = which == 0 ? A.h1n : A.h3n, *HL = which == 0 ? A.h1nm1 : A.h3nm1;
+                BCol<K> uc, dd1, dd2;
+#pragma unroll
+                for (int m = 0; m <= K; ++m) uc.v[m] = make_double2(U[bidx<K>(m)], 0.0);
+                // wrk1 = -re u0/(dt th) - re (3 h1 - h1l)/(2 th); u0 <- wrk1 - (1-th) u0''/th (solvers.f90:1127-1143)
+                bcderiv<K>(dd1, uc, A.dyde, HM);
+                bcderiv<K>(dd2, dd1, A.dyde, HM);
+#pragma unroll
+                for (int m = 0; m <= K; ++m) {
+                    const int i = bidx<K>(m);
+                    const double w1 = -A.re * uc.v[m].x / (A.dt * th) - A.re * (3.0 * H[i] - HL[i]) / (2.0 * th);
+                    const double r = (th > 0.99) ? w1 : w1 - (1.0 - th) * dd2.v[m].x / th;
+                    uc.v[m] = make_double2(r, 0.0);
+                }
+                const TauTab tm = tab_at(T, which == 0 ? TB_U0 : TB_W0, 0, NYP);
+                const double gt = which == 0 ? A.gtu : A.gtw, gb = which == 0 ? A.gbu : A.gbw;
+                bsolve_robin<K>(uc, tm, make_double2(gt, 0.0), make_double2(gb, 0.0), g1, A.c0, rj, HM);
+                __syncwarp(HM);
+#pragma unroll
+                for (int m = 0; m < K; ++m) U[t * K + m] = uc.v[m].x;
+                if (t == 15) U[NY] = uc.v[K].x;
+                __syncwarp(HM);
+            }
+        }
+        __syncwarp();
+        for (int i = lane; i < NYP; i += 32) {
+            A.h1nm1[i] = A.h1n[i];
+            A.h3nm1[i] = A.h3n[i];
+        }
+        if (mean) {
+#pragma unroll
+            for (int m = 0; m <= K; ++m) om.v[m] = zero;
+        }
+    }
+    // ---- norm(v), norm(omy); veloc (main_dns.f90:520-526, solvers.f90:1576-1659)
+    bnorm<K>(v, kx, j, A.nzh);
+    bnorm<K>(om, kx, j, A.nzh);
+    BCol<K> u, w;
+    {
+        BCol<K> dv;
+        bcderiv<K>(dv, v, A.dyde, FULL);
+#pragma unroll
+        for (int m = 0; m <= K; ++m) {
+            const double2 d = dv.v[m], o = om.v[m];
+            if (kx > 0) {
+                const double2 sa = cadd(cimul(d, -kxv), cimul(o, kzv));
+                u.v[m] = make_double2(-sa.x / w2, -sa.y / w2);
+                const double2 sb = csub(cimul(d, -kzv), cimul(o, kxv));
+                w.v[m] = make_double2(-sb.x / w2, -sb.y / w2);
+            } else if (j > 0) {
+                const double kz2 = kzv * kzv;
+                const double2 sa = cimul(o, kzv);
+                u.v[m] = make_double2(-sa.x / kz2, -sa.y / kz2);
+                const double2 sb = cimul(d, -kzv);
+                w.v[m] = make_double2(-sb.x / kz2, -sb.y / kz2);
+            } else {
+                u.v[m] = zero;
+                w.v[m] = zero;
+            }
+        }
+        if (mean) {
+#pragma unroll
+            for (int m = 0; m <= K; ++m) {
+                const int i = bidx<K>(m);
+                u.v[m] = make_double2(A.u0[i], 0.0);
+                w.v[m] = make_double2(A.w0[i], 0.0);
+                v.v[m] = zero;
+            }
+        }
+        // norm(u), norm(w): the pair is conjugate-symmetric already; zero the kz Nyquist column
+        if (j == A.nzh) {
+#pragma unroll
+            for (int m = 0; m <= K; ++m) {
+                u.v[m] = zero;
+                w.v[m] = zero;
+            }
+        }
+    }
+    bstore<K>(A.v + off, v);
+    bstore<K>(A.omy + off, om);
+    // ---- y-physical outputs: u, v, w, omega_y, du/dy, dw/dy
+    double2 *yp = A.yp;
+    bdct<K>(v, fa, fb, tw, true);
+    bstore<K>(yp + 1 * ncols * NYP + off, v);
+    bdct<K>(om, fa, fb, tw, true);
+    bstore<K>(yp + 3 * ncols * NYP + off, om);
+    bcderiv<K>(d1, u, A.dyde, FULL);
+    bdct<K>(u, fa, fb, tw, true);
+    bstore<K>(yp + 0 * ncols * NYP + off, u);
+    bdct<K>(d1, fa, fb, tw, true);
+    bstore<K>(yp + 4 * ncols * NYP + off, d1);
+    bcderiv<K>(d1, w, A.dyde, FULL);
+    bdct<K>(w, fa, fb, tw, true);
+    bstore<K>(yp + 2 * ncols * NYP + off, w);
+    bdct<K>(d1, fa, fb, tw, true);
+    bstore<K>(yp + 5 * ncols * NYP + off, d1);
+}
+
+template <int K>
+__global__ void __launch_bounds__(CB_WARPS * 32) k_bcol_bwd(ColBwdArgs A, const double2 *__restrict__ tw) {
+    constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
+    constexpr unsigned FULL = 0xffffffffu;
+    extern __shared__ double2 sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, h = lane >> 4;
+    double2 *fa = sm + (size_t)warp * 4 * L, *fb = fa + 2 * L;
+    const int npair = A.nz / 2;
+    const int pr = blockIdx.x * CB_WARPS + warp;
+    if (pr >= A.nxh * npair) return;
+    const int q = pr % npair, kx = pr / npair;
+    const int j = h == 0 ? q : (q == 0 ? A.nzh : A.nz - q);
+    const int col = kx * A.nz + j;
+    const size_t off = (size_t)col * NYP;
+    const size_t ncols = (size_t)A.nz * A.nxh;
+    const double kxv = A.wavx[kx], kzv = A.wavz[j];
+    BCol<K> h1, h2, h3;
+    bload<K>(h1, A.yo + 0 * ncols * NYP + off);
+    bdct<K>(h1, fa, fb, tw, false);
+    bload<K>(h2, A.yo + 1 * ncols * NYP + off);
+    bdct<K>(h2, fa, fb, tw, false);
+    bload<K>(h3, A.yo + 2 * ncols * NYP + off);
+    bdct<K>(h3, fa, fb, tw, false);
+    // norm(fn), norm(gn), norm(omz) after vcw3dp (main_dns.f90:620-624)
+    bnorm<K>(h2, kx, j, A.nzh);
+    bnorm<K>(h1, kx, j, A.nzh);
+    bnorm<K>(h3, kx, j, A.nzh);
+    // spectral filter (main_dns.f90:710-745)
+    const int j1 = j + 1;
+    const int jjf = (j1 > A.nzh) ? A.nz - j1 + 1 : j1 - 1;
+    const double zr = (double)jjf / (double)A.nzh;
+    const double z2 = zr * zr, z4 = z2 * z2, z8 = z4 * z4;
+    const double zs = exp(-3.0 * (z8 * z2));
+    BCol<K> sc;
+    if (A.scalar) {
+        bload<K>(sc, A.yo + 3 * ncols * NYP + off);
+        bdct<K>(sc, fa, fb, tw, false);
+        bnorm<K>(sc, kx, j, A.nzh);
+    }
+#pragma unroll
+    for (int m = 0; m <= K; ++m) {
+        const int i = bidx<K>(m);
+        const double yr = (double)i / (double)NY;
+        const double y2 = yr * yr, y4 = y2 * y2, y8 = y4 * y4;
+        const double ys = exp(-3.0 * (y8 * y2));
+        h3.v[m] = make_double2(h3.v[m].x * zs * ys, h3.v[m].y * zs * ys);
+        h1.v[m] = make_double2(h1.v[m].x * zs * ys, h1.v[m].y * zs * ys);
+        h2.v[m] = make_double2(h2.v[m].x * zs * ys, h2.v[m].y * zs * ys);
+        if (A.scalar) sc.v[m] = make_double2(sc.v[m].x * zs * ys, sc.v[m].y * zs * ys);
+    }
+    // h1n = Re gn(:,1,1), h3n = Re omz(:,1,1) (main_dns.f90:748-751)
+    if (kx == 0 && j == 0) {
+        const int t = lane & 15;
+#pragma unroll
+        for (int m = 0; m < K; ++m) {
+            A.h1n[t * K + m] = h1.v[m].x;
+            A.h3n[t * K + m] = h3.v[m].x;
+        }
+        if (t == 15) {
+            A.h1n[NY] = h1.v[K].x;
+            A.h3n[NY] = h3.v[K].x;
+        }
+    }
+    // nonlin (solvers.f90:1497-1572): fn = -k^2 h2 - d/dy(i(kz h3 + kx h1)); gn = i(kz h1 - kx h3)
+    BCol<K> tt, d;
+#pragma unroll
+    for (int m = 0; m <= K; ++m) {
+        const double2 s = make_double2(kzv * h3.v[m].x + kxv * h1.v[m].x, kzv * h3.v[m].y + kxv * h1.v[m].y);
+        tt.v[m] = make_double2(-s.y, s.x);
+    }
+    bcderiv<K>(d, tt, A.dyde, FULL);
+    const double w2 = -kxv * kxv - kzv * kzv;
+#pragma unroll
+    for (int m = 0; m <= K; ++m) {
+        h2.v[m] = make_double2(w2 * h2.v[m].x - d.v[m].x, w2 * h2.v[m].y - d.v[m].y);
+        const double2 s = make_double2(kzv * h1.v[m].x - kxv * h3.v[m].x, kzv * h1.v[m].y - kxv * h3.v[m].y);
+        h1.v[m] = make_double2(-s.y, s.x);
+    }
+    bstore<K>(A.fn + off, h2);
+    bstore<K>(A.gn + off, h1);
+    bstore<K>(A.omz + off, h3);
+    if (A.scalar) bstore<K>(A.scn + off, sc);
+    (void)h;
+}
+
+static int colblk_k(const kmm_ctx *ctx) {
+    const int ny = ctx->ny;
+    if (ny != 32 && ny != 64 && ny != 96 && ny != 128) return 0;
+    return ny / 16;
+}
+
+int kmm_colblk_fwd(kmm_ctx *ctx, const ColFwdArgs &A, const FusedTabs &T, const double *rj) {
+    const int K = colblk_k(ctx);
+    if (!K) return KMM_ERR_UNSUPPORTED;
+    const int npairs = ctx->nxh * (ctx->nz / 2);
+    const int nblk = (npairs + CB_WARPS - 1) / CB_WARPS;
+    const size_t smem = sizeof(double2) * (size_t)CB_WARPS * 4 * (2 * ctx->ny);
+#define BF(KK)                                                                                        \
+    case KK:                                                                                          \
+        RET(kmm_smem_attr(ctx, (const void *)k_bcol_fwd<KK>, smem));                                  \
+        k_bcol_fwd<KK><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(A, T, rj, ctx->wy2.tw);             \
+        break;
+    switch (K) {
+        BF(2) BF(4) BF(6) BF(8)
+    default: return KMM_ERR_UNSUPPORTED;
+    }
+#undef BF
+    CKL();
+    return KMM_OK;
+}
+
+int kmm_colblk_bwd(kmm_ctx *ctx, const ColBwdArgs &B, const double *rj) {
+    const int K = colblk_k(ctx);
+    if (!K) return KMM_ERR_UNSUPPORTED;
+    (void)rj;
+    const int npairs = ctx->nxh * (ctx->nz / 2);
+    const int nblk = (npairs + CB_WARPS - 1) / CB_WARPS;
+    const size_t smem = sizeof(double2) * (size_t)CB_WARPS * 4 * (2 * ctx->ny);
+#define BB(KK)                                                                                        \
+    case KK:                                                                                          \
+        RET(kmm_smem_attr(ctx, (const void *)k_bcol_bwd<KK>, smem));                                  \
+        k_bcol_bwd<KK><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(B, ctx->wy2.tw);                    \
+        break;
+    switch (K) {
+        BB(2) BB(4) BB(6) BB(8)
+    default: return KMM_ERR_UNSUPPORTED;
+    }
+#undef BB
+    CKL();
+    return KMM_OK;
+}

@@ -267,6 +267,7 @@ extern "C" int kmm_ctx_create(const kmm_params *p, int device, kmm_ctx **out) {
     }
     c->kmaxsurf = -1;
     c->use_fused = 1;
+    c->use_colblk = 1;
 #define DUP(dst, src, n)                                                        \
     do {                                                                        \
         CK(cudaMalloc(&(dst), sizeof(double) * (size_t)(n)));                   \
@@ -426,6 +427,7 @@ extern "C" int kmm_set_option(kmm_ctx *ctx, int option, int value) {
     if (!ctx) return KMM_ERR_ARG;
     switch (option) {
     case KMM_OPT_FUSED: ctx->use_fused = value ? 1 : 0; return KMM_OK;
+    case KMM_OPT_COLUMN_BLOCKED: ctx->use_colblk = value ? 1 : 0; return KMM_OK;
     default: return KMM_ERR_ARG;
     }
 }

@@ -20,12 +20,11 @@
 #include <math.h>
 
 #include "kmm_fft.cuh"
-#include "kmm_warpcol.cuh"
+#include "kmm_fused.cuh"
 
 // ---------------------------------------------------------------------------
 // tables
 // ---------------------------------------------------------------------------
-enum { TB_PHI = 0, TB_V = 1, TB_OMY = 2, TB_SCL = 3, TB_U0 = 4, TB_W0 = 5, TB_N = 6 };
 
 struct TabCfg {
     double g;
@@ -102,15 +101,7 @@ __global__ void k_tau_tables(double *td, double *te, double *tb1, double *tb2, d
     }
 }
 
-struct FusedTabs {
-    double *td[TB_N], *te[TB_N], *tb1[TB_N], *tb2[TB_N], *tf[TB_N];
-    double g[TB_N];
-};
 
-struct KmmFused {
-    FusedTabs tabs;
-    double2 *yp, *q, *r, *yo;
-};
 
 static int build_tables(kmm_ctx *ctx) {
     if (ctx->fused) return KMM_OK;
@@ -143,6 +134,20 @@ static int build_tables(kmm_ctx *ctx) {
                                                                ctx->dyde);
         CKL();
     }
+    // reciprocals of the tau row coefficients (the same divisions as the device's tau_rhs)
+    {
+        const int nyp = ctx->nyp;
+        double *h = (double *)calloc(3 * (size_t)nyp, sizeof(double));
+        for (int j = 2; j < nyp; ++j) {
+            h[j] = 1.0 / (double)(4 * j * (j - 1));
+            h[nyp + j] = 1.0 / (double)(2 * (j * j - 1));
+            h[2 * nyp + j] = 1.0 / (double)(4 * j * (j + 1));
+        }
+        cudaError_t e = cudaMalloc(&F->rj, sizeof(double) * 3 * nyp);
+        if (e == cudaSuccess) e = cudaMemcpy(F->rj, h, sizeof(double) * 3 * nyp, cudaMemcpyHostToDevice);
+        free(h);
+        CK(e);
+    }
     const size_t ncp = (size_t)ncols * ctx->nyp, nq = (size_t)ctx->nyp * ctx->mz * ctx->nxh;
     CK(cudaMalloc(&F->yp, sizeof(double2) * ncp * 8));
     CK(cudaMalloc(&F->q, sizeof(double2) * nq * 10));
@@ -158,20 +163,11 @@ void kmm_fused_release(kmm_ctx *ctx) {
         cudaFree(F->tabs.td[c]); cudaFree(F->tabs.te[c]); cudaFree(F->tabs.tb1[c]); cudaFree(F->tabs.tb2[c]);
         cudaFree(F->tabs.tf[c]);
     }
-    cudaFree(F->yp); cudaFree(F->q); cudaFree(F->r); cudaFree(F->yo);
+    cudaFree(F->yp); cudaFree(F->q); cudaFree(F->r); cudaFree(F->yo); cudaFree(F->rj);
     free(F);
     ctx->fused = NULL;
 }
 
-static __device__ __forceinline__ TauTab tab_at(const FusedTabs &T, int c, int col, int nyp) {
-    TauTab t;
-    t.td = T.td[c] + (size_t)col * nyp;
-    t.te = T.te[c] + (size_t)col * nyp;
-    t.tb1 = T.tb1[c] + (size_t)col * nyp;
-    t.tb2 = T.tb2[c] + (size_t)col * nyp;
-    t.tf = T.tf[c] + (size_t)col * 4;
-    return t;
-}
 
 // ---------------------------------------------------------------------------
 // column helpers
@@ -268,16 +264,6 @@ __device__ __forceinline__ void col_dct(Col<E> &x, double2 *a, double2 *b, const
 // ---------------------------------------------------------------------------
 // forward column kernel
 // ---------------------------------------------------------------------------
-struct ColFwdArgs {
-    double2 *v, *omy, *fn, *fnm1, *gn, *gnm1, *scal, *scn, *scnm1;
-    const double2 *gf1, *gf2, *dnv1b, *dnv1t, *dnv2b, *dnv2t, *denom;
-    double *u0, *w0, *h1n, *h1nm1, *h3n, *h3nm1, *scratch;
-    double2 *yp;      // y-physical outputs [8][ncols][nyp]
-    const double *wavx, *wavz;
-    int nz, nxh, nyp, nzh, scalar, nb, nt;
-    double re, dt, th, dyde, diff, c0;
-    double atu, btu, gtu, abu, bbu, gbu, atw, gtw, abw, bbw, gbw;
-};
 
 // L0 > 0: 2 ny is the compile-time constant L0 (specialised DCT); L0 = 0: runtime plan
 template <int E, int L0>
@@ -595,14 +581,6 @@ __global__ void __launch_bounds__(ZT_WARPS * 32) k_zf(const double2 *__restrict_
 // ---------------------------------------------------------------------------
 // backward column kernel
 // ---------------------------------------------------------------------------
-struct ColBwdArgs {
-    const double2 *yo;    // [nout][ncols][nyp]: h1, h2, h3 [, sc]
-    double2 *fn, *gn, *omz, *scn;
-    double *h1n, *h3n;
-    const double *wavx, *wavz;
-    int nz, nxh, nyp, nzh, scalar;
-    double dyde;
-};
 
 template <int E, int L0>
 __global__ void __launch_bounds__(64) k_col_bwd(ColBwdArgs A, DevPlan P) {
@@ -735,6 +713,9 @@ int kmm_fused_step(kmm_ctx *ctx) {
     const size_t smc = sizeof(double2) * (64 * (size_t)E + 2 * 2 * 2 * (size_t)ctx->ny);
     const int nblk = (int)(ncols / 2);
     kmm_tic(ctx);
+    int cst = ctx->use_colblk ? kmm_colblk_fwd(ctx, F, FU->tabs, FU->rj) : KMM_ERR_UNSUPPORTED;
+    if (cst != KMM_OK && cst != KMM_ERR_UNSUPPORTED) return cst;
+    if (cst == KMM_ERR_UNSUPPORTED) {
 #define COLF(EE, LL)                                                                                  \
     do {                                                                                              \
         RET(kmm_smem_attr(ctx, (const void *)k_col_fwd<EE, LL>, smc));                                \
@@ -757,6 +738,7 @@ int kmm_fused_step(kmm_ctx *ctx) {
     }
 #undef COLF
     CKL();
+    }
     kmm_toc(ctx, KMM_STAGE_COLUMN);
     // swap the history buffers: FNM1 <- old FN (read above), FN will receive the new terms
     ctx->f[KMM_FNM1] = fn_old; ctx->f[KMM_FN] = fnm1_old;
@@ -817,6 +799,9 @@ int kmm_fused_step(kmm_ctx *ctx) {
     B.wavx = ctx->d_wavx; B.wavz = ctx->d_wavz; B.nz = nz; B.nxh = nxh; B.nyp = nyp; B.nzh = ctx->nzh;
     B.scalar = scalar; B.dyde = ctx->dyde;
     kmm_tic(ctx);
+    cst = ctx->use_colblk ? kmm_colblk_bwd(ctx, B, FU->rj) : KMM_ERR_UNSUPPORTED;
+    if (cst != KMM_OK && cst != KMM_ERR_UNSUPPORTED) return cst;
+    if (cst == KMM_ERR_UNSUPPORTED) {
 #define COLB(EE, LL)                                                                                  \
     do {                                                                                              \
         RET(kmm_smem_attr(ctx, (const void *)k_col_bwd<EE, LL>, smc));                                \
@@ -839,6 +824,7 @@ int kmm_fused_step(kmm_ctx *ctx) {
     }
 #undef COLB
     CKL();
+    }
     kmm_toc(ctx, KMM_STAGE_POST);
     // tracers (solvers.f90:3463-3476) and the CFL check (3497-3514)
     int st = KMM_OK;

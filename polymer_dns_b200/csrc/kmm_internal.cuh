@@ -92,6 +92,7 @@ struct kmm_ctx {
     double *po, *drag;
     size_t po_n, drag_n;
     int use_fused;
+    int use_colblk;   // fused step: blocked-layout column kernels where compiled (default 1)
 };
 
 void kmm_fused_release(kmm_ctx *ctx);

@@ -298,7 +298,8 @@ def test_full_size_properties():
         assert 0 < g.stats().cflmax < 1.0
 
 
-@pytest.mark.parametrize("grid,scalar", [((32, 32, 32), 0), ((24, 32, 16), 1), ((16, 64, 12), 1)])
+@pytest.mark.parametrize("grid,scalar", [((32, 32, 32), 0), ((24, 32, 16), 1), ((16, 64, 12), 1), ((16, 96, 12), 0),
+                                         ((16, 128, 16), 1)])
 def test_fused_step_matches_routine_path(rt, oracle_mod, grid, scalar):
     """kmm_step's fused kernels against the routine-by-routine kernels and the oracle after 5 steps."""
     kw = dict(scalar_on=scalar, diff=1.0, scalar_bc=1, scalar_q=0.5) if scalar else {}
@@ -324,3 +325,25 @@ def test_fused_step_matches_routine_path(rt, oracle_mod, grid, scalar):
         a, b = ctxs[0].download(name), ctxs[1].download(name)
         assert kc.rel_err(a, b) <= 1e-12, name
         _cmp(ctxs[0], o, name, RUN_TOL)
+
+
+@pytest.mark.parametrize("grid", [(16, 32, 16), (16, 64, 12), (12, 96, 12), (16, 128, 16)])
+def test_blocked_columns_match_warp_columns(rt, grid):
+    """The fused step's blocked-layout column kernels (16 lanes per column) against the
+    warp-per-column kernels, with scalar, after 5 steps (KMM_OPT_COLUMN_BLOCKED on / off)."""
+    p = kc.cfg_small(*grid, scalar_on=1, diff=1.0, scalar_bc=1, scalar_q=0.5)
+    fields = kc.initial_fields(p, amp=0.05, seed=4)
+    sc = np.zeros_like(fields[0])
+    ctxs = []
+    for blocked in (1, 0):
+        g = rt.KmmContext(p)
+        g.call("set_option", 2, blocked)
+        kc.load_initial(g, p, fields, sc)
+        assert g.initial() == 0
+        ctxs.append(g)
+    for _ in range(5):
+        for g in ctxs:
+            assert g.step() == 0
+    for name in ["V", "OMY", "FN", "FNM1", "GN", "GNM1", "U0", "W0", "H1N", "H3N", "SCALAR", "SCN", "SCNM1"]:
+        a, b = ctxs[0].download(name), ctxs[1].download(name)
+        assert kc.rel_err(a, b) <= 1e-12, name
