@@ -281,6 +281,8 @@ def run_kmm(a, rank, world, local_rank):
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
         }
+        if p.precision == 0 and not a.no_mixed and a.config in ("cfg1", "cfg2"):
+            result["mixed"] = mixed_report(a, f, extra, local_rank, ms_per_step)
         if not a.no_cpu_baseline and world == 1:
             result["cpu_baseline"] = cpu_baseline(a.config, a.cpu_steps)
     ctx.close()
@@ -288,6 +290,62 @@ def run_kmm(a, rank, world, local_rank):
         dist.barrier()
         dist.destroy_process_group()
     return result
+
+
+def mixed_report(a, f, extra, local_rank, fp64_ms):
+    """The mixed-precision form (FP32 transforms and products, FP64 solves) on the same workload:
+    its device-resident speed, and its error against the FP64 drop-in from the same initial state
+    after 10 and 1000 steps (relative max-norm error of u, v, w and the scalar; bulk kinetic
+    energy and wall shear from kmm_flowstats)."""
+    from polymer_dns_b200 import runtime
+    p32, _, _ = make_config(a.config, 1)
+    p64, _, _ = make_config(a.config, 0)
+    c32 = runtime.KmmContext(p32, device=local_rank)
+    load(c32, f, extra, c32.upload)
+    c32.initial()
+    for _ in range(a.warmup):
+        c32.step()
+    c32.call("sync")
+    c32.event_record(0)
+    for _ in range(a.steps):
+        c32.step()
+    c32.event_record(1)
+    ms = c32.event_elapsed(0, 1) / a.steps
+    c32.close()
+    # accuracy: both forms from the same state
+    ctx = {}
+    for prec, pp in ((0, p64), (1, p32)):
+        c = runtime.KmmContext(pp, device=local_rank)
+        load(c, f, extra, c.upload)
+        c.initial()
+        ctx[prec] = c
+    names = {"u": "U", "v": "V", "w": "W"}
+    if p64.scalar_on:
+        names["scalar"] = "SCALAR"
+    _, s0 = ctx[0].flowstats()
+    errs = {}
+    done = 0
+    for mark in (10, 1000):
+        for c in ctx.values():
+            c.run(mark - done)
+        done = mark
+        st = {prec: c.flowstats() for prec, c in ctx.items()}   # runs veloc: u, w current
+        e = {}
+        for k, n in names.items():
+            x, y = ctx[1].download(n), ctx[0].download(n)
+            e[k] = float(np.abs(x - y).max() / max(np.abs(y).max(), 1e-300))
+        (_, s64), (_, s32) = st[0], st[1]
+        e["bulk_ke"] = float(abs(s32[3] - s64[3]) / abs(s64[3]))
+        e["wall_shear"] = float(max(abs(s32[1] - s64[1]), abs(s32[2] - s64[2])) / max(abs(s64[1]), abs(s64[2])))
+        errs[str(mark)] = {k: float("%.3e" % v) for k, v in e.items()}
+    _, s64 = ctx[0].flowstats()
+    drift = {"bulk_ke_fp64": float("%.4e" % ((s64[3] - s0[3]) / s0[3])),
+             "wall_shear_top_fp64": float("%.4e" % ((s64[1] - s0[1]) / s0[1]))}
+    for c in ctx.values():
+        c.close()
+    return {"value": round(1e3 / ms, 3), "unit": "timesteps/s", "ms_per_step": round(ms, 4),
+            "speedup_vs_fp64": round(fp64_ms / ms, 3), "dtype": "fp32 transforms/products, fp64 solves",
+            "rel_err_vs_fp64": errs, "drift_over_1000_steps": drift}
 
 
 def cpu_baseline(config, nsteps):
@@ -332,6 +390,7 @@ def main():
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision speed / error report")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3

@@ -238,6 +238,19 @@ int  kmm_run(kmm_ctx *ctx, int n);
 int  kmm_tracer_update(kmm_ctx *ctx);
 /* init_part's velocity interpolation, part_track.f90:229-292 */
 int  kmm_init_part(kmm_ctx *ctx);
+/* calcswirl (helpers.f90:197-404, solvers.f90:3421 and 3480): swirl strength from the spectral
+ * velocity gradients U11..U33 (kmm_gradv; after kmm_step run kmm_veloc first, the fused step
+ * keeps only the prognostic fields) into SWIRL3D, and at each particle into SWIRLPART.  The
+ * reference evaluates it inside every vcw3dp; here it is called at output cadence.      */
+int  kmm_calcswirl(kmm_ctx *ctx);
+/* Flow statistics of writeoutputs (helpers.f90:1227-1438) from the current state (runs
+ * kmm_veloc first).  prof: 7 * (ny+1) doubles (host) = mean u profile (solvers.f90:3486-3494),
+ * u'_rms, v_rms, w_rms, R12 = <u'v>, T12 = <du/dy>/re, and (not in the reference) the kinetic
+ * energy profile 0.5 <u^2 + v^2 + w^2>; scal: 4 doubles = bulk velocity (trapezoid of
+ * helpers.f90:1355-1359), top and bottom wall shear <du/dy>/re, bulk kinetic energy (same
+ * trapezoid).  The x-z means come from Parseval sums over the modes, which equal the
+ * reference's 3/2-grid means exactly for the dealiased fields.                          */
+int  kmm_flowstats(kmm_ctx *ctx, double *prof, double *scal);
 
 /* ---- options --------------------------------------------------------------- */
 enum kmm_option {

@@ -13,6 +13,7 @@
 #include "kmm_oracle.h"
 
 #include <complex.h>
+#include <float.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -2090,4 +2091,183 @@ int orc_run(orc_ctx *c, int n)
 /* ------------------------------------------------------------------------- */
 /* swirl strength (diagnostic), helpers.f90:197-404                           */
 /* ------------------------------------------------------------------------- */
-int orc_calcswirl(orc_ctx *c) { (void)c; return KMM_ERR_UNSUPPORTED; }
+/* eig (helpers.f90:197-275): Cardano's closed form of the eigenvalues of the 3x3 velocity-gradient
+ * matrix in complex arithmetic, restated term by term: tr = trace, P = (tr^2 - 3 M2)/9 with M2 the
+ * sum of the principal 2x2 minors, Q = tr^3/27 - tr M2/6 + det/2, S = (Q + (Q^2 - P^3)^(1/2))^(1/3)
+ * (principal powers, as the Fortran complex ** real), then
+ *   l1 = tr/3 + P/S + S,  l2,3 = tr/3 -+ sqrt(3)(P/S - S) i/2 - P/(2S) - S/2.
+ * calcswirl (helpers.f90:339-404): swirl = sqrt(Im l1^2 + Im l2^2 + Im l3^2), and 0 where that is
+ * not a finite positive number (the reference's floor(swirl/swirl) /= 1 test). */
+static double swirl_point(double r11, double r12, double r13, double r21, double r22, double r23, double r31,
+                          double r32, double r33)
+{
+    const cplx u11 = r11, u12 = r12, u13 = r13, u21 = r21, u22 = r22, u23 = r23, u31 = r31, u32 = r32, u33 = r33;
+    const cplx tr = u11 + u22 + u33;
+    const cplx P = tr * tr / 9.0 - (u11 * u22) / 3.0 + (u12 * u21) / 3.0 - (u11 * u33) / 3.0 + (u13 * u31) / 3.0 -
+                   (u22 * u33) / 3.0 + (u23 * u32) / 3.0;
+    const cplx M2 = u11 * u22 - u12 * u21 + u11 * u33 - u13 * u31 + u22 * u33 - u23 * u32;
+    const cplx Q = tr * tr * tr / 27.0 - (tr * M2) / 6.0 + (u11 * u22 * u33) / 2.0 - (u11 * u23 * u32) / 2.0 -
+                   (u12 * u21 * u33) / 2.0 + (u12 * u23 * u31) / 2.0 + (u13 * u21 * u32) / 2.0 -
+                   (u13 * u22 * u31) / 2.0;
+    const cplx S = cpow(Q + cpow(Q * Q - P * P * P, 0.5), 1.0 / 3.0);
+    const cplx PS = P / S;
+    const cplx l1 = tr / 3.0 + PS + S;
+    const cplx rot = (sqrt(3.0) * (PS - S) * I) / 2.0;
+    const cplx l2 = tr / 3.0 - rot - PS / 2.0 - S / 2.0;
+    const cplx l3 = tr / 3.0 + rot - PS / 2.0 - S / 2.0;
+    const double a = cimag(l1), b = cimag(l2), d = cimag(l3);
+    double sw = sqrt(a * a + b * b + d * d);
+    if (!(sw > 0.0 && sw <= DBL_MAX)) sw = 0.0;
+    return sw;
+}
+
+/* calcswirl: the nine velocity gradients u11..u33 (spectral, from gradv) to physical space on the
+ * 3/2 grid with the transforms of vcw3dp (solvers.f90:2241-2879), swirl at every point into
+ * SWIRL3D (nyp,mz,mx) (solvers.f90:3421), and its value at each particle into SWIRLPART
+ * (fluid_interp1, solvers.f90:3480). */
+/* one spectral field (nyp,nz,nxh) to physical values on the 3/2 grid (nyp,mz,mx), with the
+ * transforms of vcw3dp: c(i)/2 scaling and DCT-I along y (solvers.f90:2241-2546), zero-padded
+ * inverse c2c along z and c2r along x (solvers.f90:2578-2879) */
+static void to_phys3d(orc_ctx *c, const cplx *src, double *phys)
+{
+    const int nyp = c->nyp, nz = c->nz, nxh = c->nxh, mx = c->mx, mz = c->mz, ny = c->ny, nzh = c->nzh;
+    const size_t nspec = (size_t)nyp * nz * nxh;
+    const int hx = mx / 2 + 1;
+    cplx *yin = malloc(sizeof(cplx) * nspec);
+#pragma omp parallel
+    {
+        cplx *x = malloc(sizeof(cplx) * nyp), *o = malloc(sizeof(cplx) * nyp);
+        cplx *w1 = malloc(sizeof(cplx) * 2 * ny), *w2 = malloc(sizeof(cplx) * 2 * ny);
+#pragma omp for
+        for (int col = 0; col < nz * nxh; ++col) {
+            const cplx *sp = src + (size_t)col * nyp;
+            for (int i = 0; i < nyp; ++i) {
+                double fac = c->c[i] / 2.0;
+                x[i] = creal(sp[i]) * fac + I * (cimag(sp[i]) * fac);
+            }
+            dct1_c(&c->py2, x, o, w1, w2);
+            memcpy(yin + (size_t)col * nyp, o, sizeof(cplx) * nyp);
+        }
+        free(x); free(o); free(w1); free(w2);
+    }
+#pragma omp parallel
+    {
+        int wl = mx > mz ? mx : mz;
+        cplx *w1 = malloc(sizeof(cplx) * wl), *w2 = malloc(sizeof(cplx) * wl);
+        cplx *s = malloc(sizeof(cplx) * (size_t)mz * hx);
+        double *row = malloc(sizeof(double) * mx);
+#pragma omp for
+        for (int i = 0; i < nyp; ++i) {
+            memset(s, 0, sizeof(cplx) * (size_t)mz * hx);
+            for (int k = 0; k < nxh; ++k) {
+                for (int j = 0; j < mz; ++j) w1[j] = 0.0;
+                for (int j = 1; j <= nz; ++j) {
+                    int jj = (j <= nzh) ? j : (mz - nz) + j;
+                    w1[jj - 1] = yin[SIDX(c, i, j - 1, k)];
+                }
+                fft_exec(&c->pmz, w1, w2, +1);
+                for (int j = 0; j < mz; ++j) s[(size_t)j * hx + k] = w1[j];
+            }
+            for (int j = 0; j < mz; ++j) {
+                c2r_pair(&c->pmx, s + (size_t)j * hx, NULL, row, NULL, w1, w2);
+                for (int k = 0; k < mx; ++k) phys[PIDX(c, i, j, k)] = row[k];
+            }
+        }
+        free(w1); free(w2); free(s); free(row);
+    }
+    free(yin);
+}
+
+int orc_calcswirl(orc_ctx *c)
+{
+    const size_t nphys = (size_t)c->nyp * c->mz * c->mx;
+    double *phys[9];
+    for (int m = 0; m < 9; ++m) {
+        phys[m] = malloc(sizeof(double) * nphys);
+        to_phys3d(c, SF(c, KMM_U11 + m), phys[m]);
+    }
+    double *sw = RF(c, KMM_SWIRL3D);
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (size_t q = 0; q < nphys; ++q)
+        sw[q] = swirl_point(phys[0][q], phys[1][q], phys[2][q], phys[3][q], phys[4][q], phys[5][q], phys[6][q],
+                            phys[7][q], phys[8][q]);
+    int st = KMM_OK;
+    if (c->p.npart > 0) {
+        const double *xp = RF(c, KMM_XPART), *yp = RF(c, KMM_YPART), *zp = RF(c, KMM_ZPART);
+        double *spart = RF(c, KMM_SWIRLPART);
+        for (int n = 0; n < c->p.npart; ++n) {
+            double a, b;
+            if (fluid_interp(c, xp[n], yp[n], zp[n], sw, sw, sw, &spart[n], &a, &b)) st = KMM_ERR_INTERP;
+        }
+    }
+    for (int m = 0; m < 9; ++m) free(phys[m]);
+    return st;
+}
+
+/* Flow statistics of writeoutputs (helpers.f90:1227-1438) from the current state: veloc, then
+ * u, v, w and u12 = du/dy on the 3/2 grid, and the reference's loops: the mean profile (the
+ * uxmean of solvers.f90:3486-3494), u'_rms, v_rms, w_rms, R12 = <u'v>, T12 = <u12>/re, the bulk
+ * velocity by the trapezoid of helpers.f90:1355-1359, the top / bottom wall shear <u12>/re at
+ * y index 1 / nyp.  Added (not in the reference): the kinetic-energy profile 0.5 <u^2+v^2+w^2>
+ * and its bulk value by the same trapezoid.
+ *   prof[7][nyp] = umean, urms, vrms, wrms, R12, T12, ke;  scal[4] = massflux, tau_top, tau_bot, ke_bulk */
+int orc_flowstats(orc_ctx *c, double *prof, double *scal)
+{
+    const int nyp = c->nyp, mz = c->mz, mx = c->mx;
+    const size_t nphys = (size_t)nyp * mz * mx, nspec = (size_t)nyp * c->nz * c->nxh;
+    int st = orc_veloc(c);
+    if (st) return st;
+    cplx *du = malloc(sizeof(cplx) * nspec);
+    cderiv_arr(c, SF(c, KMM_U), du);
+    double *u = malloc(sizeof(double) * nphys), *v = malloc(sizeof(double) * nphys);
+    double *w = malloc(sizeof(double) * nphys), *u12 = malloc(sizeof(double) * nphys);
+    to_phys3d(c, SF(c, KMM_U), u);
+    to_phys3d(c, SF(c, KMM_V), v);
+    to_phys3d(c, SF(c, KMM_W), w);
+    to_phys3d(c, du, u12);
+    free(du);
+    double *umean = prof, *urms = prof + nyp, *vrms = prof + 2 * nyp, *wrms = prof + 3 * nyp;
+    double *R12 = prof + 4 * nyp, *T12 = prof + 5 * nyp, *ke = prof + 6 * nyp;
+    const double re = c->re, nm = (double)mx * (double)mz;
+    for (int i = 0; i < nyp; ++i) {
+        double s = 0.0;
+        for (int k = 0; k < mx; ++k) {
+            double sz = 0.0;
+            for (int j = 0; j < mz; ++j) sz += u[PIDX(c, i, j, k)];
+            s += sz / mz;
+        }
+        umean[i] = s / mx;
+    }
+    for (int i = 0; i < nyp; ++i) {
+        double a = 0.0, b = 0.0, d = 0.0, r = 0.0, t = 0.0, e = 0.0;
+        for (int k = 0; k < mx; ++k)
+            for (int j = 0; j < mz; ++j) {
+                const size_t q = PIDX(c, i, j, k);
+                const double up = u[q] - umean[i];
+                a += up * up;
+                b += v[q] * v[q];
+                d += w[q] * w[q];
+                r += up * v[q];
+                t += u12[q] / re;
+                e += 0.5 * (u[q] * u[q] + v[q] * v[q] + w[q] * w[q]);
+            }
+        urms[i] = sqrt(a / nm);
+        vrms[i] = sqrt(b / nm);
+        wrms[i] = sqrt(d / nm);
+        R12[i] = r / nm;
+        T12[i] = t / nm;
+        ke[i] = e / nm;
+    }
+    double mf = 0.0, kb = 0.0;
+    for (int i = 0; i < nyp - 1; ++i) {
+        const double dy = fabs(c->ycoord[i + 1] - c->ycoord[i]);
+        mf += 1.0 / c->yl * 0.5 * (umean[i + 1] + umean[i]) * dy;
+        kb += 1.0 / c->yl * 0.5 * (ke[i + 1] + ke[i]) * dy;
+    }
+    scal[0] = mf;
+    scal[1] = T12[0];
+    scal[2] = T12[nyp - 1];
+    scal[3] = kb;
+    free(u); free(v); free(w); free(u12);
+    return KMM_OK;
+}

@@ -82,6 +82,7 @@ int orc_tracer_update(orc_ctx *c);
 int orc_init_part(orc_ctx *c);
 /* swirl strength from the closed-form eigenvalues (helpers.f90:197-404) on the last 3/2-grid gradients */
 int orc_calcswirl(orc_ctx *c);
+int orc_flowstats(orc_ctx *c, double *prof, double *scal);
 
 #ifdef __cplusplus
 }

@@ -55,6 +55,8 @@ def lib():
             fn.argtypes = args
             fn.restype = i
         dp = ctypes.POINTER(ctypes.c_double)
+        L.orc_flowstats.argtypes = [vp, dp, dp]
+        L.orc_flowstats.restype = i
         L.orc_dct1.argtypes = [i, dp, dp]
         L.orc_fft.argtypes = [i, dp, dp, i]
         L.orc_rfft.argtypes = [i, dp, dp]
@@ -155,6 +157,16 @@ class Oracle:
 
     def dpdx(self):
         return self.L.orc_dpdx(self.h)
+
+    def flowstats(self):
+        """(prof[7][nyp], scal[4]) of orc_flowstats: umean, urms, vrms, wrms, R12, T12, ke profiles;
+        massflux, top / bottom wall shear, bulk kinetic energy."""
+        prof = np.zeros((7, self.ny + 1))
+        scal = np.zeros(4)
+        st = self.L.orc_flowstats(self.h, _dp(prof), _dp(scal))
+        if st:
+            raise RuntimeError("orc_flowstats returned %d" % st)
+        return prof, scal
 
     # convenience mirrors of the kmm_* entry points
     def initial(self):

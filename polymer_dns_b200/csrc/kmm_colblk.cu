@@ -8,6 +8,7 @@
 #include "kmm_colblk.cuh"
 
 #define CB_WARPS 4   // column pairs per block
+#define CB_MINB 3    // blocks per SM the register budget is sized for
 
 // phirhs on one column (solvers.f90:633-675)
 template <int K>
@@ -34,54 +35,119 @@ __device__ __forceinline__ void bphirhs(BCol<K> &x, const BCol<K> &fn, const BCo
         x.v[m] = make_double2(w.v[m].x - (1.0 - th) * d2.v[m].x / th, w.v[m].y - (1.0 - th) * d2.v[m].y / th);
 }
 
+// the column pair of the calling warp
+struct BPair {
+    int kx, q, j, col;
+    size_t off;
+    double kxv, kzv, w2;
+    bool mean;
+};
+
 template <int K>
-__global__ void __launch_bounds__(CB_WARPS * 32) k_bcol_fwd(ColFwdArgs A, FusedTabs T, const double *__restrict__ rj,
-                                                            const double2 *__restrict__ tw) {
+__device__ __forceinline__ bool bpair(BPair &P, int nz, int nzh, int nxh, const double *wavx, const double *wavz) {
+    const int warp = threadIdx.x >> 5, h = (threadIdx.x >> 4) & 1;
+    const int npair = nz / 2;
+    const int pr = blockIdx.x * CB_WARPS + warp;
+    if (pr >= nxh * npair) return false;
+    P.q = pr % npair;
+    P.kx = pr / npair;
+    P.j = h == 0 ? P.q : (P.q == 0 ? nzh : nz - P.q);
+    P.col = P.kx * nz + P.j;
+    P.off = (size_t)P.col * (16 * K + 1);
+    P.kxv = wavx[P.kx];
+    P.kzv = wavz[P.j];
+    P.w2 = P.kzv * P.kzv + P.kxv * P.kxv;
+    P.mean = (P.kx == 0 && P.j == 0);
+    return true;
+}
+
+// The forward column stage as four kernels, in this order (each reads only what the previous
+// ones have finished): scalar; omega_y; v (with the mean modes); u, w and the y-physical
+// outputs of the velocity.  Splitting keeps each kernel's registers and code small; the price
+// is one extra read of v and omega_y.
+
+// passive scalar (main_dns.f90:325-359): CN/AB2 right-hand side, Robin solve, norm, store; y-physical c, dc/dy
+template <int K, typename C>
+__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_scl(ColFwdArgs A, FusedTabs T, const double *__restrict__ rj,
+                                                            const C *__restrict__ tw) {
     constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ double2 sm[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, h = lane >> 4;
-    double2 *fa = sm + (size_t)warp * 4 * L, *fb = fa + 2 * L;
-    const int npair = A.nz / 2;
-    const int pr = blockIdx.x * CB_WARPS + warp;
-    if (pr >= A.nxh * npair) return;   // whole warps only: no block-wide barrier below
-    const int q = pr % npair, kx = pr / npair;
-    const int j = h == 0 ? q : (q == 0 ? A.nzh : A.nz - q);
-    const int col = kx * A.nz + j;
-    const size_t off = (size_t)col * NYP;
-    const double kxv = A.wavx[kx], kzv = A.wavz[j];
-    const double w2 = kzv * kzv + kxv * kxv;
-    const double g1 = A.re / (A.dt * A.th);
-    const bool mean = (kx == 0 && j == 0);
-    const size_t ncols = (size_t)A.nz * A.nxh;
+    C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
+    BPair P;
+    if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;   // whole warps: no block barrier below
+    const size_t fstride = (size_t)A.nz * A.nxh * NYP;
     const double2 zero = make_double2(0.0, 0.0);
-    BCol<K> d1;
-
-    // ---- passive scalar (main_dns.f90:325-359), finished first: norm, store, y-physical c, dc/dy
-    if (A.scalar) {
-        BCol<K> s;
-        bload<K>(s, A.scal + off);
-        {
-            BCol<K> n1, n0;
-            bload<K>(n1, A.scn + off);
-            bload<K>(n0, A.scnm1 + off);
-            bphirhs<K>(s, n1, n0, A.re, A.diff, A.dt, A.th, w2, A.dyde, FULL);
-        }
-        const TauTab ts = tab_at(T, TB_SCL, col, NYP);
-        bsolve_robin<K>(s, ts, zero, zero, w2 + T.g[TB_SCL], A.c0, rj, FULL);
-        bnorm<K>(s, kx, j, A.nzh);
-        bstore<K>(A.scal + off, s);
-        bcderiv<K>(d1, s, A.dyde, FULL);
-        bdct<K>(s, fa, fb, tw, true);
-        bstore<K>(A.yp + 6 * ncols * NYP + off, s);
-        bdct<K>(d1, fa, fb, tw, true);
-        bstore<K>(A.yp + 7 * ncols * NYP + off, d1);
+    BCol<K> s, d1;
+    bload<K>(s, A.scal + P.off);
+    {
+        BCol<K> n1, n0;
+        bload<K>(n1, A.scn + P.off);
+        bload<K>(n0, A.scnm1 + P.off);
+        bphirhs<K>(s, n1, n0, A.re, A.diff, A.dt, A.th, P.w2, A.dyde, FULL);
     }
-    // ---- wall-normal velocity: phi, phirhs, Helmholtz + Poisson (main_dns.f90:363-407)
+    const TauTab ts = tab_at(T, TB_SCL, P.col, NYP);
+    bsolve_robin<K>(s, ts, zero, zero, P.w2 + T.g[TB_SCL], A.c0, rj, FULL);
+    bnorm<K>(s, P.kx, P.j, A.nzh);
+    bstore<K>(A.scal + P.off, s);
+    bcderiv<K>(d1, s, A.dyde, FULL);
+    bdct_store<K, C>(s, fa, fb, tw, (C *)A.yp + 6 * fstride + P.off);
+    bdct_store<K, C>(d1, fa, fb, tw, (C *)A.yp + 7 * fstride + P.off);
+}
+
+// normal vorticity (main_dns.f90:411-422, 479-484, 500-502, 520-526): phirhs, Robin solve, zero
+// on the mean column, norm, store; y-physical omega_y
+template <int K, typename C>
+__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_omy(ColFwdArgs A, FusedTabs T, const double *__restrict__ rj,
+                                                            const C *__restrict__ tw) {
+    constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
+    constexpr unsigned FULL = 0xffffffffu;
+    extern __shared__ double2 sm[];
+    C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
+    BPair P;
+    if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;
+    const size_t fstride = (size_t)A.nz * A.nxh * NYP;
+    const double g1 = A.re / (A.dt * A.th);
+    const double2 zero = make_double2(0.0, 0.0);
+    BCol<K> om;
+    bload<K>(om, A.omy + P.off);
+    {
+        BCol<K> g1c, g0c;
+        bload<K>(g1c, A.gn + P.off);
+        bload<K>(g0c, A.gnm1 + P.off);
+        bphirhs<K>(om, g1c, g0c, A.re, 1.0, A.dt, A.th, P.w2, A.dyde, FULL);
+    }
+    const TauTab to = tab_at(T, TB_OMY, P.col, NYP);
+    bsolve_robin<K>(om, to, zero, zero, P.w2 + g1, A.c0, rj, FULL);
+    if (P.mean) {
+#pragma unroll
+        for (int m = 0; m <= K; ++m) om.v[m] = zero;
+    }
+    bnorm<K>(om, P.kx, P.j, A.nzh);
+    bstore<K>(A.omy + P.off, om);
+    bdct_store<K, C>(om, fa, fb, tw, (C *)A.yp + 3 * fstride + P.off);
+}
+
+// wall-normal velocity (main_dns.f90:363-407, 426-466, 489-502, 520): phi, phirhs, Helmholtz and
+// Poisson solves, influence-matrix correction, uzero for the mean modes, norm, store; y-physical v
+template <int K, typename C>
+__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_v(ColFwdArgs A, FusedTabs T, const double *__restrict__ rj,
+                                                          const C *__restrict__ tw) {
+    constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
+    constexpr unsigned FULL = 0xffffffffu;
+    extern __shared__ double2 sm[];
+    C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
+    const int lane = threadIdx.x & 31, h = lane >> 4;
+    BPair P;
+    if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;
+    const size_t fstride = (size_t)A.nz * A.nxh * NYP;
+    const double g1 = A.re / (A.dt * A.th);
+    const double2 zero = make_double2(0.0, 0.0);
+    const double w2 = P.w2;
     BCol<K> v;
     {
-        BCol<K> d2;
-        bload<K>(v, A.v + off);
+        BCol<K> d1, d2;
+        bload<K>(v, A.v + P.off);
         bcderiv<K>(d1, v, A.dyde, FULL);
         bcderiv<K>(d2, d1, A.dyde, FULL);
 #pragma unroll
@@ -89,26 +155,17 @@ __global__ void __launch_bounds__(CB_WARPS * 32) k_bcol_fwd(ColFwdArgs A, FusedT
     }
     {
         BCol<K> f1, f0;
-        bload<K>(f1, A.fn + off);
-        bload<K>(f0, A.fnm1 + off);
+        bload<K>(f1, A.fn + P.off);
+        bload<K>(f0, A.fnm1 + P.off);
         bphirhs<K>(v, f1, f0, A.re, 1.0, A.dt, A.th, w2, A.dyde, FULL);
     }
     {
-        const TauTab tp = tab_at(T, TB_PHI, col, NYP);
+        const TauTab tp = tab_at(T, TB_PHI, P.col, NYP);
         bsolve_dirichlet<K>(v, tp, zero, zero, w2 + g1, A.c0, rj, FULL);
-        const TauTab tv = tab_at(T, TB_V, col, NYP);
+        const TauTab tv = tab_at(T, TB_V, P.col, NYP);
         bsolve_dirichlet<K>(v, tv, zero, zero, w2, A.c0, rj, FULL);
     }
-    // ---- normal vorticity phirhs (main_dns.f90:411-422)
-    BCol<K> om;
-    bload<K>(om, A.omy + off);
-    {
-        BCol<K> g1c, g0c;
-        bload<K>(g1c, A.gn + off);
-        bload<K>(g0c, A.gnm1 + off);
-        bphirhs<K>(om, g1c, g0c, A.re, 1.0, A.dt, A.th, w2, A.dyde, FULL);
-    }
-    // ---- influence matrix (main_dns.f90:426-466)
+    // influence matrix
     {
         double2 wb, wt;
         if (A.nb == 1 && A.nt == 1) {
@@ -122,29 +179,24 @@ __global__ void __launch_bounds__(CB_WARPS * 32) k_bcol_fwd(ColFwdArgs A, FusedT
             if (A.nb == 2) wb = b2;
             if (A.nt == 2) wt = t2;
         }
-        const double2 c1 = cdiv(csub(cmul(wb, A.dnv2t[col]), cmul(wt, A.dnv2b[col])), A.denom[col]);
-        const double2 c2 = cdiv(csub(cmul(wt, A.dnv1b[col]), cmul(wb, A.dnv1t[col])), A.denom[col]);
+        const double2 c1 = cdiv(csub(cmul(wb, A.dnv2t[P.col]), cmul(wt, A.dnv2b[P.col])), A.denom[P.col]);
+        const double2 c2 = cdiv(csub(cmul(wt, A.dnv1b[P.col]), cmul(wb, A.dnv1t[P.col])), A.denom[P.col]);
         BCol<K> gfa;
-        bload<K>(gfa, A.gf1 + off);
+        bload<K>(gfa, A.gf1 + P.off);
 #pragma unroll
         for (int m = 0; m <= K; ++m) {
             const double2 a = cmul(c1, gfa.v[m]);
             v.v[m] = make_double2(v.v[m].x + a.x, v.v[m].y + a.y);
         }
-        bload<K>(gfa, A.gf2 + off);
+        bload<K>(gfa, A.gf2 + P.off);
 #pragma unroll
         for (int m = 0; m <= K; ++m) {
             const double2 b = cmul(c2, gfa.v[m]);
             v.v[m] = make_double2(v.v[m].x + b.x, v.v[m].y + b.y);
         }
     }
-    // ---- normal vorticity Robin solve (main_dns.f90:479-484)
-    {
-        const TauTab to = tab_at(T, TB_OMY, col, NYP);
-        bsolve_robin<K>(om, to, zero, zero, w2 + g1, A.c0, rj, FULL);
-    }
-    // ---- mean modes (main_dns.f90:489-502): uzero for u0 and w0 on the (0,0) column's half-warp
-    if (kx == 0 && q == 0) {
+    // mean modes: uzero for u0 and w0 on the (0,0) column's half-warp
+    if (P.kx == 0 && P.q == 0) {
         if (h == 0) {
             constexpr unsigned HM = 0x0000ffffu;
             const double th = A.th;
@@ -180,27 +232,43 @@ __global__ void __launch_bounds__(CB_WARPS * 32) k_bcol_fwd(ColFwdArgs A, FusedT
             A.h1nm1[i] = A.h1n[i];
             A.h3nm1[i] = A.h3n[i];
         }
-        if (mean) {
-#pragma unroll
-            for (int m = 0; m <= K; ++m) om.v[m] = zero;
-        }
     }
-    // ---- norm(v), norm(omy); veloc (main_dns.f90:520-526, solvers.f90:1576-1659)
-    bnorm<K>(v, kx, j, A.nzh);
-    bnorm<K>(om, kx, j, A.nzh);
+    bnorm<K>(v, P.kx, P.j, A.nzh);
+    if (P.mean) {
+#pragma unroll
+        for (int m = 0; m <= K; ++m) v.v[m] = zero;
+    }
+    bstore<K>(A.v + P.off, v);
+    bdct_store<K, C>(v, fa, fb, tw, (C *)A.yp + 1 * fstride + P.off);
+}
+
+// veloc (solvers.f90:1576-1659) from the new v and omega_y; y-physical u, du/dy, w, dw/dy
+template <int K, typename C>
+__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_uw(ColFwdArgs A, const C *__restrict__ tw) {
+    constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
+    constexpr unsigned FULL = 0xffffffffu;
+    extern __shared__ double2 sm[];
+    C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
+    BPair P;
+    if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;
+    const size_t fstride = (size_t)A.nz * A.nxh * NYP;
+    const double2 zero = make_double2(0.0, 0.0);
+    const double kxv = P.kxv, kzv = P.kzv, w2 = P.w2;
     BCol<K> u, w;
     {
-        BCol<K> dv;
+        BCol<K> v, om, dv;
+        bload<K>(v, A.v + P.off);
+        bload<K>(om, A.omy + P.off);
         bcderiv<K>(dv, v, A.dyde, FULL);
 #pragma unroll
         for (int m = 0; m <= K; ++m) {
             const double2 d = dv.v[m], o = om.v[m];
-            if (kx > 0) {
+            if (P.kx > 0) {
                 const double2 sa = cadd(cimul(d, -kxv), cimul(o, kzv));
                 u.v[m] = make_double2(-sa.x / w2, -sa.y / w2);
                 const double2 sb = csub(cimul(d, -kzv), cimul(o, kxv));
                 w.v[m] = make_double2(-sb.x / w2, -sb.y / w2);
-            } else if (j > 0) {
+            } else if (P.j > 0) {
                 const double kz2 = kzv * kzv;
                 const double2 sa = cimul(o, kzv);
                 u.v[m] = make_double2(-sa.x / kz2, -sa.y / kz2);
@@ -211,51 +279,39 @@ __global__ void __launch_bounds__(CB_WARPS * 32) k_bcol_fwd(ColFwdArgs A, FusedT
                 w.v[m] = zero;
             }
         }
-        if (mean) {
+    }
+    if (P.mean) {
 #pragma unroll
-            for (int m = 0; m <= K; ++m) {
-                const int i = bidx<K>(m);
-                u.v[m] = make_double2(A.u0[i], 0.0);
-                w.v[m] = make_double2(A.w0[i], 0.0);
-                v.v[m] = zero;
-            }
-        }
-        // norm(u), norm(w): the pair is conjugate-symmetric already; zero the kz Nyquist column
-        if (j == A.nzh) {
-#pragma unroll
-            for (int m = 0; m <= K; ++m) {
-                u.v[m] = zero;
-                w.v[m] = zero;
-            }
+        for (int m = 0; m <= K; ++m) {
+            const int i = bidx<K>(m);
+            u.v[m] = make_double2(A.u0[i], 0.0);
+            w.v[m] = make_double2(A.w0[i], 0.0);
         }
     }
-    bstore<K>(A.v + off, v);
-    bstore<K>(A.omy + off, om);
-    // ---- y-physical outputs: u, v, w, omega_y, du/dy, dw/dy
-    double2 *yp = A.yp;
-    bdct<K>(v, fa, fb, tw, true);
-    bstore<K>(yp + 1 * ncols * NYP + off, v);
-    bdct<K>(om, fa, fb, tw, true);
-    bstore<K>(yp + 3 * ncols * NYP + off, om);
+    // norm(u), norm(w): the pair is conjugate-symmetric already; zero the kz Nyquist column
+    if (P.j == A.nzh) {
+#pragma unroll
+        for (int m = 0; m <= K; ++m) {
+            u.v[m] = zero;
+            w.v[m] = zero;
+        }
+    }
+    BCol<K> d1;
     bcderiv<K>(d1, u, A.dyde, FULL);
-    bdct<K>(u, fa, fb, tw, true);
-    bstore<K>(yp + 0 * ncols * NYP + off, u);
-    bdct<K>(d1, fa, fb, tw, true);
-    bstore<K>(yp + 4 * ncols * NYP + off, d1);
+    bdct_store<K, C>(u, fa, fb, tw, (C *)A.yp + 0 * fstride + P.off);
+    bdct_store<K, C>(d1, fa, fb, tw, (C *)A.yp + 4 * fstride + P.off);
     bcderiv<K>(d1, w, A.dyde, FULL);
-    bdct<K>(w, fa, fb, tw, true);
-    bstore<K>(yp + 2 * ncols * NYP + off, w);
-    bdct<K>(d1, fa, fb, tw, true);
-    bstore<K>(yp + 5 * ncols * NYP + off, d1);
+    bdct_store<K, C>(w, fa, fb, tw, (C *)A.yp + 2 * fstride + P.off);
+    bdct_store<K, C>(d1, fa, fb, tw, (C *)A.yp + 5 * fstride + P.off);
 }
 
-template <int K>
-__global__ void __launch_bounds__(CB_WARPS * 32) k_bcol_bwd(ColBwdArgs A, const double2 *__restrict__ tw) {
+template <int K, typename C>
+__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_bwd(ColBwdArgs A, const C *__restrict__ tw) {
     constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ double2 sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, h = lane >> 4;
-    double2 *fa = sm + (size_t)warp * 4 * L, *fb = fa + 2 * L;
+    C *fa = reinterpret_cast<C *>(sm + (size_t)warp * 4 * L), *fb = fa + 2 * L;
     const int npair = A.nz / 2;
     const int pr = blockIdx.x * CB_WARPS + warp;
     if (pr >= A.nxh * npair) return;
@@ -265,40 +321,39 @@ __global__ void __launch_bounds__(CB_WARPS * 32) k_bcol_bwd(ColBwdArgs A, const 
     const size_t off = (size_t)col * NYP;
     const size_t ncols = (size_t)A.nz * A.nxh;
     const double kxv = A.wavx[kx], kzv = A.wavz[j];
-    BCol<K> h1, h2, h3;
-    bload<K>(h1, A.yo + 0 * ncols * NYP + off);
-    bdct<K>(h1, fa, fb, tw, false);
-    bload<K>(h2, A.yo + 1 * ncols * NYP + off);
-    bdct<K>(h2, fa, fb, tw, false);
-    bload<K>(h3, A.yo + 2 * ncols * NYP + off);
-    bdct<K>(h3, fa, fb, tw, false);
-    // norm(fn), norm(gn), norm(omz) after vcw3dp (main_dns.f90:620-624)
-    bnorm<K>(h2, kx, j, A.nzh);
-    bnorm<K>(h1, kx, j, A.nzh);
-    bnorm<K>(h3, kx, j, A.nzh);
-    // spectral filter (main_dns.f90:710-745)
+    // spectral filter (main_dns.f90:710-745): exp(-3 (|kz|/nzh)^10) exp(-3 (i/ny)^10)
     const int j1 = j + 1;
     const int jjf = (j1 > A.nzh) ? A.nz - j1 + 1 : j1 - 1;
     const double zr = (double)jjf / (double)A.nzh;
     const double z2 = zr * zr, z4 = z2 * z2, z8 = z4 * z4;
     const double zs = exp(-3.0 * (z8 * z2));
-    BCol<K> sc;
-    if (A.scalar) {
-        bload<K>(sc, A.yo + 3 * ncols * NYP + off);
-        bdct<K>(sc, fa, fb, tw, false);
-        bnorm<K>(sc, kx, j, A.nzh);
-    }
+    double ys[K + 1];
 #pragma unroll
     for (int m = 0; m <= K; ++m) {
-        const int i = bidx<K>(m);
-        const double yr = (double)i / (double)NY;
+        const double yr = (double)bidx<K>(m) / (double)NY;
         const double y2 = yr * yr, y4 = y2 * y2, y8 = y4 * y4;
-        const double ys = exp(-3.0 * (y8 * y2));
-        h3.v[m] = make_double2(h3.v[m].x * zs * ys, h3.v[m].y * zs * ys);
-        h1.v[m] = make_double2(h1.v[m].x * zs * ys, h1.v[m].y * zs * ys);
-        h2.v[m] = make_double2(h2.v[m].x * zs * ys, h2.v[m].y * zs * ys);
-        if (A.scalar) sc.v[m] = make_double2(sc.v[m].x * zs * ys, sc.v[m].y * zs * ys);
+        ys[m] = exp(-3.0 * (y8 * y2));
     }
+    auto filt = [&](BCol<K> &x) {
+#pragma unroll
+        for (int m = 0; m <= K; ++m) x.v[m] = make_double2(x.v[m].x * zs * ys[m], x.v[m].y * zs * ys[m]);
+    };
+    // each term: DCT back (/ny, halved ends), norm after vcw3dp (main_dns.f90:620-624), filter.
+    // The scalar term first, then h1 and h3 (gn, omz and the y-derivative fn needs), then h2.
+    if (A.scalar) {
+        BCol<K> sc;
+        bload_dct<K, C>(sc, (const C *)A.yo + 3 * ncols * NYP + off, fa, fb, tw);
+        bnorm<K>(sc, kx, j, A.nzh);
+        filt(sc);
+        bstore<K>(A.scn + off, sc);
+    }
+    BCol<K> h1, h3, d;
+    bload_dct<K, C>(h1, (const C *)A.yo + 0 * ncols * NYP + off, fa, fb, tw);
+    bload_dct<K, C>(h3, (const C *)A.yo + 2 * ncols * NYP + off, fa, fb, tw);
+    bnorm<K>(h1, kx, j, A.nzh);
+    bnorm<K>(h3, kx, j, A.nzh);
+    filt(h3);
+    filt(h1);
     // h1n = Re gn(:,1,1), h3n = Re omz(:,1,1) (main_dns.f90:748-751)
     if (kx == 0 && j == 0) {
         const int t = lane & 15;
@@ -313,24 +368,30 @@ __global__ void __launch_bounds__(CB_WARPS * 32) k_bcol_bwd(ColBwdArgs A, const 
         }
     }
     // nonlin (solvers.f90:1497-1572): fn = -k^2 h2 - d/dy(i(kz h3 + kx h1)); gn = i(kz h1 - kx h3)
-    BCol<K> tt, d;
+    {
+        BCol<K> tt;
 #pragma unroll
-    for (int m = 0; m <= K; ++m) {
-        const double2 s = make_double2(kzv * h3.v[m].x + kxv * h1.v[m].x, kzv * h3.v[m].y + kxv * h1.v[m].y);
-        tt.v[m] = make_double2(-s.y, s.x);
+        for (int m = 0; m <= K; ++m) {
+            const double2 s = make_double2(kzv * h3.v[m].x + kxv * h1.v[m].x, kzv * h3.v[m].y + kxv * h1.v[m].y);
+            tt.v[m] = make_double2(-s.y, s.x);
+        }
+        bcderiv<K>(d, tt, A.dyde, FULL);
     }
-    bcderiv<K>(d, tt, A.dyde, FULL);
-    const double w2 = -kxv * kxv - kzv * kzv;
 #pragma unroll
     for (int m = 0; m <= K; ++m) {
-        h2.v[m] = make_double2(w2 * h2.v[m].x - d.v[m].x, w2 * h2.v[m].y - d.v[m].y);
         const double2 s = make_double2(kzv * h1.v[m].x - kxv * h3.v[m].x, kzv * h1.v[m].y - kxv * h3.v[m].y);
         h1.v[m] = make_double2(-s.y, s.x);
     }
-    bstore<K>(A.fn + off, h2);
     bstore<K>(A.gn + off, h1);
     bstore<K>(A.omz + off, h3);
-    if (A.scalar) bstore<K>(A.scn + off, sc);
+    BCol<K> h2;
+    bload_dct<K, C>(h2, (const C *)A.yo + 1 * ncols * NYP + off, fa, fb, tw);
+    bnorm<K>(h2, kx, j, A.nzh);
+    filt(h2);
+    const double w2 = -kxv * kxv - kzv * kzv;
+#pragma unroll
+    for (int m = 0; m <= K; ++m) h2.v[m] = make_double2(w2 * h2.v[m].x - d.v[m].x, w2 * h2.v[m].y - d.v[m].y);
+    bstore<K>(A.fn + off, h2);
     (void)h;
 }
 
@@ -340,43 +401,79 @@ static int colblk_k(const kmm_ctx *ctx) {
     return ny / 16;
 }
 
-int kmm_colblk_fwd(kmm_ctx *ctx, const ColFwdArgs &A, const FusedTabs &T, const double *rj) {
+int kmm_colblk_fwd(kmm_ctx *ctx, const ColFwdArgs &A, const FusedTabs &T, const double *rj, const void *tw,
+                   bool fp32) {
     const int K = colblk_k(ctx);
     if (!K) return KMM_ERR_UNSUPPORTED;
     const int npairs = ctx->nxh * (ctx->nz / 2);
     const int nblk = (npairs + CB_WARPS - 1) / CB_WARPS;
     const size_t smem = sizeof(double2) * (size_t)CB_WARPS * 4 * (2 * ctx->ny);
-#define BF(KK)                                                                                        \
-    case KK:                                                                                          \
-        RET(kmm_smem_attr(ctx, (const void *)k_bcol_fwd<KK>, smem));                                  \
-        k_bcol_fwd<KK><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(A, T, rj, ctx->wy2.tw);             \
-        break;
+#define BF(KK, CC)                                                                                    \
+    do {                                                                                              \
+        const CC *twc = (const CC *)tw;                                                               \
+        if (A.scalar) {                                                                               \
+            RET(kmm_smem_attr(ctx, (const void *)k_bcol_scl<KK, CC>, smem));                          \
+            k_bcol_scl<KK, CC><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(A, T, rj, twc);             \
+            CKL();                                                                                    \
+        }                                                                                             \
+        RET(kmm_smem_attr(ctx, (const void *)k_bcol_omy<KK, CC>, smem));                              \
+        k_bcol_omy<KK, CC><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(A, T, rj, twc);                 \
+        CKL();                                                                                        \
+        RET(kmm_smem_attr(ctx, (const void *)k_bcol_v<KK, CC>, smem));                                \
+        k_bcol_v<KK, CC><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(A, T, rj, twc);                   \
+        CKL();                                                                                        \
+        RET(kmm_smem_attr(ctx, (const void *)k_bcol_uw<KK, CC>, smem));                               \
+        k_bcol_uw<KK, CC><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(A, twc);                         \
+        CKL();                                                                                        \
+        return KMM_OK;                                                                                \
+    } while (0)
+    if (fp32) {
+        switch (K) {
+        case 2: BF(2, float2);
+        case 4: BF(4, float2);
+        case 6: BF(6, float2);
+        case 8: BF(8, float2);
+        default: return KMM_ERR_UNSUPPORTED;
+        }
+    }
     switch (K) {
-        BF(2) BF(4) BF(6) BF(8)
+    case 2: BF(2, double2);
+    case 4: BF(4, double2);
+    case 6: BF(6, double2);
+    case 8: BF(8, double2);
     default: return KMM_ERR_UNSUPPORTED;
     }
 #undef BF
-    CKL();
-    return KMM_OK;
 }
 
-int kmm_colblk_bwd(kmm_ctx *ctx, const ColBwdArgs &B, const double *rj) {
+int kmm_colblk_bwd(kmm_ctx *ctx, const ColBwdArgs &B, const void *tw, bool fp32) {
     const int K = colblk_k(ctx);
     if (!K) return KMM_ERR_UNSUPPORTED;
-    (void)rj;
     const int npairs = ctx->nxh * (ctx->nz / 2);
     const int nblk = (npairs + CB_WARPS - 1) / CB_WARPS;
     const size_t smem = sizeof(double2) * (size_t)CB_WARPS * 4 * (2 * ctx->ny);
-#define BB(KK)                                                                                        \
-    case KK:                                                                                          \
-        RET(kmm_smem_attr(ctx, (const void *)k_bcol_bwd<KK>, smem));                                  \
-        k_bcol_bwd<KK><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(B, ctx->wy2.tw);                    \
-        break;
+#define BB(KK, CC)                                                                                    \
+    do {                                                                                              \
+        RET(kmm_smem_attr(ctx, (const void *)k_bcol_bwd<KK, CC>, smem));                              \
+        k_bcol_bwd<KK, CC><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(B, (const CC *)tw);             \
+        CKL();                                                                                        \
+        return KMM_OK;                                                                                \
+    } while (0)
+    if (fp32) {
+        switch (K) {
+        case 2: BB(2, float2);
+        case 4: BB(4, float2);
+        case 6: BB(6, float2);
+        case 8: BB(8, float2);
+        default: return KMM_ERR_UNSUPPORTED;
+        }
+    }
     switch (K) {
-        BB(2) BB(4) BB(6) BB(8)
+    case 2: BB(2, double2);
+    case 4: BB(4, double2);
+    case 6: BB(6, double2);
+    case 8: BB(8, double2);
     default: return KMM_ERR_UNSUPPORTED;
     }
 #undef BB
-    CKL();
-    return KMM_OK;
 }

@@ -16,6 +16,7 @@
 // half-warp (the mean-mode column).
 #pragma once
 
+#include "kmm_fft.cuh"
 #include "kmm_fused.cuh"
 
 template <int K>
@@ -172,30 +173,25 @@ __device__ __forceinline__ void btau_rhs(BCol<K> &s, double c0, const double *__
 
 // forward elimination, per parity p, positions P = 2+p .. top_p descending (top_0 = NY, the last
 // coefficient; top_1 = NY-1):  y_P = W_P - te[P] y_{P+2},  y_top = W_top.  Rows P < 2 unchanged.
+// Pass 1 composes each lane's affine map from its carry-in to its lowest slot, a shuffle scan
+// gives every lane its carry-in, pass 2 runs the recurrence serially from that carry.
 template <int K>
 __device__ __forceinline__ void bforward(BCol<K> &w, const double *__restrict__ te, unsigned mask) {
     constexpr int NY = 16 * K;
     const int t = bl_t();
-    double ap[K];
-    double2 yl[K];
     double A0 = 1.0, A1 = 1.0;
     double2 B0 = make_double2(0.0, 0.0), B1 = make_double2(0.0, 0.0);
 #pragma unroll
     for (int m = K - 1; m >= 0; --m) {
-        const int p = m & 1;
         const int P = t * K + m;
-        const double a = (P < 2 + p || P == NY - 1) ? 0.0 : -te[P];
+        const double a = (P < 2 + (m & 1) || P == NY - 1) ? 0.0 : -te[P];
         const double2 W = w.v[m];
-        if (p == 0) {
+        if ((m & 1) == 0) {
             B0 = make_double2(a * B0.x + W.x, a * B0.y + W.y);
             A0 = a * A0;
-            yl[m] = B0;
-            ap[m] = A0;
         } else {
             B1 = make_double2(a * B1.x + W.x, a * B1.y + W.y);
             A1 = a * A1;
-            yl[m] = B1;
-            ap[m] = A1;
         }
     }
     // suffix composition of the lane maps y_low(t) = A_t y_low(t+1) + B_t
@@ -219,9 +215,12 @@ __device__ __forceinline__ void bforward(BCol<K> &w, const double *__restrict__ 
         c1 = make_double2(0.0, 0.0);
     }
 #pragma unroll
-    for (int m = 0; m < K; ++m) {
-        const double2 c = (m & 1) ? c1 : c0;
-        w.v[m] = make_double2(yl[m].x + ap[m] * c.x, yl[m].y + ap[m] * c.y);
+    for (int m = K - 1; m >= 0; --m) {
+        const int P = t * K + m;
+        const double a = (P < 2 + (m & 1) || P == NY - 1) ? 0.0 : -te[P];
+        double2 &c = (m & 1) ? c1 : c0;
+        c = make_double2(a * c.x + w.v[m].x, a * c.y + w.v[m].y);
+        w.v[m] = c;
     }
 }
 
@@ -255,42 +254,39 @@ __device__ __forceinline__ void bborder(const BCol<K> &y, const double *__restri
 }
 
 // back substitution, per parity ascending: x_p = x1_p (boundary row), x_P = (y_P - a1(P) x_{P-2}) / d[P]
-// with a1(P) = wn / (4P(P-1)) (doubled for P = 2)
+// with a1(P) = wn / (4P(P-1)) (doubled for P = 2); the same two passes as bforward
 template <int K>
 __device__ __forceinline__ void bbacksub(BCol<K> &y, double2 x1e, double2 x1o, const double *__restrict__ td, double wn,
                                          const double *__restrict__ rj, unsigned mask) {
     constexpr int NY = 16 * K;
     const int t = bl_t();
-    double ap[K];
-    double2 xl[K];
+    double rd[K], am[K];
     double A0 = 1.0, A1 = 1.0;
     double2 B0 = make_double2(0.0, 0.0), B1 = make_double2(0.0, 0.0);
 #pragma unroll
     for (int m = 0; m < K; ++m) {
         const int p = m & 1;
         const int P = t * K + m;
-        double a;
         double2 b;
         if (P == p) {
-            a = 0.0;
+            rd[m] = 0.0;
+            am[m] = 0.0;
             b = p ? x1o : x1e;
         } else {
             const double r = 1.0 / td[P];
             double a1 = wn * rj[P];
             if (P == 2) a1 = 2.0 * a1;
-            a = -a1 * r;
+            rd[m] = r;
+            am[m] = -a1 * r;
             b = make_double2(y.v[m].x * r, y.v[m].y * r);
         }
+        const double a = am[m];
         if (p == 0) {
             B0 = make_double2(a * B0.x + b.x, a * B0.y + b.y);
             A0 = a * A0;
-            xl[m] = B0;
-            ap[m] = A0;
         } else {
             B1 = make_double2(a * B1.x + b.x, a * B1.y + b.y);
             A1 = a * A1;
-            xl[m] = B1;
-            ap[m] = A1;
         }
     }
     // prefix composition of the lane maps x_high(t) = A_t x_high(t-1) + B_t
@@ -312,8 +308,12 @@ __device__ __forceinline__ void bbacksub(BCol<K> &y, double2 x1e, double2 x1o, c
     }
 #pragma unroll
     for (int m = 0; m < K; ++m) {
-        const double2 c = (m & 1) ? c1 : c0;
-        y.v[m] = make_double2(xl[m].x + ap[m] * c.x, xl[m].y + ap[m] * c.y);
+        const int p = m & 1;
+        const int P = t * K + m;
+        double2 &c = p ? c1 : c0;
+        if (P == p) c = p ? x1o : x1e;
+        else c = make_double2(am[m] * c.x + y.v[m].x * rd[m], am[m] * c.y + y.v[m].y * rd[m]);
+        y.v[m] = c;
     }
     // the last coefficient (row n of the even system)
     const double2 xm2 = sh16_idx(mask, y.v[K - 2], 15);
@@ -405,6 +405,78 @@ __device__ __forceinline__ void bnorm(BCol<K> &x, int kx, int j, int nzh) {
     }
 }
 
+// park a column pair in the warp's shared buffer (swizzled like the DCT buffers) and fetch it back
+template <int K>
+__device__ __forceinline__ void bstash(const BCol<K> &x, double2 *buf) {
+    const int t = bl_t(), h = (threadIdx.x >> 4) & 1;
+#pragma unroll
+    for (int m = 0; m < K; ++m) buf[swz<double2>(h * 32 * K + t * K + m)] = x.v[m];
+    if (t == 15) buf[swz<double2>(h * 32 * K + 16 * K)] = x.v[K];
+}
+template <int K>
+__device__ __forceinline__ void bunstash(BCol<K> &x, const double2 *buf) {
+    const int t = bl_t(), h = (threadIdx.x >> 4) & 1;
+#pragma unroll
+    for (int m = 0; m < K; ++m) x.v[m] = buf[swz<double2>(h * 32 * K + t * K + m)];
+    x.v[K] = buf[swz<double2>(h * 32 * K + 16 * K)];
+}
+
+// y-physical values of the warp's two columns (DCT-I of c(i)/2-scaled coefficients,
+// solvers.f90:2241-2546) written to dst in precision C: the coefficients are rounded to C
+// before the transform, which then runs in C (the specialised FFT of length 2 NY).
+template <int K, typename C>
+__device__ __forceinline__ void bdct_store(const BCol<K> &x, C *a, C *b, const C *tw, C *__restrict__ dst) {
+    typedef typename kct::Real<C>::T T;
+    constexpr int NY = 16 * K, L = 2 * NY;
+    const int t = bl_t(), h = (threadIdx.x >> 4) & 1;
+    const int base = h * L;
+#pragma unroll
+    for (int m = 0; m <= K; ++m) {
+        if (m == K && t != 15) continue;
+        const int i = bidx<K>(m);
+        double2 v = x.v[m];
+        if (i > 0 && i < NY) v = make_double2(v.x * 0.5, v.y * 0.5);
+        const C c = kct::mk<C>((T)v.x, (T)v.y);
+        a[swz<C>(base + i)] = c;
+        if (i > 0 && i < NY) a[swz<C>(base + L - i)] = c;
+    }
+    __syncwarp();
+    const C *r = fft_warp_ct<C, L, -1, 2, true>(a, b, tw);
+#pragma unroll
+    for (int m = 0; m < K; ++m) dst[t * K + m] = r[swz<C>(base + t * K + m)];
+    if (t == 15) dst[NY] = r[swz<C>(base + NY)];
+    __syncwarp();
+}
+
+// Chebyshev coefficients of the warp's two columns from y-physical values in precision C
+// (DCT-I, /ny, first and last halved, solvers.f90:3279-3416); the transform runs in C and the
+// result is widened to FP64.
+template <int K, typename C>
+__device__ __forceinline__ void bload_dct(BCol<K> &x, const C *__restrict__ src, C *a, C *b, const C *tw) {
+    constexpr int NY = 16 * K, L = 2 * NY;
+    const int t = bl_t(), h = (threadIdx.x >> 4) & 1;
+    const int base = h * L;
+#pragma unroll
+    for (int m = 0; m <= K; ++m) {
+        if (m == K && t != 15) continue;
+        const int i = bidx<K>(m);
+        const C c = src[i];
+        a[swz<C>(base + i)] = c;
+        if (i > 0 && i < NY) a[swz<C>(base + L - i)] = c;
+    }
+    __syncwarp();
+    const C *r = fft_warp_ct<C, L, -1, 2, true>(a, b, tw);
+#pragma unroll
+    for (int m = 0; m <= K; ++m) {
+        const int i = bidx<K>(m);
+        const C c = r[swz<C>(base + i)];
+        double2 v = make_double2((double)c.x / (double)NY, (double)c.y / (double)NY);
+        if (i == 0 || i == NY) v = make_double2(v.x / 2.0, v.y / 2.0);
+        x.v[m] = v;
+    }
+    __syncwarp();
+}
+
 // DCT-I of the warp's two columns through the specialised FFT of length 2 NY (even extension):
 //   to_phys: scale by c(i)/2 first (solvers.f90:2241-2546);  !to_phys: /ny, halve the ends (3279-3416)
 // a, b: the warp's two smem buffers of 2 * 2 NY complex each.
@@ -412,22 +484,22 @@ template <int K>
 __device__ __forceinline__ void bdct(BCol<K> &x, double2 *a, double2 *b, const double2 *tw, bool to_phys) {
     constexpr int NY = 16 * K, L = 2 * NY;
     const int t = bl_t(), h = (threadIdx.x >> 4) & 1;
-    double2 *sa = a + h * L;
+    const int base = h * L;
 #pragma unroll
     for (int m = 0; m <= K; ++m) {
         if (m == K && t != 15) continue;
         const int i = bidx<K>(m);
         double2 v = x.v[m];
         if (to_phys && i > 0 && i < NY) v = make_double2(v.x * 0.5, v.y * 0.5);
-        sa[i] = v;
-        if (i > 0 && i < NY) sa[L - i] = v;
+        a[swz<double2>(base + i)] = v;
+        if (i > 0 && i < NY) a[swz<double2>(base + L - i)] = v;
     }
     __syncwarp();
-    const double2 *r = fft_warp_ct<double2, L, -1, 2>(a, b, tw) + h * L;
+    const double2 *r = fft_warp_ct<double2, L, -1, 2, true>(a, b, tw);
 #pragma unroll
     for (int m = 0; m <= K; ++m) {
         const int i = bidx<K>(m);
-        double2 v = r[i];
+        double2 v = r[swz<double2>(base + i)];
         if (!to_phys) {
             v = make_double2(v.x / (double)NY, v.y / (double)NY);
             if (i == 0 || i == NY) v = make_double2(v.x / 2.0, v.y / 2.0);

@@ -284,6 +284,7 @@ extern "C" int kmm_ctx_create(const kmm_params *p, int device, kmm_ctx **out) {
     CK(cudaMalloc(&c->d_umax, sizeof(double) * (size_t)c->nyp));
     CK(cudaMalloc(&c->d_status, sizeof(int)));
     CK(cudaMalloc(&c->d_scratch, sizeof(double) * 9 * KMM_MAX_NYP));
+    CK(cudaMallocHost(&c->h_pin, sizeof(double) * (2 * KMM_MAX_NYP + 1)));
     CK(cudaMemset(c->d_status, 0, sizeof(int)));
     for (int w = 0; w < 6; ++w) {
         CK(cudaMalloc(&c->wrk[w], sizeof(double2) * c->nspec));
@@ -316,6 +317,7 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
     for (int e = 0; e < 16; ++e)
         if (ctx->user_ev[e]) cudaEventDestroy(ctx->user_ev[e]);
     kmm_fused_release(ctx);
+    if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
     if (ctx->po) cudaFree(ctx->po);
     if (ctx->drag) cudaFree(ctx->drag);
     for (int f = 0; f < KMM_MAXF; ++f)

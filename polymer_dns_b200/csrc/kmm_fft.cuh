@@ -74,6 +74,22 @@ __device__ __forceinline__ C mul(C a, C b) { return mk<C>(a.x * b.x - a.y * b.y,
 template <typename C>
 __device__ __forceinline__ C scl(C a, typename Real<C>::T s) { return mk<C>(a.x * s, a.y * s); }
 
+}   // namespace kct
+
+// Shared-memory swizzle of the FFT buffers: element x of a 128-byte row r = x / E (E = 8 double2
+// or 16 float2 per row) is stored at column (x mod E) xor (r mod E).  Unit-stride runs, the
+// stride-R writes of a radix-R stage and the blocked K-per-lane column accesses then spread over
+// all banks.  Callers that pass SWZ = true to fft_warp_ct write the input and read the output
+// through swz<C>().
+template <typename C>
+__device__ __forceinline__ int swz(int x) {
+    constexpr int RB = sizeof(C) == 16 ? 3 : 4;
+    constexpr int RM = (1 << RB) - 1;
+    return x ^ ((x >> RB) & RM);
+}
+
+namespace kct {
+
 // radix-R DFTs, X_q = sum_r v_r exp(S 2 pi i r q / R); the same operation sequence as radix_dft /
 // radix8_dft of the runtime FFT
 template <typename C, int R, int S>
@@ -164,7 +180,7 @@ struct Dft<C, 8, S> {
 
 // one Stockham stage: butterflies j = 0..N/R-1 of each of the NQ sequences (stored N apart)
 // spread over the 32 lanes
-template <typename C, int N, int F, int S, int NQ>
+template <typename C, int N, int F, int S, int NQ, bool SWZ>
 __device__ __forceinline__ void stage(const C *__restrict__ src, C *__restrict__ dst, const C *__restrict__ tw,
                                       int lane) {
     constexpr int R = fac(N, F);
@@ -178,13 +194,13 @@ __device__ __forceinline__ void stage(const C *__restrict__ src, C *__restrict__
         if ((NQ * NR) % 32 == 0 || u < NQ * NR) {
             const int sq = NQ > 1 ? u / NR : 0;
             const int j = NQ > 1 ? u - sq * NR : u;
-            const C *sp = src + sq * N;
-            C *dp = dst + sq * N;
+            const int base = sq * N;
             const int k = j % NS;
             C v[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                C x = sp[j + r * NR];
+                const int xi = base + j + r * NR;
+                C x = src[SWZ ? swz<C>(xi) : xi];
                 if (NS > 1 && r > 0 && k) {
                     C w = __ldg(&tw[r * k * TSTEP]);
                     if (S > 0) w.y = -w.y;
@@ -193,25 +209,28 @@ __device__ __forceinline__ void stage(const C *__restrict__ src, C *__restrict__
                 v[r] = x;
             }
             Dft<C, R, S>::run(v);
-            const int idxD = (j - k) * R + k;
+            const int idxD = base + (j - k) * R + k;
 #pragma unroll
-            for (int q = 0; q < R; ++q) dp[idxD + q * NS] = v[q];
+            for (int q = 0; q < R; ++q) {
+                const int xo = idxD + q * NS;
+                dst[SWZ ? swz<C>(xo) : xo] = v[q];
+            }
         }
     }
 }
 
-template <typename C, int N, int F, int S, int NQ, bool END>
+template <typename C, int N, int F, int S, int NQ, bool SWZ, bool END>
 struct Step;
-template <typename C, int N, int F, int S, int NQ>
-struct Step<C, N, F, S, NQ, true> {
+template <typename C, int N, int F, int S, int NQ, bool SWZ>
+struct Step<C, N, F, S, NQ, SWZ, true> {
     static __device__ __forceinline__ C *go(C *src, C *, const C *, int) { return src; }
 };
-template <typename C, int N, int F, int S, int NQ>
-struct Step<C, N, F, S, NQ, false> {
+template <typename C, int N, int F, int S, int NQ, bool SWZ>
+struct Step<C, N, F, S, NQ, SWZ, false> {
     static __device__ __forceinline__ C *go(C *src, C *dst, const C *tw, int lane) {
-        stage<C, N, F, S, NQ>(src, dst, tw, lane);
+        stage<C, N, F, S, NQ, SWZ>(src, dst, tw, lane);
         __syncwarp();
-        return Step<C, N, F + 1, S, NQ, (F + 1 >= nfac(N))>::go(dst, src, tw, lane);
+        return Step<C, N, F + 1, S, NQ, SWZ, (F + 1 >= nfac(N))>::go(dst, src, tw, lane);
     }
 };
 }   // namespace kct
@@ -219,11 +238,11 @@ struct Step<C, N, F, S, NQ, false> {
 // S = -1: exp(-2 pi i jk/N) (FFTW_FORWARD), +1: exp(+...) (FFTW_BACKWARD).  NQ sequences of
 // length N lie N apart in a; b is a scratch buffer of the same size (both private to the calling
 // warp); the input must be visible to the whole warp (__syncwarp after writing it).  Returns the
-// buffer holding the result.
-template <typename C, int N, int S, int NQ = 1>
+// buffer holding the result.  SWZ: the buffers are swizzled (element x at swz<C>(x)).
+template <typename C, int N, int S, int NQ = 1, bool SWZ = false>
 __device__ __forceinline__ C *fft_warp_ct(C *a, C *b, const C *tw) {
     static_assert(kct::nfac(N) > 0, "transform length must be 2^a 3^b 5^c");
-    return kct::Step<C, N, 0, S, NQ, false>::go(a, b, tw, threadIdx.x & 31);
+    return kct::Step<C, N, 0, S, NQ, SWZ, false>::go(a, b, tw, threadIdx.x & 31);
 }
 
 // the transform lengths with compiled instances (3/2-rule grids of nx, nz = 32, 64, 96, 128, 384

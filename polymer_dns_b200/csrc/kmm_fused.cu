@@ -103,6 +103,20 @@ __global__ void k_tau_tables(double *td, double *te, double *tb1, double *tb2, d
 
 
 
+// FP32 twiddles exp(-2 pi i m/n), rounded from long double, for the mixed-precision transforms
+static int make_twf(kmm_ctx *ctx, int n, float2 **out) {
+    float2 *h = (float2 *)malloc(sizeof(float2) * (size_t)n);
+    for (int k = 0; k < n; ++k) {
+        const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
+        h[k] = make_float2((float)cosl(a), -(float)sinl(a));
+    }
+    cudaError_t e = cudaMalloc(out, sizeof(float2) * (size_t)n);
+    if (e == cudaSuccess) e = cudaMemcpy(*out, h, sizeof(float2) * (size_t)n, cudaMemcpyHostToDevice);
+    free(h);
+    CK(e);
+    return KMM_OK;
+}
+
 static int build_tables(kmm_ctx *ctx) {
     if (ctx->fused) return KMM_OK;
     KmmFused *F = (KmmFused *)calloc(1, sizeof(KmmFused));
@@ -148,6 +162,9 @@ static int build_tables(kmm_ctx *ctx) {
         free(h);
         CK(e);
     }
+    RET(make_twf(ctx, 2 * ctx->ny, &F->twf_y2));
+    RET(make_twf(ctx, ctx->mz, &F->twf_mz));
+    RET(make_twf(ctx, ctx->mx, &F->twf_mx));
     const size_t ncp = (size_t)ncols * ctx->nyp, nq = (size_t)ctx->nyp * ctx->mz * ctx->nxh;
     CK(cudaMalloc(&F->yp, sizeof(double2) * ncp * 8));
     CK(cudaMalloc(&F->q, sizeof(double2) * nq * 10));
@@ -164,6 +181,7 @@ void kmm_fused_release(kmm_ctx *ctx) {
         cudaFree(F->tabs.tf[c]);
     }
     cudaFree(F->yp); cudaFree(F->q); cudaFree(F->r); cudaFree(F->yo); cudaFree(F->rj);
+    cudaFree(F->twf_y2); cudaFree(F->twf_mz); cudaFree(F->twf_mx);
     free(F);
     ctx->fused = NULL;
 }
@@ -477,7 +495,7 @@ __global__ void __launch_bounds__(64) k_col_fwd(ColFwdArgs A, FusedTabs T, DevPl
 #define ZT_Y 4
 #define ZT_WARPS (ZT_KX * ZT_Y)
 
-// Q[g][y][z][kx], g = u v w wx wy wz [c cx cy cz], from the y-physical base fields
+// Q[g][y][z][kx], g = u v w wx wy wz [cx cy cz], from the y-physical base fields
 // MZ > 0: compile-time z length (specialised FFT); MZ = 0: runtime plan
 template <int MZ>
 __global__ void __launch_bounds__(ZT_WARPS * 32) k_zb(const double2 *__restrict__ yp, double2 *__restrict__ q,
@@ -494,15 +512,16 @@ __global__ void __launch_bounds__(ZT_WARPS * 32) k_zb(const double2 *__restrict_
     double2 *a = sm + (size_t)warp * 2 * mz, *b = a + mz;
     double2 *stage = sm + (size_t)ZT_WARPS * 2 * mz;   // [y][z][kx] tile for the store
     const double kxv = act ? wavx[kx] : 0.0;
+    auto SW = [](int x) { return MZ > 0 ? swz<double2>(x) : x; };
     for (int g = 0; g < nout; ++g) {
         if (act) {
-            for (int z = lane; z < mz; z += 32) a[z] = make_double2(0.0, 0.0);
+            for (int z = lane; z < mz; z += 32) a[SW(z)] = make_double2(0.0, 0.0);
             __syncwarp();
             for (int kz = lane; kz < nz; kz += 32) {
                 const size_t o = ((size_t)kx * nz + kz) * nyp + y;
                 const double kzv = wavz[kz];
                 double2 val;
-                switch (g) {
+                switch (g < 6 ? g : g + 1) {   // q fields: u v w wx wy wz [cx cy cz]
                 case 3: {   // wx = dw/dy - i kz v
                     const double2 dw = __ldg(yp + 5 * ncols * nyp + o), vv = __ldg(yp + 1 * ncols * nyp + o);
                     val = csub(dw, cimul(vv, kzv));
@@ -519,13 +538,13 @@ __global__ void __launch_bounds__(ZT_WARPS * 32) k_zb(const double2 *__restrict_
                 default: val = __ldg(yp + (size_t)g * ncols * nyp + o); break;   // u v w
                 }
                 const int jj = kz < nzh ? kz : (mz - nz) + kz;
-                a[jj] = val;
+                a[SW(jj)] = val;
             }
             __syncwarp();
             const double2 *r;
-            if constexpr (MZ > 0) r = fft_warp_ct<double2, MZ, +1>(a, b, P.tw);
+            if constexpr (MZ > 0) r = fft_warp_ct<double2, MZ, +1, 1, true>(a, b, P.tw);
             else r = fft_warp(P, a, b, +1);
-            for (int z = lane; z < mz; z += 32) stage[((size_t)yl * mz + z) * ZT_KX + kl] = r[z];
+            for (int z = lane; z < mz; z += 32) stage[((size_t)yl * mz + z) * ZT_KX + kl] = r[SW(z)];
         }
         __syncthreads();
         // store rows of ZT_KX consecutive kx
@@ -554,16 +573,17 @@ __global__ void __launch_bounds__(ZT_WARPS * 32) k_zf(const double2 *__restrict_
     const int nzh = nz / 2;
     double2 *a = sm + (size_t)warp * 2 * mz, *b = a + mz;
     double2 *stage = sm + (size_t)ZT_WARPS * 2 * mz;   // [kx][kz][y] tile for the store
+    auto SW = [](int x) { return MZ > 0 ? swz<double2>(x) : x; };
     for (int o = 0; o < nout; ++o) {
         if (act) {
-            for (int z = lane; z < mz; z += 32) a[z] = __ldg(r + (((size_t)o * nyp + y) * mz + z) * nxh + kx);
+            for (int z = lane; z < mz; z += 32) a[SW(z)] = __ldg(r + (((size_t)o * nyp + y) * mz + z) * nxh + kx);
             __syncwarp();
             const double2 *res;
-            if constexpr (MZ > 0) res = fft_warp_ct<double2, MZ, -1>(a, b, P.tw);
+            if constexpr (MZ > 0) res = fft_warp_ct<double2, MZ, -1, 1, true>(a, b, P.tw);
             else res = fft_warp(P, a, b, -1);
             for (int kz = lane; kz < nz; kz += 32) {
                 const int jj = kz < nzh ? kz : (mz - nz) + kz;
-                const double2 v = res[jj];
+                const double2 v = res[SW(jj)];
                 stage[((size_t)kl * nz + kz) * ZT_Y + yl] = make_double2(v.x / scale, v.y / scale);
             }
         }
@@ -573,6 +593,144 @@ __global__ void __launch_bounds__(ZT_WARPS * 32) k_zf(const double2 *__restrict_
             const int yy = t % ZT_Y, kz = (t / ZT_Y) % nz, kk = t / (ZT_Y * nz);
             if (kx0 + kk < nxh && y0 + yy < nyp)
                 yo[(size_t)o * ncols * nyp + ((size_t)(kx0 + kk) * nz + kz) * nyp + y0 + yy] = stage[t];
+        }
+        __syncthreads();
+    }
+}
+
+// Specialised z kernels for the compiled lengths MZ (nz = 2 MZ / 3), C = double2 (FP64) or
+// float2 (mixed precision), with the next field's column values fetched into registers while the
+// current field's FFT runs.
+template <int MZ, typename C>
+__global__ void __launch_bounds__(ZT_WARPS * 32) k_zb2(const C *__restrict__ yp, C *__restrict__ q,
+                                                       const double *__restrict__ wavx, const double *__restrict__ wavz,
+                                                       const C *__restrict__ tw, int nout, int nyp, int nxh) {
+    typedef typename kct::Real<C>::T T;
+    constexpr int NZ = 2 * MZ / 3, NZH = NZ / 2, NE = (NZ + 31) / 32;
+    extern __shared__ double2 smd[];
+    C *sm = reinterpret_cast<C *>(smd);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kl = warp % ZT_KX, yl = warp / ZT_KX;
+    const int kx = blockIdx.x * ZT_KX + kl, y = blockIdx.y * ZT_Y + yl;
+    const bool act = kx < nxh && y < nyp;
+    const size_t fs = (size_t)NZ * nxh * nyp;   // field stride of the column layout
+    C *a = sm + (size_t)warp * 2 * MZ, *b = a + MZ;
+    C *stage = sm + (size_t)ZT_WARPS * 2 * MZ;   // [y][z][kx] tile for the store
+    const T kxv = act ? (T)wavx[kx] : (T)0;
+    const C zc = kct::mk<C>((T)0, (T)0);
+    C pf[NE];
+    // value of q field g at (kx, kz, y) from the y-physical base fields u v w omega_y du/dy dw/dy [c dc/dy]
+    auto fetch = [&](int g) {
+#pragma unroll
+        for (int e = 0; e < NE; ++e) {
+            const int kz = lane + 32 * e;
+            C val = zc;
+            if (act && kz < NZ) {
+                const size_t o = ((size_t)kx * NZ + kz) * nyp + y;
+                const T kzv = (T)wavz[kz];
+                switch (g < 6 ? g : g + 1) {   // q fields: u v w wx wy wz [cx cy cz]
+                case 3: {                      // wx = dw/dy - i kz v
+                    const C dw = __ldg(yp + 5 * fs + o), vv = __ldg(yp + 1 * fs + o);
+                    val = kct::mk<C>(dw.x + kzv * vv.y, dw.y - kzv * vv.x);
+                } break;
+                case 4: val = __ldg(yp + 3 * fs + o); break;
+                case 5: {   // wz = i kx v - du/dy
+                    const C vv = __ldg(yp + 1 * fs + o), du = __ldg(yp + 4 * fs + o);
+                    val = kct::mk<C>(-kxv * vv.y - du.x, kxv * vv.x - du.y);
+                } break;
+                case 7: {
+                    const C cc = __ldg(yp + 6 * fs + o);
+                    val = kct::mk<C>(-kxv * cc.y, kxv * cc.x);
+                } break;
+                case 8: val = __ldg(yp + 7 * fs + o); break;
+                case 9: {
+                    const C cc = __ldg(yp + 6 * fs + o);
+                    val = kct::mk<C>(-kzv * cc.y, kzv * cc.x);
+                } break;
+                default: val = __ldg(yp + (size_t)g * fs + o); break;   // u v w
+                }
+            }
+            pf[e] = val;
+        }
+    };
+    fetch(0);
+    for (int g = 0; g < nout; ++g) {
+        if (act) {
+            for (int z = NZH + lane; z < MZ - NZH; z += 32) a[swz<C>(z)] = zc;   // padding modes
+#pragma unroll
+            for (int e = 0; e < NE; ++e) {
+                const int kz = lane + 32 * e;
+                if (kz < NZ) a[swz<C>(kz < NZH ? kz : (MZ - NZ) + kz)] = pf[e];
+            }
+            __syncwarp();
+        }
+        if (g + 1 < nout) fetch(g + 1);
+        if (act) {
+            const C *r = fft_warp_ct<C, MZ, +1, 1, true>(a, b, tw);
+            for (int z = lane; z < MZ; z += 32) stage[((size_t)yl * MZ + z) * ZT_KX + kl] = r[swz<C>(z)];
+        }
+        __syncthreads();
+        // store rows of ZT_KX consecutive kx
+        const int kx0 = blockIdx.x * ZT_KX;
+        for (int t = threadIdx.x; t < ZT_Y * MZ * ZT_KX; t += blockDim.x) {
+            const int kk = t % ZT_KX, zz = (t / ZT_KX) % MZ, yy = t / (ZT_KX * MZ);
+            const int ky = blockIdx.y * ZT_Y + yy;
+            if (ky < nyp && kx0 + kk < nxh) q[(((size_t)g * nyp + ky) * MZ + zz) * nxh + kx0 + kk] = stage[t];
+        }
+        __syncthreads();
+    }
+}
+
+template <int MZ, typename C>
+__global__ void __launch_bounds__(ZT_WARPS * 32) k_zf2(const C *__restrict__ r, C *__restrict__ yo,
+                                                       const C *__restrict__ tw, int nout, int nyp, int nxh,
+                                                       double scale) {
+    typedef typename kct::Real<C>::T T;
+    constexpr int NZ = 2 * MZ / 3, NZH = NZ / 2, NE = (MZ + 31) / 32;
+    extern __shared__ double2 smd[];
+    C *sm = reinterpret_cast<C *>(smd);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kl = warp % ZT_KX, yl = warp / ZT_KX;
+    const int kx = blockIdx.x * ZT_KX + kl, y = blockIdx.y * ZT_Y + yl;
+    const bool act = kx < nxh && y < nyp;
+    const size_t ncols = (size_t)NZ * nxh;
+    C *a = sm + (size_t)warp * 2 * MZ, *b = a + MZ;
+    C *stage = sm + (size_t)ZT_WARPS * 2 * MZ;   // [kx][kz][y] tile for the store
+    const T rs = (T)(1.0 / scale);
+    C pf[NE];
+    auto fetch = [&](int o) {
+#pragma unroll
+        for (int e = 0; e < NE; ++e) {
+            const int z = lane + 32 * e;
+            if (act && z < MZ) pf[e] = __ldg(r + (((size_t)o * nyp + y) * MZ + z) * nxh + kx);
+        }
+    };
+    fetch(0);
+    for (int o = 0; o < nout; ++o) {
+        if (act) {
+#pragma unroll
+            for (int e = 0; e < NE; ++e) {
+                const int z = lane + 32 * e;
+                if (z < MZ) a[swz<C>(z)] = pf[e];
+            }
+            __syncwarp();
+        }
+        if (o + 1 < nout) fetch(o + 1);
+        if (act) {
+            const C *res = fft_warp_ct<C, MZ, -1, 1, true>(a, b, tw);
+            for (int kz = lane; kz < NZ; kz += 32) {
+                const C v = res[swz<C>(kz < NZH ? kz : (MZ - NZ) + kz)];
+                // FP64 divides by mx mz as the reference normalises; FP32 multiplies by the reciprocal
+                stage[((size_t)kl * NZ + kz) * ZT_Y + yl] =
+                    sizeof(T) == 8 ? kct::mk<C>((T)(v.x / scale), (T)(v.y / scale)) : kct::mk<C>(v.x * rs, v.y * rs);
+            }
+        }
+        __syncthreads();
+        const int kx0 = blockIdx.x * ZT_KX, y0 = blockIdx.y * ZT_Y;
+        for (int t = threadIdx.x; t < ZT_KX * NZ * ZT_Y; t += blockDim.x) {
+            const int yy = t % ZT_Y, kz = (t / ZT_Y) % NZ, kk = t / (ZT_Y * NZ);
+            if (kx0 + kk < nxh && y0 + yy < nyp)
+                yo[(size_t)o * ncols * nyp + ((size_t)(kx0 + kk) * NZ + kz) * nyp + y0 + yy] = stage[t];
         }
         __syncthreads();
     }
@@ -662,8 +820,10 @@ __global__ void __launch_bounds__(64) k_col_bwd(ColBwdArgs A, DevPlan P) {
 // ---------------------------------------------------------------------------
 // host driver
 // ---------------------------------------------------------------------------
-int kmm_fast_x(kmm_ctx *ctx, const double2 *q, double2 *r, int nin, int nout, bool save_uvw, double *up3,
+int kmm_fast_x(kmm_ctx *ctx, const double2 *q, double2 *r, int ic, int nout, bool save_uvw, double *up3,
                double *vp3, double *wp3);
+int kmm_fast_x2(kmm_ctx *ctx, const void *q, void *r, const void *tw, bool fp32, int ic, int nout, bool save_uvw,
+                double *up3, double *vp3, double *wp3);
 int kmm_tracers(kmm_ctx *ctx);
 
 // the fused path applies when: no polymer, no immersed boundary, Dirichlet-type velocity walls
@@ -678,15 +838,34 @@ bool kmm_fused_applicable(const kmm_ctx *ctx) {
     return true;
 }
 
+static int *h_pin_status(kmm_ctx *ctx) { return (int *)(ctx->h_pin + 2 * KMM_MAX_NYP); }
+
+int kmm_tracers_enqueue(kmm_ctx *ctx);
+
 int kmm_fused_step(kmm_ctx *ctx) {
+    RET(kmm_fused_launch(ctx));
+    return kmm_fused_finish(ctx);
+}
+
+int kmm_fused_launch(kmm_ctx *ctx) {
     const int nyp = ctx->nyp, nz = ctx->nz, nxh = ctx->nxh, mz = ctx->mz;
     const size_t ncols = (size_t)nz * nxh;
     const int scalar = ctx->p.scalar_on ? 1 : 0;
-    const int nbase = scalar ? 8 : 6, nq = scalar ? 10 : 6, nout = scalar ? 4 : 3;
+    const int nbase = scalar ? 8 : 6, nq = scalar ? 9 : 6, nout = scalar ? 4 : 3;
     RET(build_tables(ctx));
     KmmFused *FU = ctx->fused;
     double2 *g_yp = FU->yp, *g_q = FU->q, *g_r = FU->r, *g_yo = FU->yo;
     (void)nbase;
+    // the mixed-precision form (FP32 transforms and products, FP64 solves) has compiled kernels
+    // for ny, nx, nz in {32, 64, 96, 128} (nx, nz: the 3/2 lengths 48 .. 192)
+    const bool f32 = ctx->p.precision == 1;
+    const bool ct_mz = (mz == 48 || mz == 96 || mz == 144 || mz == 192);
+    const bool ct_mx = (ctx->mx == 48 || ctx->mx == 96 || ctx->mx == 144 || ctx->mx == 192);
+    const bool ct_y = (ctx->ny == 32 || ctx->ny == 64 || ctx->ny == 96 || ctx->ny == 128);
+    if (f32 && !(ct_mz && ct_mx && ct_y && ctx->use_colblk)) {
+        kmm_set_error(ctx, "mixed precision needs nx, ny, nz in {32, 64, 96, 128} and the blocked column kernels");
+        return KMM_ERR_UNSUPPORTED;
+    }
     ctx->it += 1;
 
     // history copies fnm1 = fn, gnm1 = gn, scnm1 = scn become pointer swaps: the kernels read the
@@ -713,7 +892,8 @@ int kmm_fused_step(kmm_ctx *ctx) {
     const size_t smc = sizeof(double2) * (64 * (size_t)E + 2 * 2 * 2 * (size_t)ctx->ny);
     const int nblk = (int)(ncols / 2);
     kmm_tic(ctx);
-    int cst = ctx->use_colblk ? kmm_colblk_fwd(ctx, F, FU->tabs, FU->rj) : KMM_ERR_UNSUPPORTED;
+    int cst = ctx->use_colblk ? kmm_colblk_fwd(ctx, F, FU->tabs, FU->rj, f32 ? (const void *)FU->twf_y2 : (const void *)ctx->wy2.tw, f32)
+                              : KMM_ERR_UNSUPPORTED;
     if (cst != KMM_OK && cst != KMM_ERR_UNSUPPORTED) return cst;
     if (cst == KMM_ERR_UNSUPPORTED) {
 #define COLF(EE, LL)                                                                                  \
@@ -748,48 +928,81 @@ int kmm_fused_step(kmm_ctx *ctx) {
     // z inverse transforms
     CK(cudaMemsetAsync(ctx->d_cfl, 0, sizeof(double) * nyp, ctx->stream));
     CK(cudaMemsetAsync(ctx->d_umax, 0, sizeof(double) * nyp, ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
     const size_t smz = sizeof(double2) * ((size_t)ZT_WARPS * 2 * mz + (size_t)ZT_Y * mz * ZT_KX);
     const size_t smzf = sizeof(double2) * ((size_t)ZT_WARPS * 2 * mz + (size_t)ZT_KX * nz * ZT_Y);
     const dim3 gz((nxh + ZT_KX - 1) / ZT_KX, (nyp + ZT_Y - 1) / ZT_Y);
     kmm_tic(ctx);
-#define ZB(MM)                                                                                        \
+#define ZB2(MM, CC)                                                                                   \
     do {                                                                                              \
-        RET(kmm_smem_attr(ctx, (const void *)k_zb<MM>, smz));                                         \
-        k_zb<MM><<<gz, ZT_WARPS * 32, smz, ctx->stream>>>(g_yp, g_q, ctx->d_wavx, ctx->d_wavz, ctx->wmz, nq, nyp, nz, \
-                                                        nxh, mz);                                     \
+        RET(kmm_smem_attr(ctx, (const void *)k_zb2<MM, CC>, smz));                                    \
+        k_zb2<MM, CC><<<gz, ZT_WARPS * 32, smz, ctx->stream>>>((const CC *)g_yp, (CC *)g_q, ctx->d_wavx, \
+                                                             ctx->d_wavz, (const CC *)twz, nq, nyp, nxh); \
     } while (0)
-    switch (mz) {   // specialised lengths: nz = 32, 64, 96, 128
-    case 48: ZB(48); break;
-    case 96: ZB(96); break;
-    case 144: ZB(144); break;
-    case 192: ZB(192); break;
-    default: ZB(0); break;
+    const void *twz = f32 ? (const void *)FU->twf_mz : (const void *)ctx->wmz.tw;
+    if (f32) {
+        switch (mz) {
+        case 48: ZB2(48, float2); break;
+        case 96: ZB2(96, float2); break;
+        case 144: ZB2(144, float2); break;
+        default: ZB2(192, float2); break;
+        }
+    } else {
+        switch (mz) {   // specialised lengths: nz = 32, 64, 96, 128
+        case 48: ZB2(48, double2); break;
+        case 96: ZB2(96, double2); break;
+        case 144: ZB2(144, double2); break;
+        case 192: ZB2(192, double2); break;
+        default:
+            RET(kmm_smem_attr(ctx, (const void *)k_zb<0>, smz));
+            k_zb<0><<<gz, ZT_WARPS * 32, smz, ctx->stream>>>(g_yp, g_q, ctx->d_wavx, ctx->d_wavz, ctx->wmz, nq, nyp, nz,
+                                                           nxh, mz);
+            break;
+        }
     }
-#undef ZB
+#undef ZB2
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_BWD);
     // x transforms + products
     double *up3 = NULL, *vp3 = NULL, *wp3 = NULL;
     if (ctx->p.npart > 0) { up3 = REAL(ctx, KMM_UP3D); vp3 = REAL(ctx, KMM_VP3D); wp3 = REAL(ctx, KMM_WP3D); }
     kmm_tic(ctx);
-    RET(kmm_fast_x(ctx, g_q, g_r, nq, nout, ctx->p.npart > 0, up3, vp3, wp3));
+    {
+        const int xst = kmm_fast_x2(ctx, g_q, g_r, f32 ? (const void *)FU->twf_mx : (const void *)ctx->wmx.tw, f32,
+                                    scalar ? 6 : -1, nout, ctx->p.npart > 0, up3, vp3, wp3);
+        if (xst == KMM_ERR_UNSUPPORTED) RET(kmm_fast_x(ctx, g_q, g_r, scalar ? 6 : -1, nout, ctx->p.npart > 0, up3, vp3, wp3));
+        else RET(xst);
+    }
     kmm_toc(ctx, KMM_STAGE_XPHYS);
     // z forward transforms
     kmm_tic(ctx);
-#define ZF(MM)                                                                                        \
+#define ZF2(MM, CC)                                                                                   \
     do {                                                                                              \
-        RET(kmm_smem_attr(ctx, (const void *)k_zf<MM>, smzf));                                        \
-        k_zf<MM><<<gz, ZT_WARPS * 32, smzf, ctx->stream>>>(g_r, g_yo, ctx->wmz, nout, nyp, nz, nxh, mz,  \
-                                                         (double)ctx->mx * (double)mz);               \
+        RET(kmm_smem_attr(ctx, (const void *)k_zf2<MM, CC>, smzf));                                   \
+        k_zf2<MM, CC><<<gz, ZT_WARPS * 32, smzf, ctx->stream>>>((const CC *)g_r, (CC *)g_yo, (const CC *)twz, \
+                                                              nout, nyp, nxh, (double)ctx->mx * (double)mz); \
     } while (0)
-    switch (mz) {
-    case 48: ZF(48); break;
-    case 96: ZF(96); break;
-    case 144: ZF(144); break;
-    case 192: ZF(192); break;
-    default: ZF(0); break;
+    if (f32) {
+        switch (mz) {
+        case 48: ZF2(48, float2); break;
+        case 96: ZF2(96, float2); break;
+        case 144: ZF2(144, float2); break;
+        default: ZF2(192, float2); break;
+        }
+    } else {
+        switch (mz) {
+        case 48: ZF2(48, double2); break;
+        case 96: ZF2(96, double2); break;
+        case 144: ZF2(144, double2); break;
+        case 192: ZF2(192, double2); break;
+        default:
+            RET(kmm_smem_attr(ctx, (const void *)k_zf<0>, smzf));
+            k_zf<0><<<gz, ZT_WARPS * 32, smzf, ctx->stream>>>(g_r, g_yo, ctx->wmz, nout, nyp, nz, nxh, mz,
+                                                            (double)ctx->mx * (double)mz);
+            break;
+        }
     }
-#undef ZF
+#undef ZF2
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_FWD);
     // back to Chebyshev space, norm, filter, nonlin
@@ -799,7 +1012,8 @@ int kmm_fused_step(kmm_ctx *ctx) {
     B.wavx = ctx->d_wavx; B.wavz = ctx->d_wavz; B.nz = nz; B.nxh = nxh; B.nyp = nyp; B.nzh = ctx->nzh;
     B.scalar = scalar; B.dyde = ctx->dyde;
     kmm_tic(ctx);
-    cst = ctx->use_colblk ? kmm_colblk_bwd(ctx, B, FU->rj) : KMM_ERR_UNSUPPORTED;
+    cst = ctx->use_colblk ? kmm_colblk_bwd(ctx, B, f32 ? (const void *)FU->twf_y2 : (const void *)ctx->wy2.tw, f32)
+                          : KMM_ERR_UNSUPPORTED;
     if (cst != KMM_OK && cst != KMM_ERR_UNSUPPORTED) return cst;
     if (cst == KMM_ERR_UNSUPPORTED) {
 #define COLB(EE, LL)                                                                                  \
@@ -826,16 +1040,25 @@ int kmm_fused_step(kmm_ctx *ctx) {
     CKL();
     }
     kmm_toc(ctx, KMM_STAGE_POST);
-    // tracers (solvers.f90:3463-3476) and the CFL check (3497-3514)
-    int st = KMM_OK;
-    if (ctx->p.npart > 0) {
-        st = kmm_tracers(ctx);
-        if (st != KMM_OK && st != KMM_ERR_INTERP) return st;
-    }
-    double h_cfl[KMM_MAX_NYP], h_um[KMM_MAX_NYP];
+    // tracers (solvers.f90:3463-3476); the CFL maxima and the tracer status go to pinned host
+    // memory for kmm_fused_finish (solvers.f90:3497-3514)
+    RET(kmm_tracers_enqueue(ctx));
+    double *h_cfl = ctx->h_pin, *h_um = ctx->h_pin + KMM_MAX_NYP;
     CK(cudaMemcpyAsync(h_cfl, ctx->d_cfl, sizeof(double) * nyp, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(h_um, ctx->d_umax, sizeof(double) * nyp, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(h_pin_status(ctx), ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    return KMM_OK;
+}
+
+int kmm_fused_finish(kmm_ctx *ctx) {
+    const int nyp = ctx->nyp;
     CK(cudaStreamSynchronize(ctx->stream));
+    const double *h_cfl = ctx->h_pin, *h_um = ctx->h_pin + KMM_MAX_NYP;
+    int st = KMM_OK;
+    if (ctx->p.npart > 0 && *h_pin_status(ctx)) {
+        kmm_set_error(ctx, "particle interpolation cell index out of range (part_track.f90:580-590)");
+        st = KMM_ERR_INTERP;
+    }
     double cflmax = 0.0, umax = 0.0;
     bool nan = false;
     for (int i = 0; i < nyp; ++i) {

@@ -18,6 +18,7 @@ struct KmmFused {
     FusedTabs tabs;
     double2 *yp, *q, *r, *yo;
     double *rj;   // 1/(4j(j-1)), 1/(2(j^2-1)), 1/(4j(j+1)) for j = 0..ny, three rows of nyp
+    float2 *twf_y2, *twf_mz, *twf_mx;   // FP32 twiddles (mixed precision) of lengths 2 ny, mz, mx
 };
 
 static __device__ __forceinline__ TauTab tab_at(const FusedTabs &T, int c, int col, int nyp) {
@@ -51,6 +52,7 @@ struct ColBwdArgs {
 };
 
 // blocked-layout column kernels (kmm_colblk.cu) for ny = 32, 64, 96, 128; KMM_ERR_UNSUPPORTED
-// for other ny
-int kmm_colblk_fwd(kmm_ctx *ctx, const ColFwdArgs &A, const FusedTabs &T, const double *rj);
-int kmm_colblk_bwd(kmm_ctx *ctx, const ColBwdArgs &B, const double *rj);
+// for other ny.  tw: twiddles of length 2 ny in the plane precision (float2 when fp32).
+int kmm_colblk_fwd(kmm_ctx *ctx, const ColFwdArgs &A, const FusedTabs &T, const double *rj, const void *tw,
+                   bool fp32);
+int kmm_colblk_bwd(kmm_ctx *ctx, const ColBwdArgs &B, const void *tw, bool fp32);

@@ -73,6 +73,7 @@ struct kmm_ctx {
     int *d_status;               // device-raised status
     double *d_umax;              // scratch for |u| max (per plane)
     double *d_scratch;           // 9*KMM_MAX_NYP doubles for the (0,0)-mode solver
+    double *h_pin;               // pinned host: cfl[KMM_MAX_NYP], umax[KMM_MAX_NYP], status (fused-step read-back)
     double *scsource;            // (nyp,mz,mx) scalar source (scl_flag = 2)
     DevPlan py2, pmz, pmx, pnx, pnz;
     DevPlan wy2, wmz, wmx;        // same lengths, radix-8-first factorisation for the warp FFT
@@ -97,6 +98,10 @@ struct kmm_ctx {
 
 void kmm_fused_release(kmm_ctx *ctx);
 int kmm_fused_step(kmm_ctx *ctx);
+// the fused step in two halves: enqueue every kernel and the read-back of CFL / status, then wait
+// and evaluate (kmm_fused_step = launch + finish; the ensemble launches all members first)
+int kmm_fused_launch(kmm_ctx *ctx);
+int kmm_fused_finish(kmm_ctx *ctx);
 bool kmm_fused_applicable(const kmm_ctx *ctx);
 void kmm_tic(kmm_ctx *ctx);
 void kmm_toc(kmm_ctx *ctx, int stage);

@@ -463,7 +463,7 @@ int kmm_update_kmaxsurf(kmm_ctx *ctx) {
 // driver
 // ---------------------------------------------------------------------------
 int kmm_tracers(kmm_ctx *ctx);   // kmm_tracer.cu
-int kmm_fast_x(kmm_ctx *ctx, const double2 *q, double2 *r, int nin, int nout, bool save_uvw, double *up3,
+int kmm_fast_x(kmm_ctx *ctx, const double2 *q, double2 *r, int ic, int nout, bool save_uvw, double *up3,
                double *vp3, double *wp3);   // kmm_fast.cu
 
 
@@ -599,7 +599,7 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         // fused warp-per-row x stage (no polymer, no immersed boundary)
         kmm_tic(ctx);
         const bool save = ctx->p.npart > 0 || !ctx->in_step;
-        const int fst = kmm_fast_x(ctx, ctx->q_in, ctx->q_out, nin, nout, save, up3, vp3, wp3);
+        const int fst = kmm_fast_x(ctx, ctx->q_in, ctx->q_out, scal ? A.slot_of_in[S_CX] : -1, nout, save, up3, vp3, wp3);
         if (fst == KMM_OK) fast_done = true;
         else if (fst != KMM_ERR_UNSUPPORTED) return fst;
         kmm_toc(ctx, KMM_STAGE_XPHYS);
@@ -660,4 +660,227 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     if (st == KMM_OK && cflmax > 1.0) st = KMM_ERR_CFL;
     ctx->stats.status = st;
     return st;
+}
+
+// ---------------------------------------------------------------------------
+// calcswirl (helpers.f90:197-404, called at solvers.f90:3421): swirl strength on the 3/2 grid
+// from the nine velocity gradients
+// ---------------------------------------------------------------------------
+// principal powers z^(1/2), z^(1/3) as exp(p log z) = |z|^p e^(i p arg z), with CUDA's sqrt, cbrt,
+// hypot, atan2 and sincos
+__device__ __forceinline__ double2 cpow_half(double2 z) {
+    const double r = hypot(z.x, z.y), th = atan2(z.y, z.x);
+    double s, c;
+    sincos(0.5 * th, &s, &c);
+    const double m = sqrt(r);
+    return make_double2(m * c, m * s);
+}
+__device__ __forceinline__ double2 cpow_third(double2 z) {
+    const double r = hypot(z.x, z.y), th = atan2(z.y, z.x);
+    double s, c;
+    sincos(th / 3.0, &s, &c);
+    const double m = cbrt(r);
+    return make_double2(m * c, m * s);
+}
+
+// eig (helpers.f90:197-275) in Cardano's closed form for real gradients: tr = trace,
+// P = (tr^2 - 3 M2)/9 (M2: sum of principal 2x2 minors), Q = tr^3/27 - tr M2/6 + det/2,
+// S = (Q + (Q^2 - P^3)^(1/2))^(1/3); l1 = tr/3 + P/S + S, l2,3 = tr/3 -+ sqrt(3)(P/S - S) i/2 -
+// P/(2S) - S/2.  P, Q and Q^2 - P^3 are real for real gradients, so only the powers and the
+// divisions by S are complex.  swirl = sqrt(sum Im(l)^2), 0 where not finite and positive.
+__device__ __forceinline__ double swirl_point(double u11, double u12, double u13, double u21, double u22, double u23,
+                                              double u31, double u32, double u33) {
+    const double tr = u11 + u22 + u33;
+    const double P = tr * tr / 9.0 - (u11 * u22) / 3.0 + (u12 * u21) / 3.0 - (u11 * u33) / 3.0 + (u13 * u31) / 3.0 -
+                     (u22 * u33) / 3.0 + (u23 * u32) / 3.0;
+    const double M2 = u11 * u22 - u12 * u21 + u11 * u33 - u13 * u31 + u22 * u33 - u23 * u32;
+    const double Q = tr * tr * tr / 27.0 - (tr * M2) / 6.0 + (u11 * u22 * u33) / 2.0 - (u11 * u23 * u32) / 2.0 -
+                     (u12 * u21 * u33) / 2.0 + (u12 * u23 * u31) / 2.0 + (u13 * u21 * u32) / 2.0 -
+                     (u13 * u22 * u31) / 2.0;
+    const double2 sq = cpow_half(make_double2(Q * Q - P * P * P, 0.0));
+    const double2 S = cpow_third(make_double2(Q + sq.x, sq.y));
+    const double2 PS = cdiv(make_double2(P, 0.0), S);
+    const double2 D = csub(PS, S);
+    // Im of each eigenvalue: l1 = tr/3 + P/S + S; l2,3 = tr/3 -+ (sqrt(3)/2) i D - P/(2S) - S/2
+    const double im1 = PS.y + S.y;
+    const double rot_im = sqrt(3.0) * D.x / 2.0;   // Im(sqrt(3) D i / 2)
+    const double im2 = -rot_im - PS.y / 2.0 - S.y / 2.0;
+    const double im3 = rot_im - PS.y / 2.0 - S.y / 2.0;
+    double sw = sqrt(im1 * im1 + im2 * im2 + im3 * im3);
+    if (!(sw > 0.0 && sw <= 1.7976931348623157e308)) sw = 0.0;
+    return sw;
+}
+
+#define SW_WARPS 4
+// one warp per (y, z) row: Hermitian c2r of the nine gradients (two per complex FFT) into shared
+// rows, then the swirl of every x into SWIRL3D [y][z][x]
+__global__ void __launch_bounds__(SW_WARPS * 32) k_swirl_x(const double2 *__restrict__ q, double *__restrict__ sw,
+                                                           DevPlan P, int nyp, int mz, int mx, int nxh) {
+    extern __shared__ double2 sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y = blockIdx.y, z = blockIdx.x * SW_WARPS + warp;
+    if (z >= mz) return;
+    double2 *a = sm + (size_t)warp * (2 * mx + 5 * mx), *b = a + mx;
+    double *ph = (double *)(b + mx);   // [9][mx]
+    const int hx = mx / 2;
+    for (int f = 0; f < 9; f += 2) {
+        const int g = f + 1;
+        const double2 *qa = q + (((size_t)f * nyp + y) * mz + z) * nxh;
+        const double2 *qb = q + (((size_t)(g < 9 ? g : f) * nyp + y) * mz + z) * nxh;
+        for (int k = lane; k < mx; k += 32) {
+            const int kk = k <= hx ? k : mx - k;
+            double2 Av = make_double2(0.0, 0.0), Bv = make_double2(0.0, 0.0);
+            if (kk < nxh) {
+                Av = qa[kk];
+                if (g < 9) Bv = qb[kk];
+            }
+            if (k == 0 || k == hx) { Av.y = 0.0; Bv.y = 0.0; }
+            a[k] = k <= hx ? make_double2(Av.x - Bv.y, Av.y + Bv.x) : make_double2(Av.x + Bv.y, -Av.y + Bv.x);
+        }
+        __syncwarp();
+        const double2 *res = fft_warp(P, a, b, +1);
+        for (int x = lane; x < mx; x += 32) {
+            const double2 v = res[x];
+            ph[(size_t)f * mx + x] = v.x;
+            if (g < 9) ph[(size_t)g * mx + x] = v.y;
+        }
+        __syncwarp();
+    }
+    for (int x = lane; x < mx; x += 32) {
+#define PH(m) ph[(size_t)(m) * mx + x]
+        sw[((size_t)y * mz + z) * mx + x] = swirl_point(PH(0), PH(1), PH(2), PH(3), PH(4), PH(5), PH(6), PH(7), PH(8));
+#undef PH
+    }
+}
+
+int kmm_swirl_particles(kmm_ctx *ctx);
+
+extern "C" int kmm_calcswirl(kmm_ctx *ctx) {
+    if (!ctx) return KMM_ERR_ARG;
+    const int nyp = ctx->nyp, nz = ctx->nz, nxh = ctx->nxh, mz = ctx->mz, mx = ctx->mx;
+    const int ncols = nz * nxh;
+    FieldPtrs in;
+    for (int m = 0; m < 9; ++m) {
+        in.p[m] = SPEC(ctx, KMM_U11 + m);
+        if (!in.p[m]) return KMM_ERR_NOMEM;
+    }
+    double *sw = REAL(ctx, KMM_SWIRL3D);
+    if (!sw) return KMM_ERR_NOMEM;
+    RET(kmm_ensure_plane_buffers(ctx, 9, 0));
+    const size_t sm_dct = sizeof(double2) * 2 * DCT_CB * 2 * ctx->ny;
+    const size_t sm_z = sizeof(double2) * 2 * ZKB * mz;
+    const size_t sm_s = sizeof(double2) * (size_t)SW_WARPS * 7 * mx;
+    RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd, sm_dct));
+    RET(kmm_smem_attr(ctx, (const void *)k_zfft_bwd, sm_z));
+    RET(kmm_smem_attr(ctx, (const void *)k_swirl_x, sm_s));
+    k_dct_fwd<<<dim3((ncols + DCT_CB - 1) / DCT_CB, 9), 256, sm_dct, ctx->stream>>>(in, ctx->pl_in, ctx->py2, nyp, nz,
+                                                                                      nxh, ncols);
+    CKL();
+    k_zfft_bwd<<<dim3((nxh + ZKB - 1) / ZKB, nyp, 9), 256, sm_z, ctx->stream>>>(ctx->pl_in, ctx->q_in, ctx->pmz, nyp,
+                                                                                 nz, nxh, mz);
+    CKL();
+    k_swirl_x<<<dim3((mz + SW_WARPS - 1) / SW_WARPS, nyp), SW_WARPS * 32, sm_s, ctx->stream>>>(ctx->q_in, sw, ctx->wmx,
+                                                                                            nyp, mz, mx, nxh);
+    CKL();
+    return ctx->p.npart > 0 ? kmm_swirl_particles(ctx) : KMM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// flow statistics of writeoutputs (helpers.f90:1227-1438) by Parseval over the 3/2 grid: the
+// x-z mean of a product of two band-limited fields is the weighted sum of mode products
+// (weight 1 for kx = 0, 2 for kx > 0, the conjugate half); the mean profile is the (0,0) mode.
+// ---------------------------------------------------------------------------
+#define FS_THREADS 256
+// one block per y: PL[f][y][kx][kz] holds y-physical u, v, w, du/dy (f = 0..3) ->
+// acc[y][6] = umean, <u'^2>, <v^2>, <w^2>, <u'v>, <du/dy>
+__global__ void __launch_bounds__(FS_THREADS) k_flowstats(const double2 *__restrict__ pl, double *__restrict__ acc,
+                                                          int nyp, int nz, int nxh) {
+    __shared__ double red[4][FS_THREADS / 32];
+    const int y = blockIdx.x;
+    const size_t fs = (size_t)nyp * nxh * nz;
+    const double2 *pu = pl + (size_t)y * nxh * nz, *pv = pu + fs, *pw = pv + fs;
+    double su = 0.0, sv = 0.0, sw = 0.0, suv = 0.0;
+    for (int e = threadIdx.x; e < nxh * nz; e += FS_THREADS) {
+        const int kx = e / nz;
+        const double wt = kx == 0 ? 1.0 : 2.0;
+        const double2 u = pu[e], v = pv[e], w = pw[e];
+        sv += wt * (v.x * v.x + v.y * v.y);
+        sw += wt * (w.x * w.x + w.y * w.y);
+        if (e != 0) {   // u' = u - umean drops the (0,0) mode
+            su += wt * (u.x * u.x + u.y * u.y);
+            suv += wt * (u.x * v.x + u.y * v.y);
+        }
+    }
+    double vals[4] = {su, sv, sw, suv};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        double x = vals[m];
+        for (int off = 16; off; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+        if (lane == 0) red[m][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double out[4];
+        for (int m = 0; m < 4; ++m) {
+            double x = 0.0;
+            for (int w = 0; w < FS_THREADS / 32; ++w) x += red[m][w];
+            out[m] = x;
+        }
+        acc[(size_t)y * 6 + 0] = pu[0].x;
+        acc[(size_t)y * 6 + 1] = out[0];
+        acc[(size_t)y * 6 + 2] = out[1];
+        acc[(size_t)y * 6 + 3] = out[2];
+        acc[(size_t)y * 6 + 4] = out[3];
+        acc[(size_t)y * 6 + 5] = pl[3 * fs + (size_t)y * nxh * nz].x;
+    }
+}
+
+extern "C" int kmm_flowstats(kmm_ctx *ctx, double *prof, double *scal) {
+    if (!ctx || !prof || !scal) return KMM_ERR_ARG;
+    const int nyp = ctx->nyp, nz = ctx->nz, nxh = ctx->nxh;
+    const int ncols = nz * nxh;
+    RET(kmm_veloc(ctx));
+    double2 *du = ctx->wrk[0];
+    RET(kmm_internal_cderiv(ctx, SPEC(ctx, KMM_U), du));
+    FieldPtrs in;
+    in.p[0] = SPEC(ctx, KMM_U);
+    in.p[1] = SPEC(ctx, KMM_V);
+    in.p[2] = SPEC(ctx, KMM_W);
+    in.p[3] = du;
+    RET(kmm_ensure_plane_buffers(ctx, 4, 0));
+    const size_t sm_dct = sizeof(double2) * 2 * DCT_CB * 2 * ctx->ny;
+    RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd, sm_dct));
+    k_dct_fwd<<<dim3((ncols + DCT_CB - 1) / DCT_CB, 4), 256, sm_dct, ctx->stream>>>(in, ctx->pl_in, ctx->py2, nyp, nz,
+                                                                                      nxh, ncols);
+    CKL();
+    double *acc = ctx->d_scratch;   // 9 KMM_MAX_NYP doubles: 6 nyp used here
+    k_flowstats<<<nyp, FS_THREADS, 0, ctx->stream>>>(ctx->pl_in, acc, nyp, nz, nxh);
+    CKL();
+    double h[6 * KMM_MAX_NYP];
+    CK(cudaMemcpyAsync(h, acc, sizeof(double) * 6 * nyp, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    double *umean = prof, *urms = prof + nyp, *vrms = prof + 2 * nyp, *wrms = prof + 3 * nyp;
+    double *R12 = prof + 4 * nyp, *T12 = prof + 5 * nyp, *ke = prof + 6 * nyp;
+    for (int i = 0; i < nyp; ++i) {
+        const double *a = h + (size_t)i * 6;
+        umean[i] = a[0];
+        urms[i] = sqrt(a[1]);
+        vrms[i] = sqrt(a[2]);
+        wrms[i] = sqrt(a[3]);
+        R12[i] = a[4];
+        T12[i] = a[5] / ctx->re;
+        ke[i] = 0.5 * (a[0] * a[0] + a[1] + a[2] + a[3]);
+    }
+    double mf = 0.0, kb = 0.0;
+    for (int i = 0; i < nyp - 1; ++i) {
+        const double dy = fabs(ctx->h_ycoord[i + 1] - ctx->h_ycoord[i]);
+        mf += 1.0 / ctx->yl * 0.5 * (umean[i + 1] + umean[i]) * dy;
+        kb += 1.0 / ctx->yl * 0.5 * (ke[i + 1] + ke[i]) * dy;
+    }
+    scal[0] = mf;
+    scal[1] = T12[0];
+    scal[2] = T12[nyp - 1];
+    scal[3] = kb;
+    return KMM_OK;
 }

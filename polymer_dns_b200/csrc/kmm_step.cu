@@ -260,6 +260,11 @@ extern "C" int kmm_initial(kmm_ctx *ctx) {
 extern "C" int kmm_step(kmm_ctx *ctx) {
     if (!ctx) return KMM_ERR_ARG;
     if (ctx->use_fused && kmm_fused_applicable(ctx)) return kmm_fused_step(ctx);
+    if (ctx->p.precision == 1) {
+        // the mixed-precision form lives in the fused kernels only; never fall back silently to FP64
+        kmm_set_error(ctx, "mixed precision needs the fused step (no polymer, no immersed boundary, KMM_OPT_FUSED = 1)");
+        return KMM_ERR_UNSUPPORTED;
+    }
     const double re = ctx->re, dt = ctx->dt, th = ctx->theta;
     ctx->it += 1;
     const int it = ctx->it;

@@ -183,6 +183,52 @@ static int tracer_launch(kmm_ctx *ctx, bool init) {
 // called from vcw3dp: init at it == irstrt (part_track.f90:132-134), Euler/RK3 update otherwise
 int kmm_tracers(kmm_ctx *ctx) { return tracer_launch(ctx, ctx->it == ctx->p.irstrt); }
 
+// the same without waiting: the cell-index status stays in d_status for the caller to read back
+int kmm_tracers_enqueue(kmm_ctx *ctx) {
+    if (ctx->p.npart <= 0) return KMM_OK;
+    const bool init = ctx->it == ctx->p.irstrt;
+    TracerArgs T = tracer_args(ctx);
+    double *x = REAL(ctx, KMM_XPART), *y = REAL(ctx, KMM_YPART), *z = REAL(ctx, KMM_ZPART);
+    double *u = REAL(ctx, KMM_UPART), *v = REAL(ctx, KMM_VPART), *w = REAL(ctx, KMM_WPART);
+    double *f1 = REAL(ctx, KMM_UP3D), *f2 = REAL(ctx, KMM_VP3D), *f3 = REAL(ctx, KMM_WP3D);
+    if (!x || !y || !z || !u || !v || !w || !f1 || !f2 || !f3) return KMM_ERR_NOMEM;
+    const int nb = (T.npart + 255) / 256;
+    if (init) k_init_part<<<nb, 256, 0, ctx->stream>>>(T, ctx->d_ycoord, x, y, z, u, v, w, f1, f2, f3, ctx->d_status);
+    else k_tracer_update<<<nb, 256, 0, ctx->stream>>>(T, ctx->d_ycoord, x, y, z, u, v, w, f1, f2, f3, ctx->d_status);
+    CKL();
+    return KMM_OK;
+}
+
+// swirl at each particle (fluid_interp1 on swirl_3d, solvers.f90:3480)
+__global__ void k_swirl_part(TracerArgs T, const double *__restrict__ ycoord, const double *__restrict__ xp,
+                             const double *__restrict__ yp, const double *__restrict__ zp,
+                             const double *__restrict__ sw, double *__restrict__ sp, int *status) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= T.npart) return;
+    double a, b, c;
+    if (fluid_interp(T, ycoord, xp[n], yp[n], zp[n], sw, sw, sw, &a, &b, &c)) {
+        atomicOr(status, 1);
+        return;
+    }
+    sp[n] = a;
+}
+
+int kmm_swirl_particles(kmm_ctx *ctx) {
+    if (ctx->p.npart <= 0) return KMM_OK;
+    TracerArgs T = tracer_args(ctx);
+    double *x = REAL(ctx, KMM_XPART), *y = REAL(ctx, KMM_YPART), *z = REAL(ctx, KMM_ZPART);
+    double *sw = REAL(ctx, KMM_SWIRL3D), *sp = REAL(ctx, KMM_SWIRLPART);
+    if (!x || !y || !z || !sw || !sp) return KMM_ERR_NOMEM;
+    CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+    k_swirl_part<<<(T.npart + 255) / 256, 256, 0, ctx->stream>>>(T, ctx->d_ycoord, x, y, z, sw, sp, ctx->d_status);
+    CKL();
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h) kmm_set_error(ctx, "particle interpolation cell index out of range (part_track.f90:580-590)");
+    return h ? KMM_ERR_INTERP : KMM_OK;
+}
+
 extern "C" int kmm_tracer_update(kmm_ctx *ctx) { return ctx ? tracer_launch(ctx, false) : KMM_ERR_ARG; }
 extern "C" int kmm_init_part(kmm_ctx *ctx) { return ctx ? tracer_launch(ctx, true) : KMM_ERR_ARG; }
 

@@ -23,7 +23,7 @@ _ROUTINES = {
     "veloc": "", "vort": "", "nonlin": "", "vcw3dp": "", "norm": "i", "xyzfft": "ii", "polynl": "",
     "polyforce": "", "subforce": "", "filter": "", "initial": "", "step": "", "run": "i",
     "tracer_update": "", "init_part": "", "copy": "ii", "zero": "i", "set_it": "i", "sync": "",
-    "set_option": "ii",
+    "set_option": "ii", "calcswirl": "",
 }
 _CT = {"i": ctypes.c_int, "d": ctypes.c_double}
 
@@ -67,6 +67,8 @@ def lib():
         L.kmm_event_record.restype = ctypes.c_int
         L.kmm_event_elapsed.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
         L.kmm_event_elapsed.restype = ctypes.c_int
+        L.kmm_flowstats.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        L.kmm_flowstats.restype = ctypes.c_int
         L.kmm_xyzfft_noalloc.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
         L.kmm_xyzfft_noalloc.restype = ctypes.c_int
         for name, sig in _ROUTINES.items():
@@ -81,7 +83,7 @@ def exported_symbols():
     """Names the library must export (every entry point declared in include/kmm.h)."""
     base = ["kmm_ctx_create", "kmm_ctx_destroy", "kmm_last_error", "kmm_abi_version", "kmm_field_size",
             "kmm_upload", "kmm_download", "kmm_get_stats", "kmm_set_timing", "kmm_get_stage_times",
-            "kmm_launch_count", "kmm_event_record", "kmm_event_elapsed", "kmm_xyzfft_noalloc"]
+            "kmm_launch_count", "kmm_event_record", "kmm_event_elapsed", "kmm_xyzfft_noalloc", "kmm_flowstats"]
     return base + ["kmm_" + n for n in _ROUTINES]
 
 
@@ -187,6 +189,15 @@ class KmmContext:
     def download_ptr(self, f, ptr, nbytes):
         fid = self._id(f)
         self._check(self.L.kmm_download(self.h, fid, ctypes.c_void_p(ptr), nbytes), "kmm_download(%s)" % f)
+
+    def flowstats(self):
+        """(prof[7][nyp], scal[4]) of kmm_flowstats: umean, urms, vrms, wrms, R12, T12, ke profiles;
+        bulk velocity, top / bottom wall shear, bulk kinetic energy."""
+        prof = np.zeros((7, self.ny + 1))
+        scal = np.zeros(4)
+        dp = ctypes.POINTER(ctypes.c_double)
+        self._check(self.L.kmm_flowstats(self.h, prof.ctypes.data_as(dp), scal.ctypes.data_as(dp)), "kmm_flowstats")
+        return prof, scal
 
     # mirrors of the reference's main-program blocks
     def initial(self):

@@ -347,3 +347,87 @@ def test_blocked_columns_match_warp_columns(rt, grid):
     for name in ["V", "OMY", "FN", "FNM1", "GN", "GNM1", "U0", "W0", "H1N", "H3N", "SCALAR", "SCN", "SCNM1"]:
         a, b = ctxs[0].download(name), ctxs[1].download(name)
         assert kc.rel_err(a, b) <= 1e-12, name
+
+
+def test_calcswirl_matches_oracle(rt, oracle_mod):
+    """kmm_calcswirl (helpers.f90:197-404) against the oracle on the gradients of a random
+    divergence-free field, with particles.  The reference's closed form is ill-conditioned in two
+    places: near a zero discriminant Q^2 - P^3 the square root turns O(eps) rounding into
+    O(sqrt(eps)) imaginary parts, and for Q < 0 with |P|^3 << Q^2 the sum Q + sqrt(Q^2 - P^3)
+    cancels.  There each implementation returns its own rounding (up to ~1e-6 of the largest
+    swirl; where the eigenvalues are real, a residue near 1e-8 instead of 0).  Bars: of the
+    points with a clear complex pair (swirl > 1e-4 of the largest), at least 99.9% agree to 1e-9
+    of the largest swirl; every point and every particle agrees to 1e-5 of it."""
+    p = kc.cfg_small(24, 32, 16, npart=64)
+    g, o = _pair(rt, oracle_mod, p)
+    fields = kc.initial_fields(p, amp=0.3, seed=5)
+    kc.load_initial(g, p, fields)
+    kc.load_initial(o, p, fields)
+    assert g.initial() == 0 and o.initial() == 0
+    for ctx in (g, o):
+        ctx.call("veloc")
+        ctx.call("gradv")
+    xs = inputs.uniform_particles(p.npart, p.xl, p.yl, p.zl, p.ap, seed=6)
+    for name, arr in zip(("XPART", "YPART", "ZPART"), xs):
+        _put(g, o, name, arr)
+    assert g.call("calcswirl") == 0
+    assert o.call("calcswirl") == 0
+    a, b = g.download("SWIRL3D"), o.get("SWIRL3D")
+    scale = np.abs(b).max()
+    assert scale > 0
+    diff = np.abs(a - b)
+    clear = b > 1e-4 * scale
+    assert clear.mean() > 0.5
+    assert np.mean(diff[clear] > 1e-9 * scale) < 0.001
+    assert diff.max() <= 1e-5 * scale
+    sa, sb = g.download("SWIRLPART"), o.get("SWIRLPART")
+    assert np.abs(sa - sb).max() <= 1e-5 * scale
+
+
+@pytest.mark.parametrize("grid", [(32, 32, 32), (32, 64, 32)])
+def test_mixed_precision_tracks_fp64(rt, grid):
+    """The mixed-precision form (precision = 1: FP32 transforms and products, FP64 solves) against
+    the FP64 drop-in from the same state after 10 steps, with scalar and tracers.  FP32 rounding of
+    the nonlinear terms gives relative field differences of order 1e-7..1e-6; the bar is 1e-5."""
+    kw = dict(scalar_on=1, diff=1.0, scalar_bc=1, scalar_q=0.5, npart=128, tracer_scheme=1)
+    ctxs = []
+    for prec in (0, 1):
+        p = kc.cfg_small(*grid, precision=prec, **kw)
+        fields = kc.initial_fields(p, amp=0.1, seed=7)
+        g = rt.KmmContext(p)
+        kc.load_initial(g, p, fields, np.zeros_like(fields[0]))
+        parts = inputs.uniform_particles(p.npart, p.xl, p.yl, p.zl, p.ap, 3)
+        for name, arr in zip(("XPART", "YPART", "ZPART"), parts):
+            g.upload(name, arr)
+        assert g.initial() == 0
+        ctxs.append(g)
+    for _ in range(10):
+        for g in ctxs:
+            assert g.step() == 0
+    worst = 0.0
+    for name in ["V", "OMY", "FN", "GN", "U0", "W0", "SCALAR", "SCN"]:
+        e = kc.rel_err(ctxs[1].download(name), ctxs[0].download(name))
+        worst = max(worst, e)
+        assert e <= 1e-5, "%s rel err %.3e" % (name, e)
+    assert worst > 1e-12   # the mixed form really runs in FP32
+    for name in ("XPART", "YPART", "ZPART"):
+        assert kc.rel_err(ctxs[1].download(name), ctxs[0].download(name)) <= 1e-6
+
+
+def test_flowstats_matches_oracle(rt, oracle_mod):
+    """kmm_flowstats (Parseval sums over the modes) against the oracle's literal restatement of
+    writeoutputs (3/2-grid loops, helpers.f90:1227-1438) on a perturbed channel with a scalar."""
+    p = kc.cfg_small(24, 32, 16, scalar_on=1, diff=1.0)
+    g, o = _pair(rt, oracle_mod, p)
+    fields = kc.initial_fields(p, profile="loglaw", amp=0.2, seed=8)
+    kc.load_initial(g, p, fields, np.zeros_like(fields[0]))
+    kc.load_initial(o, p, fields, np.zeros_like(fields[0]))
+    assert g.initial() == 0 and o.initial() == 0
+    for _ in range(3):
+        assert g.step() == 0 and o.step() == 0
+    pg, sg = g.flowstats()
+    po, so = o.flowstats()
+    for m in range(7):
+        e = kc.rel_err(pg[m], po[m])
+        assert e <= 1e-10, "profile %d rel err %.3e" % (m, e)
+    assert np.allclose(sg, so, rtol=1e-10, atol=1e-14)

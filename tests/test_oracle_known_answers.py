@@ -318,3 +318,57 @@ def test_tracers_uniform_flow_and_trilinear(oracle_mod):
     assert o.call("tracer_update") == 0
     np.testing.assert_allclose(o.get("XPART"), np.fmod(p.xl + xp + 0.3 * p.dt, p.xl), atol=1e-14)
     np.testing.assert_allclose(o.get("YPART"), yp + 0.05 * yp * p.dt, atol=1e-14)
+
+
+def _swirl_oracle(oracle_mod, grads, p):
+    """Oracle calcswirl on constant velocity gradients u_ij = grads[i][j] (spectral (0,0) mode,
+    Chebyshev coefficient 0: constant in physical space)."""
+    o = oracle_mod.Oracle(p)
+    names = ["U11", "U12", "U13", "U21", "U22", "U23", "U31", "U32", "U33"]
+    for m, name in enumerate(names):
+        a = np.zeros((p.ny + 1, p.nz, p.nx // 2), dtype=np.complex128, order="F")
+        a[0, 0, 0] = grads[m // 3][m % 3]
+        o.set(name, a)
+    assert o.call("calcswirl") == 0
+    return o.get("SWIRL3D")
+
+
+def test_swirl_known_answers(oracle_mod):
+    """Swirl strength (helpers.f90:197-404) on uniform gradients: a solid-body rotation of rate w has
+    eigenvalues 0, +-i w, so swirl = sqrt(2) w; a pure strain has real eigenvalues, swirl ~ 0; a
+    rotation plus an axial strain keeps the complex pair."""
+    p = kc.cfg_small(16, 16, 12)
+    w = 1.7
+    rot = [[0.0, -w, 0.0], [w, 0.0, 0.0], [0.0, 0.0, 0.0]]
+    sw = _swirl_oracle(oracle_mod, rot, p)
+    assert np.allclose(sw, math.sqrt(2.0) * w, rtol=1e-12, atol=0)
+    strain = [[0.3, 0.0, 0.0], [0.0, -0.1, 0.0], [0.0, 0.0, -0.2]]
+    sw = _swirl_oracle(oracle_mod, strain, p)
+    assert np.abs(sw).max() < 1e-14
+    # rotation w about z with strain s on z: eigenvalues s, -s/2 +- i w_eff, w_eff = sqrt(w^2 - s^2/4)... use numpy
+    g = np.array([[-0.25, -w, 0.0], [w, -0.25, 0.0], [0.0, 0.0, 0.5]])
+    sw = _swirl_oracle(oracle_mod, g.tolist(), p)
+    lam = np.linalg.eigvals(g)
+    want = math.sqrt(float(np.sum(lam.imag ** 2)))
+    assert np.allclose(sw, want, rtol=1e-12, atol=0)
+
+
+def test_flowstats_laminar_poiseuille(oracle_mod):
+    """writeoutputs statistics (helpers.f90:1227-1438) on laminar Poiseuille u = 1.5 (1 - y^2)
+    (U_b = 1): mass flux 1 up to the trapezoid error of the Gauss-Lobatto grid, no fluctuations,
+    wall shear -+3/re (du/dy = -3y), kinetic energy 0.5 <u^2> = 0.6 in the bulk."""
+    p = kc.cfg_small(16, 32, 12)
+    o = oracle_mod.Oracle(p)
+    iu, iv, iw = kc.initial_fields(p, amp=0.0)
+    kc.load_initial(o, p, (iu, iv, iw))
+    assert o.initial() == 0
+    prof, scal = o.flowstats()
+    y = np.cos(np.pi * np.arange(p.ny + 1) / p.ny)
+    assert np.allclose(prof[0], 1.5 * (1 - y ** 2), atol=1e-12)
+    assert np.abs(prof[1:5]).max() < 1e-12
+    assert np.allclose(prof[5], -3.0 * y / p.re, atol=1e-12)
+    dy = np.abs(np.diff(y))
+    trap = np.sum(0.5 * (prof[0][1:] + prof[0][:-1]) * dy) / 2.0
+    assert abs(scal[0] - trap) < 1e-14 and abs(scal[0] - 1.0) < 5e-3
+    assert abs(scal[1] + 3.0 / p.re) < 1e-12 and abs(scal[2] - 3.0 / p.re) < 1e-12
+    assert abs(scal[3] - 0.6) < 5e-3
