@@ -158,6 +158,50 @@ def stage_bytes(p, nin, nout):
     }
 
 
+def fused_stage_bytes(p):
+    """Algorithmic bytes per step of each stage of the fused step (each operand read or written
+    once): complex state fields 16 B, intermediates 16 B (FP64) or 8 B (mixed), tracer copies 8 B."""
+    nyp, nz, nxh, mx, mz = p.ny + 1, p.nz, p.nx // 2, 3 * p.nx // 2, 3 * p.nz // 2
+    spec, qn, phys = nyp * nz * nxh, nyp * mz * nxh, nyp * mz * mx
+    cb = 8 if p.precision == 1 else 16
+    sc = 1 if p.scalar_on else 0
+    n_yp, nq, nr = 6 + 2 * sc, 6 + 3 * sc, 3 + sc
+    # column kernels: reads (scalar 3, omega_y 3, v 5, u/w 2), state writes (scalar, omega_y, v), y-physical writes
+    col = ((3 * sc + 3 + 5 + 2) + (sc + 2)) * spec * 16 + n_yp * spec * cb
+    return {
+        "column": col,
+        "zfft_bwd": n_yp * spec * cb + nq * qn * cb,
+        "xphys": (nq + nr) * qn * cb + (3 * phys * 8 if p.npart else 0),
+        "zfft_fwd": nr * (qn + spec) * cb,
+        "post": nr * spec * (cb + 16),
+    }
+
+
+# kernels of each fused stage (ncu names at 128x129x128, FP64)
+STAGE_KERNELS = {
+    "column": ["k_bcol_scl<8,double2>", "k_bcol_omy<8,double2>", "k_bcol_v<8,double2>", "k_bcol_uw<8,double2>"],
+    "zfft_bwd": ["k_zb2<192,double2>"], "xphys": ["k_fx2<192,double2>"], "zfft_fwd": ["k_zf2<192,double2>"],
+    "post": ["k_bcol_bwd<8,double2>"],
+}
+
+
+def profiled_traffic(p, stage):
+    """DRAM bytes per step of a stage's kernels from the committed ncu summary (FP64 128x129x128
+    only), or None when a kernel was not captured."""
+    if not (p.nx == 128 and p.ny == 128 and p.nz == 128 and p.precision == 0):
+        return None
+    try:
+        tab = {}
+        with open(os.path.join(ROOT, "profiles", "kmm_fused_fp64_128x129x128_traffic.txt")) as f:
+            for line in f:
+                if line.strip() and not line.startswith("#"):
+                    k, v = line.split("\t")
+                    tab[k.strip()] = int(v)
+        return sum(tab[k] for k in STAGE_KERNELS[stage])
+    except Exception:
+        return None
+
+
 def fused_model_bytes(p):
     """Fused-minimum bytes per step (field passes x 16 B): velocity 28, scalar +13, polymer +108,
     tracers 264 B/particle, IB 52 B per solid cell."""
@@ -245,21 +289,31 @@ def run_kmm(a, rank, world, local_rank):
     result = None
     if rank == 0:
         peaks, peaks_kind = load_peaks()
-        nin = 6 + (4 if p.scalar_on else 0) + (45 if p.polymer_on else 0)
-        nout = 3 + (1 if p.scalar_on else 0) + (18 if p.polymer_on else 0)
-        sb = stage_bytes(p, nin, nout)
+        fused = stages.get("dct_fwd", (0, 0))[1] == 0   # the fused step records no separate DCT stages
+        if fused:
+            sb = fused_stage_bytes(p)
+        else:
+            nin = 6 + (4 if p.scalar_on else 0) + (45 if p.polymer_on else 0)
+            nout = 3 + (1 if p.scalar_on else 0) + (18 if p.polymer_on else 0)
+            sb = stage_bytes(p, nin, nout)
         vc_stages = {k: v for k, v in stages.items() if k in sb and v[1] > 0}
         dom = max(vc_stages, key=lambda k: vc_stages[k][0]) if vc_stages else None
         total_stage_ms = sum(v[0] for v in stages.values())
         roof = None
+        peak = float(peaks.get("hbm_gbs", 6650.0))
+        per_stage = {}
+        for k, v in vc_stages.items():
+            per_stage[k] = round(sb[k] / (v[0] / v[1] / 1e3) / 1e9 / peak, 4)
         if dom:
             avg_ms = vc_stages[dom][0] / vc_stages[dom][1]
             ach = sb[dom] / (avg_ms / 1e3) / 1e9
-            peak = float(peaks.get("hbm_gbs", 6650.0))
-            roof = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 1), "peak": peak,
+            kern = ", ".join(STAGE_KERNELS[dom]) if fused else dom
+            roof = {"bound": "hbm", "kernel": kern, "stage": dom, "achieved": round(ach, 1), "peak": peak,
                     "peak_kind": peaks_kind, "unit": "GB/s", "frac": round(ach / peak, 4),
                     "avg_launch_ms": round(avg_ms, 4), "algorithmic_bytes_per_launch": sb[dom],
-                    "traffic": None}
+                    "traffic": profiled_traffic(p, dom) if fused else None,
+                    "frac_by_stage": per_stage,
+                    "note": "column stage = 3-4 launches per step, counted together"}
         model = fused_model_bytes(p)
         result = {
             "metric": METRIC, "value": round(value, 3), "unit": "timesteps/s", "n_gpus": world,
@@ -283,6 +337,8 @@ def run_kmm(a, rank, world, local_rank):
         }
         if p.precision == 0 and not a.no_mixed and a.config in ("cfg1", "cfg2"):
             result["mixed"] = mixed_report(a, f, extra, local_rank, ms_per_step)
+        if a.config == "cfg2" and not a.no_ensemble:
+            result["ensemble"] = ensemble_report(a, local_rank)
         if not a.no_cpu_baseline and world == 1:
             result["cpu_baseline"] = cpu_baseline(a.config, a.cpu_steps)
     ctx.close()
@@ -348,6 +404,69 @@ def mixed_report(a, f, extra, local_rank, fp64_ms):
             "rel_err_vs_fp64": errs, "drift_over_1000_steps": drift}
 
 
+ENSEMBLE_GRIDS = [(64, 64, 64)] * 4 + [(96, 96, 96)] * 4 + [(128, 128, 96)] * 4 + [(128, 128, 128)] * 4
+
+
+def ensemble_members(precision):
+    """The 16-member uneven-grid ensemble: 4 each of 64x65x64, 96x97x96, 128x129x96, 128x129x128,
+    Re_tau cycling 120 / 150 / 180, seeds 10..25, each with a scalar and 20,000 RK3 tracers, in the
+    Re_tau = 180 box (Lx = 4 pi, Lz = 4 pi / 3, dt = 0.005, re = 2800)."""
+    from polymer_dns_b200 import abi
+    out = []
+    for m, (nx, ny, nz) in enumerate(ENSEMBLE_GRIDS):
+        p = abi.default_params(nx=nx, ny=ny, nz=nz, dt=0.005, re=2800.0, r_tau=(120.0, 150.0, 180.0)[m % 3],
+                               xl=4 * math.pi, zl=4 * math.pi / 3, scalar_on=1, diff=1.0, scalar_bc=1,
+                               scalar_q=1.0, npart=20000, ap=1e-3, tracer_scheme=1, precision=precision)
+        out.append((p, dict(profile="loglaw", amp=0.1, kmax=8, seed=10 + m)))
+    return out
+
+
+def ensemble_report(a, local_rank):
+    """Ensemble steps/s of the 16 members advanced together (kmm_ensemble_run), FP64 and mixed.
+    Timed with CUDA events on a stream ordered after a device-wide synchronisation (start) and
+    recorded after every member has finished (end), so host launch gaps are included."""
+    import torch
+    from polymer_dns_b200 import runtime, inputs
+    torch.cuda.set_device(local_rank)
+    res = {"members": len(ENSEMBLE_GRIDS), "grids": ["%dx%dx%d" % (g[0], g[1] + 1, g[2]) for g in ENSEMBLE_GRIDS]}
+    member_inputs = []
+    for p, init in ensemble_members(0):
+        f = inputs.channel_initial(p.nx, p.ny, p.nz, p.xl, p.yl, p.zl, p.re, p.r_tau, init["profile"],
+                                   init["amp"], init["kmax"], init["seed"])
+        extra = {"INITSCL": np.zeros_like(f[0])}
+        x, y, z = inputs.uniform_particles(p.npart, p.xl, p.yl, p.zl, p.ap, init["seed"])
+        extra.update(XPART=x, YPART=y, ZPART=z)
+        member_inputs.append((f, extra))
+    for prec in (0, 1):
+        ctxs, model = [], 0
+        for (p, init), (f, extra) in zip(ensemble_members(prec), member_inputs):
+            c = runtime.KmmContext(p, device=local_rank)
+            load(c, f, extra, c.upload)
+            c.initial()
+            ctxs.append(c)
+            model += fused_model_bytes(p)
+        runtime.ensemble_run(ctxs, a.warmup)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = runtime.ensemble_run(ctxs, a.steps)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / a.steps
+        pts = sum(p.nx * (p.ny + 1) * p.nz for p, _ in ensemble_members(prec))
+        peak = float(load_peaks()[0].get("hbm_gbs", 6650.0))
+        res["fp64" if prec == 0 else "mixed"] = {
+            "value": round(1e3 / ms, 3), "unit": "ensemble steps/s", "ms_per_ensemble_step": round(ms, 4),
+            "member_steps_per_s": round(len(ctxs) * 1e3 / ms, 2),
+            "grid_point_steps_per_s": round(pts * 1e3 / ms, 1),
+            "fused_model_bytes_per_ensemble_step": model,
+            "frac_of_hbm": round(model / (ms / 1e3) / 1e9 / peak, 4),
+            "status": "ok" if all(s == 0 for s in st) else "member status %s" % st}
+        for c in ctxs:
+            c.close()
+    return res
+
+
 def cpu_baseline(config, nsteps):
     """The oracle (C restatement of the reference, OpenMP) on the host cores: a bounded sample."""
     from oracle import pyoracle
@@ -391,6 +510,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision speed / error report")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 16-member ensemble measurement")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3

@@ -252,6 +252,18 @@ int  kmm_calcswirl(kmm_ctx *ctx);
  * reference's 3/2-grid means exactly for the dealiased fields.                          */
 int  kmm_flowstats(kmm_ctx *ctx, double *prof, double *scal);
 
+/* ---- ensemble (no counterpart in the reference, whose multi-run driver starts independent
+ * processes, LO_multi_run/setup.py:93-101) ----------------------------------------------
+ * Advance n independent contexts (any grids, any devices) by one step each.  Every member's
+ * step is enqueued on its own stream before any is waited on, so the members overlap on the
+ * GPU; members that need the routine path (polymer, IB) step synchronously.  status[m] receives
+ * each member's kmm_step status; the return value is the first nonzero one (KMM_OK if none).
+ * The members must be distinct contexts; a context must not be used from another host thread
+ * during the call.                                                                          */
+#define KMM_MAX_ENSEMBLE 256
+int  kmm_ensemble_step(kmm_ctx **ctxs, int n, int *status);
+int  kmm_ensemble_run(kmm_ctx **ctxs, int n, int nsteps, int *status);
+
 /* ---- options --------------------------------------------------------------- */
 enum kmm_option {
     KMM_OPT_FUSED = 1,  /* 1 (default): kmm_step runs the fused kernels when the run has no polymer and no

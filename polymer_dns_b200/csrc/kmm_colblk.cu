@@ -38,6 +38,7 @@ __device__ __forceinline__ void bphirhs(BCol<K> &x, const BCol<K> &fn, const BCo
 // the column pair of the calling warp
 struct BPair {
     int kx, q, j, col;
+    int tcol;   // column whose tau tables serve this one: kz and -kz share k^2, so half 1 reads half 0's
     size_t off;
     double kxv, kzv, w2;
     bool mean;
@@ -53,6 +54,7 @@ __device__ __forceinline__ bool bpair(BPair &P, int nz, int nzh, int nxh, const 
     P.kx = pr / npair;
     P.j = h == 0 ? P.q : (P.q == 0 ? nzh : nz - P.q);
     P.col = P.kx * nz + P.j;
+    P.tcol = P.q == 0 ? P.col : P.kx * nz + P.q;   // q = 0 pairs kz = 0 with the Nyquist kz: not shared
     P.off = (size_t)P.col * (16 * K + 1);
     P.kxv = wavx[P.kx];
     P.kzv = wavz[P.j];
@@ -86,7 +88,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_scl(ColFwdArgs 
         bload<K>(n0, A.scnm1 + P.off);
         bphirhs<K>(s, n1, n0, A.re, A.diff, A.dt, A.th, P.w2, A.dyde, FULL);
     }
-    const TauTab ts = tab_at(T, TB_SCL, P.col, NYP);
+    const TauTab ts = tab_at(T, TB_SCL, P.tcol, NYP);
     bsolve_robin<K>(s, ts, zero, zero, P.w2 + T.g[TB_SCL], A.c0, rj, FULL);
     bnorm<K>(s, P.kx, P.j, A.nzh);
     bstore<K>(A.scal + P.off, s);
@@ -117,7 +119,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_omy(ColFwdArgs 
         bload<K>(g0c, A.gnm1 + P.off);
         bphirhs<K>(om, g1c, g0c, A.re, 1.0, A.dt, A.th, P.w2, A.dyde, FULL);
     }
-    const TauTab to = tab_at(T, TB_OMY, P.col, NYP);
+    const TauTab to = tab_at(T, TB_OMY, P.tcol, NYP);
     bsolve_robin<K>(om, to, zero, zero, P.w2 + g1, A.c0, rj, FULL);
     if (P.mean) {
 #pragma unroll
@@ -160,9 +162,9 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_v(ColFwdArgs A,
         bphirhs<K>(v, f1, f0, A.re, 1.0, A.dt, A.th, w2, A.dyde, FULL);
     }
     {
-        const TauTab tp = tab_at(T, TB_PHI, P.col, NYP);
+        const TauTab tp = tab_at(T, TB_PHI, P.tcol, NYP);
         bsolve_dirichlet<K>(v, tp, zero, zero, w2 + g1, A.c0, rj, FULL);
-        const TauTab tv = tab_at(T, TB_V, P.col, NYP);
+        const TauTab tv = tab_at(T, TB_V, P.tcol, NYP);
         bsolve_dirichlet<K>(v, tv, zero, zero, w2, A.c0, rj, FULL);
     }
     // influence matrix

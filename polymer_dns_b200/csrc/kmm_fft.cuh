@@ -180,7 +180,7 @@ struct Dft<C, 8, S> {
 
 // one Stockham stage: butterflies j = 0..N/R-1 of each of the NQ sequences (stored N apart)
 // spread over the 32 lanes
-template <typename C, int N, int F, int S, int NQ, bool SWZ>
+template <typename C, int N, int F, int S, int NQ, bool SWZ, int TWS>
 __device__ __forceinline__ void stage(const C *__restrict__ src, C *__restrict__ dst, const C *__restrict__ tw,
                                       int lane) {
     constexpr int R = fac(N, F);
@@ -202,7 +202,7 @@ __device__ __forceinline__ void stage(const C *__restrict__ src, C *__restrict__
                 const int xi = base + j + r * NR;
                 C x = src[SWZ ? swz<C>(xi) : xi];
                 if (NS > 1 && r > 0 && k) {
-                    C w = __ldg(&tw[r * k * TSTEP]);
+                    C w = __ldg(&tw[r * k * TSTEP * TWS]);
                     if (S > 0) w.y = -w.y;
                     x = mul(x, w);
                 }
@@ -219,18 +219,18 @@ __device__ __forceinline__ void stage(const C *__restrict__ src, C *__restrict__
     }
 }
 
-template <typename C, int N, int F, int S, int NQ, bool SWZ, bool END>
+template <typename C, int N, int F, int S, int NQ, bool SWZ, int TWS, bool END>
 struct Step;
-template <typename C, int N, int F, int S, int NQ, bool SWZ>
-struct Step<C, N, F, S, NQ, SWZ, true> {
+template <typename C, int N, int F, int S, int NQ, bool SWZ, int TWS>
+struct Step<C, N, F, S, NQ, SWZ, TWS, true> {
     static __device__ __forceinline__ C *go(C *src, C *, const C *, int) { return src; }
 };
-template <typename C, int N, int F, int S, int NQ, bool SWZ>
-struct Step<C, N, F, S, NQ, SWZ, false> {
+template <typename C, int N, int F, int S, int NQ, bool SWZ, int TWS>
+struct Step<C, N, F, S, NQ, SWZ, TWS, false> {
     static __device__ __forceinline__ C *go(C *src, C *dst, const C *tw, int lane) {
-        stage<C, N, F, S, NQ, SWZ>(src, dst, tw, lane);
+        stage<C, N, F, S, NQ, SWZ, TWS>(src, dst, tw, lane);
         __syncwarp();
-        return Step<C, N, F + 1, S, NQ, SWZ, (F + 1 >= nfac(N))>::go(dst, src, tw, lane);
+        return Step<C, N, F + 1, S, NQ, SWZ, TWS, (F + 1 >= nfac(N))>::go(dst, src, tw, lane);
     }
 };
 }   // namespace kct
@@ -238,11 +238,12 @@ struct Step<C, N, F, S, NQ, SWZ, false> {
 // S = -1: exp(-2 pi i jk/N) (FFTW_FORWARD), +1: exp(+...) (FFTW_BACKWARD).  NQ sequences of
 // length N lie N apart in a; b is a scratch buffer of the same size (both private to the calling
 // warp); the input must be visible to the whole warp (__syncwarp after writing it).  Returns the
-// buffer holding the result.  SWZ: the buffers are swizzled (element x at swz<C>(x)).
-template <typename C, int N, int S, int NQ = 1, bool SWZ = false>
+// buffer holding the result.  SWZ: the buffers are swizzled (element x at swz<C>(x)).  TWS: the
+// table holds the twiddles of length TWS N (exp(-2 pi i m/N) is entry TWS m).
+template <typename C, int N, int S, int NQ = 1, bool SWZ = false, int TWS = 1>
 __device__ __forceinline__ C *fft_warp_ct(C *a, C *b, const C *tw) {
     static_assert(kct::nfac(N) > 0, "transform length must be 2^a 3^b 5^c");
-    return kct::Step<C, N, 0, S, NQ, SWZ, false>::go(a, b, tw, threadIdx.x & 31);
+    return kct::Step<C, N, 0, S, NQ, SWZ, TWS, false>::go(a, b, tw, threadIdx.x & 31);
 }
 
 // the transform lengths with compiled instances (3/2-rule grids of nx, nz = 32, 64, 96, 128, 384

@@ -390,3 +390,49 @@ extern "C" int kmm_polynl(kmm_ctx *ctx) {
     }
     return kmm_internal_polynl(ctx, nl);
 }
+
+// ---------------------------------------------------------------------------
+// ensemble of independent runs (the reference's multi-run driver launches them as separate
+// processes, LO_multi_run/setup.py:93-101): every member's step is enqueued on its own stream
+// before any member is waited on, so the members' kernels overlap on the GPU
+// ---------------------------------------------------------------------------
+extern "C" int kmm_ensemble_step(kmm_ctx **ctxs, int n, int *status) {
+    if (!ctxs || n <= 0 || n > KMM_MAX_ENSEMBLE || !status) return KMM_ERR_ARG;
+    bool launched[KMM_MAX_ENSEMBLE];
+    for (int m = 0; m < n; ++m) {
+        kmm_ctx *c = ctxs[m];
+        launched[m] = false;
+        if (!c) {
+            status[m] = KMM_ERR_ARG;
+            continue;
+        }
+        if (cudaSetDevice(c->device) != cudaSuccess) {
+            status[m] = KMM_ERR_CUDA;
+            continue;
+        }
+        if (c->use_fused && kmm_fused_applicable(c)) {
+            status[m] = kmm_fused_launch(c);
+            launched[m] = status[m] == KMM_OK;
+        } else {
+            status[m] = kmm_step(c);   // routine path: runs to completion on its own stream
+        }
+    }
+    int first = KMM_OK;
+    for (int m = 0; m < n; ++m) {
+        if (launched[m]) {
+            cudaSetDevice(ctxs[m]->device);
+            status[m] = kmm_fused_finish(ctxs[m]);
+        }
+        if (first == KMM_OK && status[m] != KMM_OK) first = status[m];
+    }
+    return first;
+}
+
+extern "C" int kmm_ensemble_run(kmm_ctx **ctxs, int n, int nsteps, int *status) {
+    if (nsteps < 0) return KMM_ERR_ARG;
+    for (int s = 0; s < nsteps; ++s) {
+        const int st = kmm_ensemble_step(ctxs, n, status);
+        if (st != KMM_OK) return st;
+    }
+    return KMM_OK;
+}

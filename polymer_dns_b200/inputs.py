@@ -30,46 +30,53 @@ def reichardt(yplus, kappa=0.41):
 
 
 def _perturbation(nx, ny, nz, xl, yl, zl, kmax, seed):
-    """Divergence-free no-slip perturbation on the (nyp,nz,nx) physical grid."""
+    """Divergence-free no-slip perturbation on the (nyp,nz,nx) physical grid.
+
+    Each mode is a y-profile times a (z, x) wave, so every component is assembled as one
+    matrix product (profiles: nyp x M) @ (waves: M x nz*nx)."""
     rng = np.random.default_rng(seed)
     y = grid_y(ny, yl) / (yl / 2.0)                      # in [-1, 1]
     x = np.arange(nx) * xl / nx
     z = np.arange(nz) * zl / nz
-    Y, Z, X = np.meshgrid(y, z, x, indexing="ij")       # shapes (nyp, nz, nx)
     a, b = 2 * math.pi / xl, 2 * math.pi / zl
-    u = np.zeros_like(Y)
-    v = np.zeros_like(Y)
-    w = np.zeros_like(Y)
-    E2, dE2 = (1 - Y ** 2) ** 2, -4 * Y * (1 - Y ** 2)   # psi, d psi/dy vanish at the walls
-    E1, dE1 = (1 - Y ** 2), -2 * Y
+    E2, dE2 = (1 - y ** 2) ** 2, -4 * y * (1 - y ** 2)   # psi, d psi/dy vanish at the walls
+    E1 = 1 - y ** 2
+    prof = {"u": [], "v": [], "w": []}
+    wave = {"u": [], "v": [], "w": []}
+
+    def add(comp, py, pw):
+        prof[comp].append(py)
+        wave[comp].append(pw.ravel())
+
     for kx in range(0, kmax + 1):
         for kz in range(-kmax, kmax + 1):
             if kx == 0 and kz <= 0:
                 continue
-            ph = a * kx * X + b * kz * Z
+            ph = b * kz * z[:, None] + a * kx * x[None, :]   # (nz, nx)
             for comp in range(3):
                 amp = rng.standard_normal()
                 phase = rng.uniform(0, 2 * math.pi)
                 c0, c1 = rng.standard_normal(2) * [1.0, 0.5]
-                P = c0 + c1 * Y
+                P = c0 + c1 * y
                 dP = c1
                 cs, sn = np.cos(ph + phase), np.sin(ph + phase)
                 if comp == 0:      # psi1(x,y,z): u = dpsi/dy, v = -dpsi/dx
-                    psi_y = amp * (dE2 * P + E2 * dP) * cs
-                    psi_x = -amp * E2 * P * a * kx * sn
-                    u += psi_y
-                    v -= psi_x
+                    add("u", amp * (dE2 * P + E2 * dP), cs)
+                    add("v", amp * E2 * P * a * kx, sn)
                 elif comp == 1:    # psi2: w = dpsi/dy, v = -dpsi/dz
-                    psi_y = amp * (dE2 * P + E2 * dP) * cs
-                    psi_z = -amp * E2 * P * b * kz * sn
-                    w += psi_y
-                    v -= psi_z
+                    add("w", amp * (dE2 * P + E2 * dP), cs)
+                    add("v", amp * E2 * P * b * kz, sn)
                 else:              # psi3: u = dpsi/dz, w = -dpsi/dx (no v)
-                    psi_z = -amp * E1 * P * b * kz * sn
-                    psi_x = -amp * E1 * P * a * kx * sn
-                    u += psi_z
-                    w -= psi_x
-    return u, v, w
+                    add("u", -amp * E1 * P * b * kz, sn)
+                    add("w", amp * E1 * P * a * kx, sn)
+    out = []
+    for comp in ("u", "v", "w"):
+        if prof[comp]:
+            f = np.stack(prof[comp], axis=1) @ np.stack(wave[comp], axis=0)
+        else:
+            f = np.zeros((ny + 1, nz * nx))
+        out.append(f.reshape(ny + 1, nz, nx))
+    return tuple(out)
 
 
 def channel_initial(nx, ny, nz, xl, yl, zl, re, r_tau, profile="laminar", amp=0.05, kmax=4, seed=0):

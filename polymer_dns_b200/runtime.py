@@ -67,6 +67,10 @@ def lib():
         L.kmm_event_record.restype = ctypes.c_int
         L.kmm_event_elapsed.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
         L.kmm_event_elapsed.restype = ctypes.c_int
+        L.kmm_ensemble_step.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.kmm_ensemble_step.restype = ctypes.c_int
+        L.kmm_ensemble_run.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.kmm_ensemble_run.restype = ctypes.c_int
         L.kmm_flowstats.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
         L.kmm_flowstats.restype = ctypes.c_int
         L.kmm_xyzfft_noalloc.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
@@ -83,7 +87,8 @@ def exported_symbols():
     """Names the library must export (every entry point declared in include/kmm.h)."""
     base = ["kmm_ctx_create", "kmm_ctx_destroy", "kmm_last_error", "kmm_abi_version", "kmm_field_size",
             "kmm_upload", "kmm_download", "kmm_get_stats", "kmm_set_timing", "kmm_get_stage_times",
-            "kmm_launch_count", "kmm_event_record", "kmm_event_elapsed", "kmm_xyzfft_noalloc", "kmm_flowstats"]
+            "kmm_launch_count", "kmm_event_record", "kmm_event_elapsed", "kmm_xyzfft_noalloc", "kmm_flowstats",
+            "kmm_ensemble_step", "kmm_ensemble_run"]
     return base + ["kmm_" + n for n in _ROUTINES]
 
 
@@ -91,6 +96,18 @@ def xyzfft_noalloc(phys_dev_ptr, spec_dev_ptr, nx, ny, nz, stream=None):
     """kmm_xyzfft_noalloc on raw device pointers (no context, no device allocation)."""
     return lib().kmm_xyzfft_noalloc(ctypes.c_void_p(phys_dev_ptr), ctypes.c_void_p(spec_dev_ptr), int(nx), int(ny),
                                     int(nz), ctypes.c_void_p(stream) if stream else None)
+
+
+def ensemble_run(ctxs, nsteps=1):
+    """kmm_ensemble_run over KmmContext objects; returns the per-member status list (raises on
+    argument errors only, as a member's CFL or NaN status is data for the caller)."""
+    n = len(ctxs)
+    arr = (ctypes.c_void_p * n)(*[c.h.value for c in ctxs])
+    st = (ctypes.c_int * n)()
+    rc = lib().kmm_ensemble_run(arr, n, int(nsteps), st)
+    if rc == abi.ERR_ARG:
+        raise KmmError(rc, "kmm_ensemble_run")
+    return list(st)
 
 
 class KmmContext:
