@@ -248,12 +248,9 @@ def run_kmm(a, rank, world, local_rank):
     launches = ctx.launch_count() - launches0
     stages = ctx.stage_times()
     ctx.set_timing(0)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    from polymer_dns_b200 import replicas
+    ms, value = replicas.job_throughput(dist, ms, a.steps, world, "cuda")
     ms_per_step = ms / a.steps
-    value = world * a.steps / (ms / 1e3)
 
     # end-to-end through the C ABI with the restart state on the host (pinned buffers)
     state = ["V", "FN", "FNM1", "OMY", "GN", "GNM1", "U0", "H1N", "H1NM1", "W0", "H3N", "H3NM1"]
@@ -280,11 +277,7 @@ def run_kmm(a, rank, world, local_rank):
     ctx.event_record(3)
     e2e_ms = ctx.event_elapsed(2, 3)
     barrier()
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * e2e_steps / (e2e_ms / 1e3)
+    e2e_ms, e2e_value = replicas.job_throughput(dist, e2e_ms, e2e_steps, world, "cuda")
 
     result = None
     if rank == 0:
