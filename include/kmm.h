@@ -268,9 +268,13 @@ int  kmm_ensemble_run(kmm_ctx **ctxs, int n, int nsteps, int *status);
 enum kmm_option {
     KMM_OPT_FUSED = 1,  /* 1 (default): kmm_step runs the fused kernels when the run has no polymer and no
                            immersed boundary; 0: kmm_step runs the routine-by-routine kernels   */
-    KMM_OPT_COLUMN_BLOCKED = 2  /* 1 (default): the fused step's column kernels hold a column on 16
+    KMM_OPT_COLUMN_BLOCKED = 2, /* 1 (default): the fused step's column kernels hold a column on 16
                            lanes in blocks of ny/16 coefficients (ny = 32, 64, 96, 128);
                            0: one warp per column, coefficient i on lane i mod 32           */
+    KMM_OPT_GRAPH = 3          /* 1 (default): once the tracers are initialised, the fused step is
+                           captured into two CUDA graphs (the history buffers alternate between
+                           two arrangements) and replayed; 0: launched kernel by kernel.  Steps
+                           with stage timing on (kmm_set_timing) always run kernel by kernel. */
 };
 int  kmm_set_option(kmm_ctx *ctx, int option, int value);
 

@@ -117,6 +117,7 @@ extern "C" int kmm_zero(kmm_ctx *ctx, int field) {
 extern "C" int kmm_set_it(kmm_ctx *ctx, int it) {
     if (!ctx) return KMM_ERR_ARG;
     ctx->it = it;
+    kmm_graph_release(ctx);   // the captured steps assume the tracer phase of the current it
     return KMM_OK;
 }
 
@@ -268,6 +269,7 @@ extern "C" int kmm_ctx_create(const kmm_params *p, int device, kmm_ctx **out) {
     c->kmaxsurf = -1;
     c->use_fused = 1;
     c->use_colblk = 1;
+    c->use_graph = 1;
 #define DUP(dst, src, n)                                                        \
     do {                                                                        \
         CK(cudaMalloc(&(dst), sizeof(double) * (size_t)(n)));                   \
@@ -316,6 +318,7 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
         for (int e = 0; e < 2 * KMM_TIMER_RECORDS; ++e) cudaEventDestroy(ctx->tm_ev[e]);
     for (int e = 0; e < 16; ++e)
         if (ctx->user_ev[e]) cudaEventDestroy(ctx->user_ev[e]);
+    kmm_graph_release(ctx);
     kmm_fused_release(ctx);
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
     if (ctx->po) cudaFree(ctx->po);
@@ -379,7 +382,7 @@ extern "C" int kmm_set_timing(kmm_ctx *ctx, int on) {
     }
     ctx->timing_on = on;
     ctx->tm_n = 0;
-    return KMM_OK;
+    return KMM_OK;   // steps run kernel by kernel while timing is on (kmm_fused_enqueue)
 }
 
 extern "C" int kmm_get_stage_times(kmm_ctx *ctx, double *ms, int *count, int nstages) {
@@ -421,6 +424,11 @@ int kmm_smem_attr(kmm_ctx *ctx, const void *func, size_t bytes) {
         kmm_set_error(ctx, "kernel needs %zu bytes of shared memory (> 227 KB)", bytes);
         return KMM_ERR_UNSUPPORTED;
     }
+    // while a step is being captured into a graph the attribute is already set by the uncaptured
+    // step that precedes every capture
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(ctx->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return KMM_OK;
     CK(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     return KMM_OK;
 }
@@ -428,8 +436,9 @@ int kmm_smem_attr(kmm_ctx *ctx, const void *func, size_t bytes) {
 extern "C" int kmm_set_option(kmm_ctx *ctx, int option, int value) {
     if (!ctx) return KMM_ERR_ARG;
     switch (option) {
-    case KMM_OPT_FUSED: ctx->use_fused = value ? 1 : 0; return KMM_OK;
-    case KMM_OPT_COLUMN_BLOCKED: ctx->use_colblk = value ? 1 : 0; return KMM_OK;
+    case KMM_OPT_FUSED: ctx->use_fused = value ? 1 : 0; kmm_graph_release(ctx); return KMM_OK;
+    case KMM_OPT_COLUMN_BLOCKED: ctx->use_colblk = value ? 1 : 0; kmm_graph_release(ctx); return KMM_OK;
+    case KMM_OPT_GRAPH: ctx->use_graph = value ? 1 : 0; kmm_graph_release(ctx); return KMM_OK;
     default: return KMM_ERR_ARG;
     }
 }

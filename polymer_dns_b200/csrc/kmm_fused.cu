@@ -843,8 +843,78 @@ static int *h_pin_status(kmm_ctx *ctx) { return (int *)(ctx->h_pin + 2 * KMM_MAX
 int kmm_tracers_enqueue(kmm_ctx *ctx);
 
 int kmm_fused_step(kmm_ctx *ctx) {
-    RET(kmm_fused_launch(ctx));
+    RET(kmm_fused_enqueue(ctx));
     return kmm_fused_finish(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// CUDA-graph replay of the fused step.  kmm_fused_launch swaps the history buffers (FN/FNM1,
+// GN/GNM1, SCN/SCNM1) on the host after enqueueing a step, so consecutive steps use one of two
+// pointer arrangements; one graph is captured per arrangement.  Capturing runs the host code of
+// a step without executing it on the device, so the step counter is restored after each capture
+// and two captures leave the arrangement where it started.
+// ---------------------------------------------------------------------------
+void kmm_graph_release(kmm_ctx *ctx) {
+    if (!ctx->graph_ready) return;
+    cudaStreamSynchronize(ctx->stream);
+    for (int p = 0; p < 2; ++p)
+        if (ctx->gexec[p]) cudaGraphExecDestroy(ctx->gexec[p]);
+    ctx->gexec[0] = ctx->gexec[1] = NULL;
+    ctx->graph_ready = 0;
+}
+
+static void swap_history(kmm_ctx *ctx) {
+    void *t;
+    t = ctx->f[KMM_FN]; ctx->f[KMM_FN] = ctx->f[KMM_FNM1]; ctx->f[KMM_FNM1] = t;
+    t = ctx->f[KMM_GN]; ctx->f[KMM_GN] = ctx->f[KMM_GNM1]; ctx->f[KMM_GNM1] = t;
+    if (ctx->p.scalar_on) { t = ctx->f[KMM_SCN]; ctx->f[KMM_SCN] = ctx->f[KMM_SCNM1]; ctx->f[KMM_SCNM1] = t; }
+}
+
+static int capture_graphs(kmm_ctx *ctx) {
+    static const int hist[6] = {KMM_FN, KMM_FNM1, KMM_GN, KMM_GNM1, KMM_SCN, KMM_SCNM1};
+    void *saved[6];
+    for (int h = 0; h < 6; ++h) saved[h] = ctx->f[hist[h]];
+    const int it0 = ctx->it;
+    ctx->g_fn0 = ctx->f[KMM_FN];
+    for (int p = 0; p < 2; ++p) {
+        cudaGraph_t g = NULL;
+        cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        int st = KMM_OK;
+        const long long l0 = ctx->launches;
+        if (e == cudaSuccess) {
+            st = kmm_fused_launch(ctx);
+            e = cudaStreamEndCapture(ctx->stream, &g);
+        }
+        ctx->gkernels[p] = ctx->launches - l0;
+        ctx->launches = l0;
+        if (e == cudaSuccess && st == KMM_OK) e = cudaGraphInstantiate(&ctx->gexec[p], g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess || st != KMM_OK) {
+            for (int h = 0; h < 6; ++h) ctx->f[hist[h]] = saved[h];
+            ctx->it = it0;
+            for (int q = 0; q < 2; ++q)
+                if (ctx->gexec[q]) { cudaGraphExecDestroy(ctx->gexec[q]); ctx->gexec[q] = NULL; }
+            cudaGetLastError();
+            kmm_set_error(ctx, "graph capture of the fused step failed (%s)", cudaGetErrorString(e));
+            return st != KMM_OK ? st : KMM_ERR_CUDA;
+        }
+    }
+    ctx->it = it0;          // captured, not executed
+    ctx->graph_ready = 1;   // the two captured swaps restored arrangement 0
+    return KMM_OK;
+}
+
+int kmm_fused_enqueue(kmm_ctx *ctx) {
+    // graphs only after the step that initialises the tracers (it == irstrt) and the tau tables
+    const bool graphable = ctx->use_graph && !ctx->timing_on && ctx->fused != NULL && ctx->it >= ctx->p.irstrt;
+    if (!graphable) return kmm_fused_launch(ctx);
+    if (!ctx->graph_ready) RET(capture_graphs(ctx));
+    const int parity = ctx->f[KMM_FN] == ctx->g_fn0 ? 0 : 1;
+    CK(cudaGraphLaunch(ctx->gexec[parity], ctx->stream));
+    ctx->launches += ctx->gkernels[parity];
+    swap_history(ctx);
+    ctx->it += 1;
+    return KMM_OK;
 }
 
 int kmm_fused_launch(kmm_ctx *ctx) {

@@ -94,6 +94,11 @@ struct kmm_ctx {
     size_t po_n, drag_n;
     int use_fused;
     int use_colblk;   // fused step: blocked-layout column kernels where compiled (default 1)
+    // fused step replayed from CUDA graphs (one per parity of the swapped history buffers)
+    int use_graph, graph_ready;
+    cudaGraphExec_t gexec[2];
+    long long gkernels[2];   // kernels in each graph (added to the launch count per replay)
+    void *g_fn0;      // the FN buffer of parity 0
 };
 
 void kmm_fused_release(kmm_ctx *ctx);
@@ -102,6 +107,10 @@ int kmm_fused_step(kmm_ctx *ctx);
 // and evaluate (kmm_fused_step = launch + finish; the ensemble launches all members first)
 int kmm_fused_launch(kmm_ctx *ctx);
 int kmm_fused_finish(kmm_ctx *ctx);
+// one fused step enqueued on ctx->stream: through the captured graphs when enabled and ready
+// (captured on first use), else kernel by kernel
+int kmm_fused_enqueue(kmm_ctx *ctx);
+void kmm_graph_release(kmm_ctx *ctx);
 bool kmm_fused_applicable(const kmm_ctx *ctx);
 void kmm_tic(kmm_ctx *ctx);
 void kmm_toc(kmm_ctx *ctx, int stage);

@@ -180,6 +180,7 @@ static double2 *poly_scratch(kmm_ctx *ctx, int m) {
 // ---------------------------------------------------------------------------
 extern "C" int kmm_initial(kmm_ctx *ctx) {
     if (!ctx) return KMM_ERR_ARG;
+    kmm_graph_release(ctx);
     const size_t n = ctx->nspec;
     RET(kmm_gfcn(ctx));
     ctx->it = 0;
@@ -411,7 +412,7 @@ extern "C" int kmm_ensemble_step(kmm_ctx **ctxs, int n, int *status) {
             continue;
         }
         if (c->use_fused && kmm_fused_applicable(c)) {
-            status[m] = kmm_fused_launch(c);
+            status[m] = kmm_fused_enqueue(c);
             launched[m] = status[m] == KMM_OK;
         } else {
             status[m] = kmm_step(c);   // routine path: runs to completion on its own stream
