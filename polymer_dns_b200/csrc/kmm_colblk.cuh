@@ -421,31 +421,124 @@ __device__ __forceinline__ void bunstash(BCol<K> &x, const double2 *buf) {
     x.v[K] = buf[swz<double2>(h * 32 * K + 16 * K)];
 }
 
+// ---- DCT-I by a two-pass FFT with the data in registers -------------------------------------
+// The DCT-I of a column (nyp = NY + 1 values) is the DFT of its even extension of length
+// N = 2 NY = 16 M.  With n = 16 n1 + n2 and k = k1 + M k2:
+//   X[k1 + M k2] = sum_n2 W16^(n2 k2) W_N^(n2 k1) sum_n1 x[16 n1 + n2] W_M^(n1 k1)
+// Pass 1: lane n2 of the column's 16 lanes holds x[16 n1 + n2] (n1 < M), takes the M-point DFT
+// in registers and applies the twiddle W_N^(n2 k1); one shared-memory transpose; pass 2: lane
+// k1 < M takes the 16-point DFT over n2 in registers and holds X[k1 + M k2].  Two shared-memory
+// round trips per transform instead of one per Stockham stage.
+
+// in-register DFT of M points, X_k = sum_j v_j exp(-2 pi i j k / M), natural order in and out;
+// W_M^j is entry `step` j of the twiddle table tw
+template <typename C, int M>
+struct RegDft;
+template <typename C>
+struct RegDft<C, 4> {
+    static __device__ __forceinline__ void run(C *v, const C *, int) { kct::Dft<C, 4, -1>::run(v); }
+};
+template <typename C>
+struct RegDft<C, 8> {
+    static __device__ __forceinline__ void run(C *v, const C *, int) { kct::Dft<C, 8, -1>::run(v); }
+};
+// M = 4 R (R = 3, 4): j = R a + b, k = c + 4 d;  X[c + 4 d] = sum_b W_M^(bc) W_R^(bd) sum_a v[R a + b] W_4^(ac)
+template <typename C, int R>
+__device__ __forceinline__ void regdft_4r(C *v, const C *__restrict__ tw, int step) {
+    constexpr int M = 4 * R;
+    C A[R][4];
+#pragma unroll
+    for (int b = 0; b < R; ++b) {
+        C u[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) u[a] = v[R * a + b];
+        kct::Dft<C, 4, -1>::run(u);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) A[b][c] = (b * c) ? kct::mul(u[c], __ldg(tw + step * ((b * c) % M))) : u[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        C u[R];
+#pragma unroll
+        for (int b = 0; b < R; ++b) u[b] = A[b][c];
+        kct::Dft<C, R, -1>::run(u);
+#pragma unroll
+        for (int d = 0; d < R; ++d) v[c + 4 * d] = u[d];
+    }
+}
+template <typename C>
+struct RegDft<C, 12> {
+    static __device__ __forceinline__ void run(C *v, const C *tw, int step) { regdft_4r<C, 3>(v, tw, step); }
+};
+template <typename C>
+struct RegDft<C, 16> {
+    static __device__ __forceinline__ void run(C *v, const C *tw, int step) { regdft_4r<C, 4>(v, tw, step); }
+};
+
+// The two passes on the warp's two columns.  In: xin[n1] = x[16 n1 + n2] on lane (h, n2).  Out, on
+// lane (h, k1 < M): xout[k2] = X[k1 + M k2] for k2 <= 8 (the indices up to N/2 = NY).  tw: the
+// N-point twiddles exp(-2 pi i m/N); s: the warp's shared buffer (2 N elements).
+template <int K, typename C>
+__device__ __forceinline__ void bdct_passes(const C (&xin)[2 * K], C (&xout)[9], C *s, const C *__restrict__ tw) {
+    constexpr int M = 2 * K, N = 16 * M;
+    const int t = bl_t(), h = (threadIdx.x >> 4) & 1;
+    C v[M];
+#pragma unroll
+    for (int n1 = 0; n1 < M; ++n1) v[n1] = xin[n1];
+    RegDft<C, M>::run(v, tw, 16);   // W_M^j = W_N^(16 j)
+    // twiddle W_N^(n2 k1); transpose through s[h N + 16 k1 + n2]
+#pragma unroll
+    for (int k1 = 0; k1 < M; ++k1) {
+        const C w = (t * k1) ? kct::mul(v[k1], __ldg(tw + t * k1)) : v[k1];
+        s[swz<C>(h * N + 16 * k1 + t)] = w;
+    }
+    __syncwarp();
+    if (t < M) {
+        C u[16];
+#pragma unroll
+        for (int n2 = 0; n2 < 16; ++n2) u[n2] = s[swz<C>(h * N + 16 * t + n2)];
+        RegDft<C, 16>::run(u, tw, M);   // W_16^j = W_N^(M j)
+#pragma unroll
+        for (int k2 = 0; k2 <= 8; ++k2) xout[k2] = u[k2];
+    }
+    __syncwarp();
+}
+
 // y-physical values of the warp's two columns (DCT-I of c(i)/2-scaled coefficients,
 // solvers.f90:2241-2546) written to dst in precision C: the coefficients are rounded to C
-// before the transform, which then runs in C (the specialised FFT of length 2 NY).
+// before the transform, which then runs in C.
 template <int K, typename C>
 __device__ __forceinline__ void bdct_store(const BCol<K> &x, C *a, C *b, const C *tw, C *__restrict__ dst) {
     typedef typename kct::Real<C>::T T;
-    constexpr int NY = 16 * K, L = 2 * NY;
+    constexpr int NY = 16 * K, N = 2 * NY, M = 2 * K;
     const int t = bl_t(), h = (threadIdx.x >> 4) & 1;
-    const int base = h * L;
+    const int base = h * (NY + 8);
+    // the scaled column into shared memory in natural order; each lane then gathers its
+    // stride-16 subsequence of the even extension
 #pragma unroll
     for (int m = 0; m <= K; ++m) {
         if (m == K && t != 15) continue;
         const int i = bidx<K>(m);
         double2 v = x.v[m];
         if (i > 0 && i < NY) v = make_double2(v.x * 0.5, v.y * 0.5);
-        const C c = kct::mk<C>((T)v.x, (T)v.y);
-        a[swz<C>(base + i)] = c;
-        if (i > 0 && i < NY) a[swz<C>(base + L - i)] = c;
+        a[swz<C>(base + i)] = kct::mk<C>((T)v.x, (T)v.y);
     }
     __syncwarp();
-    const C *r = fft_warp_ct<C, L, -1, 2, true>(a, b, tw);
+    C xin[M], xout[9];
 #pragma unroll
-    for (int m = 0; m < K; ++m) dst[t * K + m] = r[swz<C>(base + t * K + m)];
-    if (t == 15) dst[NY] = r[swz<C>(base + NY)];
+    for (int n1 = 0; n1 < M; ++n1) {
+        const int n = 16 * n1 + t;
+        xin[n1] = a[swz<C>(base + (n <= NY ? n : N - n))];
+    }
     __syncwarp();
+    bdct_passes<K, C>(xin, xout, b, tw);
+    if (t < M) {
+#pragma unroll
+        for (int k2 = 0; k2 <= 8; ++k2) {
+            const int k = t + M * k2;
+            if (k <= NY) dst[k] = xout[k2];
+        }
+    }
 }
 
 // Chebyshev coefficients of the warp's two columns from y-physical values in precision C
@@ -453,23 +546,29 @@ __device__ __forceinline__ void bdct_store(const BCol<K> &x, C *a, C *b, const C
 // result is widened to FP64.
 template <int K, typename C>
 __device__ __forceinline__ void bload_dct(BCol<K> &x, const C *__restrict__ src, C *a, C *b, const C *tw) {
-    constexpr int NY = 16 * K, L = 2 * NY;
+    constexpr int NY = 16 * K, N = 2 * NY, M = 2 * K;
     const int t = bl_t(), h = (threadIdx.x >> 4) & 1;
-    const int base = h * L;
+    const int base = h * (NY + 8);
+    C xin[M], xout[9];
 #pragma unroll
-    for (int m = 0; m <= K; ++m) {
-        if (m == K && t != 15) continue;
-        const int i = bidx<K>(m);
-        const C c = src[i];
-        a[swz<C>(base + i)] = c;
-        if (i > 0 && i < NY) a[swz<C>(base + L - i)] = c;
+    for (int n1 = 0; n1 < M; ++n1) {
+        const int n = 16 * n1 + t;
+        xin[n1] = src[n <= NY ? n : N - n];
+    }
+    bdct_passes<K, C>(xin, xout, b, tw);
+    // X[k1 + M k2] on lane k1 -> the blocked layout through shared memory
+    if (t < M) {
+#pragma unroll
+        for (int k2 = 0; k2 <= 8; ++k2) {
+            const int k = t + M * k2;
+            if (k <= NY) a[swz<C>(base + k)] = xout[k2];
+        }
     }
     __syncwarp();
-    const C *r = fft_warp_ct<C, L, -1, 2, true>(a, b, tw);
 #pragma unroll
     for (int m = 0; m <= K; ++m) {
         const int i = bidx<K>(m);
-        const C c = r[swz<C>(base + i)];
+        const C c = a[swz<C>(base + i)];
         double2 v = make_double2((double)c.x / (double)NY, (double)c.y / (double)NY);
         if (i == 0 || i == NY) v = make_double2(v.x / 2.0, v.y / 2.0);
         x.v[m] = v;
