@@ -430,51 +430,6 @@ __device__ __forceinline__ void bunstash(BCol<K> &x, const double2 *buf) {
 // k1 < M takes the 16-point DFT over n2 in registers and holds X[k1 + M k2].  Two shared-memory
 // round trips per transform instead of one per Stockham stage.
 
-// in-register DFT of M points, X_k = sum_j v_j exp(-2 pi i j k / M), natural order in and out;
-// W_M^j is entry `step` j of the twiddle table tw
-template <typename C, int M>
-struct RegDft;
-template <typename C>
-struct RegDft<C, 4> {
-    static __device__ __forceinline__ void run(C *v, const C *, int) { kct::Dft<C, 4, -1>::run(v); }
-};
-template <typename C>
-struct RegDft<C, 8> {
-    static __device__ __forceinline__ void run(C *v, const C *, int) { kct::Dft<C, 8, -1>::run(v); }
-};
-// M = 4 R (R = 3, 4): j = R a + b, k = c + 4 d;  X[c + 4 d] = sum_b W_M^(bc) W_R^(bd) sum_a v[R a + b] W_4^(ac)
-template <typename C, int R>
-__device__ __forceinline__ void regdft_4r(C *v, const C *__restrict__ tw, int step) {
-    constexpr int M = 4 * R;
-    C A[R][4];
-#pragma unroll
-    for (int b = 0; b < R; ++b) {
-        C u[4];
-#pragma unroll
-        for (int a = 0; a < 4; ++a) u[a] = v[R * a + b];
-        kct::Dft<C, 4, -1>::run(u);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) A[b][c] = (b * c) ? kct::mul(u[c], __ldg(tw + step * ((b * c) % M))) : u[c];
-    }
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        C u[R];
-#pragma unroll
-        for (int b = 0; b < R; ++b) u[b] = A[b][c];
-        kct::Dft<C, R, -1>::run(u);
-#pragma unroll
-        for (int d = 0; d < R; ++d) v[c + 4 * d] = u[d];
-    }
-}
-template <typename C>
-struct RegDft<C, 12> {
-    static __device__ __forceinline__ void run(C *v, const C *tw, int step) { regdft_4r<C, 3>(v, tw, step); }
-};
-template <typename C>
-struct RegDft<C, 16> {
-    static __device__ __forceinline__ void run(C *v, const C *tw, int step) { regdft_4r<C, 4>(v, tw, step); }
-};
-
 // The two passes on the warp's two columns.  In: xin[n1] = x[16 n1 + n2] on lane (h, n2).  Out, on
 // lane (h, k1 < M): xout[k2] = X[k1 + M k2] for k2 <= 8 (the indices up to N/2 = NY).  tw: the
 // N-point twiddles exp(-2 pi i m/N); s: the warp's shared buffer (2 N elements).

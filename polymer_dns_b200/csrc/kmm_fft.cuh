@@ -249,3 +249,64 @@ __device__ __forceinline__ C *fft_warp_ct(C *a, C *b, const C *tw) {
 // the transform lengths with compiled instances (3/2-rule grids of nx, nz = 32, 64, 96, 128, 384
 // and the Chebyshev extensions 2 ny = 64, 128, 192, 256, 512)
 #define KMM_CT_LEN_LIST(X) X(48) X(64) X(96) X(128) X(144) X(192) X(256) X(512) X(576)
+
+// ---------------------------------------------------------------------------
+// In-register DFTs of small lengths (two-pass transforms): X_k = sum_j v_j exp(-2 pi i j k / M),
+// natural order in and out.  Lengths that are not a single radix split as M = A B with
+// j = B a + b, k = c + A d:  X[c + A d] = sum_b W_M^(bc) W_B^(bd) sum_a v[B a + b] W_A^(ac);
+// W_M^j is entry `step` j of the twiddle table tw (a table of length step M).
+// ---------------------------------------------------------------------------
+template <typename C, int A, int B>
+__device__ __forceinline__ void regdft_ab(C *v, const C *__restrict__ tw, int step) {
+    constexpr int M = A * B;
+    C Q[B][A];
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+        C u[A];
+#pragma unroll
+        for (int a = 0; a < A; ++a) u[a] = v[B * a + b];
+        kct::Dft<C, A, -1>::run(u);
+#pragma unroll
+        for (int c = 0; c < A; ++c) Q[b][c] = (b * c) ? kct::mul(u[c], __ldg(tw + step * ((b * c) % M))) : u[c];
+    }
+#pragma unroll
+    for (int c = 0; c < A; ++c) {
+        C u[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b) u[b] = Q[b][c];
+        kct::Dft<C, B, -1>::run(u);
+#pragma unroll
+        for (int d = 0; d < B; ++d) v[c + A * d] = u[d];
+    }
+}
+
+template <typename C, int M>
+struct RegDft;
+template <typename C>
+struct RegDft<C, 3> {
+    static __device__ __forceinline__ void run(C *v, const C *, int) { kct::Dft<C, 3, -1>::run(v); }
+};
+template <typename C>
+struct RegDft<C, 4> {
+    static __device__ __forceinline__ void run(C *v, const C *, int) { kct::Dft<C, 4, -1>::run(v); }
+};
+template <typename C>
+struct RegDft<C, 8> {
+    static __device__ __forceinline__ void run(C *v, const C *, int) { kct::Dft<C, 8, -1>::run(v); }
+};
+template <typename C>
+struct RegDft<C, 6> {
+    static __device__ __forceinline__ void run(C *v, const C *tw, int step) { regdft_ab<C, 2, 3>(v, tw, step); }
+};
+template <typename C>
+struct RegDft<C, 9> {
+    static __device__ __forceinline__ void run(C *v, const C *tw, int step) { regdft_ab<C, 3, 3>(v, tw, step); }
+};
+template <typename C>
+struct RegDft<C, 12> {
+    static __device__ __forceinline__ void run(C *v, const C *tw, int step) { regdft_ab<C, 4, 3>(v, tw, step); }
+};
+template <typename C>
+struct RegDft<C, 16> {
+    static __device__ __forceinline__ void run(C *v, const C *tw, int step) { regdft_ab<C, 4, 4>(v, tw, step); }
+};

@@ -299,7 +299,7 @@ def test_full_size_properties():
 
 
 @pytest.mark.parametrize("grid,scalar", [((32, 32, 32), 0), ((24, 32, 16), 1), ((16, 64, 12), 1), ((16, 96, 12), 0),
-                                         ((16, 128, 16), 1)])
+                                         ((16, 128, 16), 1), ((16, 32, 64), 1), ((16, 32, 96), 0), ((16, 32, 128), 1)])
 def test_fused_step_matches_routine_path(rt, oracle_mod, grid, scalar):
     """kmm_step's fused kernels against the routine-by-routine kernels and the oracle after 5 steps."""
     kw = dict(scalar_on=scalar, diff=1.0, scalar_bc=1, scalar_q=0.5) if scalar else {}
@@ -384,7 +384,7 @@ def test_calcswirl_matches_oracle(rt, oracle_mod):
     assert np.abs(sa - sb).max() <= 1e-5 * scale
 
 
-@pytest.mark.parametrize("grid", [(32, 32, 32), (32, 64, 32)])
+@pytest.mark.parametrize("grid", [(32, 32, 32), (32, 64, 32), (32, 32, 96)])
 def test_mixed_precision_tracks_fp64(rt, grid):
     """The mixed-precision form (precision = 1: FP32 transforms and products, FP64 solves) against
     the FP64 drop-in from the same state after 10 steps, with scalar and tracers.  FP32 rounding of
