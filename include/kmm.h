@@ -226,7 +226,11 @@ int  kmm_subforce(kmm_ctx *ctx);
 /* ---- main-program blocks (main_dns.f90) --------------------------------- */
 /* spectral smoothing of the nonlinear terms, main_dns.f90:710-745 */
 int  kmm_filter(kmm_ctx *ctx);
-/* initial(...) with irstrt = 0, main_dns.f90:1602-2231 (initial fields from KMM_INITU/V/W) */
+/* initial(...), main_dns.f90:1602-2231.  irstrt = 0: initial fields from KMM_INITU/V/W (and
+ * KMM_INITSCL).  irstrt >= 1: the host has uploaded the records of setup/restart (KMM_V, KMM_FN,
+ * KMM_FNM1, KMM_OMY, KMM_GN, KMM_GNM1, KMM_U0, KMM_H1N, KMM_H1NM1, KMM_W0, KMM_H3N, KMM_H3NM1;
+ * KMM_FXINTG/FYINTG/FZINTG) -- and of setup/c-restart with scalar + polymer and crstrt = 1 --
+ * which are used as they are (main_dns.f90:1742-1917); the step counter restarts at 0. */
 int  kmm_initial(kmm_ctx *ctx);
 /* one iteration of the time loop body, main_dns.f90:198-811, fused */
 int  kmm_step(kmm_ctx *ctx);

@@ -1898,6 +1898,38 @@ static void poly_set_constant(orc_ctx *c)
 }
 
 /* gfcn + denominator (main_dns.f90:151-161), then initial(...), main_dns.f90:1602-2231, irstrt = 0 branch */
+/* `initial` with irstrt >= 1 (main_dns.f90:1742-1917).  The host has already placed the two
+ * records of setup/restart (v, fn, fnm1, omy, gn, gnm1, u0, h1n, h1nm1, w0, h3n, h3nm1;
+ * fxintg, fyintg, fzintg) and, with the scalar and polymer modules and crstrt = 1, the five
+ * records of setup/c-restart.  None of those is normalised or recomputed; only the scalar and
+ * polymer start values are set as the reference sets them:
+ *   scalar only      : scalar and csource from setscl, NOT normalised (main_dns.f90:1810-1815)
+ *   scalar + polymer : crstrt = 0: setpoly, the scalar gradient and the conformation-tensor
+ *                      derivatives (normalised), and zero scn, cIJn, strIJn, qpIJ
+ *                      (main_dns.f90:1817-1908); crstrt = 1: all from c-restart (1909-1916).
+ * csource is zero at the start of the reference program and the crstrt = 1 branch leaves it so. */
+static int orc_initial_restart(orc_ctx *c)
+{
+    if (!c->p.scalar_on) return 0;
+    orc_zero(c, KMM_CSOURCE);
+    if (c->p.polymer_on && c->p.crstrt != 0) return 0;   /* everything from c-restart */
+    orc_xyzfft(c, KMM_SCALAR, KMM_INITSCL);
+    if (!c->p.polymer_on) return 0;
+    poly_set_constant(c);
+    orc_gradscl(c);
+    { int l[3] = {KMM_SCLX, KMM_SCLY, KMM_SCLZ}; norm_list(c, l, 3); }
+    orc_derivscji(c);
+    poly_norm_c(c);
+    poly_norm_dc(c);
+    orc_zero(c, KMM_SCN);
+    for (int m = 0; m < 6; ++m) {
+        orc_zero(c, KMM_C11N + m);
+        orc_zero(c, KMM_STR11N + m);
+        orc_zero(c, KMM_QP11 + m);
+    }
+    return 0;
+}
+
 int orc_initial(orc_ctx *c)
 {
     const int nyp = c->nyp;
@@ -1905,6 +1937,7 @@ int orc_initial(orc_ctx *c)
     /* setup part of the main program: Green's functions before initial, main_dns.f90:151-161 */
     orc_gfcn(c);
     c->it = 0;
+    if (c->p.irstrt >= 1) return orc_initial_restart(c);
     orc_xyzfft(c, KMM_U, KMM_INITU);
     orc_xyzfft(c, KMM_V, KMM_INITV);
     orc_xyzfft(c, KMM_W, KMM_INITW);

@@ -176,7 +176,39 @@ static double2 *poly_scratch(kmm_ctx *ctx, int m) {
 }
 
 // ---------------------------------------------------------------------------
-// initial (irstrt = 0), after the setup's gfcn (main_dns.f90:151-161, 1602-2231)
+// initial with irstrt >= 1 (main_dns.f90:1742-1917).  The host has uploaded the two records of
+// setup/restart (v, fn, fnm1, omy, gn, gnm1, u0, h1n, h1nm1, w0, h3n, h3nm1; fxintg, fyintg,
+// fzintg) and, with scalar + polymer and crstrt = 1, the five records of setup/c-restart; none of
+// them is normalised or recomputed.  Only the scalar / polymer start values are set:
+//   scalar only      : scalar and csource from setscl, not normalised (main_dns.f90:1810-1815)
+//   scalar + polymer : crstrt = 0: setpoly, scalar gradient and conformation-tensor derivatives
+//                      (normalised), scn, cIJn, strIJn, qpIJ zeroed (main_dns.f90:1817-1908);
+//                      crstrt = 1: everything from c-restart (main_dns.f90:1909-1916)
+// csource is zero at the start of the reference program and the crstrt = 1 branch leaves it so.
+// ---------------------------------------------------------------------------
+static int initial_restart(kmm_ctx *ctx) {
+    if (!ctx->p.scalar_on) return KMM_OK;
+    RET(kmm_zero(ctx, KMM_CSOURCE));
+    if (ctx->p.polymer_on && ctx->p.crstrt != 0) return KMM_OK;
+    RET(kmm_xyzfft(ctx, KMM_SCALAR, KMM_INITSCL));
+    if (!ctx->p.polymer_on) return KMM_OK;
+    RET(poly_set_constant(ctx));
+    RET(kmm_gradscl(ctx));
+    { static const int l[3] = {KMM_SCLX, KMM_SCLY, KMM_SCLZ}; RET(norm_ids(ctx, l, 3)); }
+    RET(kmm_derivscji(ctx));
+    RET(poly_norm_c(ctx));
+    RET(poly_norm_dc(ctx));
+    RET(kmm_zero(ctx, KMM_SCN));
+    for (int m = 0; m < 6; ++m) {
+        RET(kmm_zero(ctx, KMM_C11N + m));
+        RET(kmm_zero(ctx, KMM_STR11N + m));
+        RET(kmm_zero(ctx, kQp[m]));
+    }
+    return KMM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// initial, after the setup's gfcn (main_dns.f90:151-161, 1602-2231)
 // ---------------------------------------------------------------------------
 extern "C" int kmm_initial(kmm_ctx *ctx) {
     if (!ctx) return KMM_ERR_ARG;
@@ -184,6 +216,11 @@ extern "C" int kmm_initial(kmm_ctx *ctx) {
     const size_t n = ctx->nspec;
     RET(kmm_gfcn(ctx));
     ctx->it = 0;
+    if (ctx->p.irstrt >= 1) {
+        RET(initial_restart(ctx));
+        CK(cudaStreamSynchronize(ctx->stream));
+        return KMM_OK;
+    }
     RET(kmm_xyzfft(ctx, KMM_U, KMM_INITU));
     RET(kmm_xyzfft(ctx, KMM_V, KMM_INITV));
     RET(kmm_xyzfft(ctx, KMM_W, KMM_INITW));

@@ -216,6 +216,18 @@ class KmmContext:
         self._check(self.L.kmm_flowstats(self.h, prof.ctypes.data_as(dp), scal.ctypes.data_as(dp)), "kmm_flowstats")
         return prof, scal
 
+    def save_restart(self, path, c_path=None):
+        """outputs/last-restart (and c-last-restart when due) of the current state, in the
+        reference's unformatted record layout (main_dns.f90:775-794)."""
+        from . import restart
+        restart.save(self.download, self.params, self.stats().it, path, c_path)
+
+    def load_restart(self, path, c_path=None):
+        """Upload setup/restart (and setup/c-restart) before `initial` with irstrt >= 1
+        (main_dns.f90:1742-1916)."""
+        from . import restart
+        restart.load(self.upload, self.params, path, c_path)
+
     # mirrors of the reference's main-program blocks
     def initial(self):
         return self.call("initial")
