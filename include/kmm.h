@@ -6,7 +6,7 @@
  * subroutine names and dns.config) and the GPU implementation of the hot path:
  * solvers.f90 (Chebyshev-tau solvers, influence matrix, vcw3dp), derivatives.f90
  * (Chebyshev / Fourier derivatives), helpers.f90 (norm, xyzfft, polymer coupling)
- * and part_track.f90 (tracer integrator).
+ * and part_track.f90 (tracer and inertial-particle integrators).
  *
  * Conventions
  *  - Every entry point returns an int status (KMM_OK == 0).  The reference
@@ -52,7 +52,8 @@ enum kmm_status {
     KMM_ERR_INTERP = 5,       /* particle cell index out of range (part_track.f90:580-590) */
     KMM_ERR_TIMEOUT = 6,      /* a bounded device-side wait gave up                 */
     KMM_ERR_NOMEM = 7,        /* device allocation failed                           */
-    KMM_ERR_UNSUPPORTED = 8   /* option not available in this build                 */
+    KMM_ERR_UNSUPPORTED = 8,  /* option not available in this build                 */
+    KMM_ERR_PCFL = 9          /* inertial-particle CFL umax1 dt/ap >= 10 (part_track.f90:215-222) */
 };
 
 /* ---- run parameters -------------------------------------------------------
@@ -122,6 +123,12 @@ enum kmm_field {
 
     /* real(8) (nyp,mz,mx), 3/2-rule physical grid */
     KMM_FXINTG = 400, KMM_FYINTG, KMM_FZINTG, KMM_UP3D, KMM_VP3D, KMM_WP3D, KMM_SWIRL3D,
+    /* the physical fields of the inertial-particle path (particle_flag > 0): vorticity, velocity
+     * gradient, Laplacian, and the previous step's velocity and Laplacian (solvers.f90:1824-1829,
+     * 3464-3476) */
+    KMM_WX3D, KMM_WY3D, KMM_WZ3D,
+    KMM_U11P3D, KMM_U12P3D, KMM_U13P3D, KMM_U21P3D, KMM_U22P3D, KMM_U23P3D, KMM_U31P3D, KMM_U32P3D, KMM_U33P3D,
+    KMM_LUP3D, KMM_LVP3D, KMM_LWP3D, KMM_UOLD, KMM_VOLD, KMM_WOLD, KMM_LUNM1, KMM_LVNM1, KMM_LWNM1,
     KMM_NPHYS_END,
 
     /* integer(4) (nyp,mz,mx) */
@@ -142,6 +149,8 @@ typedef struct kmm_stats {
     double umax;         /* max |u| on the 3/2 grid                                                  */
     int    it;           /* COMMON /itime/ it after the call                                         */
     int    status;       /* last nonzero status raised on the device (0 if none)                     */
+    double pumax;        /* inertial particles: running max |u_fluid - u_particle| (umax1, part_track.f90:736-742) */
+    double pcfl;         /* inertial particles: umax1 dt / ap of the last update (part_track.f90:215-216) */
 } kmm_stats;
 
 typedef struct kmm_ctx kmm_ctx;

@@ -177,6 +177,7 @@ struct orc_ctx {
     int kmaxsurf;
     int it;
     int substep;
+    double umax1; /* part_track's saved running max of the particle relative velocity */
     void *fld[MAXF];
     kmm_stats stats;
     fftplan py2, pmz, pmx, pnx, pnz; /* 2*ny (DCT), mz, mx, nx, nz */
@@ -1487,6 +1488,155 @@ int orc_tracer_update(orc_ctx *c)
 }
 
 /* ------------------------------------------------------------------------- */
+/* part_track.f90: inertial particles (particle_flag > 0), Maxey-Riley with RK4 */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    const double *u, *v, *w, *uo, *vo, *wo, *wx, *wy, *wz, *g[9], *L[3], *Lo[3];
+} mr_fields;
+
+/* SubDerivative, part_track.f90:896-1075: the fluid's material derivative and the time
+ * derivative of its Laplacian at the particle.  The time derivatives are taken at the eight
+ * cell corners first ((f - f_old)/dt with the substep dt) and then interpolated. */
+static void mr_subderivative(const orc_ctx *c, const mr_fields *F, double dt, double uf, double vf, double wf,
+                             double xp0, double yp0, double zp0, double *sDu, double *sDv, double *sDw, double *dLu,
+                             double *dLv, double *dLw)
+{
+    const int mx = c->mx, mz = c->mz;
+    const double delxm = c->xl / (double)mx, delzm = c->zl / (double)mz;
+    const int imin = ((int)floor(xp0 / delxm) + mx) % mx + 1, imax = imin % mx + 1;
+    const int jmin = ((int)floor(zp0 / delzm) + mz) % mz + 1, jmax = jmin % mz + 1;
+    const int kmax = (int)floor(1.0 + (double)c->ny / c->pi * acos(2.0 * yp0 / c->yl)), kmin = kmax + 1;
+    const double xmin = (double)(imin - 1) * delxm, xmax = (double)(imax - 1) * delxm;
+    const double ymin = c->ycoord[kmin - 1], ymax = c->ycoord[kmax - 1];
+    const double zmin = (double)(jmin - 1) * delzm, zmax = (double)(jmax - 1) * delzm;
+    const int gk[8] = {kmin, kmin, kmin, kmin, kmax, kmax, kmax, kmax};
+    const int gj[8] = {jmin, jmin, jmax, jmax, jmin, jmin, jmax, jmax};
+    const int gi[8] = {imin, imax, imin, imax, imin, imax, imin, imax};
+    double dudt[3][8], dLudt[3][8], gv[9][8];
+    for (int n = 0; n < 8; ++n) {
+        const size_t x = PIDX(c, gk[n] - 1, gj[n] - 1, gi[n] - 1);
+        dudt[0][n] = (F->u[x] - F->uo[x]) / dt;
+        dudt[1][n] = (F->v[x] - F->vo[x]) / dt;
+        dudt[2][n] = (F->w[x] - F->wo[x]) / dt;
+        for (int m = 0; m < 3; ++m) dLudt[m][n] = (F->L[m][x] - F->Lo[m][x]) / dt;
+        for (int m = 0; m < 9; ++m) gv[m][n] = F->g[m][x];
+    }
+#define I3(a) interpolate3(xp0, yp0, zp0, xmin, xmax, ymin, ymax, zmin, zmax, (a)[0], (a)[1], (a)[2], (a)[3], (a)[4], \
+                           (a)[5], (a)[6], (a)[7])
+    double gr[9];
+    for (int m = 0; m < 9; ++m) gr[m] = I3(gv[m]);   /* dufdx, dufdy, dufdz, dvfdx, ..., dwfdz */
+    const double dudt_p = I3(dudt[0]), dvdt_p = I3(dudt[1]), dwdt_p = I3(dudt[2]);
+    *dLu = I3(dLudt[0]);
+    *dLv = I3(dLudt[1]);
+    *dLw = I3(dLudt[2]);
+#undef I3
+    *sDu = dudt_p + uf * gr[0] + vf * gr[1] + wf * gr[2];
+    *sDv = dvdt_p + uf * gr[3] + vf * gr[4] + wf * gr[5];
+    *sDw = dwdt_p + uf * gr[6] + vf * gr[7] + wf * gr[8];
+}
+
+/* RKstage, part_track.f90:759-892: forces at the stage point, then the stage update from the
+ * start-of-step state (h = dt for stage 3, dt/2 otherwise) */
+static int mr_stage(const orc_ctx *c, const mr_fields *F, int sn, double dt, double *un, double *vn, double *wn,
+                    double *xp, double *yp, double *zp, double *Ku, double *Kv, double *Kw, double xp_old,
+                    double yp_old, double zp_old, double up_old, double vp_old, double wp_old)
+{
+    const double ratio = c->p.ratio, ap = c->p.ap, re = c->re;
+    const double Pi_f = 1.0 / (ratio + 0.5), Pi_p = ratio / (ratio + 0.5), C_L = 0.5;
+    const double Height = c->ycoord[0] - ap;
+    double uf, vf, wf, wxf, wyf, wzf, Luf, Lvf, Lwf;
+    int st = fluid_interp(c, *xp, *yp, *zp, F->u, F->v, F->w, &uf, &vf, &wf);
+    st |= fluid_interp(c, *xp, *yp, *zp, F->wx, F->wy, F->wz, &wxf, &wyf, &wzf);
+    st |= fluid_interp(c, *xp, *yp, *zp, F->L[0], F->L[1], F->L[2], &Luf, &Lvf, &Lwf);
+    if (st) return KMM_ERR_INTERP;
+    double sDu, sDv, sDw, dLu, dLv, dLw;
+    mr_subderivative(c, F, dt, uf, vf, wf, *xp, *yp, *zp, &sDu, &sDv, &sDw, &dLu, &dLv, &dLw);
+    const double Re_p = 2 * ap * re * sqrt((uf - *un) * (uf - *un) + (vf - *vn) * (vf - *vn) + (wf - *wn) * (wf - *wn));
+    double C_D = 0.0;
+    if (c->p.cd_switch == 1) C_D = 16 / (2 * ap * re) * c->p.c_mu;
+    else if (c->p.cd_switch == 2) C_D = 24 / (2 * ap * re) * (1 + 0.15 * pow(Re_p, 0.687));
+    else if (c->p.cd_switch == 3) C_D = Re_p > 1.0 ? 16.31 * pow(Re_p, -0.8331) : 17.28 * pow(Re_p, -0.9711);
+    const double a6 = ap * ap / 6.0;
+    const double ru = uf - *un + a6 * Luf, rv = vf - *vn + a6 * Lvf, rw = wf - *wn + a6 * Lwf;
+    const double PGX = 1.5 * sDu, DX = C_D * 3 / (8 * ap) * ru, LX = C_L * (rv * wzf - rw * wyf);
+    const double FX = 3.0 / 20.0 * (ap * ap) * dLu;
+    const double PGY = 1.5 * sDv, DY = C_D * 3 / (8 * ap) * rv, LY = C_L * (rw * wxf - ru * wzf);
+    const double FY = 3.0 / 20.0 * (ap * ap) * dLv;
+    const double PGZ = 1.5 * sDw, DZ = C_D * 3 / (8 * ap) * rw, LZ = C_L * (ru * wyf - rv * wxf);
+    const double FZ = 3.0 / 20.0 * (ap * ap) * dLw;
+    *Ku = Pi_f * (PGX + DX + LX + FX);
+    *Kv = Pi_f * (PGY + DY + LY + FY) - c->p.gravity * (Pi_f - Pi_p);
+    *Kw = Pi_f * (PGZ + DZ + LZ + FZ);
+    const double h = sn == 3 ? dt : dt / 2.0;
+    *un = up_old + h * *Ku;
+    *vn = vp_old + h * *Kv;
+    *wn = wp_old + h * *Kw;
+    *xp = fmod(c->xl + xp_old + h * *un, c->xl);
+    *yp = fmax(fmin(yp_old + h * *vn, Height), ap + c->ycoord[c->nyp - 1]);
+    *zp = fmod(c->zl + zp_old + h * *wn, c->zl);
+    return KMM_OK;
+}
+
+/* RK4, part_track.f90:617-755: one substep of one particle; *umax1 = max(*umax1, relative speed) */
+static int mr_rk4(const orc_ctx *c, const mr_fields *F, double dt, double *xp0, double *yp0, double *zp0, double *up,
+                  double *vp, double *wp, double *umax1)
+{
+    const double ap = c->p.ap, Height = c->ycoord[0] - ap, ybot = ap + c->ycoord[c->nyp - 1];
+    double xp = *xp0, yp = *yp0, zp = *zp0, un = *up, vn = *vp, wn = *wp;
+    double K[4][3], s2[3], s3[3], s4[3];
+    int st = KMM_OK;
+    for (int sn = 1; sn <= 4; ++sn) {
+        st |= mr_stage(c, F, sn, dt, &un, &vn, &wn, &xp, &yp, &zp, &K[sn - 1][0], &K[sn - 1][1], &K[sn - 1][2], *xp0,
+                       *yp0, *zp0, *up, *vp, *wp);
+        if (st) return KMM_ERR_INTERP;
+        double *d = sn == 1 ? s2 : sn == 2 ? s3 : sn == 3 ? s4 : NULL;
+        if (d) { d[0] = un; d[1] = vn; d[2] = wn; }
+    }
+    *xp0 = fmod(c->xl + *xp0 + dt * (*up / 6 + s2[0] / 3 + s3[0] / 3 + s4[0] / 6), c->xl);
+    *yp0 = fmax(fmin(*yp0 + dt * (*vp / 6 + s2[1] / 3 + s3[1] / 3 + s4[1] / 6), Height), ybot);
+    *zp0 = fmod(c->zl + *zp0 + dt * (*wp / 6 + s2[2] / 3 + s3[2] / 3 + s4[2] / 6), c->zl);
+    *up = *up + dt * (K[0][0] / 6 + K[1][0] / 3 + K[2][0] / 3 + K[3][0] / 6);
+    const double vp_new = *vp + dt * (K[0][1] / 6 + K[1][1] / 3 + K[2][1] / 3 + K[3][1] / 6);
+    *wp = *wp + dt * (K[0][2] / 6 + K[1][2] / 3 + K[2][2] / 3 + K[3][2] / 6);
+    /* elastic bounce off a wall the particle was clamped to */
+    if ((*yp0 == Height && vp_new > 0.0) || (*yp0 == ybot && vp_new < 0.0)) *vp = -vp_new;
+    else *vp = vp_new;
+    double uf, vf, wf;
+    if (fluid_interp(c, *xp0, *yp0, *zp0, F->u, F->v, F->w, &uf, &vf, &wf)) return KMM_ERR_INTERP;
+    const double um = sqrt((uf - *up) * (uf - *up) + (vf - *vp) * (vf - *vp) + (wf - *wp) * (wf - *wp));
+    if (um > *umax1) *umax1 = um;
+    return KMM_OK;
+}
+
+/* the particle_flag > 0 branch of part_track, part_track.f90:125-176: `substep` RK4 substeps
+ * of dt/substep per particle */
+int orc_inertial_update(orc_ctx *c)
+{
+    mr_fields F;
+    F.u = RF(c, KMM_UP3D); F.v = RF(c, KMM_VP3D); F.w = RF(c, KMM_WP3D);
+    F.uo = RF(c, KMM_UOLD); F.vo = RF(c, KMM_VOLD); F.wo = RF(c, KMM_WOLD);
+    F.wx = RF(c, KMM_WX3D); F.wy = RF(c, KMM_WY3D); F.wz = RF(c, KMM_WZ3D);
+    for (int m = 0; m < 9; ++m) F.g[m] = RF(c, KMM_U11P3D + m);
+    for (int m = 0; m < 3; ++m) { F.L[m] = RF(c, KMM_LUP3D + m); F.Lo[m] = RF(c, KMM_LUNM1 + m); }
+    double *xpa = RF(c, KMM_XPART), *ypa = RF(c, KMM_YPART), *zpa = RF(c, KMM_ZPART);
+    double *upa = RF(c, KMM_UPART), *vpa = RF(c, KMM_VPART), *wpa = RF(c, KMM_WPART);
+    const double dt = c->dt / (double)c->substep;
+    const int np = c->p.npart, nsub = c->substep;
+    double umax1 = c->umax1;
+    int st = KMM_OK;
+#pragma omp parallel for reduction(max : umax1, st)
+    for (int j = 0; j < np; ++j)
+        for (int s = 0; s < nsub; ++s) {
+            double xp = xpa[j], yp = ypa[j], zp = zpa[j], up = upa[j], vp = vpa[j], wp = wpa[j];
+            int e = mr_rk4(c, &F, dt, &xp, &yp, &zp, &up, &vp, &wp, &umax1);
+            if (e > st) st = e;
+            xpa[j] = xp; ypa[j] = yp; zpa[j] = zp; upa[j] = up; vpa[j] = vp; wpa[j] = wp;
+        }
+    c->umax1 = umax1;
+    return st;
+}
+
+/* ------------------------------------------------------------------------- */
 /* solvers.f90: vcw3dp                                                        */
 /* ------------------------------------------------------------------------- */
 /* physical-plane field slots */
@@ -1608,6 +1758,13 @@ int orc_vcw3dp(orc_ctx *c)
 
     for (int i = 0; i < nyp; ++i) c->cfl[i] = 0.0;
     double *up3d = RF(c, KMM_UP3D), *vp3d = RF(c, KMM_VP3D), *wp3d = RF(c, KMM_WP3D);
+    /* inertial particles read the vorticity, velocity gradient and Laplacian on the 3/2 grid
+       (wx3d .. wz3d, u11p3d .. u33p3d, Lup3d .. Lwp3d; solvers.f90:3464-3466) */
+    const int inertial = c->p.particle_flag > 0 && c->p.npart > 0;
+    double *p3d[15];
+    for (int m = 0; m < 15; ++m) p3d[m] = inertial ? RF(c, KMM_WX3D + m) : NULL;
+    if (inertial)
+        for (int m = 0; m < 6; ++m) (void)RF(c, KMM_UOLD + m);
     const double zl2 = c->p.zlmax * c->p.zlmax;
     const int kmaxsurf = c->kmaxsurf;
 
@@ -1768,6 +1925,8 @@ int orc_vcw3dp(orc_ctx *c)
                 for (int j = 0; j < mz; ++j) {
                     size_t g = PIDX(c, i, j, k), q = (size_t)k * mz + j;
                     up3d[g] = up[q]; vp3d[g] = vp[q]; wp3d[g] = wp[q];
+                    if (inertial)
+                        for (int m = 0; m < 15; ++m) p3d[m][g] = phys[P_WX + m][q];
                 }
             /* x r2c, z c2c forward, truncate and scale: solvers.f90:3147-3273 */
             for (int o = 0; o < nout; o += 2) {
@@ -1825,7 +1984,17 @@ int orc_vcw3dp(orc_ctx *c)
     int st = KMM_OK;
     if (c->p.npart > 0) {
         if (it == c->p.irstrt) st = orc_init_part(c);
+        else if (inertial) st = orc_inertial_update(c);
         else st = orc_tracer_update(c);
+        if (inertial) {
+            /* u_old = up3d, ..., Lwnm1 = Lwp3d after part_track (solvers.f90:3469-3476) */
+            static const int cur[6] = {KMM_UP3D, KMM_VP3D, KMM_WP3D, KMM_LUP3D, KMM_LVP3D, KMM_LWP3D};
+            for (int m = 0; m < 6; ++m) orc_copy(c, KMM_UOLD + m, cur[m]);
+            /* particle CFL, part_track.f90:213-222 (umax1 keeps its value between calls) */
+            c->stats.pumax = c->umax1;
+            c->stats.pcfl = c->umax1 * c->dt / c->p.ap;
+            if (st == KMM_OK && c->stats.pcfl >= 10.0) st = KMM_ERR_PCFL;
+        }
     }
     /* mean u profile, solvers.f90:3487-3495 */
     if (c->p.flow_select == 1 || c->p.flow_select == 4) {

@@ -79,6 +79,7 @@ int orc_initial(orc_ctx *c);
 int orc_step(orc_ctx *c);
 int orc_run(orc_ctx *c, int n);
 int orc_tracer_update(orc_ctx *c);
+int orc_inertial_update(orc_ctx *c);   /* particle_flag > 0: Maxey-Riley RK4, part_track.f90:617-1075 */
 int orc_init_part(orc_ctx *c);
 /* swirl strength from the closed-form eigenvalues (helpers.f90:197-404) on the last 3/2-grid gradients */
 int orc_calcswirl(orc_ctx *c);

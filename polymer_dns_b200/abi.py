@@ -9,11 +9,11 @@ import ctypes
 KMM_ABI_VERSION = 1
 
 # status codes (enum kmm_status)
-OK, ERR_ARG, ERR_CUDA, ERR_CFL, ERR_NAN, ERR_INTERP, ERR_TIMEOUT, ERR_NOMEM, ERR_UNSUPPORTED = range(9)
+OK, ERR_ARG, ERR_CUDA, ERR_CFL, ERR_NAN, ERR_INTERP, ERR_TIMEOUT, ERR_NOMEM, ERR_UNSUPPORTED, ERR_PCFL = range(10)
 STATUS_NAMES = {
     OK: "KMM_OK", ERR_ARG: "KMM_ERR_ARG", ERR_CUDA: "KMM_ERR_CUDA", ERR_CFL: "KMM_ERR_CFL",
     ERR_NAN: "KMM_ERR_NAN", ERR_INTERP: "KMM_ERR_INTERP", ERR_TIMEOUT: "KMM_ERR_TIMEOUT",
-    ERR_NOMEM: "KMM_ERR_NOMEM", ERR_UNSUPPORTED: "KMM_ERR_UNSUPPORTED",
+    ERR_NOMEM: "KMM_ERR_NOMEM", ERR_UNSUPPORTED: "KMM_ERR_UNSUPPORTED", ERR_PCFL: "KMM_ERR_PCFL",
 }
 
 _PARAM_FIELDS = [
@@ -52,7 +52,8 @@ class KmmParams(ctypes.Structure):
 
 
 class KmmStats(ctypes.Structure):
-    _fields_ = [("cflmax", ctypes.c_double), ("umax", ctypes.c_double), ("it", ctypes.c_int), ("status", ctypes.c_int)]
+    _fields_ = [("cflmax", ctypes.c_double), ("umax", ctypes.c_double), ("it", ctypes.c_int), ("status", ctypes.c_int),
+                ("pumax", ctypes.c_double), ("pcfl", ctypes.c_double)]
 
 
 def _enum(names, start=0):
@@ -76,7 +77,9 @@ SPECTRAL_NAMES = (
 )
 MEAN_NAMES = ["U0", "W0", "H1N", "H1NM1", "H3N", "H3NM1", "UXMEAN"]
 WALL_NAMES = ["BCTOP", "BCBOT", "DNV1B", "DNV1T", "DNV2B", "DNV2T", "DENOM", "C1", "C2"]
-PHYS_NAMES = ["FXINTG", "FYINTG", "FZINTG", "UP3D", "VP3D", "WP3D", "SWIRL3D"]
+PHYS_NAMES = (["FXINTG", "FYINTG", "FZINTG", "UP3D", "VP3D", "WP3D", "SWIRL3D", "WX3D", "WY3D", "WZ3D"]
+              + ["U%d%dP3D" % (i, j) for i in (1, 2, 3) for j in (1, 2, 3)]
+              + ["LUP3D", "LVP3D", "LWP3D", "UOLD", "VOLD", "WOLD", "LUNM1", "LVNM1", "LWNM1"])
 PART_NAMES = ["XPART", "YPART", "ZPART", "UPART", "VPART", "WPART", "SWIRLPART"]
 INIT_NAMES = ["INITU", "INITV", "INITW", "INITSCL"]
 

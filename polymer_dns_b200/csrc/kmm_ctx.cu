@@ -285,6 +285,8 @@ extern "C" int kmm_ctx_create(const kmm_params *p, int device, kmm_ctx **out) {
     CK(cudaMalloc(&c->d_cfl, sizeof(double) * (size_t)c->nyp));
     CK(cudaMalloc(&c->d_umax, sizeof(double) * (size_t)c->nyp));
     CK(cudaMalloc(&c->d_status, sizeof(int)));
+    CK(cudaMalloc(&c->d_pumax, sizeof(double)));
+    CK(cudaMemset(c->d_pumax, 0, sizeof(double)));
     CK(cudaMalloc(&c->d_scratch, sizeof(double) * 9 * KMM_MAX_NYP));
     CK(cudaMallocHost(&c->h_pin, sizeof(double) * (2 * KMM_MAX_NYP + 1)));
     CK(cudaMemset(c->d_status, 0, sizeof(int)));
@@ -328,7 +330,7 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
     for (int w = 0; w < 6; ++w)
         if (ctx->wrk[w]) cudaFree(ctx->wrk[w]);
     void *ptrs[] = {ctx->d_wavx, ctx->d_wavz, ctx->d_c, ctx->d_ycoord, ctx->d_seght, ctx->d_fspread, ctx->d_cfl,
-                    ctx->d_umax, ctx->d_status, ctx->d_scratch, ctx->pl_in, ctx->pl_out, ctx->q_in, ctx->q_out, ctx->scsource};
+                    ctx->d_umax, ctx->d_status, ctx->d_pumax, ctx->d_scratch, ctx->pl_in, ctx->pl_out, ctx->q_in, ctx->q_out, ctx->scsource};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i)
         if (ptrs[i]) cudaFree(ptrs[i]);
     for (int s = 0; s < 5; ++s)

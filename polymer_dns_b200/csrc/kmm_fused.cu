@@ -831,6 +831,7 @@ int kmm_tracers(kmm_ctx *ctx);
 bool kmm_fused_applicable(const kmm_ctx *ctx) {
     if (ctx->p.polymer_on || ctx->f[KMM_IMATRIX] != NULL) return false;
     if (ctx->p.scalar_on && ctx->p.scl_flag >= 2) return false;
+    if (ctx->p.particle_flag > 0 && ctx->p.npart > 0) return false;   // inertial particles: routine vcw3dp
     const int E = (ctx->nyp + 31) / 32;
     if (!(E == 2 || E == 3 || E == 4 || E == 5 || E == 9)) return false;
     const int Ex = (ctx->mx + 31) / 32;

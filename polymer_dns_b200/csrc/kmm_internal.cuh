@@ -71,6 +71,7 @@ struct kmm_ctx {
     size_t pl_in_fields, pl_out_fields;
     double *d_cfl;               // nyp
     int *d_status;               // device-raised status
+    double *d_pumax;             // inertial particles: part_track's running max relative speed (umax1)
     double *d_umax;              // scratch for |u| max (per plane)
     double *d_scratch;           // 9*KMM_MAX_NYP doubles for the (0,0)-mode solver
     double *h_pin;               // pinned host: cfl[KMM_MAX_NYP], umax[KMM_MAX_NYP], status (fused-step read-back)

@@ -91,8 +91,12 @@ __global__ void __launch_bounds__(256) k_zfft_bwd(const double2 *__restrict__ pl
 // ---------------------------------------------------------------------------
 // input slots (order of the physical arrays used below)
 enum { S_U, S_V, S_W, S_WX, S_WY, S_WZ, S_U11, S_U12, S_U13, S_U21, S_U22, S_U23, S_U31, S_U32, S_U33,
-       S_SC, S_CX, S_CY, S_CZ, S_C11, S_DC111 = S_C11 + 9, S_NSLOT = S_DC111 + 27 };
+       S_SC, S_CX, S_CY, S_CZ, S_C11, S_DC111 = S_C11 + 9, S_LU = S_DC111 + 27, S_LV, S_LW, S_NSLOT };
 enum { O_H1, O_H2, O_H3, O_SC, O_C11N, O_STR11N = O_C11N + 6, O_QP11 = O_STR11N + 6, O_NSLOT = O_QP11 + 6 };
+
+// 3/2-grid copies kept for the inertial-particle path: wx, wy, wz, u11 .. u33 (slots S_WX .. S_U33),
+// then Lu, Lv, Lw; p[0] == NULL when the path is off
+struct Save3D { double *p[15]; };
 
 struct PhysArgs {
     int slot_of_in[S_NSLOT];    // index into the input list, -1 if not transformed
@@ -115,7 +119,7 @@ __global__ void __launch_bounds__(256) k_xphys(const double2 *__restrict__ q, do
                                                double *__restrict__ fyi, double *__restrict__ fzi,
                                                const double *__restrict__ scsource, const double *__restrict__ seght,
                                                double *__restrict__ cfl, double *__restrict__ umax, DevPlan P,
-                                               PhysArgs A, int nyp, int mz, int mx, int nxh) {
+                                               PhysArgs A, Save3D sv, int nyp, int mz, int mx, int nxh) {
     extern __shared__ double2 sm[];
     const int y = blockIdx.y;
     const int z0 = blockIdx.x * XZB;
@@ -241,6 +245,12 @@ __global__ void __launch_bounds__(256) k_xphys(const double2 *__restrict__ q, do
             if (s >= 0) po[(size_t)s * nyp * mz * mx + g3] = out[o];
         }
         if (A.save_uvw) { up3[g3] = up; vp3[g3] = vp; wp3[g3] = wp; }
+        if (sv.p[0]) {
+#pragma unroll
+            for (int m = 0; m < 12; ++m) sv.p[m][g3] = IN(S_WX + m);
+#pragma unroll
+            for (int m = 0; m < 3; ++m) sv.p[12 + m][g3] = IN(S_LU + m);
+        }
     }
 #undef IN
     // block reductions of the CFL number and |u| for this plane
@@ -463,6 +473,7 @@ int kmm_update_kmaxsurf(kmm_ctx *ctx) {
 // driver
 // ---------------------------------------------------------------------------
 int kmm_tracers(kmm_ctx *ctx);   // kmm_tracer.cu
+int kmm_inertial(kmm_ctx *ctx);  // kmm_tracer.cu
 int kmm_fast_x(kmm_ctx *ctx, const double2 *q, double2 *r, int ic, int nout, bool save_uvw, double *up3,
                double *vp3, double *wp3);   // kmm_fast.cu
 
@@ -477,6 +488,8 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     // the immersed-boundary branches run only when an imatrix was uploaded (all-fluid otherwise)
     const bool ib_any = ctx->f[KMM_IMATRIX] != NULL;
     if (ib_any) RET(kmm_update_kmaxsurf(ctx));
+    // inertial particles (particle_flag > 0) read the vorticity, gradient and Laplacian on the 3/2 grid
+    const bool inertial = ctx->p.particle_flag > 0 && ctx->p.npart > 0;
 
     // inputs actually consumed by the physics (the reference also transforms u_ij and the
     // Laplacian every step; those only feed output, swirl and the inertial-particle path)
@@ -509,9 +522,12 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         RET(add_in(S_CY, KMM_SCLY));
         RET(add_in(S_CZ, KMM_SCLZ));
     }
-    if (poly) {
-        static const int gu[9] = {KMM_U11, KMM_U12, KMM_U13, KMM_U21, KMM_U22, KMM_U23, KMM_U31, KMM_U32, KMM_U33};
+    static const int gu[9] = {KMM_U11, KMM_U12, KMM_U13, KMM_U21, KMM_U22, KMM_U23, KMM_U31, KMM_U32, KMM_U33};
+    if (poly || inertial)
         for (int m = 0; m < 9; ++m) RET(add_in(S_U11 + m, gu[m]));
+    if (inertial)
+        for (int m = 0; m < 3; ++m) RET(add_in(S_LU + m, KMM_LU + m));
+    if (poly) {
         for (int m = 0; m < 9; ++m) RET(add_in(S_C11 + m, KMM_C11 + m));
         for (int m = 0; m < 27; ++m) RET(add_in(S_DC111 + m, KMM_DC111 + m));
     }
@@ -554,6 +570,11 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     RET(kmm_ensure_plane_buffers(ctx, nin, nout));
     RET(ensure_phys(ctx, nout, ib_any));
     double *up3 = REAL(ctx, KMM_UP3D), *vp3 = REAL(ctx, KMM_VP3D), *wp3 = REAL(ctx, KMM_WP3D);
+    Save3D sv;
+    for (int m = 0; m < 15; ++m) {
+        sv.p[m] = inertial ? REAL(ctx, KMM_WX3D + m) : NULL;
+        if (inertial && !sv.p[m]) return KMM_ERR_NOMEM;
+    }
     double *fxi = NULL, *fyi = NULL, *fzi = NULL;
     int *im = NULL;
     if (ib_any) {
@@ -595,8 +616,8 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_BWD);
     bool fast_done = false;
-    if (!poly && !ib_any) {
-        // fused warp-per-row x stage (no polymer, no immersed boundary)
+    if (!poly && !ib_any && !inertial) {
+        // fused warp-per-row x stage (no polymer, no immersed boundary, no inertial particles)
         kmm_tic(ctx);
         const bool save = ctx->p.npart > 0 || !ctx->in_step;
         const int fst = kmm_fast_x(ctx, ctx->q_in, ctx->q_out, scal ? A.slot_of_in[S_CX] : -1, nout, save, up3, vp3, wp3);
@@ -608,7 +629,7 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         kmm_tic(ctx);
         k_xphys<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_x, ctx->stream>>>(
             ctx->q_in, ctx->po, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl,
-            ctx->d_umax, ctx->pmx, A, nyp, mz, mx, nxh);
+            ctx->d_umax, ctx->pmx, A, sv, nyp, mz, mx, nxh);
         CKL();
         kmm_toc(ctx, KMM_STAGE_XPHYS);
         if (ib_any && ctx->kmaxsurf > 0) {
@@ -639,8 +660,8 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     // tracers (solvers.f90:3463-3476)
     int st = KMM_OK;
     if (ctx->p.npart > 0) {
-        st = kmm_tracers(ctx);
-        if (st != KMM_OK && st != KMM_ERR_INTERP) return st;
+        st = inertial ? kmm_inertial(ctx) : kmm_tracers(ctx);
+        if (st != KMM_OK && st != KMM_ERR_INTERP && st != KMM_ERR_PCFL) return st;
     }
     // CFL check (solvers.f90:3497-3514)
     double h_cfl[KMM_MAX_NYP], h_um[KMM_MAX_NYP];

@@ -257,7 +257,7 @@ extern "C" int kmm_initial(kmm_ctx *ctx) {
         RET(poly_norm_dc(ctx));
     }
     int st = kmm_vcw3dp(ctx);
-    if (st != KMM_OK && st != KMM_ERR_CFL && st != KMM_ERR_INTERP && st != KMM_ERR_NAN) return st;
+    if (st != KMM_OK && st != KMM_ERR_CFL && st != KMM_ERR_INTERP && st != KMM_ERR_NAN && st != KMM_ERR_PCFL) return st;
     { static const int l[5] = {KMM_V, KMM_OMY, KMM_FN, KMM_GN, KMM_OMZ}; RET(norm_ids(ctx, l, 5)); }
     if (ctx->p.polymer_on) {
         RET(poly_norm_out(ctx));

@@ -199,6 +199,189 @@ int kmm_tracers_enqueue(kmm_ctx *ctx) {
     return KMM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// inertial particles (particle_flag > 0): Maxey-Riley equations with RK4, part_track.f90:617-1075
+// One thread per particle; its `substep` RK4 substeps of dt/substep run back to back.
+// ---------------------------------------------------------------------------
+struct MRFields {
+    const double *u, *v, *w, *uo, *vo, *wo, *wx, *wy, *wz, *g[9], *L[3], *Lo[3];
+};
+struct MRArgs {
+    double ratio, ap, re, c_mu, gravity;
+    int cd_switch, nsub;
+};
+
+// SubDerivative, part_track.f90:896-1075: corner time derivatives ((f - f_old)/dt with the
+// substep dt) interpolated to the particle, and the material derivative of the fluid velocity
+__device__ void mr_subderivative(const TracerArgs &T, const MRFields &F, const double *__restrict__ ycoord, double uf,
+                                 double vf, double wf, double xp0, double yp0, double zp0, double *sD, double *dL) {
+    const int mx = T.mx, mz = T.mz;
+    const int imin = ((int)floor(xp0 / T.delxm) + mx) % mx + 1, imax = imin % mx + 1;
+    const int jmin = ((int)floor(zp0 / T.delzm) + mz) % mz + 1, jmax = jmin % mz + 1;
+    const int kmax = (int)floor(1.0 + (double)T.ny / T.pi * acos(2.0 * yp0 / T.yl)), kmin = kmax + 1;
+    const double xmin = (double)(imin - 1) * T.delxm, xmax = (double)(imax - 1) * T.delxm;
+    const double ymin = ycoord[kmin - 1], ymax = ycoord[kmax - 1];
+    const double zmin = (double)(jmin - 1) * T.delzm, zmax = (double)(jmax - 1) * T.delzm;
+    // corner n: (gk, gj, gi) = ({kmin x4, kmax x4}, {jmin, jmin, jmax, jmax} x2, {imin, imax} x4)
+    size_t gx[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+        const int k = n < 4 ? kmin : kmax, j = (n & 2) ? jmax : jmin, i = (n & 1) ? imax : imin;
+        gx[n] = ((size_t)(k - 1) * mz + (j - 1)) * mx + (i - 1);
+    }
+#define I3(a) interpolate3(xp0, yp0, zp0, xmin, xmax, ymin, ymax, zmin, zmax, a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7])
+    double gr[9];
+#pragma unroll 1
+    for (int m = 0; m < 9; ++m) {
+        double c[8];
+#pragma unroll
+        for (int n = 0; n < 8; ++n) c[n] = __ldg(&F.g[m][gx[n]]);
+        gr[m] = I3(c);
+    }
+    const double *cur[6] = {F.u, F.v, F.w, F.L[0], F.L[1], F.L[2]};
+    const double *old[6] = {F.uo, F.vo, F.wo, F.Lo[0], F.Lo[1], F.Lo[2]};
+    double tdv[6];
+#pragma unroll 1
+    for (int m = 0; m < 6; ++m) {
+        double c[8];
+#pragma unroll
+        for (int n = 0; n < 8; ++n) c[n] = (__ldg(&cur[m][gx[n]]) - __ldg(&old[m][gx[n]])) / T.dt;
+        tdv[m] = I3(c);
+    }
+#undef I3
+    sD[0] = tdv[0] + uf * gr[0] + vf * gr[1] + wf * gr[2];
+    sD[1] = tdv[1] + uf * gr[3] + vf * gr[4] + wf * gr[5];
+    sD[2] = tdv[2] + uf * gr[6] + vf * gr[7] + wf * gr[8];
+    dL[0] = tdv[3];
+    dL[1] = tdv[4];
+    dL[2] = tdv[5];
+}
+
+// RKstage, part_track.f90:759-892: forces at the stage point, then the stage update from the
+// substep's start (h = dt at stage 3, dt/2 otherwise); returns nonzero on a bad cell index
+__device__ int mr_stage(const TracerArgs &T, const MRArgs &M, const MRFields &F, const double *__restrict__ ycoord,
+                        int sn, double *un, double *xp, double *K, const double *x0, const double *u0) {
+    const double ap = M.ap, re = M.re;
+    const double Pi_f = 1.0 / (M.ratio + 0.5), Pi_p = M.ratio / (M.ratio + 0.5), C_L = 0.5;
+    double uf, vf, wf, wxf, wyf, wzf, Luf, Lvf, Lwf;
+    int bad = fluid_interp(T, ycoord, xp[0], xp[1], xp[2], F.u, F.v, F.w, &uf, &vf, &wf);
+    bad |= fluid_interp(T, ycoord, xp[0], xp[1], xp[2], F.wx, F.wy, F.wz, &wxf, &wyf, &wzf);
+    bad |= fluid_interp(T, ycoord, xp[0], xp[1], xp[2], F.L[0], F.L[1], F.L[2], &Luf, &Lvf, &Lwf);
+    if (bad) return 1;
+    double sD[3], dL[3];
+    mr_subderivative(T, F, ycoord, uf, vf, wf, xp[0], xp[1], xp[2], sD, dL);
+    const double Re_p = 2 * ap * re * sqrt((uf - un[0]) * (uf - un[0]) + (vf - un[1]) * (vf - un[1]) +
+                                           (wf - un[2]) * (wf - un[2]));
+    double C_D = 0.0;
+    if (M.cd_switch == 1) C_D = 16 / (2 * ap * re) * M.c_mu;
+    else if (M.cd_switch == 2) C_D = 24 / (2 * ap * re) * (1 + 0.15 * pow(Re_p, 0.687));
+    else if (M.cd_switch == 3) C_D = Re_p > 1.0 ? 16.31 * pow(Re_p, -0.8331) : 17.28 * pow(Re_p, -0.9711);
+    const double a6 = ap * ap / 6.0;
+    const double ru = uf - un[0] + a6 * Luf, rv = vf - un[1] + a6 * Lvf, rw = wf - un[2] + a6 * Lwf;
+    const double cd = C_D * 3 / (8 * ap), fx = 3.0 / 20.0 * (ap * ap);
+    K[0] = Pi_f * (1.5 * sD[0] + cd * ru + C_L * (rv * wzf - rw * wyf) + fx * dL[0]);
+    K[1] = Pi_f * (1.5 * sD[1] + cd * rv + C_L * (rw * wxf - ru * wzf) + fx * dL[1]) - M.gravity * (Pi_f - Pi_p);
+    K[2] = Pi_f * (1.5 * sD[2] + cd * rw + C_L * (ru * wyf - rv * wxf) + fx * dL[2]);
+    const double h = sn == 3 ? T.dt : T.dt / 2.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) un[c] = u0[c] + h * K[c];
+    xp[0] = fmod(T.xl + x0[0] + h * un[0], T.xl);
+    xp[1] = fmax(fmin(x0[1] + h * un[1], T.height), T.ybot);
+    xp[2] = fmod(T.zl + x0[2] + h * un[2], T.zl);
+    return 0;
+}
+
+__global__ void __launch_bounds__(128) k_inertial(TracerArgs T, MRArgs M, MRFields F, const double *__restrict__ ycoord,
+                                                  double *xpa, double *ypa, double *zpa, double *upa, double *vpa,
+                                                  double *wpa, double *pumax, int *status) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= T.npart) return;
+    double x0[3] = {xpa[j], ypa[j], zpa[j]}, u0[3] = {upa[j], vpa[j], wpa[j]};
+    double um1 = 0.0;
+    int bad = 0;
+    for (int s = 0; s < M.nsub && !bad; ++s) {
+        // RK4, part_track.f90:617-755
+        double xp[3] = {x0[0], x0[1], x0[2]}, un[3] = {u0[0], u0[1], u0[2]};
+        double K[4][3], us[3][3];
+        for (int sn = 1; sn <= 4 && !bad; ++sn) {
+            bad |= mr_stage(T, M, F, ycoord, sn, un, xp, K[sn - 1], x0, u0);
+            if (sn < 4)
+                for (int c = 0; c < 3; ++c) us[sn - 1][c] = un[c];
+        }
+        if (bad) break;
+        const double dt = T.dt;
+        x0[0] = fmod(T.xl + x0[0] + dt * (u0[0] / 6 + us[0][0] / 3 + us[1][0] / 3 + us[2][0] / 6), T.xl);
+        x0[1] = fmax(fmin(x0[1] + dt * (u0[1] / 6 + us[0][1] / 3 + us[1][1] / 3 + us[2][1] / 6), T.height), T.ybot);
+        x0[2] = fmod(T.zl + x0[2] + dt * (u0[2] / 6 + us[0][2] / 3 + us[1][2] / 3 + us[2][2] / 6), T.zl);
+        u0[0] = u0[0] + dt * (K[0][0] / 6 + K[1][0] / 3 + K[2][0] / 3 + K[3][0] / 6);
+        const double vp_new = u0[1] + dt * (K[0][1] / 6 + K[1][1] / 3 + K[2][1] / 3 + K[3][1] / 6);
+        u0[2] = u0[2] + dt * (K[0][2] / 6 + K[1][2] / 3 + K[2][2] / 3 + K[3][2] / 6);
+        // elastic bounce off a wall the particle was clamped to
+        u0[1] = ((x0[1] == T.height && vp_new > 0.0) || (x0[1] == T.ybot && vp_new < 0.0)) ? -vp_new : vp_new;
+        double uf, vf, wf;
+        bad |= fluid_interp(T, ycoord, x0[0], x0[1], x0[2], F.u, F.v, F.w, &uf, &vf, &wf);
+        if (bad) break;
+        um1 = fmax(um1, sqrt((uf - u0[0]) * (uf - u0[0]) + (vf - u0[1]) * (vf - u0[1]) + (wf - u0[2]) * (wf - u0[2])));
+    }
+    if (bad) atomicMax(status, KMM_ERR_INTERP);
+    // running max of non-negative doubles through their bit patterns (NaN compares larger)
+    atomicMax((unsigned long long *)pumax, (unsigned long long)__double_as_longlong(um1));
+    xpa[j] = x0[0]; ypa[j] = x0[1]; zpa[j] = x0[2];
+    upa[j] = u0[0]; vpa[j] = u0[1]; wpa[j] = u0[2];
+}
+
+// the particle_flag > 0 branch of part_track (part_track.f90:125-176, 213-222) and the copies of
+// the velocity and Laplacian kept for the next step's time derivatives (solvers.f90:3469-3476)
+int kmm_inertial(kmm_ctx *ctx) {
+    if (ctx->p.npart <= 0) return KMM_OK;
+    const bool init = ctx->it == ctx->p.irstrt;
+    TracerArgs T = tracer_args(ctx);
+    double *x = REAL(ctx, KMM_XPART), *y = REAL(ctx, KMM_YPART), *z = REAL(ctx, KMM_ZPART);
+    double *u = REAL(ctx, KMM_UPART), *v = REAL(ctx, KMM_VPART), *w = REAL(ctx, KMM_WPART);
+    MRFields F;
+    F.u = REAL(ctx, KMM_UP3D); F.v = REAL(ctx, KMM_VP3D); F.w = REAL(ctx, KMM_WP3D);
+    F.uo = REAL(ctx, KMM_UOLD); F.vo = REAL(ctx, KMM_VOLD); F.wo = REAL(ctx, KMM_WOLD);
+    F.wx = REAL(ctx, KMM_WX3D); F.wy = REAL(ctx, KMM_WY3D); F.wz = REAL(ctx, KMM_WZ3D);
+    for (int m = 0; m < 9; ++m) F.g[m] = REAL(ctx, KMM_U11P3D + m);
+    for (int m = 0; m < 3; ++m) { F.L[m] = REAL(ctx, KMM_LUP3D + m); F.Lo[m] = REAL(ctx, KMM_LUNM1 + m); }
+    if (!x || !y || !z || !u || !v || !w || !F.u || !F.v || !F.w || !F.uo || !F.vo || !F.wo || !F.wx || !F.wy || !F.wz)
+        return KMM_ERR_NOMEM;
+    for (int m = 0; m < 9; ++m) if (!F.g[m]) return KMM_ERR_NOMEM;
+    for (int m = 0; m < 3; ++m) if (!F.L[m] || !F.Lo[m]) return KMM_ERR_NOMEM;
+    MRArgs M;
+    M.ratio = ctx->p.ratio; M.ap = ctx->p.ap; M.re = ctx->re; M.c_mu = ctx->p.c_mu; M.gravity = ctx->p.gravity;
+    M.cd_switch = ctx->p.cd_switch; M.nsub = ctx->substep;
+    CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+    if (init) {
+        k_init_part<<<(T.npart + 255) / 256, 256, 0, ctx->stream>>>(T, ctx->d_ycoord, x, y, z, u, v, w, F.u, F.v, F.w,
+                                                                     ctx->d_status);
+    } else {
+        k_inertial<<<(T.npart + 127) / 128, 128, 0, ctx->stream>>>(T, M, F, ctx->d_ycoord, x, y, z, u, v, w,
+                                                                   ctx->d_pumax, ctx->d_status);
+    }
+    CKL();
+    static const int cur[6] = {KMM_UP3D, KMM_VP3D, KMM_WP3D, KMM_LUP3D, KMM_LVP3D, KMM_LWP3D};
+    for (int m = 0; m < 6; ++m)
+        CK(cudaMemcpyAsync(REAL(ctx, KMM_UOLD + m), REAL(ctx, cur[m]), sizeof(double) * ctx->nphys,
+                           cudaMemcpyDeviceToDevice, ctx->stream));
+    int h = 0;
+    double um1 = 0.0;
+    CK(cudaMemcpyAsync(&h, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&um1, ctx->d_pumax, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->stats.pumax = um1;
+    ctx->stats.pcfl = um1 * ctx->dt / ctx->p.ap;   // with the full dt (part_track.f90:215)
+    if (h) {
+        kmm_set_error(ctx, "particle interpolation cell index out of range (part_track.f90:580-590)");
+        return KMM_ERR_INTERP;
+    }
+    if (ctx->stats.pcfl >= 10.0) {
+        kmm_set_error(ctx, "particle CFL %.3g >= 10 (part_track.f90:217-221)", ctx->stats.pcfl);
+        return KMM_ERR_PCFL;
+    }
+    return KMM_OK;
+}
+
 // swirl at each particle (fluid_interp1 on swirl_3d, solvers.f90:3480)
 __global__ void k_swirl_part(TracerArgs T, const double *__restrict__ ycoord, const double *__restrict__ xp,
                              const double *__restrict__ yp, const double *__restrict__ zp,
