@@ -223,6 +223,8 @@ def run_kmm(a, rank, world, local_rank):
     p, init, desc = make_config(a.config, a.precision)
     f, extra = build_inputs(p, init, a.config)
     ctx = runtime.KmmContext(p, device=local_rank)
+    if a.ztma is not None:
+        ctx.call("set_option", 4, a.ztma)
     load(ctx, f, extra, ctx.upload)
     ctx.initial()
     for _ in range(a.warmup):
@@ -509,6 +511,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision speed / error report")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 16-member ensemble measurement")
+    ap.add_argument("--ztma", type=int, default=None, choices=[0, 1],
+                    help="inverse z transform with TMA tile copies (1, the library default) or plain loads (0)")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3

@@ -284,10 +284,13 @@ enum kmm_option {
     KMM_OPT_COLUMN_BLOCKED = 2, /* 1 (default): the fused step's column kernels hold a column on 16
                            lanes in blocks of ny/16 coefficients (ny = 32, 64, 96, 128);
                            0: one warp per column, coefficient i on lane i mod 32           */
-    KMM_OPT_GRAPH = 3          /* 1 (default): once the tracers are initialised, the fused step is
+    KMM_OPT_GRAPH = 3,         /* 1 (default): once the tracers are initialised, the fused step is
                            captured into two CUDA graphs (the history buffers alternate between
                            two arrangements) and replayed; 0: launched kernel by kernel.  Steps
                            with stage timing on (kmm_set_timing) always run kernel by kernel. */
+    KMM_OPT_ZTMA = 4           /* 1 (default): the FP64 fused step's inverse z transform moves its tiles
+                           with TMA (tensor-map bulk copies, mz = 48, 96, 144, 192); 0: plain
+                           loads and stores                                                  */
 };
 int  kmm_set_option(kmm_ctx *ctx, int option, int value);
 

@@ -221,6 +221,9 @@ extern "C" int kmm_ctx_create(const kmm_params *p, int device, kmm_ctx **out) {
     ctx->device = device;
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming));
     kmm_ctx *c = ctx;
     c->nx = p->nx; c->ny = p->ny; c->nz = p->nz;
     c->nyp = c->ny + 1; c->nym = c->ny - 1; c->nxh = c->nx / 2; c->nyh = c->ny / 2; c->nzh = c->nz / 2;
@@ -270,6 +273,7 @@ extern "C" int kmm_ctx_create(const kmm_params *p, int device, kmm_ctx **out) {
     c->use_fused = 1;
     c->use_colblk = 1;
     c->use_graph = 1;
+    c->use_ztma = 1;
 #define DUP(dst, src, n)                                                        \
     do {                                                                        \
         CK(cudaMalloc(&(dst), sizeof(double) * (size_t)(n)));                   \
@@ -322,6 +326,7 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
         if (ctx->user_ev[e]) cudaEventDestroy(ctx->user_ev[e]);
     kmm_graph_release(ctx);
     kmm_fused_release(ctx);
+    kmm_ztma_release(ctx);
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
     if (ctx->po) cudaFree(ctx->po);
     if (ctx->drag) cudaFree(ctx->drag);
@@ -335,6 +340,9 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
         if (ptrs[i]) cudaFree(ptrs[i]);
     for (int s = 0; s < 5; ++s)
         if (ctx->tw_store[s]) cudaFree(ctx->tw_store[s]);
+    if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+    if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     free(ctx->h_wavx); free(ctx->h_wavz); free(ctx->h_c); free(ctx->h_ycoord); free(ctx->h_seght);
     free(ctx);
@@ -441,6 +449,7 @@ extern "C" int kmm_set_option(kmm_ctx *ctx, int option, int value) {
     case KMM_OPT_FUSED: ctx->use_fused = value ? 1 : 0; kmm_graph_release(ctx); return KMM_OK;
     case KMM_OPT_COLUMN_BLOCKED: ctx->use_colblk = value ? 1 : 0; kmm_graph_release(ctx); return KMM_OK;
     case KMM_OPT_GRAPH: ctx->use_graph = value ? 1 : 0; kmm_graph_release(ctx); return KMM_OK;
+    case KMM_OPT_ZTMA: ctx->use_ztma = value ? 1 : 0; kmm_graph_release(ctx); return KMM_OK;
     default: return KMM_ERR_ARG;
     }
 }

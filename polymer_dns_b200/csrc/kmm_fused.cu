@@ -841,7 +841,7 @@ bool kmm_fused_applicable(const kmm_ctx *ctx) {
 
 static int *h_pin_status(kmm_ctx *ctx) { return (int *)(ctx->h_pin + 2 * KMM_MAX_NYP); }
 
-int kmm_tracers_enqueue(kmm_ctx *ctx);
+int kmm_tracers_enqueue(kmm_ctx *ctx, cudaStream_t st);
 
 int kmm_fused_step(kmm_ctx *ctx) {
     RET(kmm_fused_enqueue(ctx));
@@ -1011,7 +1011,9 @@ int kmm_fused_launch(kmm_ctx *ctx) {
                                                              ctx->d_wavz, (const CC *)twz, nq, nyp, nxh); \
     } while (0)
     const void *twz = f32 ? (const void *)FU->twf_mz : (const void *)ctx->wmz.tw;
-    if (f32) {
+    if (!f32 && kmm_ztma_supported(ctx)) {
+        RET(kmm_zb_tma(ctx, g_yp, g_q, scalar ? 8 : 6, nq, (const double2 *)twz));
+    } else if (f32) {
         switch (mz) {
         case 48: ZB2(48, float2); break;
         case 96: ZB2(96, float2); break;
@@ -1045,6 +1047,15 @@ int kmm_fused_launch(kmm_ctx *ctx) {
         else RET(xst);
     }
     kmm_toc(ctx, KMM_STAGE_XPHYS);
+    // tracers (solvers.f90:3463-3476) on the side stream: they read only the particles and the
+    // 3/2-grid u, v, w just written, so they overlap the z-forward and back stages (kept in line
+    // while the stages are being timed)
+    const bool tracers_forked = ctx->p.npart > 0 && !ctx->timing_on;
+    if (tracers_forked) {
+        CK(cudaEventRecord(ctx->fork_ev, ctx->stream));
+        CK(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
+        RET(kmm_tracers_enqueue(ctx, ctx->side));
+    }
     // z forward transforms
     kmm_tic(ctx);
 #define ZF2(MM, CC)                                                                                   \
@@ -1053,7 +1064,9 @@ int kmm_fused_launch(kmm_ctx *ctx) {
         k_zf2<MM, CC><<<gz, ZT_WARPS * 32, smzf, ctx->stream>>>((const CC *)g_r, (CC *)g_yo, (const CC *)twz, \
                                                               nout, nyp, nxh, (double)ctx->mx * (double)mz); \
     } while (0)
-    if (f32) {
+    if (!f32 && kmm_ztma_supported(ctx)) {
+        RET(kmm_zf_tma(ctx, g_r, g_yo, nout, (const double2 *)twz));
+    } else if (f32) {
         switch (mz) {
         case 48: ZF2(48, float2); break;
         case 96: ZF2(96, float2); break;
@@ -1111,9 +1124,14 @@ int kmm_fused_launch(kmm_ctx *ctx) {
     CKL();
     }
     kmm_toc(ctx, KMM_STAGE_POST);
-    // tracers (solvers.f90:3463-3476); the CFL maxima and the tracer status go to pinned host
-    // memory for kmm_fused_finish (solvers.f90:3497-3514)
-    RET(kmm_tracers_enqueue(ctx));
+    if (tracers_forked) {
+        CK(cudaEventRecord(ctx->join_ev, ctx->side));
+        CK(cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0));
+    } else {
+        RET(kmm_tracers_enqueue(ctx, ctx->stream));
+    }
+    // the CFL maxima and the tracer status go to pinned host memory for kmm_fused_finish
+    // (solvers.f90:3497-3514)
     double *h_cfl = ctx->h_pin, *h_um = ctx->h_pin + KMM_MAX_NYP;
     CK(cudaMemcpyAsync(h_cfl, ctx->d_cfl, sizeof(double) * nyp, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(h_um, ctx->d_umax, sizeof(double) * nyp, cudaMemcpyDeviceToHost, ctx->stream));

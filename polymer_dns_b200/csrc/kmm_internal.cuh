@@ -44,6 +44,8 @@ struct kmm_ctx {
     kmm_params p;
     int device;
     cudaStream_t stream;
+    cudaStream_t side;           // fused step: the tracers run here, overlapping the z-forward and back stages
+    cudaEvent_t fork_ev, join_ev;
     // grid (grid_size.f90:1-47, run-time here)
     int nx, ny, nz, nyp, nym, nxh, nyh, nzh, nyhp, nyhm, mx, mz;
     size_t nspec;   // nyp*nz*nxh
@@ -100,6 +102,8 @@ struct kmm_ctx {
     cudaGraphExec_t gexec[2];
     long long gkernels[2];   // kernels in each graph (added to the launch count per replay)
     void *g_fn0;      // the FN buffer of parity 0
+    int use_ztma;     // FP64 inverse z transform through TMA tile copies (default 1)
+    void *ztma;       // its cached tensor maps (kmm_ztma.cu)
 };
 
 void kmm_fused_release(kmm_ctx *ctx);
@@ -113,6 +117,11 @@ int kmm_fused_finish(kmm_ctx *ctx);
 int kmm_fused_enqueue(kmm_ctx *ctx);
 void kmm_graph_release(kmm_ctx *ctx);
 bool kmm_fused_applicable(const kmm_ctx *ctx);
+// TMA form of the FP64 inverse z transform (kmm_ztma.cu)
+bool kmm_ztma_supported(const kmm_ctx *ctx);
+int kmm_zb_tma(kmm_ctx *ctx, const double2 *yp, double2 *q, int nbase, int nq, const double2 *tw);
+int kmm_zf_tma(kmm_ctx *ctx, const double2 *r, double2 *yo, int nout, const double2 *tw);
+void kmm_ztma_release(kmm_ctx *ctx);
 void kmm_tic(kmm_ctx *ctx);
 void kmm_toc(kmm_ctx *ctx, int stage);
 

@@ -183,8 +183,9 @@ static int tracer_launch(kmm_ctx *ctx, bool init) {
 // called from vcw3dp: init at it == irstrt (part_track.f90:132-134), Euler/RK3 update otherwise
 int kmm_tracers(kmm_ctx *ctx) { return tracer_launch(ctx, ctx->it == ctx->p.irstrt); }
 
-// the same without waiting: the cell-index status stays in d_status for the caller to read back
-int kmm_tracers_enqueue(kmm_ctx *ctx) {
+// the same without waiting, on stream `st`: the cell-index status stays in d_status for the
+// caller to read back
+int kmm_tracers_enqueue(kmm_ctx *ctx, cudaStream_t st) {
     if (ctx->p.npart <= 0) return KMM_OK;
     const bool init = ctx->it == ctx->p.irstrt;
     TracerArgs T = tracer_args(ctx);
@@ -193,8 +194,8 @@ int kmm_tracers_enqueue(kmm_ctx *ctx) {
     double *f1 = REAL(ctx, KMM_UP3D), *f2 = REAL(ctx, KMM_VP3D), *f3 = REAL(ctx, KMM_WP3D);
     if (!x || !y || !z || !u || !v || !w || !f1 || !f2 || !f3) return KMM_ERR_NOMEM;
     const int nb = (T.npart + 255) / 256;
-    if (init) k_init_part<<<nb, 256, 0, ctx->stream>>>(T, ctx->d_ycoord, x, y, z, u, v, w, f1, f2, f3, ctx->d_status);
-    else k_tracer_update<<<nb, 256, 0, ctx->stream>>>(T, ctx->d_ycoord, x, y, z, u, v, w, f1, f2, f3, ctx->d_status);
+    if (init) k_init_part<<<nb, 256, 0, st>>>(T, ctx->d_ycoord, x, y, z, u, v, w, f1, f2, f3, ctx->d_status);
+    else k_tracer_update<<<nb, 256, 0, st>>>(T, ctx->d_ycoord, x, y, z, u, v, w, f1, f2, f3, ctx->d_status);
     CKL();
     return KMM_OK;
 }

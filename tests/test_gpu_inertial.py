@@ -1,9 +1,10 @@
 """Inertial particles (particle_flag > 0) on the GPU: the Maxey-Riley RK4 integrator of
 part_track.f90:617-1075 against the oracle and against its known answers.
 
-Tolerances: the physical fields the integrator reads (vorticity, velocity gradient, Laplacian
-on the 3/2 grid) agree with the oracle to the routine bar (1e-12 relative); particle positions
-and velocities after a few steps to the whole-run bar of the FP64 drop-in (1e-10 relative).
+Tolerances: particle positions and velocities after `initial` agree with the oracle to the
+routine bar (1e-12 relative); after a few steps, the physical fields the integrator reads
+(vorticity, velocity gradient, Laplacian on the 3/2 grid, the previous step's copies) and the
+particles to the whole-run bar of the FP64 drop-in (1e-10 relative).
 """
 import math
 
@@ -58,7 +59,7 @@ def test_inertial_matches_oracle(rt, cd_switch, grid):
         assert o.step() == 0
     for name in ("WX3D", "WZ3D", "U12P3D", "U31P3D", "LVP3D", "UOLD", "LWNM1"):
         e = kc.rel_err(_get(g, name), _get(o, name))
-        assert e <= ROUTINE_TOL, (name, e)
+        assert e <= RUN_TOL, (name, e)
     for name in PART:
         e = kc.rel_err(_get(g, name), _get(o, name))
         assert e <= RUN_TOL, (name, e)
