@@ -1695,7 +1695,8 @@ int orc_vcw3dp(orc_ctx *c)
         if (!(t == 0 || t == 1 || t == 3 || t == 4 || t == 11)) return KMM_ERR_UNSUPPORTED;
     }
 
-    /* scalar source, solvers.f90:2076-2166 */
+    /* scalar source, solvers.f90:2076-2166; the targeted sources (scl_flag 4, 5) are not restated */
+    if (scal && c->p.scl_flag >= 4) return KMM_ERR_UNSUPPORTED;
     if (scal && c->p.scl_flag == 2 && it >= c->p.src_start && it <= c->p.src_stop) scalar_source_particles(c);
     else if (scal && c->p.scl_flag >= 2) {
         if (!c->scsource) c->scsource = calloc((size_t)nyp * mz * mx, sizeof(double));

@@ -470,6 +470,44 @@ int kmm_update_kmaxsurf(kmm_ctx *ctx) {
 }
 
 // ---------------------------------------------------------------------------
+// scalar source of the particles (scl_flag = 2, solvers.f90:2079-2118): a Gaussian of widths
+// sigmax, sigmay, sigmaz and weight deltaT around every particle, with the reference's cut-offs
+// (betax < 20, betax + betaz < 20, betax + betay + betaz < 18) and no periodic images.  One warp
+// per particle walks the x and z points that can pass the cut-offs (the range widened by one point
+// each side; the reference's tests decide), lanes over y; contributions are added with FP64
+// atomics (the reference sums its OpenMP threads' private copies, so its order is not fixed
+// either).  Layout [y][z][x].
+// ---------------------------------------------------------------------------
+__global__ void k_scsource(const double *__restrict__ xp, const double *__restrict__ yp, const double *__restrict__ zp,
+                           int npart, const double *__restrict__ ycoord, double *sc, int nyp, int mz, int mx,
+                           double delxm, double delzm, double sx, double sy, double sz, double dT) {
+    const int n = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (n >= npart) return;
+    const int lane = threadIdx.x & 31;
+    const double xc = xp[n], yc = yp[n], zc = zp[n];
+    const double ax = 2.0 * (sx * sx), ay = 2.0 * (sy * sy), az = 2.0 * (sz * sz);
+    const double rx = sqrt(20.0 * ax), rz = sqrt(20.0 * az);
+    const int k0 = max(0, (int)floor((xc - rx) / delxm) - 1), k1 = min(mx - 1, (int)ceil((xc + rx) / delxm) + 1);
+    const int j0 = max(0, (int)floor((zc - rz) / delzm) - 1), j1 = min(mz - 1, (int)ceil((zc + rz) / delzm) + 1);
+    for (int k = k0; k <= k1; ++k) {
+        const double dx = (double)k * delxm - xc;
+        const double bx = (dx * dx) / ax;
+        if (!(bx < 20.0)) continue;
+        for (int j = j0; j <= j1; ++j) {
+            const double dz = (double)j * delzm - zc;
+            const double bz = (dz * dz) / az;
+            if (!(bx + bz < 20.0)) continue;
+            for (int i = lane; i < nyp; i += 32) {
+                const double dy = ycoord[i] - yc;
+                const double by = (dy * dy) / ay;
+                const double b = bx + by + bz;
+                if (b < 18.0) atomicAdd(&sc[((size_t)i * mz + j) * mx + k], dT * exp(-b));
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // driver
 // ---------------------------------------------------------------------------
 int kmm_tracers(kmm_ctx *ctx);   // kmm_tracer.cu
@@ -581,14 +619,23 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         fxi = REAL(ctx, KMM_FXINTG); fyi = REAL(ctx, KMM_FYINTG); fzi = REAL(ctx, KMM_FZINTG);
         im = (int *)kmm_field_ptr(ctx, KMM_IMATRIX);
     }
+    if (scal && ctx->p.scl_flag >= 4) {
+        kmm_set_error(ctx, "scl_flag = %d (targeted scalar source, solvers.f90:2164-2210) is not built", ctx->p.scl_flag);
+        return KMM_ERR_UNSUPPORTED;
+    }
     if (scal && ctx->p.scl_flag >= 2) {
-        if (!ctx->scsource) {
-            CK(cudaMalloc(&ctx->scsource, sizeof(double) * ctx->nphys));
-            CK(cudaMemsetAsync(ctx->scsource, 0, sizeof(double) * ctx->nphys, ctx->stream));
-        }
-        if (ctx->p.scl_flag == 2 && ctx->p.npart > 0) {
-            kmm_set_error(ctx, "scl_flag = 2 particle-Gaussian scalar source is not built on the GPU path");
-            return KMM_ERR_UNSUPPORTED;
+        // the source array holds only this call's particle Gaussians (zero outside src_start..src_stop)
+        if (!ctx->scsource) CK(cudaMalloc(&ctx->scsource, sizeof(double) * ctx->nphys));
+        CK(cudaMemsetAsync(ctx->scsource, 0, sizeof(double) * ctx->nphys, ctx->stream));
+        const int np = ctx->p.npart;
+        if (ctx->p.scl_flag == 2 && np > 0 && it >= ctx->p.src_start && it <= ctx->p.src_stop) {
+            const double *xp = REAL(ctx, KMM_XPART), *yp = REAL(ctx, KMM_YPART), *zp = REAL(ctx, KMM_ZPART);
+            if (!xp || !yp || !zp) return KMM_ERR_NOMEM;
+            k_scsource<<<(np + 7) / 8, 256, 0, ctx->stream>>>(xp, yp, zp, np, ctx->d_ycoord, ctx->scsource, nyp, mz,
+                                                              mx, ctx->xl / (double)mx, ctx->zl / (double)mz,
+                                                              ctx->p.sigmax, ctx->p.sigmay, ctx->p.sigmaz,
+                                                              ctx->p.deltat);
+            CKL();
         }
     }
 
@@ -616,8 +663,10 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_BWD);
     bool fast_done = false;
-    if (!poly && !ib_any && !inertial) {
-        // fused warp-per-row x stage (no polymer, no immersed boundary, no inertial particles)
+    const bool sc_source = scal && ctx->p.scl_flag >= 2;
+    if (!poly && !ib_any && !inertial && !sc_source) {
+        // fused warp-per-row x stage (no polymer, no immersed boundary, no inertial particles, no
+        // particle scalar source)
         kmm_tic(ctx);
         const bool save = ctx->p.npart > 0 || !ctx->in_step;
         const int fst = kmm_fast_x(ctx, ctx->q_in, ctx->q_out, scal ? A.slot_of_in[S_CX] : -1, nout, save, up3, vp3, wp3);

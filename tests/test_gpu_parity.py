@@ -517,3 +517,35 @@ def test_tma_z_transform_matches_plain_loads(rt, grid, scalar):
     for name in ["V", "OMY", "FN", "GN", "U0", "W0"] + (["SCALAR", "SCN"] if scalar else []):
         e = kc.rel_err(ctxs[0].download(name), ctxs[1].download(name))
         assert e <= 1e-13, (name, e)
+
+
+def test_particle_scalar_source_matches_oracle(rt, oracle_mod):
+    """scl_flag = 2: the particle-Gaussian scalar source (solvers.f90:2079-2118, added to the
+    scalar's nonlinear term at 3061-3063) inside and after the src_start..src_stop window, with
+    the tracers moving the sources; whole-run bar after 5 steps."""
+    p = kc.cfg_small(32, 32, 32, scalar_on=1, diff=1.0, scl_flag=2, npart=200, deltat=0.5, sigmax=0.1,
+                     sigmay=0.05, sigmaz=0.1, src_start=0, src_stop=3)
+    fields = kc.initial_fields(p, amp=0.1, seed=17)
+    parts = inputs.uniform_particles(p.npart, p.xl, p.yl, p.zl, p.ap, 9)
+    sc = np.zeros_like(fields[0])
+    g, o = _pair(rt, oracle_mod, p)
+    for c in (g, o):
+        kc.load_initial(c, p, fields, sc)
+        setter = c.upload if hasattr(c, "upload") else c.set
+        for name, arr in zip(("XPART", "YPART", "ZPART"), parts):
+            setter(name, arr)
+        assert c.initial() == 0
+    for _ in range(5):
+        assert g.step() == 0
+        assert o.step() == 0
+    for name in ["SCALAR", "SCN", "SCNM1", "V", "XPART", "ZPART"]:
+        _cmp(g, o, name, RUN_TOL)
+    assert np.abs(g.download("SCALAR")).max() > 1e-3   # the source did act
+    # the targeted sources are not built: both report it instead of running without them
+    q = kc.cfg_small(16, 32, 16, scalar_on=1, diff=1.0, scl_flag=4)
+    g2, o2 = _pair(rt, oracle_mod, q)
+    f2 = kc.initial_fields(q, amp=0.05, seed=1)
+    for c in (g2, o2):
+        kc.load_initial(c, q, f2, np.zeros_like(f2[0]))
+    assert o2.initial() == abi.ERR_UNSUPPORTED
+    assert g2.call("initial", allow=(abi.ERR_UNSUPPORTED,)) == abi.ERR_UNSUPPORTED
