@@ -410,20 +410,30 @@ int kmm_colblk_fwd(kmm_ctx *ctx, const ColFwdArgs &A, const FusedTabs &T, const 
     const int npairs = ctx->nxh * (ctx->nz / 2);
     const int nblk = (npairs + CB_WARPS - 1) / CB_WARPS;
     const size_t smem = sizeof(double2) * (size_t)CB_WARPS * 4 * (2 * ctx->ny);
+    // scalar and omega_y (independent of v and of each other) on the two side streams, v on the
+    // main stream, so each kernel's last partial wave overlaps the others; u, w after all three
+    cudaStream_t s_scl = ctx->side, s_omy = ctx->side2;
+    CK(cudaEventRecord(ctx->cfork_ev, ctx->stream));
+    CK(cudaStreamWaitEvent(s_omy, ctx->cfork_ev, 0));
+    if (A.scalar) CK(cudaStreamWaitEvent(s_scl, ctx->cfork_ev, 0));
 #define BF(KK, CC)                                                                                    \
     do {                                                                                              \
         const CC *twc = (const CC *)tw;                                                               \
         if (A.scalar) {                                                                               \
             RET(kmm_smem_attr(ctx, (const void *)k_bcol_scl<KK, CC>, smem));                          \
-            k_bcol_scl<KK, CC><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(A, T, rj, twc);             \
+            k_bcol_scl<KK, CC><<<nblk, CB_WARPS * 32, smem, s_scl>>>(A, T, rj, twc);                   \
             CKL();                                                                                    \
+            CK(cudaEventRecord(ctx->cjoin_ev[0], s_scl));                                             \
         }                                                                                             \
         RET(kmm_smem_attr(ctx, (const void *)k_bcol_omy<KK, CC>, smem));                              \
-        k_bcol_omy<KK, CC><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(A, T, rj, twc);                 \
+        k_bcol_omy<KK, CC><<<nblk, CB_WARPS * 32, smem, s_omy>>>(A, T, rj, twc);                       \
         CKL();                                                                                        \
+        CK(cudaEventRecord(ctx->cjoin_ev[1], s_omy));                                                 \
         RET(kmm_smem_attr(ctx, (const void *)k_bcol_v<KK, CC>, smem));                                \
         k_bcol_v<KK, CC><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(A, T, rj, twc);                   \
         CKL();                                                                                        \
+        if (A.scalar) CK(cudaStreamWaitEvent(ctx->stream, ctx->cjoin_ev[0], 0));                      \
+        CK(cudaStreamWaitEvent(ctx->stream, ctx->cjoin_ev[1], 0));                                    \
         RET(kmm_smem_attr(ctx, (const void *)k_bcol_uw<KK, CC>, smem));                               \
         k_bcol_uw<KK, CC><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(A, twc);                         \
         CKL();                                                                                        \

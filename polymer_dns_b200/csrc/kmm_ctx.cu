@@ -222,6 +222,9 @@ extern "C" int kmm_ctx_create(const kmm_params *p, int device, kmm_ctx **out) {
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&ctx->side2, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ctx->cfork_ev, cudaEventDisableTiming));
+    for (int e = 0; e < 2; ++e) CK(cudaEventCreateWithFlags(&ctx->cjoin_ev[e], cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming));
     kmm_ctx *c = ctx;
@@ -342,6 +345,10 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
         if (ctx->tw_store[s]) cudaFree(ctx->tw_store[s]);
     if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
     if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
+    if (ctx->cfork_ev) cudaEventDestroy(ctx->cfork_ev);
+    for (int e = 0; e < 2; ++e)
+        if (ctx->cjoin_ev[e]) cudaEventDestroy(ctx->cjoin_ev[e]);
+    if (ctx->side2) cudaStreamDestroy(ctx->side2);
     if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     free(ctx->h_wavx); free(ctx->h_wavz); free(ctx->h_c); free(ctx->h_ycoord); free(ctx->h_seght);

@@ -45,7 +45,8 @@ struct kmm_ctx {
     int device;
     cudaStream_t stream;
     cudaStream_t side;           // fused step: the tracers run here, overlapping the z-forward and back stages
-    cudaEvent_t fork_ev, join_ev;
+    cudaStream_t side2;          // fused step: with `side`, the scalar and omega_y column kernels beside v's
+    cudaEvent_t fork_ev, join_ev, cfork_ev, cjoin_ev[2];
     // grid (grid_size.f90:1-47, run-time here)
     int nx, ny, nz, nyp, nym, nxh, nyh, nzh, nyhp, nyhm, mx, mz;
     size_t nspec;   // nyp*nz*nxh
