@@ -288,9 +288,9 @@ enum kmm_option {
                            captured into two CUDA graphs (the history buffers alternate between
                            two arrangements) and replayed; 0: launched kernel by kernel.  Steps
                            with stage timing on (kmm_set_timing) always run kernel by kernel. */
-    KMM_OPT_ZTMA = 4           /* 1 (default): the FP64 fused step's inverse z transform moves its tiles
-                           with TMA (tensor-map bulk copies, mz = 48, 96, 144, 192); 0: plain
-                           loads and stores                                                  */
+    KMM_OPT_ZTMA = 4           /* 1 (default): the fused step's z transforms (FP64 and mixed) move their
+                           tiles with TMA (tensor-map bulk copies, mz = 48, 96, 144, 192); 0:
+                           plain loads and stores                                            */
 };
 int  kmm_set_option(kmm_ctx *ctx, int option, int value);
 

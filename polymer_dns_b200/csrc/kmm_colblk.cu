@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_scl(ColFwdArgs 
     C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
     BPair P;
     if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;   // whole warps: no block barrier below
-    const size_t fstride = (size_t)A.nz * A.nxh * NYP;
+    const size_t fstride = (size_t)A.nz * A.nxh * col_ld<C>(NYP), yoff = (size_t)P.col * col_ld<C>(NYP);
     const double2 zero = make_double2(0.0, 0.0);
     BCol<K> s, d1;
     bload<K>(s, A.scal + P.off);
@@ -93,8 +93,8 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_scl(ColFwdArgs 
     bnorm<K>(s, P.kx, P.j, A.nzh);
     bstore<K>(A.scal + P.off, s);
     bcderiv<K>(d1, s, A.dyde, FULL);
-    bdct_store<K, C>(s, fa, fb, tw, (C *)A.yp + 6 * fstride + P.off);
-    bdct_store<K, C>(d1, fa, fb, tw, (C *)A.yp + 7 * fstride + P.off);
+    bdct_store<K, C>(s, fa, fb, tw, (C *)A.yp + 6 * fstride + yoff);
+    bdct_store<K, C>(d1, fa, fb, tw, (C *)A.yp + 7 * fstride + yoff);
 }
 
 // normal vorticity (main_dns.f90:411-422, 479-484, 500-502, 520-526): phirhs, Robin solve, zero
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_omy(ColFwdArgs 
     C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
     BPair P;
     if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;
-    const size_t fstride = (size_t)A.nz * A.nxh * NYP;
+    const size_t fstride = (size_t)A.nz * A.nxh * col_ld<C>(NYP), yoff = (size_t)P.col * col_ld<C>(NYP);
     const double g1 = A.re / (A.dt * A.th);
     const double2 zero = make_double2(0.0, 0.0);
     BCol<K> om;
@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_omy(ColFwdArgs 
     }
     bnorm<K>(om, P.kx, P.j, A.nzh);
     bstore<K>(A.omy + P.off, om);
-    bdct_store<K, C>(om, fa, fb, tw, (C *)A.yp + 3 * fstride + P.off);
+    bdct_store<K, C>(om, fa, fb, tw, (C *)A.yp + 3 * fstride + yoff);
 }
 
 // wall-normal velocity (main_dns.f90:363-407, 426-466, 489-502, 520): phi, phirhs, Helmholtz and
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_v(ColFwdArgs A,
     const int lane = threadIdx.x & 31, h = lane >> 4;
     BPair P;
     if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;
-    const size_t fstride = (size_t)A.nz * A.nxh * NYP;
+    const size_t fstride = (size_t)A.nz * A.nxh * col_ld<C>(NYP), yoff = (size_t)P.col * col_ld<C>(NYP);
     const double g1 = A.re / (A.dt * A.th);
     const double2 zero = make_double2(0.0, 0.0);
     const double w2 = P.w2;
@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_v(ColFwdArgs A,
         for (int m = 0; m <= K; ++m) v.v[m] = zero;
     }
     bstore<K>(A.v + P.off, v);
-    bdct_store<K, C>(v, fa, fb, tw, (C *)A.yp + 1 * fstride + P.off);
+    bdct_store<K, C>(v, fa, fb, tw, (C *)A.yp + 1 * fstride + yoff);
 }
 
 // veloc (solvers.f90:1576-1659) from the new v and omega_y; y-physical u, du/dy, w, dw/dy
@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_uw(ColFwdArgs A
     C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
     BPair P;
     if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;
-    const size_t fstride = (size_t)A.nz * A.nxh * NYP;
+    const size_t fstride = (size_t)A.nz * A.nxh * col_ld<C>(NYP), yoff = (size_t)P.col * col_ld<C>(NYP);
     const double2 zero = make_double2(0.0, 0.0);
     const double kxv = P.kxv, kzv = P.kzv, w2 = P.w2;
     BCol<K> u, w;
@@ -300,11 +300,11 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_uw(ColFwdArgs A
     }
     BCol<K> d1;
     bcderiv<K>(d1, u, A.dyde, FULL);
-    bdct_store<K, C>(u, fa, fb, tw, (C *)A.yp + 0 * fstride + P.off);
-    bdct_store<K, C>(d1, fa, fb, tw, (C *)A.yp + 4 * fstride + P.off);
+    bdct_store<K, C>(u, fa, fb, tw, (C *)A.yp + 0 * fstride + yoff);
+    bdct_store<K, C>(d1, fa, fb, tw, (C *)A.yp + 4 * fstride + yoff);
     bcderiv<K>(d1, w, A.dyde, FULL);
-    bdct_store<K, C>(w, fa, fb, tw, (C *)A.yp + 2 * fstride + P.off);
-    bdct_store<K, C>(d1, fa, fb, tw, (C *)A.yp + 5 * fstride + P.off);
+    bdct_store<K, C>(w, fa, fb, tw, (C *)A.yp + 2 * fstride + yoff);
+    bdct_store<K, C>(d1, fa, fb, tw, (C *)A.yp + 5 * fstride + yoff);
 }
 
 template <int K, typename C>
@@ -344,14 +344,14 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_bwd(ColBwdArgs 
     // The scalar term first, then h1 and h3 (gn, omz and the y-derivative fn needs), then h2.
     if (A.scalar) {
         BCol<K> sc;
-        bload_dct<K, C>(sc, (const C *)A.yo + 3 * ncols * NYP + off, fa, fb, tw);
+        bload_dct<K, C>(sc, (const C *)A.yo + (3 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
         bnorm<K>(sc, kx, j, A.nzh);
         filt(sc);
         bstore<K>(A.scn + off, sc);
     }
     BCol<K> h1, h3, d;
-    bload_dct<K, C>(h1, (const C *)A.yo + 0 * ncols * NYP + off, fa, fb, tw);
-    bload_dct<K, C>(h3, (const C *)A.yo + 2 * ncols * NYP + off, fa, fb, tw);
+    bload_dct<K, C>(h1, (const C *)A.yo + (0 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
+    bload_dct<K, C>(h3, (const C *)A.yo + (2 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
     bnorm<K>(h1, kx, j, A.nzh);
     bnorm<K>(h3, kx, j, A.nzh);
     filt(h3);
@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_bwd(ColBwdArgs 
     bstore<K>(A.gn + off, h1);
     bstore<K>(A.omz + off, h3);
     BCol<K> h2;
-    bload_dct<K, C>(h2, (const C *)A.yo + 1 * ncols * NYP + off, fa, fb, tw);
+    bload_dct<K, C>(h2, (const C *)A.yo + (1 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
     bnorm<K>(h2, kx, j, A.nzh);
     filt(h2);
     const double w2 = -kxv * kxv - kzv * kzv;

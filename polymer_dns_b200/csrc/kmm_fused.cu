@@ -613,7 +613,8 @@ __global__ void __launch_bounds__(ZT_WARPS * 32) k_zb2(const C *__restrict__ yp,
     const int kl = warp % ZT_KX, yl = warp / ZT_KX;
     const int kx = blockIdx.x * ZT_KX + kl, y = blockIdx.y * ZT_Y + yl;
     const bool act = kx < nxh && y < nyp;
-    const size_t fs = (size_t)NZ * nxh * nyp;   // field stride of the column layout
+    const int ldc = col_ld<C>(nyp);
+    const size_t fs = (size_t)NZ * nxh * ldc;   // field stride of the column layout
     C *a = sm + (size_t)warp * 2 * MZ, *b = a + MZ;
     C *stage = sm + (size_t)ZT_WARPS * 2 * MZ;   // [y][z][kx] tile for the store
     const T kxv = act ? (T)wavx[kx] : (T)0;
@@ -626,7 +627,7 @@ __global__ void __launch_bounds__(ZT_WARPS * 32) k_zb2(const C *__restrict__ yp,
             const int kz = lane + 32 * e;
             C val = zc;
             if (act && kz < NZ) {
-                const size_t o = ((size_t)kx * NZ + kz) * nyp + y;
+                const size_t o = ((size_t)kx * NZ + kz) * ldc + y;
                 const T kzv = (T)wavz[kz];
                 switch (g < 6 ? g : g + 1) {   // q fields: u v w wx wy wz [cx cy cz]
                 case 3: {                      // wx = dw/dy - i kz v
@@ -730,7 +731,7 @@ __global__ void __launch_bounds__(ZT_WARPS * 32) k_zf2(const C *__restrict__ r, 
         for (int t = threadIdx.x; t < ZT_KX * NZ * ZT_Y; t += blockDim.x) {
             const int yy = t % ZT_Y, kz = (t / ZT_Y) % NZ, kk = t / (ZT_Y * NZ);
             if (kx0 + kk < nxh && y0 + yy < nyp)
-                yo[(size_t)o * ncols * nyp + ((size_t)(kx0 + kk) * NZ + kz) * nyp + y0 + yy] = stage[t];
+                yo[((size_t)o * ncols + (size_t)(kx0 + kk) * NZ + kz) * col_ld<C>(nyp) + y0 + yy] = stage[t];
         }
         __syncthreads();
     }
@@ -1013,6 +1014,8 @@ int kmm_fused_launch(kmm_ctx *ctx) {
     const void *twz = f32 ? (const void *)FU->twf_mz : (const void *)ctx->wmz.tw;
     if (!f32 && kmm_ztma_supported(ctx)) {
         RET(kmm_zb_tma(ctx, g_yp, g_q, scalar ? 8 : 6, nq, (const double2 *)twz));
+    } else if (f32 && kmm_ztma_supported(ctx)) {
+        RET(kmm_zb_tma32(ctx, (const float2 *)g_yp, (float2 *)g_q, scalar ? 8 : 6, nq, (const float2 *)twz));
     } else if (f32) {
         switch (mz) {
         case 48: ZB2(48, float2); break;
@@ -1066,6 +1069,8 @@ int kmm_fused_launch(kmm_ctx *ctx) {
     } while (0)
     if (!f32 && kmm_ztma_supported(ctx)) {
         RET(kmm_zf_tma(ctx, g_r, g_yo, nout, (const double2 *)twz));
+    } else if (f32 && kmm_ztma_supported(ctx)) {
+        RET(kmm_zf_tma32(ctx, (const float2 *)g_r, (float2 *)g_yo, nout, (const float2 *)twz));
     } else if (f32) {
         switch (mz) {
         case 48: ZF2(48, float2); break;

@@ -14,6 +14,12 @@ struct FusedTabs {
     double g[TB_N];
 };
 
+// leading dimension of the column-layout intermediates Y[f][kx][kz][y] and Yo: FP32 columns are
+// padded to an even length so that every column starts on a 16-byte boundary (a TMA row); FP64
+// columns (16 nyp bytes) need no padding
+template <typename C>
+__host__ __device__ __forceinline__ int col_ld(int nyp) { return sizeof(C) == 8 ? ((nyp + 1) & ~1) : nyp; }
+
 struct KmmFused {
     FusedTabs tabs;
     double2 *yp, *q, *r, *yo;

@@ -118,10 +118,12 @@ int kmm_fused_finish(kmm_ctx *ctx);
 int kmm_fused_enqueue(kmm_ctx *ctx);
 void kmm_graph_release(kmm_ctx *ctx);
 bool kmm_fused_applicable(const kmm_ctx *ctx);
-// TMA form of the FP64 inverse z transform (kmm_ztma.cu)
+// TMA forms of the z transforms, FP64 and FP32 (kmm_ztma.cu)
 bool kmm_ztma_supported(const kmm_ctx *ctx);
 int kmm_zb_tma(kmm_ctx *ctx, const double2 *yp, double2 *q, int nbase, int nq, const double2 *tw);
 int kmm_zf_tma(kmm_ctx *ctx, const double2 *r, double2 *yo, int nout, const double2 *tw);
+int kmm_zb_tma32(kmm_ctx *ctx, const float2 *yp, float2 *q, int nbase, int nq, const float2 *tw);
+int kmm_zf_tma32(kmm_ctx *ctx, const float2 *r, float2 *yo, int nout, const float2 *tw);
 void kmm_ztma_release(kmm_ctx *ctx);
 void kmm_tic(kmm_ctx *ctx);
 void kmm_toc(kmm_ctx *ctx, int stage);

@@ -1,4 +1,5 @@
-// kmm_ztma.cu -- the fused step's inverse z transform (FP64) with TMA tile copies.
+// kmm_ztma.cu -- the fused step's z transforms (FP64 and the FP32 of the mixed form) with TMA
+// tile copies.
 //
 // Work of the stage (solvers.f90:2578-2803 for the velocity, vorticity and scalar-gradient
 // fields): from the y-physical base fields u, v, w, omega_y, du/dy, dw/dy [, c, dc/dy] in column
@@ -22,6 +23,7 @@
 
 #include "kmm_internal.cuh"
 #include "kmm_fft.cuh"
+#include "kmm_fused.cuh"
 
 #define ZTM_YT 4       // y columns per CTA (= warps)
 #define ZTM_WARPS ZTM_YT
@@ -231,13 +233,165 @@ __global__ void __launch_bounds__(ZTM_WARPS * 32, 2)
 }
 
 // ---------------------------------------------------------------------------
+// FP32 forms (mixed precision: float2 intermediates).  A TMA row must hold at least 16 bytes, so a
+// CTA covers two kx (one 16-byte row of the [y][z][kx] planes) and 4 y: 8 columns, one warp each.
+// Column tiles [kx][kz][4 y] have 32-byte rows with the 32-byte swizzle (16-byte chunk index XOR
+// bit 7 of the byte offset); FP32 columns are padded to an even length (col_ld) so that each
+// starts on a 16-byte boundary.  Same work and operation order as k_zb2 / k_zf2 with float2.
+// ---------------------------------------------------------------------------
+#define ZT32_KX 2
+#define ZT32_WARPS (ZT32_KX * ZTM_YT)
+
+// float2 element (kz, y) of a [kz][4 y] tile with 32-byte rows, 32-byte swizzle
+__device__ __forceinline__ int ztile32_idx(int kz, int y) {
+    return kz * ZTM_YT + ((((y >> 1) ^ ((kz >> 2) & 1)) << 1) | (y & 1));
+}
+
+template <int MZ>
+__global__ void __launch_bounds__(ZT32_WARPS * 32, 2)
+    k_zb_tma32(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout,
+               const double *__restrict__ wavx, const double *__restrict__ wavz, const float2 *__restrict__ tw,
+               int nbase, int nq, int *status) {
+    constexpr int NZ = 2 * MZ / 3, NZH = NZ / 2, TILE = NZ * ZTM_YT;   // float2 per (field, kx) tile
+    extern __shared__ unsigned char zsm_raw[];
+    // tiles [nbase][KX][NZ][YT], scratch [warps][2][MZ], stage [YT][MZ][KX], barriers
+    float2 *tiles = reinterpret_cast<float2 *>((reinterpret_cast<uintptr_t>(zsm_raw) + 1023) & ~(uintptr_t)1023);
+    float2 *scr = tiles + (size_t)nbase * ZT32_KX * TILE;
+    float2 *stage = scr + (size_t)ZT32_WARPS * 2 * MZ;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(stage + (size_t)ZTM_YT * MZ * ZT32_KX);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kx0 = blockIdx.x * ZT32_KX, y0 = blockIdx.y * ZTM_YT;
+    const int kl = warp / ZTM_YT, y = warp % ZTM_YT, kx = kx0 + kl;
+    if (threadIdx.x == 0) {
+        for (int f = 0; f < nbase; ++f) mbar_init(&bar[f], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int f = 0; f < nbase; ++f) {
+            mbar_expect_tx(&bar[f], (unsigned)(ZT32_KX * TILE * sizeof(float2)));
+            tma_load4(tiles + (size_t)f * ZT32_KX * TILE, &tin, 2 * y0, 0, kx0, f, &bar[f]);
+        }
+    }
+    const float kxv = (float)wavx[kx];
+    float2 *a = scr + (size_t)warp * 2 * MZ, *b = a + MZ;
+    unsigned ready = 0;
+    bool ok = true;
+    auto need = [&](int f) {
+        if (!((ready >> f) & 1u)) {
+            ok = mbar_wait(&bar[f], 0) && ok;
+            ready |= 1u << f;
+        }
+    };
+    for (int g = 0; g < nq; ++g) {
+        int f0, f1 = -1;
+        switch (g) {
+        case 3: f0 = 5; f1 = 1; break;
+        case 4: f0 = 3; break;
+        case 5: f0 = 1; f1 = 4; break;
+        case 6: case 8: f0 = 6; break;
+        case 7: f0 = 7; break;
+        default: f0 = g; break;
+        }
+        need(f0);
+        if (f1 >= 0) need(f1);
+        const float2 *t0 = tiles + ((size_t)f0 * ZT32_KX + kl) * TILE;
+        const float2 *t1 = f1 >= 0 ? tiles + ((size_t)f1 * ZT32_KX + kl) * TILE : t0;
+        for (int z = lane; z < MZ; z += 32) {
+            float2 val = make_float2(0.f, 0.f);
+            if (z < NZH || z >= MZ - NZH) {
+                const int kz = z < NZH ? z : z - (MZ - NZ);
+                const int ti = ztile32_idx(kz, y);
+                const float2 p = ok ? t0[ti] : val;
+                switch (g) {
+                case 3: {   // wx = dw/dy - i kz v
+                    const float kzv = (float)wavz[kz];
+                    const float2 vv = ok ? t1[ti] : val;
+                    val = make_float2(p.x + kzv * vv.y, p.y - kzv * vv.x);
+                } break;
+                case 5: {   // wz = i kx v - du/dy
+                    const float2 du = ok ? t1[ti] : val;
+                    val = make_float2(-kxv * p.y - du.x, kxv * p.x - du.y);
+                } break;
+                case 6: val = make_float2(-kxv * p.y, kxv * p.x); break;
+                case 8: {
+                    const float kzv = (float)wavz[kz];
+                    val = make_float2(-kzv * p.y, kzv * p.x);
+                } break;
+                default: val = p; break;
+                }
+            }
+            a[swz<float2>(z)] = val;
+        }
+        __syncwarp();
+        const float2 *r = fft_warp_ct<float2, MZ, +1, 1, true>(a, b, tw);
+        if (threadIdx.x == 0) tma_store_wait_read();
+        __syncthreads();
+        for (int z = lane; z < MZ; z += 32) stage[((size_t)y * MZ + z) * ZT32_KX + kl] = r[swz<float2>(z)];
+        fence_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) tma_store4(&tout, 2 * kx0, 0, y0, g, stage);
+    }
+    if (threadIdx.x == 0) tma_store_wait_read();
+    if (!ok && lane == 0) atomicMax(status, KMM_ERR_TIMEOUT);
+}
+
+template <int MZ>
+__global__ void __launch_bounds__(ZT32_WARPS * 32, 2)
+    k_zf_tma32(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout,
+               const float2 *__restrict__ tw, int nout, float rscale, int *status) {
+    constexpr int NZ = 2 * MZ / 3, NZH = NZ / 2, TIN = MZ * ZTM_YT * ZT32_KX, TOUT = NZ * ZTM_YT;
+    extern __shared__ unsigned char zsm_raw[];
+    // out stage [KX][NZ][YT] (swizzled), in tiles [nout][YT][MZ][KX], scratch, barriers
+    float2 *stage = reinterpret_cast<float2 *>((reinterpret_cast<uintptr_t>(zsm_raw) + 1023) & ~(uintptr_t)1023);
+    float2 *tiles = stage + (size_t)ZT32_KX * TOUT;
+    float2 *scr = tiles + (size_t)nout * TIN;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(scr + (size_t)ZT32_WARPS * 2 * MZ);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kx0 = blockIdx.x * ZT32_KX, y0 = blockIdx.y * ZTM_YT;
+    const int kl = warp / ZTM_YT, y = warp % ZTM_YT;
+    if (threadIdx.x == 0) {
+        for (int o = 0; o < nout; ++o) mbar_init(&bar[o], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int o = 0; o < nout; ++o) {
+            mbar_expect_tx(&bar[o], (unsigned)(TIN * sizeof(float2)));
+            tma_load4(tiles + (size_t)o * TIN, &tin, 2 * kx0, 0, y0, o, &bar[o]);
+        }
+    }
+    float2 *a = scr + (size_t)warp * 2 * MZ, *b = a + MZ;
+    bool ok = true;
+    for (int o = 0; o < nout; ++o) {
+        ok = mbar_wait(&bar[o], 0) && ok;
+        const float2 *t = tiles + (size_t)o * TIN;
+        for (int z = lane; z < MZ; z += 32)
+            a[swz<float2>(z)] = ok ? t[((size_t)y * MZ + z) * ZT32_KX + kl] : make_float2(0.f, 0.f);
+        __syncwarp();
+        const float2 *r = fft_warp_ct<float2, MZ, -1, 1, true>(a, b, tw);
+        if (threadIdx.x == 0) tma_store_wait_read();
+        __syncthreads();
+        for (int kz = lane; kz < NZ; kz += 32) {
+            const float2 v = r[swz<float2>(kz < NZH ? kz : (MZ - NZ) + kz)];
+            stage[(size_t)kl * TOUT + ztile32_idx(kz, y)] = make_float2(v.x * rscale, v.y * rscale);
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) tma_store4(&tout, 2 * y0, 0, kx0, o, stage);
+    }
+    if (threadIdx.x == 0) tma_store_wait_read();
+    if (!ok && lane == 0) atomicMax(status, KMM_ERR_TIMEOUT);
+}
+
+// ---------------------------------------------------------------------------
 // host side: tensor maps (cached per context, re-encoded when a buffer or size changes) and the
 // launches
 // ---------------------------------------------------------------------------
 struct ZtmaPair {
     CUtensorMap in, out;
     const void *src, *dst;
-    int nyp, nz, nxh, mz, nsrc, ndst;
+    int nyp, nz, nxh, mz, nsrc, ndst, f32;
 };
 struct ZtmaMaps {
     ZtmaPair inv, fwd;   // inverse: Y (base fields) -> Q; forward: R -> Yo
@@ -262,7 +416,7 @@ void kmm_ztma_release(kmm_ctx *ctx) {
 
 bool kmm_ztma_supported(const kmm_ctx *ctx) {
     const int mz = ctx->mz;
-    return ctx->use_ztma && ctx->p.precision == 0 && (mz == 48 || mz == 96 || mz == 144 || mz == 192);
+    return ctx->use_ztma && (mz == 48 || mz == 96 || mz == 144 || mz == 192);
 }
 
 static ZtmaMaps *ztma_maps(kmm_ctx *ctx) {
@@ -275,37 +429,45 @@ static ZtmaMaps *ztma_maps(kmm_ctx *ctx) {
     return (ZtmaMaps *)ctx->ztma;
 }
 
-static bool pair_current(const ZtmaPair &P, const void *src, const void *dst, const kmm_ctx *ctx, int nsrc, int ndst) {
+static bool pair_current(const ZtmaPair &P, const void *src, const void *dst, const kmm_ctx *ctx, int nsrc, int ndst,
+                         int f32) {
     return P.src == src && P.dst == dst && P.nyp == ctx->nyp && P.nz == ctx->nz && P.nxh == ctx->nxh &&
-           P.mz == ctx->mz && P.nsrc == nsrc && P.ndst == ndst;
+           P.mz == ctx->mz && P.nsrc == nsrc && P.ndst == ndst && P.f32 == f32;
 }
 
-// column layout [f][kx][kz][y] as doubles: (2 nyp, nz, nxh, nf), box (2 YT, nz, 1, 1), 64-byte swizzle
+// column layout [f][kx][kz][y] as reals (a complex value is 2 reals; FP32 columns padded to an
+// even length): (2 nyp, nz, nxh, nf); FP64 box (2 YT, nz, 1, 1) with 64-byte rows and swizzle,
+// FP32 box (2 YT, nz, 2, 1) with 32-byte rows and swizzle
 static CUresult map_columns(PFN_cuTensorMapEncodeTiled_v12000 enc, CUtensorMap *m, const void *base,
-                            const kmm_ctx *ctx, int nf, CUtensorMapL2promotion l2) {
+                            const kmm_ctx *ctx, int nf, CUtensorMapL2promotion l2, bool f32) {
     const int nyp = ctx->nyp, nz = ctx->nz, nxh = ctx->nxh;
+    const cuuint64_t cb = f32 ? (cuuint64_t)8 * col_ld<float2>(nyp) : (cuuint64_t)16 * nyp;   // column bytes
     cuuint64_t d[4] = {(cuuint64_t)2 * nyp, (cuuint64_t)nz, (cuuint64_t)nxh, (cuuint64_t)nf};
-    cuuint64_t st[3] = {(cuuint64_t)nyp * 16, (cuuint64_t)nz * nyp * 16, (cuuint64_t)nz * nxh * nyp * 16};
-    cuuint32_t box[4] = {2 * ZTM_YT, (cuuint32_t)nz, 1, 1};
+    cuuint64_t st[3] = {cb, (cuuint64_t)nz * cb, (cuuint64_t)nz * nxh * cb};
+    cuuint32_t box[4] = {2 * ZTM_YT, (cuuint32_t)nz, f32 ? (cuuint32_t)ZT32_KX : 1u, 1};
     cuuint32_t es[4] = {1, 1, 1, 1};
-    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void *)base, d, st, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-               CU_TENSOR_MAP_SWIZZLE_64B, l2, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return enc(m, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void *)base, d, st, box,
+               es, CU_TENSOR_MAP_INTERLEAVE_NONE, f32 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_64B, l2,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }
 
-// plane layout [f][y][z][kx] as doubles: (2 nxh, mz, nyp, nf), box (2, mz, YT, 1), no swizzle
+// plane layout [f][y][z][kx] as reals: (2 nxh, mz, nyp, nf), box (16 bytes of kx, mz, YT, 1): one
+// kx in FP64, two in FP32; no swizzle
 static CUresult map_planes(PFN_cuTensorMapEncodeTiled_v12000 enc, CUtensorMap *m, const void *base,
-                           const kmm_ctx *ctx, int nf, CUtensorMapL2promotion l2) {
+                           const kmm_ctx *ctx, int nf, CUtensorMapL2promotion l2, bool f32) {
     const int nyp = ctx->nyp, nxh = ctx->nxh, mz = ctx->mz;
+    const cuuint64_t eb = f32 ? 8 : 16;   // bytes per complex value
     cuuint64_t d[4] = {(cuuint64_t)2 * nxh, (cuuint64_t)mz, (cuuint64_t)nyp, (cuuint64_t)nf};
-    cuuint64_t st[3] = {(cuuint64_t)nxh * 16, (cuuint64_t)mz * nxh * 16, (cuuint64_t)nyp * mz * nxh * 16};
-    cuuint32_t box[4] = {2, (cuuint32_t)mz, ZTM_YT, 1};
+    cuuint64_t st[3] = {(cuuint64_t)nxh * eb, (cuuint64_t)mz * nxh * eb, (cuuint64_t)nyp * mz * nxh * eb};
+    cuuint32_t box[4] = {f32 ? 4u : 2u, (cuuint32_t)mz, ZTM_YT, 1};
     cuuint32_t es[4] = {1, 1, 1, 1};
-    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void *)base, d, st, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-               CU_TENSOR_MAP_SWIZZLE_NONE, l2, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return enc(m, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void *)base, d, st, box,
+               es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, l2, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }
 
-static int pair_encode(kmm_ctx *ctx, ZtmaPair &P, bool inverse, const void *src, const void *dst, int nsrc, int ndst) {
-    if (pair_current(P, src, dst, ctx, nsrc, ndst)) return KMM_OK;
+static int pair_encode(kmm_ctx *ctx, ZtmaPair &P, bool inverse, const void *src, const void *dst, int nsrc, int ndst,
+                       bool f32) {
+    if (pair_current(P, src, dst, ctx, nsrc, ndst, f32 ? 1 : 0)) return KMM_OK;
     PFN_cuTensorMapEncodeTiled_v12000 enc = ztma_encoder();
     if (!enc) {
         kmm_set_error(ctx, "cuTensorMapEncodeTiled is not available from the driver");
@@ -313,18 +475,18 @@ static int pair_encode(kmm_ctx *ctx, ZtmaPair &P, bool inverse, const void *src,
     }
     CUresult r1, r2;
     if (inverse) {
-        r1 = map_columns(enc, &P.in, src, ctx, nsrc, CU_TENSOR_MAP_L2_PROMOTION_L2_128B);
-        r2 = map_planes(enc, &P.out, dst, ctx, ndst, CU_TENSOR_MAP_L2_PROMOTION_NONE);
+        r1 = map_columns(enc, &P.in, src, ctx, nsrc, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, f32);
+        r2 = map_planes(enc, &P.out, dst, ctx, ndst, CU_TENSOR_MAP_L2_PROMOTION_NONE, f32);
     } else {
-        r1 = map_planes(enc, &P.in, src, ctx, nsrc, CU_TENSOR_MAP_L2_PROMOTION_L2_128B);
-        r2 = map_columns(enc, &P.out, dst, ctx, ndst, CU_TENSOR_MAP_L2_PROMOTION_NONE);
+        r1 = map_planes(enc, &P.in, src, ctx, nsrc, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, f32);
+        r2 = map_columns(enc, &P.out, dst, ctx, ndst, CU_TENSOR_MAP_L2_PROMOTION_NONE, f32);
     }
     if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS) {
         kmm_set_error(ctx, "tensor map encoding failed (%d, %d)", (int)r1, (int)r2);
         P.src = NULL;
         return KMM_ERR_CUDA;
     }
-    P.src = src; P.dst = dst; P.nsrc = nsrc; P.ndst = ndst;
+    P.src = src; P.dst = dst; P.nsrc = nsrc; P.ndst = ndst; P.f32 = f32 ? 1 : 0;
     P.nyp = ctx->nyp; P.nz = ctx->nz; P.nxh = ctx->nxh; P.mz = ctx->mz;
     return KMM_OK;
 }
@@ -333,7 +495,7 @@ int kmm_zb_tma(kmm_ctx *ctx, const double2 *yp, double2 *q, int nbase, int nq, c
     const int nyp = ctx->nyp, nz = ctx->nz, nxh = ctx->nxh, mz = ctx->mz;
     ZtmaMaps *M = ztma_maps(ctx);
     if (!M) return KMM_ERR_NOMEM;
-    RET(pair_encode(ctx, M->inv, true, yp, q, nbase, nq));
+    RET(pair_encode(ctx, M->inv, true, yp, q, nbase, nq, false));
     const size_t smem = 1024 + sizeof(double2) * ((size_t)nbase * nz * ZTM_YT + (size_t)ZTM_WARPS * 2 * mz +
                                                   (size_t)ZTM_YT * mz) + 8 * sizeof(uint64_t);
     const dim3 grid(nxh, (nyp + ZTM_YT - 1) / ZTM_YT);
@@ -358,7 +520,7 @@ int kmm_zf_tma(kmm_ctx *ctx, const double2 *r, double2 *yo, int nout, const doub
     const int nyp = ctx->nyp, nz = ctx->nz, nxh = ctx->nxh, mz = ctx->mz;
     ZtmaMaps *M = ztma_maps(ctx);
     if (!M) return KMM_ERR_NOMEM;
-    RET(pair_encode(ctx, M->fwd, false, r, yo, nout, nout));
+    RET(pair_encode(ctx, M->fwd, false, r, yo, nout, nout, false));
     const size_t smem = 1024 + sizeof(double2) * ((size_t)nz * ZTM_YT + (size_t)nout * mz * ZTM_YT +
                                                   (size_t)ZTM_WARPS * 2 * mz) + 8 * sizeof(uint64_t);
     const dim3 grid(nxh, (nyp + ZTM_YT - 1) / ZTM_YT);
@@ -378,4 +540,58 @@ int kmm_zf_tma(kmm_ctx *ctx, const double2 *r, double2 *yo, int nout, const doub
     }
 #undef ZTF_LAUNCH
     return KMM_OK;   // the caller checks the launch and counts it
+}
+
+// FP32 forms (mixed precision)
+int kmm_zb_tma32(kmm_ctx *ctx, const float2 *yp, float2 *q, int nbase, int nq, const float2 *tw) {
+    const int nyp = ctx->nyp, nz = ctx->nz, nxh = ctx->nxh, mz = ctx->mz;
+    if (nxh % ZT32_KX) return KMM_ERR_UNSUPPORTED;
+    ZtmaMaps *M = ztma_maps(ctx);
+    if (!M) return KMM_ERR_NOMEM;
+    RET(pair_encode(ctx, M->inv, true, yp, q, nbase, nq, true));
+    const size_t smem = 1024 + sizeof(float2) * ((size_t)nbase * ZT32_KX * nz * ZTM_YT + (size_t)ZT32_WARPS * 2 * mz +
+                                                 (size_t)ZTM_YT * mz * ZT32_KX) + 8 * sizeof(uint64_t);
+    const dim3 grid(nxh / ZT32_KX, (nyp + ZTM_YT - 1) / ZTM_YT);
+#define ZTM32_LAUNCH(MM)                                                                                      \
+    do {                                                                                                      \
+        RET(kmm_smem_attr(ctx, (const void *)k_zb_tma32<MM>, smem));                                          \
+        k_zb_tma32<MM><<<grid, ZT32_WARPS * 32, smem, ctx->stream>>>(M->inv.in, M->inv.out, ctx->d_wavx,      \
+                                                                     ctx->d_wavz, tw, nbase, nq, ctx->d_status); \
+    } while (0)
+    switch (mz) {
+    case 48: ZTM32_LAUNCH(48); break;
+    case 96: ZTM32_LAUNCH(96); break;
+    case 144: ZTM32_LAUNCH(144); break;
+    case 192: ZTM32_LAUNCH(192); break;
+    default: return KMM_ERR_UNSUPPORTED;
+    }
+#undef ZTM32_LAUNCH
+    return KMM_OK;   // the caller checks the launch and counts it
+}
+
+int kmm_zf_tma32(kmm_ctx *ctx, const float2 *r, float2 *yo, int nout, const float2 *tw) {
+    const int nyp = ctx->nyp, nz = ctx->nz, nxh = ctx->nxh, mz = ctx->mz;
+    if (nxh % ZT32_KX) return KMM_ERR_UNSUPPORTED;
+    ZtmaMaps *M = ztma_maps(ctx);
+    if (!M) return KMM_ERR_NOMEM;
+    RET(pair_encode(ctx, M->fwd, false, r, yo, nout, nout, true));
+    const size_t smem = 1024 + sizeof(float2) * ((size_t)ZT32_KX * nz * ZTM_YT + (size_t)nout * mz * ZTM_YT * ZT32_KX +
+                                                 (size_t)ZT32_WARPS * 2 * mz) + 8 * sizeof(uint64_t);
+    const dim3 grid(nxh / ZT32_KX, (nyp + ZTM_YT - 1) / ZTM_YT);
+    const float rscale = (float)(1.0 / ((double)ctx->mx * (double)mz));
+#define ZTF32_LAUNCH(MM)                                                                                    \
+    do {                                                                                                    \
+        RET(kmm_smem_attr(ctx, (const void *)k_zf_tma32<MM>, smem));                                        \
+        k_zf_tma32<MM><<<grid, ZT32_WARPS * 32, smem, ctx->stream>>>(M->fwd.in, M->fwd.out, tw, nout, rscale, \
+                                                                     ctx->d_status);                        \
+    } while (0)
+    switch (mz) {
+    case 48: ZTF32_LAUNCH(48); break;
+    case 96: ZTF32_LAUNCH(96); break;
+    case 144: ZTF32_LAUNCH(144); break;
+    case 192: ZTF32_LAUNCH(192); break;
+    default: return KMM_ERR_UNSUPPORTED;
+    }
+#undef ZTF32_LAUNCH
+    return KMM_OK;
 }
