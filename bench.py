@@ -180,7 +180,7 @@ def fused_stage_bytes(p):
 # kernels of each fused stage (ncu names at 128x129x128, FP64)
 STAGE_KERNELS = {
     "column": ["k_bcol_scl<8,double2>", "k_bcol_omy<8,double2>", "k_bcol_v<8,double2>", "k_bcol_uw<8,double2>"],
-    "zfft_bwd": ["k_zb2<192,double2>"], "xphys": ["k_fx2<192,double2>"], "zfft_fwd": ["k_zf2<192,double2>"],
+    "zfft_bwd": ["k_zb_tma<192>"], "xphys": ["k_fx2<192,double2>"], "zfft_fwd": ["k_zf_tma<192>"],
     "post": ["k_bcol_bwd<8,double2>"],
 }
 
