@@ -9,6 +9,11 @@
 
 #define CB_WARPS 4   // column pairs per block
 #define CB_MINB 3    // blocks per SM the register budget is sized for
+// blocks per SM for kernels that spill at CB_MINB's register budget: FP64 scalar and u/w kernels
+// and the back kernel run faster with two blocks and no (or little) spilling; the FP32 forms of
+// the scalar and u/w kernels keep three
+template <typename C> struct CbMinB { static constexpr int fwd = sizeof(C) == 16 ? 2 : CB_MINB; };
+#define CB_MINB_BWD 2
 
 // phirhs on one column (solvers.f90:633-675)
 template <int K>
@@ -70,7 +75,7 @@ __device__ __forceinline__ bool bpair(BPair &P, int nz, int nzh, int nxh, const 
 
 // passive scalar (main_dns.f90:325-359): CN/AB2 right-hand side, Robin solve, norm, store; y-physical c, dc/dy
 template <int K, typename C>
-__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_scl(ColFwdArgs A, FusedTabs T, const double *__restrict__ rj,
+__global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::fwd) k_bcol_scl(ColFwdArgs A, FusedTabs T, const double *__restrict__ rj,
                                                             const C *__restrict__ tw) {
     constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
     constexpr unsigned FULL = 0xffffffffu;
@@ -246,7 +251,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_v(ColFwdArgs A,
 
 // veloc (solvers.f90:1576-1659) from the new v and omega_y; y-physical u, du/dy, w, dw/dy
 template <int K, typename C>
-__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_uw(ColFwdArgs A, const C *__restrict__ tw) {
+__global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::fwd) k_bcol_uw(ColFwdArgs A, const C *__restrict__ tw) {
     constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ double2 sm[];
@@ -308,7 +313,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_uw(ColFwdArgs A
 }
 
 template <int K, typename C>
-__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_bwd(ColBwdArgs A, const C *__restrict__ tw) {
+__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB_BWD) k_bcol_bwd(ColBwdArgs A, const C *__restrict__ tw) {
     constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ double2 sm[];
