@@ -18,6 +18,7 @@
 #include <math.h>
 
 #include "kmm_internal.cuh"
+#include "kmm_fft.cuh"
 
 #define MAXIO 64
 
@@ -111,6 +112,107 @@ __device__ __forceinline__ void atomic_max_pos(double *addr, double v) {
     atomicMax((unsigned long long *)addr, (unsigned long long)__double_as_longlong(v));
 }
 
+// the pointwise terms of one 3/2-grid point (solvers.f90:2885-3063): u x omega, -u.grad(c) and
+// its sources, the polymer source / stress / qp terms, CFL, immersed-boundary forces and dPdx,
+// the tracer / inertial-particle copies; `in(slot)` is the physical value of an input slot here
+template <typename IN_T>
+__device__ __forceinline__ void xphys_point(const IN_T &in, const PhysArgs &A, const Save3D &sv, int y, int z, int k,
+                                            int nyp, int mz, int mx, double sg, double *__restrict__ po,
+                                            double *__restrict__ drag, double *__restrict__ up3,
+                                            double *__restrict__ vp3, double *__restrict__ wp3,
+                                            const int *__restrict__ imatrix, double *__restrict__ fxi,
+                                            double *__restrict__ fyi, double *__restrict__ fzi,
+                                            const double *__restrict__ scsource, double &cmax, double &umx) {
+#define IN(s) in(s)
+    const double up = IN(S_U), vp = IN(S_V), wp = IN(S_W);
+    const double wxp = IN(S_WX), wyp = IN(S_WY), wzp = IN(S_WZ);
+    double out[O_NSLOT];
+    out[O_H1] = vp * wzp - wp * wyp;
+    out[O_H2] = -up * wzp + wp * wxp;
+    out[O_H3] = up * wyp - vp * wxp;
+    if (A.scalar) out[O_SC] = -(up * IN(S_CX) + vp * IN(S_CY) + wp * IN(S_CZ));
+    if (A.polymer) {
+        double c[9], gu[9];
+#pragma unroll
+        for (int m = 0; m < 9; ++m) { c[m] = IN(S_C11 + m); gu[m] = IN(S_U11 + m); }
+        const double c11 = c[0], c12 = c[1], c13 = c[2], c21 = c[3], c22 = c[4], c23 = c[5], c31 = c[6], c32 = c[7], c33 = c[8];
+        const double u11 = gu[0], u12 = gu[1], u13 = gu[2], u21 = gu[3], u22 = gu[4], u23 = gu[5], u31 = gu[6], u32 = gu[7], u33 = gu[8];
+#define DC(ij, kk) IN(S_DC111 + 3 * (ij) + (kk))
+        out[O_C11N + 0] = c11 * u11 + c12 * u12 + c13 * u13 + c11 * u11 + c21 * u12 + c31 * u13 - (up * DC(0, 0) + vp * DC(0, 1) + wp * DC(0, 2));
+        out[O_C11N + 1] = c11 * u21 + c12 * u22 + c13 * u23 + c12 * u11 + c22 * u12 + c32 * u13 - (up * DC(1, 0) + vp * DC(1, 1) + wp * DC(1, 2));
+        out[O_C11N + 2] = c11 * u31 + c12 * u32 + c13 * u33 + c13 * u11 + c23 * u12 + c33 * u13 - (up * DC(2, 0) + vp * DC(2, 1) + wp * DC(2, 2));
+        out[O_C11N + 3] = c21 * u21 + c22 * u22 + c23 * u23 + c12 * u21 + c22 * u22 + c32 * u23 - (up * DC(4, 0) + vp * DC(4, 1) + wp * DC(4, 2));
+        out[O_C11N + 4] = c21 * u31 + c22 * u32 + c23 * u33 + c13 * u21 + c23 * u22 + c33 * u23 - (up * DC(5, 0) + vp * DC(5, 1) + wp * DC(5, 2));
+        out[O_C11N + 5] = c31 * u31 + c32 * u32 + c33 * u33 + c13 * u31 + c23 * u32 + c33 * u33 - (up * DC(8, 0) + vp * DC(8, 1) + wp * DC(8, 2));
+#undef DC
+        const double trp = c11 + c22 + c33;
+        const double s6[6] = {c11, c12, c13, c22, c23, c33};
+        const double pf = (A.zl2 - 3.0) / (A.zl2 - trp);
+#pragma unroll
+        for (int m = 0; m < 6; ++m) out[O_STR11N + m] = A.ipeter == 0 ? s6[m] : pf * s6[m];
+        out[O_STR11N + 0] -= 1.0;
+        out[O_STR11N + 3] -= 1.0;
+        out[O_STR11N + 5] -= 1.0;
+        double beta_poly = A.qbeta;
+        if (A.itarget == 1) {
+            const double sc = fabs(A.scalar ? IN(S_SC) : 0.0);
+            if (A.alpha_poly * sc < 18.0) beta_poly = exp(-A.alpha_poly * sc);
+        } else if (A.itarget == 2) {
+            const double sc = fabs(A.scalar ? IN(S_SC) : 0.0);
+            beta_poly = 1.0 / (A.alpha_poly * sc + 1.0);
+        }
+        const double zbeta1 = (1.0 - beta_poly) / (A.re * beta_poly * A.tpoly);
+#pragma unroll
+        for (int m = 0; m < 6; ++m) out[O_QP11 + m] = zbeta1 * out[O_STR11N + m];
+    }
+    const double cflcheck = (fabs(up) / A.delxm + fabs(vp) / sg + fabs(wp) / A.delzm) * A.dt;
+    cmax = fmax(cmax, cflcheck);
+    if (cflcheck != cflcheck) cmax = cflcheck;
+    umx = fmax(umx, fabs(up));
+    // immersed boundary (solvers.f90:2996-3059); fxintg etc. in [y][z][x] layout
+    const size_t g3 = ((size_t)y * mz + z) * mx + k;
+    double dx = 0.0, dy = 0.0, dz = 0.0;
+    if (A.ib_any) {
+        const int t = imatrix[g3];
+        if (t == 1 || (t == 4 && A.it <= A.perturbtime)) {
+            const double fx = fxi[g3] + up, fy = fyi[g3] + vp, fz = fzi[g3] + wp;
+            fxi[g3] = fx; fyi[g3] = fy; fzi[g3] = fz;
+            dx = (-A.ugain * up) - A.gain * fx;
+            dy = (-A.ugain * vp) - A.gain * fy;
+            dz = (-A.ugain * wp) - A.gain * fz;
+        } else if (t == 3) {
+            const double fz = fzi[g3] + wp;
+            fzi[g3] = fz;
+            dz = -A.ugain * wp - A.gain * fz;
+        } else if (t == 11) {
+            dx = 1.0;
+        } else if (t == 0 && A.flow_select == 1) {
+            out[O_H1] = out[O_H1] - A.dPdx;
+        }
+        drag[0 * (size_t)nyp * mz * mx + g3] = dx;
+        drag[1 * (size_t)nyp * mz * mx + g3] = dy;
+        drag[2 * (size_t)nyp * mz * mx + g3] = dz;
+    } else if (A.flow_select == 1) {
+        out[O_H1] = out[O_H1] - A.dPdx;
+    }
+    if (A.scalar) {
+        if (A.scl_flag >= 2) out[O_SC] = out[O_SC] + scsource[g3] / A.dt;
+        if (A.scalar_q != 0.0) out[O_SC] = out[O_SC] + A.scalar_q;
+    }
+    for (int o = 0; o < O_NSLOT; ++o) {
+        const int s = A.slot_of_out[o];
+        if (s >= 0) po[(size_t)s * nyp * mz * mx + g3] = out[o];
+    }
+    if (A.save_uvw) { up3[g3] = up; vp3[g3] = vp; wp3[g3] = wp; }
+    if (sv.p[0]) {
+#pragma unroll
+        for (int m = 0; m < 12; ++m) sv.p[m][g3] = IN(S_WX + m);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) sv.p[12 + m][g3] = IN(S_LU + m);
+    }
+#undef IN
+}
+
 #define XZB 2
 __global__ void __launch_bounds__(256) k_xphys(const double2 *__restrict__ q, double *__restrict__ po,
                                                double *__restrict__ drag, double *__restrict__ up3,
@@ -161,98 +263,12 @@ __global__ void __launch_bounds__(256) k_xphys(const double2 *__restrict__ q, do
     // pointwise terms, solvers.f90:2885-3063
     double cmax = 0.0, umx = 0.0;
     const double sg = seght[y];
-#define IN(s) phys[((size_t)A.slot_of_in[s] * XZB + rr) * mx + k]
     for (int e = threadIdx.x; e < nzr * mx; e += blockDim.x) {
         const int rr = e / mx, k = e - rr * mx;
-        const int z = z0 + rr;
-        const double up = IN(S_U), vp = IN(S_V), wp = IN(S_W);
-        const double wxp = IN(S_WX), wyp = IN(S_WY), wzp = IN(S_WZ);
-        double out[O_NSLOT];
-        out[O_H1] = vp * wzp - wp * wyp;
-        out[O_H2] = -up * wzp + wp * wxp;
-        out[O_H3] = up * wyp - vp * wxp;
-        if (A.scalar) out[O_SC] = -(up * IN(S_CX) + vp * IN(S_CY) + wp * IN(S_CZ));
-        if (A.polymer) {
-            double c[9], gu[9];
-#pragma unroll
-            for (int m = 0; m < 9; ++m) { c[m] = IN(S_C11 + m); gu[m] = IN(S_U11 + m); }
-            const double c11 = c[0], c12 = c[1], c13 = c[2], c21 = c[3], c22 = c[4], c23 = c[5], c31 = c[6], c32 = c[7], c33 = c[8];
-            const double u11 = gu[0], u12 = gu[1], u13 = gu[2], u21 = gu[3], u22 = gu[4], u23 = gu[5], u31 = gu[6], u32 = gu[7], u33 = gu[8];
-#define DC(ij, kk) IN(S_DC111 + 3 * (ij) + (kk))
-            out[O_C11N + 0] = c11 * u11 + c12 * u12 + c13 * u13 + c11 * u11 + c21 * u12 + c31 * u13 - (up * DC(0, 0) + vp * DC(0, 1) + wp * DC(0, 2));
-            out[O_C11N + 1] = c11 * u21 + c12 * u22 + c13 * u23 + c12 * u11 + c22 * u12 + c32 * u13 - (up * DC(1, 0) + vp * DC(1, 1) + wp * DC(1, 2));
-            out[O_C11N + 2] = c11 * u31 + c12 * u32 + c13 * u33 + c13 * u11 + c23 * u12 + c33 * u13 - (up * DC(2, 0) + vp * DC(2, 1) + wp * DC(2, 2));
-            out[O_C11N + 3] = c21 * u21 + c22 * u22 + c23 * u23 + c12 * u21 + c22 * u22 + c32 * u23 - (up * DC(4, 0) + vp * DC(4, 1) + wp * DC(4, 2));
-            out[O_C11N + 4] = c21 * u31 + c22 * u32 + c23 * u33 + c13 * u21 + c23 * u22 + c33 * u23 - (up * DC(5, 0) + vp * DC(5, 1) + wp * DC(5, 2));
-            out[O_C11N + 5] = c31 * u31 + c32 * u32 + c33 * u33 + c13 * u31 + c23 * u32 + c33 * u33 - (up * DC(8, 0) + vp * DC(8, 1) + wp * DC(8, 2));
-#undef DC
-            const double trp = c11 + c22 + c33;
-            const double s6[6] = {c11, c12, c13, c22, c23, c33};
-            const double pf = (A.zl2 - 3.0) / (A.zl2 - trp);
-#pragma unroll
-            for (int m = 0; m < 6; ++m) out[O_STR11N + m] = A.ipeter == 0 ? s6[m] : pf * s6[m];
-            out[O_STR11N + 0] -= 1.0;
-            out[O_STR11N + 3] -= 1.0;
-            out[O_STR11N + 5] -= 1.0;
-            double beta_poly = A.qbeta;
-            if (A.itarget == 1) {
-                const double sc = fabs(A.scalar ? IN(S_SC) : 0.0);
-                if (A.alpha_poly * sc < 18.0) beta_poly = exp(-A.alpha_poly * sc);
-            } else if (A.itarget == 2) {
-                const double sc = fabs(A.scalar ? IN(S_SC) : 0.0);
-                beta_poly = 1.0 / (A.alpha_poly * sc + 1.0);
-            }
-            const double zbeta1 = (1.0 - beta_poly) / (A.re * beta_poly * A.tpoly);
-#pragma unroll
-            for (int m = 0; m < 6; ++m) out[O_QP11 + m] = zbeta1 * out[O_STR11N + m];
-        }
-        const double cflcheck = (fabs(up) / A.delxm + fabs(vp) / sg + fabs(wp) / A.delzm) * A.dt;
-        cmax = fmax(cmax, cflcheck);
-        if (cflcheck != cflcheck) cmax = cflcheck;
-        umx = fmax(umx, fabs(up));
-        // immersed boundary (solvers.f90:2996-3059); fxintg etc. in [y][z][x] layout
-        const size_t g3 = ((size_t)y * mz + z) * mx + k;
-        double dx = 0.0, dy = 0.0, dz = 0.0;
-        if (A.ib_any) {
-            const int t = imatrix[g3];
-            if (t == 1 || (t == 4 && A.it <= A.perturbtime)) {
-                const double fx = fxi[g3] + up, fy = fyi[g3] + vp, fz = fzi[g3] + wp;
-                fxi[g3] = fx; fyi[g3] = fy; fzi[g3] = fz;
-                dx = (-A.ugain * up) - A.gain * fx;
-                dy = (-A.ugain * vp) - A.gain * fy;
-                dz = (-A.ugain * wp) - A.gain * fz;
-            } else if (t == 3) {
-                const double fz = fzi[g3] + wp;
-                fzi[g3] = fz;
-                dz = -A.ugain * wp - A.gain * fz;
-            } else if (t == 11) {
-                dx = 1.0;
-            } else if (t == 0 && A.flow_select == 1) {
-                out[O_H1] = out[O_H1] - A.dPdx;
-            }
-            drag[0 * (size_t)nyp * mz * mx + g3] = dx;
-            drag[1 * (size_t)nyp * mz * mx + g3] = dy;
-            drag[2 * (size_t)nyp * mz * mx + g3] = dz;
-        } else if (A.flow_select == 1) {
-            out[O_H1] = out[O_H1] - A.dPdx;
-        }
-        if (A.scalar) {
-            if (A.scl_flag >= 2) out[O_SC] = out[O_SC] + scsource[g3] / A.dt;
-            if (A.scalar_q != 0.0) out[O_SC] = out[O_SC] + A.scalar_q;
-        }
-        for (int o = 0; o < O_NSLOT; ++o) {
-            const int s = A.slot_of_out[o];
-            if (s >= 0) po[(size_t)s * nyp * mz * mx + g3] = out[o];
-        }
-        if (A.save_uvw) { up3[g3] = up; vp3[g3] = vp; wp3[g3] = wp; }
-        if (sv.p[0]) {
-#pragma unroll
-            for (int m = 0; m < 12; ++m) sv.p[m][g3] = IN(S_WX + m);
-#pragma unroll
-            for (int m = 0; m < 3; ++m) sv.p[12 + m][g3] = IN(S_LU + m);
-        }
+        auto in = [&](int sl) { return phys[((size_t)A.slot_of_in[sl] * XZB + rr) * mx + k]; };
+        xphys_point(in, A, sv, y, z0 + rr, k, nyp, mz, mx, sg, po, drag, up3, vp3, wp3, imatrix, fxi, fyi, fzi, scsource,
+                    cmax, umx);
     }
-#undef IN
     // block reductions of the CFL number and |u| for this plane
     __shared__ double red[2][32];
     for (int off = 16; off; off >>= 1) {
@@ -271,6 +287,112 @@ __global__ void __launch_bounds__(256) k_xphys(const double2 *__restrict__ q, do
         }
         atomic_max_pos(&cfl[y], cmax);
         atomic_max_pos(&umax[y], umx);
+    }
+}
+
+// 3'. the same x stage for the compiled lengths MX = 48, 96, 144, 192 (nx = 32 .. 128): one block
+// per (y, z) row, XW warps.  Each warp takes field pairs in turn: the Hermitian extension of A + iB
+// (modes nxh .. mx - nxh not carried; c2r ignores Im of the DC mode) through the compile-time
+// warp FFT into the row's physical table in shared memory; then the block evaluates the pointwise
+// terms.  The generic k_xphys tiles two rows per block and transforms them with the runtime
+// block FFT; this form keeps more independent FFTs in flight per SM.
+#define XW 4
+template <int MX>
+__global__ void __launch_bounds__(XW * 32) k_xphys2(const double2 *__restrict__ q, double *__restrict__ po,
+                                                    double *__restrict__ drag, double *__restrict__ up3,
+                                                    double *__restrict__ vp3, double *__restrict__ wp3,
+                                                    const int *__restrict__ imatrix, double *__restrict__ fxi,
+                                                    double *__restrict__ fyi, double *__restrict__ fzi,
+                                                    const double *__restrict__ scsource,
+                                                    const double *__restrict__ seght, double *__restrict__ cfl,
+                                                    double *__restrict__ umax, const double2 *__restrict__ tw,
+                                                    PhysArgs A, Save3D sv, int nyp, int mz) {
+    constexpr int NXH = MX / 3, HX = MX / 2;
+    extern __shared__ double2 sm[];
+    double *phys = reinterpret_cast<double *>(sm);                       // [nin][MX]
+    double2 *fab = reinterpret_cast<double2 *>(phys + (size_t)A.nin * MX);  // per warp: a, b [MX]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int z = blockIdx.x, y = blockIdx.y;
+    double2 *a = fab + (size_t)warp * 2 * MX, *b = a + MX;
+    const int npairs = (A.nin + 1) / 2;
+    for (int pr = warp; pr < npairs; pr += XW) {
+        const int f = 2 * pr, g = f + 1 < A.nin ? f + 1 : -1;
+        const double2 *qa = q + (((size_t)f * nyp + y) * mz + z) * NXH;
+        const double2 *qb = g >= 0 ? q + (((size_t)g * nyp + y) * mz + z) * NXH : qa;
+        for (int k = lane; k < MX; k += 32) {
+            const int kk = k <= HX ? k : MX - k;   // source mode
+            double2 A_ = make_double2(0.0, 0.0), B_ = make_double2(0.0, 0.0);
+            if (kk < NXH) {
+                A_ = qa[kk];
+                if (g >= 0) B_ = qb[kk];
+            }
+            if (k == 0 || k == HX) { A_.y = 0.0; B_.y = 0.0; }
+            a[swz<double2>(k)] = k <= HX ? make_double2(A_.x - B_.y, A_.y + B_.x)     // A + iB
+                                         : make_double2(A_.x + B_.y, -A_.y + B_.x);   // conj(A) + i conj(B)
+        }
+        __syncwarp();
+        const double2 *r = fft_warp_ct<double2, MX, +1, 1, true>(a, b, tw);
+        for (int x = lane; x < MX; x += 32) {
+            const double2 v = r[swz<double2>(x)];
+            phys[(size_t)f * MX + x] = v.x;
+            if (g >= 0) phys[(size_t)g * MX + x] = v.y;
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    double cmax = 0.0, umx = 0.0;
+    const double sg = seght[y];
+    for (int k = threadIdx.x; k < MX; k += blockDim.x) {
+        auto in = [&](int sl) { return phys[(size_t)A.slot_of_in[sl] * MX + k]; };
+        xphys_point(in, A, sv, y, z, k, nyp, mz, MX, sg, po, drag, up3, vp3, wp3, imatrix, fxi, fyi, fzi, scsource, cmax,
+                    umx);
+    }
+    __shared__ double red[2][XW];
+    for (int off = 16; off; off >>= 1) {
+        const double c2 = __shfl_down_sync(0xffffffffu, cmax, off);
+        const double u2 = __shfl_down_sync(0xffffffffu, umx, off);
+        cmax = (c2 != c2) ? c2 : fmax(cmax, c2);
+        umx = fmax(umx, u2);
+    }
+    if (lane == 0) { red[0][warp] = cmax; red[1][warp] = umx; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < XW; ++w) {
+            cmax = (red[0][w] != red[0][w]) ? red[0][w] : fmax(cmax, red[0][w]);
+            umx = fmax(umx, red[1][w]);
+        }
+        atomic_max_pos(&cfl[y], cmax);
+        atomic_max_pos(&umax[y], umx);
+    }
+}
+
+// 5'. r2c along x for the compiled lengths: one block per (y, z) row, warps over output pairs
+// (two real rows packed as one complex FFT, split by Hermitian symmetry, modes kx < nxh kept)
+template <int MX>
+__global__ void __launch_bounds__(XW * 32) k_xfwd2(const double *__restrict__ po, double2 *__restrict__ q,
+                                                   const double2 *__restrict__ tw, int nout, int nyp, int mz) {
+    constexpr int NXH = MX / 3;
+    extern __shared__ double2 sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int z = blockIdx.x, y = blockIdx.y;
+    double2 *a = sm + (size_t)warp * 2 * MX, *b = a + MX;
+    const size_t n3 = (size_t)nyp * mz * MX, g3 = ((size_t)y * mz + z) * MX;
+    for (int pr = warp; pr < (nout + 1) / 2; pr += XW) {
+        const int o = 2 * pr, g = o + 1 < nout ? o + 1 : -1;
+        for (int x = lane; x < MX; x += 32)
+            a[swz<double2>(x)] = make_double2(po[(size_t)o * n3 + g3 + x], g >= 0 ? po[(size_t)g * n3 + g3 + x] : 0.0);
+        __syncwarp();
+        const double2 *r = fft_warp_ct<double2, MX, -1, 1, true>(a, b, tw);
+        for (int k = lane; k < NXH; k += 32) {
+            const double2 Z = r[swz<double2>(k)];
+            const double2 Zc = cconj(r[swz<double2>(k == 0 ? 0 : MX - k)]);
+            q[(((size_t)o * nyp + y) * mz + z) * NXH + k] = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
+            if (g >= 0) {
+                const double2 dd = csub(Z, Zc);   // -i/2 (Z - Zc)
+                q[(((size_t)g * nyp + y) * mz + z) * NXH + k] = make_double2(0.5 * dd.y, -0.5 * dd.x);
+            }
+        }
+        __syncwarp();
     }
 }
 
@@ -676,9 +798,26 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     }
     if (!fast_done) {
         kmm_tic(ctx);
-        k_xphys<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_x, ctx->stream>>>(
-            ctx->q_in, ctx->po, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl,
-            ctx->d_umax, ctx->pmx, A, sv, nyp, mz, mx, nxh);
+        const size_t sm_x2 = sizeof(double) * (size_t)nin * mx + sizeof(double2) * 2 * XW * (size_t)mx;
+#define XP2(MM)                                                                                                  \
+    do {                                                                                                         \
+        RET(kmm_smem_attr(ctx, (const void *)k_xphys2<MM>, sm_x2));                                              \
+        k_xphys2<MM><<<dim3(mz, nyp), XW * 32, sm_x2, ctx->stream>>>(                                             \
+            ctx->q_in, ctx->po, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl, \
+            ctx->d_umax, ctx->wmx.tw, A, sv, nyp, mz);                                                           \
+    } while (0)
+        switch (mx) {
+        case 48: XP2(48); break;
+        case 96: XP2(96); break;
+        case 144: XP2(144); break;
+        case 192: XP2(192); break;
+        default:
+            k_xphys<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_x, ctx->stream>>>(
+                ctx->q_in, ctx->po, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl,
+                ctx->d_umax, ctx->pmx, A, sv, nyp, mz, mx, nxh);
+            break;
+        }
+#undef XP2
         CKL();
         kmm_toc(ctx, KMM_STAGE_XPHYS);
         if (ib_any && ctx->kmaxsurf > 0) {
@@ -689,8 +828,23 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
             CKL();
         }
         kmm_tic(ctx);
-        k_xfwd<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_xf, ctx->stream>>>(ctx->po, ctx->q_out, ctx->pmx, nout, nyp, mz,
-                                                                             mx, nxh);
+        const size_t sm_xf2 = sizeof(double2) * 2 * XW * (size_t)mx;
+#define XF2(MM)                                                                                                 \
+    do {                                                                                                        \
+        RET(kmm_smem_attr(ctx, (const void *)k_xfwd2<MM>, sm_xf2));                                             \
+        k_xfwd2<MM><<<dim3(mz, nyp), XW * 32, sm_xf2, ctx->stream>>>(ctx->po, ctx->q_out, ctx->wmx.tw, nout, nyp, mz); \
+    } while (0)
+        switch (mx) {
+        case 48: XF2(48); break;
+        case 96: XF2(96); break;
+        case 144: XF2(144); break;
+        case 192: XF2(192); break;
+        default:
+            k_xfwd<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_xf, ctx->stream>>>(ctx->po, ctx->q_out, ctx->pmx, nout, nyp,
+                                                                                 mz, mx, nxh);
+            break;
+        }
+#undef XF2
         CKL();
         kmm_toc(ctx, KMM_STAGE_XFWD);
     }
