@@ -463,6 +463,65 @@ int kmm_colblk_fwd(kmm_ctx *ctx, const ColFwdArgs &A, const FusedTabs &T, const 
 #undef BF
 }
 
+// ---------------------------------------------------------------------------
+// The routine path's solve (Dirichlet, solvers.f90:174-553) and penta (Robin, 680-1061) with
+// ib = 0 over a whole field in the blocked layout: one warp per (kz, -kz) pair, the boundary
+// values from bctop / bcbot, the configuration's tables from the per-context cache.
+// ---------------------------------------------------------------------------
+template <int K>
+__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bsolve(double2 *u, const double2 *__restrict__ gtop,
+                                                                  const double2 *__restrict__ gbot, const double *td,
+                                                                  const double *te, const double *tb1,
+                                                                  const double *tb2, const double *tf,
+                                                                  const double *__restrict__ rj,
+                                                                  const double *__restrict__ wavx,
+                                                                  const double *__restrict__ wavz, int nz, int nzh,
+                                                                  int nxh, double g, int robin, double c0) {
+    constexpr int NYP = 16 * K + 1;
+    constexpr unsigned FULL = 0xffffffffu;
+    BPair P;
+    if (!bpair<K>(P, nz, nzh, nxh, wavx, wavz)) return;
+    TauTab T;
+    T.td = td + (size_t)P.tcol * NYP;
+    T.te = te + (size_t)P.tcol * NYP;
+    T.tb1 = tb1 + (size_t)P.tcol * NYP;
+    T.tb2 = tb2 + (size_t)P.tcol * NYP;
+    T.tf = tf + (size_t)P.tcol * 4;
+    BCol<K> s;
+    bload<K>(s, u + P.off);
+    const double2 gt = gtop[P.col], gb = gbot[P.col];
+    if (robin) bsolve_robin<K>(s, T, gt, gb, P.w2 + g, c0, rj, FULL);
+    else bsolve_dirichlet<K>(s, T, gt, gb, P.w2 + g, c0, rj, FULL);
+    bstore<K>(u + P.off, s);
+}
+
+int kmm_colblk_solve(kmm_ctx *ctx, double2 *u, double g, int robin, double at, double bt, double ab, double bb,
+                     const double2 *gt, const double2 *gb) {
+    const int K = colblk_k(ctx);
+    if (!K || !ctx->use_colblk) return KMM_ERR_UNSUPPORTED;
+    const double *tb[5], *rj = NULL;
+    const int st = kmm_tau_tabset(ctx, g, robin, at, bt, ab, bb, tb, &rj);
+    if (st != KMM_OK) return st;
+    const int npairs = ctx->nxh * (ctx->nz / 2);
+    const int nblk = (npairs + CB_WARPS - 1) / CB_WARPS;
+#define BS(KK)                                                                                                      \
+    do {                                                                                                            \
+        k_bsolve<KK><<<nblk, CB_WARPS * 32, 0, ctx->stream>>>(u, gt, gb, tb[0], tb[1], tb[2], tb[3], tb[4], rj,       \
+                                                              ctx->d_wavx, ctx->d_wavz, ctx->nz, ctx->nzh, ctx->nxh, g, \
+                                                              robin, ctx->h_c[0]);                                  \
+        CKL();                                                                                                      \
+        return KMM_OK;                                                                                              \
+    } while (0)
+    switch (K) {
+    case 2: BS(2);
+    case 4: BS(4);
+    case 6: BS(6);
+    case 8: BS(8);
+    default: return KMM_ERR_UNSUPPORTED;
+    }
+#undef BS
+}
+
 int kmm_colblk_bwd(kmm_ctx *ctx, const ColBwdArgs &B, const void *tw, bool fp32) {
     const int K = colblk_k(ctx);
     if (!K) return KMM_ERR_UNSUPPORTED;

@@ -360,6 +360,10 @@ __global__ void __launch_bounds__(TPB) k_solve(double2 *__restrict__ u, const do
 }
 
 int kmm_internal_solve(kmm_ctx *ctx, double2 *u, double g, int ib, const double2 *bct, const double2 *bcb) {
+    if (ib == 0) {   // blocked column kernels with cached tables where they are compiled
+        const int st = kmm_colblk_solve(ctx, u, g, 0, 0.0, 0.0, 0.0, 0.0, bct, bcb);
+        if (st != KMM_ERR_UNSUPPORTED) return st;
+    }
     const int ncols = ctx->nz * ctx->nxh;
     const size_t smem = tile_smem(ctx->nyp, 1) + sizeof(double) * TILE * (size_t)(ctx->nyhp + 1);
     RET(kmm_smem_attr(ctx, (const void *)k_solve, smem));
@@ -477,6 +481,10 @@ __global__ void __launch_bounds__(TPB) k_penta(double2 *__restrict__ u, const do
 
 int kmm_internal_penta(kmm_ctx *ctx, double2 *u, double g, int ib, double at, double bt, double ab, double bb,
                        const double2 *gt, const double2 *gb) {
+    if (ib == 0) {   // blocked column kernels with cached tables where they are compiled
+        const int st = kmm_colblk_solve(ctx, u, g, 1, at, bt, ab, bb, gt, gb);
+        if (st != KMM_ERR_UNSUPPORTED) return st;
+    }
     const int ncols = ctx->nz * ctx->nxh;
     const size_t smem = tile_smem(ctx->nyp, 1) + sizeof(double) * TILE * 2 * (size_t)(ctx->nyhp + 1);
     RET(kmm_smem_attr(ctx, (const void *)k_penta, smem));

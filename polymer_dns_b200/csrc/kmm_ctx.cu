@@ -330,6 +330,7 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
     kmm_graph_release(ctx);
     kmm_fused_release(ctx);
     kmm_ztma_release(ctx);
+    kmm_tau_release(ctx);
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
     if (ctx->po) cudaFree(ctx->po);
     if (ctx->drag) cudaFree(ctx->drag);

@@ -173,6 +173,74 @@ static int build_tables(kmm_ctx *ctx) {
     return KMM_OK;
 }
 
+// tau tables of the routine path's solve / penta calls: one set per (g, boundary-condition)
+// configuration met, built on first use with the same recurrences as the fused step's and kept
+// for the context's lifetime (a run meets a handful: v's two solves, omega_y, the scalar and the
+// polymer components)
+#define KMM_TAU_SETS 12
+struct TauCache {
+    int n;
+    TabCfg cfg[KMM_TAU_SETS];
+    double *tabs[KMM_TAU_SETS][5];   // td, te, tb1, tb2, tf
+    double *rj;
+};
+
+int kmm_tau_tabset(kmm_ctx *ctx, double g, int robin, double at, double bt, double ab, double bb, const double **tabs,
+                   const double **rj) {
+    TauCache *C = (TauCache *)ctx->tauc;
+    if (!C) {
+        C = (TauCache *)calloc(1, sizeof(TauCache));
+        if (!C) return KMM_ERR_NOMEM;
+        ctx->tauc = C;
+        const int nyp = ctx->nyp;
+        double *h = (double *)calloc(3 * (size_t)nyp, sizeof(double));
+        for (int j = 2; j < nyp; ++j) {
+            h[j] = 1.0 / (double)(4 * j * (j - 1));
+            h[nyp + j] = 1.0 / (double)(2 * (j * j - 1));
+            h[2 * nyp + j] = 1.0 / (double)(4 * j * (j + 1));
+        }
+        cudaError_t e = cudaMalloc(&C->rj, sizeof(double) * 3 * nyp);
+        if (e == cudaSuccess) e = cudaMemcpy(C->rj, h, sizeof(double) * 3 * nyp, cudaMemcpyHostToDevice);
+        free(h);
+        CK(e);
+    }
+    const TabCfg want = {g, robin, robin ? at : 0.0, robin ? bt : 0.0, robin ? ab : 0.0, robin ? bb : 0.0, 1.0};
+    int s = -1;
+    for (int i = 0; i < C->n && s < 0; ++i) {
+        const TabCfg &c = C->cfg[i];
+        if (c.g == want.g && c.robin == want.robin && c.at == want.at && c.bt == want.bt && c.ab == want.ab &&
+            c.bb == want.bb)
+            s = i;
+    }
+    if (s < 0) {
+        if (C->n == KMM_TAU_SETS) return KMM_ERR_UNSUPPORTED;   // the caller keeps the table-free kernels
+        s = C->n;
+        const int ncols = ctx->nz * ctx->nxh;
+        const size_t n = (size_t)ncols * ctx->nyp;
+        for (int a = 0; a < 4; ++a) CK(cudaMalloc(&C->tabs[s][a], sizeof(double) * n));
+        CK(cudaMalloc(&C->tabs[s][4], sizeof(double) * 4 * ncols));
+        k_tau_tables<<<(ncols + 127) / 128, 128, 0, ctx->stream>>>(C->tabs[s][0], C->tabs[s][1], C->tabs[s][2],
+                                                                  C->tabs[s][3], C->tabs[s][4], want, ctx->d_wavx,
+                                                                  ctx->d_wavz, ncols, ctx->nz, ctx->nyp, ctx->dyde);
+        CKL();
+        C->cfg[s] = want;
+        C->n = s + 1;
+    }
+    for (int a = 0; a < 5; ++a) tabs[a] = C->tabs[s][a];
+    *rj = C->rj;
+    return KMM_OK;
+}
+
+void kmm_tau_release(kmm_ctx *ctx) {
+    TauCache *C = (TauCache *)ctx->tauc;
+    if (!C) return;
+    for (int i = 0; i < C->n; ++i)
+        for (int a = 0; a < 5; ++a) cudaFree(C->tabs[i][a]);
+    cudaFree(C->rj);
+    free(C);
+    ctx->tauc = NULL;
+}
+
 void kmm_fused_release(kmm_ctx *ctx) {
     KmmFused *F = ctx->fused;
     if (!F) return;

@@ -105,6 +105,7 @@ struct kmm_ctx {
     void *g_fn0;      // the FN buffer of parity 0
     int use_ztma;     // FP64 inverse z transform through TMA tile copies (default 1)
     void *ztma;       // its cached tensor maps (kmm_ztma.cu)
+    void *tauc;       // tau tables of the routine solves' (g, boundary-condition) configurations (kmm_fused.cu)
 };
 
 void kmm_fused_release(kmm_ctx *ctx);
@@ -141,6 +142,14 @@ int kmm_internal_cderiv(kmm_ctx *ctx, const double2 *f, double2 *df);
 int kmm_internal_norm(kmm_ctx *ctx, double2 *a);
 int kmm_internal_wallderiv(kmm_ctx *ctx, const double2 *f, int order, int wall, double2 *out, int iy);
 int kmm_internal_solve(kmm_ctx *ctx, double2 *u, double g, int ib, const double2 *bct, const double2 *bcb);
+// the routine solve / penta with the blocked column kernels (ny = 32, 64, 96, 128; ib = 0);
+// KMM_ERR_UNSUPPORTED where they do not apply (kmm_colblk.cu)
+int kmm_colblk_solve(kmm_ctx *ctx, double2 *u, double g, int robin, double at, double bt, double ab, double bb,
+                     const double2 *gt, const double2 *gb);
+// the cached tau tables of one configuration and the tau-row reciprocals (kmm_fused.cu)
+int kmm_tau_tabset(kmm_ctx *ctx, double g, int robin, double at, double bt, double ab, double bb, const double **tabs,
+                   const double **rj);
+void kmm_tau_release(kmm_ctx *ctx);
 int kmm_internal_penta(kmm_ctx *ctx, double2 *u, double g, int ib, double at, double bt, double ab, double bb,
                        const double2 *gt, const double2 *gb);
 int kmm_internal_axpy_spec(kmm_ctx *ctx, double2 *y, const double2 *x, double a);
