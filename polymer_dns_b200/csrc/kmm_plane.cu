@@ -25,6 +25,35 @@
 struct FieldPtrs { const double2 *p[MAXIO]; };
 struct FieldPtrsW { double2 *p[MAXIO]; };
 
+// batched FFT of NB sequences of length N lying N apart in a (b: scratch of the same size) by the
+// block's 8 warps, NB / 8 sequences each, with the compile-time warp FFT; returns the buffer
+// holding the result, visible to the whole block
+template <int N, int S, int NB>
+__device__ __forceinline__ double2 *fft_block_ct(double2 *a, double2 *b, const double2 *tw) {
+    constexpr int NQ = NB / 8;
+    static_assert(NB % 8 == 0, "8 warps share the sequences");
+    const size_t w = (size_t)(threadIdx.x >> 5) * NQ * N;
+    double2 *r = fft_warp_ct<double2, N, S, NQ, false>(a + w, b + w, tw);
+    __syncthreads();
+    return r - w;
+}
+
+// the same for the compiled lengths (the 3/2 grids of 32 .. 128 and 2 ny for ny = 32 .. 128), the
+// runtime block FFT for any other; blockDim = 256
+template <int S, int NB>
+__device__ double2 *fft_block(const DevPlan &P, double2 *a, double2 *b, int n) {
+    switch (n) {
+    case 48: return fft_block_ct<48, S, NB>(a, b, P.tw);
+    case 64: return fft_block_ct<64, S, NB>(a, b, P.tw);
+    case 96: return fft_block_ct<96, S, NB>(a, b, P.tw);
+    case 128: return fft_block_ct<128, S, NB>(a, b, P.tw);
+    case 144: return fft_block_ct<144, S, NB>(a, b, P.tw);
+    case 192: return fft_block_ct<192, S, NB>(a, b, P.tw);
+    case 256: return fft_block_ct<256, S, NB>(a, b, P.tw);
+    default: return fft_smem(P, a, b, NB, n, S);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // 1. forward Chebyshev -> physical y (scaled by c(i)/2), columns -> plane layout
 // ---------------------------------------------------------------------------
@@ -48,7 +77,7 @@ __global__ void __launch_bounds__(256) k_dct_fwd(FieldPtrs in, double2 *__restri
     }
     for (int e = threadIdx.x + ncb * L; e < DCT_CB * L; e += blockDim.x) a[e] = make_double2(0.0, 0.0);
     __syncthreads();
-    double2 *r = fft_smem(P, a, b, DCT_CB, L, -1);
+    double2 *r = fft_block<-1, DCT_CB>(P, a, b, L);
     // PL[f][y][kx][kz]: col = kx*nz + kz
     for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
         const int y = e / ncb, c = e - y * ncb;
@@ -79,7 +108,7 @@ __global__ void __launch_bounds__(256) k_zfft_bwd(const double2 *__restrict__ pl
         a[c * mz + jj] = src[e];
     }
     __syncthreads();
-    double2 *r = fft_smem(P, a, b, ZKB, mz, +1);
+    double2 *r = fft_block<+1, ZKB>(P, a, b, mz);
     double2 *dst = q + (((size_t)f * nyp + y) * mz) * nxh;
     for (int e = threadIdx.x; e < nk * mz; e += blockDim.x) {
         const int z = e / nk, c = e - z * nk;
@@ -498,7 +527,7 @@ __global__ void __launch_bounds__(256) k_zfft_fwd(const double2 *__restrict__ q,
         a[c * mz + z] = c < nk ? src[(size_t)z * nxh + kx0 + c] : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    double2 *r = fft_smem(P, a, b, ZKB, mz, -1);
+    double2 *r = fft_block<-1, ZKB>(P, a, b, mz);
     double2 *dst = pl + (((size_t)f * nyp + y) * nxh + kx0) * nz;
     for (int e = threadIdx.x; e < nk * nz; e += blockDim.x) {
         const int c = e / nz, j = e - c * nz;
@@ -530,7 +559,7 @@ __global__ void __launch_bounds__(256) k_dct_bwd(const double2 *__restrict__ pl,
         if (y > 0 && y < ny) a[c * L + L - y] = v;
     }
     __syncthreads();
-    double2 *r = fft_smem(P, a, b, DCT_CB, L, -1);
+    double2 *r = fft_block<-1, DCT_CB>(P, a, b, L);
     double2 *dst = out.p[f] + (size_t)col0 * nyp;
     for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
         const int c = e / nyp, i = e - c * nyp;
