@@ -231,7 +231,21 @@ int kmm_tau_tabset(kmm_ctx *ctx, double g, int robin, double at, double bt, doub
     return KMM_OK;
 }
 
+int kmm_routine_tw32(kmm_ctx *ctx, const float2 **y2, const float2 **mz, const float2 **mx) {
+    const int n[3] = {2 * ctx->ny, ctx->mz, ctx->mx};
+    for (int t = 0; t < 3; ++t)
+        if (!ctx->rtw32[t]) RET(make_twf(ctx, n[t], &ctx->rtw32[t]));
+    *y2 = ctx->rtw32[0];
+    *mz = ctx->rtw32[1];
+    *mx = ctx->rtw32[2];
+    return KMM_OK;
+}
+
 void kmm_tau_release(kmm_ctx *ctx) {
+    for (int t = 0; t < 3; ++t) {
+        if (ctx->rtw32[t]) cudaFree(ctx->rtw32[t]);
+        ctx->rtw32[t] = NULL;
+    }
     TauCache *C = (TauCache *)ctx->tauc;
     if (!C) return;
     for (int i = 0; i < C->n; ++i)

@@ -106,6 +106,7 @@ struct kmm_ctx {
     int use_ztma;     // FP64 inverse z transform through TMA tile copies (default 1)
     void *ztma;       // its cached tensor maps (kmm_ztma.cu)
     void *tauc;       // tau tables of the routine solves' (g, boundary-condition) configurations (kmm_fused.cu)
+    float2 *rtw32[3]; // FP32 twiddles of 2 ny, mz, mx for the routine path's mixed form (kmm_fused.cu)
 };
 
 void kmm_fused_release(kmm_ctx *ctx);
@@ -150,6 +151,8 @@ int kmm_colblk_solve(kmm_ctx *ctx, double2 *u, double g, int robin, double at, d
 int kmm_tau_tabset(kmm_ctx *ctx, double g, int robin, double at, double bt, double ab, double bb, const double **tabs,
                    const double **rj);
 void kmm_tau_release(kmm_ctx *ctx);
+// FP32 twiddle tables (2 ny, mz, mx) of the routine path's mixed form, built on first use (kmm_fused.cu)
+int kmm_routine_tw32(kmm_ctx *ctx, const float2 **y2, const float2 **mz, const float2 **mx);
 int kmm_internal_penta(kmm_ctx *ctx, double2 *u, double g, int ib, double at, double bt, double ab, double bb,
                        const double2 *gt, const double2 *gb);
 int kmm_internal_axpy_spec(kmm_ctx *ctx, double2 *y, const double2 *x, double a);

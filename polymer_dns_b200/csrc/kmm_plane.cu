@@ -28,29 +28,32 @@ struct FieldPtrsW { double2 *p[MAXIO]; };
 // batched FFT of NB sequences of length N lying N apart in a (b: scratch of the same size) by the
 // block's 8 warps, NB / 8 sequences each, with the compile-time warp FFT; returns the buffer
 // holding the result, visible to the whole block
-template <int N, int S, int NB>
-__device__ __forceinline__ double2 *fft_block_ct(double2 *a, double2 *b, const double2 *tw) {
+template <typename C, int N, int S, int NB>
+__device__ __forceinline__ C *fft_block_ct(C *a, C *b, const C *tw) {
     constexpr int NQ = NB / 8;
     static_assert(NB % 8 == 0, "8 warps share the sequences");
     const size_t w = (size_t)(threadIdx.x >> 5) * NQ * N;
-    double2 *r = fft_warp_ct<double2, N, S, NQ, false>(a + w, b + w, tw);
+    C *r = fft_warp_ct<C, N, S, NQ, false>(a + w, b + w, tw);
     __syncthreads();
     return r - w;
 }
 
 // the same for the compiled lengths (the 3/2 grids of 32 .. 128 and 2 ny for ny = 32 .. 128), the
-// runtime block FFT for any other; blockDim = 256
-template <int S, int NB>
-__device__ double2 *fft_block(const DevPlan &P, double2 *a, double2 *b, int n) {
+// runtime block FFT for any other (FP64 only: the FP32 forms of the mixed precision run at the
+// compiled lengths, which the host checks); blockDim = 256; tw: the table of length n in C
+template <typename C, int S, int NB>
+__device__ C *fft_block(const DevPlan &P, C *a, C *b, const C *tw, int n) {
     switch (n) {
-    case 48: return fft_block_ct<48, S, NB>(a, b, P.tw);
-    case 64: return fft_block_ct<64, S, NB>(a, b, P.tw);
-    case 96: return fft_block_ct<96, S, NB>(a, b, P.tw);
-    case 128: return fft_block_ct<128, S, NB>(a, b, P.tw);
-    case 144: return fft_block_ct<144, S, NB>(a, b, P.tw);
-    case 192: return fft_block_ct<192, S, NB>(a, b, P.tw);
-    case 256: return fft_block_ct<256, S, NB>(a, b, P.tw);
-    default: return fft_smem(P, a, b, NB, n, S);
+    case 48: return fft_block_ct<C, 48, S, NB>(a, b, tw);
+    case 64: return fft_block_ct<C, 64, S, NB>(a, b, tw);
+    case 96: return fft_block_ct<C, 96, S, NB>(a, b, tw);
+    case 128: return fft_block_ct<C, 128, S, NB>(a, b, tw);
+    case 144: return fft_block_ct<C, 144, S, NB>(a, b, tw);
+    case 192: return fft_block_ct<C, 192, S, NB>(a, b, tw);
+    case 256: return fft_block_ct<C, 256, S, NB>(a, b, tw);
+    default:
+        if constexpr (sizeof(C) == sizeof(double2)) return fft_smem(P, a, b, NB, n, S);
+        else return a;
     }
 }
 
@@ -58,26 +61,29 @@ __device__ double2 *fft_block(const DevPlan &P, double2 *a, double2 *b, int n) {
 // 1. forward Chebyshev -> physical y (scaled by c(i)/2), columns -> plane layout
 // ---------------------------------------------------------------------------
 #define DCT_CB 8
-__global__ void __launch_bounds__(256) k_dct_fwd(FieldPtrs in, double2 *__restrict__ pl, DevPlan P, int nyp, int nz,
-                                                 int nxh, int ncols) {
-    extern __shared__ double2 sm[];
+template <typename C>
+__global__ void __launch_bounds__(256) k_dct_fwd(FieldPtrs in, C *__restrict__ pl, DevPlan P, const C *__restrict__ tw,
+                                                 int nyp, int nz, int nxh, int ncols) {
+    typedef typename kct::Real<C>::T T;
+    extern __shared__ double2 smd[];
+    C *sm = reinterpret_cast<C *>(smd);
     const int ny = nyp - 1, L = 2 * ny;
     const int f = blockIdx.y;
     const int col0 = blockIdx.x * DCT_CB;
     const int ncb = min(DCT_CB, ncols - col0);
-    double2 *a = sm, *b = sm + (size_t)DCT_CB * L;
+    C *a = sm, *b = sm + (size_t)DCT_CB * L;
     const double2 *src = in.p[f] + (size_t)col0 * nyp;
     for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
         const int c = e / nyp, i = e - c * nyp;
-        double2 v = src[e];
+        const double2 w = src[e];
         const double fac = (i == 0 || i == ny) ? 1.0 : 0.5;   // c(i)/2.0
-        v = make_double2(v.x * fac, v.y * fac);
+        const C v = kct::mk<C>((T)(w.x * fac), (T)(w.y * fac));
         a[c * L + i] = v;
         if (i > 0 && i < ny) a[c * L + L - i] = v;
     }
-    for (int e = threadIdx.x + ncb * L; e < DCT_CB * L; e += blockDim.x) a[e] = make_double2(0.0, 0.0);
+    for (int e = threadIdx.x + ncb * L; e < DCT_CB * L; e += blockDim.x) a[e] = kct::mk<C>((T)0, (T)0);
     __syncthreads();
-    double2 *r = fft_block<-1, DCT_CB>(P, a, b, L);
+    C *r = fft_block<C, -1, DCT_CB>(P, a, b, tw, L);
     // PL[f][y][kx][kz]: col = kx*nz + kz
     for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
         const int y = e / ncb, c = e - y * ncb;
@@ -91,25 +97,28 @@ __global__ void __launch_bounds__(256) k_dct_fwd(FieldPtrs in, double2 *__restri
 // 2. z: zero-pad + inverse c2c (FFTW_BACKWARD)
 // ---------------------------------------------------------------------------
 #define ZKB 16
-__global__ void __launch_bounds__(256) k_zfft_bwd(const double2 *__restrict__ pl, double2 *__restrict__ q, DevPlan P,
-                                                  int nyp, int nz, int nxh, int mz) {
-    extern __shared__ double2 sm[];
+template <typename C>
+__global__ void __launch_bounds__(256) k_zfft_bwd(const C *__restrict__ pl, C *__restrict__ q, DevPlan P,
+                                                  const C *__restrict__ tw, int nyp, int nz, int nxh, int mz) {
+    typedef typename kct::Real<C>::T T;
+    extern __shared__ double2 smd[];
+    C *sm = reinterpret_cast<C *>(smd);
     const int y = blockIdx.y, f = blockIdx.z;
     const int kx0 = blockIdx.x * ZKB;
     const int nk = min(ZKB, nxh - kx0);
     const int nzh = nz / 2;
-    double2 *a = sm, *b = sm + (size_t)ZKB * mz;
-    for (int e = threadIdx.x; e < ZKB * mz; e += blockDim.x) a[e] = make_double2(0.0, 0.0);
+    C *a = sm, *b = sm + (size_t)ZKB * mz;
+    for (int e = threadIdx.x; e < ZKB * mz; e += blockDim.x) a[e] = kct::mk<C>((T)0, (T)0);
     __syncthreads();
-    const double2 *src = pl + (((size_t)f * nyp + y) * nxh + kx0) * nz;
+    const C *src = pl + (((size_t)f * nyp + y) * nxh + kx0) * nz;
     for (int e = threadIdx.x; e < nk * nz; e += blockDim.x) {
         const int c = e / nz, j = e - c * nz;
         const int jj = (j < nzh) ? j : (mz - nz) + j;
         a[c * mz + jj] = src[e];
     }
     __syncthreads();
-    double2 *r = fft_block<+1, ZKB>(P, a, b, mz);
-    double2 *dst = q + (((size_t)f * nyp + y) * mz) * nxh;
+    C *r = fft_block<C, +1, ZKB>(P, a, b, tw, mz);
+    C *dst = q + (((size_t)f * nyp + y) * mz) * nxh;
     for (int e = threadIdx.x; e < nk * mz; e += blockDim.x) {
         const int z = e / nk, c = e - z * nk;
         dst[(size_t)z * nxh + kx0 + c] = r[c * mz + z];
@@ -144,9 +153,9 @@ __device__ __forceinline__ void atomic_max_pos(double *addr, double v) {
 // the pointwise terms of one 3/2-grid point (solvers.f90:2885-3063): u x omega, -u.grad(c) and
 // its sources, the polymer source / stress / qp terms, CFL, immersed-boundary forces and dPdx,
 // the tracer / inertial-particle copies; `in(slot)` is the physical value of an input slot here
-template <typename IN_T>
+template <typename IN_T, typename PO_T>
 __device__ __forceinline__ void xphys_point(const IN_T &in, const PhysArgs &A, const Save3D &sv, int y, int z, int k,
-                                            int nyp, int mz, int mx, double sg, double *__restrict__ po,
+                                            int nyp, int mz, int mx, double sg, PO_T *__restrict__ po,
                                             double *__restrict__ drag, double *__restrict__ up3,
                                             double *__restrict__ vp3, double *__restrict__ wp3,
                                             const int *__restrict__ imatrix, double *__restrict__ fxi,
@@ -230,7 +239,7 @@ __device__ __forceinline__ void xphys_point(const IN_T &in, const PhysArgs &A, c
     }
     for (int o = 0; o < O_NSLOT; ++o) {
         const int s = A.slot_of_out[o];
-        if (s >= 0) po[(size_t)s * nyp * mz * mx + g3] = out[o];
+        if (s >= 0) po[(size_t)s * nyp * mz * mx + g3] = (PO_T)out[o];
     }
     if (A.save_uvw) { up3[g3] = up; vp3[g3] = vp; wp3[g3] = wp; }
     if (sv.p[0]) {
@@ -326,43 +335,44 @@ __global__ void __launch_bounds__(256) k_xphys(const double2 *__restrict__ q, do
 // terms.  The generic k_xphys tiles two rows per block and transforms them with the runtime
 // block FFT; this form keeps more independent FFTs in flight per SM.
 #define XW 4
-template <int MX>
-__global__ void __launch_bounds__(XW * 32) k_xphys2(const double2 *__restrict__ q, double *__restrict__ po,
+template <int MX, typename C>
+__global__ void __launch_bounds__(XW * 32) k_xphys2(const C *__restrict__ q, typename kct::Real<C>::T *__restrict__ po,
                                                     double *__restrict__ drag, double *__restrict__ up3,
                                                     double *__restrict__ vp3, double *__restrict__ wp3,
                                                     const int *__restrict__ imatrix, double *__restrict__ fxi,
                                                     double *__restrict__ fyi, double *__restrict__ fzi,
                                                     const double *__restrict__ scsource,
                                                     const double *__restrict__ seght, double *__restrict__ cfl,
-                                                    double *__restrict__ umax, const double2 *__restrict__ tw,
+                                                    double *__restrict__ umax, const C *__restrict__ tw,
                                                     PhysArgs A, Save3D sv, int nyp, int mz) {
+    typedef typename kct::Real<C>::T T;
     constexpr int NXH = MX / 3, HX = MX / 2;
-    extern __shared__ double2 sm[];
-    double *phys = reinterpret_cast<double *>(sm);                       // [nin][MX]
-    double2 *fab = reinterpret_cast<double2 *>(phys + (size_t)A.nin * MX);  // per warp: a, b [MX]
+    extern __shared__ double2 smd[];
+    C *fab = reinterpret_cast<C *>(smd);                                  // per warp: a, b [MX]
+    T *phys = reinterpret_cast<T *>(fab + (size_t)XW * 2 * MX);           // [nin][MX]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int z = blockIdx.x, y = blockIdx.y;
-    double2 *a = fab + (size_t)warp * 2 * MX, *b = a + MX;
+    C *a = fab + (size_t)warp * 2 * MX, *b = a + MX;
     const int npairs = (A.nin + 1) / 2;
     for (int pr = warp; pr < npairs; pr += XW) {
         const int f = 2 * pr, g = f + 1 < A.nin ? f + 1 : -1;
-        const double2 *qa = q + (((size_t)f * nyp + y) * mz + z) * NXH;
-        const double2 *qb = g >= 0 ? q + (((size_t)g * nyp + y) * mz + z) * NXH : qa;
+        const C *qa = q + (((size_t)f * nyp + y) * mz + z) * NXH;
+        const C *qb = g >= 0 ? q + (((size_t)g * nyp + y) * mz + z) * NXH : qa;
         for (int k = lane; k < MX; k += 32) {
             const int kk = k <= HX ? k : MX - k;   // source mode
-            double2 A_ = make_double2(0.0, 0.0), B_ = make_double2(0.0, 0.0);
+            C A_ = kct::mk<C>((T)0, (T)0), B_ = A_;
             if (kk < NXH) {
                 A_ = qa[kk];
                 if (g >= 0) B_ = qb[kk];
             }
-            if (k == 0 || k == HX) { A_.y = 0.0; B_.y = 0.0; }
-            a[swz<double2>(k)] = k <= HX ? make_double2(A_.x - B_.y, A_.y + B_.x)     // A + iB
-                                         : make_double2(A_.x + B_.y, -A_.y + B_.x);   // conj(A) + i conj(B)
+            if (k == 0 || k == HX) { A_.y = (T)0; B_.y = (T)0; }
+            a[swz<C>(k)] = k <= HX ? kct::mk<C>(A_.x - B_.y, A_.y + B_.x)     // A + iB
+                                   : kct::mk<C>(A_.x + B_.y, -A_.y + B_.x);   // conj(A) + i conj(B)
         }
         __syncwarp();
-        const double2 *r = fft_warp_ct<double2, MX, +1, 1, true>(a, b, tw);
+        const C *r = fft_warp_ct<C, MX, +1, 1, true>(a, b, tw);
         for (int x = lane; x < MX; x += 32) {
-            const double2 v = r[swz<double2>(x)];
+            const C v = r[swz<C>(x)];
             phys[(size_t)f * MX + x] = v.x;
             if (g >= 0) phys[(size_t)g * MX + x] = v.y;
         }
@@ -372,7 +382,7 @@ __global__ void __launch_bounds__(XW * 32) k_xphys2(const double2 *__restrict__ 
     double cmax = 0.0, umx = 0.0;
     const double sg = seght[y];
     for (int k = threadIdx.x; k < MX; k += blockDim.x) {
-        auto in = [&](int sl) { return phys[(size_t)A.slot_of_in[sl] * MX + k]; };
+        auto in = [&](int sl) { return (double)phys[(size_t)A.slot_of_in[sl] * MX + k]; };
         xphys_point(in, A, sv, y, z, k, nyp, mz, MX, sg, po, drag, up3, vp3, wp3, imatrix, fxi, fyi, fzi, scsource, cmax,
                     umx);
     }
@@ -397,29 +407,30 @@ __global__ void __launch_bounds__(XW * 32) k_xphys2(const double2 *__restrict__ 
 
 // 5'. r2c along x for the compiled lengths: one block per (y, z) row, warps over output pairs
 // (two real rows packed as one complex FFT, split by Hermitian symmetry, modes kx < nxh kept)
-template <int MX>
-__global__ void __launch_bounds__(XW * 32) k_xfwd2(const double *__restrict__ po, double2 *__restrict__ q,
-                                                   const double2 *__restrict__ tw, int nout, int nyp, int mz) {
+template <int MX, typename C>
+__global__ void __launch_bounds__(XW * 32) k_xfwd2(const typename kct::Real<C>::T *__restrict__ po, C *__restrict__ q,
+                                                   const C *__restrict__ tw, int nout, int nyp, int mz) {
+    typedef typename kct::Real<C>::T T;
     constexpr int NXH = MX / 3;
-    extern __shared__ double2 sm[];
+    extern __shared__ double2 smd[];
+    C *sm = reinterpret_cast<C *>(smd);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int z = blockIdx.x, y = blockIdx.y;
-    double2 *a = sm + (size_t)warp * 2 * MX, *b = a + MX;
+    C *a = sm + (size_t)warp * 2 * MX, *b = a + MX;
     const size_t n3 = (size_t)nyp * mz * MX, g3 = ((size_t)y * mz + z) * MX;
     for (int pr = warp; pr < (nout + 1) / 2; pr += XW) {
         const int o = 2 * pr, g = o + 1 < nout ? o + 1 : -1;
         for (int x = lane; x < MX; x += 32)
-            a[swz<double2>(x)] = make_double2(po[(size_t)o * n3 + g3 + x], g >= 0 ? po[(size_t)g * n3 + g3 + x] : 0.0);
+            a[swz<C>(x)] = kct::mk<C>(po[(size_t)o * n3 + g3 + x], g >= 0 ? po[(size_t)g * n3 + g3 + x] : (T)0);
         __syncwarp();
-        const double2 *r = fft_warp_ct<double2, MX, -1, 1, true>(a, b, tw);
+        const C *r = fft_warp_ct<C, MX, -1, 1, true>(a, b, tw);
         for (int k = lane; k < NXH; k += 32) {
-            const double2 Z = r[swz<double2>(k)];
-            const double2 Zc = cconj(r[swz<double2>(k == 0 ? 0 : MX - k)]);
-            q[(((size_t)o * nyp + y) * mz + z) * NXH + k] = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
-            if (g >= 0) {
-                const double2 dd = csub(Z, Zc);   // -i/2 (Z - Zc)
-                q[(((size_t)g * nyp + y) * mz + z) * NXH + k] = make_double2(0.5 * dd.y, -0.5 * dd.x);
-            }
+            const C Z = r[swz<C>(k)];
+            C Zc = r[swz<C>(k == 0 ? 0 : MX - k)];
+            Zc.y = -Zc.y;
+            q[(((size_t)o * nyp + y) * mz + z) * NXH + k] = kct::mk<C>((T)0.5 * (Z.x + Zc.x), (T)0.5 * (Z.y + Zc.y));
+            if (g >= 0)   // -i/2 (Z - Zc)
+                q[(((size_t)g * nyp + y) * mz + z) * NXH + k] = kct::mk<C>((T)0.5 * (Z.y - Zc.y), (T)-0.5 * (Z.x - Zc.x));
         }
         __syncwarp();
     }
@@ -434,7 +445,8 @@ __global__ void __launch_bounds__(XW * 32) k_xfwd2(const double *__restrict__ po
 //    `j .ge. 3 .or. j .le. mz-2` is always true), so j+jj outside 1..mz lands in the next or
 //    previous x column; targets outside the plane array are dropped.
 // ---------------------------------------------------------------------------
-__global__ void k_spread(double *__restrict__ po, const double *__restrict__ drag, const double *__restrict__ fspread,
+template <typename PO_T>
+__global__ void k_spread(PO_T *__restrict__ po, const double *__restrict__ drag, const double *__restrict__ fspread,
                          int nyp, int mz, int mx, int kmaxsurf, int o1, int o2, int o3) {
     const size_t nplane = (size_t)mz * mx;
     const int y = blockIdx.y;
@@ -463,9 +475,9 @@ __global__ void k_spread(double *__restrict__ po, const double *__restrict__ dra
             }
         const int jt = (int)(t % mz), kt = (int)(t / mz);
         const size_t gt = ((size_t)y * mz + jt) * mx + kt;
-        if (o1 >= 0) po[(size_t)o1 * n3 + gt] += ax;
-        if (o2 >= 0) po[(size_t)o2 * n3 + gt] += ay;
-        if (o3 >= 0) po[(size_t)o3 * n3 + gt] += az;
+        if (o1 >= 0) po[(size_t)o1 * n3 + gt] = (PO_T)((double)po[(size_t)o1 * n3 + gt] + ax);
+        if (o2 >= 0) po[(size_t)o2 * n3 + gt] = (PO_T)((double)po[(size_t)o2 * n3 + gt] + ay);
+        if (o3 >= 0) po[(size_t)o3 * n3 + gt] = (PO_T)((double)po[(size_t)o3 * n3 + gt] + az);
     }
 }
 
@@ -513,58 +525,65 @@ __global__ void __launch_bounds__(256) k_xfwd(const double *__restrict__ po, dou
 // ---------------------------------------------------------------------------
 // 6. z: forward c2c, truncate to nz, /(mx*mz)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_zfft_fwd(const double2 *__restrict__ q, double2 *__restrict__ pl, DevPlan P,
-                                                  int nyp, int nz, int nxh, int mz, double scale) {
-    extern __shared__ double2 sm[];
+template <typename C>
+__global__ void __launch_bounds__(256) k_zfft_fwd(const C *__restrict__ q, C *__restrict__ pl, DevPlan P,
+                                                  const C *__restrict__ tw, int nyp, int nz, int nxh, int mz,
+                                                  double scale) {
+    typedef typename kct::Real<C>::T T;
+    extern __shared__ double2 smd[];
+    C *sm = reinterpret_cast<C *>(smd);
     const int y = blockIdx.y, f = blockIdx.z;
     const int kx0 = blockIdx.x * ZKB;
     const int nk = min(ZKB, nxh - kx0);
     const int nzh = nz / 2;
-    double2 *a = sm, *b = sm + (size_t)ZKB * mz;
-    const double2 *src = q + (((size_t)f * nyp + y) * mz) * nxh;
+    C *a = sm, *b = sm + (size_t)ZKB * mz;
+    const C *src = q + (((size_t)f * nyp + y) * mz) * nxh;
     for (int e = threadIdx.x; e < ZKB * mz; e += blockDim.x) {
         const int z = e / ZKB, c = e - z * ZKB;
-        a[c * mz + z] = c < nk ? src[(size_t)z * nxh + kx0 + c] : make_double2(0.0, 0.0);
+        a[c * mz + z] = c < nk ? src[(size_t)z * nxh + kx0 + c] : kct::mk<C>((T)0, (T)0);
     }
     __syncthreads();
-    double2 *r = fft_block<-1, ZKB>(P, a, b, mz);
-    double2 *dst = pl + (((size_t)f * nyp + y) * nxh + kx0) * nz;
+    C *r = fft_block<C, -1, ZKB>(P, a, b, tw, mz);
+    C *dst = pl + (((size_t)f * nyp + y) * nxh + kx0) * nz;
     for (int e = threadIdx.x; e < nk * nz; e += blockDim.x) {
         const int c = e / nz, j = e - c * nz;
         const int jj = (j < nzh) ? j : (mz - nz) + j;
-        const double2 v = r[c * mz + jj];
-        dst[e] = make_double2(v.x / scale, v.y / scale);
+        const C v = r[c * mz + jj];
+        dst[e] = kct::mk<C>((T)(v.x / scale), (T)(v.y / scale));
     }
 }
 
 // ---------------------------------------------------------------------------
 // 7. y: DCT-I back to Chebyshev coefficients, /ny, halve the end coefficients
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_dct_bwd(const double2 *__restrict__ pl, FieldPtrsW out, DevPlan P, int nyp,
-                                                 int nz, int nxh, int ncols) {
-    extern __shared__ double2 sm[];
+template <typename C>
+__global__ void __launch_bounds__(256) k_dct_bwd(const C *__restrict__ pl, FieldPtrsW out, DevPlan P,
+                                                 const C *__restrict__ tw, int nyp, int nz, int nxh, int ncols) {
+    typedef typename kct::Real<C>::T T;
+    extern __shared__ double2 smd[];
+    C *sm = reinterpret_cast<C *>(smd);
     const int ny = nyp - 1, L = 2 * ny;
     const int f = blockIdx.y;
     const int col0 = blockIdx.x * DCT_CB;
     const int ncb = min(DCT_CB, ncols - col0);
-    double2 *a = sm, *b = sm + (size_t)DCT_CB * L;
-    for (int e = threadIdx.x; e < DCT_CB * L; e += blockDim.x) a[e] = make_double2(0.0, 0.0);
+    C *a = sm, *b = sm + (size_t)DCT_CB * L;
+    for (int e = threadIdx.x; e < DCT_CB * L; e += blockDim.x) a[e] = kct::mk<C>((T)0, (T)0);
     __syncthreads();
     for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
         const int y = e / ncb, c = e - y * ncb;
         const int col = col0 + c;
         const int kx = col / nz, kz = col - kx * nz;
-        const double2 v = pl[(((size_t)f * nyp + y) * nxh + kx) * nz + kz];
+        const C v = pl[(((size_t)f * nyp + y) * nxh + kx) * nz + kz];
         a[c * L + y] = v;
         if (y > 0 && y < ny) a[c * L + L - y] = v;
     }
     __syncthreads();
-    double2 *r = fft_block<-1, DCT_CB>(P, a, b, L);
+    C *r = fft_block<C, -1, DCT_CB>(P, a, b, tw, L);
     double2 *dst = out.p[f] + (size_t)col0 * nyp;
     for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
         const int c = e / nyp, i = e - c * nyp;
-        double2 v = r[c * L + i];
-        v = make_double2(v.x / (double)ny, v.y / (double)ny);
+        const C rv = r[c * L + i];
+        double2 v = make_double2((double)rv.x / (double)ny, (double)rv.y / (double)ny);
         if (i == 0 || i == ny) v = make_double2(v.x / 2.0, v.y / 2.0);
         dst[e] = v;
     }
@@ -794,28 +813,48 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     const size_t sm_z = sizeof(double2) * 2 * ZKB * mz;
     const size_t sm_x = sizeof(double) * (size_t)nin * XZB * mx + sizeof(double2) * 2 * XZB * mx;
     const size_t sm_xf = sizeof(double2) * 2 * XZB * mx;
-    RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd, sm_dct));
-    RET(kmm_smem_attr(ctx, (const void *)k_dct_bwd, sm_dct));
-    RET(kmm_smem_attr(ctx, (const void *)k_zfft_bwd, sm_z));
-    RET(kmm_smem_attr(ctx, (const void *)k_zfft_fwd, sm_z));
+    RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd<double2>, sm_dct));
+    RET(kmm_smem_attr(ctx, (const void *)k_dct_bwd<double2>, sm_dct));
+    RET(kmm_smem_attr(ctx, (const void *)k_zfft_bwd<double2>, sm_z));
+    RET(kmm_smem_attr(ctx, (const void *)k_zfft_fwd<double2>, sm_z));
+    RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd<float2>, sm_dct));
+    RET(kmm_smem_attr(ctx, (const void *)k_dct_bwd<float2>, sm_dct));
+    RET(kmm_smem_attr(ctx, (const void *)k_zfft_bwd<float2>, sm_z));
+    RET(kmm_smem_attr(ctx, (const void *)k_zfft_fwd<float2>, sm_z));
     RET(kmm_smem_attr(ctx, (const void *)k_xphys, sm_x));
     RET(kmm_smem_attr(ctx, (const void *)k_xfwd, sm_xf));
     CK(cudaMemsetAsync(ctx->d_cfl, 0, sizeof(double) * nyp, ctx->stream));
     CK(cudaMemsetAsync(ctx->d_umax, 0, sizeof(double) * nyp, ctx->stream));
 
+    // the mixed form (FP32 transforms and plane intermediates, pointwise terms evaluated in FP64 from
+    // the FP32 values, FP64 state) inside kmm_step; FP64 elsewhere (initial, diagnostics)
+    const bool f32 = ctx->p.precision == 1 && ctx->in_step;
+    const float2 *tw_y2 = NULL, *tw_mz = NULL, *tw_mx = NULL;
+    if (f32) RET(kmm_routine_tw32(ctx, &tw_y2, &tw_mz, &tw_mx));
+    float2 *pl_in32 = (float2 *)ctx->pl_in, *q_in32 = (float2 *)ctx->q_in;
+    float2 *pl_out32 = (float2 *)ctx->pl_out, *q_out32 = (float2 *)ctx->q_out;
+    float *po32 = (float *)ctx->po;
     kmm_tic(ctx);
-    k_dct_fwd<<<dim3((ncols + DCT_CB - 1) / DCT_CB, nin), 256, sm_dct, ctx->stream>>>(in, ctx->pl_in, ctx->py2, nyp,
-                                                                                        nz, nxh, ncols);
+    if (f32)
+        k_dct_fwd<float2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nin), 256, sm_dct, ctx->stream>>>(
+            in, pl_in32, ctx->py2, tw_y2, nyp, nz, nxh, ncols);
+    else
+        k_dct_fwd<double2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nin), 256, sm_dct, ctx->stream>>>(
+            in, ctx->pl_in, ctx->py2, ctx->py2.tw, nyp, nz, nxh, ncols);
     CKL();
     kmm_toc(ctx, KMM_STAGE_DCT_FWD);
     kmm_tic(ctx);
-    k_zfft_bwd<<<dim3((nxh + ZKB - 1) / ZKB, nyp, nin), 256, sm_z, ctx->stream>>>(ctx->pl_in, ctx->q_in, ctx->pmz,
-                                                                                   nyp, nz, nxh, mz);
+    if (f32)
+        k_zfft_bwd<float2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nin), 256, sm_z, ctx->stream>>>(pl_in32, q_in32, ctx->pmz,
+                                                                                               tw_mz, nyp, nz, nxh, mz);
+    else
+        k_zfft_bwd<double2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nin), 256, sm_z, ctx->stream>>>(
+            ctx->pl_in, ctx->q_in, ctx->pmz, ctx->pmz.tw, nyp, nz, nxh, mz);
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_BWD);
     bool fast_done = false;
     const bool sc_source = scal && ctx->p.scl_flag >= 2;
-    if (!poly && !ib_any && !inertial && !sc_source) {
+    if (!poly && !ib_any && !inertial && !sc_source && !f32) {
         // fused warp-per-row x stage (no polymer, no immersed boundary, no inertial particles, no
         // particle scalar source)
         kmm_tic(ctx);
@@ -827,65 +866,91 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     }
     if (!fast_done) {
         kmm_tic(ctx);
-        const size_t sm_x2 = sizeof(double) * (size_t)nin * mx + sizeof(double2) * 2 * XW * (size_t)mx;
-#define XP2(MM)                                                                                                  \
+        const size_t eb = f32 ? sizeof(float) : sizeof(double);   // bytes per real of the intermediates
+        const size_t sm_x2 = eb * (size_t)nin * mx + 2 * eb * 2 * XW * (size_t)mx;
+#define XP2(MM, CC, QQ, PO, TW)                                                                                  \
     do {                                                                                                         \
-        RET(kmm_smem_attr(ctx, (const void *)k_xphys2<MM>, sm_x2));                                              \
-        k_xphys2<MM><<<dim3(mz, nyp), XW * 32, sm_x2, ctx->stream>>>(                                             \
-            ctx->q_in, ctx->po, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl, \
-            ctx->d_umax, ctx->wmx.tw, A, sv, nyp, mz);                                                           \
+        RET(kmm_smem_attr(ctx, (const void *)k_xphys2<MM, CC>, sm_x2));                                          \
+        k_xphys2<MM, CC><<<dim3(mz, nyp), XW * 32, sm_x2, ctx->stream>>>(                                         \
+            QQ, PO, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl,          \
+            ctx->d_umax, TW, A, sv, nyp, mz);                                                                    \
+    } while (0)
+#define XP2S(MM)                                                                                                 \
+    do {                                                                                                         \
+        if (f32) XP2(MM, float2, q_in32, po32, tw_mx);                                                           \
+        else XP2(MM, double2, ctx->q_in, ctx->po, ctx->wmx.tw);                                                  \
     } while (0)
         switch (mx) {
-        case 48: XP2(48); break;
-        case 96: XP2(96); break;
-        case 144: XP2(144); break;
-        case 192: XP2(192); break;
+        case 48: XP2S(48); break;
+        case 96: XP2S(96); break;
+        case 144: XP2S(144); break;
+        case 192: XP2S(192); break;
         default:
             k_xphys<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_x, ctx->stream>>>(
                 ctx->q_in, ctx->po, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl,
                 ctx->d_umax, ctx->pmx, A, sv, nyp, mz, mx, nxh);
             break;
         }
+#undef XP2S
 #undef XP2
         CKL();
         kmm_toc(ctx, KMM_STAGE_XPHYS);
         if (ib_any && ctx->kmaxsurf > 0) {
             const int ksp = ctx->kmaxsurf < nyp ? ctx->kmaxsurf : nyp;
-            k_spread<<<dim3(kmm_blocks((size_t)mz * mx, 256) > 64 ? 64 : kmm_blocks((size_t)mz * mx, 256), ksp), 256, 0,
-                       ctx->stream>>>(ctx->po, ctx->drag, ctx->d_fspread, nyp, mz, mx, ctx->kmaxsurf, A.slot_of_out[O_H1],
-                                      A.slot_of_out[O_H2], A.slot_of_out[O_H3]);
+            const dim3 gs(kmm_blocks((size_t)mz * mx, 256) > 64 ? 64 : kmm_blocks((size_t)mz * mx, 256), ksp);
+            if (f32)
+                k_spread<float><<<gs, 256, 0, ctx->stream>>>(po32, ctx->drag, ctx->d_fspread, nyp, mz, mx, ctx->kmaxsurf,
+                                                             A.slot_of_out[O_H1], A.slot_of_out[O_H2],
+                                                             A.slot_of_out[O_H3]);
+            else
+                k_spread<double><<<gs, 256, 0, ctx->stream>>>(ctx->po, ctx->drag, ctx->d_fspread, nyp, mz, mx,
+                                                              ctx->kmaxsurf, A.slot_of_out[O_H1], A.slot_of_out[O_H2],
+                                                              A.slot_of_out[O_H3]);
             CKL();
         }
         kmm_tic(ctx);
-        const size_t sm_xf2 = sizeof(double2) * 2 * XW * (size_t)mx;
-#define XF2(MM)                                                                                                 \
+        const size_t sm_xf2 = 2 * eb * 2 * XW * (size_t)mx;
+#define XF2(MM, CC, PO, QQ, TW)                                                                                 \
     do {                                                                                                        \
-        RET(kmm_smem_attr(ctx, (const void *)k_xfwd2<MM>, sm_xf2));                                             \
-        k_xfwd2<MM><<<dim3(mz, nyp), XW * 32, sm_xf2, ctx->stream>>>(ctx->po, ctx->q_out, ctx->wmx.tw, nout, nyp, mz); \
+        RET(kmm_smem_attr(ctx, (const void *)k_xfwd2<MM, CC>, sm_xf2));                                         \
+        k_xfwd2<MM, CC><<<dim3(mz, nyp), XW * 32, sm_xf2, ctx->stream>>>(PO, QQ, TW, nout, nyp, mz);             \
+    } while (0)
+#define XF2S(MM)                                                                                                \
+    do {                                                                                                        \
+        if (f32) XF2(MM, float2, po32, q_out32, tw_mx);                                                         \
+        else XF2(MM, double2, ctx->po, ctx->q_out, ctx->wmx.tw);                                                \
     } while (0)
         switch (mx) {
-        case 48: XF2(48); break;
-        case 96: XF2(96); break;
-        case 144: XF2(144); break;
-        case 192: XF2(192); break;
+        case 48: XF2S(48); break;
+        case 96: XF2S(96); break;
+        case 144: XF2S(144); break;
+        case 192: XF2S(192); break;
         default:
             k_xfwd<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_xf, ctx->stream>>>(ctx->po, ctx->q_out, ctx->pmx, nout, nyp,
                                                                                  mz, mx, nxh);
             break;
         }
+#undef XF2S
 #undef XF2
         CKL();
         kmm_toc(ctx, KMM_STAGE_XFWD);
     }
     kmm_tic(ctx);
-    k_zfft_fwd<<<dim3((nxh + ZKB - 1) / ZKB, nyp, nout), 256, sm_z, ctx->stream>>>(ctx->q_out, ctx->pl_out, ctx->pmz,
-                                                                                    nyp, nz, nxh, mz,
-                                                                                    (double)mx * (double)mz);
+    if (f32)
+        k_zfft_fwd<float2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nout), 256, sm_z, ctx->stream>>>(
+            q_out32, pl_out32, ctx->pmz, tw_mz, nyp, nz, nxh, mz, (double)mx * (double)mz);
+    else
+        k_zfft_fwd<double2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nout), 256, sm_z, ctx->stream>>>(
+            ctx->q_out, ctx->pl_out, ctx->pmz, ctx->pmz.tw, nyp, nz, nxh, mz, (double)mx * (double)mz);
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_FWD);
     kmm_tic(ctx);
-    k_dct_bwd<<<dim3((ncols + DCT_CB - 1) / DCT_CB, nout), 256, sm_dct, ctx->stream>>>(ctx->pl_out, outp, ctx->py2,
-                                                                                        nyp, nz, nxh, ncols);
+    if (f32)
+        k_dct_bwd<float2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nout), 256, sm_dct, ctx->stream>>>(
+            pl_out32, outp, ctx->py2, tw_y2, nyp, nz, nxh, ncols);
+    else
+        k_dct_bwd<double2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nout), 256, sm_dct, ctx->stream>>>(
+            ctx->pl_out, outp, ctx->py2, ctx->py2.tw, nyp, nz, nxh, ncols);
     CKL();
     kmm_toc(ctx, KMM_STAGE_DCT_BWD);
 
@@ -1023,14 +1088,16 @@ extern "C" int kmm_calcswirl(kmm_ctx *ctx) {
     const size_t sm_dct = sizeof(double2) * 2 * DCT_CB * 2 * ctx->ny;
     const size_t sm_z = sizeof(double2) * 2 * ZKB * mz;
     const size_t sm_s = sizeof(double2) * (size_t)SW_WARPS * 7 * mx;
-    RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd, sm_dct));
-    RET(kmm_smem_attr(ctx, (const void *)k_zfft_bwd, sm_z));
+    RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd<double2>, sm_dct));
+    RET(kmm_smem_attr(ctx, (const void *)k_zfft_bwd<double2>, sm_z));
     RET(kmm_smem_attr(ctx, (const void *)k_swirl_x, sm_s));
-    k_dct_fwd<<<dim3((ncols + DCT_CB - 1) / DCT_CB, 9), 256, sm_dct, ctx->stream>>>(in, ctx->pl_in, ctx->py2, nyp, nz,
-                                                                                      nxh, ncols);
+    k_dct_fwd<double2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, 9), 256, sm_dct, ctx->stream>>>(in, ctx->pl_in, ctx->py2,
+                                                                                               ctx->py2.tw, nyp, nz,
+                                                                                               nxh, ncols);
     CKL();
-    k_zfft_bwd<<<dim3((nxh + ZKB - 1) / ZKB, nyp, 9), 256, sm_z, ctx->stream>>>(ctx->pl_in, ctx->q_in, ctx->pmz, nyp,
-                                                                                 nz, nxh, mz);
+    k_zfft_bwd<double2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, 9), 256, sm_z, ctx->stream>>>(ctx->pl_in, ctx->q_in,
+                                                                                          ctx->pmz, ctx->pmz.tw, nyp,
+                                                                                          nz, nxh, mz);
     CKL();
     k_swirl_x<<<dim3((mz + SW_WARPS - 1) / SW_WARPS, nyp), SW_WARPS * 32, sm_s, ctx->stream>>>(ctx->q_in, sw, ctx->wmx,
                                                                                             nyp, mz, mx, nxh);
@@ -1103,9 +1170,10 @@ extern "C" int kmm_flowstats(kmm_ctx *ctx, double *prof, double *scal) {
     in.p[3] = du;
     RET(kmm_ensure_plane_buffers(ctx, 4, 0));
     const size_t sm_dct = sizeof(double2) * 2 * DCT_CB * 2 * ctx->ny;
-    RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd, sm_dct));
-    k_dct_fwd<<<dim3((ncols + DCT_CB - 1) / DCT_CB, 4), 256, sm_dct, ctx->stream>>>(in, ctx->pl_in, ctx->py2, nyp, nz,
-                                                                                      nxh, ncols);
+    RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd<double2>, sm_dct));
+    k_dct_fwd<double2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, 4), 256, sm_dct, ctx->stream>>>(in, ctx->pl_in, ctx->py2,
+                                                                                               ctx->py2.tw, nyp, nz,
+                                                                                               nxh, ncols);
     CKL();
     double *acc = ctx->d_scratch;   // 9 KMM_MAX_NYP doubles: 6 nyp used here
     k_flowstats<<<nyp, FS_THREADS, 0, ctx->stream>>>(ctx->pl_in, acc, nyp, nz, nxh);

@@ -299,9 +299,16 @@ extern "C" int kmm_step(kmm_ctx *ctx) {
     if (!ctx) return KMM_ERR_ARG;
     if (ctx->use_fused && kmm_fused_applicable(ctx)) return kmm_fused_step(ctx);
     if (ctx->p.precision == 1) {
-        // the mixed-precision form lives in the fused kernels only; never fall back silently to FP64
-        kmm_set_error(ctx, "mixed precision needs the fused step (no polymer, no immersed boundary, KMM_OPT_FUSED = 1)");
-        return KMM_ERR_UNSUPPORTED;
+        // the routine path's mixed form runs its transforms at the compiled lengths only; never fall
+        // back silently to FP64
+        const int ly = 2 * ctx->ny, mz = ctx->mz, mx = ctx->mx;
+        const bool ok_y = ly == 64 || ly == 128 || ly == 192 || ly == 256;
+        const bool ok_z = mz == 48 || mz == 96 || mz == 144 || mz == 192;
+        const bool ok_x = mx == 48 || mx == 96 || mx == 144 || mx == 192;
+        if (!(ok_y && ok_z && ok_x)) {
+            kmm_set_error(ctx, "mixed precision needs nx, ny, nz in {32, 64, 96, 128}");
+            return KMM_ERR_UNSUPPORTED;
+        }
     }
     const double re = ctx->re, dt = ctx->dt, th = ctx->theta;
     ctx->it += 1;

@@ -554,3 +554,49 @@ def test_particle_scalar_source_matches_oracle(rt, oracle_mod):
         kc.load_initial(c, q, f2, np.zeros_like(f2[0]))
     assert o2.initial() == abi.ERR_UNSUPPORTED
     assert g2.call("initial", allow=(abi.ERR_UNSUPPORTED,)) == abi.ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("variant", ["polymer_ib", "inertial", "routine_plain"])
+def test_mixed_precision_routine_path_tracks_fp64(rt, variant):
+    """The mixed form on the routine path (polymer + IB, inertial particles, or a plain run with the
+    fused step switched off): FP32 y / z / x transforms and plane intermediates, pointwise terms
+    from the FP32 values, FP64 solves and state, against the FP64 drop-in from the same state after
+    10 steps; the bar is 1e-5 relative, as for the fused mixed form."""
+    kw = dict(scalar_on=1, diff=1.0, scalar_bc=1, scalar_q=0.5)
+    im = None
+    if variant == "polymer_ib":
+        kw.update(polymer_on=1, zlmax=30.0, tpoly=20.0, qbeta=0.9, diffpoly=1000.0, gain=-400.0, ugain=-40.0,
+                  dt=0.005)
+    elif variant == "inertial":
+        kw.update(particle_flag=1, npart=200, ap=0.002, ratio=2.0, gravity=0.1, cd_switch=2, c_mu=1.0)
+    names = ["V", "OMY", "FN", "GN", "U0", "W0", "SCALAR", "SCN"]
+    if variant == "polymer_ib":
+        names += ["C11", "C12", "C22", "C33", "STR11N"]
+    ctxs = []
+    for prec in (0, 1):
+        p = kc.cfg_small(32, 32, 32, precision=prec, **kw)
+        fields = kc.initial_fields(p, amp=0.1, seed=19)
+        g = rt.KmmContext(p)
+        if variant == "routine_plain":
+            g.call("set_option", 1, 0)
+        kc.load_initial(g, p, fields, np.zeros_like(fields[0]))
+        if variant == "polymer_ib":
+            g.upload("IMATRIX", inputs.cylinder_imatrix(p.nx, p.ny, p.nz, p.xl, p.yl, math.pi, 0.0, 0.25))
+        if variant == "inertial":
+            for name, arr in zip(("XPART", "YPART", "ZPART"), inputs.uniform_particles(p.npart, p.xl, p.yl, p.zl,
+                                                                                      p.ap, 5)):
+                g.upload(name, arr)
+        assert g.initial() == 0
+        ctxs.append(g)
+    for _ in range(10):
+        for g in ctxs:
+            assert g.step() == 0
+    worst = 0.0
+    for name in names:
+        e = kc.rel_err(ctxs[1].download(name), ctxs[0].download(name))
+        worst = max(worst, e)
+        assert e <= 1e-5, "%s rel err %.3e" % (name, e)
+    assert worst > 1e-12   # the mixed form really runs in FP32
+    if variant == "inertial":
+        for name in ("XPART", "YPART", "VPART"):
+            assert kc.rel_err(ctxs[1].download(name), ctxs[0].download(name)) <= 1e-5
