@@ -339,6 +339,8 @@ def run_kmm(a, rank, world, local_rank):
             result["mixed"] = mixed_report(a, f, extra, local_rank, ms_per_step)
         if a.config == "cfg2" and not a.no_ensemble:
             result["ensemble"] = ensemble_report(a, local_rank)
+        if a.config == "cfg2" and not a.no_polymer and world == 1:
+            result["polymer"] = polymer_report(a, local_rank)
         if not a.no_cpu_baseline and world == 1:
             result["cpu_baseline"] = cpu_baseline(a.config, a.cpu_steps)
     ctx.close()
@@ -402,6 +404,65 @@ def mixed_report(a, f, extra, local_rank, fp64_ms):
     return {"value": round(1e3 / ms, 3), "unit": "timesteps/s", "ms_per_step": round(ms, 4),
             "speedup_vs_fp64": round(fp64_ms / ms, 3), "dtype": "fp32 transforms/products, fp64 solves",
             "rel_err_vs_fp64": errs, "drift_over_1000_steps": drift}
+
+
+def polymer_report(a, local_rank):
+    """The polymer + immersed-boundary configuration (the Re_tau = 180 case with FENE-P Wi = 20,
+    beta = 0.9, L^2 = 900 and the cylinder IB; routine path): FP64 and mixed-precision steps/s, the
+    mixed form's relative error against FP64 from the same state after 10 and 1000 steps (u, v, w,
+    scalar and the six conformation-tensor components), and the oracle on the host cores."""
+    from polymer_dns_b200 import runtime
+    p64, init, desc = make_config("cfg3", 0)
+    f, extra = build_inputs(p64, init, "cfg3")
+    nst = 5
+    ms = {}
+    for prec in (0, 1):
+        p, _, _ = make_config("cfg3", prec)
+        c = runtime.KmmContext(p, device=local_rank)
+        load(c, f, extra, c.upload)
+        c.initial()
+        for _ in range(3):
+            c.step()
+        c.call("sync")
+        c.event_record(0)
+        for _ in range(nst):
+            c.step()
+        c.event_record(1)
+        ms[prec] = c.event_elapsed(0, 1) / nst
+        c.close()
+    ctx = {}
+    for prec in (0, 1):
+        p, _, _ = make_config("cfg3", prec)
+        c = runtime.KmmContext(p, device=local_rank)
+        load(c, f, extra, c.upload)
+        c.initial()
+        ctx[prec] = c
+    names = {"u": "U", "v": "V", "w": "W", "scalar": "SCALAR", "c11": "C11", "c12": "C12", "c13": "C13",
+             "c22": "C22", "c23": "C23", "c33": "C33"}
+    from polymer_dns_b200 import abi
+    errs, done, stopped = {}, 0, None
+    for mark in (10, 100, 1000):
+        sts = [c.call("run", mark - done, allow=(abi.ERR_CFL, abi.ERR_NAN)) for c in ctx.values()]
+        if any(sts):
+            stopped = "a run stopped between steps %d and %d (%s): CFL > 1 or a non-finite value" % (
+                done, mark, ", ".join(abi.STATUS_NAMES.get(x, str(x)) for x in sts))
+            break
+        done = mark
+        for c in ctx.values():
+            c.call("veloc")   # u, w from the current v, omega_y (the step keeps them current too)
+        e = {}
+        for k, n in names.items():
+            x, y = ctx[1].download(n), ctx[0].download(n)
+            e[k] = float("%.3e" % (np.abs(x - y).max() / max(np.abs(y).max(), 1e-300)))
+        errs[str(mark)] = e
+    for c in ctx.values():
+        c.close()
+    cpu = cpu_baseline("cfg3", 1) if not a.no_cpu_baseline else None
+    return {"workload": desc, "fp64": {"value": round(1e3 / ms[0], 3), "unit": "timesteps/s",
+                                       "ms_per_step": round(ms[0], 4)},
+            "mixed": {"value": round(1e3 / ms[1], 3), "unit": "timesteps/s", "ms_per_step": round(ms[1], 4),
+                      "speedup_vs_fp64": round(ms[0] / ms[1], 3)},
+            "mixed_rel_err_vs_fp64": errs, "long_run": stopped or "both forms ran 1000 steps", "cpu_baseline": cpu}
 
 
 ENSEMBLE_GRIDS = [(64, 64, 64)] * 4 + [(96, 96, 96)] * 4 + [(128, 128, 96)] * 4 + [(128, 128, 128)] * 4
@@ -511,6 +572,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision speed / error report")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 16-member ensemble measurement")
+    ap.add_argument("--no-polymer", action="store_true", help="skip the polymer + IB (FP64 / mixed) measurement")
     ap.add_argument("--ztma", type=int, default=None, choices=[0, 1],
                     help="inverse z transform with TMA tile copies (1, the library default) or plain loads (0)")
     a = ap.parse_args()
