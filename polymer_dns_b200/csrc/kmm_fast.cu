@@ -12,6 +12,9 @@
 #include "kmm_fft.cuh"
 
 #define FX_WARPS 4
+// blocks per SM the specialised x stage is register-sized for: three in FP64 (four spill and run no
+// faster), four for the FP32 form of the mixed precision (no spills; 7 % faster than three)
+template <typename C> struct Fx2MinB { static constexpr int v = sizeof(C) == 16 ? 3 : 4; };
 
 struct FxArgs {
     int nout, ic, flow_select, save_uvw;   // ic: index in q of dc/dx (dc/dy, dc/dz follow), -1 without scalar
@@ -161,7 +164,7 @@ __global__ void __launch_bounds__(FX_WARPS * 32, 3) k_fx(const double2 *__restri
 //   - C = double2 (FP64) or float2 (FP32 transforms and products of the mixed-precision form;
 //     the CFL numbers and the tracer copies of u, v, w are widened to FP64).
 template <int MX, typename C>
-__global__ void __launch_bounds__(FX_WARPS * 32, 3) k_fx2(const C *__restrict__ q, C *__restrict__ r,
+__global__ void __launch_bounds__(FX_WARPS * 32, Fx2MinB<C>::v) k_fx2(const C *__restrict__ q, C *__restrict__ r,
                                                           double *__restrict__ up3, double *__restrict__ vp3,
                                                           double *__restrict__ wp3, const double *__restrict__ seght,
                                                           double *__restrict__ cfl, double *__restrict__ umax,
