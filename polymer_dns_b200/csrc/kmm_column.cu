@@ -69,8 +69,79 @@ __global__ void __launch_bounds__(TPB) k_cderiv(const double2 *__restrict__ f, d
     tile_store(df, sd, col0, ncol, nyp);
 }
 
+// The same two chains with a half-warp per column for ny = 16 K: lane t holds the K consecutive
+// coefficients t K .. t K + K - 1 in registers and the chains run lane by lane from the top, the
+// carries D[(t+1) K] and D[(t+1) K + 1] handed down by shuffles, so every D[i] is the same sum in
+// the same order as above (bitwise equal) while the columns keep the whole SM busy.
+template <int K>
+__global__ void __launch_bounds__(128) k_cderiv_hw(const double2 *f, double2 *df, int ncols, double dyde) {
+    constexpr int NY = 16 * K, NYP = NY + 1;
+    const int col = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 4);
+    if (col >= ncols) return;   // whole half-warps
+    const int t = threadIdx.x & 15;
+    // both columns of the warp present -> the full mask; else the present half alone
+    const unsigned mask = (col | 1) < ncols ? 0xffffffffu : ((threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu);
+    const double2 *F = f + (size_t)col * NYP;
+    double2 v[K];
+#pragma unroll
+    for (int m = 0; m < K; ++m) v[m] = F[t * K + m];
+    const double2 ftop = F[NY];
+    double2 fnext;   // F[(t+1) K]
+    fnext.x = __shfl_down_sync(mask, v[0].x, 1, 16);
+    fnext.y = __shfl_down_sync(mask, v[0].y, 1, 16);
+    if (t == 15) fnext = ftop;
+    // terms of D[j] = D[j+2] + 2 (j+1) F[j+1] dyde, j = t K + m
+    double2 w[K];
+#pragma unroll
+    for (int m = 0; m < K; ++m) {
+        const double s = 2.0 * (double)(t * K + m + 1);
+        const double2 fv = m + 1 < K ? v[m + 1] : fnext;
+        w[m] = make_double2(s * fv.x * dyde, s * fv.y * dyde);
+    }
+    // carries from above lane 15: D[NY] = 0, and D[NY-1] = 2 NY F[NY] dyde is lane 15's top term
+    double2 clo = make_double2(0.0, 0.0), chi = make_double2(0.0, 0.0);
+    double2 d[K];
+#pragma unroll
+    for (int m = 0; m < K; ++m) d[m] = make_double2(0.0, 0.0);
+    for (int r = 15; r >= 0; --r) {
+        if (t == r) {
+            // top two slots from the carries (lane 15: D[NY-1] is its term alone, D[NY-2] = D[NY] + term)
+            d[K - 1] = t == 15 ? w[K - 1] : make_double2(chi.x + w[K - 1].x, chi.y + w[K - 1].y);
+            d[K - 2] = make_double2(clo.x + w[K - 2].x, clo.y + w[K - 2].y);
+#pragma unroll
+            for (int m = K - 3; m >= 0; --m) d[m] = make_double2(d[m + 2].x + w[m].x, d[m + 2].y + w[m].y);
+        }
+        if (r > 0) {
+            chi.x = __shfl_sync(mask, d[1].x, r, 16);
+            chi.y = __shfl_sync(mask, d[1].y, r, 16);
+            clo.x = __shfl_sync(mask, d[0].x, r, 16);
+            clo.y = __shfl_sync(mask, d[0].y, r, 16);
+        }
+    }
+    if (t == 0) d[0] = make_double2(0.5 * d[0].x, 0.5 * d[0].y);
+    double2 *D = df + (size_t)col * NYP;
+#pragma unroll
+    for (int m = 0; m < K; ++m) D[t * K + m] = d[m];
+    if (t == 15) D[NY] = make_double2(0.0, 0.0);
+}
+
 int kmm_internal_cderiv(kmm_ctx *ctx, const double2 *f, double2 *df) {
     const int ncols = ctx->nz * ctx->nxh;
+    const int ny = ctx->nyp - 1;
+    if (ctx->use_colblk && ny % 16 == 0 && ny >= 32 && ny <= 128) {
+        const int nblk = (int)(((size_t)ncols * 16 + 127) / 128);
+        switch (ny / 16) {
+        case 2: k_cderiv_hw<2><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
+        case 3: k_cderiv_hw<3><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
+        case 4: k_cderiv_hw<4><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
+        case 5: k_cderiv_hw<5><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
+        case 6: k_cderiv_hw<6><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
+        case 7: k_cderiv_hw<7><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
+        case 8: k_cderiv_hw<8><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
+        }
+        CKL();
+        return KMM_OK;
+    }
     const size_t sm = tile_smem(ctx->nyp, 2);
     RET(kmm_smem_attr(ctx, (const void *)k_cderiv, sm));
     k_cderiv<<<(ncols + TILE - 1) / TILE, TPB, sm, ctx->stream>>>(f, df, ncols, ctx->nyp, ctx->dyde);
@@ -145,7 +216,13 @@ extern "C" int kmm_wallderiv(kmm_ctx *ctx, int f, int order, int wall, int out, 
 // ---------------------------------------------------------------------------
 // norm(a), helpers.f90:91-158
 // ---------------------------------------------------------------------------
-__global__ void k_norm(double2 *a, int nyp, int nz, int nxh, int nzh) {
+// one launch norms up to KMM_NORM_BATCH distinct fields, blockIdx.y picking the field
+struct NormList {
+    double2 *p[KMM_NORM_BATCH];
+};
+
+__global__ void k_norm(NormList list, int nyp, int nz, int nxh, int nzh) {
+    double2 *a = list.p[blockIdx.y];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int npair = nyp * (nz / 2);      // j = 1..nz/2 (0-based j = 0 handles the (0,0) mode)
     if (t < npair) {
@@ -169,12 +246,22 @@ __global__ void k_norm(double2 *a, int nyp, int nz, int nxh, int nzh) {
     }
 }
 
-int kmm_internal_norm(kmm_ctx *ctx, double2 *a) {
+int kmm_internal_norm_many(kmm_ctx *ctx, double2 *const *a, int nf) {
     const int n = ctx->nyp * (ctx->nz / 2) + ctx->nyp * ctx->nxh;
-    k_norm<<<(n + 255) / 256, 256, 0, ctx->stream>>>(a, ctx->nyp, ctx->nz, ctx->nxh, ctx->nzh);
-    CKL();
+    for (int f0 = 0; f0 < nf; f0 += KMM_NORM_BATCH) {
+        NormList list;
+        const int nb = nf - f0 < KMM_NORM_BATCH ? nf - f0 : KMM_NORM_BATCH;
+        for (int m = 0; m < nb; ++m) {
+            if (!a[f0 + m]) return KMM_ERR_NOMEM;
+            list.p[m] = a[f0 + m];
+        }
+        k_norm<<<dim3((n + 255) / 256, nb), 256, 0, ctx->stream>>>(list, ctx->nyp, ctx->nz, ctx->nxh, ctx->nzh);
+        CKL();
+    }
     return KMM_OK;
 }
+
+int kmm_internal_norm(kmm_ctx *ctx, double2 *a) { return kmm_internal_norm_many(ctx, &a, 1); }
 
 extern "C" int kmm_norm(kmm_ctx *ctx, int f) {
     if (!ctx || f < 0 || f >= KMM_NSPECTRAL) return KMM_ERR_ARG;
@@ -512,12 +599,14 @@ __device__ void cderiv1d_dev(const double *f, double *df, int nyp, double dyde) 
     df[0] = 0.5 * df[0];
 }
 
-__global__ void k_uzero(double *u0, const double *h1, const double *h1l, int nyp, double re, double dt, double th,
-                        double dyde, double at, double bt, double gtop, double ab, double bb, double gbot, double c0,
-                        double wz0, double *scratch) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// the serial body runs on one thread over shared-memory copies (every scratch row and the
+// profile itself), so each dependent step of the recurrences waits on a shared-memory load rather
+// than on an L2 round trip
+__device__ void uzero_body(double *u0, const double *h1, const double *h1l, int nyp, double re, double dt, double th,
+                           double dyde, double at, double bt, double gtop, double ab, double bb, double gbot, double c0,
+                           double wz0, double *scratch) {
     const int ny = nyp - 1, nyh = ny / 2, nyhm = nyh - 1, nyhp = nyh + 1;
-    const int L = KMM_MAX_NYP;
+    const int L = nyp;
     double *wrk1 = scratch, *t = scratch + L, *out = scratch + 2 * L;
     double *cs[2] = {scratch + 3 * L, scratch + 4 * L}, *ds[2] = {scratch + 5 * L, scratch + 6 * L};
     double *gs[2] = {scratch + 7 * L, scratch + 8 * L};
@@ -607,19 +696,41 @@ __global__ void k_uzero(double *u0, const double *h1, const double *h1l, int nyp
     for (int i = 0; i < nyp; ++i) u0[i] = out[i];
 }
 
+// shared memory: the profile, h1, h1l and nine scratch rows of nyp doubles
+static inline size_t uzero_smem(int nyp) { return sizeof(double) * 12 * (size_t)nyp; }
+
+__global__ void __launch_bounds__(128) k_uzero(double *u0, const double *h1, const double *h1l, int nyp, double re,
+                                               double dt, double th, double dyde, double at, double bt, double gtop,
+                                               double ab, double bb, double gbot, double c0, double wz0) {
+    extern __shared__ double su[];
+    double *su0 = su, *sh1 = su + nyp, *sh1l = su + 2 * nyp;
+    for (int i = threadIdx.x; i < nyp; i += blockDim.x) {
+        su0[i] = u0[i];
+        sh1[i] = h1[i];
+        sh1l[i] = h1l[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        uzero_body(su0, sh1, sh1l, nyp, re, dt, th, dyde, at, bt, gtop, ab, bb, gbot, c0, wz0, su + 3 * nyp);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nyp; i += blockDim.x) u0[i] = su0[i];
+}
+
 extern "C" int kmm_uzero(kmm_ctx *ctx, int uflag) {
     if (!ctx || (uflag != 1 && uflag != 3)) return KMM_ERR_ARG;
     double *u0 = REAL(ctx, uflag == 1 ? KMM_U0 : KMM_W0);
     double *h1 = REAL(ctx, uflag == 1 ? KMM_H1N : KMM_H3N);
     double *h1l = REAL(ctx, uflag == 1 ? KMM_H1NM1 : KMM_H3NM1);
     if (!u0 || !h1 || !h1l) return KMM_ERR_NOMEM;
+    const size_t sm = uzero_smem(ctx->nyp);
+    RET(kmm_smem_attr(ctx, (const void *)k_uzero, sm));
     // uflag 3 passes btu, as the reference does (solvers.f90:1173)
     if (uflag == 1)
-        k_uzero<<<1, 1, 0, ctx->stream>>>(u0, h1, h1l, ctx->nyp, ctx->re, ctx->dt, ctx->theta, ctx->dyde, ctx->atu,
-                                          ctx->btu, ctx->gtu, ctx->abu, ctx->bbu, ctx->gbu, ctx->h_c[0], ctx->h_wavz[0], ctx->d_scratch);
+        k_uzero<<<1, 128, sm, ctx->stream>>>(u0, h1, h1l, ctx->nyp, ctx->re, ctx->dt, ctx->theta, ctx->dyde, ctx->atu,
+                                             ctx->btu, ctx->gtu, ctx->abu, ctx->bbu, ctx->gbu, ctx->h_c[0], ctx->h_wavz[0]);
     else
-        k_uzero<<<1, 1, 0, ctx->stream>>>(u0, h1, h1l, ctx->nyp, ctx->re, ctx->dt, ctx->theta, ctx->dyde, ctx->atw,
-                                          ctx->btu, ctx->gtw, ctx->abw, ctx->bbw, ctx->gbw, ctx->h_c[0], ctx->h_wavz[0], ctx->d_scratch);
+        k_uzero<<<1, 128, sm, ctx->stream>>>(u0, h1, h1l, ctx->nyp, ctx->re, ctx->dt, ctx->theta, ctx->dyde, ctx->atw,
+                                             ctx->btu, ctx->gtw, ctx->abw, ctx->bbw, ctx->gbw, ctx->h_c[0], ctx->h_wavz[0]);
     CKL();
     return KMM_OK;
 }

@@ -141,6 +141,9 @@ static inline double *REAL(kmm_ctx *ctx, int f) { return (double *)kmm_field_ptr
 // internal entry points shared between translation units
 int kmm_internal_cderiv(kmm_ctx *ctx, const double2 *f, double2 *df);
 int kmm_internal_norm(kmm_ctx *ctx, double2 *a);
+// norm of nf distinct fields, KMM_NORM_BATCH to a launch (the same values as one call per field)
+#define KMM_NORM_BATCH 32
+int kmm_internal_norm_many(kmm_ctx *ctx, double2 *const *a, int nf);
 int kmm_internal_wallderiv(kmm_ctx *ctx, const double2 *f, int order, int wall, double2 *out, int iy);
 int kmm_internal_solve(kmm_ctx *ctx, double2 *u, double g, int ib, const double2 *bct, const double2 *bcb);
 // the routine solve / penta with the blocked column kernels (ny = 32, 64, 96, 128; ib = 0);

@@ -130,11 +130,26 @@ __global__ void k_add(double2 *y, const double2 *x, size_t n) {
         y[idx] = cadd(y[idx], x[idx]);
 }
 
+// norm of a list of distinct fields in one launch per KMM_NORM_BATCH of them
 static int norm_ids(kmm_ctx *ctx, const int *ids, int n) {
-    for (int m = 0; m < n; ++m) {
-        double2 *a = SPEC(ctx, ids[m]);
-        if (!a) return KMM_ERR_NOMEM;
-        RET(kmm_internal_norm(ctx, a));
+    double2 *a[KMM_NORM_BATCH];
+    for (int m0 = 0; m0 < n; m0 += KMM_NORM_BATCH) {
+        const int nb = n - m0 < KMM_NORM_BATCH ? n - m0 : KMM_NORM_BATCH;
+        for (int m = 0; m < nb; ++m) {
+            a[m] = SPEC(ctx, ids[m0 + m]);
+            if (!a[m]) return KMM_ERR_NOMEM;
+        }
+        RET(kmm_internal_norm_many(ctx, a, nb));
+    }
+    return KMM_OK;
+}
+
+static int norm_range(kmm_ctx *ctx, int first, int n) {
+    int ids[KMM_NORM_BATCH];
+    for (int m0 = 0; m0 < n; m0 += KMM_NORM_BATCH) {
+        const int nb = n - m0 < KMM_NORM_BATCH ? n - m0 : KMM_NORM_BATCH;
+        for (int m = 0; m < nb; ++m) ids[m] = first + m0 + m;
+        RET(norm_ids(ctx, ids, nb));
     }
     return KMM_OK;
 }
@@ -142,20 +157,14 @@ static int norm_ids(kmm_ctx *ctx, const int *ids, int n) {
 static const int kPolyComp[6] = {KMM_C11, KMM_C12, KMM_C13, KMM_C22, KMM_C23, KMM_C33};
 static const int kQp[6] = {KMM_QP11, KMM_QP12, KMM_QP13, KMM_QP22, KMM_QP23, KMM_QP33};
 
-static int poly_norm_c(kmm_ctx *ctx) {
-    for (int m = 0; m < 9; ++m) RET(kmm_norm(ctx, KMM_C11 + m));
-    return KMM_OK;
-}
+static int poly_norm_c(kmm_ctx *ctx) { return norm_range(ctx, KMM_C11, 9); }
 
-static int poly_norm_dc(kmm_ctx *ctx) {
-    for (int m = 0; m < 27; ++m) RET(kmm_norm(ctx, KMM_DC111 + m));
-    return KMM_OK;
-}
+static int poly_norm_dc(kmm_ctx *ctx) { return norm_range(ctx, KMM_DC111, 27); }
 
 static int poly_norm_out(kmm_ctx *ctx) {
     RET(poly_norm_c(ctx));
-    for (int m = 0; m < 6; ++m) RET(kmm_norm(ctx, KMM_C11N + m));
-    for (int m = 0; m < 6; ++m) RET(kmm_norm(ctx, KMM_STR11N + m));
+    RET(norm_range(ctx, KMM_C11N, 6));
+    RET(norm_range(ctx, KMM_STR11N, 6));
     return norm_ids(ctx, kQp, 6);
 }
 
