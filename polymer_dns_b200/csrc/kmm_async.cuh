@@ -1,0 +1,55 @@
+// kmm_async.cuh -- mbarrier and one-dimensional bulk-copy helpers (sm_90+ PTX) for kernels that
+// stage global rows into shared memory with the asynchronous copy engine.  Every wait is bounded:
+// after ~2 s of %globaltimer it gives up and returns false, and the caller records an error.
+#pragma once
+
+#include <stdint.h>
+
+namespace kasync {
+
+__device__ __forceinline__ uint32_t sm_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sm_addr(bar)), "r"(count) : "memory");
+}
+
+// make the initialised barriers visible to the asynchronous proxy
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm_addr(bar)), "r"(bytes) : "memory");
+}
+
+// wait for phase `phase` of a barrier, at most ~2 s; false if the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase) {
+    const unsigned long long t0 = gtimer();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(sm_addr(bar)), "r"(phase)
+            : "memory");
+        if (done) return true;
+        if (gtimer() - t0 > 2000000000ull) return false;
+    }
+}
+
+// global -> shared copy of `bytes` bytes (both addresses 16-byte aligned, bytes a multiple of 16),
+// completing on `bar` (no multicast)
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     sm_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(sm_addr(bar))
+                 : "memory");
+}
+
+}  // namespace kasync

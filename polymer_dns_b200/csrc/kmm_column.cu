@@ -599,121 +599,181 @@ __device__ void cderiv1d_dev(const double *f, double *df, int nyp, double dyde) 
     df[0] = 0.5 * df[0];
 }
 
-// the serial body runs on one thread over shared-memory copies (every scratch row and the
-// profile itself), so each dependent step of the recurrences waits on a shared-memory load rather
-// than on an L2 round trip
-__device__ void uzero_body(double *u0, const double *h1, const double *h1l, int nyp, double re, double dt, double th,
-                           double dyde, double at, double bt, double gtop, double ab, double bb, double gbot, double c0,
-                           double wz0, double *scratch) {
-    const int ny = nyp - 1, nyh = ny / 2, nyhm = nyh - 1, nyhp = nyh + 1;
+// The (0,0)-mode solve on one block, over shared-memory copies of the profile and every scratch
+// row.  What the serial reference does row by row with no dependence between rows (the right-hand
+// sides, the tau rows, the boundary rows t) is spread over the block's threads; the recurrences
+// (the elimination of each parity, the two boundary-row eliminations of each parity, the sum
+// into s, the back substitution of each parity) run on one thread each, the independent ones at
+// the same time.  Each value is formed by the same expression in the same order as the serial
+// loop (solvers.f90:1065-1493), so the result is the same to the bit.
+#define UZ_ROWS 26
+static inline size_t uzero_smem(int nyp) { return sizeof(double) * UZ_ROWS * (size_t)nyp; }
+
+__global__ void __launch_bounds__(128) k_uzero(double *u0g, const double *h1g, const double *h1lg, int nyp, double re,
+                                               double dt, double th, double dyde, double at, double bt, double gtop,
+                                               double ab, double bb, double gbot, double c0, double wz0) {
+    extern __shared__ double su[];
+    __shared__ double fq[2][2][2];   // [par][pass]: the final ff, the first term taken from s
     const int L = nyp;
-    double *wrk1 = scratch, *t = scratch + L, *out = scratch + 2 * L;
-    double *cs[2] = {scratch + 3 * L, scratch + 4 * L}, *ds[2] = {scratch + 5 * L, scratch + 6 * L};
-    double *gs[2] = {scratch + 7 * L, scratch + 8 * L};
-    for (int i = 0; i < nyp; ++i) wrk1[i] = -re * u0[i] / (dt * th) - re * (3.0 * h1[i] - h1l[i]) / (2.0 * th);
+    double *u0 = su, *h1 = su + L, *h1l = su + 2 * L, *wrk1 = su + 3 * L, *tmp = su + 4 * L, *out = su + 5 * L;
+    // per-parity rows (pointer arithmetic, not arrays of pointers, so nothing goes to local memory)
+#define UZ_ROW(r, par) (su + (size_t)((r) + (par)) * L)
+#define CS(par) UZ_ROW(6, par)     // sub-diagonal c
+#define DS(par) UZ_ROW(8, par)     // eliminated diagonal d
+#define GS(par) UZ_ROW(10, par)    // right-hand side g
+#define WRK(par) UZ_ROW(12, par)   // p1devns / p1dodds rows
+#define A2(par) UZ_ROW(14, par)    // tau-row diagonal
+#define A3(par) UZ_ROW(16, par)    // tau-row super-diagonal
+    // rows 18 .. 25: t and the ss terms q of (par, pass)
+    const int ny = nyp - 1, nyh = ny / 2, nyhm = nyh - 1, nyhp = nyh + 1;
+    const int tid = threadIdx.x, nth = blockDim.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < nyp; i += nth) {
+        u0[i] = u0g[i];
+        h1[i] = h1g[i];
+        h1l[i] = h1lg[i];
+    }
+    __syncthreads();
+    for (int i = tid; i < nyp; i += nth) wrk1[i] = -re * u0[i] / (dt * th) - re * (3.0 * h1[i] - h1l[i]) / (2.0 * th);
+    __syncthreads();
     if (th > 0.99) {
-        for (int i = 0; i < nyp; ++i) u0[i] = wrk1[i];
+        for (int i = tid; i < nyp; i += nth) u0[i] = wrk1[i];
     } else {
-        cderiv1d_dev(u0, t, nyp, dyde);
-        cderiv1d_dev(t, u0, nyp, dyde);
-        for (int i = 0; i < nyp; ++i) u0[i] = wrk1[i] - (1.0 - th) * u0[i] / th;
+        if (tid == 0) {
+            cderiv1d_dev(u0, tmp, nyp, dyde);
+            cderiv1d_dev(tmp, u0, nyp, dyde);
+        }
+        __syncthreads();
+        for (int i = tid; i < nyp; i += nth) u0[i] = wrk1[i] - (1.0 - th) * u0[i] / th;
     }
     const double g = re / (th * dt);
     // psolve1d, solvers.f90:1180-1245 with mixedbc1d (minus sign in tb, solvers.f90:1249-1269)
     const double wn = wz0 * wz0 + 0.0 + g;
-    double f[2][2], s[2];
-    double *wrk = wrk1;   // reuse
-    s[0] = gtop;
-    s[1] = gbot;
-    for (int par = 0; par < 2; ++par) {
-        const int n = par == 0 ? nyhp : nyh, m = n - 1, mm1 = m - 1;
-        // RHS rows (p1devns / p1dodds)
-        for (int q = 0; q < nyp; ++q) wrk[q] = 0.0;
+    for (int q = tid; q < 2 * nyp; q += nth) WRK(q / nyp)[q % nyp] = 0.0;
+    __syncthreads();
+    // right-hand-side rows (p1devns / p1dodds) and the tau rows of both parities, row by row
+    for (int e = tid; e < 2 * nyp; e += nth) {
+        const int par = e / nyp, i = e % nyp;
+        const int n = par == 0 ? nyhp : nyh, m = n - 1;
         if (par == 0) {
-            for (int i = 2; i <= nyhm; ++i) {
+            if (i >= 2 && i <= nyhm) {
                 int j = 2 * i - 2;
                 double rj1 = 1.0 / (double)(4 * j * (j - 1)), rj2 = 1.0 / (double)(2 * (j * j - 1)), rj3 = 1.0 / (double)(4 * j * (j + 1));
                 double cm = (j - 2 == 0) ? c0 : 1.0;
-                wrk[i - 1] = -cm * u0[j - 2] * rj1 + u0[j] * rj2 - u0[j + 2] * rj3;
+                WRK(0)[i - 1] = -cm * u0[j - 2] * rj1 + u0[j] * rj2 - u0[j + 2] * rj3;
+            } else if (i == nyh) {
+                int j = ny - 2;
+                double rj1 = 1.0 / (double)(4 * j * (j - 1)), rj2 = 1.0 / (double)(2 * (j * j - 1));
+                WRK(0)[nyh - 1] = -u0[j - 2] * rj1 + u0[j] * rj2;
+            } else if (i == nyhp) {
+                int j = ny;
+                double rj1 = 1.0 / (double)(4 * j * (j - 1));
+                WRK(0)[nyhp - 1] = -u0[j - 2] * rj1;
             }
-            int j = ny - 2;
-            double rj1 = 1.0 / (double)(4 * j * (j - 1)), rj2 = 1.0 / (double)(2 * (j * j - 1));
-            wrk[nyh - 1] = -u0[j - 2] * rj1 + u0[j] * rj2;
-            j = ny;
-            rj1 = 1.0 / (double)(4 * j * (j - 1));
-            wrk[nyhp - 1] = -u0[j - 2] * rj1;
         } else {
-            for (int i = 2; i <= nyhm - 1; ++i) {
+            if (i >= 2 && i <= nyhm - 1) {
                 int j = 2 * i - 1;
                 double rj1 = 1.0 / (double)(4 * j * (j - 1)), rj2 = 1.0 / (double)(2 * (j * j - 1)), rj3 = 1.0 / (double)(4 * j * (j + 1));
-                wrk[i - 1] = -u0[j - 2] * rj1 + u0[j] * rj2 - u0[j + 2] * rj3;
+                WRK(1)[i - 1] = -u0[j - 2] * rj1 + u0[j] * rj2 - u0[j + 2] * rj3;
+            } else if (i == nyhm) {
+                int j = ny - 3;
+                double rj1 = 1.0 / (double)(4 * j * (j - 1)), rj2 = 1.0 / (double)(2 * (j * j - 1));
+                WRK(1)[nyhm - 1] = -u0[j - 2] * rj1 + u0[j] * rj2;
+            } else if (i == nyh) {
+                int j = ny - 1;
+                double rj1 = 1.0 / (double)(4 * j * (j - 1));
+                WRK(1)[nyh - 1] = -u0[j - 2] * rj1;
             }
-            int j = ny - 3;
-            double rj1 = 1.0 / (double)(4 * j * (j - 1)), rj2 = 1.0 / (double)(2 * (j * j - 1));
-            wrk[nyhm - 1] = -u0[j - 2] * rj1 + u0[j] * rj2;
-            j = ny - 1;
-            rj1 = 1.0 / (double)(4 * j * (j - 1));
-            wrk[nyh - 1] = -u0[j - 2] * rj1;
         }
-        // p1dsolve
-        for (int i = 1; i <= m; ++i) { gs[par][i] = wrk[i - 1]; cs[par][i] = tau_row(i, par, wn, dyde, nyh, nyhm).a1; }
-        ds[par][m] = tau_row(m, par, wn, dyde, nyh, nyhm).a2;
-        gs[par][n] = wrk[n - 1];
+        if (i >= 1 && i <= m) {
+            const TauRow r = tau_row(i, par, wn, dyde, nyh, nyhm);
+            CS(par)[i] = r.a1;
+            A2(par)[i] = r.a2;
+            A3(par)[i] = r.a3;
+        }
+    }
+    __syncthreads();
+    // p1dsolve elimination: one thread per parity
+    if (lane == 0 && warp < 2) {
+        const int par = warp;
+        const int n = par == 0 ? nyhp : nyh, m = n - 1, mm1 = m - 1;
+        for (int i = 1; i <= m; ++i) GS(par)[i] = WRK(par)[i - 1];
+        DS(par)[m] = A2(par)[m];
+        GS(par)[n] = WRK(par)[n - 1];
         for (int i = mm1; i >= 1; --i) {
-            TauRow ri = tau_row(i, par, wn, dyde, nyh, nyhm);
-            ds[par][i] = ri.a2 - ri.a3 * cs[par][i + 1] / ds[par][i + 1];
-            gs[par][i + 1] = gs[par][i + 1] - ri.a3 * gs[par][i + 2] / ds[par][i + 1];
-        }
-        for (int ipass = 1; ipass <= 2; ++ipass) {
-            const int js = ipass == 1 ? 2 : 1;
-            for (int q = 1; q <= n; ++q) {
-                int jj = par == 0 ? 2 * q - 1 : 2 * q, j1 = jj - 1;
-                double v = ipass == 2 ? at + dyde * bt * (double)(j1 * j1) : ab - dyde * bb * (double)(j1 * j1);
-                if (ipass == 1 && jj % 2 == 0) v = -v;
-                t[q - 1] = v;
-            }
-            double ff = t[m - 1] - t[n - 1] * cs[par][m] / ds[par][m];
-            double ss = s[js - 1] - t[n - 1] * gs[par][n] / ds[par][m];
-            for (int i = mm1; i >= 1; --i) {
-                ss = ss - ff * gs[par][i + 1] / ds[par][i];
-                ff = t[i - 1] - ff * cs[par][i] / ds[par][i];
-            }
-            s[js - 1] = ss;
-            f[js - 1][par] = ff;
+            DS(par)[i] = A2(par)[i] - A3(par)[i] * CS(par)[i + 1] / DS(par)[i + 1];
+            GS(par)[i + 1] = GS(par)[i + 1] - A3(par)[i] * GS(par)[i + 2] / DS(par)[i + 1];
         }
     }
-    const double det = f[0][0] * f[1][1] - f[1][0] * f[0][1];
-    out[0] = (s[0] * f[1][1] - s[1] * f[0][1]) / det;
-    out[1] = (s[1] * f[0][0] - s[0] * f[1][0]) / det;
-    for (int i = 2; i <= nyhp; ++i) {
-        int ii = 2 * i - 1;
-        out[ii - 1] = (gs[0][i] - cs[0][i - 1] * out[ii - 3]) / ds[0][i - 1];
-    }
-    for (int i = 2; i <= nyh; ++i) {
-        int ii = 2 * i;
-        out[ii - 1] = (gs[1][i] - cs[1][i - 1] * out[ii - 3]) / ds[1][i - 1];
-    }
-    for (int i = 0; i < nyp; ++i) u0[i] = out[i];
-}
-
-// shared memory: the profile, h1, h1l and nine scratch rows of nyp doubles
-static inline size_t uzero_smem(int nyp) { return sizeof(double) * 12 * (size_t)nyp; }
-
-__global__ void __launch_bounds__(128) k_uzero(double *u0, const double *h1, const double *h1l, int nyp, double re,
-                                               double dt, double th, double dyde, double at, double bt, double gtop,
-                                               double ab, double bb, double gbot, double c0, double wz0) {
-    extern __shared__ double su[];
-    double *su0 = su, *sh1 = su + nyp, *sh1l = su + 2 * nyp;
-    for (int i = threadIdx.x; i < nyp; i += blockDim.x) {
-        su0[i] = u0[i];
-        sh1[i] = h1[i];
-        sh1l[i] = h1l[i];
+    // the boundary rows t of (par, pass)
+    for (int e = tid; e < 4 * nyp; e += nth) {
+        const int k = e / nyp, q = e % nyp + 1;
+        const int par = k >> 1, ipass = (k & 1) + 1;
+        const int n = par == 0 ? nyhp : nyh;
+        if (q <= n) {
+            int jj = par == 0 ? 2 * q - 1 : 2 * q, j1 = jj - 1;
+            double v = ipass == 2 ? at + dyde * bt * (double)(j1 * j1) : ab - dyde * bb * (double)(j1 * j1);
+            if (ipass == 1 && jj % 2 == 0) v = -v;
+            su[(size_t)(18 + k) * L + q - 1] = v;
+        }
     }
     __syncthreads();
-    if (threadIdx.x == 0)
-        uzero_body(su0, sh1, sh1l, nyp, re, dt, th, dyde, at, bt, gtop, ab, bb, gbot, c0, wz0, su + 3 * nyp);
+    // the boundary-row eliminations: one thread per (par, pass); the terms leaving s are kept
+    if (lane == 0) {
+        const int k = warp, par = k >> 1, ipass = (k & 1) + 1;
+        const int n = par == 0 ? nyhp : nyh, m = n - 1, mm1 = m - 1;
+        const double *t = su + (size_t)(18 + k) * L;
+        double *q = su + (size_t)(22 + k) * L;
+        double ff = t[m - 1] - t[n - 1] * CS(par)[m] / DS(par)[m];
+        fq[par][ipass - 1][1] = t[n - 1] * GS(par)[n] / DS(par)[m];
+        for (int i = mm1; i >= 1; --i) {
+            q[i] = ff * GS(par)[i + 1] / DS(par)[i];
+            ff = t[i - 1] - ff * CS(par)[i] / DS(par)[i];
+        }
+        fq[par][ipass - 1][0] = ff;
+    }
     __syncthreads();
-    for (int i = threadIdx.x; i < nyp; i += blockDim.x) u0[i] = su0[i];
+    // s in the reference's order (parity 0 then 1, pass 1 then 2), the 2x2 system for out(1:2)
+    if (tid == 0) {
+        double f[2][2], s[2];
+        s[0] = gtop;
+        s[1] = gbot;
+        for (int par = 0; par < 2; ++par) {
+            const int n = par == 0 ? nyhp : nyh, m = n - 1, mm1 = m - 1;
+            for (int ipass = 1; ipass <= 2; ++ipass) {
+                const int js = ipass == 1 ? 2 : 1;
+                const double *q = su + (size_t)(22 + 2 * par + ipass - 1) * L;
+                double ss = s[js - 1] - fq[par][ipass - 1][1];
+                for (int i = mm1; i >= 1; --i) ss = ss - q[i];
+                s[js - 1] = ss;
+                f[js - 1][par] = fq[par][ipass - 1][0];
+            }
+        }
+        const double det = f[0][0] * f[1][1] - f[1][0] * f[0][1];
+        out[0] = (s[0] * f[1][1] - s[1] * f[0][1]) / det;
+        out[1] = (s[1] * f[0][0] - s[0] * f[1][0]) / det;
+    }
+    __syncthreads();
+    // back substitution: one thread per parity
+    if (lane == 0 && warp == 0) {
+        for (int i = 2; i <= nyhp; ++i) {
+            int ii = 2 * i - 1;
+            out[ii - 1] = (GS(0)[i] - CS(0)[i - 1] * out[ii - 3]) / DS(0)[i - 1];
+        }
+    } else if (lane == 0 && warp == 1) {
+        for (int i = 2; i <= nyh; ++i) {
+            int ii = 2 * i;
+            out[ii - 1] = (GS(1)[i] - CS(1)[i - 1] * out[ii - 3]) / DS(1)[i - 1];
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < nyp; i += nth) u0g[i] = out[i];
+#undef CS
+#undef DS
+#undef GS
+#undef WRK
+#undef A2
+#undef A3
+#undef UZ_ROW
 }
 
 extern "C" int kmm_uzero(kmm_ctx *ctx, int uflag) {

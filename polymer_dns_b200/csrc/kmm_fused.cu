@@ -922,7 +922,6 @@ bool kmm_fused_applicable(const kmm_ctx *ctx) {
     return true;
 }
 
-static int *h_pin_status(kmm_ctx *ctx) { return (int *)(ctx->h_pin + 2 * KMM_MAX_NYP); }
 
 int kmm_tracers_enqueue(kmm_ctx *ctx, cudaStream_t st);
 
@@ -1222,7 +1221,7 @@ int kmm_fused_launch(kmm_ctx *ctx) {
     double *h_cfl = ctx->h_pin, *h_um = ctx->h_pin + KMM_MAX_NYP;
     CK(cudaMemcpyAsync(h_cfl, ctx->d_cfl, sizeof(double) * nyp, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(h_um, ctx->d_umax, sizeof(double) * nyp, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(h_pin_status(ctx), ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(kmm_h_pin_status(ctx), ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     return KMM_OK;
 }
 
@@ -1231,7 +1230,7 @@ int kmm_fused_finish(kmm_ctx *ctx) {
     CK(cudaStreamSynchronize(ctx->stream));
     const double *h_cfl = ctx->h_pin, *h_um = ctx->h_pin + KMM_MAX_NYP;
     int st = KMM_OK;
-    if (ctx->p.npart > 0 && *h_pin_status(ctx)) {
+    if (ctx->p.npart > 0 && *kmm_h_pin_status(ctx)) {
         kmm_set_error(ctx, "particle interpolation cell index out of range (part_track.f90:580-590)");
         st = KMM_ERR_INTERP;
     }

@@ -77,7 +77,7 @@ struct kmm_ctx {
     double *d_pumax;             // inertial particles: part_track's running max relative speed (umax1)
     double *d_umax;              // scratch for |u| max (per plane)
     double *d_scratch;           // 9*KMM_MAX_NYP doubles for the (0,0)-mode solver
-    double *h_pin;               // pinned host: cfl[KMM_MAX_NYP], umax[KMM_MAX_NYP], status (fused-step read-back)
+    double *h_pin;               // pinned host: cfl[KMM_MAX_NYP], umax[KMM_MAX_NYP], status (step read-backs)
     double *scsource;            // (nyp,mz,mx) scalar source (scl_flag = 2)
     DevPlan py2, pmz, pmx, pnx, pnz;
     DevPlan wy2, wmz, wmx;        // same lengths, radix-8-first factorisation for the warp FFT
@@ -137,6 +137,8 @@ int kmm_field_info(const kmm_ctx *ctx, int field, size_t *nelem, int *eb);
 void *kmm_field_ptr(kmm_ctx *ctx, int field);   // allocates (zeroed) on first use, NULL on failure
 static inline double2 *SPEC(kmm_ctx *ctx, int f) { return (double2 *)kmm_field_ptr(ctx, f); }
 static inline double *REAL(kmm_ctx *ctx, int f) { return (double *)kmm_field_ptr(ctx, f); }
+// the pinned status word after the cfl and umax rows of h_pin
+static inline int *kmm_h_pin_status(kmm_ctx *ctx) { return (int *)(ctx->h_pin + 2 * KMM_MAX_NYP); }
 
 // internal entry points shared between translation units
 int kmm_internal_cderiv(kmm_ctx *ctx, const double2 *f, double2 *df);

@@ -19,21 +19,47 @@
 
 #include "kmm_internal.cuh"
 #include "kmm_fft.cuh"
+#include "kmm_async.cuh"
 
 #define MAXIO 64
 
 struct FieldPtrs { const double2 *p[MAXIO]; };
 struct FieldPtrsW { double2 *p[MAXIO]; };
 
-// batched FFT of NB sequences of length N lying N apart in a (b: scratch of the same size) by the
-// block's 8 warps, NB / 8 sequences each, with the compile-time warp FFT; returns the buffer
-// holding the result, visible to the whole block
+// Block FFT buffers.  At the compiled lengths each of the 8 warps owns NQ = NB / 8 consecutive
+// sequences, stored swizzled (swz<C>, kmm_fft.cuh) within the warp's region, and the warps'
+// regions lie FB_PAD elements further apart than NQ n: the radix stages then run free of bank
+// conflicts, and so do the transposing loads and stores around the transform, whose 8 (or 16)
+// concurrent sequences would otherwise sit n apart on the same banks.  The runtime FFT of the
+// other lengths keeps the plain layout (sequence c at c n).
+#define FB_PAD 1
+
+// elements of one buffer (a or b) of NB sequences of length n
+__host__ __device__ constexpr int fb_len(int nb, int n) { return nb * n + 8 * FB_PAD; }
+
+__device__ __forceinline__ bool fb_compiled(int n) {
+    return n == 48 || n == 64 || n == 96 || n == 128 || n == 144 || n == 192 || n == 256;
+}
+
+// position of element i of sequence c (ct: n is a compiled length)
+template <typename C, int NB>
+__device__ __forceinline__ int fb_at(int c, int i, int n, bool ct) {
+    constexpr int NQ = NB / 8;
+    if (!ct) return c * n + i;
+    const int wq = c / NQ, q = c - wq * NQ;
+    return wq * (NQ * n + FB_PAD) + swz<C>(q * n + i);
+}
+
+// batched FFT of NB sequences of length N (layout of fb_at) by the block's 8 warps, NB / 8
+// sequences each, with the compile-time warp FFT; returns the buffer holding the result, visible
+// to the whole block
 template <typename C, int N, int S, int NB>
 __device__ __forceinline__ C *fft_block_ct(C *a, C *b, const C *tw) {
     constexpr int NQ = NB / 8;
     static_assert(NB % 8 == 0, "8 warps share the sequences");
-    const size_t w = (size_t)(threadIdx.x >> 5) * NQ * N;
-    C *r = fft_warp_ct<C, N, S, NQ, false>(a + w, b + w, tw);
+    static_assert(N % (sizeof(C) == 16 ? 8 : 16) == 0, "swizzle rows of 128 bytes");
+    const size_t w = (size_t)(threadIdx.x >> 5) * (NQ * N + FB_PAD);
+    C *r = fft_warp_ct<C, N, S, NQ, true>(a + w, b + w, tw);
     __syncthreads();
     return r - w;
 }
@@ -71,17 +97,19 @@ __global__ void __launch_bounds__(256) k_dct_fwd(FieldPtrs in, C *__restrict__ p
     const int f = blockIdx.y;
     const int col0 = blockIdx.x * DCT_CB;
     const int ncb = min(DCT_CB, ncols - col0);
-    C *a = sm, *b = sm + (size_t)DCT_CB * L;
+    C *a = sm, *b = sm + fb_len(DCT_CB, L);
+    const bool ct = fb_compiled(L);
     const double2 *src = in.p[f] + (size_t)col0 * nyp;
     for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
         const int c = e / nyp, i = e - c * nyp;
         const double2 w = src[e];
         const double fac = (i == 0 || i == ny) ? 1.0 : 0.5;   // c(i)/2.0
         const C v = kct::mk<C>((T)(w.x * fac), (T)(w.y * fac));
-        a[c * L + i] = v;
-        if (i > 0 && i < ny) a[c * L + L - i] = v;
+        a[fb_at<C, DCT_CB>(c, i, L, ct)] = v;
+        if (i > 0 && i < ny) a[fb_at<C, DCT_CB>(c, L - i, L, ct)] = v;
     }
-    for (int e = threadIdx.x + ncb * L; e < DCT_CB * L; e += blockDim.x) a[e] = kct::mk<C>((T)0, (T)0);
+    for (int e = threadIdx.x; e < (DCT_CB - ncb) * L; e += blockDim.x)
+        a[fb_at<C, DCT_CB>(ncb + e / L, e % L, L, ct)] = kct::mk<C>((T)0, (T)0);
     __syncthreads();
     C *r = fft_block<C, -1, DCT_CB>(P, a, b, tw, L);
     // PL[f][y][kx][kz]: col = kx*nz + kz
@@ -89,7 +117,7 @@ __global__ void __launch_bounds__(256) k_dct_fwd(FieldPtrs in, C *__restrict__ p
         const int y = e / ncb, c = e - y * ncb;
         const int col = col0 + c;
         const int kx = col / nz, kz = col - kx * nz;
-        pl[(((size_t)f * nyp + y) * nxh + kx) * nz + kz] = r[c * L + y];
+        pl[(((size_t)f * nyp + y) * nxh + kx) * nz + kz] = r[fb_at<C, DCT_CB>(c, y, L, ct)];
     }
 }
 
@@ -107,21 +135,22 @@ __global__ void __launch_bounds__(256) k_zfft_bwd(const C *__restrict__ pl, C *_
     const int kx0 = blockIdx.x * ZKB;
     const int nk = min(ZKB, nxh - kx0);
     const int nzh = nz / 2;
-    C *a = sm, *b = sm + (size_t)ZKB * mz;
-    for (int e = threadIdx.x; e < ZKB * mz; e += blockDim.x) a[e] = kct::mk<C>((T)0, (T)0);
+    C *a = sm, *b = sm + fb_len(ZKB, mz);
+    const bool ct = fb_compiled(mz);
+    for (int e = threadIdx.x; e < fb_len(ZKB, mz); e += blockDim.x) a[e] = kct::mk<C>((T)0, (T)0);
     __syncthreads();
     const C *src = pl + (((size_t)f * nyp + y) * nxh + kx0) * nz;
     for (int e = threadIdx.x; e < nk * nz; e += blockDim.x) {
         const int c = e / nz, j = e - c * nz;
         const int jj = (j < nzh) ? j : (mz - nz) + j;
-        a[c * mz + jj] = src[e];
+        a[fb_at<C, ZKB>(c, jj, mz, ct)] = src[e];
     }
     __syncthreads();
     C *r = fft_block<C, +1, ZKB>(P, a, b, tw, mz);
     C *dst = q + (((size_t)f * nyp + y) * mz) * nxh;
     for (int e = threadIdx.x; e < nk * mz; e += blockDim.x) {
         const int z = e / nk, c = e - z * nk;
-        dst[(size_t)z * nxh + kx0 + c] = r[c * mz + z];
+        dst[(size_t)z * nxh + kx0 + c] = r[fb_at<C, ZKB>(c, z, mz, ct)];
     }
 }
 
@@ -344,20 +373,44 @@ __global__ void __launch_bounds__(XW * 32) k_xphys2(const C *__restrict__ q, typ
                                                     const double *__restrict__ scsource,
                                                     const double *__restrict__ seght, double *__restrict__ cfl,
                                                     double *__restrict__ umax, const C *__restrict__ tw,
-                                                    PhysArgs A, Save3D sv, int nyp, int mz) {
+                                                    PhysArgs A, Save3D sv, int nyp, int mz, int *status) {
     typedef typename kct::Real<C>::T T;
     constexpr int NXH = MX / 3, HX = MX / 2;
+    constexpr unsigned ROWB = NXH * sizeof(C);   // one field's row of kx modes
+    static_assert(ROWB % 16 == 0 && (MX * sizeof(T)) % 16 == 0, "16-byte bulk copies");
     extern __shared__ double2 smd[];
     C *fab = reinterpret_cast<C *>(smd);                                  // per warp: a, b [MX]
     T *phys = reinterpret_cast<T *>(fab + (size_t)XW * 2 * MX);           // [nin][MX]
+    __shared__ uint64_t xbar[MAXIO / 2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int z = blockIdx.x, y = blockIdx.y;
     C *a = fab + (size_t)warp * 2 * MX, *b = a + MX;
     const int npairs = (A.nin + 1) / 2;
+    // every input row of this (y, z) goes into the first 2 MX / 3 reals of its field's phys row by
+    // one bulk copy, issued up front (one barrier per field pair), so the whole row set is in
+    // flight at once; each pair's transform later overwrites its own rows only
+    if (threadIdx.x == 0) {
+        for (int pr = 0; pr < npairs; ++pr) kasync::mbar_init(&xbar[pr], 1);
+        kasync::mbar_init_fence();
+        for (int pr = 0; pr < npairs; ++pr) {
+            const int f = 2 * pr, g = f + 1 < A.nin ? f + 1 : -1;
+            kasync::mbar_expect_tx(&xbar[pr], g >= 0 ? 2 * ROWB : ROWB);
+            kasync::bulk_g2s(phys + (size_t)f * MX, q + (((size_t)f * nyp + y) * mz + z) * NXH, ROWB, &xbar[pr]);
+            if (g >= 0)
+                kasync::bulk_g2s(phys + (size_t)g * MX, q + (((size_t)g * nyp + y) * mz + z) * NXH, ROWB, &xbar[pr]);
+        }
+    }
+    __syncthreads();
+    bool ok = true;
     for (int pr = warp; pr < npairs; pr += XW) {
         const int f = 2 * pr, g = f + 1 < A.nin ? f + 1 : -1;
-        const C *qa = q + (((size_t)f * nyp + y) * mz + z) * NXH;
-        const C *qb = g >= 0 ? q + (((size_t)g * nyp + y) * mz + z) * NXH : qa;
+        // every lane waits (its own acquire of the copied rows); the warp goes on only if all saw them
+        if (!__all_sync(0xffffffffu, kasync::mbar_wait(&xbar[pr], 0))) {
+            ok = false;
+            continue;
+        }
+        const C *qa = reinterpret_cast<const C *>(phys + (size_t)f * MX);
+        const C *qb = g >= 0 ? reinterpret_cast<const C *>(phys + (size_t)g * MX) : qa;
         for (int k = lane; k < MX; k += 32) {
             const int kk = k <= HX ? k : MX - k;   // source mode
             C A_ = kct::mk<C>((T)0, (T)0), B_ = A_;
@@ -377,6 +430,12 @@ __global__ void __launch_bounds__(XW * 32) k_xphys2(const C *__restrict__ q, typ
             if (g >= 0) phys[(size_t)g * MX + x] = v.y;
         }
         __syncwarp();
+    }
+    if (!__all_sync(0xffffffffu, ok)) {
+        // a copy that never completed: record it, give the copies in flight a second bounded wait
+        // (shared memory must outlive them) and leave this row
+        if (lane == 0) atomicMax(status, KMM_ERR_TIMEOUT);
+        for (int pr = warp; pr < npairs; pr += XW) kasync::mbar_wait(&xbar[pr], 0);
     }
     __syncthreads();
     double cmax = 0.0, umx = 0.0;
@@ -536,11 +595,12 @@ __global__ void __launch_bounds__(256) k_zfft_fwd(const C *__restrict__ q, C *__
     const int kx0 = blockIdx.x * ZKB;
     const int nk = min(ZKB, nxh - kx0);
     const int nzh = nz / 2;
-    C *a = sm, *b = sm + (size_t)ZKB * mz;
+    C *a = sm, *b = sm + fb_len(ZKB, mz);
+    const bool ct = fb_compiled(mz);
     const C *src = q + (((size_t)f * nyp + y) * mz) * nxh;
     for (int e = threadIdx.x; e < ZKB * mz; e += blockDim.x) {
         const int z = e / ZKB, c = e - z * ZKB;
-        a[c * mz + z] = c < nk ? src[(size_t)z * nxh + kx0 + c] : kct::mk<C>((T)0, (T)0);
+        a[fb_at<C, ZKB>(c, z, mz, ct)] = c < nk ? src[(size_t)z * nxh + kx0 + c] : kct::mk<C>((T)0, (T)0);
     }
     __syncthreads();
     C *r = fft_block<C, -1, ZKB>(P, a, b, tw, mz);
@@ -548,7 +608,7 @@ __global__ void __launch_bounds__(256) k_zfft_fwd(const C *__restrict__ q, C *__
     for (int e = threadIdx.x; e < nk * nz; e += blockDim.x) {
         const int c = e / nz, j = e - c * nz;
         const int jj = (j < nzh) ? j : (mz - nz) + j;
-        const C v = r[c * mz + jj];
+        const C v = r[fb_at<C, ZKB>(c, jj, mz, ct)];
         dst[e] = kct::mk<C>((T)(v.x / scale), (T)(v.y / scale));
     }
 }
@@ -566,23 +626,24 @@ __global__ void __launch_bounds__(256) k_dct_bwd(const C *__restrict__ pl, Field
     const int f = blockIdx.y;
     const int col0 = blockIdx.x * DCT_CB;
     const int ncb = min(DCT_CB, ncols - col0);
-    C *a = sm, *b = sm + (size_t)DCT_CB * L;
-    for (int e = threadIdx.x; e < DCT_CB * L; e += blockDim.x) a[e] = kct::mk<C>((T)0, (T)0);
+    C *a = sm, *b = sm + fb_len(DCT_CB, L);
+    const bool ct = fb_compiled(L);
+    for (int e = threadIdx.x; e < fb_len(DCT_CB, L); e += blockDim.x) a[e] = kct::mk<C>((T)0, (T)0);
     __syncthreads();
     for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
         const int y = e / ncb, c = e - y * ncb;
         const int col = col0 + c;
         const int kx = col / nz, kz = col - kx * nz;
         const C v = pl[(((size_t)f * nyp + y) * nxh + kx) * nz + kz];
-        a[c * L + y] = v;
-        if (y > 0 && y < ny) a[c * L + L - y] = v;
+        a[fb_at<C, DCT_CB>(c, y, L, ct)] = v;
+        if (y > 0 && y < ny) a[fb_at<C, DCT_CB>(c, L - y, L, ct)] = v;
     }
     __syncthreads();
     C *r = fft_block<C, -1, DCT_CB>(P, a, b, tw, L);
     double2 *dst = out.p[f] + (size_t)col0 * nyp;
     for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
         const int c = e / nyp, i = e - c * nyp;
-        const C rv = r[c * L + i];
+        const C rv = r[fb_at<C, DCT_CB>(c, i, L, ct)];
         double2 v = make_double2((double)rv.x / (double)ny, (double)rv.y / (double)ny);
         if (i == 0 || i == ny) v = make_double2(v.x / 2.0, v.y / 2.0);
         dst[e] = v;
@@ -711,6 +772,7 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     auto add_in = [&](int slot, int fid) -> int {
         double2 *p = SPEC(ctx, fid);
         if (!p) return KMM_ERR_NOMEM;
+        if (nin >= MAXIO) return KMM_ERR_UNSUPPORTED;
         A.slot_of_in[slot] = nin;
         in.p[nin++] = p;
         return KMM_OK;
@@ -718,6 +780,7 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     auto add_out = [&](int slot, int fid) -> int {
         double2 *p = SPEC(ctx, fid);
         if (!p) return KMM_ERR_NOMEM;
+        if (nout >= MAXIO) return KMM_ERR_UNSUPPORTED;
         A.slot_of_out[slot] = nout;
         outp.p[nout++] = p;
         return KMM_OK;
@@ -809,8 +872,8 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         }
     }
 
-    const size_t sm_dct = sizeof(double2) * 2 * DCT_CB * 2 * ctx->ny;
-    const size_t sm_z = sizeof(double2) * 2 * ZKB * mz;
+    const size_t sm_dct = sizeof(double2) * 2 * (size_t)fb_len(DCT_CB, 2 * ctx->ny);
+    const size_t sm_z = sizeof(double2) * 2 * (size_t)fb_len(ZKB, mz);
     const size_t sm_x = sizeof(double) * (size_t)nin * XZB * mx + sizeof(double2) * 2 * XZB * mx;
     const size_t sm_xf = sizeof(double2) * 2 * XZB * mx;
     RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd<double2>, sm_dct));
@@ -852,7 +915,7 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
             ctx->pl_in, ctx->q_in, ctx->pmz, ctx->pmz.tw, nyp, nz, nxh, mz);
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_BWD);
-    bool fast_done = false;
+    bool fast_done = false, xstat = false;
     const bool sc_source = scal && ctx->p.scl_flag >= 2;
     if (!poly && !ib_any && !inertial && !sc_source && !f32) {
         // fused warp-per-row x stage (no polymer, no immersed boundary, no inertial particles, no
@@ -866,6 +929,8 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     }
     if (!fast_done) {
         kmm_tic(ctx);
+        // status of the x stage's bulk copies (KMM_ERR_TIMEOUT), read back with the CFL numbers
+        CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
         const size_t eb = f32 ? sizeof(float) : sizeof(double);   // bytes per real of the intermediates
         const size_t sm_x2 = eb * (size_t)nin * mx + 2 * eb * 2 * XW * (size_t)mx;
 #define XP2(MM, CC, QQ, PO, TW)                                                                                  \
@@ -873,7 +938,7 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         RET(kmm_smem_attr(ctx, (const void *)k_xphys2<MM, CC>, sm_x2));                                          \
         k_xphys2<MM, CC><<<dim3(mz, nyp), XW * 32, sm_x2, ctx->stream>>>(                                         \
             QQ, PO, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl,          \
-            ctx->d_umax, TW, A, sv, nyp, mz);                                                                    \
+            ctx->d_umax, TW, A, sv, nyp, mz, ctx->d_status);                                                     \
     } while (0)
 #define XP2S(MM)                                                                                                 \
     do {                                                                                                         \
@@ -894,6 +959,8 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
 #undef XP2S
 #undef XP2
         CKL();
+        CK(cudaMemcpyAsync(kmm_h_pin_status(ctx), ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        xstat = true;
         kmm_toc(ctx, KMM_STAGE_XPHYS);
         if (ib_any && ctx->kmaxsurf > 0) {
             const int ksp = ctx->kmaxsurf < nyp ? ctx->kmaxsurf : nyp;
@@ -974,6 +1041,10 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     }
     ctx->stats.cflmax = nan ? NAN : cflmax;
     ctx->stats.umax = umax;
+    if (xstat && *kmm_h_pin_status(ctx) == KMM_ERR_TIMEOUT) {
+        kmm_set_error(ctx, "x stage: a bulk copy of the input rows did not complete");
+        st = KMM_ERR_TIMEOUT;
+    }
     if (st == KMM_OK && nan) st = KMM_ERR_NAN;
     if (st == KMM_OK && cflmax > 1.0) st = KMM_ERR_CFL;
     ctx->stats.status = st;
@@ -1085,8 +1156,8 @@ extern "C" int kmm_calcswirl(kmm_ctx *ctx) {
     double *sw = REAL(ctx, KMM_SWIRL3D);
     if (!sw) return KMM_ERR_NOMEM;
     RET(kmm_ensure_plane_buffers(ctx, 9, 0));
-    const size_t sm_dct = sizeof(double2) * 2 * DCT_CB * 2 * ctx->ny;
-    const size_t sm_z = sizeof(double2) * 2 * ZKB * mz;
+    const size_t sm_dct = sizeof(double2) * 2 * (size_t)fb_len(DCT_CB, 2 * ctx->ny);
+    const size_t sm_z = sizeof(double2) * 2 * (size_t)fb_len(ZKB, mz);
     const size_t sm_s = sizeof(double2) * (size_t)SW_WARPS * 7 * mx;
     RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd<double2>, sm_dct));
     RET(kmm_smem_attr(ctx, (const void *)k_zfft_bwd<double2>, sm_z));
@@ -1169,7 +1240,7 @@ extern "C" int kmm_flowstats(kmm_ctx *ctx, double *prof, double *scal) {
     in.p[2] = SPEC(ctx, KMM_W);
     in.p[3] = du;
     RET(kmm_ensure_plane_buffers(ctx, 4, 0));
-    const size_t sm_dct = sizeof(double2) * 2 * DCT_CB * 2 * ctx->ny;
+    const size_t sm_dct = sizeof(double2) * 2 * (size_t)fb_len(DCT_CB, 2 * ctx->ny);
     RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd<double2>, sm_dct));
     k_dct_fwd<double2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, 4), 256, sm_dct, ctx->stream>>>(in, ctx->pl_in, ctx->py2,
                                                                                                ctx->py2.tw, nyp, nz,
