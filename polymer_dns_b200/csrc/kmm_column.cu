@@ -72,64 +72,95 @@ __global__ void __launch_bounds__(TPB) k_cderiv(const double2 *__restrict__ f, d
 // The same two chains with a half-warp per column for ny = 16 K: lane t holds the K consecutive
 // coefficients t K .. t K + K - 1 in registers and the chains run lane by lane from the top, the
 // carries D[(t+1) K] and D[(t+1) K + 1] handed down by shuffles, so every D[i] is the same sum in
-// the same order as above (bitwise equal) while the columns keep the whole SM busy.
+// the same order as above (bitwise equal) while the columns keep the whole SM busy.  The block's
+// 8 columns (one contiguous run in global memory) pass through shared memory with coalesced loads
+// and stores; coefficient i sits at i + i / K there, so a lane's K values start K + 1 slots after
+// its neighbour's and the 16 lanes' accesses spread over the banks.
 template <int K>
 __global__ void __launch_bounds__(128) k_cderiv_hw(const double2 *f, double2 *df, int ncols, double dyde) {
-    constexpr int NY = 16 * K, NYP = NY + 1;
-    const int col = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 4);
-    if (col >= ncols) return;   // whole half-warps
-    const int t = threadIdx.x & 15;
-    // both columns of the warp present -> the full mask; else the present half alone
-    const unsigned mask = (col | 1) < ncols ? 0xffffffffu : ((threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu);
-    const double2 *F = f + (size_t)col * NYP;
-    double2 v[K];
+    constexpr int NY = 16 * K, NYP = NY + 1, SK = K + 1, CS = 16 * SK + 1;
+    __shared__ double2 s[8 * CS];
+    const int col0 = blockIdx.x * 8;
+    const int ncb = min(8, ncols - col0);
+    const double2 *src = f + (size_t)col0 * NYP;
+    {   // every load of the block's columns in flight at once, then into shared memory
+        constexpr int NLD = (8 * NYP + 127) / 128;
+        double2 tmp[NLD];
 #pragma unroll
-    for (int m = 0; m < K; ++m) v[m] = F[t * K + m];
-    const double2 ftop = F[NY];
-    double2 fnext;   // F[(t+1) K]
-    fnext.x = __shfl_down_sync(mask, v[0].x, 1, 16);
-    fnext.y = __shfl_down_sync(mask, v[0].y, 1, 16);
-    if (t == 15) fnext = ftop;
-    // terms of D[j] = D[j+2] + 2 (j+1) F[j+1] dyde, j = t K + m
-    double2 w[K];
-#pragma unroll
-    for (int m = 0; m < K; ++m) {
-        const double s = 2.0 * (double)(t * K + m + 1);
-        const double2 fv = m + 1 < K ? v[m + 1] : fnext;
-        w[m] = make_double2(s * fv.x * dyde, s * fv.y * dyde);
-    }
-    // carries from above lane 15: D[NY] = 0, and D[NY-1] = 2 NY F[NY] dyde is lane 15's top term
-    double2 clo = make_double2(0.0, 0.0), chi = make_double2(0.0, 0.0);
-    double2 d[K];
-#pragma unroll
-    for (int m = 0; m < K; ++m) d[m] = make_double2(0.0, 0.0);
-    for (int r = 15; r >= 0; --r) {
-        if (t == r) {
-            // top two slots from the carries (lane 15: D[NY-1] is its term alone, D[NY-2] = D[NY] + term)
-            d[K - 1] = t == 15 ? w[K - 1] : make_double2(chi.x + w[K - 1].x, chi.y + w[K - 1].y);
-            d[K - 2] = make_double2(clo.x + w[K - 2].x, clo.y + w[K - 2].y);
-#pragma unroll
-            for (int m = K - 3; m >= 0; --m) d[m] = make_double2(d[m + 2].x + w[m].x, d[m + 2].y + w[m].y);
+        for (int u = 0; u < NLD; ++u) {
+            const int e = threadIdx.x + 128 * u;
+            if (e < ncb * NYP) tmp[u] = src[e];
         }
-        if (r > 0) {
-            chi.x = __shfl_sync(mask, d[1].x, r, 16);
-            chi.y = __shfl_sync(mask, d[1].y, r, 16);
-            clo.x = __shfl_sync(mask, d[0].x, r, 16);
-            clo.y = __shfl_sync(mask, d[0].y, r, 16);
+#pragma unroll
+        for (int u = 0; u < NLD; ++u) {
+            const int e = threadIdx.x + 128 * u;
+            if (e < ncb * NYP) {
+                const int c = e / NYP, i = e - c * NYP;
+                s[c * CS + i + i / K] = tmp[u];
+            }
         }
     }
-    if (t == 0) d[0] = make_double2(0.5 * d[0].x, 0.5 * d[0].y);
-    double2 *D = df + (size_t)col * NYP;
+    __syncthreads();
+    const int c = threadIdx.x >> 4, t = threadIdx.x & 15;
+    if (c < ncb) {
+        // both columns of the warp present -> the full mask; else the present half alone
+        const unsigned mask = (c | 1) < ncb ? 0xffffffffu : ((threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu);
+        double2 *S = s + c * CS;
+        double2 v[K];
 #pragma unroll
-    for (int m = 0; m < K; ++m) D[t * K + m] = d[m];
-    if (t == 15) D[NY] = make_double2(0.0, 0.0);
+        for (int m = 0; m < K; ++m) v[m] = S[t * SK + m];
+        const double2 ftop = S[16 * SK];
+        double2 fnext;   // F[(t+1) K]
+        fnext.x = __shfl_down_sync(mask, v[0].x, 1, 16);
+        fnext.y = __shfl_down_sync(mask, v[0].y, 1, 16);
+        if (t == 15) fnext = ftop;
+        // terms of D[j] = D[j+2] + 2 (j+1) F[j+1] dyde, j = t K + m
+        double2 w[K];
+#pragma unroll
+        for (int m = 0; m < K; ++m) {
+            const double sc = 2.0 * (double)(t * K + m + 1);
+            const double2 fv = m + 1 < K ? v[m + 1] : fnext;
+            w[m] = make_double2(sc * fv.x * dyde, sc * fv.y * dyde);
+        }
+        // carries from above lane 15: D[NY] = 0, and D[NY-1] = 2 NY F[NY] dyde is lane 15's top term
+        double2 clo = make_double2(0.0, 0.0), chi = make_double2(0.0, 0.0);
+        double2 d[K];
+#pragma unroll
+        for (int m = 0; m < K; ++m) d[m] = make_double2(0.0, 0.0);
+        for (int r = 15; r >= 0; --r) {
+            if (t == r) {
+                // top two slots from the carries (lane 15: D[NY-1] is its term alone, D[NY-2] = D[NY] + term)
+                d[K - 1] = t == 15 ? w[K - 1] : make_double2(chi.x + w[K - 1].x, chi.y + w[K - 1].y);
+                d[K - 2] = make_double2(clo.x + w[K - 2].x, clo.y + w[K - 2].y);
+#pragma unroll
+                for (int m = K - 3; m >= 0; --m) d[m] = make_double2(d[m + 2].x + w[m].x, d[m + 2].y + w[m].y);
+            }
+            if (r > 0) {
+                chi.x = __shfl_sync(mask, d[1].x, r, 16);
+                chi.y = __shfl_sync(mask, d[1].y, r, 16);
+                clo.x = __shfl_sync(mask, d[0].x, r, 16);
+                clo.y = __shfl_sync(mask, d[0].y, r, 16);
+            }
+        }
+        if (t == 0) d[0] = make_double2(0.5 * d[0].x, 0.5 * d[0].y);
+        __syncwarp(mask);   // every lane of the column has read its values before they are overwritten
+#pragma unroll
+        for (int m = 0; m < K; ++m) S[t * SK + m] = d[m];
+        if (t == 15) S[16 * SK] = make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    double2 *dst = df + (size_t)col0 * NYP;
+    for (int e = threadIdx.x; e < ncb * NYP; e += blockDim.x) {
+        const int c2 = e / NYP, i = e - c2 * NYP;
+        dst[e] = s[c2 * CS + i + i / K];
+    }
 }
 
 int kmm_internal_cderiv(kmm_ctx *ctx, const double2 *f, double2 *df) {
     const int ncols = ctx->nz * ctx->nxh;
     const int ny = ctx->nyp - 1;
     if (ctx->use_colblk && ny % 16 == 0 && ny >= 32 && ny <= 128) {
-        const int nblk = (int)(((size_t)ncols * 16 + 127) / 128);
+        const int nblk = (ncols + 7) / 8;
         switch (ny / 16) {
         case 2: k_cderiv_hw<2><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
         case 3: k_cderiv_hw<3><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;

@@ -87,6 +87,7 @@ __device__ C *fft_block(const DevPlan &P, C *a, C *b, const C *tw, int n) {
 // 1. forward Chebyshev -> physical y (scaled by c(i)/2), columns -> plane layout
 // ---------------------------------------------------------------------------
 #define DCT_CB 8
+#define LDG 4   // global loads per thread issued together in the transforms' staging loops
 template <typename C>
 __global__ void __launch_bounds__(256) k_dct_fwd(FieldPtrs in, C *__restrict__ pl, DevPlan P, const C *__restrict__ tw,
                                                  int nyp, int nz, int nxh, int ncols) {
@@ -100,13 +101,23 @@ __global__ void __launch_bounds__(256) k_dct_fwd(FieldPtrs in, C *__restrict__ p
     C *a = sm, *b = sm + fb_len(DCT_CB, L);
     const bool ct = fb_compiled(L);
     const double2 *src = in.p[f] + (size_t)col0 * nyp;
-    for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
-        const int c = e / nyp, i = e - c * nyp;
-        const double2 w = src[e];
-        const double fac = (i == 0 || i == ny) ? 1.0 : 0.5;   // c(i)/2.0
-        const C v = kct::mk<C>((T)(w.x * fac), (T)(w.y * fac));
-        a[fb_at<C, DCT_CB>(c, i, L, ct)] = v;
-        if (i > 0 && i < ny) a[fb_at<C, DCT_CB>(c, L - i, L, ct)] = v;
+    // loads in groups of LDG per thread, all in flight before their shared-memory stores
+    for (int e0 = threadIdx.x; e0 < ncb * nyp; e0 += LDG * 256) {
+        double2 wv[LDG];
+#pragma unroll
+        for (int u = 0; u < LDG; ++u)
+            if (e0 + 256 * u < ncb * nyp) wv[u] = src[e0 + 256 * u];
+#pragma unroll
+        for (int u = 0; u < LDG; ++u) {
+            const int e = e0 + 256 * u;
+            if (e >= ncb * nyp) break;
+            const int c = e / nyp, i = e - c * nyp;
+            const double2 w = wv[u];
+            const double fac = (i == 0 || i == ny) ? 1.0 : 0.5;   // c(i)/2.0
+            const C v = kct::mk<C>((T)(w.x * fac), (T)(w.y * fac));
+            a[fb_at<C, DCT_CB>(c, i, L, ct)] = v;
+            if (i > 0 && i < ny) a[fb_at<C, DCT_CB>(c, L - i, L, ct)] = v;
+        }
     }
     for (int e = threadIdx.x; e < (DCT_CB - ncb) * L; e += blockDim.x)
         a[fb_at<C, DCT_CB>(ncb + e / L, e % L, L, ct)] = kct::mk<C>((T)0, (T)0);
@@ -140,10 +151,19 @@ __global__ void __launch_bounds__(256) k_zfft_bwd(const C *__restrict__ pl, C *_
     for (int e = threadIdx.x; e < fb_len(ZKB, mz); e += blockDim.x) a[e] = kct::mk<C>((T)0, (T)0);
     __syncthreads();
     const C *src = pl + (((size_t)f * nyp + y) * nxh + kx0) * nz;
-    for (int e = threadIdx.x; e < nk * nz; e += blockDim.x) {
-        const int c = e / nz, j = e - c * nz;
-        const int jj = (j < nzh) ? j : (mz - nz) + j;
-        a[fb_at<C, ZKB>(c, jj, mz, ct)] = src[e];
+    for (int e0 = threadIdx.x; e0 < nk * nz; e0 += LDG * 256) {
+        C wv[LDG];
+#pragma unroll
+        for (int u = 0; u < LDG; ++u)
+            if (e0 + 256 * u < nk * nz) wv[u] = src[e0 + 256 * u];
+#pragma unroll
+        for (int u = 0; u < LDG; ++u) {
+            const int e = e0 + 256 * u;
+            if (e >= nk * nz) break;
+            const int c = e / nz, j = e - c * nz;
+            const int jj = (j < nzh) ? j : (mz - nz) + j;
+            a[fb_at<C, ZKB>(c, jj, mz, ct)] = wv[u];
+        }
     }
     __syncthreads();
     C *r = fft_block<C, +1, ZKB>(P, a, b, tw, mz);
@@ -512,8 +532,10 @@ __global__ void k_spread(PO_T *__restrict__ po, const double *__restrict__ drag,
     if (y + 1 > kmaxsurf) return;
     const size_t n3 = (size_t)nyp * nplane;
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nplane; e += (size_t)gridDim.x * blockDim.x) {
-        // target t in reference flat order: t = jt + kt*mz (0-based)
-        const long t = (long)e;
+        // target t in reference flat order: t = jt + kt*mz (0-based); consecutive threads take
+        // consecutive kt, the contiguous x index of po and drag
+        const int jt = (int)(e / mx), kt = (int)(e % mx);
+        const long t = (long)jt + (long)kt * mz;
         double ax = 0.0, ay = 0.0, az = 0.0;
         for (int ii = -2; ii <= 2; ++ii)
             for (int jj = -2; jj <= 2; ++jj) {
@@ -532,7 +554,6 @@ __global__ void k_spread(PO_T *__restrict__ po, const double *__restrict__ drag,
                 ay += sw * drag[n3 + gq];
                 az += sw * drag[2 * n3 + gq];
             }
-        const int jt = (int)(t % mz), kt = (int)(t / mz);
         const size_t gt = ((size_t)y * mz + jt) * mx + kt;
         if (o1 >= 0) po[(size_t)o1 * n3 + gt] = (PO_T)((double)po[(size_t)o1 * n3 + gt] + ax);
         if (o2 >= 0) po[(size_t)o2 * n3 + gt] = (PO_T)((double)po[(size_t)o2 * n3 + gt] + ay);
@@ -598,9 +619,21 @@ __global__ void __launch_bounds__(256) k_zfft_fwd(const C *__restrict__ q, C *__
     C *a = sm, *b = sm + fb_len(ZKB, mz);
     const bool ct = fb_compiled(mz);
     const C *src = q + (((size_t)f * nyp + y) * mz) * nxh;
-    for (int e = threadIdx.x; e < ZKB * mz; e += blockDim.x) {
-        const int z = e / ZKB, c = e - z * ZKB;
-        a[fb_at<C, ZKB>(c, z, mz, ct)] = c < nk ? src[(size_t)z * nxh + kx0 + c] : kct::mk<C>((T)0, (T)0);
+    for (int e0 = threadIdx.x; e0 < ZKB * mz; e0 += LDG * 256) {
+        C wv[LDG];
+#pragma unroll
+        for (int u = 0; u < LDG; ++u) {
+            const int e = e0 + 256 * u;
+            const int z = e / ZKB, c = e - z * ZKB;
+            wv[u] = (e < ZKB * mz && c < nk) ? src[(size_t)z * nxh + kx0 + c] : kct::mk<C>((T)0, (T)0);
+        }
+#pragma unroll
+        for (int u = 0; u < LDG; ++u) {
+            const int e = e0 + 256 * u;
+            if (e >= ZKB * mz) break;
+            const int z = e / ZKB, c = e - z * ZKB;
+            a[fb_at<C, ZKB>(c, z, mz, ct)] = wv[u];
+        }
     }
     __syncthreads();
     C *r = fft_block<C, -1, ZKB>(P, a, b, tw, mz);
@@ -630,13 +663,26 @@ __global__ void __launch_bounds__(256) k_dct_bwd(const C *__restrict__ pl, Field
     const bool ct = fb_compiled(L);
     for (int e = threadIdx.x; e < fb_len(DCT_CB, L); e += blockDim.x) a[e] = kct::mk<C>((T)0, (T)0);
     __syncthreads();
-    for (int e = threadIdx.x; e < ncb * nyp; e += blockDim.x) {
-        const int y = e / ncb, c = e - y * ncb;
-        const int col = col0 + c;
-        const int kx = col / nz, kz = col - kx * nz;
-        const C v = pl[(((size_t)f * nyp + y) * nxh + kx) * nz + kz];
-        a[fb_at<C, DCT_CB>(c, y, L, ct)] = v;
-        if (y > 0 && y < ny) a[fb_at<C, DCT_CB>(c, L - y, L, ct)] = v;
+    for (int e0 = threadIdx.x; e0 < ncb * nyp; e0 += LDG * 256) {
+        C wv[LDG];
+#pragma unroll
+        for (int u = 0; u < LDG; ++u) {
+            const int e = e0 + 256 * u;
+            if (e < ncb * nyp) {
+                const int y = e / ncb, c = e - y * ncb;
+                const int col = col0 + c;
+                const int kx = col / nz, kz = col - kx * nz;
+                wv[u] = pl[(((size_t)f * nyp + y) * nxh + kx) * nz + kz];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < LDG; ++u) {
+            const int e = e0 + 256 * u;
+            if (e >= ncb * nyp) break;
+            const int y = e / ncb, c = e - y * ncb;
+            a[fb_at<C, DCT_CB>(c, y, L, ct)] = wv[u];
+            if (y > 0 && y < ny) a[fb_at<C, DCT_CB>(c, L - y, L, ct)] = wv[u];
+        }
     }
     __syncthreads();
     C *r = fft_block<C, -1, DCT_CB>(P, a, b, tw, L);
