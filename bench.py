@@ -44,6 +44,10 @@ def load_peaks():
         return PEAKS_FALLBACK, "fallback"
 
 
+# --grid N: the cfg2 / cfg3 workload at N x (N+1) x N (small cases for single-kernel profiles)
+GRID_OVERRIDE = None
+
+
 def make_config(name, precision=0):
     from polymer_dns_b200 import abi
     if name == "cfg1":
@@ -61,6 +65,10 @@ def make_config(name, precision=0):
         if name == "cfg3":
             kw.update(polymer_on=1, zlmax=30.0, tpoly=20.0, qbeta=0.9, diffpoly=1000.0, gain=-400.0, ugain=-40.0)
             desc += ", FENE-P (Wi=20, beta=0.9, L^2=900), IB cylinder r=0.25 at (pi,0)"
+        if GRID_OVERRIDE:
+            n = GRID_OVERRIDE
+            kw.update(nx=n, ny=n, nz=n)
+            desc = desc.replace("128x129x128", "%dx%dx%d" % (n, n + 1, n))
         p = abi.default_params(**kw)
         init = dict(profile="loglaw", amp=0.1, kmax=8, seed=1)
     else:
@@ -575,7 +583,11 @@ def main():
     ap.add_argument("--no-polymer", action="store_true", help="skip the polymer + IB (FP64 / mixed) measurement")
     ap.add_argument("--ztma", type=int, default=None, choices=[0, 1],
                     help="inverse z transform with TMA tile copies (1, the library default) or plain loads (0)")
+    ap.add_argument("--grid", type=int, default=None,
+                    help="run the cfg2 / cfg3 workload at N x (N+1) x N instead of 128 x 129 x 128 (profiling)")
     a = ap.parse_args()
+    global GRID_OVERRIDE
+    GRID_OVERRIDE = a.grid
     if a.warmup < 3:
         a.warmup = 3
     rank = int(os.environ.get("RANK", 0))
