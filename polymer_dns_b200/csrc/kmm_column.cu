@@ -76,10 +76,18 @@ __global__ void __launch_bounds__(TPB) k_cderiv(const double2 *__restrict__ f, d
 // 8 columns (one contiguous run in global memory) pass through shared memory with coalesced loads
 // and stores; coefficient i sits at i + i / K there, so a lane's K values start K + 1 slots after
 // its neighbour's and the 16 lanes' accesses spread over the banks.
+// up to KMM_CDERIV_BATCH independent (input, output) pairs per launch, blockIdx.y picking the pair
+struct CderivList {
+    const double2 *f[KMM_CDERIV_BATCH];
+    double2 *df[KMM_CDERIV_BATCH];
+};
+
 template <int K>
-__global__ void __launch_bounds__(128) k_cderiv_hw(const double2 *f, double2 *df, int ncols, double dyde) {
+__global__ void __launch_bounds__(128) k_cderiv_hw(CderivList list, int ncols, double dyde) {
     constexpr int NY = 16 * K, NYP = NY + 1, SK = K + 1, CS = 16 * SK + 1;
     __shared__ double2 s[8 * CS];
+    const double2 *f = list.f[blockIdx.y];
+    double2 *df = list.df[blockIdx.y];
     const int col0 = blockIdx.x * 8;
     const int ncb = min(8, ncols - col0);
     const double2 *src = f + (size_t)col0 * NYP;
@@ -156,29 +164,42 @@ __global__ void __launch_bounds__(128) k_cderiv_hw(const double2 *f, double2 *df
     }
 }
 
-int kmm_internal_cderiv(kmm_ctx *ctx, const double2 *f, double2 *df) {
+int kmm_internal_cderiv_many(kmm_ctx *ctx, const double2 *const *f, double2 *const *df, int n) {
     const int ncols = ctx->nz * ctx->nxh;
     const int ny = ctx->nyp - 1;
     if (ctx->use_colblk && ny % 16 == 0 && ny >= 32 && ny <= 128) {
         const int nblk = (ncols + 7) / 8;
-        switch (ny / 16) {
-        case 2: k_cderiv_hw<2><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
-        case 3: k_cderiv_hw<3><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
-        case 4: k_cderiv_hw<4><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
-        case 5: k_cderiv_hw<5><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
-        case 6: k_cderiv_hw<6><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
-        case 7: k_cderiv_hw<7><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
-        case 8: k_cderiv_hw<8><<<nblk, 128, 0, ctx->stream>>>(f, df, ncols, ctx->dyde); break;
+        for (int p0 = 0; p0 < n; p0 += KMM_CDERIV_BATCH) {
+            const int nb = n - p0 < KMM_CDERIV_BATCH ? n - p0 : KMM_CDERIV_BATCH;
+            CderivList list;
+            for (int m = 0; m < nb; ++m) {
+                list.f[m] = f[p0 + m];
+                list.df[m] = df[p0 + m];
+            }
+            const dim3 grid(nblk, nb);
+            switch (ny / 16) {
+            case 2: k_cderiv_hw<2><<<grid, 128, 0, ctx->stream>>>(list, ncols, ctx->dyde); break;
+            case 3: k_cderiv_hw<3><<<grid, 128, 0, ctx->stream>>>(list, ncols, ctx->dyde); break;
+            case 4: k_cderiv_hw<4><<<grid, 128, 0, ctx->stream>>>(list, ncols, ctx->dyde); break;
+            case 5: k_cderiv_hw<5><<<grid, 128, 0, ctx->stream>>>(list, ncols, ctx->dyde); break;
+            case 6: k_cderiv_hw<6><<<grid, 128, 0, ctx->stream>>>(list, ncols, ctx->dyde); break;
+            case 7: k_cderiv_hw<7><<<grid, 128, 0, ctx->stream>>>(list, ncols, ctx->dyde); break;
+            case 8: k_cderiv_hw<8><<<grid, 128, 0, ctx->stream>>>(list, ncols, ctx->dyde); break;
+            }
+            CKL();
         }
-        CKL();
         return KMM_OK;
     }
     const size_t sm = tile_smem(ctx->nyp, 2);
     RET(kmm_smem_attr(ctx, (const void *)k_cderiv, sm));
-    k_cderiv<<<(ncols + TILE - 1) / TILE, TPB, sm, ctx->stream>>>(f, df, ncols, ctx->nyp, ctx->dyde);
-    CKL();
+    for (int m = 0; m < n; ++m) {
+        k_cderiv<<<(ncols + TILE - 1) / TILE, TPB, sm, ctx->stream>>>(f[m], df[m], ncols, ctx->nyp, ctx->dyde);
+        CKL();
+    }
     return KMM_OK;
 }
+
+int kmm_internal_cderiv(kmm_ctx *ctx, const double2 *f, double2 *df) { return kmm_internal_cderiv_many(ctx, &f, &df, 1); }
 
 extern "C" int kmm_cderiv(kmm_ctx *ctx, int f, int df) {
     if (!ctx || f == df) return KMM_ERR_ARG;
@@ -1018,8 +1039,11 @@ extern "C" int kmm_vort(kmm_ctx *ctx) {
     double2 *u = SPEC(ctx, KMM_U), *v = SPEC(ctx, KMM_V), *w = SPEC(ctx, KMM_W);
     double2 *omx = SPEC(ctx, KMM_OMX), *omz = SPEC(ctx, KMM_OMZ);
     if (!u || !v || !w || !omx || !omz) return KMM_ERR_NOMEM;
-    RET(kmm_internal_cderiv(ctx, u, omz));
-    RET(kmm_internal_cderiv(ctx, w, omx));
+    {
+        const double2 *in[2] = {u, w};
+        double2 *out[2] = {omz, omx};
+        RET(kmm_internal_cderiv_many(ctx, in, out, 2));
+    }
     k_vort<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(v, omx, omz, ctx->d_wavx, ctx->d_wavz, ctx->nspec,
                                                                  ctx->nyp, ctx->nz);
     CKL();
@@ -1054,12 +1078,12 @@ extern "C" int kmm_gradv(kmm_ctx *ctx) {
     if (!ctx) return KMM_ERR_ARG;
     double2 *u = SPEC(ctx, KMM_U), *v = SPEC(ctx, KMM_V), *w = SPEC(ctx, KMM_W);
     double2 *u12 = SPEC(ctx, KMM_U12), *u22 = SPEC(ctx, KMM_U22), *u32 = SPEC(ctx, KMM_U32);
-    RET(kmm_internal_cderiv(ctx, u, u12));
-    RET(kmm_internal_cderiv(ctx, v, u22));
-    RET(kmm_internal_cderiv(ctx, w, u32));
-    RET(kmm_internal_cderiv(ctx, u12, ctx->wrk[0]));
-    RET(kmm_internal_cderiv(ctx, u22, ctx->wrk[1]));
-    RET(kmm_internal_cderiv(ctx, u32, ctx->wrk[2]));
+    {
+        const double2 *in1[3] = {u, v, w}, *in2[3] = {u12, u22, u32};
+        double2 *out1[3] = {u12, u22, u32}, *out2[3] = {ctx->wrk[0], ctx->wrk[1], ctx->wrk[2]};
+        RET(kmm_internal_cderiv_many(ctx, in1, out1, 3));
+        RET(kmm_internal_cderiv_many(ctx, in2, out2, 3));
+    }
     k_gradv<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(
         u, v, w, SPEC(ctx, KMM_U11), SPEC(ctx, KMM_U21), SPEC(ctx, KMM_U31), SPEC(ctx, KMM_U13), SPEC(ctx, KMM_U23),
         SPEC(ctx, KMM_U33), SPEC(ctx, KMM_LU), SPEC(ctx, KMM_LV), SPEC(ctx, KMM_LW), ctx->wrk[0], ctx->wrk[1],
@@ -1091,9 +1115,18 @@ extern "C" int kmm_gradscl(kmm_ctx *ctx) {
 
 extern "C" int kmm_derivscji(kmm_ctx *ctx) {
     if (!ctx) return KMM_ERR_ARG;
+    {   // the nine y derivatives in one launch, then the x / z ones
+        const double2 *in[9];
+        double2 *out[9];
+        for (int ij = 0; ij < 9; ++ij) {
+            in[ij] = SPEC(ctx, KMM_C11 + ij);
+            out[ij] = SPEC(ctx, KMM_DC111 + 3 * ij + 1);
+            if (!in[ij] || !out[ij]) return KMM_ERR_NOMEM;
+        }
+        RET(kmm_internal_cderiv_many(ctx, in, out, 9));
+    }
     for (int ij = 0; ij < 9; ++ij) {
         double2 *cf = SPEC(ctx, KMM_C11 + ij);
-        RET(kmm_internal_cderiv(ctx, cf, SPEC(ctx, KMM_DC111 + 3 * ij + 1)));
         k_dxdz<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(cf, SPEC(ctx, KMM_DC111 + 3 * ij),
                                                                      SPEC(ctx, KMM_DC111 + 3 * ij + 2), ctx->d_wavx,
                                                                      ctx->d_wavz, ctx->nspec, ctx->nyp, ctx->nz);
@@ -1211,9 +1244,11 @@ extern "C" int kmm_polyforce(kmm_ctx *ctx) {
     if (!ctx) return KMM_ERR_ARG;
     double2 *s11 = SPEC(ctx, KMM_QP11), *s12 = SPEC(ctx, KMM_QP12), *s13 = SPEC(ctx, KMM_QP13);
     double2 *s22 = SPEC(ctx, KMM_QP22), *s23 = SPEC(ctx, KMM_QP23), *s33 = SPEC(ctx, KMM_QP33);
-    RET(kmm_internal_cderiv(ctx, s12, ctx->wrk[0]));
-    RET(kmm_internal_cderiv(ctx, s22, ctx->wrk[1]));
-    RET(kmm_internal_cderiv(ctx, s23, ctx->wrk[2]));
+    {
+        const double2 *in[3] = {s12, s22, s23};
+        double2 *out[3] = {ctx->wrk[0], ctx->wrk[1], ctx->wrk[2]};
+        RET(kmm_internal_cderiv_many(ctx, in, out, 3));
+    }
     k_polyforce<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(
         s11, s12, s13, s22, s23, s33, ctx->wrk[0], ctx->wrk[1], ctx->wrk[2], SPEC(ctx, KMM_T1), SPEC(ctx, KMM_T2),
         SPEC(ctx, KMM_T3), ctx->d_wavx, ctx->d_wavz, ctx->nspec, ctx->nyp, ctx->nz);

@@ -142,6 +142,10 @@ static inline int *kmm_h_pin_status(kmm_ctx *ctx) { return (int *)(ctx->h_pin + 
 
 // internal entry points shared between translation units
 int kmm_internal_cderiv(kmm_ctx *ctx, const double2 *f, double2 *df);
+// cderiv of n independent (input, output) pairs, KMM_CDERIV_BATCH to a launch (no output may be
+// another pair's input; an output may be its own pair's input)
+#define KMM_CDERIV_BATCH 16
+int kmm_internal_cderiv_many(kmm_ctx *ctx, const double2 *const *f, double2 *const *df, int n);
 int kmm_internal_norm(kmm_ctx *ctx, double2 *a);
 // norm of nf distinct fields, KMM_NORM_BATCH to a launch (the same values as one call per field)
 #define KMM_NORM_BATCH 32

@@ -64,6 +64,37 @@ def test_cderiv_wallderiv_norm(rt, oracle_mod, grid):
     assert np.array_equal(g.download("WRKC"), o.get("WRKC"))
 
 
+@pytest.mark.parametrize("ny", [48, 64, 96, 128])
+def test_cderiv_half_warp_is_bitwise(rt, oracle_mod, ny):
+    """cderiv at ny = 16 K runs a half-warp per column with the chains handed lane to lane; the
+    sums keep the serial order, so the result is bitwise the oracle's."""
+    p = kc.cfg_small(20, ny, 12)
+    g, o = _pair(rt, oracle_mod, p)
+    rng = np.random.default_rng(17 + ny)
+    a = kc.random_spectral(rng, p, hermitian=False)
+    _put(g, o, "WRKC", a)
+    g.call("cderiv", "WRKC", "WRK1")
+    o.call("cderiv", "WRKC", "WRK1")
+    assert np.array_equal(g.download("WRK1"), o.get("WRK1"))
+
+
+@pytest.mark.parametrize("ny,theta", [(16, 0.5), (32, 1.0), (64, 0.5), (128, 0.5), (128, 1.0)])
+def test_uzero_block_solve(rt, oracle_mod, ny, theta):
+    """The (0,0)-mode solve with its row work spread over a block and its recurrences on single
+    threads, against the oracle for both theta branches (theta > 0.99 skips the two cderivs)."""
+    p = kc.cfg_small(16, ny, 12, theta=theta)
+    g, o = _pair(rt, oracle_mod, p)
+    rng = np.random.default_rng(5 + ny)
+    for name in ("U0", "W0", "H1N", "H1NM1", "H3N", "H3NM1"):
+        v = np.zeros(p.ny + 1)
+        v[: min(12, p.ny + 1)] = rng.standard_normal(min(12, p.ny + 1))
+        _put(g, o, name, v)
+    for uflag, name in ((1, "U0"), (3, "W0")):
+        g.call("uzero", uflag)
+        o.call("uzero", uflag)
+        _cmp(g, o, name)
+
+
 @pytest.mark.parametrize("grid", GRIDS)
 def test_tau_solvers(rt, oracle_mod, grid):
     p = kc.cfg_small(*grid)
