@@ -378,14 +378,17 @@ __global__ void __launch_bounds__(256) k_xphys(const double2 *__restrict__ q, do
 }
 
 // 3'. the same x stage for the compiled lengths MX = 48, 96, 144, 192 (nx = 32 .. 128): one block
-// per (y, z) row, XW warps.  Each warp takes field pairs in turn: the Hermitian extension of A + iB
-// (modes nxh .. mx - nxh not carried; c2r ignores Im of the DC mode) through the compile-time
-// warp FFT into the row's physical table in shared memory; then the block evaluates the pointwise
-// terms.  The generic k_xphys tiles two rows per block and transforms them with the runtime
-// block FFT; this form keeps more independent FFTs in flight per SM.
-#define XW 4
+// per (y, z) row, XPW warps.  Each warp takes field pairs in turn: the Hermitian extension of
+// A + iB (modes nxh .. mx - nxh not carried; c2r ignores Im of the DC mode) through the
+// compile-time warp FFT into the row's physical table in shared memory; then the block evaluates
+// the pointwise terms.  The two physical rows of a pair are one buffer of MX complex values, which
+// serves as the FFT's second (ping-pong) buffer once the pair's input has been read out of it, so
+// a warp needs only one private buffer and two 8-warp blocks fit on an SM even with 55 fields.
+// The generic k_xphys tiles two rows per block and transforms them with the runtime block FFT.
+#define XW 4    // warps of k_xfwd2
+#define XPW 8   // warps of k_xphys2
 template <int MX, typename C>
-__global__ void __launch_bounds__(XW * 32) k_xphys2(const C *__restrict__ q, typename kct::Real<C>::T *__restrict__ po,
+__global__ void __launch_bounds__(XPW * 32) k_xphys2(const C *__restrict__ q, typename kct::Real<C>::T *__restrict__ po,
                                                     double *__restrict__ drag, double *__restrict__ up3,
                                                     double *__restrict__ vp3, double *__restrict__ wp3,
                                                     const int *__restrict__ imatrix, double *__restrict__ fxi,
@@ -395,16 +398,16 @@ __global__ void __launch_bounds__(XW * 32) k_xphys2(const C *__restrict__ q, typ
                                                     double *__restrict__ umax, const C *__restrict__ tw,
                                                     PhysArgs A, Save3D sv, int nyp, int mz, int *status) {
     typedef typename kct::Real<C>::T T;
-    constexpr int NXH = MX / 3, HX = MX / 2;
+    constexpr int NXH = MX / 3;
     constexpr unsigned ROWB = NXH * sizeof(C);   // one field's row of kx modes
     static_assert(ROWB % 16 == 0 && (MX * sizeof(T)) % 16 == 0, "16-byte bulk copies");
     extern __shared__ double2 smd[];
-    C *fab = reinterpret_cast<C *>(smd);                                  // per warp: a, b [MX]
-    T *phys = reinterpret_cast<T *>(fab + (size_t)XW * 2 * MX);           // [nin][MX]
+    C *fab = reinterpret_cast<C *>(smd);                                  // per warp: a [MX]
+    T *phys = reinterpret_cast<T *>(fab + (size_t)XPW * MX);              // [nin rounded up to even][MX]
     __shared__ uint64_t xbar[MAXIO / 2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int z = blockIdx.x, y = blockIdx.y;
-    C *a = fab + (size_t)warp * 2 * MX, *b = a + MX;
+    C *a = fab + (size_t)warp * MX;
     const int npairs = (A.nin + 1) / 2;
     // every input row of this (y, z) goes into the first 2 MX / 3 reals of its field's phys row by
     // one bulk copy, issued up front (one barrier per field pair), so the whole row set is in
@@ -422,8 +425,9 @@ __global__ void __launch_bounds__(XW * 32) k_xphys2(const C *__restrict__ q, typ
     }
     __syncthreads();
     bool ok = true;
-    for (int pr = warp; pr < npairs; pr += XW) {
+    for (int pr = warp; pr < npairs; pr += XPW) {
         const int f = 2 * pr, g = f + 1 < A.nin ? f + 1 : -1;
+        C *b = reinterpret_cast<C *>(phys + (size_t)f * MX);   // the pair's rows f, f + 1
         // every lane waits (its own acquire of the copied rows); the warp goes on only if all saw them
         if (!__all_sync(0xffffffffu, kasync::mbar_wait(&xbar[pr], 0))) {
             ok = false;
@@ -431,23 +435,32 @@ __global__ void __launch_bounds__(XW * 32) k_xphys2(const C *__restrict__ q, typ
         }
         const C *qa = reinterpret_cast<const C *>(phys + (size_t)f * MX);
         const C *qb = g >= 0 ? reinterpret_cast<const C *>(phys + (size_t)g * MX) : qa;
-        for (int k = lane; k < MX; k += 32) {
-            const int kk = k <= HX ? k : MX - k;   // source mode
-            C A_ = kct::mk<C>((T)0, (T)0), B_ = A_;
-            if (kk < NXH) {
-                A_ = qa[kk];
-                if (g >= 0) B_ = qb[kk];
-            }
-            if (k == 0 || k == HX) { A_.y = (T)0; B_.y = (T)0; }
-            a[swz<C>(k)] = k <= HX ? kct::mk<C>(A_.x - B_.y, A_.y + B_.x)     // A + iB
-                                   : kct::mk<C>(A_.x + B_.y, -A_.y + B_.x);   // conj(A) + i conj(B)
+        // Hermitian extension: Z_k = A_k + i B_k for k < nxh, conj(A) + i conj(B) at mx - k, and the
+        // modes nxh .. mx - nxh (the Nyquist mode mx / 2 among them) not carried
+        const C zc = kct::mk<C>((T)0, (T)0);
+        for (int k = NXH + lane; k <= MX - NXH; k += 32) a[swz<C>(k)] = zc;
+        for (int kk = lane; kk < NXH; kk += 32) {
+            C A_ = qa[kk], B_ = g >= 0 ? qb[kk] : zc;
+            if (kk == 0) { A_.y = (T)0; B_.y = (T)0; }   // c2r ignores Im of the mean mode
+            a[swz<C>(kk)] = kct::mk<C>(A_.x - B_.y, A_.y + B_.x);
+            if (kk > 0) a[swz<C>(MX - kk)] = kct::mk<C>(A_.x + B_.y, -A_.y + B_.x);
         }
         __syncwarp();
         const C *r = fft_warp_ct<C, MX, +1, 1, true>(a, b, tw);
-        for (int x = lane; x < MX; x += 32) {
-            const C v = r[swz<C>(x)];
-            phys[(size_t)f * MX + x] = v.x;
-            if (g >= 0) phys[(size_t)g * MX + x] = v.y;
+        // the result may sit in the pair's own rows: read it all before writing the real rows
+        constexpr int E = (MX + 31) / 32;
+        C rv[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+            if (lane + 32 * e < MX) rv[e] = r[swz<C>(lane + 32 * e)];
+        __syncwarp();
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int x = lane + 32 * e;
+            if (x < MX) {
+                phys[(size_t)f * MX + x] = rv[e].x;
+                if (g >= 0) phys[(size_t)g * MX + x] = rv[e].y;
+            }
         }
         __syncwarp();
     }
@@ -455,7 +468,7 @@ __global__ void __launch_bounds__(XW * 32) k_xphys2(const C *__restrict__ q, typ
         // a copy that never completed: record it, give the copies in flight a second bounded wait
         // (shared memory must outlive them) and leave this row
         if (lane == 0) atomicMax(status, KMM_ERR_TIMEOUT);
-        for (int pr = warp; pr < npairs; pr += XW) kasync::mbar_wait(&xbar[pr], 0);
+        for (int pr = warp; pr < npairs; pr += XPW) kasync::mbar_wait(&xbar[pr], 0);
     }
     __syncthreads();
     double cmax = 0.0, umx = 0.0;
@@ -465,7 +478,7 @@ __global__ void __launch_bounds__(XW * 32) k_xphys2(const C *__restrict__ q, typ
         xphys_point(in, A, sv, y, z, k, nyp, mz, MX, sg, po, drag, up3, vp3, wp3, imatrix, fxi, fyi, fzi, scsource, cmax,
                     umx);
     }
-    __shared__ double red[2][XW];
+    __shared__ double red[2][XPW];
     for (int off = 16; off; off >>= 1) {
         const double c2 = __shfl_down_sync(0xffffffffu, cmax, off);
         const double u2 = __shfl_down_sync(0xffffffffu, umx, off);
@@ -475,7 +488,7 @@ __global__ void __launch_bounds__(XW * 32) k_xphys2(const C *__restrict__ q, typ
     if (lane == 0) { red[0][warp] = cmax; red[1][warp] = umx; }
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int w = 1; w < XW; ++w) {
+        for (int w = 1; w < XPW; ++w) {
             cmax = (red[0][w] != red[0][w]) ? red[0][w] : fmax(cmax, red[0][w]);
             umx = fmax(umx, red[1][w]);
         }
@@ -978,11 +991,11 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         // status of the x stage's bulk copies (KMM_ERR_TIMEOUT), read back with the CFL numbers
         CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
         const size_t eb = f32 ? sizeof(float) : sizeof(double);   // bytes per real of the intermediates
-        const size_t sm_x2 = eb * (size_t)nin * mx + 2 * eb * 2 * XW * (size_t)mx;
+        const size_t sm_x2 = eb * (size_t)(nin + (nin & 1)) * mx + 2 * eb * XPW * (size_t)mx;
 #define XP2(MM, CC, QQ, PO, TW)                                                                                  \
     do {                                                                                                         \
         RET(kmm_smem_attr(ctx, (const void *)k_xphys2<MM, CC>, sm_x2));                                          \
-        k_xphys2<MM, CC><<<dim3(mz, nyp), XW * 32, sm_x2, ctx->stream>>>(                                         \
+        k_xphys2<MM, CC><<<dim3(mz, nyp), XPW * 32, sm_x2, ctx->stream>>>(                                         \
             QQ, PO, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl,          \
             ctx->d_umax, TW, A, sv, nyp, mz, ctx->d_status);                                                     \
     } while (0)
