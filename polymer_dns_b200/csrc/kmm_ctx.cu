@@ -435,11 +435,16 @@ extern "C" int kmm_event_elapsed(kmm_ctx *ctx, int a, int b, double *ms) {
     return KMM_OK;
 }
 
-// raise a kernel's dynamic shared-memory limit to `bytes` (>48 KB needs the opt-in; max 227 KB)
+// raise a kernel's dynamic shared-memory limit to `bytes` (static + dynamic above 48 KB needs the
+// opt-in; max 227 KB)
 int kmm_smem_attr(kmm_ctx *ctx, const void *func, size_t bytes) {
-    if (bytes <= 48 * 1024) return KMM_OK;
-    if (bytes > 227 * 1024) {
-        kmm_set_error(ctx, "kernel needs %zu bytes of shared memory (> 227 KB)", bytes);
+    if (bytes <= 16 * 1024) return KMM_OK;   // the kernels here keep < 32 KB static shared memory
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, func));
+    const size_t total = bytes + fa.sharedSizeBytes;
+    if (total <= 48 * 1024) return KMM_OK;
+    if (total > 227 * 1024) {
+        kmm_set_error(ctx, "kernel needs %zu bytes of shared memory (> 227 KB)", total);
         return KMM_ERR_UNSUPPORTED;
     }
     // while a step is being captured into a graph the attribute is already set by the uncaptured

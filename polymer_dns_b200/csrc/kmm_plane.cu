@@ -386,9 +386,15 @@ __global__ void __launch_bounds__(256) k_xphys(const double2 *__restrict__ q, do
 // a warp needs only one private buffer and two 8-warp blocks fit on an SM even with 55 fields.
 // The generic k_xphys tiles two rows per block and transforms them with the runtime block FFT.
 #define XW 4    // warps of k_xfwd2
-#define XPW 8   // warps of k_xphys2
+// warps of k_xphys2: 8 in FP64 (two blocks per SM, held by shared memory and registers); 4 in
+// FP32, whose halved row buffer already lets four blocks share an SM, where 8-warp blocks would
+// be held to two by registers with more idle threads in the pointwise pass
+template <typename C>
+struct XpW {
+    static constexpr int n = sizeof(C) == 16 ? 8 : 4;
+};
 template <int MX, typename C>
-__global__ void __launch_bounds__(XPW * 32) k_xphys2(const C *__restrict__ q, typename kct::Real<C>::T *__restrict__ po,
+__global__ void __launch_bounds__(XpW<C>::n * 32) k_xphys2(const C *__restrict__ q, typename kct::Real<C>::T *__restrict__ po,
                                                     double *__restrict__ drag, double *__restrict__ up3,
                                                     double *__restrict__ vp3, double *__restrict__ wp3,
                                                     const int *__restrict__ imatrix, double *__restrict__ fxi,
@@ -398,6 +404,7 @@ __global__ void __launch_bounds__(XPW * 32) k_xphys2(const C *__restrict__ q, ty
                                                     double *__restrict__ umax, const C *__restrict__ tw,
                                                     PhysArgs A, Save3D sv, int nyp, int mz, int *status) {
     typedef typename kct::Real<C>::T T;
+    constexpr int XPW = XpW<C>::n;
     constexpr int NXH = MX / 3;
     constexpr unsigned ROWB = NXH * sizeof(C);   // one field's row of kx modes
     static_assert(ROWB % 16 == 0 && (MX * sizeof(T)) % 16 == 0, "16-byte bulk copies");
@@ -991,11 +998,12 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         // status of the x stage's bulk copies (KMM_ERR_TIMEOUT), read back with the CFL numbers
         CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
         const size_t eb = f32 ? sizeof(float) : sizeof(double);   // bytes per real of the intermediates
-        const size_t sm_x2 = eb * (size_t)(nin + (nin & 1)) * mx + 2 * eb * XPW * (size_t)mx;
+        const size_t xpw = f32 ? XpW<float2>::n : XpW<double2>::n;
+        const size_t sm_x2 = eb * (size_t)(nin + (nin & 1)) * mx + 2 * eb * xpw * (size_t)mx;
 #define XP2(MM, CC, QQ, PO, TW)                                                                                  \
     do {                                                                                                         \
         RET(kmm_smem_attr(ctx, (const void *)k_xphys2<MM, CC>, sm_x2));                                          \
-        k_xphys2<MM, CC><<<dim3(mz, nyp), XPW * 32, sm_x2, ctx->stream>>>(                                         \
+        k_xphys2<MM, CC><<<dim3(mz, nyp), XpW<CC>::n * 32, sm_x2, ctx->stream>>>(                                         \
             QQ, PO, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl,          \
             ctx->d_umax, TW, A, sv, nyp, mz, ctx->d_status);                                                     \
     } while (0)
