@@ -468,8 +468,12 @@ int kmm_colblk_fwd(kmm_ctx *ctx, const ColFwdArgs &A, const FusedTabs &T, const 
 // ib = 0 over a whole field in the blocked layout: one warp per (kz, -kz) pair, the boundary
 // values from bctop / bcbot, the configuration's tables from the per-context cache.
 // ---------------------------------------------------------------------------
+struct SolveList {
+    double2 *u[KMM_SOLVE_BATCH];
+};
+
 template <int K>
-__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bsolve(double2 *u, const double2 *__restrict__ gtop,
+__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bsolve(SolveList ul, const double2 *__restrict__ gtop,
                                                                   const double2 *__restrict__ gbot, const double *td,
                                                                   const double *te, const double *tb1,
                                                                   const double *tb2, const double *tf,
@@ -479,6 +483,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bsolve(double2 *u, c
                                                                   int nxh, double g, int robin, double c0) {
     constexpr int NYP = 16 * K + 1;
     constexpr unsigned FULL = 0xffffffffu;
+    double2 *u = ul.u[blockIdx.y];
     BPair P;
     if (!bpair<K>(P, nz, nzh, nxh, wavx, wavz)) return;
     TauTab T;
@@ -495,8 +500,8 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bsolve(double2 *u, c
     bstore<K>(u + P.off, s);
 }
 
-int kmm_colblk_solve(kmm_ctx *ctx, double2 *u, double g, int robin, double at, double bt, double ab, double bb,
-                     const double2 *gt, const double2 *gb) {
+int kmm_colblk_solve_many(kmm_ctx *ctx, double2 *const *u, int nf, double g, int robin, double at, double bt,
+                          double ab, double bb, const double2 *gt, const double2 *gb) {
     const int K = colblk_k(ctx);
     if (!K || !ctx->use_colblk) return KMM_ERR_UNSUPPORTED;
     const double *tb[5], *rj = NULL;
@@ -504,22 +509,31 @@ int kmm_colblk_solve(kmm_ctx *ctx, double2 *u, double g, int robin, double at, d
     if (st != KMM_OK) return st;
     const int npairs = ctx->nxh * (ctx->nz / 2);
     const int nblk = (npairs + CB_WARPS - 1) / CB_WARPS;
+    for (int f0 = 0; f0 < nf; f0 += KMM_SOLVE_BATCH) {
+        const int nb = nf - f0 < KMM_SOLVE_BATCH ? nf - f0 : KMM_SOLVE_BATCH;
+        SolveList ul;
+        for (int m = 0; m < nb; ++m) ul.u[m] = u[f0 + m];
+        const dim3 grid(nblk, nb);
 #define BS(KK)                                                                                                      \
-    do {                                                                                                            \
-        k_bsolve<KK><<<nblk, CB_WARPS * 32, 0, ctx->stream>>>(u, gt, gb, tb[0], tb[1], tb[2], tb[3], tb[4], rj,       \
-                                                              ctx->d_wavx, ctx->d_wavz, ctx->nz, ctx->nzh, ctx->nxh, g, \
-                                                              robin, ctx->h_c[0]);                                  \
-        CKL();                                                                                                      \
-        return KMM_OK;                                                                                              \
-    } while (0)
-    switch (K) {
-    case 2: BS(2);
-    case 4: BS(4);
-    case 6: BS(6);
-    case 8: BS(8);
-    default: return KMM_ERR_UNSUPPORTED;
-    }
+    k_bsolve<KK><<<grid, CB_WARPS * 32, 0, ctx->stream>>>(ul, gt, gb, tb[0], tb[1], tb[2], tb[3], tb[4], rj,         \
+                                                          ctx->d_wavx, ctx->d_wavz, ctx->nz, ctx->nzh, ctx->nxh, g, \
+                                                          robin, ctx->h_c[0])
+        switch (K) {
+        case 2: BS(2); break;
+        case 4: BS(4); break;
+        case 6: BS(6); break;
+        case 8: BS(8); break;
+        default: return KMM_ERR_UNSUPPORTED;
+        }
 #undef BS
+        CKL();
+    }
+    return KMM_OK;
+}
+
+int kmm_colblk_solve(kmm_ctx *ctx, double2 *u, double g, int robin, double at, double bt, double ab, double bb,
+                     const double2 *gt, const double2 *gb) {
+    return kmm_colblk_solve_many(ctx, &u, 1, g, robin, at, bt, ab, bb, gt, gb);
 }
 
 int kmm_colblk_bwd(kmm_ctx *ctx, const ColBwdArgs &B, const void *tw, bool fp32) {

@@ -618,6 +618,14 @@ __global__ void __launch_bounds__(TPB) k_penta(double2 *__restrict__ u, const do
     tile_store(u, sm, col0, ncol, nyp);
 }
 
+int kmm_internal_penta_many(kmm_ctx *ctx, double2 *const *u, int nf, double g, double at, double bt, double ab,
+                            double bb, const double2 *gt, const double2 *gb) {
+    const int st = kmm_colblk_solve_many(ctx, u, nf, g, 1, at, bt, ab, bb, gt, gb);
+    if (st != KMM_ERR_UNSUPPORTED) return st;
+    for (int m = 0; m < nf; ++m) RET(kmm_internal_penta(ctx, u[m], g, 0, at, bt, ab, bb, gt, gb));
+    return KMM_OK;
+}
+
 int kmm_internal_penta(kmm_ctx *ctx, double2 *u, double g, int ib, double at, double bt, double ab, double bb,
                        const double2 *gt, const double2 *gb) {
     if (ib == 0) {   // blocked column kernels with cached tables where they are compiled
@@ -859,9 +867,20 @@ extern "C" int kmm_uzero(kmm_ctx *ctx, int uflag) {
     (void)i; (void)j; (void)k;
 
 // phirhs first part, solvers.f90:633-664: wrkc = -re var/(dt th) v - re var/(2 th)(3 fn - fnm1) [+ (1-th) w2 v/th]
-__global__ void k_phirhs_a(double2 *__restrict__ v, const double2 *__restrict__ fn, const double2 *__restrict__ fnm1,
-                           double2 *__restrict__ wrkc, const double *__restrict__ wavx, const double *__restrict__ wavz,
-                           size_t n, int nyp, int nz, double re, double var, double dt, double th) {
+// up to KMM_PHI_BATCH independent fields per launch (blockIdx.y picks the field)
+struct PhiList {
+    double2 *v[KMM_PHI_BATCH];
+    const double2 *fn[KMM_PHI_BATCH];
+    const double2 *fnm1[KMM_PHI_BATCH];
+    double2 *wrkc[KMM_PHI_BATCH];
+};
+
+__global__ void k_phirhs_a(PhiList L, const double *__restrict__ wavx, const double *__restrict__ wavz, size_t n,
+                           int nyp, int nz, double re, double var, double dt, double th) {
+    double2 *__restrict__ v = L.v[blockIdx.y];
+    const double2 *__restrict__ fn = L.fn[blockIdx.y];
+    const double2 *__restrict__ fnm1 = L.fnm1[blockIdx.y];
+    double2 *__restrict__ wrkc = L.wrkc[blockIdx.y];
     const double a = -re * var / (dt * th), b = re * var / (2.0 * th);
     GRID_LOOP(n) {
         DECOMP();
@@ -879,7 +898,9 @@ __global__ void k_phirhs_a(double2 *__restrict__ v, const double2 *__restrict__ 
 }
 
 // phirhs last part, solvers.f90:668-675: v = wrkc - (1-th) v''/th
-__global__ void k_phirhs_b(double2 *__restrict__ v, const double2 *__restrict__ wrkc, size_t n, double th) {
+__global__ void k_phirhs_b(PhiList L, size_t n, double th) {
+    double2 *__restrict__ v = L.v[blockIdx.y];
+    const double2 *__restrict__ wrkc = L.wrkc[blockIdx.y];
     GRID_LOOP(n) {
         double2 w = wrkc[idx], d = v[idx];
         v[idx] = make_double2(w.x - (1.0 - th) * d.x / th, w.y - (1.0 - th) * d.y / th);
@@ -897,21 +918,34 @@ extern "C" int kmm_phirhs(kmm_ctx *ctx, int v, int fn, int fnm1, double var) {
     return kmm_internal_phirhs(ctx, V, F, FM, var);
 }
 
-int kmm_internal_phirhs(kmm_ctx *ctx, double2 *V, const double2 *F, const double2 *FM, double var) {
+int kmm_internal_phirhs_many(kmm_ctx *ctx, double2 *const *V, const double2 *const *F, const double2 *const *FM,
+                             int nf, double var, double2 *const *wrkc, double2 *const *wrk1) {
     double2 *bt = SPEC(ctx, KMM_BCTOP), *bb = SPEC(ctx, KMM_BCBOT);
     if (!bt || !bb) return KMM_ERR_NOMEM;
+    if (nf < 1 || nf > KMM_PHI_BATCH) return KMM_ERR_ARG;
     const size_t nw = (size_t)ctx->nz * ctx->nxh, n = ctx->nspec;
     k_zero_wall<<<kmm_blocks(nw, 256), 256, 0, ctx->stream>>>(bt, bb, nw);
     CKL();
-    double2 *wrkc = ctx->wrk[0], *wrk1 = ctx->wrk[1];
-    k_phirhs_a<<<kmm_blocks(n, 256), 256, 0, ctx->stream>>>(V, F, FM, wrkc, ctx->d_wavx, ctx->d_wavz, n, ctx->nyp,
-                                                            ctx->nz, ctx->re, var, ctx->dt, ctx->theta);
+    PhiList L;
+    for (int m = 0; m < nf; ++m) {
+        L.v[m] = V[m];
+        L.fn[m] = F[m];
+        L.fnm1[m] = FM[m];
+        L.wrkc[m] = wrkc[m];
+    }
+    const dim3 grid(kmm_blocks(n, 256), nf);
+    k_phirhs_a<<<grid, 256, 0, ctx->stream>>>(L, ctx->d_wavx, ctx->d_wavz, n, ctx->nyp, ctx->nz, ctx->re, var, ctx->dt,
+                                              ctx->theta);
     CKL();
-    RET(kmm_internal_cderiv(ctx, V, wrk1));
-    RET(kmm_internal_cderiv(ctx, wrk1, V));
-    k_phirhs_b<<<kmm_blocks(n, 256), 256, 0, ctx->stream>>>(V, wrkc, n, ctx->theta);
+    RET(kmm_internal_cderiv_many(ctx, V, wrk1, nf));
+    RET(kmm_internal_cderiv_many(ctx, wrk1, V, nf));
+    k_phirhs_b<<<grid, 256, 0, ctx->stream>>>(L, n, ctx->theta);
     CKL();
     return KMM_OK;
+}
+
+int kmm_internal_phirhs(kmm_ctx *ctx, double2 *V, const double2 *F, const double2 *FM, double var) {
+    return kmm_internal_phirhs_many(ctx, &V, &F, &FM, 1, var, &ctx->wrk[0], &ctx->wrk[1]);
 }
 
 // main_dns.f90:363-375

@@ -156,6 +156,18 @@ int kmm_internal_solve(kmm_ctx *ctx, double2 *u, double g, int ib, const double2
 // KMM_ERR_UNSUPPORTED where they do not apply (kmm_colblk.cu)
 int kmm_colblk_solve(kmm_ctx *ctx, double2 *u, double g, int robin, double at, double bt, double ab, double bb,
                      const double2 *gt, const double2 *gb);
+// the same over nf distinct fields of one configuration (same g, boundary coefficients and
+// boundary values), KMM_SOLVE_BATCH to a launch
+#define KMM_SOLVE_BATCH 8
+int kmm_colblk_solve_many(kmm_ctx *ctx, double2 *const *u, int nf, double g, int robin, double at, double bt,
+                          double ab, double bb, const double2 *gt, const double2 *gb);
+// penta (ib = 0) of nf distinct fields of one configuration
+int kmm_internal_penta_many(kmm_ctx *ctx, double2 *const *u, int nf, double g, double at, double bt, double ab,
+                            double bb, const double2 *gt, const double2 *gb);
+// phirhs of nf independent fields (at most KMM_PHI_BATCH), each with its own two scratch fields
+#define KMM_PHI_BATCH 8
+int kmm_internal_phirhs_many(kmm_ctx *ctx, double2 *const *V, const double2 *const *F, const double2 *const *FM,
+                             int nf, double var, double2 *const *wrkc, double2 *const *wrk1);
 // the cached tau tables of one configuration and the tau-row reciprocals (kmm_fused.cu)
 int kmm_tau_tabset(kmm_ctx *ctx, double g, int robin, double at, double bt, double ab, double bb, const double **tabs,
                    const double **rj);

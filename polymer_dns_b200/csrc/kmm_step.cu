@@ -332,12 +332,21 @@ extern "C" int kmm_step(kmm_ctx *ctx) {
                 if (!nl[m]) return KMM_ERR_NOMEM;
             }
             RET(kmm_internal_polynl(ctx, nl));
-            double2 *nl2 = poly_scratch(ctx, 6);
-            if (!nl2) return KMM_ERR_NOMEM;
+            // the six components' phirhs in batched launches, each component with its own 2 nl,
+            // wrkc and wrk1 (scratch ids 6 .. 23)
+            double2 *nl2[6], *wc[6], *w1[6], *cm[6];
+            const double2 *nlc[6], *nl2c[6];
             for (int m = 0; m < 6; ++m) {
-                RET(kmm_internal_axpy_spec(ctx, nl2, nl[m], 2.0));
-                RET(kmm_internal_phirhs(ctx, SPEC(ctx, kPolyComp[m]), nl[m], nl2, ctx->p.diffpoly));
+                nl2[m] = poly_scratch(ctx, 6 + m);
+                wc[m] = poly_scratch(ctx, 12 + m);
+                w1[m] = poly_scratch(ctx, 18 + m);
+                cm[m] = SPEC(ctx, kPolyComp[m]);
+                if (!nl2[m] || !wc[m] || !w1[m] || !cm[m]) return KMM_ERR_NOMEM;
+                nlc[m] = nl[m];
+                nl2c[m] = nl2[m];
+                RET(kmm_internal_axpy_spec(ctx, nl2[m], nl[m], 2.0));
             }
+            RET(kmm_internal_phirhs_many(ctx, cm, nlc, nl2c, 6, ctx->p.diffpoly, wc, w1));
             for (int m = 0; m < 6; ++m) {
                 RET(kmm_copy(ctx, KMM_C11NM1 + m, KMM_C11N + m));
                 RET(kmm_copy(ctx, KMM_STR11NM1 + m, KMM_STR11N + m));
@@ -345,7 +354,7 @@ extern "C" int kmm_step(kmm_ctx *ctx) {
             const double g = (re * ctx->p.diffpoly) / (dt * th);
             RET(kmm_zero(ctx, KMM_BCTOP));
             RET(kmm_zero(ctx, KMM_BCBOT));
-            for (int m = 0; m < 6; ++m) RET(kmm_penta(ctx, kPolyComp[m], g, 0, 0.0, 1.0, 0.0, 1.0));
+            RET(kmm_internal_penta_many(ctx, cm, 6, g, 0.0, 1.0, 0.0, 1.0, SPEC(ctx, KMM_BCTOP), SPEC(ctx, KMM_BCBOT)));
             RET(norm_ids(ctx, kPolyComp, 6));
             RET(kmm_copy(ctx, KMM_C21, KMM_C12));
             RET(kmm_copy(ctx, KMM_C31, KMM_C13));
