@@ -1137,6 +1137,25 @@ __global__ void k_dxdz(const double2 *__restrict__ a, double2 *__restrict__ dx, 
     }
 }
 
+// k_dxdz over up to 9 fields (blockIdx.y picks the field)
+struct DxdzList {
+    const double2 *a[9];
+    double2 *dx[9], *dz[9];
+};
+
+__global__ void k_dxdz_many(DxdzList L, const double *__restrict__ wavx, const double *__restrict__ wavz, size_t n,
+                            int nyp, int nz) {
+    const double2 *__restrict__ a = L.a[blockIdx.y];
+    double2 *__restrict__ dx = L.dx[blockIdx.y];
+    double2 *__restrict__ dz = L.dz[blockIdx.y];
+    GRID_LOOP(n) {
+        DECOMP();
+        const double2 v = a[idx];
+        dx[idx] = cimul(v, wavx[k]);
+        dz[idx] = cimul(v, wavz[j]);
+    }
+}
+
 extern "C" int kmm_gradscl(kmm_ctx *ctx) {
     if (!ctx) return KMM_ERR_ARG;
     double2 *s = SPEC(ctx, KMM_SCALAR);
@@ -1159,13 +1178,16 @@ extern "C" int kmm_derivscji(kmm_ctx *ctx) {
         }
         RET(kmm_internal_cderiv_many(ctx, in, out, 9));
     }
+    DxdzList L;
     for (int ij = 0; ij < 9; ++ij) {
-        double2 *cf = SPEC(ctx, KMM_C11 + ij);
-        k_dxdz<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(cf, SPEC(ctx, KMM_DC111 + 3 * ij),
-                                                                     SPEC(ctx, KMM_DC111 + 3 * ij + 2), ctx->d_wavx,
-                                                                     ctx->d_wavz, ctx->nspec, ctx->nyp, ctx->nz);
-        CKL();
+        L.a[ij] = SPEC(ctx, KMM_C11 + ij);
+        L.dx[ij] = SPEC(ctx, KMM_DC111 + 3 * ij);
+        L.dz[ij] = SPEC(ctx, KMM_DC111 + 3 * ij + 2);
+        if (!L.dx[ij] || !L.dz[ij]) return KMM_ERR_NOMEM;
     }
+    k_dxdz_many<<<dim3(kmm_blocks(ctx->nspec, 256), 9), 256, 0, ctx->stream>>>(L, ctx->d_wavx, ctx->d_wavz, ctx->nspec,
+                                                                              ctx->nyp, ctx->nz);
+    CKL();
     return KMM_OK;
 }
 
@@ -1250,8 +1272,18 @@ extern "C" int kmm_filter(kmm_ctx *ctx) {
 }
 
 // polyNL, helpers.f90:610-674 -> scratch NL fields in ctx->wrk? (six fields: use T1..T3 + WRKC/WRK1 is not enough)
-__global__ void k_polynl(double2 *nl, const double2 *cn, const double2 *cnm1, const double2 *sn, const double2 *snm1,
-                         size_t n, double tinv) {
+// the six components in one launch (blockIdx.y picks the component)
+struct PolyNlList {
+    double2 *nl[6];
+    const double2 *cn[6], *cnm1[6], *sn[6], *snm1[6];
+};
+
+__global__ void k_polynl(PolyNlList L, size_t n, double tinv) {
+    double2 *__restrict__ nl = L.nl[blockIdx.y];
+    const double2 *__restrict__ cn = L.cn[blockIdx.y];
+    const double2 *__restrict__ cnm1 = L.cnm1[blockIdx.y];
+    const double2 *__restrict__ sn = L.sn[blockIdx.y];
+    const double2 *__restrict__ snm1 = L.snm1[blockIdx.y];
     GRID_LOOP(n) {
         double2 a = cn[idx], b = sn[idx], c = cnm1[idx], d = snm1[idx];
         nl[idx] = make_double2(3.0 * (a.x - tinv * b.x) - (c.x - tinv * d.x), 3.0 * (a.y - tinv * b.y) - (c.y - tinv * d.y));
@@ -1322,12 +1354,17 @@ int kmm_internal_axpy_spec(kmm_ctx *ctx, double2 *y, const double2 *x, double a)
 // polyNL into six caller-provided buffers
 int kmm_internal_polynl(kmm_ctx *ctx, double2 *const *nl) {
     const double tinv = 1.0 / ctx->p.tpoly;
+    PolyNlList L;
     for (int m = 0; m < 6; ++m) {
-        k_polynl<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(nl[m], SPEC(ctx, KMM_C11N + m),
-                                                                       SPEC(ctx, KMM_C11NM1 + m), SPEC(ctx, KMM_STR11N + m),
-                                                                       SPEC(ctx, KMM_STR11NM1 + m), ctx->nspec, tinv);
-        CKL();
+        L.nl[m] = nl[m];
+        L.cn[m] = SPEC(ctx, KMM_C11N + m);
+        L.cnm1[m] = SPEC(ctx, KMM_C11NM1 + m);
+        L.sn[m] = SPEC(ctx, KMM_STR11N + m);
+        L.snm1[m] = SPEC(ctx, KMM_STR11NM1 + m);
+        if (!L.cn[m] || !L.cnm1[m] || !L.sn[m] || !L.snm1[m]) return KMM_ERR_NOMEM;
     }
+    k_polynl<<<dim3(kmm_blocks(ctx->nspec, 256), 6), 256, 0, ctx->stream>>>(L, ctx->nspec, tinv);
+    CKL();
     return KMM_OK;
 }
 
