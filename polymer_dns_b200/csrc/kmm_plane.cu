@@ -132,6 +132,118 @@ __global__ void __launch_bounds__(256) k_dct_fwd(FieldPtrs in, C *__restrict__ p
     }
 }
 
+// DCT-I of one column by an N-point FFT (N = ny, a compiled length), on one warp:
+//   X_k = x_0 + (-1)^k x_N + 2 sum_{n=1}^{N-1} x_n cos(pi n k / N),  k = 0 .. N,
+// the DFT of the even extension of length 2N that k_dct_fwd / k_dct_bwd transform otherwise.
+// With y_j = (x_j + x_{N-j}) / 2 + sin(pi j / N) (x_j - x_{N-j}) (j < N) and Y = FFT_N(y):
+//   X_{2m} = Y_m + Y_{N-m} (Y_N = Y_0),  X_{2m+1} = X_{2m-1} - i (Y_m - Y_{N-m}),
+//   X_1 = x_0 - x_N + 2 sum_{n=1}^{N-1} x_n cos(pi n / N)
+// (the half-length form of the DCT-I; the real and imaginary parts of the column are two real
+// sequences, carried together).  x: the column's N + 1 values in shared memory, overwritten by X;
+// a, b: the warp's FFT buffers (N elements, swizzled); tw: the 2N-point twiddles exp(-i pi m / N).
+template <typename C, int N>
+__device__ __forceinline__ void dct1_half(C *x, C *a, C *b, const C *__restrict__ tw) {
+    typedef typename kct::Real<C>::T T;
+    constexpr int H = N / 2, Q = (H + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    C seed = kct::mk<C>((T)0, (T)0);
+    for (int j = lane; j < N; j += 32) {
+        const C xj = x[j], xr = x[N - j];
+        const C w = tw[j];   // (cos, -sin) of pi j / N
+        const C sm = kct::add(xj, xr), df = kct::sub(xj, xr);
+        const T sn = -w.y;
+        a[swz<C>(j)] = kct::mk<C>((T)0.5 * sm.x + sn * df.x, (T)0.5 * sm.y + sn * df.y);
+        seed = j == 0 ? kct::add(seed, df) : kct::add(seed, kct::scl(xj, (T)2 * w.x));
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1)
+        seed = kct::add(seed, kct::mk<C>(__shfl_xor_sync(0xffffffffu, seed.x, o), __shfl_xor_sync(0xffffffffu, seed.y, o)));
+    __syncwarp();
+    const C *Y = fft_warp_ct<C, N, -1, 1, true, 2>(a, b, tw);
+    // odd outputs: X_{2m+1} = seed + sum_{t=1}^{m} d_t, d_t = -i (Y_t - Y_{N-t}); lane holds m = lane Q .. lane Q + Q - 1
+    C d[Q];
+    C tot = kct::mk<C>((T)0, (T)0);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int m = lane * Q + q;
+        C v = kct::mk<C>((T)0, (T)0);
+        if (m >= 1 && m < H) {
+            const C df = kct::sub(Y[swz<C>(m)], Y[swz<C>(N - m)]);
+            v = kct::mk<C>(df.y, -df.x);
+        }
+        tot = kct::add(tot, v);
+        d[q] = tot;   // inclusive prefix within the lane
+    }
+    C excl = tot;   // inclusive scan of the lane totals, then shifted to exclusive
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const C u = kct::mk<C>(__shfl_up_sync(0xffffffffu, excl.x, o), __shfl_up_sync(0xffffffffu, excl.y, o));
+        if (lane >= o) excl = kct::add(excl, u);
+    }
+    excl = kct::sub(excl, tot);
+    // even outputs (all lanes read Y before anyone writes x)
+    C ev[(H + 1 + 31) / 32];
+#pragma unroll
+    for (int e = 0; e < (H + 1 + 31) / 32; ++e) {
+        const int m = lane + 32 * e;
+        if (m <= H) ev[e] = kct::add(Y[swz<C>(m)], Y[swz<C>(m == 0 ? 0 : N - m)]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < (H + 1 + 31) / 32; ++e) {
+        const int m = lane + 32 * e;
+        if (m <= H) x[2 * m] = ev[e];
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int m = lane * Q + q;
+        if (m < H) x[2 * m + 1] = kct::add(seed, kct::add(excl, d[q]));
+    }
+    __syncwarp();
+}
+
+// k_dct_fwd for ny in {48, 64, 96, 128} with the half-length DCT-I: a warp per column, the
+// block's 8 columns staged in shared memory (column stride N + 1, odd: the transposing store
+// reads 8 columns at one y without bank conflicts)
+template <typename C, int N>
+__global__ void __launch_bounds__(256) k_dct_fwd_h(FieldPtrs in, C *__restrict__ pl, const C *__restrict__ tw, int nz,
+                                                   int nxh, int ncols) {
+    typedef typename kct::Real<C>::T T;
+    constexpr int NYP = N + 1;
+    extern __shared__ double2 smd[];
+    C *xs = reinterpret_cast<C *>(smd);
+    C *a = xs + DCT_CB * NYP, *b = a + fb_len(DCT_CB, N);
+    const int f = blockIdx.y;
+    const int col0 = blockIdx.x * DCT_CB;
+    const int ncb = min(DCT_CB, ncols - col0);
+    const double2 *src = in.p[f] + (size_t)col0 * NYP;
+    for (int e0 = threadIdx.x; e0 < ncb * NYP; e0 += LDG * 256) {
+        double2 wv[LDG];
+#pragma unroll
+        for (int u = 0; u < LDG; ++u)
+            if (e0 + 256 * u < ncb * NYP) wv[u] = src[e0 + 256 * u];
+#pragma unroll
+        for (int u = 0; u < LDG; ++u) {
+            const int e = e0 + 256 * u;
+            if (e >= ncb * NYP) break;
+            const int i = e % NYP;
+            const double fac = (i == 0 || i == N) ? 1.0 : 0.5;   // c(i)/2.0
+            xs[e] = kct::mk<C>((T)(wv[u].x * fac), (T)(wv[u].y * fac));
+        }
+    }
+    __syncthreads();
+    const int c = threadIdx.x >> 5;
+    if (c < ncb) dct1_half<C, N>(xs + c * NYP, a + c * (N + FB_PAD), b + c * (N + FB_PAD), tw);
+    __syncthreads();
+    // PL[f][y][kx][kz]: col = kx*nz + kz
+    for (int e = threadIdx.x; e < ncb * NYP; e += blockDim.x) {
+        const int y = e / ncb, cc = e - y * ncb;
+        const int col = col0 + cc;
+        const int kx = col / nz, kz = col - kx * nz;
+        pl[(((size_t)f * NYP + y) * nxh + kx) * nz + kz] = xs[cc * NYP + y];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // 2. z: zero-pad + inverse c2c (FFTW_BACKWARD)
 // ---------------------------------------------------------------------------
@@ -716,6 +828,97 @@ __global__ void __launch_bounds__(256) k_dct_bwd(const C *__restrict__ pl, Field
     }
 }
 
+// k_dct_bwd for ny in {48, 64, 96, 128} with the half-length DCT-I (layout as k_dct_fwd_h)
+template <typename C, int N>
+__global__ void __launch_bounds__(256) k_dct_bwd_h(const C *__restrict__ pl, FieldPtrsW out, const C *__restrict__ tw,
+                                                   int nz, int nxh, int ncols) {
+    constexpr int NYP = N + 1;
+    extern __shared__ double2 smd[];
+    C *xs = reinterpret_cast<C *>(smd);
+    C *a = xs + DCT_CB * NYP, *b = a + fb_len(DCT_CB, N);
+    const int f = blockIdx.y;
+    const int col0 = blockIdx.x * DCT_CB;
+    const int ncb = min(DCT_CB, ncols - col0);
+    for (int e0 = threadIdx.x; e0 < ncb * NYP; e0 += LDG * 256) {
+        C wv[LDG];
+#pragma unroll
+        for (int u = 0; u < LDG; ++u) {
+            const int e = e0 + 256 * u;
+            if (e < ncb * NYP) {
+                const int y = e / ncb, cc = e - y * ncb;
+                const int col = col0 + cc;
+                const int kx = col / nz, kz = col - kx * nz;
+                wv[u] = pl[(((size_t)f * NYP + y) * nxh + kx) * nz + kz];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < LDG; ++u) {
+            const int e = e0 + 256 * u;
+            if (e >= ncb * NYP) break;
+            const int y = e / ncb, cc = e - y * ncb;
+            xs[cc * NYP + y] = wv[u];
+        }
+    }
+    __syncthreads();
+    const int c = threadIdx.x >> 5;
+    if (c < ncb) dct1_half<C, N>(xs + c * NYP, a + c * (N + FB_PAD), b + c * (N + FB_PAD), tw);
+    __syncthreads();
+    double2 *dst = out.p[f] + (size_t)col0 * NYP;
+    for (int e = threadIdx.x; e < ncb * NYP; e += blockDim.x) {
+        const C rv = xs[e];
+        const int i = e % NYP;
+        double2 v = make_double2((double)rv.x / (double)N, (double)rv.y / (double)N);
+        if (i == 0 || i == N) v = make_double2(v.x / 2.0, v.y / 2.0);
+        dst[e] = v;
+    }
+}
+
+// launch the half-length DCT-I kernels where ny is one of their lengths: KMM_ERR_UNSUPPORTED
+// otherwise (the caller then runs k_dct_fwd / k_dct_bwd)
+template <typename C>
+static int dct_h_fwd(kmm_ctx *ctx, int nf, const FieldPtrs &in, C *pl, const C *tw, int nz, int nxh, int ncols) {
+    const int ny = ctx->nyp - 1;
+    const size_t sm = sizeof(C) * ((size_t)DCT_CB * (ny + 1) + 2 * (size_t)fb_len(DCT_CB, ny));
+    const dim3 grid((ncols + DCT_CB - 1) / DCT_CB, nf);
+#define DH(NN)                                                                                            \
+    do {                                                                                                  \
+        RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd_h<C, NN>, sm));                                    \
+        k_dct_fwd_h<C, NN><<<grid, 256, sm, ctx->stream>>>(in, pl, tw, nz, nxh, ncols);                     \
+        CKL();                                                                                            \
+        return KMM_OK;                                                                                    \
+    } while (0)
+    switch (ny) {
+    case 48: DH(48);
+    case 64: DH(64);
+    case 96: DH(96);
+    case 128: DH(128);
+    default: return KMM_ERR_UNSUPPORTED;
+    }
+#undef DH
+}
+
+template <typename C>
+static int dct_h_bwd(kmm_ctx *ctx, int nf, const C *pl, const FieldPtrsW &out, const C *tw, int nz, int nxh, int ncols) {
+    const int ny = ctx->nyp - 1;
+    const size_t sm = sizeof(C) * ((size_t)DCT_CB * (ny + 1) + 2 * (size_t)fb_len(DCT_CB, ny));
+    const dim3 grid((ncols + DCT_CB - 1) / DCT_CB, nf);
+#define DH(NN)                                                                                            \
+    do {                                                                                                  \
+        RET(kmm_smem_attr(ctx, (const void *)k_dct_bwd_h<C, NN>, sm));                                    \
+        k_dct_bwd_h<C, NN><<<grid, 256, sm, ctx->stream>>>(pl, out, tw, nz, nxh, ncols);                    \
+        CKL();                                                                                            \
+        return KMM_OK;                                                                                    \
+    } while (0)
+    switch (ny) {
+    case 48: DH(48);
+    case 64: DH(64);
+    case 96: DH(96);
+    case 128: DH(128);
+    default: return KMM_ERR_UNSUPPORTED;
+    }
+#undef DH
+}
+
 // ---------------------------------------------------------------------------
 // physical scratch (outputs, drag) sized on demand
 // ---------------------------------------------------------------------------
@@ -964,13 +1167,21 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     float2 *pl_out32 = (float2 *)ctx->pl_out, *q_out32 = (float2 *)ctx->q_out;
     float *po32 = (float *)ctx->po;
     kmm_tic(ctx);
-    if (f32)
-        k_dct_fwd<float2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nin), 256, sm_dct, ctx->stream>>>(
-            in, pl_in32, ctx->py2, tw_y2, nyp, nz, nxh, ncols);
-    else
-        k_dct_fwd<double2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nin), 256, sm_dct, ctx->stream>>>(
-            in, ctx->pl_in, ctx->py2, ctx->py2.tw, nyp, nz, nxh, ncols);
-    CKL();
+    {
+        const int dst = f32 ? dct_h_fwd<float2>(ctx, nin, in, pl_in32, tw_y2, nz, nxh, ncols)
+                            : dct_h_fwd<double2>(ctx, nin, in, ctx->pl_in, ctx->py2.tw, nz, nxh, ncols);
+        if (dst != KMM_ERR_UNSUPPORTED) {
+            RET(dst);
+        } else {
+            if (f32)
+                k_dct_fwd<float2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nin), 256, sm_dct, ctx->stream>>>(
+                    in, pl_in32, ctx->py2, tw_y2, nyp, nz, nxh, ncols);
+            else
+                k_dct_fwd<double2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nin), 256, sm_dct, ctx->stream>>>(
+                    in, ctx->pl_in, ctx->py2, ctx->py2.tw, nyp, nz, nxh, ncols);
+            CKL();
+        }
+    }
     kmm_toc(ctx, KMM_STAGE_DCT_FWD);
     kmm_tic(ctx);
     if (f32)
@@ -1079,13 +1290,21 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_FWD);
     kmm_tic(ctx);
-    if (f32)
-        k_dct_bwd<float2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nout), 256, sm_dct, ctx->stream>>>(
-            pl_out32, outp, ctx->py2, tw_y2, nyp, nz, nxh, ncols);
-    else
-        k_dct_bwd<double2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nout), 256, sm_dct, ctx->stream>>>(
-            ctx->pl_out, outp, ctx->py2, ctx->py2.tw, nyp, nz, nxh, ncols);
-    CKL();
+    {
+        const int dst = f32 ? dct_h_bwd<float2>(ctx, nout, pl_out32, outp, tw_y2, nz, nxh, ncols)
+                            : dct_h_bwd<double2>(ctx, nout, ctx->pl_out, outp, ctx->py2.tw, nz, nxh, ncols);
+        if (dst != KMM_ERR_UNSUPPORTED) {
+            RET(dst);
+        } else {
+            if (f32)
+                k_dct_bwd<float2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nout), 256, sm_dct, ctx->stream>>>(
+                    pl_out32, outp, ctx->py2, tw_y2, nyp, nz, nxh, ncols);
+            else
+                k_dct_bwd<double2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nout), 256, sm_dct, ctx->stream>>>(
+                    ctx->pl_out, outp, ctx->py2, ctx->py2.tw, nyp, nz, nxh, ncols);
+            CKL();
+        }
+    }
     kmm_toc(ctx, KMM_STAGE_DCT_BWD);
 
     // tracers (solvers.f90:3463-3476)

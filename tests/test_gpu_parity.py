@@ -190,8 +190,11 @@ def test_vcw3dp_fluid(rt, oracle_mod, grid):
     assert abs(g.stats().cflmax - o.stats().cflmax) <= 1e-12 * o.stats().cflmax
 
 
-def test_vcw3dp_scalar_polymer_ib(rt, oracle_mod):
-    p = kc.cfg_small(16, 24, 16, dt=1e-5, scalar_on=1, polymer_on=1, scalar_q=0.3, zlmax=30.0, tpoly=20.0,
+@pytest.mark.parametrize("grid", [(16, 24, 16), (32, 48, 32), (16, 64, 16)])
+def test_vcw3dp_scalar_polymer_ib(rt, oracle_mod, grid):
+    """All 55 input fields through vcw3dp; ny = 48 and 64 take the half-length DCT-I kernels, ny = 24
+    the 2 ny-point FFT form."""
+    p = kc.cfg_small(*grid, dt=1e-5, scalar_on=1, polymer_on=1, scalar_q=0.3, zlmax=30.0, tpoly=20.0,
                      qbeta=0.9, gain=-400.0, ugain=-40.0)
     g, o = _pair(rt, oracle_mod, p)
     rng = np.random.default_rng(16)
