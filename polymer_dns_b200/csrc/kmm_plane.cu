@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(256) k_dct_fwd_h(FieldPtrs in, C *__restrict__
 // ---------------------------------------------------------------------------
 // 2. z: zero-pad + inverse c2c (FFTW_BACKWARD)
 // ---------------------------------------------------------------------------
-#define ZKB 16
+#define ZKB 8   // kx columns per block of the z transforms (one sequence per warp)
 template <typename C>
 __global__ void __launch_bounds__(256) k_zfft_bwd(const C *__restrict__ pl, C *__restrict__ q, DevPlan P,
                                                   const C *__restrict__ tw, int nyp, int nz, int nxh, int mz) {
