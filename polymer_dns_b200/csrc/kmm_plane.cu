@@ -247,9 +247,9 @@ __global__ void __launch_bounds__(256) k_dct_fwd_h(FieldPtrs in, C *__restrict__
 // ---------------------------------------------------------------------------
 // 2. z: zero-pad + inverse c2c (FFTW_BACKWARD)
 // ---------------------------------------------------------------------------
-#define ZKB 8   // kx columns per block of the z transforms (one sequence per warp)
+#define ZKB 8   // kx columns per block of the z transforms (one sequence per warp; 4 blocks per SM)
 template <typename C>
-__global__ void __launch_bounds__(256) k_zfft_bwd(const C *__restrict__ pl, C *__restrict__ q, DevPlan P,
+__global__ void __launch_bounds__(256, 4) k_zfft_bwd(const C *__restrict__ pl, C *__restrict__ q, DevPlan P,
                                                   const C *__restrict__ tw, int nyp, int nz, int nxh, int mz) {
     typedef typename kct::Real<C>::T T;
     extern __shared__ double2 smd[];
@@ -738,7 +738,7 @@ __global__ void __launch_bounds__(256) k_xfwd(const double *__restrict__ po, dou
 // 6. z: forward c2c, truncate to nz, /(mx*mz)
 // ---------------------------------------------------------------------------
 template <typename C>
-__global__ void __launch_bounds__(256) k_zfft_fwd(const C *__restrict__ q, C *__restrict__ pl, DevPlan P,
+__global__ void __launch_bounds__(256, 4) k_zfft_fwd(const C *__restrict__ q, C *__restrict__ pl, DevPlan P,
                                                   const C *__restrict__ tw, int nyp, int nz, int nxh, int mz,
                                                   double scale) {
     typedef typename kct::Real<C>::T T;
