@@ -49,105 +49,118 @@ GRID_OVERRIDE = None
 
 
 def make_config(name, precision=0):
-    from polymer_dns_b200 import abi
-    if name == "cfg1":
-        re = 1400.0
-        p = abi.default_params(nx=32, ny=32, nz=32, dt=0.01, re=re, r_tau=math.sqrt(3 * re), xl=4 * math.pi,
-                               zl=2 * math.pi, precision=precision)
-        init = dict(profile="laminar", amp=0.05, kmax=4, seed=0)
-        desc = "cfg1 32x33x32 laminar+perturbation, 100-step case"
-    elif name in ("cfg2", "cfg3"):
-        re, r_tau = 2800.0, 180.0
-        kw = dict(nx=128, ny=128, nz=128, dt=0.005, re=re, r_tau=r_tau, xl=4 * math.pi, zl=4 * math.pi / 3,
-                  scalar_on=1, diff=1.0, scalar_bc=1, scalar_q=1.0, npart=100000, ap=1e-3, tracer_scheme=1,
-                  precision=precision)
-        desc = "Re_tau=180 channel 128x129x128, scalar (Sc=1, uniform source, Dirichlet walls), 100k RK3 tracers"
-        if name == "cfg3":
-            kw.update(polymer_on=1, zlmax=30.0, tpoly=20.0, qbeta=0.9, diffpoly=1000.0, gain=-400.0, ugain=-40.0)
-            desc += ", FENE-P (Wi=20, beta=0.9, L^2=900), IB cylinder r=0.25 at (pi,0)"
-        if GRID_OVERRIDE:
-            n = GRID_OVERRIDE
-            kw.update(nx=n, ny=n, nz=n)
-            desc = desc.replace("128x129x128", "%dx%dx%d" % (n, n + 1, n))
-        p = abi.default_params(**kw)
-        init = dict(profile="loglaw", amp=0.1, kmax=8, seed=1)
-    else:
-        raise SystemExit("unknown config %s" % name)
-    return p, init, desc
+    from polymer_dns_b200 import configs
+    return configs.make(name, precision, grid=GRID_OVERRIDE if name in ("cfg2", "cfg3") else None)
 
 
 def build_inputs(p, init, name):
-    from polymer_dns_b200 import inputs
-    f = inputs.channel_initial(p.nx, p.ny, p.nz, p.xl, p.yl, p.zl, p.re, p.r_tau, init["profile"], init["amp"],
-                               init["kmax"], init["seed"])
-    extra = {}
-    if p.scalar_on:
-        extra["INITSCL"] = np.zeros_like(f[0])
-    if p.npart > 0:
-        x, y, z = inputs.uniform_particles(p.npart, p.xl, p.yl, p.zl, p.ap, 2)
-        extra.update(XPART=x, YPART=y, ZPART=z)
-    if name == "cfg3":
-        extra["IMATRIX"] = inputs.cylinder_imatrix(p.nx, p.ny, p.nz, p.xl, p.yl, math.pi, 0.0, 0.25)
-    return f, extra
+    from polymer_dns_b200 import configs
+    return configs.build_inputs(p, init, name)
 
 
 def load(ctx, f, extra, setter):
-    setter("INITU", f[0])
-    setter("INITV", f[1])
-    setter("INITW", f[2])
-    for k, v in extra.items():
-        setter(k, v)
+    from polymer_dns_b200 import configs
+    configs.load(f, extra, setter)
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+    """SM clock and clock-event (throttle) reasons sampled every ~2 ms through NVML while the timed
+    region runs (read-only queries; nothing is set).  Falls back to nvidia-smi at 100 ms when NVML
+    is unavailable."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
-    def __init__(self, gpu):
+    def __init__(self, gpu, period_s=0.002):
         self.gpu = gpu
-        self.rows = []
+        self.period = period_s
+        self.rows = []          # (sm_mhz, max_mhz, set of reason names)
+        self.stop = threading.Event()
+        self.t = None
         self.proc = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = None
+            try:   # the CUDA ordinal's NVML handle through its PCI address (CUDA_VISIBLE_DEVICES renumbers)
+                import torch
+                pr = torch.cuda.get_device_properties(self.gpu)
+                bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+                self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+            except Exception:
+                self.h = None
+            if self.h is None:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.maxmhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.t = threading.Thread(target=self._poll_nvml, daemon=True)
             self.t.start()
         except Exception:
-            self.proc = None
+            self.nv = None
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=clocks.sm,clocks.max.sm,"
+                                              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                                              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                                              "--format=csv,noheader,nounits", "-lms", "100"],
+                                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.t = threading.Thread(target=self._read_smi, daemon=True)
+                self.t.start()
+            except Exception:
+                self.proc = None
         return self
 
-    def _read(self):
+    def _poll_nvml(self):
+        nv = self.nv
+        while not self.stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                rs = {n for n, attr in self.REASONS if bits & getattr(nv, attr)}
+                self.rows.append((float(mhz), float(self.maxmhz), rs))
+            except Exception:
+                return
+            time.sleep(self.period)
+
+    def _read_smi(self):
+        names = [n for n, _ in self.REASONS]
         for line in self.proc.stdout:
-            self.rows.append([c.strip() for c in line.split(",")])
+            c = [x.strip() for x in line.split(",")]
+            try:
+                self.rows.append((float(c[0]), float(c[1]), {n for n, v in zip(names, c[2:]) if v.lower() == "active"}))
+            except Exception:
+                pass
 
     def __exit__(self, *a):
+        self.stop.set()
         if self.proc:
-            time.sleep(0.25)
+            time.sleep(0.15)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        if self.nv:
+            try:
+                self.nv.nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self):
         if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [r[0] for r in self.rows]
         reasons = set()
         for r in self.rows:
-            for i, n in enumerate(names):
-                if len(r) > 5 + i and r[5 + i].lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+            reasons |= r[2]
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(r[1] for r in self.rows),
+                "sm_mhz_min": min(sm), "reasons": sorted(reasons), "samples": len(self.rows),
+                "source": "nvml" if self.nv else "nvidia-smi"}
 
 
 # per-stage algorithmic bytes per launch (each operand read or written once)
@@ -341,7 +354,8 @@ def run_kmm(a, rank, world, local_rank):
             "e2e": {"value": round(e2e_value, 3), "unit": "timesteps/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "steps": e2e_steps},
             "gpu_launches": int(launches),
-            "clocks": clk.summary(),
+            "clocks": dict(clk.summary(), **({"ms_per_step_x_median_mhz": round(ms_per_step * clk.summary()["sm_mhz"], 2)}
+                                             if clk.summary().get("sm_mhz") else {})),
         }
         if p.precision == 0 and not a.no_mixed and a.config in ("cfg1", "cfg2"):
             result["mixed"] = mixed_report(a, f, extra, local_rank, ms_per_step)
@@ -350,7 +364,7 @@ def run_kmm(a, rank, world, local_rank):
         if a.config == "cfg2" and not a.no_polymer and world == 1:
             result["polymer"] = polymer_report(a, local_rank)
         if not a.no_cpu_baseline and world == 1:
-            result["cpu_baseline"] = cpu_baseline(a.config, a.cpu_steps)
+            result["cpu_baseline"] = cpu_baseline(a.config, a.cpu_steps, one_thread_steps=2)
     ctx.close()
     if dist is not None:
         dist.barrier()
@@ -465,7 +479,7 @@ def polymer_report(a, local_rank):
         errs[str(mark)] = e
     for c in ctx.values():
         c.close()
-    cpu = cpu_baseline("cfg3", 1) if not a.no_cpu_baseline else None
+    cpu = cpu_baseline("cfg3", a.cpu_steps, one_thread_steps=1) if not a.no_cpu_baseline else None
     return {"workload": desc, "fp64": {"value": round(1e3 / ms[0], 3), "unit": "timesteps/s",
                                        "ms_per_step": round(ms[0], 4)},
             "mixed": {"value": round(1e3 / ms[1], 3), "unit": "timesteps/s", "ms_per_step": round(ms[1], 4),
@@ -536,22 +550,53 @@ def ensemble_report(a, local_rank):
     return res
 
 
-def cpu_baseline(config, nsteps):
-    """The oracle (C restatement of the reference, OpenMP) on the host cores: a bounded sample."""
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def cpu_baseline(config, nsteps, one_thread_steps=1, skip=10):
+    """The oracle (C restatement of the reference, OpenMP over y-planes / kx slabs) on the host cores,
+    timed like the reference's cadence timer (main_dns.f90:797-809): steps 1..skip run untimed
+    (setup, first-touch, the start-up transient), then steps skip+1 .. skip+nsteps are timed with all
+    host cores, then `one_thread_steps` further steps with one thread."""
     from oracle import pyoracle
     p, init, desc = make_config(config)
     f, extra = build_inputs(p, init, config)
+    cores = pyoracle.set_threads(0)
     o = pyoracle.Oracle(p)
     load(o, f, extra, o.set)
     o.initial()
+    for _ in range(skip):
+        o.step()
     t0 = time.perf_counter()
     for _ in range(nsteps):
         o.step()
     dt = time.perf_counter() - t0
+    one = None
+    if one_thread_steps > 0:
+        pyoracle.set_threads(1)
+        t1 = time.perf_counter()
+        for _ in range(one_thread_steps):
+            o.step()
+        d1 = time.perf_counter() - t1
+        pyoracle.set_threads(0)
+        one = {"value": round(one_thread_steps / d1, 5), "unit": "timesteps/s", "cores": 1,
+               "sample": "step%s %s (%.1f s)" % ("s" if one_thread_steps > 1 else "",
+                                                 "%d..%d" % (skip + nsteps + 1, skip + nsteps + one_thread_steps)
+                                                 if one_thread_steps > 1 else str(skip + nsteps + 1), d1)}
     o.close()
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return {"value": round(nsteps / dt, 5), "unit": "timesteps/s", "cores": cores, "kind": "port",
-            "sample": "%d steps of the same workload after initial (%.1f s)" % (nsteps, dt)}
+            "cpu_model": cpu_model(), "nproc": os.cpu_count(),
+            "sample": "steps %d..%d of the same workload after %d untimed steps (%.1f s)" % (
+                skip + 1, skip + nsteps, skip, dt),
+            "one_thread": one}
 
 
 def run_reference(a, rank, world):
@@ -559,9 +604,9 @@ def run_reference(a, rank, world):
         return None
     p, init, desc = make_config(a.config)
     steps = max(1, min(a.steps, a.cpu_steps))
-    cb = cpu_baseline(a.config, steps)
+    cb = cpu_baseline(a.config, steps, one_thread_steps=0)
     return {"metric": METRIC, "value": cb["value"], "unit": "timesteps/s", "n_gpus": world, "steps": steps,
-            "warmup": 0, "ms_per_step": round(1e3 / cb["value"], 3), "higher_is_better": True, "scaling": "weak",
+            "warmup": 10, "ms_per_step": round(1e3 / cb["value"], 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": {"workload": desc, "grid": [p.nx, p.ny + 1, p.nz], "npart": p.npart},
             "cpu_baseline": cb,
@@ -576,7 +621,7 @@ def main():
     ap.add_argument("--impl", default="kmm", choices=["kmm", "reference"])
     ap.add_argument("--config", default="cfg2", choices=["cfg1", "cfg2", "cfg3"])
     ap.add_argument("--precision", type=int, default=0)
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=5, help="timed oracle steps after the 10 untimed ones")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision speed / error report")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 16-member ensemble measurement")

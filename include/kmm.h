@@ -86,6 +86,15 @@ typedef struct kmm_params {
     double scalar_q;       /* uniform volumetric scalar source added to -u.grad(c); 0: none           */
     int    tracer_scheme;  /* 0: explicit Euler (part_track.f90:416-421); 1: Williamson RK3           */
     int    precision;      /* 0: FP64 drop-in; 1: mixed (FP32 transforms / products, FP64 solves)     */
+    int    ib_spread_all;  /* 0: immersed-boundary drag is spread only in the y-planes i <= kmaxsurf, the
+                              reference's test (solvers.f90:3069; kmaxsurf is the largest solid x index,
+                              main_dns.f90:1526-1535); 1: in every y-plane, so each solid cell's drag is
+                              spread in its own plane (geometries whose solid y-planes lie above kmaxsurf,
+                              such as a cylinder in mid-channel, otherwise receive no force)             */
+    double flow_rate;      /* 0: constant mean pressure gradient dPdx (init_flow.f90:117); > 0: constant
+                              flow rate -- after each mean-mode solve a uniform pressure-gradient
+                              correction holds the trapezoid bulk velocity of helpers.f90:1355-1359 at
+                              this value (the correction of the last step is kmm_stats.dpdx - dPdx)     */
 } kmm_params;
 
 /* ---- field ids -------------------------------------------------------------
@@ -151,6 +160,8 @@ typedef struct kmm_stats {
     int    status;       /* last nonzero status raised on the device (0 if none)                     */
     double pumax;        /* inertial particles: running max |u_fluid - u_particle| (umax1, part_track.f90:736-742) */
     double pcfl;         /* inertial particles: umax1 dt / ap of the last update (part_track.f90:215-216) */
+    double dpdx;         /* mean pressure gradient that drove the last step: dPdx, plus the flow-rate
+                            correction when kmm_params.flow_rate > 0                                    */
 } kmm_stats;
 
 typedef struct kmm_ctx kmm_ctx;
@@ -251,6 +262,12 @@ int  kmm_run(kmm_ctx *ctx, int n);
 int  kmm_tracer_update(kmm_ctx *ctx);
 /* init_part's velocity interpolation, part_track.f90:229-292 */
 int  kmm_init_part(kmm_ctx *ctx);
+/* The interpolation cell of every particle at its current position, as fluid_interp looks it up
+ * (part_track.f90:560-577): cells[p] = imin (x, 1..mx), cells[npart + p] = jmin (z, 1..mz),
+ * cells[2 npart + p] = kmax (y, the upper Chebyshev node; kmin = kmax + 1), 1-based.  `n` is
+ * the number of ints in `cells` (>= 3 npart).  Returns KMM_ERR_INTERP if any particle's index is
+ * out of range (the reference stops there); its entries are then 0.                           */
+int  kmm_tracer_cells(kmm_ctx *ctx, int *cells, size_t n);
 /* calcswirl (helpers.f90:197-404, solvers.f90:3421 and 3480): swirl strength from the spectral
  * velocity gradients U11..U33 (kmm_gradv; after kmm_step run kmm_veloc first, the fused step
  * keeps only the prognostic fields) into SWIRL3D, and at each particle into SWIRLPART.  The
@@ -288,11 +305,23 @@ enum kmm_option {
                            captured into two CUDA graphs (the history buffers alternate between
                            two arrangements) and replayed; 0: launched kernel by kernel.  Steps
                            with stage timing on (kmm_set_timing) always run kernel by kernel. */
-    KMM_OPT_ZTMA = 4           /* 1 (default): the fused step's z transforms (FP64 and mixed) move their
+    KMM_OPT_ZTMA = 4,          /* 1 (default): the fused step's z transforms (FP64 and mixed) move their
                            tiles with TMA (tensor-map bulk copies, mz = 48, 96, 144, 192); 0:
                            plain loads and stores                                            */
+    KMM_OPT_WAIT_LIMIT_MS = 5  /* limit of every device-side wait on an mbarrier (bulk / TMA copies), in
+                           milliseconds, 100 .. 60000 (default 2000).  A wait that runs out records
+                           KMM_ERR_TIMEOUT in the step status.  The limit is per device and
+                           process-wide (every context on the device shares it).            */
 };
 int  kmm_set_option(kmm_ctx *ctx, int option, int value);
+
+/* ---- bounded-wait check (no counterpart in the reference) ---------------------------
+ * Runs the library's bounded mbarrier wait, with a limit of `limit_ms` (0 < limit_ms <= 10000),
+ * on a barrier that nothing arrives on and no copy targets, so the wait must run out; the kernel
+ * then records KMM_ERR_TIMEOUT and returns, as the step kernels do.  Returns KMM_ERR_TIMEOUT when
+ * the wait gave up (the expected outcome), KMM_OK if it did not, another status on a CUDA error.
+ * The context stays usable afterwards.                                                    */
+int  kmm_wait_selftest(kmm_ctx *ctx, double limit_ms);
 
 /* ---- transform without device allocation --------------------------------------
  * kmm_xyzfft_noalloc has no counterpart in the reference.  It is kmm_xyzfft (the physical ->
@@ -305,10 +334,13 @@ int  kmm_set_option(kmm_ctx *ctx, int option, int value);
  * the working copy of the physical field lives in a file-scope device array of
  * KMM_XYZFFT_NOALLOC_MAX doubles (32 MiB) that every GPU loading the library holds until the
  * process exits; (ny+1)*nz*nx above that limit is rejected with KMM_ERR_ARG before any work, as are
- * transform lengths 2*ny, nx, nz that are not 2^a 3^b 5^c or exceed 4096.  The first call on each
- * device (the current one) resolves the array's device address once.  Every call on a device
- * shares the array and overwrites it completely; calls that overlap on the GPU (other streams or
- * host threads) race on it, so serialise them.                                          */
+ * transform lengths 2*ny, nx, nz that are not 2^a 3^b 5^c or exceed 4096.  Each call looks up the
+ * array's device address on the current device (cudaGetSymbolAddress, which allocates nothing).
+ * A call whose transform lengths differ from the previous call's on that device first sends new
+ * twiddle tables from pageable host memory, so it returns only when the stream has reached that
+ * copy.  Every call on a device shares the array and overwrites it completely; calls that overlap
+ * on the GPU (other streams) race on it, and calls from two host threads at once also race on the
+ * library's host-side cache of addresses and twiddle lengths, so serialise all calls.   */
 #define KMM_XYZFFT_NOALLOC_MAX (4 * 1024 * 1024)
 int  kmm_xyzfft_noalloc(const double *phys, double *spec, int nx, int ny, int nz, void *stream);
 

@@ -18,6 +18,9 @@
 #include <stdlib.h>
 #include <string.h>
 #include <stdint.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 typedef double complex cplx;
 
@@ -183,6 +186,8 @@ struct orc_ctx {
     fftplan py2, pmz, pmx, pnx, pnz; /* 2*ny (DCT), mz, mx, nx, nz */
     double *cfl;
     double *scsource; /* (nyp,mz,mx) */
+    int frate_ready;                    /* constant flow rate: W and G built */
+    double frate_w[1025], frate_g[1025];
 };
 
 #define SIDX(C, i, j, k) ((((size_t)(k)) * (size_t)(C)->nz + (size_t)(j)) * (size_t)(C)->nyp + (size_t)(i))
@@ -238,6 +243,18 @@ int orc_zero(orc_ctx *c, int f)
 int orc_set_it(orc_ctx *c, int it) { c->it = it; return KMM_OK; }
 int orc_get_stats(orc_ctx *c, kmm_stats *s) { c->stats.it = c->it; *s = c->stats; return KMM_OK; }
 double orc_dpdx(orc_ctx *c) { return c->dPdx; }
+
+/* OpenMP threads of the parallel loops (n <= 0: all host cores); returns the count in effect */
+int orc_set_threads(int n)
+{
+#ifdef _OPENMP
+    omp_set_num_threads(n > 0 ? n : omp_get_num_procs());
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
 
 /* setbcs, main_dns.f90:1175-1418 */
 static void setbcs(orc_ctx *c)
@@ -302,6 +319,7 @@ int orc_ctx_create(const kmm_params *p, orc_ctx **out)
     setbcs(c);
     /* init_flow.f90:117 (channel): dPdx = -2/yl (2 R_tau/(yl re))^2 */
     c->dPdx = -2.0 / c->yl * pow(2.0 * p->r_tau / (c->yl * c->re), 2);
+    c->stats.dpdx = c->dPdx;
     /* forcepre: force-spreading matrix, main_dns.f90:1551-1558 */
     for (int i = 1; i <= 10; ++i)
         for (int j = 1; j <= 10; ++j) {
@@ -980,12 +998,9 @@ static void psolve1d(const orc_ctx *c, double *u, double g, double dyde, double 
 }
 
 /* uzero(u0,h1,h1l,uflag), solvers.f90:1065-1176 */
-int orc_uzero(orc_ctx *c, int uflag)
+/* uzero on explicit arrays (u0 in / out, h1 = h_n, h1l = h_(n-1)) */
+static void uzero_arrays(orc_ctx *c, int uflag, double *u0, const double *h1, const double *h1l)
 {
-    if (c->nyp > 1024) return KMM_ERR_ARG;
-    double *u0 = RF(c, uflag == 1 ? KMM_U0 : KMM_W0);
-    double *h1 = RF(c, uflag == 1 ? KMM_H1N : KMM_H3N);
-    double *h1l = RF(c, uflag == 1 ? KMM_H1NM1 : KMM_H3NM1);
     double wrk1[1025], t[1025];
     const double re = c->re, dt = c->dt, th = c->theta;
     for (int i = 0; i < c->nyp; ++i) wrk1[i] = -re * u0[i] / (dt * th) - re * (3.0 * h1[i] - h1l[i]) / (2.0 * th);
@@ -999,7 +1014,54 @@ int orc_uzero(orc_ctx *c, int uflag)
     double g = re / (th * dt);
     if (uflag == 1) psolve1d(c, u0, g, c->dyde, c->atu, c->btu, c->gtu, c->abu, c->bbu, c->gbu);
     else psolve1d(c, u0, g, c->dyde, c->atw, c->btu, c->gtw, c->abw, c->bbw, c->gbw); /* btu: as the reference passes */
+}
+
+int orc_uzero(orc_ctx *c, int uflag)
+{
+    if (c->nyp > 1024) return KMM_ERR_ARG;
+    uzero_arrays(c, uflag, RF(c, uflag == 1 ? KMM_U0 : KMM_W0), RF(c, uflag == 1 ? KMM_H1N : KMM_H3N),
+                 RF(c, uflag == 1 ? KMM_H1NM1 : KMM_H3NM1));
     return KMM_OK;
+}
+
+/* Constant flow rate (kmm_params.flow_rate > 0; no counterpart in the reference, which holds dPdx
+ * constant, init_flow.f90:117, solvers.f90:3044-3045).  The bulk velocity is the trapezoid of
+ * writeoutputs (helpers.f90:1355-1359) over the Gauss-Lobatto points of the mean profile
+ * u(y_i) = sum_n u0_n cos(n pi i / ny), i.e. Q = sum_n W_n u0_n with
+ * W_n = (1/yl) sum_i (cos(n pi i/ny) + cos(n pi (i+1)/ny)) / 2 |y_(i+1) - y_i|.  G is the response of
+ * the u0 step (uzero) to a unit uniform acceleration over one step with homogeneous walls: the
+ * solve with h_n = h_(n-1) = T_0 from u0 = 0, less the solve with zero forcing (which carries the
+ * wall values).  After each u0 solve, delta = (flow_rate - Q) / (W . G) and u0 += delta G: the step
+ * was driven by the mean pressure gradient dPdx - delta. */
+static void frate_setup(orc_ctx *c)
+{
+    const int nyp = c->nyp, ny = c->ny;
+    for (int n = 0; n < nyp; ++n) {
+        double w = 0.0;
+        for (int i = 0; i < ny; ++i)
+            w += 1.0 / c->yl * 0.5 * (cos((double)n * c->pi * (double)(i + 1) / (double)ny) +
+                                      cos((double)n * c->pi * (double)i / (double)ny)) *
+                 fabs(c->ycoord[i + 1] - c->ycoord[i]);
+        c->frate_w[n] = w;
+    }
+    double ua[1025] = {0.0}, ub[1025] = {0.0}, ha[1025] = {0.0}, hb[1025] = {0.0};
+    ha[0] = 1.0;
+    uzero_arrays(c, 1, ua, ha, ha);
+    uzero_arrays(c, 1, ub, hb, hb);
+    for (int i = 0; i < nyp; ++i) c->frate_g[i] = ua[i] - ub[i];
+    c->frate_ready = 1;
+}
+
+static void frate_apply(orc_ctx *c)
+{
+    if (!(c->p.flow_rate > 0.0)) { c->stats.dpdx = c->dPdx; return; }
+    if (!c->frate_ready) frate_setup(c);
+    double *u0 = RF(c, KMM_U0);
+    double q = 0.0, wg = 0.0;
+    for (int i = 0; i < c->nyp; ++i) { q += c->frate_w[i] * u0[i]; wg += c->frate_w[i] * c->frate_g[i]; }
+    const double d = (c->p.flow_rate - q) / wg;
+    for (int i = 0; i < c->nyp; ++i) u0[i] += d * c->frate_g[i];
+    c->stats.dpdx = c->dPdx - d;
 }
 
 /* ------------------------------------------------------------------------- */
@@ -1435,6 +1497,31 @@ static int fluid_interp(const orc_ctx *c, double xp, double yp, double zp, const
 #undef INTERP
 #undef P3
     return KMM_OK;
+}
+
+/* the interpolation cell fluid_interp looks up for every particle (part_track.f90:560-577):
+ * cells[p] = imin, cells[np + p] = jmin, cells[2 np + p] = kmax, 1-based; 0 and KMM_ERR_INTERP
+ * where the reference stops (part_track.f90:580-590) */
+int orc_tracer_cells(orc_ctx *c, int *cells, size_t n)
+{
+    const int np = c->p.npart, mx = c->mx, mz = c->mz;
+    if (np <= 0) return KMM_OK;
+    if (n < 3 * (size_t)np) return KMM_ERR_ARG;
+    const double *xpa = RF(c, KMM_XPART), *ypa = RF(c, KMM_YPART), *zpa = RF(c, KMM_ZPART);
+    const double delxm = c->xl / (double)mx, delzm = c->zl / (double)mz;
+    int st = KMM_OK;
+    for (int p = 0; p < np; ++p) {
+        int imin = ((int)floor(xpa[p] / delxm) + mx) % mx + 1;
+        int jmin = ((int)floor(zpa[p] / delzm) + mz) % mz + 1;
+        int kmax = (int)floor(1.0 + (double)c->ny / c->pi * acos(2.0 * ypa[p] / c->yl));
+        int kmin = kmax + 1;
+        int ok = !(imin < 1 || jmin < 1 || kmin < 1 || kmin > c->nyp || kmax < 1);
+        cells[p] = ok ? imin : 0;
+        cells[np + p] = ok ? jmin : 0;
+        cells[2 * np + p] = ok ? kmax : 0;
+        if (!ok) st = KMM_ERR_INTERP;
+    }
+    return st;
 }
 
 /* init_part, part_track.f90:229-292: particle velocity forced to the fluid's */
@@ -1901,8 +1988,9 @@ int orc_vcw3dp(orc_ctx *c)
                     /* 5x5 force spreading, solvers.f90:3069-3108.  The j-range test of the reference
                      * (j >= 3 .or. j <= mz-2) is always true, so targets j+jj fall outside 1..mz and
                      * land in the neighbouring x column of the column-major plane; targets outside the
-                     * plane array itself are dropped here. */
-                    if (i + 1 <= kmaxsurf) {
+                     * plane array itself are dropped here.  With ib_spread_all (no counterpart in the
+                     * reference) every plane spreads once any solid cell exists. */
+                    if ((c->p.ib_spread_all && kmaxsurf > 0) || i + 1 <= kmaxsurf) {
                         for (int ii = -2; ii <= 2; ++ii) {
                             int ipii = k + ii;
                             int idif = 1 + abs(ii);
@@ -2235,6 +2323,7 @@ int orc_step(orc_ctx *c)
     orc_influence(c);
     orc_penta(c, KMM_OMY, re / (dt * th), 0, c->atu, c->btu, c->abu, c->bbu);
     orc_uzero(c, 1);
+    frate_apply(c);
     orc_uzero(c, 3);
     cplx *omy = SF(c, KMM_OMY);
     for (int i = 0; i < nyp; ++i) omy[SIDX(c, i, 0, 0)] = 0.0;

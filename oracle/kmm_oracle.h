@@ -45,6 +45,8 @@ int    orc_zero(orc_ctx *c, int field);
 int    orc_set_it(orc_ctx *c, int it);
 int    orc_get_stats(orc_ctx *c, kmm_stats *s);
 double orc_dpdx(orc_ctx *c);
+/* OpenMP threads of the parallel loops (n <= 0: all host cores); returns the count in effect */
+int    orc_set_threads(int n);
 
 /* transforms (the FFTW conventions the reference relies on) */
 int    orc_dct1(int n, const double *in, double *out);                 /* REDFT00, length n      */
@@ -81,6 +83,8 @@ int orc_run(orc_ctx *c, int n);
 int orc_tracer_update(orc_ctx *c);
 int orc_inertial_update(orc_ctx *c);   /* particle_flag > 0: Maxey-Riley RK4, part_track.f90:617-1075 */
 int orc_init_part(orc_ctx *c);
+/* interpolation cells of the particles, as kmm_tracer_cells (part_track.f90:560-577) */
+int orc_tracer_cells(orc_ctx *c, int *cells, size_t n);
 /* swirl strength from the closed-form eigenvalues (helpers.f90:197-404) on the last 3/2-grid gradients */
 int orc_calcswirl(orc_ctx *c);
 int orc_flowstats(orc_ctx *c, double *prof, double *scal);

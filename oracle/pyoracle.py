@@ -57,12 +57,21 @@ def lib():
         dp = ctypes.POINTER(ctypes.c_double)
         L.orc_flowstats.argtypes = [vp, dp, dp]
         L.orc_flowstats.restype = i
+        L.orc_tracer_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_size_t]
+        L.orc_tracer_cells.restype = i
+        L.orc_set_threads.argtypes = [i]
+        L.orc_set_threads.restype = i
         L.orc_dct1.argtypes = [i, dp, dp]
         L.orc_fft.argtypes = [i, dp, dp, i]
         L.orc_rfft.argtypes = [i, dp, dp]
         L.orc_irfft.argtypes = [i, dp, dp]
         _lib = L
     return _lib
+
+
+def set_threads(n):
+    """OpenMP threads of the oracle's parallel loops (n <= 0: all host cores); returns the count."""
+    return int(lib().orc_set_threads(int(n)))
 
 
 def _dp(a):
@@ -157,6 +166,14 @@ class Oracle:
 
     def dpdx(self):
         return self.L.orc_dpdx(self.h)
+
+    def tracer_cells(self):
+        """orc_tracer_cells: (3, npart) int32 1-based interpolation cells (imin, jmin, kmax)."""
+        cells = np.zeros(3 * self.npart, np.int32)
+        st = self.L.orc_tracer_cells(self.h, cells.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), cells.size)
+        if st:
+            raise RuntimeError("orc_tracer_cells returned %d" % st)
+        return cells.reshape(3, self.npart)
 
     def flowstats(self):
         """(prof[7][nyp], scal[4]) of orc_flowstats: umean, urms, vrms, wrms, R12, T12, ke profiles;

@@ -8,6 +8,9 @@ import ctypes
 
 KMM_ABI_VERSION = 1
 
+# options (enum kmm_option)
+OPT_FUSED, OPT_COLUMN_BLOCKED, OPT_GRAPH, OPT_ZTMA, OPT_WAIT_LIMIT_MS = 1, 2, 3, 4, 5
+
 # status codes (enum kmm_status)
 OK, ERR_ARG, ERR_CUDA, ERR_CFL, ERR_NAN, ERR_INTERP, ERR_TIMEOUT, ERR_NOMEM, ERR_UNSUPPORTED, ERR_PCFL = range(10)
 STATUS_NAMES = {
@@ -44,6 +47,8 @@ _PARAM_FIELDS = [
     ("scalar_q", ctypes.c_double),
     ("tracer_scheme", ctypes.c_int),
     ("precision", ctypes.c_int),
+    ("ib_spread_all", ctypes.c_int),
+    ("flow_rate", ctypes.c_double),
 ]
 
 
@@ -53,7 +58,7 @@ class KmmParams(ctypes.Structure):
 
 class KmmStats(ctypes.Structure):
     _fields_ = [("cflmax", ctypes.c_double), ("umax", ctypes.c_double), ("it", ctypes.c_int), ("status", ctypes.c_int),
-                ("pumax", ctypes.c_double), ("pcfl", ctypes.c_double)]
+                ("pumax", ctypes.c_double), ("pcfl", ctypes.c_double), ("dpdx", ctypes.c_double)]
 
 
 def _enum(names, start=0):
@@ -133,7 +138,7 @@ def field_shape(fid, nx, ny, nz, npart=0):
 def default_params(**kw):
     """Reference defaults for a plain channel (flow_select = 1, theta = 0.5), overridable by keyword."""
     p = KmmParams()
-    base = dict(nsteps=1, iprnfrq=1000, dt=0.01, gain=-400.0, ugain=-40.0, theta=0.5,
+    base = dict(nsteps=1, iprnfrq=1000, dt=0.01, gain=400.0, ugain=40.0, theta=0.5,
                 ny=32, nz=32, nx=32, bftail=0, yl=2.0, zl=6.283185307179586, xl=12.566370614359172,
                 re=1400.0, xstart=0.0, uinf=0.0, kwall=0, perturbtime=0, r_tau=64.80740698407860,
                 gravity=0.0, irstrt=0, crstrt=0, print3d=0, geomtype=0, particle_flag=0, flow_select=1,
@@ -141,7 +146,8 @@ def default_params(**kw):
                 c_mu=1.0, cd_switch=0, zlmax=30.0, tpoly=20.0, alpha_poly=0.0, diffpoly=1000.0,
                 c11z=1.0, c22z=1.0, c33z=1.0, qbeta=0.9, diff=1.0, deltat=0.0, sigmax=0.01, sigmay=0.01,
                 sigmaz=0.01, src_start=0, src_stop=-1, scltarg=0, cadence=1000000, spts=0.0,
-                scalar_on=0, polymer_on=0, scalar_bc=0, scalar_q=0.0, tracer_scheme=0, precision=0)
+                scalar_on=0, polymer_on=0, scalar_bc=0, scalar_q=0.0, tracer_scheme=0, precision=0,
+                ib_spread_all=0, flow_rate=0.0)
     base.update(kw)
     for k, v in base.items():
         if not hasattr(p, k):

@@ -6,6 +6,7 @@ Objects go to polymer_dns_b200/_build/ (ignored by git); the shared library land
 next to this file so it travels with the source tree.
 """
 import argparse
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -43,16 +44,23 @@ def _stale(target, deps):
 def build(force=False, verbose=False, extra=()):
     os.makedirs(BUILD, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "kmm.h")]
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
-            cmd = [nvcc()] + ARCH + COMMON + PER_FILE.get(src, []) + list(extra) + ["-c", s, "-o", o]
+            cmds.append([nvcc()] + ARCH + COMMON + PER_FILE.get(src, []) + list(extra) + ["-c", s, "-o", o])
+    # the translation units compile independently: run them side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        futs = []
+        for cmd in cmds:
             if verbose:
                 print(" ".join(cmd), flush=True)
-            subprocess.check_call(cmd)
+            futs.append(ex.submit(subprocess.run, cmd))
+        for cmd, f in zip(cmds, futs):
+            if f.result().returncode != 0:
+                raise subprocess.CalledProcessError(f.result().returncode, cmd)
     if force or _stale(LIB, objs):
         cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"]
         if verbose:

@@ -1,8 +1,10 @@
 // kmm_async.cuh -- mbarrier and one-dimensional bulk-copy helpers (sm_90+ PTX) for kernels that
 // stage global rows into shared memory with the asynchronous copy engine.  Every wait is bounded:
-// after ~2 s of %globaltimer it gives up and returns false, and the caller records an error.
+// after the unit's limit (default 2 s) of %globaltimer it gives up and returns false, and the caller
+// records an error.
 #pragma once
 
+#include <cuda_runtime.h>
 #include <stdint.h>
 
 namespace kasync {
@@ -26,8 +28,12 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm_addr(bar)), "r"(bytes) : "memory");
 }
 
-// wait for phase `phase` of a barrier, at most ~2 s; false if the limit ran out
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase) {
+// limit of the bounded waits in nanoseconds (default 2 s).  `static`: every translation unit that
+// includes this header has its own copy, set through kasync_set_wait_limit from that unit.
+static __device__ unsigned long long kasync_wait_ns = 2000000000ull;
+
+// wait for phase `phase` of a barrier, at most `limit_ns` of %globaltimer; false if the limit ran out
+__device__ __forceinline__ bool mbar_wait_for(uint64_t *bar, unsigned phase, unsigned long long limit_ns) {
     const unsigned long long t0 = gtimer();
     for (;;) {
         uint32_t done;
@@ -39,8 +45,18 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase) {
             : "r"(sm_addr(bar)), "r"(phase)
             : "memory");
         if (done) return true;
-        if (gtimer() - t0 > 2000000000ull) return false;
+        if (gtimer() - t0 > limit_ns) return false;
     }
+}
+
+// the same with the unit's current limit (kasync_wait_ns)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase) {
+    return mbar_wait_for(bar, phase, kasync_wait_ns);
+}
+
+// set this translation unit's wait limit on the current device (synchronous; not during capture)
+static inline cudaError_t kasync_set_wait_limit(unsigned long long ns) {
+    return cudaMemcpyToSymbol(kasync_wait_ns, &ns, sizeof(ns));
 }
 
 // global -> shared copy of `bytes` bytes (both addresses 16-byte aligned, bytes a multiple of 16),

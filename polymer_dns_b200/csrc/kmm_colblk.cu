@@ -437,6 +437,7 @@ int kmm_colblk_fwd(kmm_ctx *ctx, const ColFwdArgs &A, const FusedTabs &T, const 
         RET(kmm_smem_attr(ctx, (const void *)k_bcol_v<KK, CC>, smem));                                \
         k_bcol_v<KK, CC><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(A, T, rj, twc);                   \
         CKL();                                                                                        \
+        RET(kmm_flowrate_apply(ctx, ctx->stream));                                                    \
         if (A.scalar) CK(cudaStreamWaitEvent(ctx->stream, ctx->cjoin_ev[0], 0));                      \
         CK(cudaStreamWaitEvent(ctx->stream, ctx->cjoin_ev[1], 0));                                    \
         RET(kmm_smem_attr(ctx, (const void *)k_bcol_uw<KK, CC>, smem));                               \

@@ -856,6 +856,97 @@ extern "C" int kmm_uzero(kmm_ctx *ctx, int uflag) {
 }
 
 // ---------------------------------------------------------------------------
+// Constant flow rate (kmm_params.flow_rate > 0; no counterpart in the reference, which holds the
+// mean pressure gradient dPdx of init_flow.f90:117 constant).  The bulk velocity is the trapezoid
+// of writeoutputs (helpers.f90:1355-1359) over the Gauss-Lobatto points of the mean profile
+// u(y_i) = sum_n u0_n cos(n pi i / ny): Q = W . u0 with
+// W_n = (1/yl) sum_i (cos(n pi i/ny) + cos(n pi (i+1)/ny)) / 2 |y_(i+1) - y_i| (FP64, host).  G is the
+// response of the u0 step to a unit uniform acceleration over one step with homogeneous walls: the
+// uzero solve with h_n = h_(n-1) = T_0 from u0 = 0, less the same solve with zero forcing.  After
+// each u0 solve one warp sets delta = (flow_rate - W . u0) / (W . G) and u0 += delta G; the step was
+// then driven by dPdx - delta (kmm_stats.dpdx).
+// d_frate layout: W [nyp] | G [nyp] | delta [1] | scratch 4 nyp (ua, ha, ub, hb)
+// ---------------------------------------------------------------------------
+__global__ void k_frate_fill(double *s, int nyp) {
+    for (int i = threadIdx.x; i < 4 * nyp; i += blockDim.x) s[i] = (i == nyp) ? 1.0 : 0.0;   // ha[0] = 1
+}
+
+__global__ void k_frate_g(double *G, const double *ua, const double *ub, int nyp) {
+    for (int i = threadIdx.x; i < nyp; i += blockDim.x) G[i] = ua[i] - ub[i];
+}
+
+__global__ void k_flowrate(double *__restrict__ u0, const double *__restrict__ W, const double *__restrict__ G, int nyp,
+                           double target, double *__restrict__ delta) {
+    const int lane = threadIdx.x & 31;
+    double q = 0.0, wg = 0.0;
+    for (int i = lane; i < nyp; i += 32) {
+        q += W[i] * u0[i];
+        wg += W[i] * G[i];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        q += __shfl_xor_sync(0xffffffffu, q, o);
+        wg += __shfl_xor_sync(0xffffffffu, wg, o);
+    }
+    const double d = (target - q) / wg;
+    for (int i = lane; i < nyp; i += 32) u0[i] += d * G[i];
+    if (lane == 0) *delta = d;
+}
+
+int kmm_flowrate_setup(kmm_ctx *ctx) {
+    if (!(ctx->p.flow_rate > 0.0) || ctx->frate_ready) return KMM_OK;
+    const int nyp = ctx->nyp, ny = ctx->ny;
+    if (!ctx->d_frate) CK(cudaMalloc(&ctx->d_frate, sizeof(double) * (6 * (size_t)nyp + 1)));
+    double *W = ctx->d_frate, *G = W + nyp, *sc = W + 2 * nyp + 1;
+    double *hw = (double *)malloc(sizeof(double) * (size_t)nyp);
+    for (int n = 0; n < nyp; ++n) {
+        double w = 0.0;
+        for (int i = 0; i < ny; ++i)
+            w += 1.0 / ctx->yl * 0.5 * (cos((double)n * ctx->pi * (double)(i + 1) / (double)ny) +
+                                        cos((double)n * ctx->pi * (double)i / (double)ny)) *
+                 fabs(ctx->h_ycoord[i + 1] - ctx->h_ycoord[i]);
+        hw[n] = w;
+    }
+    cudaError_t e = cudaMemcpyAsync(W, hw, sizeof(double) * (size_t)nyp, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    free(hw);
+    CK(e);
+    k_frate_fill<<<1, 256, 0, ctx->stream>>>(sc, nyp);
+    CKL();
+    double *ua = sc, *ha = sc + nyp, *ub = sc + 2 * nyp, *hb = sc + 3 * nyp;
+    const size_t sm = uzero_smem(nyp);
+    RET(kmm_smem_attr(ctx, (const void *)k_uzero, sm));
+    k_uzero<<<1, 128, sm, ctx->stream>>>(ua, ha, ha, nyp, ctx->re, ctx->dt, ctx->theta, ctx->dyde, ctx->atu, ctx->btu,
+                                         ctx->gtu, ctx->abu, ctx->bbu, ctx->gbu, ctx->h_c[0], ctx->h_wavz[0]);
+    CKL();
+    k_uzero<<<1, 128, sm, ctx->stream>>>(ub, hb, hb, nyp, ctx->re, ctx->dt, ctx->theta, ctx->dyde, ctx->atu, ctx->btu,
+                                         ctx->gtu, ctx->abu, ctx->bbu, ctx->gbu, ctx->h_c[0], ctx->h_wavz[0]);
+    CKL();
+    k_frate_g<<<1, 256, 0, ctx->stream>>>(G, ua, ub, nyp);
+    CKL();
+    CK(cudaMemsetAsync(W + 2 * nyp, 0, sizeof(double), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->frate_ready = 1;
+    return KMM_OK;
+}
+
+// after the u0 solve (main_dns.f90:489-492), on stream st; the correction goes to the pinned slot
+// read by kmm_get_stats
+int kmm_flowrate_apply(kmm_ctx *ctx, cudaStream_t st) {
+    if (!(ctx->p.flow_rate > 0.0)) return KMM_OK;
+    if (!ctx->frate_ready) {
+        kmm_set_error(ctx, "constant flow rate: kmm_initial has not run");
+        return KMM_ERR_ARG;
+    }
+    const int nyp = ctx->nyp;
+    double *W = ctx->d_frate, *G = W + nyp, *delta = W + 2 * nyp;
+    k_flowrate<<<1, 32, 0, st>>>(REAL(ctx, KMM_U0), W, G, nyp, ctx->p.flow_rate, delta);
+    CKL();
+    CK(cudaMemcpyAsync(kmm_h_pin_delta(ctx), delta, sizeof(double), cudaMemcpyDeviceToHost, st));
+    return KMM_OK;
+}
+
+// ---------------------------------------------------------------------------
 // pointwise spectral kernels
 // ---------------------------------------------------------------------------
 #define GRID_LOOP(n) for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < (n); idx += (size_t)gridDim.x * blockDim.x)

@@ -131,6 +131,7 @@ extern "C" int kmm_get_stats(kmm_ctx *ctx, kmm_stats *out) {
     if (!ctx || !out) return KMM_ERR_ARG;
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->stats.it = ctx->it;
+    ctx->stats.dpdx = ctx->dPdx - (ctx->p.flow_rate > 0.0 ? *kmm_h_pin_delta(ctx) : 0.0);
     *out = ctx->stats;
     return KMM_OK;
 }
@@ -295,7 +296,8 @@ extern "C" int kmm_ctx_create(const kmm_params *p, int device, kmm_ctx **out) {
     CK(cudaMalloc(&c->d_pumax, sizeof(double)));
     CK(cudaMemset(c->d_pumax, 0, sizeof(double)));
     CK(cudaMalloc(&c->d_scratch, sizeof(double) * 9 * KMM_MAX_NYP));
-    CK(cudaMallocHost(&c->h_pin, sizeof(double) * (2 * KMM_MAX_NYP + 1)));
+    CK(cudaMallocHost(&c->h_pin, sizeof(double) * KMM_H_PIN_DOUBLES));
+    memset(c->h_pin, 0, sizeof(double) * KMM_H_PIN_DOUBLES);
     CK(cudaMemset(c->d_status, 0, sizeof(int)));
     for (int w = 0; w < 6; ++w) {
         CK(cudaMalloc(&c->wrk[w], sizeof(double2) * c->nspec));
@@ -334,6 +336,7 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
     if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
     if (ctx->po) cudaFree(ctx->po);
     if (ctx->drag) cudaFree(ctx->drag);
+    if (ctx->d_frate) cudaFree(ctx->d_frate);
     for (int f = 0; f < KMM_MAXF; ++f)
         if (ctx->f[f]) cudaFree(ctx->f[f]);
     for (int w = 0; w < 6; ++w)
@@ -463,6 +466,20 @@ extern "C" int kmm_set_option(kmm_ctx *ctx, int option, int value) {
     case KMM_OPT_COLUMN_BLOCKED: ctx->use_colblk = value ? 1 : 0; kmm_graph_release(ctx); return KMM_OK;
     case KMM_OPT_GRAPH: ctx->use_graph = value ? 1 : 0; kmm_graph_release(ctx); return KMM_OK;
     case KMM_OPT_ZTMA: ctx->use_ztma = value ? 1 : 0; kmm_graph_release(ctx); return KMM_OK;
+    case KMM_OPT_WAIT_LIMIT_MS: {
+        if (value < 100 || value > 60000) {
+            kmm_set_error(ctx, "wait limit %d ms outside 100 .. 60000", value);
+            return KMM_ERR_ARG;
+        }
+        const unsigned long long ns = (unsigned long long)value * 1000000ull;
+        CK(cudaSetDevice(ctx->device));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (kmm_plane_set_wait_limit(ns) || kmm_ztma_set_wait_limit(ns)) {
+            kmm_set_error(ctx, "setting the wait limit failed");
+            return KMM_ERR_CUDA;
+        }
+        return KMM_OK;
+    }
     default: return KMM_ERR_ARG;
     }
 }

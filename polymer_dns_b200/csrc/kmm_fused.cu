@@ -913,6 +913,10 @@ int kmm_tracers(kmm_ctx *ctx);
 // (nb = nt = 1 or 2), nyp in the compiled register layouts, and the x transform instance exists
 bool kmm_fused_applicable(const kmm_ctx *ctx) {
     if (ctx->p.polymer_on || ctx->f[KMM_IMATRIX] != NULL) return false;
+    // the flow-rate correction sits between the v and the u, w column kernels, which only the
+    // blocked kernels (ny = 32, 64, 96, 128) launch separately
+    const bool blocked = ctx->use_colblk && (ctx->ny == 32 || ctx->ny == 64 || ctx->ny == 96 || ctx->ny == 128);
+    if (ctx->p.flow_rate > 0.0 && !blocked) return false;
     if (ctx->p.scalar_on && ctx->p.scl_flag >= 2) return false;
     if (ctx->p.particle_flag > 0 && ctx->p.npart > 0) return false;   // inertial particles: routine vcw3dp
     const int E = (ctx->nyp + 31) / 32;

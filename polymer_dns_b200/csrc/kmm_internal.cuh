@@ -107,6 +107,8 @@ struct kmm_ctx {
     void *ztma;       // its cached tensor maps (kmm_ztma.cu)
     void *tauc;       // tau tables of the routine solves' (g, boundary-condition) configurations (kmm_fused.cu)
     float2 *rtw32[3]; // FP32 twiddles of 2 ny, mz, mx for the routine path's mixed form (kmm_fused.cu)
+    double *d_frate;  // constant flow rate: W, G, the last correction, scratch (kmm_column.cu)
+    int frate_ready;
 };
 
 void kmm_fused_release(kmm_ctx *ctx);
@@ -127,6 +129,9 @@ int kmm_zf_tma(kmm_ctx *ctx, const double2 *r, double2 *yo, int nout, const doub
 int kmm_zb_tma32(kmm_ctx *ctx, const float2 *yp, float2 *q, int nbase, int nq, const float2 *tw);
 int kmm_zf_tma32(kmm_ctx *ctx, const float2 *r, float2 *yo, int nout, const float2 *tw);
 void kmm_ztma_release(kmm_ctx *ctx);
+// bounded-wait limits of the units with mbarrier waits (on the current device; nonzero on failure)
+int kmm_ztma_set_wait_limit(unsigned long long ns);
+int kmm_plane_set_wait_limit(unsigned long long ns);
 void kmm_tic(kmm_ctx *ctx);
 void kmm_toc(kmm_ctx *ctx, int stage);
 
@@ -137,8 +142,10 @@ int kmm_field_info(const kmm_ctx *ctx, int field, size_t *nelem, int *eb);
 void *kmm_field_ptr(kmm_ctx *ctx, int field);   // allocates (zeroed) on first use, NULL on failure
 static inline double2 *SPEC(kmm_ctx *ctx, int f) { return (double2 *)kmm_field_ptr(ctx, f); }
 static inline double *REAL(kmm_ctx *ctx, int f) { return (double *)kmm_field_ptr(ctx, f); }
-// the pinned status word after the cfl and umax rows of h_pin
+// the pinned status word after the cfl and umax rows of h_pin, and the flow-rate correction after it
 static inline int *kmm_h_pin_status(kmm_ctx *ctx) { return (int *)(ctx->h_pin + 2 * KMM_MAX_NYP); }
+static inline double *kmm_h_pin_delta(kmm_ctx *ctx) { return ctx->h_pin + 2 * KMM_MAX_NYP + 1; }
+#define KMM_H_PIN_DOUBLES (2 * KMM_MAX_NYP + 2)
 
 // internal entry points shared between translation units
 int kmm_internal_cderiv(kmm_ctx *ctx, const double2 *f, double2 *df);
@@ -186,6 +193,10 @@ int kmm_ensure_plane_buffers(kmm_ctx *ctx, int nin, int nout);
 int kmm_phys_layout(kmm_ctx *ctx, int field, void *dev, const void *host_src, void *host_dst);
 int kmm_internal_polynl(kmm_ctx *ctx, double2 *const *nl);
 int kmm_internal_phirhs(kmm_ctx *ctx, double2 *V, const double2 *F, const double2 *FM, double var);
+// constant flow rate (kmm_params.flow_rate > 0): tables built once by kmm_initial, the correction
+// after every u0 solve (kmm_column.cu)
+int kmm_flowrate_setup(kmm_ctx *ctx);
+int kmm_flowrate_apply(kmm_ctx *ctx, cudaStream_t st);
 
 // ---------------------------------------------------------------------------
 // complex helpers on double2

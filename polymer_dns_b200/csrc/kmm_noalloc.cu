@@ -52,16 +52,21 @@ extern "C" int kmm_xyzfft_noalloc(const double *phys, double *spec, int nx, int 
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return KMM_ERR_CUDA;
     cudaStream_t st = (cudaStream_t)stream;
-    // set-up once per device (the device that is current): resolve the arrays' device addresses
-    if (!s_scratch[dev]) {
+    // the arrays' device addresses on the current device, resolved on every call (a lookup that
+    // allocates nothing); if they moved (the device was reset and the module reloaded), the
+    // twiddles cached there are gone and are sent again
+    {
         void *a = NULL, *b = NULL;
         if (cudaGetSymbolAddress(&a, g_noalloc_scratch) != cudaSuccess) return KMM_ERR_CUDA;
         if (cudaGetSymbolAddress(&b, g_noalloc_tw) != cudaSuccess) return KMM_ERR_CUDA;
+        if ((double *)a != s_scratch[dev] || (double2 *)b != s_tw[dev])
+            for (int t = 0; t < 3; ++t) s_tw_len[dev][t] = 0;
         s_scratch[dev] = (double *)a;
         s_tw[dev] = (double2 *)b;
     }
     // twiddles exp(-2 pi i m/n), computed in long double as the context plans are; re-sent only
-    // when a transform length changes
+    // when a transform length changes.  The staging buffer is ordinary (pageable) host memory, so
+    // such a call returns only once the stream has reached the copy.
     const int lens[3] = {2 * ny, nx, nz};
     DevPlan *plans[3] = {&py2, &pnx, &pnz};
     for (int t = 0; t < 3; ++t) {

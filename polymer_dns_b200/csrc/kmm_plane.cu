@@ -9,7 +9,7 @@
 //                  pointwise u x omega, -u.grad(c), polymer source/stress, CFL, immersed
 //                  boundary forces and dPdx; physical outputs -> PO[o][y][z][x],
 //                  u,v,w -> 3/2-grid copies for the tracers                 (solvers.f90:2806-3139)
-//   4. k_spread  : 5x5 force spreading for the planes i <= kmaxsurf       (solvers.f90:3069-3108)
+//   4. k_spread  : 5x5 force spreading for the planes i <= kmaxsurf (or all, ib_spread_all) (solvers.f90:3069-3108)
 //   5. k_xfwd    : r2c along x, keep kx < nxh                              (solvers.f90:3147-3177)
 //   6. k_zfft_fwd: c2c along z, truncate to nz, /(mx*mz) -> PL[o][y][kx][kz] (solvers.f90:3180-3273)
 //   7. k_dct_bwd : DCT-I along y, /ny, halve first and last coefficient    (solvers.f90:3279-3416)
@@ -1241,15 +1241,17 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         xstat = true;
         kmm_toc(ctx, KMM_STAGE_XPHYS);
         if (ib_any && ctx->kmaxsurf > 0) {
-            const int ksp = ctx->kmaxsurf < nyp ? ctx->kmaxsurf : nyp;
+            // the reference spreads in the planes i <= kmaxsurf (an x extent, main_dns.f90:1526-1535);
+            // ib_spread_all (no counterpart in the reference) spreads in every plane
+            const int ksp = (ctx->p.ib_spread_all || ctx->kmaxsurf >= nyp) ? nyp : ctx->kmaxsurf;
             const dim3 gs(kmm_blocks((size_t)mz * mx, 256) > 64 ? 64 : kmm_blocks((size_t)mz * mx, 256), ksp);
             if (f32)
-                k_spread<float><<<gs, 256, 0, ctx->stream>>>(po32, ctx->drag, ctx->d_fspread, nyp, mz, mx, ctx->kmaxsurf,
+                k_spread<float><<<gs, 256, 0, ctx->stream>>>(po32, ctx->drag, ctx->d_fspread, nyp, mz, mx, ksp,
                                                              A.slot_of_out[O_H1], A.slot_of_out[O_H2],
                                                              A.slot_of_out[O_H3]);
             else
                 k_spread<double><<<gs, 256, 0, ctx->stream>>>(ctx->po, ctx->drag, ctx->d_fspread, nyp, mz, mx,
-                                                              ctx->kmaxsurf, A.slot_of_out[O_H1], A.slot_of_out[O_H2],
+                                                              ksp, A.slot_of_out[O_H1], A.slot_of_out[O_H2],
                                                               A.slot_of_out[O_H3]);
             CKL();
         }
@@ -1561,4 +1563,38 @@ extern "C" int kmm_flowstats(kmm_ctx *ctx, double *prof, double *scal) {
     scal[2] = T12[nyp - 1];
     scal[3] = kb;
     return KMM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// bounded-wait check: one mbarrier that nothing arrives on and no copy targets, waited on with the
+// same bounded wait the bulk-copy kernels use; when the limit runs out the CTA records
+// KMM_ERR_TIMEOUT and returns, exactly as k_xphys2 and the TMA z kernels do.  No copy is in
+// flight, so giving up leaves nothing behind.
+// ---------------------------------------------------------------------------
+__global__ void k_wait_selftest(int *status, unsigned long long limit_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        kasync::mbar_init(&bar, 1);
+        kasync::mbar_init_fence();
+    }
+    __syncthreads();
+    const bool ok = kasync::mbar_wait_for(&bar, 0, limit_ns);
+    if (!__all_sync(0xffffffffu, ok) && (threadIdx.x & 31) == 0) atomicMax(status, KMM_ERR_TIMEOUT);
+}
+
+// this unit's bounded-wait limit on the current device (KMM_OPT_WAIT_LIMIT_MS)
+int kmm_plane_set_wait_limit(unsigned long long ns) { return kasync::kasync_set_wait_limit(ns) == cudaSuccess ? 0 : 1; }
+
+extern "C" int kmm_wait_selftest(kmm_ctx *ctx, double limit_ms) {
+    if (!ctx || !(limit_ms > 0.0) || limit_ms > 10000.0) return KMM_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+    k_wait_selftest<<<1, 32, 0, ctx->stream>>>(ctx->d_status, (unsigned long long)(limit_ms * 1e6));
+    CKL();
+    int st = 0;
+    CK(cudaMemcpyAsync(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (st == KMM_ERR_TIMEOUT) kmm_set_error(ctx, "bounded wait ran out after %.3f ms (expected)", limit_ms);
+    return st;
 }

@@ -224,6 +224,7 @@ extern "C" int kmm_initial(kmm_ctx *ctx) {
     kmm_graph_release(ctx);
     const size_t n = ctx->nspec;
     RET(kmm_gfcn(ctx));
+    RET(kmm_flowrate_setup(ctx));
     ctx->it = 0;
     if (ctx->p.irstrt >= 1) {
         RET(initial_restart(ctx));
@@ -380,6 +381,7 @@ extern "C" int kmm_step(kmm_ctx *ctx) {
     RET(kmm_influence(ctx));
     RET(kmm_penta(ctx, KMM_OMY, re / (dt * th), 0, ctx->atu, ctx->btu, ctx->abu, ctx->bbu));
     RET(kmm_uzero(ctx, 1));
+    RET(kmm_flowrate_apply(ctx, ctx->stream));
     RET(kmm_uzero(ctx, 3));
     k_zero_mean<<<1, 256, 0, ctx->stream>>>(SPEC(ctx, KMM_OMY), ctx->nyp);
     CKL();
@@ -459,8 +461,19 @@ extern "C" int kmm_polynl(kmm_ctx *ctx) {
 // processes, LO_multi_run/setup.py:93-101): every member's step is enqueued on its own stream
 // before any member is waited on, so the members' kernels overlap on the GPU
 // ---------------------------------------------------------------------------
+static int ensemble_step_all(kmm_ctx **ctxs, int n, int *status);
+
+// the caller's current device is restored before returning
 extern "C" int kmm_ensemble_step(kmm_ctx **ctxs, int n, int *status) {
     if (!ctxs || n <= 0 || n > KMM_MAX_ENSEMBLE || !status) return KMM_ERR_ARG;
+    int dev0 = 0;
+    if (cudaGetDevice(&dev0) != cudaSuccess) return KMM_ERR_CUDA;
+    const int st = ensemble_step_all(ctxs, n, status);
+    cudaSetDevice(dev0);
+    return st;
+}
+
+static int ensemble_step_all(kmm_ctx **ctxs, int n, int *status) {
     bool launched[KMM_MAX_ENSEMBLE];
     for (int m = 0; m < n; ++m) {
         kmm_ctx *c = ctxs[m];

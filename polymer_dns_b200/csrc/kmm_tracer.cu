@@ -416,6 +416,51 @@ int kmm_swirl_particles(kmm_ctx *ctx) {
 extern "C" int kmm_tracer_update(kmm_ctx *ctx) { return ctx ? tracer_launch(ctx, false) : KMM_ERR_ARG; }
 extern "C" int kmm_init_part(kmm_ctx *ctx) { return ctx ? tracer_launch(ctx, true) : KMM_ERR_ARG; }
 
+// the interpolation cell of each particle, the lookup of fluid_interp (part_track.f90:560-577)
+// with the same expressions as fluid_interp above; out-of-range entries are 0 and raise *bad
+__global__ void k_tracer_cells(TracerArgs T, const double *__restrict__ xpa, const double *__restrict__ ypa,
+                               const double *__restrict__ zpa, int *__restrict__ cells, int *bad) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= T.npart) return;
+    const double xp = xpa[p], yp = ypa[p], zp = zpa[p];
+    const int imin = ((int)floor(xp / T.delxm) + T.mx) % T.mx + 1;
+    const int jmin = ((int)floor(zp / T.delzm) + T.mz) % T.mz + 1;
+    const int kmax = (int)floor(1.0 + (double)T.ny / T.pi * acos(2.0 * yp / T.yl));
+    const int kmin = kmax + 1;
+    const bool ok = !(imin < 1 || jmin < 1 || kmin < 1 || kmin > T.nyp || kmax < 1);
+    cells[p] = ok ? imin : 0;
+    cells[T.npart + p] = ok ? jmin : 0;
+    cells[2 * T.npart + p] = ok ? kmax : 0;
+    if (!ok) atomicExch(bad, 1);
+}
+
+extern "C" int kmm_tracer_cells(kmm_ctx *ctx, int *cells, size_t n) {
+    if (!ctx || !cells) return KMM_ERR_ARG;
+    const int np = ctx->p.npart;
+    if (np <= 0) return KMM_OK;
+    if (n < 3 * (size_t)np) {
+        kmm_set_error(ctx, "kmm_tracer_cells: %zu ints given, 3 npart = %zu needed", n, 3 * (size_t)np);
+        return KMM_ERR_ARG;
+    }
+    const double *xp = REAL(ctx, KMM_XPART), *yp = REAL(ctx, KMM_YPART), *zp = REAL(ctx, KMM_ZPART);
+    if (!xp || !yp || !zp) return KMM_ERR_NOMEM;
+    int *d = NULL;
+    CK(cudaMallocAsync(&d, sizeof(int) * (3 * (size_t)np + 1), ctx->stream));
+    CK(cudaMemsetAsync(d + 3 * (size_t)np, 0, sizeof(int), ctx->stream));
+    k_tracer_cells<<<(np + 255) / 256, 256, 0, ctx->stream>>>(tracer_args(ctx), xp, yp, zp, d, d + 3 * (size_t)np);
+    CKL();
+    int bad = 0;
+    CK(cudaMemcpyAsync(cells, d, sizeof(int) * 3 * (size_t)np, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&bad, d + 3 * (size_t)np, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaFreeAsync(d, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (bad) {
+        kmm_set_error(ctx, "particle interpolation cell index out of range (part_track.f90:580-590)");
+        return KMM_ERR_INTERP;
+    }
+    return KMM_OK;
+}
+
 // ---------------------------------------------------------------------------
 // xyzfft(a,b,-1), helpers.f90:6-87: physical (nyp,nz,nx) -> spectral (nyp,nz,nxh)
 // ---------------------------------------------------------------------------

@@ -16,12 +16,14 @@
 // 101 KB of shared memory per CTA at mz = 192, so two CTAs share an SM and one's copies overlap
 // the other's FFTs.
 //
-// Every wait on an mbarrier is bounded (2 s of %globaltimer); a wait that runs out records
-// KMM_ERR_TIMEOUT in the step's status word and the CTA finishes without the data.
+// Every wait on an mbarrier is bounded (KMM_OPT_WAIT_LIMIT_MS, default 2 s of %globaltimer); a wait
+// that runs out records KMM_ERR_TIMEOUT in the step's status word and the CTA finishes without the
+// data.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
 #include "kmm_internal.cuh"
+#include "kmm_async.cuh"
 #include "kmm_fft.cuh"
 #include "kmm_fused.cuh"
 
@@ -32,12 +34,6 @@ namespace {
 
 __device__ __forceinline__ uint32_t sm_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ unsigned long long gtimer() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
 __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sm_addr(bar)), "r"(count) : "memory");
 }
@@ -46,22 +42,8 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm_addr(bar)), "r"(bytes) : "memory");
 }
 
-// wait for phase `phase` of a barrier, at most ~2 s; false if the limit ran out
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase) {
-    const unsigned long long t0 = gtimer();
-    for (;;) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(sm_addr(bar)), "r"(phase)
-            : "memory");
-        if (done) return true;
-        if (gtimer() - t0 > 2000000000ull) return false;
-    }
-}
+// wait for phase `phase` of a barrier, at most the unit's limit (kasync_wait_ns, default 2 s)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase) { return kasync::mbar_wait(bar, phase); }
 
 __device__ __forceinline__ void tma_load4(void *dst, const CUtensorMap *tm, int c0, int c1, int c2, int c3,
                                           uint64_t *bar) {
@@ -408,6 +390,9 @@ static PFN_cuTensorMapEncodeTiled_v12000 ztma_encoder() {
     }
     return fn;
 }
+
+// this unit's bounded-wait limit on the current device (KMM_OPT_WAIT_LIMIT_MS)
+int kmm_ztma_set_wait_limit(unsigned long long ns) { return kasync::kasync_set_wait_limit(ns) == cudaSuccess ? 0 : 1; }
 
 void kmm_ztma_release(kmm_ctx *ctx) {
     free(ctx->ztma);

@@ -75,6 +75,10 @@ def lib():
         L.kmm_flowstats.restype = ctypes.c_int
         L.kmm_xyzfft_noalloc.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
         L.kmm_xyzfft_noalloc.restype = ctypes.c_int
+        L.kmm_tracer_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_size_t]
+        L.kmm_tracer_cells.restype = ctypes.c_int
+        L.kmm_wait_selftest.argtypes = [vp, ctypes.c_double]
+        L.kmm_wait_selftest.restype = ctypes.c_int
         for name, sig in _ROUTINES.items():
             f = getattr(L, "kmm_" + name)
             f.argtypes = [vp] + [_CT[c] for c in sig]
@@ -88,7 +92,7 @@ def exported_symbols():
     base = ["kmm_ctx_create", "kmm_ctx_destroy", "kmm_last_error", "kmm_abi_version", "kmm_field_size",
             "kmm_upload", "kmm_download", "kmm_get_stats", "kmm_set_timing", "kmm_get_stage_times",
             "kmm_launch_count", "kmm_event_record", "kmm_event_elapsed", "kmm_xyzfft_noalloc", "kmm_flowstats",
-            "kmm_ensemble_step", "kmm_ensemble_run"]
+            "kmm_ensemble_step", "kmm_ensemble_run", "kmm_tracer_cells", "kmm_wait_selftest"]
     return base + ["kmm_" + n for n in _ROUTINES]
 
 
@@ -206,6 +210,19 @@ class KmmContext:
     def download_ptr(self, f, ptr, nbytes):
         fid = self._id(f)
         self._check(self.L.kmm_download(self.h, fid, ctypes.c_void_p(ptr), nbytes), "kmm_download(%s)" % f)
+
+    def tracer_cells(self):
+        """kmm_tracer_cells: the 1-based interpolation cell (imin, jmin, kmax) of every particle,
+        shape (3, npart) int32, as part_track.f90:560-577 looks it up."""
+        cells = np.zeros(3 * self.npart, np.int32)
+        self._check(self.L.kmm_tracer_cells(self.h, cells.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), cells.size),
+                    "kmm_tracer_cells")
+        return cells.reshape(3, self.npart)
+
+    def wait_selftest(self, limit_ms):
+        """kmm_wait_selftest: status of a bounded wait on a barrier nothing arrives on
+        (KMM_ERR_TIMEOUT expected)."""
+        return int(self.L.kmm_wait_selftest(self.h, float(limit_ms)))
 
     def flowstats(self):
         """(prof[7][nyp], scal[4]) of kmm_flowstats: umean, urms, vrms, wrms, R12, T12, ke profiles;

@@ -372,3 +372,55 @@ def test_flowstats_laminar_poiseuille(oracle_mod):
     assert abs(scal[0] - trap) < 1e-14 and abs(scal[0] - 1.0) < 5e-3
     assert abs(scal[1] + 3.0 / p.re) < 1e-12 and abs(scal[2] - 3.0 / p.re) < 1e-12
     assert abs(scal[3] - 0.6) < 5e-3
+
+
+def test_constant_flow_rate_recovers_poiseuille_gradient(oracle_mod):
+    """Constant flow rate (flow_rate > 0, a variant the reference does not have) on the laminar
+    Poiseuille profile with the wrong constant dPdx (twice the balance): each step's correction
+    makes the driving gradient exactly the Poiseuille value -3/re (u'' = -3 for u = 1.5 (1 - y^2)),
+    the profile stays steady and the trapezoid bulk velocity stays at its target."""
+    re = 1400.0
+    p0 = kc.cfg_small(16, 32, 12, re=re)
+    o0 = oracle_mod.Oracle(p0)
+    kc.load_initial(o0, p0, kc.initial_fields(p0, amp=0.0))
+    assert o0.initial() == 0
+    target = o0.flowstats()[1][0]          # the laminar profile's own trapezoid bulk velocity (~1)
+    p = kc.cfg_small(16, 32, 12, re=re, r_tau=math.sqrt(6.0 / re) * re, flow_rate=target)
+    o = oracle_mod.Oracle(p)
+    kc.load_initial(o, p, kc.initial_fields(p0, amp=0.0))     # the U_b = 1 profile of the balanced case
+    assert o.initial() == 0
+    assert abs(o.dpdx() + 6.0 / re) < 1e-15
+    u0 = o.get("U0")
+    for _ in range(5):
+        assert o.step() == 0
+        assert abs(o.stats().dpdx + 3.0 / re) < 1e-9 * 3.0 / re   # delta from a 2e-5 change of Q ~ 1
+    np.testing.assert_allclose(o.get("U0"), u0, atol=1e-12)
+    assert abs(o.flowstats()[1][0] - target) < 1e-13
+    # without the constraint the wrong gradient accelerates the flow
+    q = kc.cfg_small(16, 32, 12, re=re, r_tau=math.sqrt(6.0 / re) * re)
+    o2 = oracle_mod.Oracle(q)
+    kc.load_initial(o2, q, kc.initial_fields(p0, amp=0.0))
+    assert o2.initial() == 0 and o2.run(5) == 0
+    assert o2.flowstats()[1][0] > target + 1e-3 * 5 * q.dt
+    assert o2.stats().dpdx == o2.dpdx()
+
+
+def test_tracer_cells_follow_fluid_interp_lookup(oracle_mod):
+    """orc_tracer_cells is fluid_interp's lookup (part_track.f90:560-577): x, z cells by floor on
+    the 3/2 grid with periodic wrap, y cell from the Chebyshev angle acos(2 y / yl)."""
+    p = kc.cfg_small(16, 32, 12, npart=6, ap=1e-3)
+    o = oracle_mod.Oracle(p)
+    mx, mz = 3 * p.nx // 2, 3 * p.nz // 2
+    dx, dz = p.xl / mx, p.zl / mz
+    x = np.array([0.0, 0.5 * dx, 1.5 * dx, p.xl - 0.25 * dx, -0.5 * dx, 3.2])
+    z = np.array([0.0, 0.5 * dz, 2.5 * dz, p.zl - 0.1 * dz, -0.5 * dz, 1.1])
+    y = np.array([0.999, 0.5, 0.0, -0.5, -0.999, 0.123])
+    for n, a in (("XPART", x), ("YPART", y), ("ZPART", z)):
+        o.set(n, a)
+    c = o.tracer_cells()
+    np.testing.assert_array_equal(c[0], (np.floor(x / dx).astype(int) % mx) + 1)
+    np.testing.assert_array_equal(c[1], (np.floor(z / dz).astype(int) % mz) + 1)
+    kmax = np.floor(1 + p.ny / np.pi * np.arccos(2 * y / p.yl)).astype(int)
+    np.testing.assert_array_equal(c[2], kmax)
+    ycoord = np.cos(np.pi * np.arange(p.ny + 1) / p.ny)
+    assert np.all(ycoord[kmax - 1] >= y) and np.all(ycoord[kmax] <= y)   # y lies in [y(kmin), y(kmax)]
