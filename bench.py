@@ -246,6 +246,8 @@ def run_kmm(a, rank, world, local_rank):
     ctx = runtime.KmmContext(p, device=local_rank)
     if a.ztma is not None:
         ctx.call("set_option", 4, a.ztma)
+    if a.tc_dct is not None:
+        ctx.call("set_option", 7, a.tc_dct)
     load(ctx, f, extra, ctx.upload)
     ctx.initial()
     for _ in range(a.warmup):
@@ -363,6 +365,8 @@ def run_kmm(a, rank, world, local_rank):
             result["ensemble"] = ensemble_report(a, local_rank)
         if a.config == "cfg2" and not a.no_polymer and world == 1:
             result["polymer"] = polymer_report(a, local_rank)
+        if a.config == "cfg2" and not a.no_cfg5 and world == 1:
+            result["cfg5"] = cfg5_report(a, local_rank)
         if not a.no_cpu_baseline and world == 1:
             result["cpu_baseline"] = cpu_baseline(a.config, a.cpu_steps, one_thread_steps=2)
     ctx.close()
@@ -485,6 +489,62 @@ def polymer_report(a, local_rank):
             "mixed": {"value": round(1e3 / ms[1], 3), "unit": "timesteps/s", "ms_per_step": round(ms[1], 4),
                       "speedup_vs_fp64": round(ms[0] / ms[1], 3)},
             "mixed_rel_err_vs_fp64": errs, "long_run": stopped or "both forms ran 1000 steps", "cpu_baseline": cpu}
+
+
+def cfg5_report(a, local_rank, nsteps=5):
+    """The large single run (384 x 257 x 384, Re_tau = 395, polymer + scalar + IB cylinder + 1 M RK3
+    tracers) in FP64 on the routine path: steps/s, device memory held, and size-independent checks
+    after the timed steps (continuity of the spectral velocity, finite CFL, tracer cells in range).
+    The mixed form has no compiled FP32 transforms at these lengths (KMM_ERR_UNSUPPORTED)."""
+    import torch
+    from polymer_dns_b200 import abi, configs, runtime
+    torch.cuda.set_device(local_rank)
+    p, init, desc = configs.make("cfg5", 0)
+    f, extra = configs.build_inputs(p, init, "cfg5")
+    free0, total = torch.cuda.mem_get_info()
+    c = runtime.KmmContext(p, device=local_rank)
+    out = {"workload": desc, "grid": [p.nx, p.ny + 1, p.nz], "npart": p.npart}
+    try:
+        configs.load(f, extra, c.upload)
+        del f, extra
+        st = c.call("initial", allow=(abi.ERR_CFL, abi.ERR_NOMEM, abi.ERR_UNSUPPORTED))
+        if st:
+            out["status"] = abi.STATUS_NAMES.get(st, st) + ": " + c.error()
+            return out
+        for _ in range(2):
+            st = c.call("step", allow=(abi.ERR_CFL, abi.ERR_NAN, abi.ERR_NOMEM))
+            if st:
+                out["status"] = abi.STATUS_NAMES.get(st, st) + " in warm-up: " + c.error()
+                return out
+        c.call("sync")
+        free1, _ = torch.cuda.mem_get_info()
+        c.event_record(0)
+        sts = [c.call("step", allow=(abi.ERR_CFL, abi.ERR_NAN)) for _ in range(nsteps)]
+        c.event_record(1)
+        ms = c.event_elapsed(0, 1) / nsteps
+        c.call("veloc")
+        u, w = c.download("U"), c.download("W")
+        c.call("cderiv", "V", "WRKC")
+        dv = c.download("WRKC")
+        kx = np.arange(p.nx // 2) * 2 * math.pi / p.xl
+        kz = np.fft.fftfreq(p.nz, 1.0 / p.nz) * 2 * math.pi / p.zl
+        div = 1j * kx[None, None, :] * u + dv + 1j * kz[None, :, None] * w
+        cells = c.tracer_cells()
+        out.update({"fp64": {"value": round(1e3 / ms, 3), "unit": "timesteps/s", "ms_per_step": round(ms, 3),
+                             "grid_point_steps_per_s": round(1e3 / ms * p.nx * (p.ny + 1) * p.nz, 1),
+                             "fused_model_bytes_per_step": fused_model_bytes(p),
+                             "frac_of_hbm": round(fused_model_bytes(p) / (ms / 1e3) / 1e9 /
+                                                  float(load_peaks()[0].get("hbm_gbs", 6650.0)), 4),
+                             "steps": nsteps, "status": [abi.STATUS_NAMES.get(x, x) for x in sts]},
+                    "device_memory_gb": round((free0 - free1) / 1e9, 2), "device_total_gb": round(total / 1e9, 1),
+                    "checks": {"max_divergence_rel": float("%.3e" % (np.abs(div).max() / np.abs(u).max())),
+                               "cflmax": round(c.stats().cflmax, 5),
+                               "tracer_cells_in_range": bool(cells.min() >= 1)},
+                    "mixed": "KMM_ERR_UNSUPPORTED: no compiled FP32 transforms at mx = mz = 576, 2 ny = 512",
+                    "status": "ok"})
+    finally:
+        c.close()
+    return out
 
 
 ENSEMBLE_GRIDS = [(64, 64, 64)] * 4 + [(96, 96, 96)] * 4 + [(128, 128, 96)] * 4 + [(128, 128, 128)] * 4
@@ -619,15 +679,18 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kmm", choices=["kmm", "reference"])
-    ap.add_argument("--config", default="cfg2", choices=["cfg1", "cfg2", "cfg3"])
+    ap.add_argument("--config", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg5"])
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--cpu-steps", type=int, default=5, help="timed oracle steps after the 10 untimed ones")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision speed / error report")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 16-member ensemble measurement")
     ap.add_argument("--no-polymer", action="store_true", help="skip the polymer + IB (FP64 / mixed) measurement")
+    ap.add_argument("--no-cfg5", action="store_true", help="skip the 384x257x384 polymer + IB + 1M tracer run")
     ap.add_argument("--ztma", type=int, default=None, choices=[0, 1],
                     help="inverse z transform with TMA tile copies (1, the library default) or plain loads (0)")
+    ap.add_argument("--tc-dct", type=int, default=None, choices=[0, 1],
+                    help="mixed routine path: y transforms on the tensor cores (1) or as FP32 FFTs (0)")
     ap.add_argument("--grid", type=int, default=None,
                     help="run the cfg2 / cfg3 workload at N x (N+1) x N instead of 128 x 129 x 128 (profiling)")
     a = ap.parse_args()

@@ -308,10 +308,17 @@ enum kmm_option {
     KMM_OPT_ZTMA = 4,          /* 1 (default): the fused step's z transforms (FP64 and mixed) move their
                            tiles with TMA (tensor-map bulk copies, mz = 48, 96, 144, 192); 0:
                            plain loads and stores                                            */
-    KMM_OPT_WAIT_LIMIT_MS = 5  /* limit of every device-side wait on an mbarrier (bulk / TMA copies), in
+    KMM_OPT_WAIT_LIMIT_MS = 5, /* limit of every device-side wait on an mbarrier (bulk / TMA copies), in
                            milliseconds, 100 .. 60000 (default 2000).  A wait that runs out records
                            KMM_ERR_TIMEOUT in the step status.  The limit is per device and
                            process-wide (every context on the device shares it).            */
+    KMM_OPT_XBIG = 6,          /* 0 (default): the routine path's FP64 x stage keeps a row of every input
+                           field in shared memory, and passes through an HBM buffer of the physical
+                           inputs only where that does not fit (long 3/2 grids with polymer); 1:
+                           always the two-pass form (same transforms and pointwise terms)    */
+    KMM_OPT_TC_DCT = 7         /* the routine path's mixed form (precision = 1): 1 runs its y (Chebyshev)
+                           transforms as 3xTF32 GEMMs of the cosine matrix on the tcgen05 tensor
+                           cores (ny = 32, 64, 96, 128); 0 as FP32 FFTs of the even extension */
 };
 int  kmm_set_option(kmm_ctx *ctx, int option, int value);
 

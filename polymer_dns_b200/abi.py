@@ -9,7 +9,7 @@ import ctypes
 KMM_ABI_VERSION = 1
 
 # options (enum kmm_option)
-OPT_FUSED, OPT_COLUMN_BLOCKED, OPT_GRAPH, OPT_ZTMA, OPT_WAIT_LIMIT_MS = 1, 2, 3, 4, 5
+OPT_FUSED, OPT_COLUMN_BLOCKED, OPT_GRAPH, OPT_ZTMA, OPT_WAIT_LIMIT_MS, OPT_XBIG, OPT_TC_DCT = 1, 2, 3, 4, 5, 6, 7
 
 # status codes (enum kmm_status)
 OK, ERR_ARG, ERR_CUDA, ERR_CFL, ERR_NAN, ERR_INTERP, ERR_TIMEOUT, ERR_NOMEM, ERR_UNSUPPORTED, ERR_PCFL = range(10)
@@ -138,7 +138,7 @@ def field_shape(fid, nx, ny, nz, npart=0):
 def default_params(**kw):
     """Reference defaults for a plain channel (flow_select = 1, theta = 0.5), overridable by keyword."""
     p = KmmParams()
-    base = dict(nsteps=1, iprnfrq=1000, dt=0.01, gain=400.0, ugain=40.0, theta=0.5,
+    base = dict(nsteps=1, iprnfrq=1000, dt=0.01, gain=50.0, ugain=50.0, theta=0.5,
                 ny=32, nz=32, nx=32, bftail=0, yl=2.0, zl=6.283185307179586, xl=12.566370614359172,
                 re=1400.0, xstart=0.0, uinf=0.0, kwall=0, perturbtime=0, r_tau=64.80740698407860,
                 gravity=0.0, irstrt=0, crstrt=0, print3d=0, geomtype=0, particle_flag=0, flow_select=1,

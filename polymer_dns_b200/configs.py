@@ -16,9 +16,14 @@
 
 Unit mapping to the reference's dns.config values (main_dns.f90:934-1068):
   - re = 1 / nu with the half-height h = 1 (yl = 2); dPdx = -(Re_tau / re)^2 (init_flow.f90:117).
-  - Goldstein alpha, beta -> gain = -alpha, ugain = -beta: the reference's drag is
-    -ugain u - gain sum(u) (solvers.f90:2996-3001, the integral a plain running sum), so negative
-    alpha, beta (damping) are positive gain, ugain.
+  - Goldstein alpha, beta -> gain = -alpha dt, ugain = -beta.  The feedback force is
+    f = alpha int_0^t u dt' + beta u; the reference accumulates the integral as a plain running sum
+    fxintg += u (no dt) and applies drag = -ugain u - gain fxintg (solvers.f90:2996-3001), so
+    int u dt' = dt fxintg gives gain = -alpha dt (= 2 at dt = 0.005) and ugain = -beta (= 40).
+    Reading gain = -alpha = 400 instead makes the feedback loop of the explicit (AB2) step unstable:
+    the amplification factor of u_(n+1) = u_n + dt (3/2 f_n - 1/2 f_(n-1)), f_n = -ugain u_n -
+    gain S_n, S_n = S_(n-1) + u_n, has modulus 1.59 at dt = 0.005 (0.92 with gain = 2), and the
+    128 x 129 x 128 run leaves CFL 1 within four steps.
   - FENE-P: zlmax = L = 30, qbeta = beta, tpoly = Wi (code time units), ipeter = 1 (FENE-P), and
     diffpoly such that the conformation diffusivity 1 / (re diffpoly) is the stated 1e-3.
   - The cylinder's solid y-planes lie above the reference's spreading limit kmaxsurf (an x index,
@@ -51,8 +56,8 @@ def make(name, precision=0, grid=None, **overrides):
                   precision=precision)
         desc = "Re_tau=180 channel 128x129x128, scalar (Sc=1, uniform source, Dirichlet walls), 100k RK3 tracers"
         if name == "cfg3":
-            kw.update(polymer_on=1, zlmax=30.0, tpoly=20.0, qbeta=0.9, diffpoly=1.0 / (re * 1e-3), gain=400.0,
-                      ugain=40.0, ib_spread_all=1)
+            kw.update(polymer_on=1, zlmax=30.0, tpoly=20.0, qbeta=0.9, diffpoly=1.0 / (re * 1e-3),
+                      gain=400.0 * kw["dt"], ugain=40.0, ib_spread_all=1)
             desc += (", FENE-P (Wi=20, beta=0.9, L^2=900, diffusivity 1e-3), Goldstein IB (alpha=-400, beta=-40) on a "
                      "cylinder r=0.25 at (pi,0)")
         if grid:
@@ -64,7 +69,7 @@ def make(name, precision=0, grid=None, **overrides):
         re = 10 ** (math.log10(r_tau / 0.09) / 0.88) / 2.0   # Dean: Re_tau = 0.09 Re_b^0.88; re = Re_b / 2
         kw = dict(nx=384, ny=256, nz=384, dt=0.002, re=re, r_tau=r_tau, xl=2 * math.pi, zl=math.pi,
                   scalar_on=1, diff=1.0, scalar_bc=1, scalar_q=1.0, npart=1000000, ap=1e-3, tracer_scheme=1,
-                  polymer_on=1, zlmax=30.0, tpoly=20.0, qbeta=0.9, diffpoly=1.0 / (re * 1e-3), gain=400.0,
+                  polymer_on=1, zlmax=30.0, tpoly=20.0, qbeta=0.9, diffpoly=1.0 / (re * 1e-3), gain=400.0 * 0.002,
                   ugain=40.0, ib_spread_all=1, precision=precision)
         init = dict(profile="loglaw", amp=0.1, kmax=8, seed=3)
         desc = ("Re_tau=395 channel 384x257x384, scalar, 1M RK3 tracers, FENE-P (Wi=20, beta=0.9, L^2=900), "

@@ -293,6 +293,8 @@ extern "C" int kmm_ctx_create(const kmm_params *p, int device, kmm_ctx **out) {
     CK(cudaMalloc(&c->d_cfl, sizeof(double) * (size_t)c->nyp));
     CK(cudaMalloc(&c->d_umax, sizeof(double) * (size_t)c->nyp));
     CK(cudaMalloc(&c->d_status, sizeof(int)));
+    CK(cudaMalloc(&c->d_tcstat, sizeof(int)));
+    CK(cudaMemset(c->d_tcstat, 0, sizeof(int)));
     CK(cudaMalloc(&c->d_pumax, sizeof(double)));
     CK(cudaMemset(c->d_pumax, 0, sizeof(double)));
     CK(cudaMalloc(&c->d_scratch, sizeof(double) * 9 * KMM_MAX_NYP));
@@ -337,12 +339,13 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
     if (ctx->po) cudaFree(ctx->po);
     if (ctx->drag) cudaFree(ctx->drag);
     if (ctx->d_frate) cudaFree(ctx->d_frate);
+    if (ctx->xbig) cudaFree(ctx->xbig);
     for (int f = 0; f < KMM_MAXF; ++f)
         if (ctx->f[f]) cudaFree(ctx->f[f]);
     for (int w = 0; w < 6; ++w)
         if (ctx->wrk[w]) cudaFree(ctx->wrk[w]);
     void *ptrs[] = {ctx->d_wavx, ctx->d_wavz, ctx->d_c, ctx->d_ycoord, ctx->d_seght, ctx->d_fspread, ctx->d_cfl,
-                    ctx->d_umax, ctx->d_status, ctx->d_pumax, ctx->d_scratch, ctx->pl_in, ctx->pl_out, ctx->q_in, ctx->q_out, ctx->scsource};
+                    ctx->d_umax, ctx->d_status, ctx->d_tcstat, ctx->d_pumax, ctx->d_scratch, ctx->pl_in, ctx->pl_out, ctx->q_in, ctx->q_out, ctx->scsource};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i)
         if (ptrs[i]) cudaFree(ptrs[i]);
     for (int s = 0; s < 5; ++s)
@@ -466,6 +469,8 @@ extern "C" int kmm_set_option(kmm_ctx *ctx, int option, int value) {
     case KMM_OPT_COLUMN_BLOCKED: ctx->use_colblk = value ? 1 : 0; kmm_graph_release(ctx); return KMM_OK;
     case KMM_OPT_GRAPH: ctx->use_graph = value ? 1 : 0; kmm_graph_release(ctx); return KMM_OK;
     case KMM_OPT_ZTMA: ctx->use_ztma = value ? 1 : 0; kmm_graph_release(ctx); return KMM_OK;
+    case KMM_OPT_XBIG: ctx->force_xbig = value ? 1 : 0; return KMM_OK;
+    case KMM_OPT_TC_DCT: ctx->use_tcdct = value ? 1 : 0; return KMM_OK;
     case KMM_OPT_WAIT_LIMIT_MS: {
         if (value < 100 || value > 60000) {
             kmm_set_error(ctx, "wait limit %d ms outside 100 .. 60000", value);

@@ -96,6 +96,11 @@ struct kmm_ctx {
     struct KmmFused *fused;
     double *po, *drag;
     size_t po_n, drag_n;
+    double *xbig;     // physical inputs of the two-pass x stage (3/2 grids past the shared-memory rows)
+    size_t xbig_n;
+    int force_xbig;   // KMM_OPT_XBIG
+    int use_tcdct;    // KMM_OPT_TC_DCT: the mixed routine path's y transforms on the tensor cores
+    int *d_tcstat;    // device status word of the tensor-core transforms (KMM_ERR_TIMEOUT)
     int use_fused;
     int use_colblk;   // fused step: blocked-layout column kernels where compiled (default 1)
     // fused step replayed from CUDA graphs (one per parity of the swapped history buffers)
@@ -145,7 +150,8 @@ static inline double *REAL(kmm_ctx *ctx, int f) { return (double *)kmm_field_ptr
 // the pinned status word after the cfl and umax rows of h_pin, and the flow-rate correction after it
 static inline int *kmm_h_pin_status(kmm_ctx *ctx) { return (int *)(ctx->h_pin + 2 * KMM_MAX_NYP); }
 static inline double *kmm_h_pin_delta(kmm_ctx *ctx) { return ctx->h_pin + 2 * KMM_MAX_NYP + 1; }
-#define KMM_H_PIN_DOUBLES (2 * KMM_MAX_NYP + 2)
+static inline int *kmm_h_pin_tcstat(kmm_ctx *ctx) { return (int *)(ctx->h_pin + 2 * KMM_MAX_NYP + 2); }
+#define KMM_H_PIN_DOUBLES (2 * KMM_MAX_NYP + 3)
 
 // internal entry points shared between translation units
 int kmm_internal_cderiv(kmm_ctx *ctx, const double2 *f, double2 *df);
@@ -193,6 +199,10 @@ int kmm_ensure_plane_buffers(kmm_ctx *ctx, int nin, int nout);
 int kmm_phys_layout(kmm_ctx *ctx, int field, void *dev, const void *host_src, void *host_dst);
 int kmm_internal_polynl(kmm_ctx *ctx, double2 *const *nl);
 int kmm_internal_phirhs(kmm_ctx *ctx, double2 *V, const double2 *F, const double2 *FM, double var);
+// the y transforms of nf fields (dir 0: FP64 columns -> FP32 planes; 1: FP32 planes -> FP64
+// columns) as 3xTF32 tcgen05 GEMMs (kmm_tcdct.cu); KMM_ERR_UNSUPPORTED where they do not apply
+#define KMM_TC_MAXF 64
+int kmm_tc_dct(kmm_ctx *ctx, int dir, const void *const *in, void *const *out, int nf);
 // constant flow rate (kmm_params.flow_rate > 0): tables built once by kmm_initial, the correction
 // after every u0 solve (kmm_column.cu)
 int kmm_flowrate_setup(kmm_ctx *ctx);

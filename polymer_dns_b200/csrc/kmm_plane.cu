@@ -489,6 +489,85 @@ __global__ void __launch_bounds__(256) k_xphys(const double2 *__restrict__ q, do
     }
 }
 
+// 3''. the x stage for 3/2 grids too long for a row of every input field to fit in shared memory
+// (k_xphys needs nin x 2 rows x mx doubles: 507 KB for the 55 polymer inputs at mx = 576).  Two
+// passes through HBM: k_xinv_big takes the Hermitian c2r of one field pair for XZB rows with the
+// runtime block FFT (the same transform as k_xphys) into a physical buffer [f][y][z][x]; k_xpoint
+// evaluates the same pointwise terms (xphys_point) with one thread per 3/2-grid point, every block
+// inside one y-plane for the CFL / |u| reductions.
+__global__ void __launch_bounds__(256) k_xinv_big(const double2 *__restrict__ q, double *__restrict__ pb, DevPlan P,
+                                                  int nin, int nyp, int mz, int mx, int nxh) {
+    extern __shared__ double2 sm[];
+    const int y = blockIdx.y, f = 2 * blockIdx.z, g = f + 1 < nin ? f + 1 : -1;
+    const int z0 = blockIdx.x * XZB, nzr = min(XZB, mz - z0), hx = mx / 2;
+    double2 *fa = sm, *fb = sm + (size_t)XZB * mx;
+    const size_t nphys = (size_t)nyp * mz * mx;
+    for (int e = threadIdx.x; e < XZB * mx; e += blockDim.x) {
+        const int r = e / mx, k = e - r * mx;
+        double2 v = make_double2(0.0, 0.0);
+        if (r < nzr) {
+            const int z = z0 + r;
+            const int kk = k <= hx ? k : mx - k;
+            double2 A_ = make_double2(0.0, 0.0), B_ = make_double2(0.0, 0.0);
+            if (kk < nxh) {
+                A_ = q[(((size_t)f * nyp + y) * mz + z) * nxh + kk];
+                if (g >= 0) B_ = q[(((size_t)g * nyp + y) * mz + z) * nxh + kk];
+            }
+            if (k == 0 || k == hx) { A_.y = 0.0; B_.y = 0.0; }
+            if (k <= hx) v = make_double2(A_.x - B_.y, A_.y + B_.x);
+            else v = make_double2(A_.x + B_.y, -A_.y + B_.x);
+        }
+        fa[e] = v;
+    }
+    __syncthreads();
+    double2 *r = fft_smem(P, fa, fb, XZB, mx, +1);
+    for (int e = threadIdx.x; e < nzr * mx; e += blockDim.x) {
+        const int rr = e / mx, k = e - rr * mx;
+        const size_t g3 = ((size_t)y * mz + z0 + rr) * mx + k;
+        pb[(size_t)f * nphys + g3] = r[e].x;
+        if (g >= 0) pb[(size_t)g * nphys + g3] = r[e].y;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_xpoint(const double *__restrict__ pb, double *__restrict__ po,
+                                                double *__restrict__ drag, double *__restrict__ up3,
+                                                double *__restrict__ vp3, double *__restrict__ wp3,
+                                                const int *__restrict__ imatrix, double *__restrict__ fxi,
+                                                double *__restrict__ fyi, double *__restrict__ fzi,
+                                                const double *__restrict__ scsource, const double *__restrict__ seght,
+                                                double *__restrict__ cfl, double *__restrict__ umax, PhysArgs A,
+                                                Save3D sv, int nyp, int mz, int mx) {
+    const int y = blockIdx.y;
+    const size_t nplane = (size_t)mz * mx, nphys = (size_t)nyp * nplane;
+    double cmax = 0.0, umx = 0.0;
+    const double sg = seght[y];
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nplane; e += (size_t)gridDim.x * blockDim.x) {
+        const int z = (int)(e / mx), k = (int)(e - (size_t)z * mx);
+        const size_t g3 = (size_t)y * nplane + e;
+        auto in = [&](int sl) { return pb[(size_t)A.slot_of_in[sl] * nphys + g3]; };
+        xphys_point(in, A, sv, y, z, k, nyp, mz, mx, sg, po, drag, up3, vp3, wp3, imatrix, fxi, fyi, fzi, scsource, cmax,
+                    umx);
+    }
+    __shared__ double red[2][32];
+    for (int off = 16; off; off >>= 1) {
+        double c2 = __shfl_down_sync(0xffffffffu, cmax, off);
+        double u2 = __shfl_down_sync(0xffffffffu, umx, off);
+        cmax = (c2 != c2) ? c2 : fmax(cmax, c2);
+        umx = fmax(umx, u2);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { red[0][w] = cmax; red[1][w] = umx; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q2 = 1; q2 < (int)(blockDim.x >> 5); ++q2) {
+            cmax = (red[0][q2] != red[0][q2]) ? red[0][q2] : fmax(cmax, red[0][q2]);
+            umx = fmax(umx, red[1][q2]);
+        }
+        atomic_max_pos(&cfl[y], cmax);
+        atomic_max_pos(&umax[y], umx);
+    }
+}
+
 // 3'. the same x stage for the compiled lengths MX = 48, 96, 144, 192 (nx = 32 .. 128): one block
 // per (y, z) row, XPW warps.  Each warp takes field pairs in turn: the Hermitian extension of
 // A + iB (modes nxh .. mx - nxh not carried; c2r ignores Im of the DC mode) through the
@@ -939,6 +1018,23 @@ static int ensure_phys(kmm_ctx *ctx, int nout, bool need_drag) {
     return KMM_OK;
 }
 
+// physical input buffer of the two-pass x stage: nin fields of (nyp, mz, mx) doubles
+static int ensure_xbig(kmm_ctx *ctx, int nin) {
+    const size_t n = ctx->nphys * (size_t)nin;
+    if (n > ctx->xbig_n) {
+        if (ctx->xbig) { CK(cudaStreamSynchronize(ctx->stream)); cudaFree(ctx->xbig); }
+        ctx->xbig = NULL;
+        ctx->xbig_n = 0;
+        if (cudaMalloc(&ctx->xbig, sizeof(double) * n) != cudaSuccess) {
+            cudaGetLastError();
+            kmm_set_error(ctx, "two-pass x stage: cudaMalloc(%zu) failed", sizeof(double) * n);
+            return KMM_ERR_NOMEM;
+        }
+        ctx->xbig_n = n;
+    }
+    return KMM_OK;
+}
+
 __global__ void k_kmaxsurf(const int *__restrict__ im, int *out, int nyp, int mz, int mx) {
     const size_t n = (size_t)nyp * mz * mx;
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
@@ -1153,7 +1249,16 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     RET(kmm_smem_attr(ctx, (const void *)k_dct_bwd<float2>, sm_dct));
     RET(kmm_smem_attr(ctx, (const void *)k_zfft_bwd<float2>, sm_z));
     RET(kmm_smem_attr(ctx, (const void *)k_zfft_fwd<float2>, sm_z));
-    RET(kmm_smem_attr(ctx, (const void *)k_xphys, sm_x));
+    // rows of every input field in shared memory (k_xphys) unless that exceeds the 227 KB limit:
+    // then the two-pass x stage through an HBM buffer of the physical inputs (k_xinv_big, k_xpoint)
+    const bool mx_compiled = mx == 48 || mx == 96 || mx == 144 || mx == 192;
+    const bool xbig = (!mx_compiled && sm_x + 1024 > 227 * 1024) || (ctx->force_xbig && ctx->p.precision == 0);
+    if (xbig) {
+        RET(ensure_xbig(ctx, nin));
+        RET(kmm_smem_attr(ctx, (const void *)k_xinv_big, sm_xf));
+    } else {
+        RET(kmm_smem_attr(ctx, (const void *)k_xphys, sm_x));
+    }
     RET(kmm_smem_attr(ctx, (const void *)k_xfwd, sm_xf));
     CK(cudaMemsetAsync(ctx->d_cfl, 0, sizeof(double) * nyp, ctx->stream));
     CK(cudaMemsetAsync(ctx->d_umax, 0, sizeof(double) * nyp, ctx->stream));
@@ -1167,7 +1272,22 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     float2 *pl_out32 = (float2 *)ctx->pl_out, *q_out32 = (float2 *)ctx->q_out;
     float *po32 = (float *)ctx->po;
     kmm_tic(ctx);
-    {
+    // the tensor-core y transforms of the mixed form (KMM_OPT_TC_DCT); their status word is read
+    // back with the CFL numbers
+    const bool tcd = f32 && ctx->use_tcdct;
+    if (tcd) CK(cudaMemsetAsync(ctx->d_tcstat, 0, sizeof(int), ctx->stream));
+    int tcf = KMM_ERR_UNSUPPORTED;
+    if (tcd) {
+        const void *pin[MAXIO];
+        void *pout[MAXIO];
+        for (int m = 0; m < nin; ++m) {
+            pin[m] = in.p[m];
+            pout[m] = pl_in32 + (size_t)m * ctx->nspec;
+        }
+        tcf = kmm_tc_dct(ctx, 0, pin, pout, nin);
+        if (tcf != KMM_OK && tcf != KMM_ERR_UNSUPPORTED) return tcf;
+    }
+    if (tcf != KMM_OK) {
         const int dst = f32 ? dct_h_fwd<float2>(ctx, nin, in, pl_in32, tw_y2, nz, nxh, ncols)
                             : dct_h_fwd<double2>(ctx, nin, in, ctx->pl_in, ctx->py2.tw, nz, nxh, ncols);
         if (dst != KMM_ERR_UNSUPPORTED) {
@@ -1223,15 +1343,25 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         if (f32) XP2(MM, float2, q_in32, po32, tw_mx);                                                           \
         else XP2(MM, double2, ctx->q_in, ctx->po, ctx->wmx.tw);                                                  \
     } while (0)
-        switch (mx) {
+        switch (xbig ? 0 : mx) {
         case 48: XP2S(48); break;
         case 96: XP2S(96); break;
         case 144: XP2S(144); break;
         case 192: XP2S(192); break;
         default:
-            k_xphys<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_x, ctx->stream>>>(
-                ctx->q_in, ctx->po, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl,
-                ctx->d_umax, ctx->pmx, A, sv, nyp, mz, mx, nxh);
+            if (!xbig) {
+                k_xphys<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_x, ctx->stream>>>(
+                    ctx->q_in, ctx->po, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght,
+                    ctx->d_cfl, ctx->d_umax, ctx->pmx, A, sv, nyp, mz, mx, nxh);
+            } else {
+                k_xinv_big<<<dim3((mz + XZB - 1) / XZB, nyp, (nin + 1) / 2), 256, sm_xf, ctx->stream>>>(
+                    ctx->q_in, ctx->xbig, ctx->pmx, nin, nyp, mz, mx, nxh);
+                CKL();
+                const int bpp = (int)(((size_t)mz * mx + 255) / 256);
+                k_xpoint<<<dim3(bpp < 64 ? bpp : 64, nyp), 256, 0, ctx->stream>>>(
+                    ctx->xbig, ctx->po, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght,
+                    ctx->d_cfl, ctx->d_umax, A, sv, nyp, mz, mx);
+            }
             break;
         }
 #undef XP2S
@@ -1292,7 +1422,19 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_FWD);
     kmm_tic(ctx);
-    {
+    int tcb = KMM_ERR_UNSUPPORTED;
+    if (tcd) {
+        const void *pin[MAXIO];
+        void *pout[MAXIO];
+        for (int m = 0; m < nout; ++m) {
+            pin[m] = pl_out32 + (size_t)m * ctx->nspec;
+            pout[m] = outp.p[m];
+        }
+        tcb = kmm_tc_dct(ctx, 1, pin, pout, nout);
+        if (tcb != KMM_OK && tcb != KMM_ERR_UNSUPPORTED) return tcb;
+        CK(cudaMemcpyAsync(kmm_h_pin_tcstat(ctx), ctx->d_tcstat, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (tcb != KMM_OK) {
         const int dst = f32 ? dct_h_bwd<float2>(ctx, nout, pl_out32, outp, tw_y2, nz, nxh, ncols)
                             : dct_h_bwd<double2>(ctx, nout, ctx->pl_out, outp, ctx->py2.tw, nz, nxh, ncols);
         if (dst != KMM_ERR_UNSUPPORTED) {
@@ -1331,6 +1473,10 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     ctx->stats.umax = umax;
     if (xstat && *kmm_h_pin_status(ctx) == KMM_ERR_TIMEOUT) {
         kmm_set_error(ctx, "x stage: a bulk copy of the input rows did not complete");
+        st = KMM_ERR_TIMEOUT;
+    }
+    if (tcd && *kmm_h_pin_tcstat(ctx) == KMM_ERR_TIMEOUT) {
+        kmm_set_error(ctx, "tensor-core y transform: an MMA completion wait ran out");
         st = KMM_ERR_TIMEOUT;
     }
     if (st == KMM_OK && nan) st = KMM_ERR_NAN;

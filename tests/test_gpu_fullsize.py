@@ -83,7 +83,7 @@ def test_cfg3_routine_path_matches_oracle(rt, oracle_mod):
     """Polymer + Goldstein IB cylinder + scalar + tracers at 128 x 129 x 128 on the routine path:
     10 steps, with the IB force acting (spread in every plane)."""
     p, g, o = _setup(rt, oracle_mod, "cfg3")
-    assert p.polymer_on == 1 and p.ib_spread_all == 1 and p.gain > 0 and p.ugain > 0
+    assert p.polymer_on == 1 and p.ib_spread_all == 1 and abs(p.gain - 2.0) < 1e-12 and p.ugain == 40.0
     for _ in range(10):
         assert g.step() == 0
         assert o.step() == 0
@@ -168,3 +168,50 @@ def test_bounded_wait_runs_out_and_context_survives(rt, oracle_mod):
     for name in ("V", "OMY", "FN", "GN"):
         _cmp(g, o, name)
     g.close()
+
+
+def test_two_pass_x_stage_matches_shared_memory_form(rt):
+    """The x stage through an HBM buffer of the physical inputs (used where a row of every input
+    field does not fit in shared memory) evaluates the same pointwise terms as the shared-memory
+    form; its c2r is the runtime block FFT instead of the compiled warp FFT, so the states agree
+    to FFT rounding (1e-12 relative) after 3 polymer + IB + scalar steps."""
+    p, init, _ = configs.make("cfg3", grid=32, npart=300)
+    f, extra = configs.build_inputs(p, init, "cfg3")
+    ctxs = []
+    for big in (1, 0):
+        g = rt.KmmContext(p)
+        g.call("set_option", abi.OPT_XBIG, big)
+        configs.load(f, extra, g.upload)
+        assert g.initial() == 0
+        ctxs.append(g)
+    for _ in range(3):
+        for g in ctxs:
+            assert g.step() == 0
+    for name in ("V", "OMY", "FN", "GN", "SCALAR", "C11", "C23", "QP12", "FXINTG", "XPART"):
+        e = kc.rel_err(ctxs[0].download(name), ctxs[1].download(name))
+        assert e <= 1e-12, "%s rel err %.3e" % (name, e)
+    for g in ctxs:
+        g.close()
+
+
+@pytest.mark.parametrize("grid", [(384, 32, 16), (16, 256, 12)])
+def test_cfg5_lengths_match_oracle(rt, oracle_mod, grid):
+    """The transform lengths of the 384 x 257 x 384 workload on small grids the oracle runs in
+    seconds: mx = 576 (the two-pass x stage with 55 polymer inputs) and ny = 256 (2 ny = 512 DCTs,
+    the one-thread-per-column solves), polymer + scalar + IB cylinder + tracers, 3 steps."""
+    nx, ny, nz = grid
+    p, init, _ = configs.make("cfg5", nx=nx, ny=ny, nz=nz, npart=2000, dt=0.002)
+    f, extra = configs.build_inputs(p, init, "cfg5")
+    g = rt.KmmContext(p)
+    o = oracle_mod.Oracle(p)
+    configs.load(f, extra, g.upload)
+    configs.load(f, extra, o.set)
+    assert g.initial() == 0 and o.initial() == 0
+    for _ in range(3):
+        assert g.step() == 0
+        assert o.step() == 0
+    for name in ("V", "OMY", "FN", "GN", "SCALAR", "C11", "C12", "C33", "QP12", "FXINTG", "XPART", "YPART"):
+        _cmp(g, o, name)
+    _cells_identical(g, o, p)
+    g.close()
+    o.close()

@@ -195,7 +195,7 @@ def test_vcw3dp_scalar_polymer_ib(rt, oracle_mod, grid):
     """All 55 input fields through vcw3dp; ny = 48 and 64 take the half-length DCT-I kernels, ny = 24
     the 2 ny-point FFT form."""
     p = kc.cfg_small(*grid, dt=1e-5, scalar_on=1, polymer_on=1, scalar_q=0.3, zlmax=30.0, tpoly=20.0,
-                     qbeta=0.9, gain=400.0, ugain=40.0)
+                     qbeta=0.9, gain=2.0, ugain=40.0)
     g, o = _pair(rt, oracle_mod, p)
     rng = np.random.default_rng(16)
     names = ["U", "V", "W", "OMX", "OMY", "OMZ", "U11", "U12", "U13", "U21", "U22", "U23", "U31", "U32", "U33",
@@ -298,7 +298,7 @@ def test_dropin_scalar_tracers_10_steps(rt, oracle_mod):
 
 def test_dropin_polymer_ib_10_steps(rt, oracle_mod):
     p = kc.cfg_small(32, 32, 32, scalar_on=1, polymer_on=1, diff=1.0, scalar_bc=1, scalar_q=1.0,
-                     zlmax=30.0, tpoly=20.0, qbeta=0.9, diffpoly=1000.0, gain=400.0, ugain=40.0, dt=0.005)
+                     zlmax=30.0, tpoly=20.0, qbeta=0.9, diffpoly=1000.0, gain=2.0, ugain=40.0, dt=0.005)
     fields = kc.initial_fields(p, amp=0.05, seed=1)
     im = inputs.cylinder_imatrix(p.nx, p.ny, p.nz, p.xl, p.yl, xc=math.pi, yc=0.0, radius=0.25)
     g, o = _run_pair(rt, oracle_mod, p, 10, fields, scalar=np.zeros_like(fields[0]), imatrix=im)
@@ -599,7 +599,7 @@ def test_mixed_precision_routine_path_tracks_fp64(rt, variant):
     kw = dict(scalar_on=1, diff=1.0, scalar_bc=1, scalar_q=0.5)
     im = None
     if variant == "polymer_ib":
-        kw.update(polymer_on=1, zlmax=30.0, tpoly=20.0, qbeta=0.9, diffpoly=1000.0, gain=400.0, ugain=40.0,
+        kw.update(polymer_on=1, zlmax=30.0, tpoly=20.0, qbeta=0.9, diffpoly=1000.0, gain=2.0, ugain=40.0,
                   dt=0.005)
     elif variant == "inertial":
         kw.update(particle_flag=1, npart=200, ap=0.002, ratio=2.0, gravity=0.1, cd_switch=2, c_mu=1.0)
@@ -643,7 +643,7 @@ def test_polymer_ib_step_at_compiled_grids(rt, n):
     memory near its largest), in both precisions: every launch succeeds and the mixed form tracks
     the FP64 drop-in within 1e-5 after 2 steps."""
     kw = dict(scalar_on=1, diff=1.0, scalar_bc=1, scalar_q=0.5, polymer_on=1, zlmax=30.0, tpoly=20.0, qbeta=0.9,
-              diffpoly=1000.0, gain=400.0, ugain=40.0, dt=0.005)
+              diffpoly=1000.0, gain=2.0, ugain=40.0, dt=0.005)
     ctxs = []
     for prec in (0, 1):
         p = kc.cfg_small(n, n, n, precision=prec, **kw)
