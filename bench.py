@@ -434,9 +434,11 @@ def mixed_report(a, f, extra, local_rank, fp64_ms):
 
 def polymer_report(a, local_rank):
     """The polymer + immersed-boundary configuration (the Re_tau = 180 case with FENE-P Wi = 20,
-    beta = 0.9, L^2 = 900 and the cylinder IB; routine path): FP64 and mixed-precision steps/s, the
-    mixed form's relative error against FP64 from the same state after 10 and 1000 steps (u, v, w,
-    scalar and the six conformation-tensor components), and the oracle on the host cores."""
+    beta = 0.9, L^2 = 900 and the Goldstein force on the cylinder; routine path): FP64 and
+    mixed-precision steps/s; the mixed form's relative error against FP64 from the same state after
+    10, 100 and 1000 steps (u, v, w, scalar, the six conformation-tensor components, bulk kinetic
+    energy, wall shear) or up to the step where a run stops; the same for the reference's spreading
+    test (cylinder inert) over 1000 steps; the oracle on the host cores."""
     from polymer_dns_b200 import runtime
     p64, init, desc = make_config("cfg3", 0)
     f, extra = build_inputs(p64, init, "cfg3")
@@ -456,39 +458,61 @@ def polymer_report(a, local_rank):
         c.event_record(1)
         ms[prec] = c.event_elapsed(0, 1) / nst
         c.close()
-    ctx = {}
-    for prec in (0, 1):
-        p, _, _ = make_config("cfg3", prec)
-        c = runtime.KmmContext(p, device=local_rank)
-        load(c, f, extra, c.upload)
-        c.initial()
-        ctx[prec] = c
+    from polymer_dns_b200 import abi, configs
     names = {"u": "U", "v": "V", "w": "W", "scalar": "SCALAR", "c11": "C11", "c12": "C12", "c13": "C13",
              "c22": "C22", "c23": "C23", "c33": "C33"}
-    from polymer_dns_b200 import abi
-    errs, done, stopped = {}, 0, None
-    for mark in (10, 100, 1000):
-        sts = [c.call("run", mark - done, allow=(abi.ERR_CFL, abi.ERR_NAN)) for c in ctx.values()]
-        if any(sts):
-            stopped = "a run stopped between steps %d and %d (%s): CFL > 1 or a non-finite value" % (
-                done, mark, ", ".join(abi.STATUS_NAMES.get(x, str(x)) for x in sts))
-            break
-        done = mark
+
+    def accuracy_run(marks, **over):
+        """FP64 and mixed from the same state: relative max-norm errors at each mark, the bulk
+        kinetic energy and wall shear, where a run stopped (if one did) and the largest trace of
+        the conformation tensor seen on the 3/2 grid's spectral means at that point."""
+        ctx = {}
+        for prec in (0, 1):
+            p, _, _ = configs.make("cfg3", prec, **over)
+            c = runtime.KmmContext(p, device=local_rank)
+            load(c, f, extra, c.upload)
+            c.initial()
+            ctx[prec] = c
+        errs, done, stopped = {}, 0, None
+        for mark in marks:
+            for step in range(done + 1, mark + 1):
+                sts = [c.call("step", allow=(abi.ERR_CFL, abi.ERR_NAN)) for c in ctx.values()]
+                if any(sts):
+                    c11 = max(np.abs(c.download("C11")).max() for c in ctx.values())
+                    stopped = ("step %d: %s (CFL %.2f; max |C11| coefficient %.1f against L^2 = %.0f)" % (
+                        step, ", ".join(abi.STATUS_NAMES.get(x, str(x)) for x in sts),
+                        max(c.stats().cflmax for c in ctx.values()), c11, p64.zlmax ** 2))
+                    break
+            if stopped:
+                break
+            done = mark
+            st = {prec: c.flowstats() for prec, c in ctx.items()}   # runs veloc: u, w current
+            e = {}
+            for k, n in names.items():
+                x, y = ctx[1].download(n), ctx[0].download(n)
+                e[k] = float("%.3e" % (np.abs(x - y).max() / max(np.abs(y).max(), 1e-300)))
+            (_, s64), (_, s32) = st[0], st[1]
+            e["bulk_ke"] = float("%.3e" % (abs(s32[3] - s64[3]) / abs(s64[3])))
+            e["wall_shear"] = float("%.3e" % (max(abs(s32[1] - s64[1]), abs(s32[2] - s64[2])) /
+                                              max(abs(s64[1]), abs(s64[2]))))
+            errs[str(mark)] = e
         for c in ctx.values():
-            c.call("veloc")   # u, w from the current v, omega_y (the step keeps them current too)
-        e = {}
-        for k, n in names.items():
-            x, y = ctx[1].download(n), ctx[0].download(n)
-            e[k] = float("%.3e" % (np.abs(x - y).max() / max(np.abs(y).max(), 1e-300)))
-        errs[str(mark)] = e
-    for c in ctx.values():
-        c.close()
+            c.close()
+        return errs, stopped or "both forms ran %d steps" % marks[-1]
+
+    errs, stopped = accuracy_run((10, 100, 1000))
+    # the same workload with the reference's spreading test, under which the cylinder's planes get
+    # no force (kmaxsurf is an x index): the polymer-laden channel itself over 1000 steps
+    errs_ref, stopped_ref = accuracy_run((10, 1000), ib_spread_all=0)
     cpu = cpu_baseline("cfg3", a.cpu_steps, one_thread_steps=1) if not a.no_cpu_baseline else None
     return {"workload": desc, "fp64": {"value": round(1e3 / ms[0], 3), "unit": "timesteps/s",
                                        "ms_per_step": round(ms[0], 4)},
             "mixed": {"value": round(1e3 / ms[1], 3), "unit": "timesteps/s", "ms_per_step": round(ms[1], 4),
                       "speedup_vs_fp64": round(ms[0] / ms[1], 3)},
-            "mixed_rel_err_vs_fp64": errs, "long_run": stopped or "both forms ran 1000 steps", "cpu_baseline": cpu}
+            "mixed_rel_err_vs_fp64": errs, "long_run": stopped,
+            "reference_spreading": {"note": "ib_spread_all = 0: the reference's i <= kmaxsurf test, the cylinder inert",
+                                    "mixed_rel_err_vs_fp64": errs_ref, "long_run": stopped_ref},
+            "cpu_baseline": cpu}
 
 
 def cfg5_report(a, local_rank, nsteps=5):

@@ -345,6 +345,238 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tcdct(TcFields in, TcFieldsW 
     }
 }
 
+__device__ __forceinline__ void mma_tf32_ts(uint32_t d, uint32_t a_tmem, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(d),
+        "r"(a_tmem), "l"(b), "r"(idesc), "r"(acc));
+}
+
+// 8 consecutive 32-bit TMEM columns of this warp's 32 lanes from registers
+__device__ __forceinline__ void tmem_st8(uint32_t ta, const uint32_t *r) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(ta), "r"(r[0]),
+                 "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// The forward transform with the cosine matrix in TMEM and the input tiles staged by bulk copies.
+// TMEM (512 columns): T_hi in columns [0, K), T_lo in [K, 2K) (one row per lane), accumulators at
+// 384 and 448.  Shared memory: two staging buffers holding one tile's 32 raw FP64 columns each
+// (a contiguous 32 (ny+1) x 16-byte range, one cp.async.bulk), the B operand (hi / lo), the signed
+// sums of the ny row.  While tile i is converted and multiplied, tile i + 1 is in flight; the copy
+// of tile i + 2 is issued as soon as tile i's staging buffer has been read.
+template <int NY>
+struct TcFwd2 {
+    static constexpr int NYP = NY + 1, K = TcShape<NY>::K, KG = K / 4, G = (KG + 7) / 8;
+    static constexpr int STG_BYTES = TC_CT * NYP * 16;
+    static constexpr int B_BYTES = TC_N * K * 4, LBO_B = (TC_N / 8) * 128;
+    static constexpr int XN_DOUBLES = 2 * 8 * 32 * 2;
+    static constexpr size_t SMEM = 2 * (size_t)STG_BYTES + 2 * (size_t)B_BYTES + XN_DOUBLES * 8 + 128;
+    static constexpr uint32_t D0 = 384;   // TMEM column of the first accumulator
+};
+
+template <int NY>
+__global__ void __launch_bounds__(TC_THREADS, 1) k_tcdct_fwd2(TcFields in, TcFieldsW out, const double2 *__restrict__ tw2,
+                                                              int nf, int ncols, int *status) {
+    using S = TcFwd2<NY>;
+    constexpr int NYP = S::NYP, K = S::K, KG = S::KG, G = S::G;
+    constexpr uint32_t IDESC = tc_idesc(TC_M, TC_N);
+    extern __shared__ __align__(1024) uint8_t tsm[];
+    uint8_t *stg0 = tsm, *stg1 = tsm + S::STG_BYTES;
+    uint8_t *Bhi = tsm + 2 * S::STG_BYTES, *Blo = Bhi + S::B_BYTES;
+    double *xn = reinterpret_cast<double *>(Blo + S::B_BYTES);
+    uint64_t *tbar = reinterpret_cast<uint64_t *>(xn + S::XN_DOUBLES);   // [2] staging copies
+    uint64_t *mbar = tbar + 2;                                             // [2] MMA commits
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tpf = ncols / TC_CT, ntiles = nf * tpf;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tslot)), "r"(512)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    auto tile_src = [&](int t) -> const void * {
+        const int f = t / tpf, c0 = (t - f * tpf) * TC_CT;
+        return reinterpret_cast<const double2 *>(in.p[f]) + (size_t)c0 * NYP;
+    };
+    bool pend[2] = {false, false};
+    if (tid == 0) {
+        for (int b = 0; b < 2; ++b) {
+            kasync::mbar_init(&tbar[b], 1);
+            kasync::mbar_init(&mbar[b], 1);
+        }
+        kasync::mbar_init_fence();
+        for (int b = 0; b < 2; ++b) {
+            const int t = blockIdx.x + b * gridDim.x;
+            if (t < ntiles) {
+                kasync::mbar_expect_tx(&tbar[b], S::STG_BYTES);
+                kasync::bulk_g2s(b ? stg1 : stg0, tile_src(t), S::STG_BYTES, &tbar[b]);
+                pend[b] = true;
+            }
+        }
+    }
+    for (int e = tid; e < S::B_BYTES / 4; e += TC_THREADS) {
+        reinterpret_cast<uint32_t *>(Bhi)[e] = 0u;
+        reinterpret_cast<uint32_t *>(Blo)[e] = 0u;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    // the cosine matrix into TMEM: warp w writes rows (lanes) 32 w .. 32 w + 31
+    if (warp < 4) {
+        const int m = 32 * warp + lane;
+        const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
+#pragma unroll 1
+        for (int k0 = 0; k0 < K; k0 += 8) {
+            uint32_t h[8], l[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int k = k0 + q;
+                const double v = (m <= NY && k <= NY) ? tw2[(m * k) % (2 * NY)].x : 0.0;
+                split_tf32(v, h[q], l[q]);
+            }
+            tmem_st8(trow + (uint32_t)k0, h);
+            tmem_st8(trow + (uint32_t)(K + k0), l);
+        }
+        tmem_wait_st();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+
+    uint32_t tph[2] = {0u, 0u}, mph[2] = {0u, 0u};
+    bool ok = true;
+    int pf = 0, pc0 = 0;
+    for (int it = 0, t = blockIdx.x;; ++it, t += gridDim.x) {
+        const int s = it & 1;
+        const bool have = t < ntiles && ok;
+        if (it > 0) {   // the previous tile's MMAs: B free, accumulator s ^ 1 ready
+            ok = tc_wait(&mbar[s ^ 1], mph[s ^ 1], status) && ok;
+            tc_fence_after();
+        }
+        if (have) {     // this tile's staging copy
+            const bool got = kasync::mbar_wait(&tbar[s], tph[s]);
+            tph[s] ^= 1u;
+            if (tid == 0) pend[s] = false;
+            if (!got) {
+                if (lane == 0) atomicMax(status, KMM_ERR_TIMEOUT);
+                ok = false;
+            }
+        }
+        if (it > 0 && ok) {   // drain the previous tile's accumulator
+            if (warp < 4) {
+                const uint32_t ta = tmem + S::D0 + (uint32_t)(64 * (s ^ 1)) + ((uint32_t)(32 * warp) << 16);
+                const int m = 32 * warp + lane;
+#pragma unroll 1
+                for (int cb = 0; cb < TC_CT; cb += 16) {
+                    uint32_t r[32];
+                    tmem_ld16(ta + (uint32_t)cb, r);
+                    tmem_ld16(ta + (uint32_t)(32 + cb), r + 16);
+                    tmem_wait_ld();
+                    if (m <= NY) {
+                        float4 *dst = reinterpret_cast<float4 *>(reinterpret_cast<float2 *>(out.p[pf]) +
+                                                                 (size_t)m * ncols + pc0 + cb);
+#pragma unroll
+                        for (int c = 0; c < 16; c += 2)
+                            dst[c / 2] = make_float4(__uint_as_float(r[c]), __uint_as_float(r[16 + c]),
+                                                     __uint_as_float(r[c + 1]), __uint_as_float(r[17 + c]));
+                    }
+                }
+            }
+            if (NY == 128 && warp == 4) {
+                double sre = 0.0, sim = 0.0;
+#pragma unroll
+                for (int w = 0; w < 8; ++w) {
+                    sre += xn[(((s ^ 1) * 8 + w) * 32 + lane) * 2];
+                    sim += xn[(((s ^ 1) * 8 + w) * 32 + lane) * 2 + 1];
+                }
+                reinterpret_cast<float2 *>(out.p[pf])[(size_t)NY * ncols + pc0 + lane] =
+                    make_float2((float)sre, (float)sim);
+            }
+            tc_fence_before();
+        }
+        if (!have || !ok) break;
+        const int f = t / tpf, c0 = (t - f * tpf) * TC_CT;
+        // split the staged tile into B: lane = column, re in row lane, im in row 32 + lane
+        const double2 *st = reinterpret_cast<const double2 *>(s ? stg1 : stg0) + (size_t)lane * NYP;
+        double sre = 0.0, sim = 0.0;
+#pragma unroll
+        for (int gi = 0; gi < G; ++gi) {
+            const int g = warp + 8 * gi;
+            if (g < KG) {
+                uint32_t phr[4], plr[4], phi[4], pli[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int n = 4 * g + q;
+                    const double2 x = n < NYP ? st[n] : make_double2(0.0, 0.0);
+                    split_tf32(x.x, phr[q], plr[q]);
+                    split_tf32(x.y, phi[q], pli[q]);
+                    if (NY == 128 && n <= NY) {
+                        const double wgt = (n & 1) ? -1.0 : 1.0;
+                        sre += wgt * x.x;
+                        sim += wgt * x.y;
+                    }
+                }
+                const uint32_t ore = kmaj_off(lane, 4 * g, TC_N), oim = kmaj_off(32 + lane, 4 * g, TC_N);
+                *reinterpret_cast<uint4 *>(Bhi + ore) = make_uint4(phr[0], phr[1], phr[2], phr[3]);
+                *reinterpret_cast<uint4 *>(Blo + ore) = make_uint4(plr[0], plr[1], plr[2], plr[3]);
+                *reinterpret_cast<uint4 *>(Bhi + oim) = make_uint4(phi[0], phi[1], phi[2], phi[3]);
+                *reinterpret_cast<uint4 *>(Blo + oim) = make_uint4(pli[0], pli[1], pli[2], pli[3]);
+            }
+        }
+        if (NY == 128) {
+            xn[((s * 8 + warp) * 32 + lane) * 2] = sre;
+            xn[((s * 8 + warp) * 32 + lane) * 2 + 1] = sim;
+        }
+        proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            // staging buffer s has been read: the copy of the tile two ahead goes into it
+            const int tn = t + 2 * gridDim.x;
+            if (tn < ntiles) {
+                kasync::mbar_expect_tx(&tbar[s], S::STG_BYTES);
+                kasync::bulk_g2s(s ? stg1 : stg0, tile_src(tn), S::STG_BYTES, &tbar[s]);
+                pend[s] = true;
+            }
+            const uint32_t d = tmem + S::D0 + (uint32_t)(64 * s);
+            const uint32_t bh = su32(Bhi), bl = su32(Blo);
+            uint32_t acc = 0u;
+#pragma unroll 1
+            for (int pass = 0; pass < 3; ++pass) {   // T_lo P_hi, T_hi P_lo, T_hi P_hi
+                const uint32_t acol = pass == 0 ? (uint32_t)K : 0u, b0 = pass == 1 ? bl : bh;
+#pragma unroll 1
+                for (int ks = 0; ks < K / 8; ++ks) {
+                    mma_tf32_ts(d, tmem + acol + (uint32_t)(8 * ks), sdesc(b0 + (uint32_t)(2 * ks * S::LBO_B), S::LBO_B, 128),
+                                IDESC, acc);
+                    acc = 1u;
+                }
+            }
+            mma_commit(&mbar[s]);
+        }
+        pf = f;
+        pc0 = c0;
+    }
+    // after a timeout: wait (bounded) for the MMAs and copies that may still be in flight
+    if (!ok && tid == 0) {
+        kasync::mbar_wait(&mbar[0], mph[0]);
+        kasync::mbar_wait(&mbar[1], mph[1]);
+        for (int b = 0; b < 2; ++b)
+            if (pend[b]) kasync::mbar_wait(&tbar[b], tph[b]);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+    }
+}
+
 }  // namespace
 
 // the y transforms of nf fields as tcgen05 GEMMs; KMM_ERR_UNSUPPORTED where they do not apply
@@ -373,14 +605,23 @@ int kmm_tc_dct(kmm_ctx *ctx, int dir, const void *const *in, void *const *out, i
         CKL();                                                                                               \
         return KMM_OK;                                                                                       \
     } while (0)
+#define TF(NN)                                                                                               \
+    do {                                                                                                     \
+        const size_t sm = TcFwd2<NN>::SMEM;                                                                  \
+        RET(kmm_smem_attr(ctx, (const void *)k_tcdct_fwd2<NN>, sm));                                        \
+        k_tcdct_fwd2<NN><<<grid, TC_THREADS, sm, ctx->stream>>>(fi, fo, tw, nf, ncols, ctx->d_tcstat);      \
+        CKL();                                                                                               \
+        return KMM_OK;                                                                                       \
+    } while (0)
     if (dir == 0) {
         switch (ny) {
-        case 32: TC(32, 0);
-        case 64: TC(64, 0);
-        case 96: TC(96, 0);
-        default: TC(128, 0);
+        case 32: TF(32);
+        case 64: TF(64);
+        case 96: TF(96);
+        default: TF(128);
         }
     }
+#undef TF
     switch (ny) {
     case 32: TC(32, 1);
     case 64: TC(64, 1);

@@ -73,16 +73,25 @@ __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.a
 // (16-byte chunk index XOR bits 7-8 of the byte offset)
 __device__ __forceinline__ int ztile_idx(int kz, int y) { return kz * ZTM_YT + (y ^ ((kz >> 1) & 3)); }
 
+// The base-field tiles pass through a ring of ZB_SLOTS shared-memory slots: the q fields are formed
+// in the order ZB_ORDER (each needs at most two base fields live), every base field is loaded into
+// slot ZB_SLOT[f] -- fields 0, 2, 3 at the start, then ZB_AFTER[k] once step k has read the slot's
+// previous tile -- so a CTA holds 3 tiles instead of 8 and three CTAs share an SM.
+#define ZB_SLOTS 3
+__device__ __forceinline__ int zb_order(int k) { return k == 1 ? 2 : k == 2 ? 4 : k == 3 ? 1 : k == 4 ? 3 : k == 7 ? 8 : k == 8 ? 7 : k; }
+__device__ __forceinline__ int zb_slot(int f) { return (f == 0 || f == 1 || f == 7) ? 0 : (f == 2 || f == 5 || f == 6) ? 1 : 2; }
+__device__ __forceinline__ int zb_after(int k) { return k == 0 ? 1 : k == 1 ? 5 : k == 2 ? 4 : k == 4 ? 6 : k == 5 ? 7 : -1; }
+
 template <int MZ>
-__global__ void __launch_bounds__(ZTM_WARPS * 32, 2)
+__global__ void __launch_bounds__(ZTM_WARPS * 32, 3)
     k_zb_tma(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout,
              const double *__restrict__ wavx, const double *__restrict__ wavz, const double2 *__restrict__ tw,
              int nbase, int nq, int *status) {
     constexpr int NZ = 2 * MZ / 3, NZH = NZ / 2, TILE = NZ * ZTM_YT;
     extern __shared__ unsigned char zsm_raw[];
-    // 1024-byte aligned base: tiles [nbase][NZ][YT], FFT scratch [warps][2][MZ], stage [YT][MZ], barriers
+    // 1024-byte aligned base: tiles [ZB_SLOTS][NZ][YT], FFT scratch [warps][2][MZ], stage [YT][MZ], barriers
     double2 *tiles = reinterpret_cast<double2 *>((reinterpret_cast<uintptr_t>(zsm_raw) + 1023) & ~(uintptr_t)1023);
-    double2 *scr = tiles + (size_t)nbase * TILE;
+    double2 *scr = tiles + (size_t)ZB_SLOTS * TILE;
     double2 *stage = scr + (size_t)ZTM_WARPS * 2 * MZ;
     uint64_t *bar = reinterpret_cast<uint64_t *>(stage + (size_t)ZTM_YT * MZ);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -92,11 +101,17 @@ __global__ void __launch_bounds__(ZTM_WARPS * 32, 2)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    unsigned issued = 0;   // base fields whose tile load has been issued (thread 0)
+    auto load = [&](int f) {
+        if (f < 0 || f >= nbase) return;
+        mbar_expect_tx(&bar[f], (unsigned)(TILE * sizeof(double2)));
+        tma_load4(tiles + (size_t)zb_slot(f) * TILE, &tin, 2 * y0, 0, kx, f, &bar[f]);
+        issued |= 1u << f;
+    };
     if (threadIdx.x == 0) {
-        for (int f = 0; f < nbase; ++f) {
-            mbar_expect_tx(&bar[f], (unsigned)(TILE * sizeof(double2)));
-            tma_load4(tiles + (size_t)f * TILE, &tin, 2 * y0, 0, kx, f, &bar[f]);
-        }
+        load(0);
+        load(2);
+        load(3);
     }
     const double kxv = wavx[kx];
     const int y = warp;
@@ -109,7 +124,8 @@ __global__ void __launch_bounds__(ZTM_WARPS * 32, 2)
             ready |= 1u << f;
         }
     };
-    for (int g = 0; g < nq; ++g) {
+    for (int k = 0; k < nq; ++k) {
+        const int g = zb_order(k);
         // base fields of q field g (u v w wx wy wz cx cy cz)
         int f0, f1 = -1;
         switch (g) {
@@ -122,7 +138,7 @@ __global__ void __launch_bounds__(ZTM_WARPS * 32, 2)
         }
         need(f0);
         if (f1 >= 0) need(f1);
-        const double2 *t0 = tiles + (size_t)f0 * TILE, *t1 = f1 >= 0 ? tiles + (size_t)f1 * TILE : t0;
+        const double2 *t0 = tiles + (size_t)zb_slot(f0) * TILE, *t1 = f1 >= 0 ? tiles + (size_t)zb_slot(f1) * TILE : t0;
         for (int z = lane; z < MZ; z += 32) {
             double2 val = make_double2(0.0, 0.0);
             if (z < NZH || z >= MZ - NZH) {
@@ -154,11 +170,20 @@ __global__ void __launch_bounds__(ZTM_WARPS * 32, 2)
         if (threadIdx.x == 0) tma_store_wait_read();   // the previous field's store has read the stage
         __syncthreads();
         for (int z = lane; z < MZ; z += 32) stage[(size_t)y * MZ + z] = r[swz<double2>(z)];
-        fence_async_smem();
+        fence_async_smem();   // also orders this step's tile reads before the next load into the slot
         __syncthreads();
-        if (threadIdx.x == 0) tma_store4(&tout, 2 * kx, 0, y0, g, stage);
+        if (threadIdx.x == 0) {
+            tma_store4(&tout, 2 * kx, 0, y0, g, stage);
+            load(zb_after(k));
+        }
     }
-    if (threadIdx.x == 0) tma_store_wait_read();   // shared memory must outlive the last store's read
+    if (threadIdx.x == 0) {
+        tma_store_wait_read();   // shared memory must outlive the last store's read
+        // after a timeout, wait (bounded) for any tile load still in flight before the CTA exits
+        if (!ok)
+            for (int f = 0; f < nbase; ++f)
+                if (((issued >> f) & 1u) && !((ready >> f) & 1u)) mbar_wait(&bar[f], 0);
+    }
     if (!ok && lane == 0) atomicMax(status, KMM_ERR_TIMEOUT);
 }
 
@@ -167,16 +192,19 @@ __global__ void __launch_bounds__(ZTM_WARPS * 32, 2)
 // layout Yo[o][kx][kz][y].  One CTA per (kx, 4 consecutive y): one TMA load per field (box 1 kx x
 // mz z x 4 y, rows of 16 B), one warp per y column, and a TMA store per field of the [kz][4 y]
 // result tile (64 B rows, 64-byte swizzle: the layout of the inverse transform's input tiles).
+// The output tiles pass through two shared-memory slots: fields 0 and 1 are loaded at the start,
+// field o + 2 into slot o mod 2 once field o has been read, so three CTAs share an SM.
+#define ZF_SLOTS 2
 template <int MZ>
-__global__ void __launch_bounds__(ZTM_WARPS * 32, 2)
+__global__ void __launch_bounds__(ZTM_WARPS * 32, 3)
     k_zf_tma(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout,
              const double2 *__restrict__ tw, int nout, double scale, int *status) {
     constexpr int NZ = 2 * MZ / 3, NZH = NZ / 2, TIN = MZ * ZTM_YT, TOUT = NZ * ZTM_YT;
     extern __shared__ unsigned char zsm_raw[];
-    // 1024-byte aligned: out stage [NZ][YT] (swizzled), in tiles [nout][YT][MZ], scratch, barriers
+    // 1024-byte aligned: out stage [NZ][YT] (swizzled), in tiles [ZF_SLOTS][YT][MZ], scratch, barriers
     double2 *stage = reinterpret_cast<double2 *>((reinterpret_cast<uintptr_t>(zsm_raw) + 1023) & ~(uintptr_t)1023);
     double2 *tiles = stage + TOUT;
-    double2 *scr = tiles + (size_t)nout * TIN;
+    double2 *scr = tiles + (size_t)ZF_SLOTS * TIN;
     uint64_t *bar = reinterpret_cast<uint64_t *>(scr + (size_t)ZTM_WARPS * 2 * MZ);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int kx = blockIdx.x, y0 = blockIdx.y * ZTM_YT;
@@ -185,18 +213,24 @@ __global__ void __launch_bounds__(ZTM_WARPS * 32, 2)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    unsigned issued = 0, ready = 0;
+    auto load = [&](int o) {
+        if (o >= nout) return;
+        mbar_expect_tx(&bar[o], (unsigned)(TIN * sizeof(double2)));
+        tma_load4(tiles + (size_t)(o % ZF_SLOTS) * TIN, &tin, 2 * kx, 0, y0, o, &bar[o]);
+        issued |= 1u << o;
+    };
     if (threadIdx.x == 0) {
-        for (int o = 0; o < nout; ++o) {
-            mbar_expect_tx(&bar[o], (unsigned)(TIN * sizeof(double2)));
-            tma_load4(tiles + (size_t)o * TIN, &tin, 2 * kx, 0, y0, o, &bar[o]);
-        }
+        load(0);
+        load(1);
     }
     const int y = warp;
     double2 *a = scr + (size_t)warp * 2 * MZ, *b = a + MZ;
     bool ok = true;
     for (int o = 0; o < nout; ++o) {
         ok = mbar_wait(&bar[o], 0) && ok;
-        const double2 *t = tiles + (size_t)o * TIN + (size_t)y * MZ;
+        ready |= 1u << o;
+        const double2 *t = tiles + (size_t)(o % ZF_SLOTS) * TIN + (size_t)y * MZ;
         for (int z = lane; z < MZ; z += 32) a[swz<double2>(z)] = ok ? t[z] : make_double2(0.0, 0.0);
         __syncwarp();
         const double2 *r = fft_warp_ct<double2, MZ, -1, 1, true>(a, b, tw);
@@ -206,11 +240,19 @@ __global__ void __launch_bounds__(ZTM_WARPS * 32, 2)
             const double2 v = r[swz<double2>(kz < NZH ? kz : (MZ - NZ) + kz)];
             stage[ztile_idx(kz, y)] = make_double2(v.x / scale, v.y / scale);   // the reference's /(mx mz)
         }
-        fence_async_smem();
+        fence_async_smem();   // also orders this field's tile reads before the next load into the slot
         __syncthreads();
-        if (threadIdx.x == 0) tma_store4(&tout, 2 * y0, 0, kx, o, stage);
+        if (threadIdx.x == 0) {
+            tma_store4(&tout, 2 * y0, 0, kx, o, stage);
+            load(o + ZF_SLOTS);
+        }
     }
-    if (threadIdx.x == 0) tma_store_wait_read();
+    if (threadIdx.x == 0) {
+        tma_store_wait_read();
+        if (!ok)
+            for (int o = 0; o < nout; ++o)
+                if (((issued >> o) & 1u) && !((ready >> o) & 1u)) mbar_wait(&bar[o], 0);
+    }
     if (!ok && lane == 0) atomicMax(status, KMM_ERR_TIMEOUT);
 }
 
@@ -481,7 +523,7 @@ int kmm_zb_tma(kmm_ctx *ctx, const double2 *yp, double2 *q, int nbase, int nq, c
     ZtmaMaps *M = ztma_maps(ctx);
     if (!M) return KMM_ERR_NOMEM;
     RET(pair_encode(ctx, M->inv, true, yp, q, nbase, nq, false));
-    const size_t smem = 1024 + sizeof(double2) * ((size_t)nbase * nz * ZTM_YT + (size_t)ZTM_WARPS * 2 * mz +
+    const size_t smem = 1024 + sizeof(double2) * ((size_t)ZB_SLOTS * nz * ZTM_YT + (size_t)ZTM_WARPS * 2 * mz +
                                                   (size_t)ZTM_YT * mz) + 8 * sizeof(uint64_t);
     const dim3 grid(nxh, (nyp + ZTM_YT - 1) / ZTM_YT);
 #define ZTM_LAUNCH(MM)                                                                                           \
@@ -506,7 +548,7 @@ int kmm_zf_tma(kmm_ctx *ctx, const double2 *r, double2 *yo, int nout, const doub
     ZtmaMaps *M = ztma_maps(ctx);
     if (!M) return KMM_ERR_NOMEM;
     RET(pair_encode(ctx, M->fwd, false, r, yo, nout, nout, false));
-    const size_t smem = 1024 + sizeof(double2) * ((size_t)nz * ZTM_YT + (size_t)nout * mz * ZTM_YT +
+    const size_t smem = 1024 + sizeof(double2) * ((size_t)nz * ZTM_YT + (size_t)ZF_SLOTS * mz * ZTM_YT +
                                                   (size_t)ZTM_WARPS * 2 * mz) + 8 * sizeof(uint64_t);
     const dim3 grid(nxh, (nyp + ZTM_YT - 1) / ZTM_YT);
     const double scale = (double)ctx->mx * (double)mz;
