@@ -604,10 +604,17 @@ def ensemble_report(a, local_rank):
         x, y, z = inputs.uniform_particles(p.npart, p.xl, p.yl, p.zl, p.ap, init["seed"])
         extra.update(XPART=x, YPART=y, ZPART=z)
         member_inputs.append((f, extra))
+    from polymer_dns_b200 import autotune
     for prec in (0, 1):
         ctxs, model = [], 0
+        tuned = {}
         for (p, init), (f, extra) in zip(ensemble_members(prec), member_inputs):
+            # the runtime variants of each member shape, picked by timing them once per shape
+            best, timings = autotune.tune(runtime, p, lambda cc, f=f, extra=extra: load(cc, f, extra, cc.upload),
+                                          device=local_rank)
+            tuned["%dx%dx%d" % (p.nx, p.ny + 1, p.nz)] = {"chosen": autotune.describe(best), "ms_per_step": timings}
             c = runtime.KmmContext(p, device=local_rank)
+            autotune.apply(c, best)
             load(c, f, extra, c.upload)
             c.initial()
             ctxs.append(c)
@@ -628,6 +635,7 @@ def ensemble_report(a, local_rank):
             "grid_point_steps_per_s": round(pts * 1e3 / ms, 1),
             "fused_model_bytes_per_ensemble_step": model,
             "frac_of_hbm": round(model / (ms / 1e3) / 1e9 / peak, 4),
+            "autotune": tuned,
             "status": "ok" if all(s == 0 for s in st) else "member status %s" % st}
         for c in ctxs:
             c.close()

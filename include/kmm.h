@@ -316,9 +316,18 @@ enum kmm_option {
                            field in shared memory, and passes through an HBM buffer of the physical
                            inputs only where that does not fit (long 3/2 grids with polymer); 1:
                            always the two-pass form (same transforms and pointwise terms)    */
-    KMM_OPT_TC_DCT = 7         /* the routine path's mixed form (precision = 1): 1 runs its y (Chebyshev)
+    KMM_OPT_TC_DCT = 7,        /* the routine path's mixed form (precision = 1): 1 runs its y (Chebyshev)
                            transforms as 3xTF32 GEMMs of the cosine matrix on the tcgen05 tensor
-                           cores (ny = 32, 64, 96, 128); 0 as FP32 FFTs of the even extension */
+                           cores (ny = 32, 64, 96, 128); 0 (default) as FP32 FFTs of the even
+                           extension                                                          */
+    KMM_OPT_DERIVED_INPUTS = 8 /* 1 (default): inside the routine step, vcw3dp forms the x and z derivatives
+                           of its inputs (i kx, i kz times the y-transformed field, in the z
+                           inverse) instead of transforming them as separate spectral fields,
+                           and the step computes only the y derivatives; 0: every input
+                           materialised (gradv, gradscl, derivscji) as in the reference.  Off
+                           with inertial particles, which read the gradient on the 3/2 grid.
+                           The U11 .. DC333 mirrors then hold only their y-derivative members
+                           after a step (kmm_gradv / kmm_derivscji recompute them)          */
 };
 int  kmm_set_option(kmm_ctx *ctx, int option, int value);
 

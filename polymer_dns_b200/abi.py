@@ -9,7 +9,8 @@ import ctypes
 KMM_ABI_VERSION = 1
 
 # options (enum kmm_option)
-OPT_FUSED, OPT_COLUMN_BLOCKED, OPT_GRAPH, OPT_ZTMA, OPT_WAIT_LIMIT_MS, OPT_XBIG, OPT_TC_DCT = 1, 2, 3, 4, 5, 6, 7
+OPT_FUSED, OPT_COLUMN_BLOCKED, OPT_GRAPH, OPT_ZTMA, OPT_WAIT_LIMIT_MS, OPT_XBIG, OPT_TC_DCT, OPT_DERIVED_INPUTS = (
+    1, 2, 3, 4, 5, 6, 7, 8)
 
 # status codes (enum kmm_status)
 OK, ERR_ARG, ERR_CUDA, ERR_CFL, ERR_NAN, ERR_INTERP, ERR_TIMEOUT, ERR_NOMEM, ERR_UNSUPPORTED, ERR_PCFL = range(10)

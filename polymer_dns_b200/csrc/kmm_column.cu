@@ -1324,7 +1324,7 @@ extern "C" int kmm_nonlin(kmm_ctx *ctx) {
 // reference's formulas; exp of an argument evaluated identically on every call)
 struct PtrList16 { double2 *p[16]; };
 
-__global__ void k_filter(PtrList16 ptrs, int nptr, size_t n, int nyp, int nz, int nzh, int ny) {
+__global__ void k_filter(const __grid_constant__ PtrList16 ptrs, int nptr, size_t n, int nyp, int nz, int nzh, int ny) {
     GRID_LOOP(n) {
         DECOMP();
         const int j1 = j + 1;

@@ -278,6 +278,7 @@ extern "C" int kmm_ctx_create(const kmm_params *p, int device, kmm_ctx **out) {
     c->use_colblk = 1;
     c->use_graph = 1;
     c->use_ztma = 1;
+    c->use_derived = 1;
 #define DUP(dst, src, n)                                                        \
     do {                                                                        \
         CK(cudaMalloc(&(dst), sizeof(double) * (size_t)(n)));                   \
@@ -471,6 +472,7 @@ extern "C" int kmm_set_option(kmm_ctx *ctx, int option, int value) {
     case KMM_OPT_ZTMA: ctx->use_ztma = value ? 1 : 0; kmm_graph_release(ctx); return KMM_OK;
     case KMM_OPT_XBIG: ctx->force_xbig = value ? 1 : 0; return KMM_OK;
     case KMM_OPT_TC_DCT: ctx->use_tcdct = value ? 1 : 0; return KMM_OK;
+    case KMM_OPT_DERIVED_INPUTS: ctx->use_derived = value ? 1 : 0; return KMM_OK;
     case KMM_OPT_WAIT_LIMIT_MS: {
         if (value < 100 || value > 60000) {
             kmm_set_error(ctx, "wait limit %d ms outside 100 .. 60000", value);

@@ -29,7 +29,7 @@ template <int E, int MX>
 __global__ void __launch_bounds__(FX_WARPS * 32, 3) k_fx(const double2 *__restrict__ q, double2 *__restrict__ r,
                                                       double *__restrict__ up3, double *__restrict__ vp3,
                                                       double *__restrict__ wp3, const double *__restrict__ seght,
-                                                      double *__restrict__ cfl, double *__restrict__ umax, DevPlan P,
+                                                      double *__restrict__ cfl, double *__restrict__ umax, const __grid_constant__ DevPlan P,
                                                       FxArgs A, int nyp, int mz, int mx_rt, int nxh) {
     extern __shared__ double2 sm[];
     const int mx = MX > 0 ? MX : mx_rt;

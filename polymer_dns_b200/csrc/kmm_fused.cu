@@ -367,7 +367,7 @@ __device__ __forceinline__ void col_dct(Col<E> &x, double2 *a, double2 *b, const
 
 // L0 > 0: 2 ny is the compile-time constant L0 (specialised DCT); L0 = 0: runtime plan
 template <int E, int L0>
-__global__ void __launch_bounds__(64) k_col_fwd(ColFwdArgs A, FusedTabs T, DevPlan P) {
+__global__ void __launch_bounds__(64) k_col_fwd(ColFwdArgs A, FusedTabs T, const __grid_constant__ DevPlan P) {
     extern __shared__ double2 sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nyp = A.nyp, ny = nyp - 1, L = 2 * ny;
@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(64) k_col_fwd(ColFwdArgs A, FusedTabs T, DevPl
 template <int MZ>
 __global__ void __launch_bounds__(ZT_WARPS * 32) k_zb(const double2 *__restrict__ yp, double2 *__restrict__ q,
                                                       const double *__restrict__ wavx, const double *__restrict__ wavz,
-                                                      DevPlan P, int nout, int nyp, int nz, int nxh, int mz_rt) {
+                                                      const __grid_constant__ DevPlan P, int nout, int nyp, int nz, int nxh, int mz_rt) {
     const int mz = MZ > 0 ? MZ : mz_rt;
     extern __shared__ double2 sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -643,7 +643,7 @@ __global__ void __launch_bounds__(ZT_WARPS * 32) k_zb(const double2 *__restrict_
 
 // y-physical outputs [o][ncols][nyp] from R[o][y][z][kx]
 template <int MZ>
-__global__ void __launch_bounds__(ZT_WARPS * 32) k_zf(const double2 *__restrict__ r, double2 *__restrict__ yo, DevPlan P,
+__global__ void __launch_bounds__(ZT_WARPS * 32) k_zf(const double2 *__restrict__ r, double2 *__restrict__ yo, const __grid_constant__ DevPlan P,
                                                       int nout, int nyp, int nz, int nxh, int mz_rt, double scale) {
     const int mz = MZ > 0 ? MZ : mz_rt;
     extern __shared__ double2 sm[];
@@ -824,7 +824,7 @@ __global__ void __launch_bounds__(ZT_WARPS * 32) k_zf2(const C *__restrict__ r, 
 // ---------------------------------------------------------------------------
 
 template <int E, int L0>
-__global__ void __launch_bounds__(64) k_col_bwd(ColBwdArgs A, DevPlan P) {
+__global__ void __launch_bounds__(64) k_col_bwd(ColBwdArgs A, const __grid_constant__ DevPlan P) {
     extern __shared__ double2 sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nyp = A.nyp, ny = nyp - 1, L = 2 * ny;

@@ -100,6 +100,7 @@ struct kmm_ctx {
     size_t xbig_n;
     int force_xbig;   // KMM_OPT_XBIG
     int use_tcdct;    // KMM_OPT_TC_DCT: the mixed routine path's y transforms on the tensor cores
+    int use_derived;  // KMM_OPT_DERIVED_INPUTS: vcw3dp forms the x / z derivative inputs itself
     int *d_tcstat;    // device status word of the tensor-core transforms (KMM_ERR_TIMEOUT)
     int use_fused;
     int use_colblk;   // fused step: blocked-layout column kernels where compiled (default 1)
@@ -203,6 +204,7 @@ int kmm_internal_phirhs(kmm_ctx *ctx, double2 *V, const double2 *F, const double
 // columns) as 3xTF32 tcgen05 GEMMs (kmm_tcdct.cu); KMM_ERR_UNSUPPORTED where they do not apply
 #define KMM_TC_MAXF 64
 int kmm_tc_dct(kmm_ctx *ctx, int dir, const void *const *in, void *const *out, int nf);
+bool kmm_derived_inputs(const kmm_ctx *ctx);
 // constant flow rate (kmm_params.flow_rate > 0): tables built once by kmm_initial, the correction
 // after every u0 solve (kmm_column.cu)
 int kmm_flowrate_setup(kmm_ctx *ctx);

@@ -89,7 +89,7 @@ __device__ C *fft_block(const DevPlan &P, C *a, C *b, const C *tw, int n) {
 #define DCT_CB 8
 #define LDG 4   // global loads per thread issued together in the transforms' staging loops
 template <typename C>
-__global__ void __launch_bounds__(256) k_dct_fwd(FieldPtrs in, C *__restrict__ pl, DevPlan P, const C *__restrict__ tw,
+__global__ void __launch_bounds__(256) k_dct_fwd(const __grid_constant__ FieldPtrs in, C *__restrict__ pl, const __grid_constant__ DevPlan P, const C *__restrict__ tw,
                                                  int nyp, int nz, int nxh, int ncols) {
     typedef typename kct::Real<C>::T T;
     extern __shared__ double2 smd[];
@@ -206,7 +206,7 @@ __device__ __forceinline__ void dct1_half(C *x, C *a, C *b, const C *__restrict_
 // block's 8 columns staged in shared memory (column stride N + 1, odd: the transposing store
 // reads 8 columns at one y without bank conflicts)
 template <typename C, int N>
-__global__ void __launch_bounds__(256) k_dct_fwd_h(FieldPtrs in, C *__restrict__ pl, const C *__restrict__ tw, int nz,
+__global__ void __launch_bounds__(256) k_dct_fwd_h(const __grid_constant__ FieldPtrs in, C *__restrict__ pl, const C *__restrict__ tw, int nz,
                                                    int nxh, int ncols) {
     typedef typename kct::Real<C>::T T;
     constexpr int NYP = N + 1;
@@ -248,13 +248,22 @@ __global__ void __launch_bounds__(256) k_dct_fwd_h(FieldPtrs in, C *__restrict__
 // 2. z: zero-pad + inverse c2c (FFTW_BACKWARD)
 // ---------------------------------------------------------------------------
 #define ZKB 8   // kx columns per block of the z transforms (one sequence per warp; 4 blocks per SM)
+// where each output field of the z inverse comes from: plane base[f] of the y-transformed inputs,
+// multiplied by 1 (mult 0), i kx (1) or i kz (2) -- the x and z derivatives of a field formed here
+// instead of as separate spectral fields with their own y transforms
+struct ZRecipe {
+    unsigned char base[MAXIO], mult[MAXIO];
+};
+
 template <typename C>
-__global__ void __launch_bounds__(256, 4) k_zfft_bwd(const C *__restrict__ pl, C *__restrict__ q, DevPlan P,
-                                                  const C *__restrict__ tw, int nyp, int nz, int nxh, int mz) {
+__global__ void __launch_bounds__(256, 4) k_zfft_bwd(const C *__restrict__ pl, C *__restrict__ q, const __grid_constant__ DevPlan P,
+                                                  const C *__restrict__ tw, int nyp, int nz, int nxh, int mz,
+                                                  const __grid_constant__ ZRecipe R, const double *__restrict__ wavx,
+                                                  const double *__restrict__ wavz) {
     typedef typename kct::Real<C>::T T;
     extern __shared__ double2 smd[];
     C *sm = reinterpret_cast<C *>(smd);
-    const int y = blockIdx.y, f = blockIdx.z;
+    const int y = blockIdx.y, f = blockIdx.z, fb = R.base[f], mult = R.mult[f];
     const int kx0 = blockIdx.x * ZKB;
     const int nk = min(ZKB, nxh - kx0);
     const int nzh = nz / 2;
@@ -262,7 +271,7 @@ __global__ void __launch_bounds__(256, 4) k_zfft_bwd(const C *__restrict__ pl, C
     const bool ct = fb_compiled(mz);
     for (int e = threadIdx.x; e < fb_len(ZKB, mz); e += blockDim.x) a[e] = kct::mk<C>((T)0, (T)0);
     __syncthreads();
-    const C *src = pl + (((size_t)f * nyp + y) * nxh + kx0) * nz;
+    const C *src = pl + (((size_t)fb * nyp + y) * nxh + kx0) * nz;
     for (int e0 = threadIdx.x; e0 < nk * nz; e0 += LDG * 256) {
         C wv[LDG];
 #pragma unroll
@@ -274,7 +283,12 @@ __global__ void __launch_bounds__(256, 4) k_zfft_bwd(const C *__restrict__ pl, C
             if (e >= nk * nz) break;
             const int c = e / nz, j = e - c * nz;
             const int jj = (j < nzh) ? j : (mz - nz) + j;
-            a[fb_at<C, ZKB>(c, jj, mz, ct)] = wv[u];
+            C v = wv[u];
+            if (mult) {   // i k v
+                const T k = (T)(mult == 1 ? wavx[kx0 + c] : wavz[j]);
+                v = kct::mk<C>(-k * v.y, k * v.x);
+            }
+            a[fb_at<C, ZKB>(c, jj, mz, ct)] = v;
         }
     }
     __syncthreads();
@@ -419,7 +433,7 @@ __global__ void __launch_bounds__(256) k_xphys(const double2 *__restrict__ q, do
                                                const int *__restrict__ imatrix, double *__restrict__ fxi,
                                                double *__restrict__ fyi, double *__restrict__ fzi,
                                                const double *__restrict__ scsource, const double *__restrict__ seght,
-                                               double *__restrict__ cfl, double *__restrict__ umax, DevPlan P,
+                                               double *__restrict__ cfl, double *__restrict__ umax, const __grid_constant__ DevPlan P,
                                                PhysArgs A, Save3D sv, int nyp, int mz, int mx, int nxh) {
     extern __shared__ double2 sm[];
     const int y = blockIdx.y;
@@ -495,7 +509,7 @@ __global__ void __launch_bounds__(256) k_xphys(const double2 *__restrict__ q, do
 // runtime block FFT (the same transform as k_xphys) into a physical buffer [f][y][z][x]; k_xpoint
 // evaluates the same pointwise terms (xphys_point) with one thread per 3/2-grid point, every block
 // inside one y-plane for the CFL / |u| reductions.
-__global__ void __launch_bounds__(256) k_xinv_big(const double2 *__restrict__ q, double *__restrict__ pb, DevPlan P,
+__global__ void __launch_bounds__(256) k_xinv_big(const double2 *__restrict__ q, double *__restrict__ pb, const __grid_constant__ DevPlan P,
                                                   int nin, int nyp, int mz, int mx, int nxh) {
     extern __shared__ double2 sm[];
     const int y = blockIdx.y, f = 2 * blockIdx.z, g = f + 1 < nin ? f + 1 : -1;
@@ -775,7 +789,7 @@ __global__ void k_spread(PO_T *__restrict__ po, const double *__restrict__ drag,
 // ---------------------------------------------------------------------------
 // 5. x: r2c (two real rows per complex FFT), keep kx < nxh
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_xfwd(const double *__restrict__ po, double2 *__restrict__ q, DevPlan P,
+__global__ void __launch_bounds__(256) k_xfwd(const double *__restrict__ po, double2 *__restrict__ q, const __grid_constant__ DevPlan P,
                                               int nout, int nyp, int mz, int mx, int nxh) {
     extern __shared__ double2 sm[];
     const int y = blockIdx.y;
@@ -817,7 +831,7 @@ __global__ void __launch_bounds__(256) k_xfwd(const double *__restrict__ po, dou
 // 6. z: forward c2c, truncate to nz, /(mx*mz)
 // ---------------------------------------------------------------------------
 template <typename C>
-__global__ void __launch_bounds__(256, 4) k_zfft_fwd(const C *__restrict__ q, C *__restrict__ pl, DevPlan P,
+__global__ void __launch_bounds__(256, 4) k_zfft_fwd(const C *__restrict__ q, C *__restrict__ pl, const __grid_constant__ DevPlan P,
                                                   const C *__restrict__ tw, int nyp, int nz, int nxh, int mz,
                                                   double scale) {
     typedef typename kct::Real<C>::T T;
@@ -861,7 +875,7 @@ __global__ void __launch_bounds__(256, 4) k_zfft_fwd(const C *__restrict__ q, C 
 // 7. y: DCT-I back to Chebyshev coefficients, /ny, halve the end coefficients
 // ---------------------------------------------------------------------------
 template <typename C>
-__global__ void __launch_bounds__(256) k_dct_bwd(const C *__restrict__ pl, FieldPtrsW out, DevPlan P,
+__global__ void __launch_bounds__(256) k_dct_bwd(const C *__restrict__ pl, const __grid_constant__ FieldPtrsW out, const __grid_constant__ DevPlan P,
                                                  const C *__restrict__ tw, int nyp, int nz, int nxh, int ncols) {
     typedef typename kct::Real<C>::T T;
     extern __shared__ double2 smd[];
@@ -909,7 +923,7 @@ __global__ void __launch_bounds__(256) k_dct_bwd(const C *__restrict__ pl, Field
 
 // k_dct_bwd for ny in {48, 64, 96, 128} with the half-length DCT-I (layout as k_dct_fwd_h)
 template <typename C, int N>
-__global__ void __launch_bounds__(256) k_dct_bwd_h(const C *__restrict__ pl, FieldPtrsW out, const C *__restrict__ tw,
+__global__ void __launch_bounds__(256) k_dct_bwd_h(const C *__restrict__ pl, const __grid_constant__ FieldPtrsW out, const C *__restrict__ tw,
                                                    int nz, int nxh, int ncols) {
     constexpr int NYP = N + 1;
     extern __shared__ double2 smd[];
@@ -1131,17 +1145,36 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     memset(&A, 0, sizeof(A));
     for (int s = 0; s < S_NSLOT; ++s) A.slot_of_in[s] = -1;
     for (int o = 0; o < O_NSLOT; ++o) A.slot_of_out[o] = -1;
-    FieldPtrs in;
+    FieldPtrs in;       // the fields that are y-transformed (the planes the z inverse reads)
     FieldPtrsW outp;
-    int nin = 0, nout = 0;
-    auto add_in = [&](int slot, int fid) -> int {
-        double2 *p = SPEC(ctx, fid);
-        if (!p) return KMM_ERR_NOMEM;
+    ZRecipe zr;         // for each input slot's z-inverse output: its plane and multiplier
+    int nin = 0, nout = 0, nbase = 0;
+    // Inside a routine step without inertial particles the x and z derivatives among the inputs
+    // (the velocity gradient's i kx / i kz columns, the scalar's, the conformation tensor's) are
+    // formed in the z inverse from their field's plane, and the symmetric tensor's duplicate
+    // components share one plane: 23 y transforms instead of 55 with polymer and scalar.  The
+    // step computes only the y derivatives for it (kmm_step).
+    const bool derived = kmm_derived_inputs(ctx) && ctx->in_step;
+    auto add_base = [&](int fid) -> int {
+        const double2 *p = SPEC(ctx, fid);
+        if (!p) return -1;
+        for (int b = 0; b < nbase; ++b)
+            if (in.p[b] == p) return b;
+        if (nbase >= MAXIO) return -1;
+        in.p[nbase] = p;
+        return nbase++;
+    };
+    auto add_in_from = [&](int slot, int base_fid, int mult) -> int {
+        const int b = add_base(base_fid);
+        if (b < 0) return KMM_ERR_NOMEM;
         if (nin >= MAXIO) return KMM_ERR_UNSUPPORTED;
         A.slot_of_in[slot] = nin;
-        in.p[nin++] = p;
+        zr.base[nin] = (unsigned char)b;
+        zr.mult[nin] = (unsigned char)mult;
+        ++nin;
         return KMM_OK;
     };
+    auto add_in = [&](int slot, int fid) -> int { return add_in_from(slot, fid, 0); };
     auto add_out = [&](int slot, int fid) -> int {
         double2 *p = SPEC(ctx, fid);
         if (!p) return KMM_ERR_NOMEM;
@@ -1154,18 +1187,36 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     for (int m = 0; m < 6; ++m) RET(add_in(S_U + m, fl[m]));
     if (scal) {
         RET(add_in(S_SC, KMM_SCALAR));
-        RET(add_in(S_CX, KMM_SCLX));
-        RET(add_in(S_CY, KMM_SCLY));
-        RET(add_in(S_CZ, KMM_SCLZ));
+        if (derived) {
+            RET(add_in_from(S_CX, KMM_SCALAR, 1));
+            RET(add_in(S_CY, KMM_SCLY));
+            RET(add_in_from(S_CZ, KMM_SCALAR, 2));
+        } else {
+            RET(add_in(S_CX, KMM_SCLX));
+            RET(add_in(S_CY, KMM_SCLY));
+            RET(add_in(S_CZ, KMM_SCLZ));
+        }
     }
     static const int gu[9] = {KMM_U11, KMM_U12, KMM_U13, KMM_U21, KMM_U22, KMM_U23, KMM_U31, KMM_U32, KMM_U33};
     if (poly || inertial)
-        for (int m = 0; m < 9; ++m) RET(add_in(S_U11 + m, gu[m]));
+        for (int m = 0; m < 9; ++m) {
+            // u_ij = d u_i / d x_j: j = x, z from u_i itself, j = y the cderiv field
+            const int comp = m / 3, dir = m % 3;
+            if (derived && dir != 1) RET(add_in_from(S_U11 + m, KMM_U + comp, dir == 0 ? 1 : 2));
+            else RET(add_in(S_U11 + m, gu[m]));
+        }
     if (inertial)
         for (int m = 0; m < 3; ++m) RET(add_in(S_LU + m, KMM_LU + m));
     if (poly) {
-        for (int m = 0; m < 9; ++m) RET(add_in(S_C11 + m, KMM_C11 + m));
-        for (int m = 0; m < 27; ++m) RET(add_in(S_DC111 + m, KMM_DC111 + m));
+        // c_ij and dc_ijk = d c_ij / d x_k; c21 = c12, c31 = c13, c32 = c23 (copied by the step)
+        static const int uniq[9] = {0, 1, 2, 1, 4, 5, 2, 5, 8};
+        for (int m = 0; m < 9; ++m) RET(add_in(S_C11 + m, KMM_C11 + (derived ? uniq[m] : m)));
+        for (int m = 0; m < 27; ++m) {
+            const int ij = m / 3, k = m % 3;
+            if (!derived) RET(add_in(S_DC111 + m, KMM_DC111 + m));
+            else if (k == 1) RET(add_in(S_DC111 + m, KMM_DC111 + 3 * uniq[ij] + 1));
+            else RET(add_in_from(S_DC111 + m, KMM_C11 + uniq[ij], k == 0 ? 1 : 2));
+        }
     }
     RET(add_out(O_H1, KMM_GN));
     RET(add_out(O_H2, KMM_FN));
@@ -1280,24 +1331,24 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     if (tcd) {
         const void *pin[MAXIO];
         void *pout[MAXIO];
-        for (int m = 0; m < nin; ++m) {
+        for (int m = 0; m < nbase; ++m) {
             pin[m] = in.p[m];
             pout[m] = pl_in32 + (size_t)m * ctx->nspec;
         }
-        tcf = kmm_tc_dct(ctx, 0, pin, pout, nin);
+        tcf = kmm_tc_dct(ctx, 0, pin, pout, nbase);
         if (tcf != KMM_OK && tcf != KMM_ERR_UNSUPPORTED) return tcf;
     }
     if (tcf != KMM_OK) {
-        const int dst = f32 ? dct_h_fwd<float2>(ctx, nin, in, pl_in32, tw_y2, nz, nxh, ncols)
-                            : dct_h_fwd<double2>(ctx, nin, in, ctx->pl_in, ctx->py2.tw, nz, nxh, ncols);
+        const int dst = f32 ? dct_h_fwd<float2>(ctx, nbase, in, pl_in32, tw_y2, nz, nxh, ncols)
+                            : dct_h_fwd<double2>(ctx, nbase, in, ctx->pl_in, ctx->py2.tw, nz, nxh, ncols);
         if (dst != KMM_ERR_UNSUPPORTED) {
             RET(dst);
         } else {
             if (f32)
-                k_dct_fwd<float2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nin), 256, sm_dct, ctx->stream>>>(
+                k_dct_fwd<float2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nbase), 256, sm_dct, ctx->stream>>>(
                     in, pl_in32, ctx->py2, tw_y2, nyp, nz, nxh, ncols);
             else
-                k_dct_fwd<double2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nin), 256, sm_dct, ctx->stream>>>(
+                k_dct_fwd<double2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nbase), 256, sm_dct, ctx->stream>>>(
                     in, ctx->pl_in, ctx->py2, ctx->py2.tw, nyp, nz, nxh, ncols);
             CKL();
         }
@@ -1305,11 +1356,11 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     kmm_toc(ctx, KMM_STAGE_DCT_FWD);
     kmm_tic(ctx);
     if (f32)
-        k_zfft_bwd<float2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nin), 256, sm_z, ctx->stream>>>(pl_in32, q_in32, ctx->pmz,
-                                                                                               tw_mz, nyp, nz, nxh, mz);
+        k_zfft_bwd<float2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nin), 256, sm_z, ctx->stream>>>(
+            pl_in32, q_in32, ctx->pmz, tw_mz, nyp, nz, nxh, mz, zr, ctx->d_wavx, ctx->d_wavz);
     else
         k_zfft_bwd<double2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nin), 256, sm_z, ctx->stream>>>(
-            ctx->pl_in, ctx->q_in, ctx->pmz, ctx->pmz.tw, nyp, nz, nxh, mz);
+            ctx->pl_in, ctx->q_in, ctx->pmz, ctx->pmz.tw, nyp, nz, nxh, mz, zr, ctx->d_wavx, ctx->d_wavz);
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_BWD);
     bool fast_done = false, xstat = false;
@@ -1538,7 +1589,7 @@ __device__ __forceinline__ double swirl_point(double u11, double u12, double u13
 // one warp per (y, z) row: Hermitian c2r of the nine gradients (two per complex FFT) into shared
 // rows, then the swirl of every x into SWIRL3D [y][z][x]
 __global__ void __launch_bounds__(SW_WARPS * 32) k_swirl_x(const double2 *__restrict__ q, double *__restrict__ sw,
-                                                           DevPlan P, int nyp, int mz, int mx, int nxh) {
+                                                           const __grid_constant__ DevPlan P, int nyp, int mz, int mx, int nxh) {
     extern __shared__ double2 sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y = blockIdx.y, z = blockIdx.x * SW_WARPS + warp;
@@ -1600,9 +1651,13 @@ extern "C" int kmm_calcswirl(kmm_ctx *ctx) {
                                                                                                ctx->py2.tw, nyp, nz,
                                                                                                nxh, ncols);
     CKL();
-    k_zfft_bwd<double2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, 9), 256, sm_z, ctx->stream>>>(ctx->pl_in, ctx->q_in,
-                                                                                          ctx->pmz, ctx->pmz.tw, nyp,
-                                                                                          nz, nxh, mz);
+    ZRecipe zr;
+    for (int m = 0; m < 9; ++m) {
+        zr.base[m] = (unsigned char)m;
+        zr.mult[m] = 0;
+    }
+    k_zfft_bwd<double2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, 9), 256, sm_z, ctx->stream>>>(
+        ctx->pl_in, ctx->q_in, ctx->pmz, ctx->pmz.tw, nyp, nz, nxh, mz, zr, ctx->d_wavx, ctx->d_wavz);
     CKL();
     k_swirl_x<<<dim3((mz + SW_WARPS - 1) / SW_WARPS, nyp), SW_WARPS * 32, sm_s, ctx->stream>>>(ctx->q_in, sw, ctx->wmx,
                                                                                             nyp, mz, mx, nxh);

@@ -302,6 +302,13 @@ extern "C" int kmm_initial(kmm_ctx *ctx) {
     return st;
 }
 
+// vcw3dp inside the routine step forms the x and z derivatives among its inputs in its z inverse
+// (KMM_OPT_DERIVED_INPUTS, default 1), except where inertial particles need the materialised
+// velocity gradient and Laplacian on the 3/2 grid
+bool kmm_derived_inputs(const kmm_ctx *ctx) {
+    return ctx->use_derived && !(ctx->p.particle_flag > 0 && ctx->p.npart > 0);
+}
+
 // ---------------------------------------------------------------------------
 // one iteration of the time loop, main_dns.f90:198-811
 // ---------------------------------------------------------------------------
@@ -392,23 +399,57 @@ extern "C" int kmm_step(kmm_ctx *ctx) {
     { static const int l[2] = {KMM_U, KMM_W}; RET(norm_ids(ctx, l, 2)); }
     RET(kmm_vort(ctx));
     { static const int l[2] = {KMM_OMX, KMM_OMZ}; RET(norm_ids(ctx, l, 2)); }
+    // with derived inputs vcw3dp forms the x and z derivatives itself (in its z inverse): only the
+    // y derivatives are computed here, in one batched cderiv launch
+    const bool derived = kmm_derived_inputs(ctx);
+    const double2 *dsrc[KMM_CDERIV_BATCH];
+    double2 *ddst[KMM_CDERIV_BATCH];
+    int nd = 0;
+    int dnorm[KMM_CDERIV_BATCH];
+    auto want_dy = [&](int f, int df) -> int {
+        dsrc[nd] = SPEC(ctx, f);
+        ddst[nd] = SPEC(ctx, df);
+        if (!dsrc[nd] || !ddst[nd]) return KMM_ERR_NOMEM;
+        dnorm[nd++] = df;
+        return KMM_OK;
+    };
     if (ctx->p.scalar_on) {
         RET(kmm_norm(ctx, KMM_SCALAR));
-        RET(kmm_gradscl(ctx));
-        static const int l[3] = {KMM_SCLX, KMM_SCLY, KMM_SCLZ};
-        RET(norm_ids(ctx, l, 3));
+        if (derived) {
+            RET(want_dy(KMM_SCALAR, KMM_SCLY));
+        } else {
+            RET(kmm_gradscl(ctx));
+            static const int l[3] = {KMM_SCLX, KMM_SCLY, KMM_SCLZ};
+            RET(norm_ids(ctx, l, 3));
+        }
     }
     if (ctx->p.polymer_on || ctx->p.particle_flag > 0) {
         // the velocity gradient / Laplacian feed only the polymer terms and inertial particles
-        RET(kmm_gradv(ctx));
-        static const int l[12] = {KMM_U11, KMM_U12, KMM_U13, KMM_U21, KMM_U22, KMM_U23, KMM_U31, KMM_U32, KMM_U33,
-                                  KMM_LU, KMM_LV, KMM_LW};
-        RET(norm_ids(ctx, l, 12));
+        if (derived) {
+            RET(want_dy(KMM_U, KMM_U12));
+            RET(want_dy(KMM_V, KMM_U22));
+            RET(want_dy(KMM_W, KMM_U32));
+        } else {
+            RET(kmm_gradv(ctx));
+            static const int l[12] = {KMM_U11, KMM_U12, KMM_U13, KMM_U21, KMM_U22, KMM_U23, KMM_U31, KMM_U32,
+                                      KMM_U33, KMM_LU, KMM_LV, KMM_LW};
+            RET(norm_ids(ctx, l, 12));
+        }
     }
     if (ctx->p.polymer_on) {
-        RET(kmm_derivscji(ctx));
-        RET(poly_norm_c(ctx));
-        RET(poly_norm_dc(ctx));
+        if (derived) {
+            RET(poly_norm_c(ctx));
+            static const int uq[6] = {0, 1, 2, 4, 5, 8};   // c11 c12 c13 c22 c23 c33
+            for (int m = 0; m < 6; ++m) RET(want_dy(KMM_C11 + uq[m], KMM_DC111 + 3 * uq[m] + 1));
+        } else {
+            RET(kmm_derivscji(ctx));
+            RET(poly_norm_c(ctx));
+            RET(poly_norm_dc(ctx));
+        }
+    }
+    if (nd) {
+        RET(kmm_internal_cderiv_many(ctx, dsrc, ddst, nd));
+        RET(norm_ids(ctx, dnorm, nd));
     }
     kmm_toc(ctx, KMM_STAGE_COLUMN);
     ctx->in_step = 1;

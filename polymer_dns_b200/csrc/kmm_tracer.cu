@@ -465,7 +465,7 @@ extern "C" int kmm_tracer_cells(kmm_ctx *ctx, int *cells, size_t n) {
 // xyzfft(a,b,-1), helpers.f90:6-87: physical (nyp,nz,nx) -> spectral (nyp,nz,nxh)
 // ---------------------------------------------------------------------------
 // y: DCT-I of each real column, /ny, halve the end values (in place on a real copy)
-__global__ void k_xyz_y(double *__restrict__ b, DevPlan P, int nyp, int ncols) {
+__global__ void k_xyz_y(double *__restrict__ b, const __grid_constant__ DevPlan P, int nyp, int ncols) {
     extern __shared__ double2 sm[];
     const int ny = nyp - 1, L = 2 * ny;
     const int col = blockIdx.x;
@@ -487,7 +487,7 @@ __global__ void k_xyz_y(double *__restrict__ b, DevPlan P, int nyp, int ncols) {
 }
 
 // x: r2c over nx for each (i,j) line (stride nz*nyp), /nx, keep k < nxh -> complex work (nyp,nz,nxh)
-__global__ void k_xyz_x(const double *__restrict__ b, double2 *__restrict__ a, DevPlan P, int nyp, int nz, int nx) {
+__global__ void k_xyz_x(const double *__restrict__ b, double2 *__restrict__ a, const __grid_constant__ DevPlan P, int nyp, int nz, int nx) {
     extern __shared__ double2 sm[];
     const int line = blockIdx.x;   // i + nyp*j
     const int i = line % nyp, j = line / nyp;
@@ -503,7 +503,7 @@ __global__ void k_xyz_x(const double *__restrict__ b, double2 *__restrict__ a, D
 }
 
 // z: forward c2c over nz for each (i,k) line, /nz
-__global__ void k_xyz_z(double2 *__restrict__ a, DevPlan P, int nyp, int nz) {
+__global__ void k_xyz_z(double2 *__restrict__ a, const __grid_constant__ DevPlan P, int nyp, int nz) {
     extern __shared__ double2 sm[];
     const int line = blockIdx.x;   // i + nyp*k
     const int i = line % nyp, k = line / nyp;

@@ -215,3 +215,35 @@ def test_cfg5_lengths_match_oracle(rt, oracle_mod, grid):
     _cells_identical(g, o, p)
     g.close()
     o.close()
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_derived_inputs_match_materialised(rt, prec):
+    """vcw3dp inside the routine step forming the x and z derivatives of its inputs in the z inverse
+    (KMM_OPT_DERIVED_INPUTS = 1, the default: 23 y transforms with polymer and scalar) against the
+    reference's sequence of materialised derivative fields (gradv, gradscl, derivscji; 55 y
+    transforms): i kx, i kz commute with the y transform, so the states agree to transform rounding
+    after 5 polymer + IB + scalar steps (1e-12 relative FP64; 1e-5 for the mixed form's state and
+    1e-4 for its nonlinear terms, where the derivative is now taken of the FP32 plane)."""
+    p, init, _ = configs.make("cfg3", precision=prec, grid=64, npart=300)
+    f, extra = configs.build_inputs(p, init, "cfg3")
+    ctxs = []
+    for dv in (1, 0):
+        g = rt.KmmContext(p)
+        g.call("set_option", abi.OPT_DERIVED_INPUTS, dv)
+        configs.load(f, extra, g.upload)
+        assert g.initial() == 0
+        ctxs.append(g)
+    for _ in range(5):
+        for g in ctxs:
+            assert g.step() == 0
+    # the state to 1e-12 (FP64) / 1e-5 (mixed); the nonlinear terms of the mixed form, formed from
+    # FP32 planes either way, to 1e-4
+    state = ("V", "OMY", "U0", "SCALAR", "C11", "C12", "C23", "FXINTG", "XPART")
+    terms = ("FN", "GN", "SCN", "QP13", "STR22N")
+    for names, tol in ((state, 1e-12 if prec == 0 else 1e-5), (terms, 1e-12 if prec == 0 else 1e-4)):
+        for name in names:
+            e = kc.rel_err(ctxs[0].download(name), ctxs[1].download(name))
+            assert e <= tol, "%s rel err %.3e" % (name, e)
+    for g in ctxs:
+        g.close()

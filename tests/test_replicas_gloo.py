@@ -61,3 +61,19 @@ def test_replicas_two_gloo_ranks(oracle_mod):
     assert m0 == m1 == pytest.approx(max(l0, l1))          # the job time is the slowest rank's
     assert v0 == pytest.approx(2 * 2 / (max(l0, l1) / 1e3))  # every rank's steps count
     assert s0 == s1 and s0[0] == s0[1]                     # identical replicas, no exchange
+
+
+def test_autotune_candidates_follow_the_configuration():
+    """The tuner times only the variants that apply: TMA z tiles, blocked columns and graph replay
+    on the fused step; the tensor-core y transforms on the mixed routine path; nothing else."""
+    from polymer_dns_b200 import abi, autotune
+    fused = abi.default_params(nx=64, ny=64, nz=64)
+    c = autotune.candidates(fused)
+    assert len(c) == 8 and {abi.OPT_ZTMA, abi.OPT_COLUMN_BLOCKED, abi.OPT_GRAPH} == set(c[0])
+    assert len(autotune.candidates(abi.default_params(nx=64, ny=64, nz=64, precision=1))) == 4
+    assert autotune.candidates(abi.default_params(nx=64, ny=64, nz=64, polymer_on=1)) == [{}]
+    mixed_poly = autotune.candidates(abi.default_params(nx=64, ny=64, nz=64, polymer_on=1, precision=1))
+    assert mixed_poly == [{abi.OPT_TC_DCT: 0}, {abi.OPT_TC_DCT: 1}]
+    assert autotune.shape_key(fused) != autotune.shape_key(abi.default_params(nx=64, ny=64, nz=96))
+    assert autotune.describe({abi.OPT_ZTMA: 1, abi.OPT_GRAPH: 0}) == "ztma=1,graph=0" or \
+        autotune.describe({abi.OPT_ZTMA: 1, abi.OPT_GRAPH: 0}) == "graph=0,ztma=1"
