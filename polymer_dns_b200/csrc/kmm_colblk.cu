@@ -361,27 +361,77 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB_BWD) k_bcol_bwd(ColBwdA
         filt(sc);
         bstore<K>(A.scn + off, sc);
     }
-    // one column variable live through each transform: h3 is stored as omz and re-read (from L2)
-    // once h1 has been transformed, and -d waits in fn's output column while h2 is transformed
-    {
-        BCol<K> h3;
+    if constexpr (sizeof(C) == 16) {
+        // one column variable live through each transform: h3 is stored as omz and re-read (from L2)
+        // once h1 has been transformed, and -d waits in fn's output column while h2 is transformed
+        {
+            BCol<K> h3;
+            bload_dct<K, C>(h3, (const C *)A.yo + (2 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
+            bnorm<K>(h3, kx, j, A.nzh);
+            filt(h3);
+            bstore<K>(A.omz + off, h3);
+        }
+        BCol<K> d;
+        {
+            BCol<K> h1, h3;
+            bload_dct<K, C>(h1, (const C *)A.yo + (0 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
+            bnorm<K>(h1, kx, j, A.nzh);
+            filt(h1);
+            __syncwarp();
+            bload<K>(h3, A.omz + off);
+            // h1n = Re gn(:,1,1), h3n = Re omz(:,1,1) (main_dns.f90:748-751)
+            if (kx == 0 && j == 0) {
+                const int t = lane & 15;
+    #pragma unroll
+                for (int m = 0; m < K; ++m) {
+                    A.h1n[t * K + m] = h1.v[m].x;
+                    A.h3n[t * K + m] = h3.v[m].x;
+                }
+                if (t == 15) {
+                    A.h1n[NY] = h1.v[K].x;
+                    A.h3n[NY] = h3.v[K].x;
+                }
+            }
+            // nonlin (solvers.f90:1497-1572): fn = -k^2 h2 - d/dy(i(kz h3 + kx h1)); gn = i(kz h1 - kx h3)
+            BCol<K> tt;
+    #pragma unroll
+            for (int m = 0; m <= K; ++m) {
+                const double2 s = make_double2(kzv * h3.v[m].x + kxv * h1.v[m].x, kzv * h3.v[m].y + kxv * h1.v[m].y);
+                tt.v[m] = make_double2(-s.y, s.x);
+            }
+    #pragma unroll
+            for (int m = 0; m <= K; ++m) {
+                const double2 s = make_double2(kzv * h1.v[m].x - kxv * h3.v[m].x, kzv * h1.v[m].y - kxv * h3.v[m].y);
+                h1.v[m] = make_double2(-s.y, s.x);
+            }
+            bstore<K>(A.gn + off, h1);
+            bcderiv<K>(d, tt, A.dyde, FULL);
+        }
+    #pragma unroll
+        for (int m = 0; m <= K; ++m) d.v[m] = make_double2(-d.v[m].x, -d.v[m].y);
+        bstore<K>(A.fn + off, d);
+        BCol<K> h2;
+        bload_dct<K, C>(h2, (const C *)A.yo + (1 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
+        bnorm<K>(h2, kx, j, A.nzh);
+        filt(h2);
+        __syncwarp();
+        bload<K>(d, A.fn + off);
+        const double w2 = -kxv * kxv - kzv * kzv;
+    #pragma unroll
+        for (int m = 0; m <= K; ++m) h2.v[m] = make_double2(w2 * h2.v[m].x + d.v[m].x, w2 * h2.v[m].y + d.v[m].y);
+        bstore<K>(A.fn + off, h2);
+    } else {   // FP32 transforms: the register budget holds h1, h3 and d at once
+        BCol<K> h1, h3, d;
+        bload_dct<K, C>(h1, (const C *)A.yo + (0 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
         bload_dct<K, C>(h3, (const C *)A.yo + (2 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
+        bnorm<K>(h1, kx, j, A.nzh);
         bnorm<K>(h3, kx, j, A.nzh);
         filt(h3);
-        bstore<K>(A.omz + off, h3);
-    }
-    BCol<K> d;
-    {
-        BCol<K> h1, h3;
-        bload_dct<K, C>(h1, (const C *)A.yo + (0 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
-        bnorm<K>(h1, kx, j, A.nzh);
         filt(h1);
-        __syncwarp();
-        bload<K>(h3, A.omz + off);
         // h1n = Re gn(:,1,1), h3n = Re omz(:,1,1) (main_dns.f90:748-751)
         if (kx == 0 && j == 0) {
             const int t = lane & 15;
-#pragma unroll
+    #pragma unroll
             for (int m = 0; m < K; ++m) {
                 A.h1n[t * K + m] = h1.v[m].x;
                 A.h3n[t * K + m] = h3.v[m].x;
@@ -392,33 +442,31 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB_BWD) k_bcol_bwd(ColBwdA
             }
         }
         // nonlin (solvers.f90:1497-1572): fn = -k^2 h2 - d/dy(i(kz h3 + kx h1)); gn = i(kz h1 - kx h3)
-        BCol<K> tt;
-#pragma unroll
-        for (int m = 0; m <= K; ++m) {
-            const double2 s = make_double2(kzv * h3.v[m].x + kxv * h1.v[m].x, kzv * h3.v[m].y + kxv * h1.v[m].y);
-            tt.v[m] = make_double2(-s.y, s.x);
+        {
+            BCol<K> tt;
+    #pragma unroll
+            for (int m = 0; m <= K; ++m) {
+                const double2 s = make_double2(kzv * h3.v[m].x + kxv * h1.v[m].x, kzv * h3.v[m].y + kxv * h1.v[m].y);
+                tt.v[m] = make_double2(-s.y, s.x);
+            }
+            bcderiv<K>(d, tt, A.dyde, FULL);
         }
-#pragma unroll
+    #pragma unroll
         for (int m = 0; m <= K; ++m) {
             const double2 s = make_double2(kzv * h1.v[m].x - kxv * h3.v[m].x, kzv * h1.v[m].y - kxv * h3.v[m].y);
             h1.v[m] = make_double2(-s.y, s.x);
         }
         bstore<K>(A.gn + off, h1);
-        bcderiv<K>(d, tt, A.dyde, FULL);
+        bstore<K>(A.omz + off, h3);
+        BCol<K> h2;
+        bload_dct<K, C>(h2, (const C *)A.yo + (1 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
+        bnorm<K>(h2, kx, j, A.nzh);
+        filt(h2);
+        const double w2 = -kxv * kxv - kzv * kzv;
+    #pragma unroll
+        for (int m = 0; m <= K; ++m) h2.v[m] = make_double2(w2 * h2.v[m].x - d.v[m].x, w2 * h2.v[m].y - d.v[m].y);
+        bstore<K>(A.fn + off, h2);
     }
-#pragma unroll
-    for (int m = 0; m <= K; ++m) d.v[m] = make_double2(-d.v[m].x, -d.v[m].y);
-    bstore<K>(A.fn + off, d);
-    BCol<K> h2;
-    bload_dct<K, C>(h2, (const C *)A.yo + (1 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
-    bnorm<K>(h2, kx, j, A.nzh);
-    filt(h2);
-    __syncwarp();
-    bload<K>(d, A.fn + off);
-    const double w2 = -kxv * kxv - kzv * kzv;
-#pragma unroll
-    for (int m = 0; m <= K; ++m) h2.v[m] = make_double2(w2 * h2.v[m].x + d.v[m].x, w2 * h2.v[m].y + d.v[m].y);
-    bstore<K>(A.fn + off, h2);
     (void)h;
 }
 

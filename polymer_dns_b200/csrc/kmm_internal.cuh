@@ -60,6 +60,7 @@ struct kmm_ctx {
     int it;
     int in_step;                 // inside kmm_step (intermediate copies only kept when needed)
     int kmaxsurf;
+    int ib_ylo, ib_yhi;          // 1-based y-planes holding the solid cells (0, 0: none)
     // host and device copies of wavenumbers, Chebyshev weights, grid
     double *h_wavx, *h_wavz, *h_c, *h_ycoord, *h_seght;
     double *d_wavx, *d_wavz, *d_c, *d_ycoord, *d_seght;

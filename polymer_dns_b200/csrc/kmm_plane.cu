@@ -751,9 +751,9 @@ __global__ void __launch_bounds__(XW * 32) k_xfwd2(const typename kct::Real<C>::
 // ---------------------------------------------------------------------------
 template <typename PO_T>
 __global__ void k_spread(PO_T *__restrict__ po, const double *__restrict__ drag, const double *__restrict__ fspread,
-                         int nyp, int mz, int mx, int kmaxsurf, int o1, int o2, int o3) {
+                         int nyp, int mz, int mx, int kmaxsurf, int y0, int o1, int o2, int o3) {
     const size_t nplane = (size_t)mz * mx;
-    const int y = blockIdx.y;
+    const int y = y0 + blockIdx.y;
     if (y + 1 > kmaxsurf) return;
     const size_t n3 = (size_t)nyp * nplane;
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nplane; e += (size_t)gridDim.x * blockDim.x) {
@@ -1055,6 +1055,11 @@ __global__ void k_kmaxsurf(const int *__restrict__ im, int *out, int nyp, int mz
         const int t = im[e];
         if (t == 1 || t == 3 || t == 4) atomicMax(out, (int)(e % mx) + 1);   // 1-based x index k
         if (!(t == 0 || t == 1 || t == 3 || t == 4 || t == 11)) atomicOr(out + 1, 1);
+        if (t == 1 || t == 3 || t == 4 || t == 11) {   // y-planes that can hold a nonzero drag
+            const int y1 = (int)(e / ((size_t)mz * mx)) + 1;
+            atomicMin(out + 2, y1);
+            atomicMax(out + 3, y1);
+        }
     }
 }
 
@@ -1062,13 +1067,13 @@ int kmm_update_kmaxsurf(kmm_ctx *ctx) {
     if (ctx->kmaxsurf >= 0) return KMM_OK;
     int *im = (int *)kmm_field_ptr(ctx, KMM_IMATRIX);
     if (!im) return KMM_ERR_NOMEM;
-    int h[2] = {0, 0};
+    int h[4] = {0, 0, 1 << 30, 0};
     int *tmp = NULL;
-    CK(cudaMallocAsync((void **)&tmp, 2 * sizeof(int), ctx->stream));
-    CK(cudaMemsetAsync(tmp, 0, 2 * sizeof(int), ctx->stream));
+    CK(cudaMallocAsync((void **)&tmp, 4 * sizeof(int), ctx->stream));
+    CK(cudaMemcpyAsync(tmp, h, 4 * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     k_kmaxsurf<<<kmm_blocks(ctx->nphys, 256), 256, 0, ctx->stream>>>(im, tmp, ctx->nyp, ctx->mz, ctx->mx);
     CKL();
-    CK(cudaMemcpyAsync(h, tmp, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(h, tmp, 4 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaFreeAsync(tmp, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (h[1]) {
@@ -1076,6 +1081,8 @@ int kmm_update_kmaxsurf(kmm_ctx *ctx) {
         return KMM_ERR_UNSUPPORTED;
     }
     ctx->kmaxsurf = h[0];
+    ctx->ib_ylo = h[3] > 0 ? h[2] : 0;
+    ctx->ib_yhi = h[3];
     return KMM_OK;
 }
 
@@ -1425,16 +1432,21 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
             // the reference spreads in the planes i <= kmaxsurf (an x extent, main_dns.f90:1526-1535);
             // ib_spread_all (no counterpart in the reference) spreads in every plane
             const int ksp = (ctx->p.ib_spread_all || ctx->kmaxsurf >= nyp) ? nyp : ctx->kmaxsurf;
-            const dim3 gs(kmm_blocks((size_t)mz * mx, 256) > 64 ? 64 : kmm_blocks((size_t)mz * mx, 256), ksp);
-            if (f32)
-                k_spread<float><<<gs, 256, 0, ctx->stream>>>(po32, ctx->drag, ctx->d_fspread, nyp, mz, mx, ksp,
-                                                             A.slot_of_out[O_H1], A.slot_of_out[O_H2],
-                                                             A.slot_of_out[O_H3]);
-            else
-                k_spread<double><<<gs, 256, 0, ctx->stream>>>(ctx->po, ctx->drag, ctx->d_fspread, nyp, mz, mx,
-                                                              ksp, A.slot_of_out[O_H1], A.slot_of_out[O_H2],
-                                                              A.slot_of_out[O_H3]);
-            CKL();
+            // planes without a solid cell carry zero drag and add nothing: only the planes
+            // ib_ylo .. min(ib_yhi, ksp) (1-based) are swept
+            const int y0 = ctx->ib_ylo > 0 ? ctx->ib_ylo - 1 : 0, y1 = ctx->ib_yhi < ksp ? ctx->ib_yhi : ksp;
+            if (ctx->ib_ylo > 0 && y1 > y0) {
+                const dim3 gs(kmm_blocks((size_t)mz * mx, 256) > 64 ? 64 : kmm_blocks((size_t)mz * mx, 256), y1 - y0);
+                if (f32)
+                    k_spread<float><<<gs, 256, 0, ctx->stream>>>(po32, ctx->drag, ctx->d_fspread, nyp, mz, mx, ksp, y0,
+                                                                 A.slot_of_out[O_H1], A.slot_of_out[O_H2],
+                                                                 A.slot_of_out[O_H3]);
+                else
+                    k_spread<double><<<gs, 256, 0, ctx->stream>>>(ctx->po, ctx->drag, ctx->d_fspread, nyp, mz, mx,
+                                                                  ksp, y0, A.slot_of_out[O_H1], A.slot_of_out[O_H2],
+                                                                  A.slot_of_out[O_H3]);
+                CKL();
+            }
         }
         kmm_tic(ctx);
         const size_t sm_xf2 = 2 * eb * 2 * XW * (size_t)mx;
