@@ -1427,7 +1427,6 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         CKL();
         CK(cudaMemcpyAsync(kmm_h_pin_status(ctx), ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         xstat = true;
-        kmm_toc(ctx, KMM_STAGE_XPHYS);
         if (ib_any && ctx->kmaxsurf > 0) {
             // the reference spreads in the planes i <= kmaxsurf (an x extent, main_dns.f90:1526-1535);
             // ib_spread_all (no counterpart in the reference) spreads in every plane
@@ -1448,6 +1447,7 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
                 CKL();
             }
         }
+        kmm_toc(ctx, KMM_STAGE_XPHYS);   // the spreading counts with the pointwise stage
         kmm_tic(ctx);
         const size_t sm_xf2 = 2 * eb * 2 * XW * (size_t)mx;
 #define XF2(MM, CC, PO, QQ, TW)                                                                                 \
