@@ -515,59 +515,85 @@ def polymer_report(a, local_rank):
             "cpu_baseline": cpu}
 
 
-def cfg5_report(a, local_rank, nsteps=5):
+def cfg5_report(a, local_rank, nsteps=5, mark=10):
     """The large single run (384 x 257 x 384, Re_tau = 395, polymer + scalar + IB cylinder + 1 M RK3
-    tracers) in FP64 on the routine path: steps/s, device memory held, and size-independent checks
-    after the timed steps (continuity of the spectral velocity, finite CFL, tracer cells in range).
-    The mixed form has no compiled FP32 transforms at these lengths (KMM_ERR_UNSUPPORTED)."""
+    tracers) on the routine path, FP64 and mixed in turn (one context at a time: the FP64 form holds
+    about 158 GB): steps/s, device memory held, size-independent checks after the timed steps
+    (continuity of the spectral velocity, finite CFL, tracer cells in range), and the mixed form's
+    relative error against FP64 from the same inputs after `mark` steps (u, v, w, scalar, the six
+    conformation components, bulk kinetic energy, wall shear).  1000 steps of this workload take
+    about five minutes per form and are left out of the default run."""
     import torch
     from polymer_dns_b200 import abi, configs, runtime
     torch.cuda.set_device(local_rank)
-    p, init, desc = configs.make("cfg5", 0)
-    f, extra = configs.build_inputs(p, init, "cfg5")
-    free0, total = torch.cuda.mem_get_info()
-    c = runtime.KmmContext(p, device=local_rank)
-    out = {"workload": desc, "grid": [p.nx, p.ny + 1, p.nz], "npart": p.npart}
-    try:
-        configs.load(f, extra, c.upload)
-        del f, extra
-        st = c.call("initial", allow=(abi.ERR_CFL, abi.ERR_NOMEM, abi.ERR_UNSUPPORTED))
-        if st:
-            out["status"] = abi.STATUS_NAMES.get(st, st) + ": " + c.error()
-            return out
-        for _ in range(2):
-            st = c.call("step", allow=(abi.ERR_CFL, abi.ERR_NAN, abi.ERR_NOMEM))
+    p64, init, desc = configs.make("cfg5", 0)
+    f, extra = configs.build_inputs(p64, init, "cfg5")
+    names = {"u": "U", "v": "V", "w": "W", "scalar": "SCALAR", "c11": "C11", "c12": "C12", "c13": "C13",
+             "c22": "C22", "c23": "C23", "c33": "C33"}
+    out = {"workload": desc, "grid": [p64.nx, p64.ny + 1, p64.nz], "npart": p64.npart}
+    fields, flow = {}, {}
+    for prec in (0, 1):
+        key = "fp64" if prec == 0 else "mixed"
+        p, _, _ = configs.make("cfg5", prec)
+        free0, total = torch.cuda.mem_get_info()
+        c = runtime.KmmContext(p, device=local_rank)
+        try:
+            configs.load(f, extra, c.upload)
+            st = c.call("initial", allow=(abi.ERR_CFL, abi.ERR_NOMEM, abi.ERR_UNSUPPORTED))
             if st:
-                out["status"] = abi.STATUS_NAMES.get(st, st) + " in warm-up: " + c.error()
-                return out
-        c.call("sync")
-        free1, _ = torch.cuda.mem_get_info()
-        c.event_record(0)
-        sts = [c.call("step", allow=(abi.ERR_CFL, abi.ERR_NAN)) for _ in range(nsteps)]
-        c.event_record(1)
-        ms = c.event_elapsed(0, 1) / nsteps
-        c.call("veloc")
-        u, w = c.download("U"), c.download("W")
-        c.call("cderiv", "V", "WRKC")
-        dv = c.download("WRKC")
-        kx = np.arange(p.nx // 2) * 2 * math.pi / p.xl
-        kz = np.fft.fftfreq(p.nz, 1.0 / p.nz) * 2 * math.pi / p.zl
-        div = 1j * kx[None, None, :] * u + dv + 1j * kz[None, :, None] * w
-        cells = c.tracer_cells()
-        out.update({"fp64": {"value": round(1e3 / ms, 3), "unit": "timesteps/s", "ms_per_step": round(ms, 3),
-                             "grid_point_steps_per_s": round(1e3 / ms * p.nx * (p.ny + 1) * p.nz, 1),
-                             "fused_model_bytes_per_step": fused_model_bytes(p),
-                             "frac_of_hbm": round(fused_model_bytes(p) / (ms / 1e3) / 1e9 /
-                                                  float(load_peaks()[0].get("hbm_gbs", 6650.0)), 4),
-                             "steps": nsteps, "status": [abi.STATUS_NAMES.get(x, x) for x in sts]},
-                    "device_memory_gb": round((free0 - free1) / 1e9, 2), "device_total_gb": round(total / 1e9, 1),
-                    "checks": {"max_divergence_rel": float("%.3e" % (np.abs(div).max() / np.abs(u).max())),
-                               "cflmax": round(c.stats().cflmax, 5),
-                               "tracer_cells_in_range": bool(cells.min() >= 1)},
-                    "mixed": "KMM_ERR_UNSUPPORTED: no compiled FP32 transforms at mx = mz = 576, 2 ny = 512",
-                    "status": "ok"})
-    finally:
-        c.close()
+                out[key] = abi.STATUS_NAMES.get(st, st) + ": " + c.error()
+                continue
+            bad = None
+            for _ in range(2):
+                st = c.call("step", allow=(abi.ERR_CFL, abi.ERR_NAN, abi.ERR_NOMEM, abi.ERR_UNSUPPORTED))
+                if st:
+                    bad = abi.STATUS_NAMES.get(st, st) + " in warm-up: " + c.error()
+                    break
+            if bad:
+                out[key] = bad
+                continue
+            c.call("sync")
+            free1, _ = torch.cuda.mem_get_info()
+            c.event_record(0)
+            sts = [c.call("step", allow=(abi.ERR_CFL, abi.ERR_NAN)) for _ in range(nsteps)]
+            c.event_record(1)
+            ms = c.event_elapsed(0, 1) / nsteps
+            for _ in range(mark - 2 - nsteps):
+                sts.append(c.call("step", allow=(abi.ERR_CFL, abi.ERR_NAN)))
+            flow[prec] = c.flowstats()   # runs veloc: u, w current
+            fields[prec] = {k: c.download(n) for k, n in names.items()}
+            u, w = fields[prec]["u"], fields[prec]["w"]
+            c.call("cderiv", "V", "WRKC")
+            dv = c.download("WRKC")
+            kx = np.arange(p.nx // 2) * 2 * math.pi / p.xl
+            kz = np.fft.fftfreq(p.nz, 1.0 / p.nz) * 2 * math.pi / p.zl
+            div = 1j * kx[None, None, :] * u + dv + 1j * kz[None, :, None] * w
+            cells = c.tracer_cells()
+            out[key] = {"value": round(1e3 / ms, 3), "unit": "timesteps/s", "ms_per_step": round(ms, 3),
+                        "grid_point_steps_per_s": round(1e3 / ms * p.nx * (p.ny + 1) * p.nz, 1),
+                        "fused_model_bytes_per_step": fused_model_bytes(p),
+                        "frac_of_hbm": round(fused_model_bytes(p) / (ms / 1e3) / 1e9 /
+                                             float(load_peaks()[0].get("hbm_gbs", 6650.0)), 4),
+                        "timed_steps": nsteps, "steps_run": mark, "status": sorted({abi.STATUS_NAMES.get(x, x) for x in sts}),
+                        "device_memory_gb": round((free0 - free1) / 1e9, 2),
+                        "checks": {"max_divergence_rel": float("%.3e" % (np.abs(div).max() / np.abs(u).max())),
+                                   "cflmax": round(c.stats().cflmax, 5),
+                                   "tracer_cells_in_range": bool(cells.min() >= 1)}}
+            out["device_total_gb"] = round(total / 1e9, 1)
+        finally:
+            c.close()
+    if 0 in fields and 1 in fields:
+        e = {}
+        for k in names:
+            x, y = fields[1][k], fields[0][k]
+            e[k] = float("%.3e" % (np.abs(x - y).max() / max(np.abs(y).max(), 1e-300)))
+        (_, s64), (_, s32) = flow[0], flow[1]
+        e["bulk_ke"] = float("%.3e" % (abs(s32[3] - s64[3]) / abs(s64[3])))
+        e["wall_shear"] = float("%.3e" % (max(abs(s32[1] - s64[1]), abs(s32[2] - s64[2])) /
+                                          max(abs(s64[1]), abs(s64[2]))))
+        out["mixed_rel_err_vs_fp64"] = {str(mark): e}
+        out["mixed"]["speedup_vs_fp64"] = round(out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"], 3)
+    out["status"] = "ok" if isinstance(out.get("fp64"), dict) and isinstance(out.get("mixed"), dict) else "incomplete"
     return out
 
 

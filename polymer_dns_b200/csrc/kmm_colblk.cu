@@ -470,9 +470,11 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB_BWD) k_bcol_bwd(ColBwdA
     (void)h;
 }
 
+// K = ny / 16 where blocked kernels are compiled: the fused column kernels for ny = 32 .. 128 (K <=
+// 8), the routine path's solver also for ny = 256
 static int colblk_k(const kmm_ctx *ctx) {
     const int ny = ctx->ny;
-    if (ny != 32 && ny != 64 && ny != 96 && ny != 128) return 0;
+    if (ny != 32 && ny != 64 && ny != 96 && ny != 128 && ny != 256) return 0;
     return ny / 16;
 }
 
@@ -592,6 +594,7 @@ int kmm_colblk_solve_many(kmm_ctx *ctx, double2 *const *u, int nf, double g, int
         case 4: BS(4); break;
         case 6: BS(6); break;
         case 8: BS(8); break;
+        case 16: BS(16); break;
         default: return KMM_ERR_UNSUPPORTED;
         }
 #undef BS

@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(128) k_cderiv_hw(CderivList list, int ncols, d
 int kmm_internal_cderiv_many(kmm_ctx *ctx, const double2 *const *f, double2 *const *df, int n) {
     const int ncols = ctx->nz * ctx->nxh;
     const int ny = ctx->nyp - 1;
-    if (ctx->use_colblk && ny % 16 == 0 && ny >= 32 && ny <= 128) {
+    if (ctx->use_colblk && ny % 16 == 0 && ny >= 32 && (ny <= 128 || ny == 256)) {
         const int nblk = (ncols + 7) / 8;
         for (int p0 = 0; p0 < n; p0 += KMM_CDERIV_BATCH) {
             const int nb = n - p0 < KMM_CDERIV_BATCH ? n - p0 : KMM_CDERIV_BATCH;
@@ -185,6 +185,7 @@ int kmm_internal_cderiv_many(kmm_ctx *ctx, const double2 *const *f, double2 *con
             case 6: k_cderiv_hw<6><<<grid, 128, 0, ctx->stream>>>(list, ncols, ctx->dyde); break;
             case 7: k_cderiv_hw<7><<<grid, 128, 0, ctx->stream>>>(list, ncols, ctx->dyde); break;
             case 8: k_cderiv_hw<8><<<grid, 128, 0, ctx->stream>>>(list, ncols, ctx->dyde); break;
+            case 16: k_cderiv_hw<16><<<grid, 128, 0, ctx->stream>>>(list, ncols, ctx->dyde); break;
             }
             CKL();
         }

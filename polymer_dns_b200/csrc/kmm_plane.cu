@@ -38,7 +38,7 @@ struct FieldPtrsW { double2 *p[MAXIO]; };
 __host__ __device__ constexpr int fb_len(int nb, int n) { return nb * n + 8 * FB_PAD; }
 
 __device__ __forceinline__ bool fb_compiled(int n) {
-    return n == 48 || n == 64 || n == 96 || n == 128 || n == 144 || n == 192 || n == 256;
+    return n == 48 || n == 64 || n == 96 || n == 128 || n == 144 || n == 192 || n == 256 || n == 576;
 }
 
 // position of element i of sequence c (ct: n is a compiled length)
@@ -64,7 +64,7 @@ __device__ __forceinline__ C *fft_block_ct(C *a, C *b, const C *tw) {
     return r - w;
 }
 
-// the same for the compiled lengths (the 3/2 grids of 32 .. 128 and 2 ny for ny = 32 .. 128), the
+// the same for the compiled lengths (the 3/2 grids of 32 .. 128 and 384, 2 ny for ny = 32 .. 128), the
 // runtime block FFT for any other (FP64 only: the FP32 forms of the mixed precision run at the
 // compiled lengths, which the host checks); blockDim = 256; tw: the table of length n in C
 template <typename C, int S, int NB>
@@ -77,6 +77,7 @@ __device__ C *fft_block(const DevPlan &P, C *a, C *b, const C *tw, int n) {
     case 144: return fft_block_ct<C, 144, S, NB>(a, b, tw);
     case 192: return fft_block_ct<C, 192, S, NB>(a, b, tw);
     case 256: return fft_block_ct<C, 256, S, NB>(a, b, tw);
+    case 576: return fft_block_ct<C, 576, S, NB>(a, b, tw);
     default:
         if constexpr (sizeof(C) == sizeof(double2)) return fft_smem(P, a, b, NB, n, S);
         else return a;
@@ -202,7 +203,7 @@ __device__ __forceinline__ void dct1_half(C *x, C *a, C *b, const C *__restrict_
     __syncwarp();
 }
 
-// k_dct_fwd for ny in {48, 64, 96, 128} with the half-length DCT-I: a warp per column, the
+// k_dct_fwd for ny in {48, 64, 96, 128, 256} with the half-length DCT-I: a warp per column, the
 // block's 8 columns staged in shared memory (column stride N + 1, odd: the transposing store
 // reads 8 columns at one y without bank conflicts)
 template <typename C, int N>
@@ -543,7 +544,43 @@ __global__ void __launch_bounds__(256) k_xinv_big(const double2 *__restrict__ q,
     }
 }
 
-__global__ void __launch_bounds__(256) k_xpoint(const double *__restrict__ pb, double *__restrict__ po,
+// pass 1 at the compiled lengths (MX = 576: nx = 384), in either precision: one warp per (y, z)
+// row and field pair, the Hermitian extension of A + iB (as in k_xphys2) through the compile-time
+// warp FFT, the two real rows stored to the physical buffer in precision C
+#define XBW 4   // rows (warps) per block of k_xinv_big2
+template <int MX, typename C>
+__global__ void __launch_bounds__(XBW * 32) k_xinv_big2(const C *__restrict__ q, typename kct::Real<C>::T *__restrict__ pb,
+                                                        const C *__restrict__ tw, int nin, int nyp, int mz) {
+    typedef typename kct::Real<C>::T T;
+    constexpr int NXH = MX / 3;
+    extern __shared__ double2 smd[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int z = blockIdx.x * XBW + warp, y = blockIdx.y, f = 2 * blockIdx.z, g = f + 1 < nin ? f + 1 : -1;
+    if (z >= mz) return;   // whole warps: no block barrier below
+    C *a = reinterpret_cast<C *>(smd) + (size_t)warp * 2 * MX, *b = a + MX;
+    const C *qa = q + (((size_t)f * nyp + y) * mz + z) * NXH;
+    const C *qb = q + (((size_t)(g >= 0 ? g : f) * nyp + y) * mz + z) * NXH;
+    const C zc = kct::mk<C>((T)0, (T)0);
+    for (int k = NXH + lane; k <= MX - NXH; k += 32) a[swz<C>(k)] = zc;
+    for (int kk = lane; kk < NXH; kk += 32) {
+        C A_ = qa[kk], B_ = g >= 0 ? qb[kk] : zc;
+        if (kk == 0) { A_.y = (T)0; B_.y = (T)0; }   // c2r ignores Im of the mean mode
+        a[swz<C>(kk)] = kct::mk<C>(A_.x - B_.y, A_.y + B_.x);
+        if (kk > 0) a[swz<C>(MX - kk)] = kct::mk<C>(A_.x + B_.y, -A_.y + B_.x);
+    }
+    __syncwarp();
+    const C *r = fft_warp_ct<C, MX, +1, 1, true>(a, b, tw);
+    const size_t nphys = (size_t)nyp * mz * MX, g3 = ((size_t)y * mz + z) * MX;
+    for (int x = lane; x < MX; x += 32) {
+        const C v = r[swz<C>(x)];
+        pb[(size_t)f * nphys + g3 + x] = v.x;
+        if (g >= 0) pb[(size_t)g * nphys + g3 + x] = v.y;
+    }
+}
+
+// pass 2: the pointwise terms from the physical buffer (precision T) into po (precision T)
+template <typename T>
+__global__ void __launch_bounds__(256) k_xpoint(const T *__restrict__ pb, T *__restrict__ po,
                                                 double *__restrict__ drag, double *__restrict__ up3,
                                                 double *__restrict__ vp3, double *__restrict__ wp3,
                                                 const int *__restrict__ imatrix, double *__restrict__ fxi,
@@ -558,7 +595,7 @@ __global__ void __launch_bounds__(256) k_xpoint(const double *__restrict__ pb, d
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nplane; e += (size_t)gridDim.x * blockDim.x) {
         const int z = (int)(e / mx), k = (int)(e - (size_t)z * mx);
         const size_t g3 = (size_t)y * nplane + e;
-        auto in = [&](int sl) { return pb[(size_t)A.slot_of_in[sl] * nphys + g3]; };
+        auto in = [&](int sl) { return (double)pb[(size_t)A.slot_of_in[sl] * nphys + g3]; };
         xphys_point(in, A, sv, y, z, k, nyp, mz, mx, sg, po, drag, up3, vp3, wp3, imatrix, fxi, fyi, fzi, scsource, cmax,
                     umx);
     }
@@ -921,7 +958,7 @@ __global__ void __launch_bounds__(256) k_dct_bwd(const C *__restrict__ pl, const
     }
 }
 
-// k_dct_bwd for ny in {48, 64, 96, 128} with the half-length DCT-I (layout as k_dct_fwd_h)
+// k_dct_bwd for ny in {48, 64, 96, 128, 256} with the half-length DCT-I (layout as k_dct_fwd_h)
 template <typename C, int N>
 __global__ void __launch_bounds__(256) k_dct_bwd_h(const C *__restrict__ pl, const __grid_constant__ FieldPtrsW out, const C *__restrict__ tw,
                                                    int nz, int nxh, int ncols) {
@@ -985,6 +1022,7 @@ static int dct_h_fwd(kmm_ctx *ctx, int nf, const FieldPtrs &in, C *pl, const C *
     case 64: DH(64);
     case 96: DH(96);
     case 128: DH(128);
+    case 256: DH(256);
     default: return KMM_ERR_UNSUPPORTED;
     }
 #undef DH
@@ -1007,6 +1045,7 @@ static int dct_h_bwd(kmm_ctx *ctx, int nf, const C *pl, const FieldPtrsW &out, c
     case 64: DH(64);
     case 96: DH(96);
     case 128: DH(128);
+    case 256: DH(256);
     default: return KMM_ERR_UNSUPPORTED;
     }
 #undef DH
@@ -1309,8 +1348,10 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     RET(kmm_smem_attr(ctx, (const void *)k_zfft_fwd<float2>, sm_z));
     // rows of every input field in shared memory (k_xphys) unless that exceeds the 227 KB limit:
     // then the two-pass x stage through an HBM buffer of the physical inputs (k_xinv_big, k_xpoint)
+    // (always at mx = 576, whose compiled transforms serve the two-pass form in both precisions)
     const bool mx_compiled = mx == 48 || mx == 96 || mx == 144 || mx == 192;
-    const bool xbig = (!mx_compiled && sm_x + 1024 > 227 * 1024) || (ctx->force_xbig && ctx->p.precision == 0);
+    const bool xbig = (!mx_compiled && (sm_x + 1024 > 227 * 1024 || mx == 576)) ||
+                      (ctx->force_xbig && ctx->p.precision == 0);
     if (xbig) {
         RET(ensure_xbig(ctx, nin));
         RET(kmm_smem_attr(ctx, (const void *)k_xinv_big, sm_xf));
@@ -1412,13 +1453,30 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
                     ctx->q_in, ctx->po, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght,
                     ctx->d_cfl, ctx->d_umax, ctx->pmx, A, sv, nyp, mz, mx, nxh);
             } else {
-                k_xinv_big<<<dim3((mz + XZB - 1) / XZB, nyp, (nin + 1) / 2), 256, sm_xf, ctx->stream>>>(
-                    ctx->q_in, ctx->xbig, ctx->pmx, nin, nyp, mz, mx, nxh);
+                const dim3 g1((mz + XBW - 1) / XBW, nyp, (nin + 1) / 2);
+                const size_t sm_b2 = 2 * eb * 2 * XBW * (size_t)mx;
+                if (mx == 576 && f32) {
+                    RET(kmm_smem_attr(ctx, (const void *)k_xinv_big2<576, float2>, sm_b2));
+                    k_xinv_big2<576, float2><<<g1, XBW * 32, sm_b2, ctx->stream>>>(q_in32, (float *)ctx->xbig, tw_mx,
+                                                                                    nin, nyp, mz);
+                } else if (mx == 576) {
+                    RET(kmm_smem_attr(ctx, (const void *)k_xinv_big2<576, double2>, sm_b2));
+                    k_xinv_big2<576, double2><<<g1, XBW * 32, sm_b2, ctx->stream>>>(ctx->q_in, ctx->xbig, ctx->wmx.tw,
+                                                                                     nin, nyp, mz);
+                } else {
+                    k_xinv_big<<<dim3((mz + XZB - 1) / XZB, nyp, (nin + 1) / 2), 256, sm_xf, ctx->stream>>>(
+                        ctx->q_in, ctx->xbig, ctx->pmx, nin, nyp, mz, mx, nxh);
+                }
                 CKL();
                 const int bpp = (int)(((size_t)mz * mx + 255) / 256);
-                k_xpoint<<<dim3(bpp < 64 ? bpp : 64, nyp), 256, 0, ctx->stream>>>(
-                    ctx->xbig, ctx->po, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght,
-                    ctx->d_cfl, ctx->d_umax, A, sv, nyp, mz, mx);
+                if (f32)
+                    k_xpoint<float><<<dim3(bpp < 64 ? bpp : 64, nyp), 256, 0, ctx->stream>>>(
+                        (const float *)ctx->xbig, po32, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource,
+                        ctx->d_seght, ctx->d_cfl, ctx->d_umax, A, sv, nyp, mz, mx);
+                else
+                    k_xpoint<double><<<dim3(bpp < 64 ? bpp : 64, nyp), 256, 0, ctx->stream>>>(
+                        ctx->xbig, ctx->po, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght,
+                        ctx->d_cfl, ctx->d_umax, A, sv, nyp, mz, mx);
             }
             break;
         }
@@ -1465,6 +1523,7 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         case 96: XF2S(96); break;
         case 144: XF2S(144); break;
         case 192: XF2S(192); break;
+        case 576: XF2S(576); break;
         default:
             k_xfwd<<<dim3((mz + XZB - 1) / XZB, nyp), 256, sm_xf, ctx->stream>>>(ctx->po, ctx->q_out, ctx->pmx, nout, nyp,
                                                                                  mz, mx, nxh);

@@ -319,11 +319,11 @@ extern "C" int kmm_step(kmm_ctx *ctx) {
         // the routine path's mixed form runs its transforms at the compiled lengths only; never fall
         // back silently to FP64
         const int ly = 2 * ctx->ny, mz = ctx->mz, mx = ctx->mx;
-        const bool ok_y = ly == 64 || ly == 128 || ly == 192 || ly == 256;
-        const bool ok_z = mz == 48 || mz == 96 || mz == 144 || mz == 192;
-        const bool ok_x = mx == 48 || mx == 96 || mx == 144 || mx == 192;
+        const bool ok_y = ly == 64 || ly == 128 || ly == 192 || ly == 256 || ly == 512;
+        const bool ok_z = mz == 48 || mz == 96 || mz == 144 || mz == 192 || mz == 576;
+        const bool ok_x = mx == 48 || mx == 96 || mx == 144 || mx == 192 || mx == 576;
         if (!(ok_y && ok_z && ok_x)) {
-            kmm_set_error(ctx, "mixed precision needs nx, ny, nz in {32, 64, 96, 128}");
+            kmm_set_error(ctx, "mixed precision needs nx, nz in {32, 64, 96, 128, 384} and ny in {32, 64, 96, 128, 256}");
             return KMM_ERR_UNSUPPORTED;
         }
     }

@@ -217,6 +217,31 @@ def test_cfg5_lengths_match_oracle(rt, oracle_mod, grid):
     o.close()
 
 
+@pytest.mark.parametrize("grid", [(384, 32, 384), (32, 256, 32)])
+def test_cfg5_lengths_mixed_matches_fp64(rt, grid):
+    """The mixed form at the transform lengths of the 384 x 257 x 384 workload: FP32 576-point x
+    (two-pass x stage) and z transforms, and the FP32 half-length DCT-I at ny = 256, against the FP64
+    drop-in from the same inputs after 3 polymer + scalar + IB + tracer steps, 1e-5 relative in the
+    state (the FP64 form itself meets the oracle at these lengths, test_cfg5_lengths_match_oracle)."""
+    nx, ny, nz = grid
+    ctxs = []
+    for prec in (0, 1):
+        p, init, _ = configs.make("cfg5", precision=prec, nx=nx, ny=ny, nz=nz, npart=2000, dt=0.002)
+        f, extra = configs.build_inputs(p, init, "cfg5")
+        g = rt.KmmContext(p)
+        configs.load(f, extra, g.upload)
+        assert g.initial() == 0
+        ctxs.append(g)
+    for _ in range(3):
+        for g in ctxs:
+            assert g.step() == 0
+    for name in ("V", "OMY", "U0", "SCALAR", "C11", "C12", "C33", "FXINTG", "XPART", "YPART"):
+        e = kc.rel_err(ctxs[1].download(name), ctxs[0].download(name))
+        assert e <= 1e-5, "%s rel err %.3e" % (name, e)
+    for g in ctxs:
+        g.close()
+
+
 @pytest.mark.parametrize("prec", [0, 1])
 def test_derived_inputs_match_materialised(rt, prec):
     """vcw3dp inside the routine step forming the x and z derivatives of its inputs in the z inverse
