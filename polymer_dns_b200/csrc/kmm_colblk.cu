@@ -87,22 +87,23 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::fwd) k_bcol_scl(ColF
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ double2 sm[];
     C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
+    double2 *wsm = sm + (size_t)(threadIdx.x >> 5) * 4 * L;   // bload_s / bstore_s scratch (fa's space)
     BPair P;
     if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;   // whole warps: no block barrier below
     const size_t fstride = (size_t)A.nz * A.nxh * col_ld<C>(NYP), yoff = (size_t)P.col * col_ld<C>(NYP);
     const double2 zero = make_double2(0.0, 0.0);
     BCol<K> s, d1;
-    bload<K>(s, A.scal + P.off);
+    bload_s<K>(s, A.scal + P.off, wsm);
     {
         BCol<K> n1, n0;
-        bload<K>(n1, A.scn + P.off);
-        bload<K>(n0, A.scnm1 + P.off);
+        bload_s<K>(n1, A.scn + P.off, wsm);
+        bload_s<K>(n0, A.scnm1 + P.off, wsm);
         bphirhs<K>(s, n1, n0, A.re, A.diff, A.dt, A.th, P.w2, A.dyde, FULL);
     }
     const TauTab ts = tab_at(T, TB_SCL, P.tcol, NYP);
     bsolve_robin<K>(s, ts, zero, zero, P.w2 + T.g[TB_SCL], A.c0, rj, FULL);
     bnorm<K>(s, P.kx, P.j, A.nzh);
-    bstore<K>(A.scal + P.off, s);
+    bstore_s<K>(A.scal + P.off, s, wsm);
     // one column variable live through each transform (the register-resident FFT needs the rest)
     bdct_store<K, C>(s, fa, fb, tw, (C *)A.yp + 6 * fstride + yoff);
     bcderiv<K>(d1, s, A.dyde, FULL);
@@ -118,17 +119,18 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_omy(ColFwdArgs 
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ double2 sm[];
     C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
+    double2 *wsm = sm + (size_t)(threadIdx.x >> 5) * 4 * L;   // bload_s / bstore_s scratch (fa's space)
     BPair P;
     if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;
     const size_t fstride = (size_t)A.nz * A.nxh * col_ld<C>(NYP), yoff = (size_t)P.col * col_ld<C>(NYP);
     const double g1 = A.re / (A.dt * A.th);
     const double2 zero = make_double2(0.0, 0.0);
     BCol<K> om;
-    bload<K>(om, A.omy + P.off);
+    bload_s<K>(om, A.omy + P.off, wsm);
     {
         BCol<K> g1c, g0c;
-        bload<K>(g1c, A.gn + P.off);
-        bload<K>(g0c, A.gnm1 + P.off);
+        bload_s<K>(g1c, A.gn + P.off, wsm);
+        bload_s<K>(g0c, A.gnm1 + P.off, wsm);
         bphirhs<K>(om, g1c, g0c, A.re, 1.0, A.dt, A.th, P.w2, A.dyde, FULL);
     }
     const TauTab to = tab_at(T, TB_OMY, P.tcol, NYP);
@@ -138,7 +140,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_omy(ColFwdArgs 
         for (int m = 0; m <= K; ++m) om.v[m] = zero;
     }
     bnorm<K>(om, P.kx, P.j, A.nzh);
-    bstore<K>(A.omy + P.off, om);
+    bstore_s<K>(A.omy + P.off, om, wsm);
     bdct_store<K, C>(om, fa, fb, tw, (C *)A.yp + 3 * fstride + yoff);
 }
 
@@ -151,6 +153,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_v(ColFwdArgs A,
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ double2 sm[];
     C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
+    double2 *wsm = sm + (size_t)(threadIdx.x >> 5) * 4 * L;   // bload_s / bstore_s scratch (fa's space)
     const int lane = threadIdx.x & 31, h = lane >> 4;
     BPair P;
     if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;
@@ -161,7 +164,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_v(ColFwdArgs A,
     BCol<K> v;
     {
         BCol<K> d1, d2;
-        bload<K>(v, A.v + P.off);
+        bload_s<K>(v, A.v + P.off, wsm);
         bcderiv<K>(d1, v, A.dyde, FULL);
         bcderiv<K>(d2, d1, A.dyde, FULL);
 #pragma unroll
@@ -169,8 +172,8 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_v(ColFwdArgs A,
     }
     {
         BCol<K> f1, f0;
-        bload<K>(f1, A.fn + P.off);
-        bload<K>(f0, A.fnm1 + P.off);
+        bload_s<K>(f1, A.fn + P.off, wsm);
+        bload_s<K>(f0, A.fnm1 + P.off, wsm);
         bphirhs<K>(v, f1, f0, A.re, 1.0, A.dt, A.th, w2, A.dyde, FULL);
     }
     {
@@ -196,13 +199,13 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_v(ColFwdArgs A,
         const double2 c1 = cdiv(csub(cmul(wb, A.dnv2t[P.col]), cmul(wt, A.dnv2b[P.col])), A.denom[P.col]);
         const double2 c2 = cdiv(csub(cmul(wt, A.dnv1b[P.col]), cmul(wb, A.dnv1t[P.col])), A.denom[P.col]);
         BCol<K> gfa;
-        bload<K>(gfa, A.gf1 + P.off);
+        bload_s<K>(gfa, A.gf1 + P.off, wsm);
 #pragma unroll
         for (int m = 0; m <= K; ++m) {
             const double2 a = cmul(c1, gfa.v[m]);
             v.v[m] = make_double2(v.v[m].x + a.x, v.v[m].y + a.y);
         }
-        bload<K>(gfa, A.gf2 + P.off);
+        bload_s<K>(gfa, A.gf2 + P.off, wsm);
 #pragma unroll
         for (int m = 0; m <= K; ++m) {
             const double2 b = cmul(c2, gfa.v[m]);
@@ -252,7 +255,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_v(ColFwdArgs A,
 #pragma unroll
         for (int m = 0; m <= K; ++m) v.v[m] = zero;
     }
-    bstore<K>(A.v + P.off, v);
+    bstore_s<K>(A.v + P.off, v, wsm);
     bdct_store<K, C>(v, fa, fb, tw, (C *)A.yp + 1 * fstride + yoff);
 }
 
@@ -263,6 +266,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::fwd) k_bcol_uw(ColFw
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ double2 sm[];
     C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
+    double2 *wsm = sm + (size_t)(threadIdx.x >> 5) * 4 * L;   // bload_s / bstore_s scratch (fa's space)
     BPair P;
     if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;
     const size_t fstride = (size_t)A.nz * A.nxh * col_ld<C>(NYP), yoff = (size_t)P.col * col_ld<C>(NYP);
@@ -271,8 +275,8 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::fwd) k_bcol_uw(ColFw
     BCol<K> u, w;
     {
         BCol<K> v, om, dv;
-        bload<K>(v, A.v + P.off);
-        bload<K>(om, A.omy + P.off);
+        bload_s<K>(v, A.v + P.off, wsm);
+        bload_s<K>(om, A.omy + P.off, wsm);
         bcderiv<K>(dv, v, A.dyde, FULL);
 #pragma unroll
         for (int m = 0; m <= K; ++m) {
@@ -326,6 +330,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB_BWD) k_bcol_bwd(ColBwdA
     extern __shared__ double2 sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, h = lane >> 4;
     C *fa = reinterpret_cast<C *>(sm + (size_t)warp * 4 * L), *fb = fa + 2 * L;
+    double2 *wsm = sm + (size_t)warp * 4 * L;   // bload_s / bstore_s scratch (fa's space)
     const int npair = A.nz / 2;
     const int pr = blockIdx.x * CB_WARPS + warp;
     if (pr >= A.nxh * npair) return;
@@ -359,7 +364,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB_BWD) k_bcol_bwd(ColBwdA
         bload_dct<K, C>(sc, (const C *)A.yo + (3 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
         bnorm<K>(sc, kx, j, A.nzh);
         filt(sc);
-        bstore<K>(A.scn + off, sc);
+        bstore_s<K>(A.scn + off, sc, wsm);
     }
     if constexpr (sizeof(C) == 16) {
         // one column variable live through each transform: h3 is stored as omz and re-read (from L2)
@@ -369,7 +374,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB_BWD) k_bcol_bwd(ColBwdA
             bload_dct<K, C>(h3, (const C *)A.yo + (2 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
             bnorm<K>(h3, kx, j, A.nzh);
             filt(h3);
-            bstore<K>(A.omz + off, h3);
+            bstore_s<K>(A.omz + off, h3, wsm);
         }
         BCol<K> d;
         {
@@ -378,7 +383,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB_BWD) k_bcol_bwd(ColBwdA
             bnorm<K>(h1, kx, j, A.nzh);
             filt(h1);
             __syncwarp();
-            bload<K>(h3, A.omz + off);
+            bload_s<K>(h3, A.omz + off, wsm);
             // h1n = Re gn(:,1,1), h3n = Re omz(:,1,1) (main_dns.f90:748-751)
             if (kx == 0 && j == 0) {
                 const int t = lane & 15;
@@ -404,22 +409,22 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB_BWD) k_bcol_bwd(ColBwdA
                 const double2 s = make_double2(kzv * h1.v[m].x - kxv * h3.v[m].x, kzv * h1.v[m].y - kxv * h3.v[m].y);
                 h1.v[m] = make_double2(-s.y, s.x);
             }
-            bstore<K>(A.gn + off, h1);
+            bstore_s<K>(A.gn + off, h1, wsm);
             bcderiv<K>(d, tt, A.dyde, FULL);
         }
     #pragma unroll
         for (int m = 0; m <= K; ++m) d.v[m] = make_double2(-d.v[m].x, -d.v[m].y);
-        bstore<K>(A.fn + off, d);
+        bstore_s<K>(A.fn + off, d, wsm);
         BCol<K> h2;
         bload_dct<K, C>(h2, (const C *)A.yo + (1 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
         bnorm<K>(h2, kx, j, A.nzh);
         filt(h2);
         __syncwarp();
-        bload<K>(d, A.fn + off);
+        bload_s<K>(d, A.fn + off, wsm);
         const double w2 = -kxv * kxv - kzv * kzv;
     #pragma unroll
         for (int m = 0; m <= K; ++m) h2.v[m] = make_double2(w2 * h2.v[m].x + d.v[m].x, w2 * h2.v[m].y + d.v[m].y);
-        bstore<K>(A.fn + off, h2);
+        bstore_s<K>(A.fn + off, h2, wsm);
     } else {   // FP32 transforms: the register budget holds h1, h3 and d at once
         BCol<K> h1, h3, d;
         bload_dct<K, C>(h1, (const C *)A.yo + (0 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
@@ -456,8 +461,8 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB_BWD) k_bcol_bwd(ColBwdA
             const double2 s = make_double2(kzv * h1.v[m].x - kxv * h3.v[m].x, kzv * h1.v[m].y - kxv * h3.v[m].y);
             h1.v[m] = make_double2(-s.y, s.x);
         }
-        bstore<K>(A.gn + off, h1);
-        bstore<K>(A.omz + off, h3);
+        bstore_s<K>(A.gn + off, h1, wsm);
+        bstore_s<K>(A.omz + off, h3, wsm);
         BCol<K> h2;
         bload_dct<K, C>(h2, (const C *)A.yo + (1 * ncols + col) * col_ld<C>(NYP), fa, fb, tw);
         bnorm<K>(h2, kx, j, A.nzh);
@@ -465,7 +470,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB_BWD) k_bcol_bwd(ColBwdA
         const double w2 = -kxv * kxv - kzv * kzv;
     #pragma unroll
         for (int m = 0; m <= K; ++m) h2.v[m] = make_double2(w2 * h2.v[m].x - d.v[m].x, w2 * h2.v[m].y - d.v[m].y);
-        bstore<K>(A.fn + off, h2);
+        bstore_s<K>(A.fn + off, h2, wsm);
     }
     (void)h;
 }
@@ -554,6 +559,8 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bsolve(SolveList ul,
                                                                   int nxh, double g, int robin, double c0) {
     constexpr int NYP = 16 * K + 1;
     constexpr unsigned FULL = 0xffffffffu;
+    __shared__ double2 sbuf[CB_WARPS][2 * (16 * K + 8)];
+    double2 *wsm = sbuf[threadIdx.x >> 5];   // bload_s / bstore_s scratch
     double2 *u = ul.u[blockIdx.y];
     BPair P;
     if (!bpair<K>(P, nz, nzh, nxh, wavx, wavz)) return;
@@ -564,11 +571,11 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bsolve(SolveList ul,
     T.tb2 = tb2 + (size_t)P.tcol * NYP;
     T.tf = tf + (size_t)P.tcol * 4;
     BCol<K> s;
-    bload<K>(s, u + P.off);
+    bload_s<K>(s, u + P.off, wsm);
     const double2 gt = gtop[P.col], gb = gbot[P.col];
     if (robin) bsolve_robin<K>(s, T, gt, gb, P.w2 + g, c0, rj, FULL);
     else bsolve_dirichlet<K>(s, T, gt, gb, P.w2 + g, c0, rj, FULL);
-    bstore<K>(u + P.off, s);
+    bstore_s<K>(u + P.off, s, wsm);
 }
 
 int kmm_colblk_solve_many(kmm_ctx *ctx, double2 *const *u, int nf, double g, int robin, double at, double bt,

@@ -14,6 +14,12 @@
 //     pivot / multiplier / border tables the reference's recurrences give (k_tau_tables).
 // Every primitive takes the shuffle mask of the lanes that execute it: the full warp, or one
 // half-warp (the mean-mode column).
+//
+// The tau tables and the tau row reciprocals rj are read in the lane-blocked order (bpos): a
+// column's table holds coefficient P = t K + m (m < K) at m * 16 + t and P = 16 K at 16 K, so the
+// 16 lanes' reads of one slot m are 128 contiguous bytes; the pivot table holds 1 / d(P), the
+// pivots being used only as divisors (the same correctly rounded quotient, formed once when the
+// tables are built).
 #pragma once
 
 #include "kmm_fft.cuh"
@@ -49,6 +55,12 @@ __device__ __forceinline__ int bidx(int m) {
     return m < K ? bl_t() * K + m : 16 * K;
 }
 
+// position of slot m's coefficient in a lane-blocked table
+template <int K>
+__device__ __forceinline__ int bpos(int m) {
+    return m < K ? m * 16 + bl_t() : 16 * K;
+}
+
 template <int K>
 __device__ __forceinline__ void bload(BCol<K> &c, const double2 *__restrict__ p) {
     const int t = bl_t();
@@ -63,6 +75,40 @@ __device__ __forceinline__ void bstore(double2 *__restrict__ p, const BCol<K> &c
 #pragma unroll
     for (int m = 0; m < K; ++m) p[t * K + m] = c.v[m];
     if (t == 15) p[16 * K] = c.v[K];
+}
+
+// bload / bstore through the warp's shared scratch buf (2 (16 K + 8) double2): the 16 lanes of a
+// column move 16 consecutive coefficients per access (256 contiguous bytes) instead of lane-blocked
+// runs 128 B apart, and the blocked layout is formed in shared memory (swizzled rows: both the
+// contiguous and the blocked accesses take the minimum number of wavefronts).  Every lane of the
+// warp takes part; buf is free again on return.
+template <int K>
+__device__ __forceinline__ void bload_s(BCol<K> &c, const double2 *__restrict__ p, double2 *buf) {
+    const int t = bl_t();
+    double2 *b = buf + ((threadIdx.x >> 4) & 1) * (16 * K + 8);
+    double2 r[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) r[j] = p[t + 16 * j];
+    c.v[K] = p[16 * K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) b[swz<double2>(t + 16 * j)] = r[j];
+    __syncwarp();
+#pragma unroll
+    for (int m = 0; m < K; ++m) c.v[m] = b[swz<double2>(t * K + m)];
+    __syncwarp();
+}
+
+template <int K>
+__device__ __forceinline__ void bstore_s(double2 *__restrict__ p, const BCol<K> &c, double2 *buf) {
+    const int t = bl_t();
+    double2 *b = buf + ((threadIdx.x >> 4) & 1) * (16 * K + 8);
+#pragma unroll
+    for (int m = 0; m < K; ++m) b[swz<double2>(t * K + m)] = c.v[m];
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < K; ++j) p[t + 16 * j] = b[swz<double2>(t + 16 * j)];
+    if (t == 15) p[16 * K] = c.v[K];
+    __syncwarp();
 }
 
 // sum over the 16 lanes (every lane gets the total)
@@ -139,7 +185,8 @@ __device__ __forceinline__ void btau_rhs(BCol<K> &s, double c0, const double *__
         const double2 a = m == K ? topm2 : (m >= 2 ? s.v[m - 2] : (m == 0 ? lo0 : lo1));
         const double2 b = s.v[m];
         const double2 c = m == K ? make_double2(0.0, 0.0) : (m + 2 < K ? s.v[m + 2] : (m + 2 == K ? hi0 : hi1));
-        const double rj1 = rj[j], rj2 = rj[NYP + j], rj3 = rj[2 * NYP + j];
+        const int q = bpos<K>(m);
+        const double rj1 = rj[q], rj2 = rj[NYP + q], rj3 = rj[2 * NYP + q];
         double2 w;
         if ((j & 1) == 0) {
             if (j <= NY - 4) {
@@ -184,7 +231,7 @@ __device__ __forceinline__ void bforward(BCol<K> &w, const double *__restrict__ 
 #pragma unroll
     for (int m = K - 1; m >= 0; --m) {
         const int P = t * K + m;
-        const double a = (P < 2 + (m & 1) || P == NY - 1) ? 0.0 : -te[P];
+        const double a = (P < 2 + (m & 1) || P == NY - 1) ? 0.0 : -te[m * 16 + t];
         const double2 W = w.v[m];
         if ((m & 1) == 0) {
             B0 = make_double2(a * B0.x + W.x, a * B0.y + W.y);
@@ -217,7 +264,7 @@ __device__ __forceinline__ void bforward(BCol<K> &w, const double *__restrict__ 
 #pragma unroll
     for (int m = K - 1; m >= 0; --m) {
         const int P = t * K + m;
-        const double a = (P < 2 + (m & 1) || P == NY - 1) ? 0.0 : -te[P];
+        const double a = (P < 2 + (m & 1) || P == NY - 1) ? 0.0 : -te[m * 16 + t];
         double2 &c = (m & 1) ? c1 : c0;
         c = make_double2(a * c.x + w.v[m].x, a * c.y + w.v[m].y);
         w.v[m] = c;
@@ -234,7 +281,7 @@ __device__ __forceinline__ void bborder(const BCol<K> &y, const double *__restri
     for (int m = 0; m < K; ++m) {
         const int P = t * K + m;
         if (P >= 2 + (m & 1)) {
-            const double tv = tb[P];
+            const double tv = tb[m * 16 + t];
             if (m & 1) {
                 ao.x += tv * y.v[m].x;
                 ao.y += tv * y.v[m].y;
@@ -273,8 +320,8 @@ __device__ __forceinline__ void bbacksub(BCol<K> &y, double2 x1e, double2 x1o, c
             am[m] = 0.0;
             b = p ? x1o : x1e;
         } else {
-            const double r = 1.0 / td[P];
-            double a1 = wn * rj[P];
+            const double r = td[m * 16 + t];   // 1 / d(P)
+            double a1 = wn * rj[m * 16 + t];
             if (P == 2) a1 = 2.0 * a1;
             rd[m] = r;
             am[m] = -a1 * r;
@@ -317,7 +364,7 @@ __device__ __forceinline__ void bbacksub(BCol<K> &y, double2 x1e, double2 x1o, c
     }
     // the last coefficient (row n of the even system)
     const double2 xm2 = sh16_idx(mask, y.v[K - 2], 15);
-    const double r = 1.0 / td[NY];
+    const double r = td[NY];
     const double a = -(wn * rj[NY]) * r;
     y.v[K] = make_double2(a * xm2.x + y.v[K].x * r, a * xm2.y + y.v[K].y * r);
 }

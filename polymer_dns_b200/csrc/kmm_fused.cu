@@ -103,6 +103,57 @@ __global__ void k_tau_tables(double *td, double *te, double *tb1, double *tb2, d
 
 
 
+// lane-blocked copy of per-column tables for the blocked column kernels (kmm_colblk.cuh, K = ny / 16):
+// coefficient P = t K + m (m < K) of a column at m * 16 + t, P = 16 K in place; recip stores 1 / v
+__global__ void k_tab_block(const double *__restrict__ src, double *__restrict__ dst, int ncols, int nyp, int K,
+                            int recip) {
+    const size_t n = (size_t)ncols * nyp;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t col = e / nyp;
+        const int P = (int)(e - col * nyp);
+        const int d = P < 16 * K ? (P % K) * 16 + P / K : P;
+        const double v = src[e];
+        dst[col * nyp + d] = recip ? 1.0 / v : v;
+    }
+}
+
+// the blocked copies of one configuration's td (as 1 / d), te, tb1, tb2 (tf is per column, unchanged)
+static int block_tables(kmm_ctx *ctx, const double *const src[4], double *dst[4], int ncols) {
+    const int K = ctx->ny / 16;
+    const size_t n = (size_t)ncols * ctx->nyp;
+    const int nb = (int)((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184);
+    for (int a = 0; a < 4; ++a) {
+        CK(cudaMalloc(&dst[a], sizeof(double) * n));
+        k_tab_block<<<nb, 256, 0, ctx->stream>>>(src[a], dst[a], ncols, ctx->nyp, K, a == 0);
+        CKL();
+    }
+    return KMM_OK;
+}
+
+// the three rj rows (1/(4j(j-1)), 1/(2(j^2-1)), 1/(4j(j+1))) on the host, in natural or lane-blocked order
+static void rj_rows(double *h, int nyp, bool blocked) {
+    const int ny = nyp - 1, K = ny / 16;
+    for (int j = 0; j < 3 * nyp; ++j) h[j] = 0.0;
+    for (int j = 2; j < nyp; ++j) {
+        const int d = (blocked && j < 16 * K) ? (j % K) * 16 + j / K : j;
+        h[d] = 1.0 / (double)(4 * j * (j - 1));
+        h[nyp + d] = 1.0 / (double)(2 * (j * j - 1));
+        h[2 * nyp + d] = 1.0 / (double)(4 * j * (j + 1));
+    }
+}
+
+static int upload_rj(kmm_ctx *ctx, double **out, bool blocked) {
+    const int nyp = ctx->nyp;
+    double *h = (double *)calloc(3 * (size_t)nyp, sizeof(double));
+    if (!h) return KMM_ERR_NOMEM;
+    rj_rows(h, nyp, blocked);
+    cudaError_t e = cudaMalloc(out, sizeof(double) * 3 * nyp);
+    if (e == cudaSuccess) e = cudaMemcpy(*out, h, sizeof(double) * 3 * nyp, cudaMemcpyHostToDevice);
+    free(h);
+    CK(e);
+    return KMM_OK;
+}
+
 // FP32 twiddles exp(-2 pi i m/n), rounded from long double, for the mixed-precision transforms
 static int make_twf(kmm_ctx *ctx, int n, float2 **out) {
     float2 *h = (float2 *)malloc(sizeof(float2) * (size_t)n);
@@ -149,18 +200,18 @@ static int build_tables(kmm_ctx *ctx) {
         CKL();
     }
     // reciprocals of the tau row coefficients (the same divisions as the device's tau_rhs)
-    {
-        const int nyp = ctx->nyp;
-        double *h = (double *)calloc(3 * (size_t)nyp, sizeof(double));
-        for (int j = 2; j < nyp; ++j) {
-            h[j] = 1.0 / (double)(4 * j * (j - 1));
-            h[nyp + j] = 1.0 / (double)(2 * (j * j - 1));
-            h[2 * nyp + j] = 1.0 / (double)(4 * j * (j + 1));
+    RET(upload_rj(ctx, &F->rj, false));
+    if (ctx->ny % 16 == 0) {   // the blocked column kernels' copies
+        for (int c = 0; c < TB_N; ++c) {
+            const int nc = (c == TB_U0 || c == TB_W0) ? 1 : ncols;
+            const double *src[4] = {T.td[c], T.te[c], T.tb1[c], T.tb2[c]};
+            double *dst[4];
+            RET(block_tables(ctx, src, dst, nc));
+            F->btabs.td[c] = dst[0]; F->btabs.te[c] = dst[1]; F->btabs.tb1[c] = dst[2]; F->btabs.tb2[c] = dst[3];
+            F->btabs.tf[c] = T.tf[c];
+            F->btabs.g[c] = T.g[c];
         }
-        cudaError_t e = cudaMalloc(&F->rj, sizeof(double) * 3 * nyp);
-        if (e == cudaSuccess) e = cudaMemcpy(F->rj, h, sizeof(double) * 3 * nyp, cudaMemcpyHostToDevice);
-        free(h);
-        CK(e);
+        RET(upload_rj(ctx, &F->brj, true));
     }
     RET(make_twf(ctx, 2 * ctx->ny, &F->twf_y2));
     RET(make_twf(ctx, ctx->mz, &F->twf_mz));
@@ -181,8 +232,8 @@ static int build_tables(kmm_ctx *ctx) {
 struct TauCache {
     int n;
     TabCfg cfg[KMM_TAU_SETS];
-    double *tabs[KMM_TAU_SETS][5];   // td, te, tb1, tb2, tf
-    double *rj;
+    double *tabs[KMM_TAU_SETS][5];   // td (as 1 / d), te, tb1, tb2 in the lane-blocked order; tf
+    double *rj;                      // lane-blocked rj rows
 };
 
 int kmm_tau_tabset(kmm_ctx *ctx, double g, int robin, double at, double bt, double ab, double bb, const double **tabs,
@@ -192,17 +243,7 @@ int kmm_tau_tabset(kmm_ctx *ctx, double g, int robin, double at, double bt, doub
         C = (TauCache *)calloc(1, sizeof(TauCache));
         if (!C) return KMM_ERR_NOMEM;
         ctx->tauc = C;
-        const int nyp = ctx->nyp;
-        double *h = (double *)calloc(3 * (size_t)nyp, sizeof(double));
-        for (int j = 2; j < nyp; ++j) {
-            h[j] = 1.0 / (double)(4 * j * (j - 1));
-            h[nyp + j] = 1.0 / (double)(2 * (j * j - 1));
-            h[2 * nyp + j] = 1.0 / (double)(4 * j * (j + 1));
-        }
-        cudaError_t e = cudaMalloc(&C->rj, sizeof(double) * 3 * nyp);
-        if (e == cudaSuccess) e = cudaMemcpy(C->rj, h, sizeof(double) * 3 * nyp, cudaMemcpyHostToDevice);
-        free(h);
-        CK(e);
+        RET(upload_rj(ctx, &C->rj, true));
     }
     const TabCfg want = {g, robin, robin ? at : 0.0, robin ? bt : 0.0, robin ? ab : 0.0, robin ? bb : 0.0, 1.0};
     int s = -1;
@@ -217,12 +258,18 @@ int kmm_tau_tabset(kmm_ctx *ctx, double g, int robin, double at, double bt, doub
         s = C->n;
         const int ncols = ctx->nz * ctx->nxh;
         const size_t n = (size_t)ncols * ctx->nyp;
-        for (int a = 0; a < 4; ++a) CK(cudaMalloc(&C->tabs[s][a], sizeof(double) * n));
+        double *canon[4] = {NULL, NULL, NULL, NULL};
+        for (int a = 0; a < 4; ++a) CK(cudaMalloc(&canon[a], sizeof(double) * n));
         CK(cudaMalloc(&C->tabs[s][4], sizeof(double) * 4 * ncols));
-        k_tau_tables<<<(ncols + 127) / 128, 128, 0, ctx->stream>>>(C->tabs[s][0], C->tabs[s][1], C->tabs[s][2],
-                                                                  C->tabs[s][3], C->tabs[s][4], want, ctx->d_wavx,
-                                                                  ctx->d_wavz, ncols, ctx->nz, ctx->nyp, ctx->dyde);
+        k_tau_tables<<<(ncols + 127) / 128, 128, 0, ctx->stream>>>(canon[0], canon[1], canon[2], canon[3],
+                                                                  C->tabs[s][4], want, ctx->d_wavx, ctx->d_wavz,
+                                                                  ncols, ctx->nz, ctx->nyp, ctx->dyde);
         CKL();
+        const double *src[4] = {canon[0], canon[1], canon[2], canon[3]};
+        const int bst = block_tables(ctx, src, C->tabs[s], ncols);
+        CK(cudaStreamSynchronize(ctx->stream));   // once per configuration, before the canonical copies go
+        for (int a = 0; a < 4; ++a) cudaFree(canon[a]);
+        RET(bst);
         C->cfg[s] = want;
         C->n = s + 1;
     }
@@ -261,8 +308,9 @@ void kmm_fused_release(kmm_ctx *ctx) {
     for (int c = 0; c < TB_N; ++c) {
         cudaFree(F->tabs.td[c]); cudaFree(F->tabs.te[c]); cudaFree(F->tabs.tb1[c]); cudaFree(F->tabs.tb2[c]);
         cudaFree(F->tabs.tf[c]);
+        cudaFree(F->btabs.td[c]); cudaFree(F->btabs.te[c]); cudaFree(F->btabs.tb1[c]); cudaFree(F->btabs.tb2[c]);
     }
-    cudaFree(F->yp); cudaFree(F->q); cudaFree(F->r); cudaFree(F->yo); cudaFree(F->rj);
+    cudaFree(F->yp); cudaFree(F->q); cudaFree(F->r); cudaFree(F->yo); cudaFree(F->rj); cudaFree(F->brj);
     cudaFree(F->twf_y2); cudaFree(F->twf_mz); cudaFree(F->twf_mx);
     free(F);
     ctx->fused = NULL;
@@ -1049,7 +1097,7 @@ int kmm_fused_launch(kmm_ctx *ctx) {
     const size_t smc = sizeof(double2) * (64 * (size_t)E + 2 * 2 * 2 * (size_t)ctx->ny);
     const int nblk = (int)(ncols / 2);
     kmm_tic(ctx);
-    int cst = ctx->use_colblk ? kmm_colblk_fwd(ctx, F, FU->tabs, FU->rj, f32 ? (const void *)FU->twf_y2 : (const void *)ctx->wy2.tw, f32)
+    int cst = ctx->use_colblk ? kmm_colblk_fwd(ctx, F, FU->btabs, FU->brj, f32 ? (const void *)FU->twf_y2 : (const void *)ctx->wy2.tw, f32)
                               : KMM_ERR_UNSUPPORTED;
     if (cst != KMM_OK && cst != KMM_ERR_UNSUPPORTED) return cst;
     if (cst == KMM_ERR_UNSUPPORTED) {

@@ -22,8 +22,12 @@ __host__ __device__ __forceinline__ int col_ld(int nyp) { return sizeof(C) == 8 
 
 struct KmmFused {
     FusedTabs tabs;
+    // the same tables and rj rows in the lane-blocked order of the blocked column kernels
+    // (kmm_colblk.cuh), td there holding 1 / d; built where ny is a multiple of 16
+    FusedTabs btabs;
     double2 *yp, *q, *r, *yo;
     double *rj;   // 1/(4j(j-1)), 1/(2(j^2-1)), 1/(4j(j+1)) for j = 0..ny, three rows of nyp
+    double *brj;
     float2 *twf_y2, *twf_mz, *twf_mx;   // FP32 twiddles (mixed precision) of lengths 2 ny, mz, mx
 };
 
