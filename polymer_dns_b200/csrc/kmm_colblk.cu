@@ -8,18 +8,24 @@
 #include "kmm_colblk.cuh"
 
 #define CB_WARPS 4   // column pairs per block
-#define CB_MINB 3    // blocks per SM the register budget is sized for
+#ifndef KMM_CB_MINB
+#define KMM_CB_MINB 3
+#endif
+#define CB_MINB KMM_CB_MINB   // blocks per SM the register budget is sized for
 // blocks per SM for kernels that spill at CB_MINB's register budget: FP64 scalar and u/w kernels
 // and the back kernel run faster with two blocks and no (or little) spilling; the FP32 forms of
 // the scalar and u/w kernels keep three
 #ifndef KMM_CB_MINB_FWD
 #define KMM_CB_MINB_FWD 2
 #endif
-template <typename C> struct CbMinB { static constexpr int fwd = sizeof(C) == 16 ? KMM_CB_MINB_FWD : CB_MINB; };
 #ifndef KMM_CB_MINB_BWD
 #define KMM_CB_MINB_BWD 2
 #endif
-#define CB_MINB_BWD KMM_CB_MINB_BWD
+// the FP32 back kernel runs faster with three blocks per SM, the FP64 one with two
+template <typename C> struct CbMinB {
+    static constexpr int fwd = sizeof(C) == 16 ? KMM_CB_MINB_FWD : CB_MINB;
+    static constexpr int bwd = sizeof(C) == 16 ? KMM_CB_MINB_BWD : 3;
+};
 
 // phirhs on one column (solvers.f90:633-675)
 template <int K>
@@ -324,7 +330,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::fwd) k_bcol_uw(ColFw
 }
 
 template <int K, typename C>
-__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB_BWD) k_bcol_bwd(ColBwdArgs A, const C *__restrict__ tw) {
+__global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::bwd) k_bcol_bwd(ColBwdArgs A, const C *__restrict__ tw) {
     constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ double2 sm[];
