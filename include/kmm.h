@@ -138,6 +138,10 @@ enum kmm_field {
     KMM_WX3D, KMM_WY3D, KMM_WZ3D,
     KMM_U11P3D, KMM_U12P3D, KMM_U13P3D, KMM_U21P3D, KMM_U22P3D, KMM_U23P3D, KMM_U31P3D, KMM_U32P3D, KMM_U33P3D,
     KMM_LUP3D, KMM_LVP3D, KMM_LWP3D, KMM_UOLD, KMM_VOLD, KMM_WOLD, KMM_LUNM1, KMM_LVNM1, KMM_LWNM1,
+    /* the scalar source vcw3dp adds (scsource, solvers.f90:2076-2210): the particle Gaussians of
+     * scl_flag = 2 or the targeted source of scl_flag = 4, 5; written by every vcw3dp with
+     * scl_flag >= 2 */
+    KMM_SCSOURCE,
     KMM_NPHYS_END,
 
     /* integer(4) (nyp,mz,mx) */
@@ -273,6 +277,12 @@ int  kmm_tracer_cells(kmm_ctx *ctx, int *cells, size_t n);
  * keeps only the prognostic fields) into SWIRL3D, and at each particle into SWIRLPART.  The
  * reference evaluates it inside every vcw3dp; here it is called at output cadence.      */
 int  kmm_calcswirl(kmm_ctx *ctx);
+/* The targets of the last scl_flag = 4 source (findmaxQ, helpers.f90:678-953, placed at
+ * solvers.f90:2170-2203): 1-based (x, y, z) grid indices of the 3/2 grid, 3 ints each, in
+ * placement order, into ijk (n ints available).  Returns their number (0 .. 1023), or a negative
+ * status (KMM_ERR_ARG) for bad arguments.  Replaces reading the reference's Qx/Qy/Qz after the
+ * loop; not in the reference's interface.                                                       */
+int  kmm_target_list(kmm_ctx *ctx, int *ijk, int n);
 /* Flow statistics of writeoutputs (helpers.f90:1227-1438) from the current state (runs
  * kmm_veloc first).  prof: 7 * (ny+1) doubles (host) = mean u profile (solvers.f90:3486-3494),
  * u'_rms, v_rms, w_rms, R12 = <u'v>, T12 = <du/dy>/re, and (not in the reference) the kinetic

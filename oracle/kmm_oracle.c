@@ -185,9 +185,11 @@ struct orc_ctx {
     kmm_stats stats;
     fftplan py2, pmz, pmx, pnx, pnz; /* 2*ny (DCT), mz, mx, nx, nz */
     double *cfl;
-    double *scsource; /* (nyp,mz,mx) */
+    double *scsource; /* the KMM_SCSOURCE field's storage */
     int frate_ready;                    /* constant flow rate: W and G built */
     double frate_w[1025], frate_g[1025];
+    int ntarg;                          /* scl_flag = 4: the targets of the last source, 3 ints each */
+    int targ[3 * 1023];
 };
 
 #define SIDX(C, i, j, k) ((((size_t)(k)) * (size_t)(C)->nz + (size_t)(j)) * (size_t)(C)->nyp + (size_t)(i))
@@ -350,7 +352,7 @@ void orc_ctx_destroy(orc_ctx *c)
 {
     if (!c) return;
     for (int f = 0; f < MAXF; ++f) free(c->fld[f]);
-    free(c->wavx); free(c->wavz); free(c->c); free(c->ycoord); free(c->seght); free(c->cfl); free(c->scsource);
+    free(c->wavx); free(c->wavz); free(c->c); free(c->ycoord); free(c->seght); free(c->cfl);
     plan_free(&c->py2); plan_free(&c->pmz); plan_free(&c->pmx); plan_free(&c->pnx); plan_free(&c->pnz);
     free(c);
 }
@@ -1736,11 +1738,181 @@ enum {
 };
 enum { O_GN, O_FN, O_OMZ, O_SCN, O_C11N, O_STR11N = O_C11N + 6, O_QP11 = O_STR11N + 6, O_NOUT = O_QP11 + 6 };
 
+static double swirl_point(double r11, double r12, double r13, double r21, double r22, double r23, double r31,
+                          double r32, double r33);
+static void to_phys3d(orc_ctx *c, const cplx *src, double *phys);
+
+/* ------------------------------------------------------------------------- */
+/* targeted scalar sources (solvers.f90:2164-2206)                            */
+/* ------------------------------------------------------------------------- */
+#define ORC_QN 32768    /* grid_size.f90:2, the length of findmaxQ's candidate list */
+#define ORC_NTARG 1023  /* solvers.f90:2172: targets are added while cnt < 1024 */
+
+/* calcQ (helpers.f90:1519-1552): Q = (rotation - strain) / 2 */
+static double q_point(double u11, double u12, double u13, double u21, double u22, double u23, double u31,
+                      double u32, double u33)
+{
+    const double strain = u11 * u11 + u22 * u22 + u33 * u33;
+    const double rot = -2.0 * (u12 * u21 + u13 * u31 + u23 * u32);
+    return 0.5 * (rot - strain);
+}
+
+/* Shell_Sort (helpers.f90:1557-1594), 1-based as written: increments n/2, then *5/11 (2 -> 1);
+ * b, c, d follow a's moves */
+static void shell_sort(double *a, int *b, int *c, int *d, int n)
+{
+    int inc = n / 2;
+    while (inc > 0) {
+        for (int i = inc + 1; i <= n; ++i) {
+            int j = i;
+            const double t1 = a[i - 1];
+            const int t2 = b[i - 1], t3 = c[i - 1], t4 = d[i - 1];
+            while (j >= inc + 1 && a[j - inc - 1] > t1) {
+                a[j - 1] = a[j - inc - 1];
+                b[j - 1] = b[j - inc - 1];
+                c[j - 1] = c[j - inc - 1];
+                d[j - 1] = d[j - inc - 1];
+                j -= inc;
+            }
+            a[j - 1] = t1;
+            b[j - 1] = t2;
+            c[j - 1] = t3;
+            d[j - 1] = t4;
+        }
+        inc = inc == 2 ? 1 : inc * 5 / 11;
+    }
+}
+
+/* scl_flag = 4 (solvers.f90:2164-2204 with findmaxQ, helpers.f90:678-953): the nine gradients and
+ * the scalar on the 3/2 grid, beta = exp(-alpha_poly |c|), Q (calcQ) negated; the interior grid
+ * minima of -Q that are negative, in the reference's loop order (x outer, then z, y inner) and at
+ * most qn of them; Shell_Sort of the qn-long list; then, walking the sorted list, a Gaussian of
+ * widths sigma around every point with beta > 0.8 until 1023 have been placed.  Where the
+ * reference is undefined the restatement chooses:
+ *   - the scalar enters with its real and imaginary parts (findmaxQ assigns the imaginary part to
+ *     scr, helpers.f90:774, and never sets sci);
+ *   - the list starts from zeros on every call (the reference's Qmin keeps the previous call's
+ *     entries, solvers.f90:1938, whose indices have been reset to 0);
+ *   - the walk stops at the end of the found minima (the reference reads on past them). */
+static void target_findmaxq(orc_ctx *c)
+{
+    const int nyp = c->nyp, mz = c->mz, mx = c->mx, ny = c->ny;
+    const size_t nphys = (size_t)nyp * mz * mx;
+    double *g[9], *sc = malloc(sizeof(double) * nphys), *qc = malloc(sizeof(double) * nphys);
+    for (int m = 0; m < 9; ++m) {
+        g[m] = malloc(sizeof(double) * nphys);
+        to_phys3d(c, SF(c, KMM_U11 + m), g[m]);
+    }
+    to_phys3d(c, SF(c, KMM_SCALAR), sc);
+#pragma omp parallel for
+    for (size_t q = 0; q < nphys; ++q) {
+        qc[q] = -q_point(g[0][q], g[1][q], g[2][q], g[3][q], g[4][q], g[5][q], g[6][q], g[7][q], g[8][q]);
+        sc[q] = exp(-c->p.alpha_poly * fabs(sc[q]));   /* beta */
+    }
+    double *qmin = calloc(ORC_QN, sizeof(double));
+    int *qx = calloc(ORC_QN, sizeof(int)), *qy = calloc(ORC_QN, sizeof(int)), *qz = calloc(ORC_QN, sizeof(int));
+    int cnt = 1;
+#define QC(i, j, k) qc[PIDX(c, (i) - 1, (j) - 1, (k) - 1)]
+    for (int k = 2; k <= mx - 1; ++k)
+        for (int j = 2; j <= mz - 1; ++j)
+            for (int i = 2; i <= ny; ++i) {
+                const double v = QC(i, j, k);
+                if (v < 0 && cnt <= ORC_QN && v < QC(i + 1, j, k) && v < QC(i - 1, j, k) && v < QC(i, j + 1, k) &&
+                    v < QC(i, j - 1, k) && v < QC(i, j, k + 1) && v < QC(i, j, k - 1)) {
+                    qmin[cnt - 1] = v;
+                    qx[cnt - 1] = k;
+                    qy[cnt - 1] = i;
+                    qz[cnt - 1] = j;
+                    ++cnt;
+                }
+            }
+#undef QC
+    shell_sort(qmin, qx, qy, qz, ORC_QN);
+    double *out = c->scsource;
+    memset(out, 0, sizeof(double) * nphys);
+    const double delxm = c->xl / (double)mx, delzm = c->zl / (double)mz;
+    const double sx = c->p.sigmax, sy = c->p.sigmay, sz = c->p.sigmaz, dT = c->p.deltat;
+    c->ntarg = 0;
+    for (int n = 1, placed = 1; placed < ORC_NTARG + 1 && n <= ORC_QN; ++n) {
+        const int kk = qx[n - 1], ii = qy[n - 1], jj = qz[n - 1];
+        if (kk == 0) break;   /* the end of the found minima */
+        if (!(sc[PIDX(c, ii - 1, jj - 1, kk - 1)] > 0.8)) continue;
+        const double xc1 = delxm * (double)(kk - 1), yc1 = c->ycoord[ii - 1], zc1 = delzm * (double)(jj - 1);
+#pragma omp parallel for
+        for (int k = 1; k <= mx; ++k) {
+            const double xsq = pow((double)(k - 1) * delxm - xc1, 2), betax = xsq / (2.0 * sx * sx);
+            if (betax < 18.0)
+                for (int j = 1; j <= mz; ++j) {
+                    const double zsq = pow((double)(j - 1) * delzm - zc1, 2), betaz = zsq / (2.0 * sz * sz);
+                    if (betax + betaz < 18.0)
+                        for (int i = 1; i <= nyp; ++i) {
+                            const double ysq = pow(c->ycoord[i - 1] - yc1, 2), betay = ysq / (2.0 * sy * sy);
+                            if (betax + betay + betaz < 18.0)
+                                out[PIDX(c, i - 1, j - 1, k - 1)] += dT * exp(-(betax + betay + betaz));
+                        }
+                }
+        }
+        c->targ[3 * c->ntarg] = kk;
+        c->targ[3 * c->ntarg + 1] = ii;
+        c->targ[3 * c->ntarg + 2] = jj;
+        ++c->ntarg;
+        ++placed;
+    }
+    for (int m = 0; m < 9; ++m) free(g[m]);
+    free(sc); free(qc); free(qmin); free(qx); free(qy); free(qz);
+}
+
+/* scl_flag = 5 (solvers.f90:2205-2206 with newtarget, helpers.f90:957-1222): the swirl strength of
+ * the 3/2-grid gradients (calcswirl) scaled to [0, 1] by its maximum, then by spts over its volume
+ * integral with the cells' widths Lx, Lz and the half-spacings Ly of the Chebyshev nodes, summed in
+ * the reference's loop order (x outer, z, y inner; the reference leaves scsum unset, 0 here). */
+static void target_newtarget(orc_ctx *c)
+{
+    const int nyp = c->nyp, mz = c->mz, mx = c->mx, ny = c->ny;
+    const size_t nphys = (size_t)nyp * mz * mx;
+    double *g[9];
+    for (int m = 0; m < 9; ++m) {
+        g[m] = malloc(sizeof(double) * nphys);
+        to_phys3d(c, SF(c, KMM_U11 + m), g[m]);
+    }
+    double *out = c->scsource;
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (size_t q = 0; q < nphys; ++q)
+        out[q] = swirl_point(g[0][q], g[1][q], g[2][q], g[3][q], g[4][q], g[5][q], g[6][q], g[7][q], g[8][q]);
+    double qmax = out[0];
+    for (size_t q = 1; q < nphys; ++q)
+        if (out[q] > qmax) qmax = out[q];
+    const double lx = c->xl / (double)mx, lz = c->zl / (double)mz;
+    const double *yc = c->ycoord;
+    double scsum = 0.0;
+    for (int k = 0; k < mx; ++k)
+        for (int j = 0; j < mz; ++j)
+            for (int i = 0; i < nyp; ++i) {
+                double ly;
+                if (i == 0) ly = fabs(yc[1] - yc[0]) / 2.0;
+                else if (i == nyp - 1) ly = fabs(yc[nyp - 1] - yc[ny - 1]) / 2.0;
+                else ly = fabs(yc[i + 1] - yc[i]) / 2.0 + fabs(yc[i] - yc[i - 1]) / 2.0;
+                const size_t q = PIDX(c, i, j, k);
+                out[q] = out[q] / qmax;
+                scsum = scsum + out[q] * lx * ly * lz;
+            }
+    const double var1 = c->p.spts / scsum;
+    for (size_t q = 0; q < nphys; ++q) out[q] = out[q] * var1;
+    for (int m = 0; m < 9; ++m) free(g[m]);
+}
+
+int orc_target_list(orc_ctx *c, int *ijk, int n)
+{
+    if (!c || (n > 0 && !ijk)) return -1;
+    for (int m = 0; m < 3 * c->ntarg && m < n; ++m) ijk[m] = c->targ[m];
+    return c->ntarg;
+}
+
 /* scalar source scl_flag == 2, solvers.f90:2079-2118 */
 static void scalar_source_particles(orc_ctx *c)
 {
     const size_t n = (size_t)c->nyp * c->mz * c->mx;
-    if (!c->scsource) c->scsource = calloc(n, sizeof(double));
+    c->scsource = RF(c, KMM_SCSOURCE);
     double *sc = c->scsource;
     memset(sc, 0, n * sizeof(double));
     const double delxm = c->xl / (double)c->mx, delzm = c->zl / (double)c->mz;
@@ -1782,11 +1954,13 @@ int orc_vcw3dp(orc_ctx *c)
         if (!(t == 0 || t == 1 || t == 3 || t == 4 || t == 11)) return KMM_ERR_UNSUPPORTED;
     }
 
-    /* scalar source, solvers.f90:2076-2166; the targeted sources (scl_flag 4, 5) are not restated */
-    if (scal && c->p.scl_flag >= 4) return KMM_ERR_UNSUPPORTED;
-    if (scal && c->p.scl_flag == 2 && it >= c->p.src_start && it <= c->p.src_stop) scalar_source_particles(c);
+    /* scalar source, solvers.f90:2076-2210: particle Gaussians (2), targeted (4, 5), else zero */
+    const int in_window = it >= c->p.src_start && it <= c->p.src_stop;
+    if (scal && c->p.scl_flag >= 2) c->scsource = RF(c, KMM_SCSOURCE);   /* the field's storage */
+    if (scal && c->p.scl_flag == 2 && in_window) scalar_source_particles(c);
+    else if (scal && c->p.scl_flag == 4 && in_window) target_findmaxq(c);
+    else if (scal && c->p.scl_flag == 5 && in_window) target_newtarget(c);
     else if (scal && c->p.scl_flag >= 2) {
-        if (!c->scsource) c->scsource = calloc((size_t)nyp * mz * mx, sizeof(double));
         memset(c->scsource, 0, sizeof(double) * (size_t)nyp * mz * mx);
     }
 

@@ -87,6 +87,9 @@ int orc_init_part(orc_ctx *c);
 int orc_tracer_cells(orc_ctx *c, int *cells, size_t n);
 /* swirl strength from the closed-form eigenvalues (helpers.f90:197-404) on the last 3/2-grid gradients */
 int orc_calcswirl(orc_ctx *c);
+/* scl_flag = 4: the targets (x, y, z grid indices, 1-based, 3 ints each) the last source was placed
+ * at, in order; returns their number (n: ints available in ijk) */
+int orc_target_list(orc_ctx *c, int *ijk, int n);
 int orc_flowstats(orc_ctx *c, double *prof, double *scal);
 
 #ifdef __cplusplus

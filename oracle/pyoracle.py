@@ -59,6 +59,8 @@ def lib():
         L.orc_flowstats.restype = i
         L.orc_tracer_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_size_t]
         L.orc_tracer_cells.restype = i
+        L.orc_target_list.argtypes = [vp, ctypes.POINTER(ctypes.c_int), i]
+        L.orc_target_list.restype = i
         L.orc_set_threads.argtypes = [i]
         L.orc_set_threads.restype = i
         L.orc_dct1.argtypes = [i, dp, dp]
@@ -174,6 +176,15 @@ class Oracle:
         if st:
             raise RuntimeError("orc_tracer_cells returned %d" % st)
         return cells.reshape(3, self.npart)
+
+    def target_list(self):
+        """orc_target_list: (n, 3) int32 1-based (x, y, z) grid indices of the last scl_flag = 4
+        source's targets, in placement order."""
+        buf = np.zeros(3 * 1023, np.int32)
+        n = self.L.orc_target_list(self.h, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), buf.size)
+        if n < 0:
+            raise RuntimeError("orc_target_list returned %d" % n)
+        return buf[:3 * n].reshape(n, 3)
 
     def flowstats(self):
         """(prof[7][nyp], scal[4]) of orc_flowstats: umean, urms, vrms, wrms, R12, T12, ke profiles;

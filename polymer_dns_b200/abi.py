@@ -85,7 +85,7 @@ MEAN_NAMES = ["U0", "W0", "H1N", "H1NM1", "H3N", "H3NM1", "UXMEAN"]
 WALL_NAMES = ["BCTOP", "BCBOT", "DNV1B", "DNV1T", "DNV2B", "DNV2T", "DENOM", "C1", "C2"]
 PHYS_NAMES = (["FXINTG", "FYINTG", "FZINTG", "UP3D", "VP3D", "WP3D", "SWIRL3D", "WX3D", "WY3D", "WZ3D"]
               + ["U%d%dP3D" % (i, j) for i in (1, 2, 3) for j in (1, 2, 3)]
-              + ["LUP3D", "LVP3D", "LWP3D", "UOLD", "VOLD", "WOLD", "LUNM1", "LVNM1", "LWNM1"])
+              + ["LUP3D", "LVP3D", "LWP3D", "UOLD", "VOLD", "WOLD", "LUNM1", "LVNM1", "LWNM1", "SCSOURCE"])
 PART_NAMES = ["XPART", "YPART", "ZPART", "UPART", "VPART", "WPART", "SWIRLPART"]
 INIT_NAMES = ["INITU", "INITV", "INITW", "INITSCL"]
 

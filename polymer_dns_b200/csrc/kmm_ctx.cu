@@ -346,7 +346,8 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
     for (int w = 0; w < 6; ++w)
         if (ctx->wrk[w]) cudaFree(ctx->wrk[w]);
     void *ptrs[] = {ctx->d_wavx, ctx->d_wavz, ctx->d_c, ctx->d_ycoord, ctx->d_seght, ctx->d_fspread, ctx->d_cfl,
-                    ctx->d_umax, ctx->d_status, ctx->d_tcstat, ctx->d_pumax, ctx->d_scratch, ctx->pl_in, ctx->pl_out, ctx->q_in, ctx->q_out, ctx->scsource};
+                    ctx->d_umax, ctx->d_status, ctx->d_tcstat, ctx->d_pumax, ctx->d_scratch, ctx->pl_in, ctx->pl_out, ctx->q_in, ctx->q_out,
+                    ctx->d_tgtq, ctx->d_tgtc, ctx->d_tgtred, ctx->d_tgtlist, ctx->d_tgtcnt};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i)
         if (ptrs[i]) cudaFree(ptrs[i]);
     for (int s = 0; s < 5; ++s)
@@ -360,6 +361,8 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
     if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     free(ctx->h_wavx); free(ctx->h_wavz); free(ctx->h_c); free(ctx->h_ycoord); free(ctx->h_seght);
+    if (ctx->h_tgtlist) cudaFreeHost(ctx->h_tgtlist);
+    free(ctx->h_targ);
     free(ctx);
     return KMM_OK;
 }

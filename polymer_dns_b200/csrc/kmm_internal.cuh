@@ -79,7 +79,15 @@ struct kmm_ctx {
     double *d_umax;              // scratch for |u| max (per plane)
     double *d_scratch;           // 9*KMM_MAX_NYP doubles for the (0,0)-mode solver
     double *h_pin;               // pinned host: cfl[KMM_MAX_NYP], umax[KMM_MAX_NYP], status (step read-backs)
-    double *scsource;            // (nyp,mz,mx) scalar source (scl_flag = 2)
+    double *scsource;            // the KMM_SCSOURCE field's storage (scl_flag = 2, 4, 5)
+    // targeted sources (scl_flag = 4, 5): -Q on the 3/2 grid, the candidate list and its count,
+    // the placed targets' centres, reduction scratch; the host copy of the last targets
+    double *d_tgtq, *d_tgtc, *d_tgtred;
+    void *d_tgtlist, *h_tgtlist;
+    unsigned *d_tgtcnt;
+    size_t tgt_cap;
+    int ntarg;
+    int *h_targ;                 // 3 * 1023 ints: x, y, z grid indices (1-based) of the targets
     DevPlan py2, pmz, pmx, pnx, pnz;
     DevPlan wy2, wmz, wmx;        // same lengths, radix-8-first factorisation for the warp FFT
     double2 *tw_store[5];

@@ -17,6 +17,9 @@
 // reference's (nyp,mz,mx) arrays.
 #include <math.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "kmm_internal.cuh"
 #include "kmm_fft.cuh"
 #include "kmm_async.cuh"
@@ -1172,6 +1175,8 @@ int kmm_fast_x(kmm_ctx *ctx, const double2 *q, double2 *r, int ic, int nout, boo
                double *vp3, double *wp3);   // kmm_fast.cu
 
 
+int kmm_target_source(kmm_ctx *ctx);
+
 extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     if (!ctx) return KMM_ERR_ARG;
     const int nyp = ctx->nyp, nz = ctx->nz, nxh = ctx->nxh, mx = ctx->mx, mz = ctx->mz;
@@ -1314,16 +1319,16 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         fxi = REAL(ctx, KMM_FXINTG); fyi = REAL(ctx, KMM_FYINTG); fzi = REAL(ctx, KMM_FZINTG);
         im = (int *)kmm_field_ptr(ctx, KMM_IMATRIX);
     }
-    if (scal && ctx->p.scl_flag >= 4) {
-        kmm_set_error(ctx, "scl_flag = %d (targeted scalar source, solvers.f90:2164-2210) is not built", ctx->p.scl_flag);
-        return KMM_ERR_UNSUPPORTED;
-    }
     if (scal && ctx->p.scl_flag >= 2) {
-        // the source array holds only this call's particle Gaussians (zero outside src_start..src_stop)
-        if (!ctx->scsource) CK(cudaMalloc(&ctx->scsource, sizeof(double) * ctx->nphys));
+        // the source array holds only this call's source: the particle Gaussians (scl_flag = 2) or
+        // the targeted source (4, 5) inside src_start..src_stop, zero otherwise (solvers.f90:2076-2210)
+        ctx->scsource = REAL(ctx, KMM_SCSOURCE);   // the field's storage (freed with the fields)
+        if (!ctx->scsource) return KMM_ERR_NOMEM;
         CK(cudaMemsetAsync(ctx->scsource, 0, sizeof(double) * ctx->nphys, ctx->stream));
         const int np = ctx->p.npart;
-        if (ctx->p.scl_flag == 2 && np > 0 && it >= ctx->p.src_start && it <= ctx->p.src_stop) {
+        const bool window = it >= ctx->p.src_start && it <= ctx->p.src_stop;
+        if ((ctx->p.scl_flag == 4 || ctx->p.scl_flag == 5) && window) RET(kmm_target_source(ctx));
+        if (ctx->p.scl_flag == 2 && np > 0 && window) {
             const double *xp = REAL(ctx, KMM_XPART), *yp = REAL(ctx, KMM_YPART), *zp = REAL(ctx, KMM_ZPART);
             if (!xp || !yp || !zp) return KMM_ERR_NOMEM;
             k_scsource<<<(np + 7) / 8, 256, 0, ctx->stream>>>(xp, yp, zp, np, ctx->d_ycoord, ctx->scsource, nyp, mz,
@@ -1734,6 +1739,346 @@ extern "C" int kmm_calcswirl(kmm_ctx *ctx) {
                                                                                             nyp, mz, mx, nxh);
     CKL();
     return ctx->p.npart > 0 ? kmm_swirl_particles(ctx) : KMM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// targeted scalar sources of vcw3dp (solvers.f90:2164-2206)
+//   scl_flag = 4 (findmaxQ, helpers.f90:678-953): Gaussians of widths sigma at the strongest local
+//     maxima of the Q criterion (calcQ, helpers.f90:1519-1552) where the polymer factor
+//     beta = exp(-alpha_poly |c|) exceeds 0.8, at most 1023 of them;
+//   scl_flag = 5 (newtarget, helpers.f90:957-1222): the swirl strength scaled to [0, 1] by its
+//     maximum and then to a volume integral of spts.
+// Where the reference is undefined: the scalar enters findmaxQ with its real and imaginary parts
+// (the reference assigns the imaginary part to scr and never sets sci, helpers.f90:774); the
+// candidate list starts from zeros on every call (the reference's saved Qmin keeps the previous
+// call's values, with indices reset to 0, solvers.f90:1938); the walk over the sorted list stops at
+// the end of the found minima; newtarget's sum starts from 0 (scsum is left unset).
+// ---------------------------------------------------------------------------
+#define TG_QN 32768     // findmaxQ's list length (grid_size.f90:2)
+#define TG_NTARG 1023   // targets placed while cnt < 1024 (solvers.f90:2172)
+
+__device__ __forceinline__ double q_point(double u11, double u12, double u13, double u21, double u22, double u23,
+                                          double u31, double u32, double u33) {
+    const double strain = u11 * u11 + u22 * u22 + u33 * u33;
+    const double rot = -2.0 * (u12 * u21 + u13 * u31 + u23 * u32);
+    return 0.5 * (rot - strain);
+}
+
+// one warp per (y, z) row: Hermitian c2r of the nf inputs in pairs (the nine gradients, and for
+// MODE 4 the scalar), then per x: MODE 5 the swirl into o0; MODE 4 -Q into o0 and beta into o1
+template <int MODE>
+__global__ void __launch_bounds__(SW_WARPS * 32) k_target_x(const double2 *__restrict__ q, double *__restrict__ o0,
+                                                            double *__restrict__ o1, const __grid_constant__ DevPlan P,
+                                                            double alpha_poly, int nyp, int mz, int mx, int nxh) {
+    constexpr int NF = MODE == 4 ? 10 : 9;
+    extern __shared__ double2 sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y = blockIdx.y, z = blockIdx.x * SW_WARPS + warp;
+    if (z >= mz) return;
+    double2 *a = sm + (size_t)warp * (2 * mx + 5 * mx), *b = a + mx;
+    double *ph = (double *)(b + mx);   // [NF][mx]
+    const int hx = mx / 2;
+    for (int f = 0; f < NF; f += 2) {
+        const int g = f + 1;
+        const double2 *qa = q + (((size_t)f * nyp + y) * mz + z) * nxh;
+        const double2 *qb = q + (((size_t)(g < NF ? g : f) * nyp + y) * mz + z) * nxh;
+        for (int k = lane; k < mx; k += 32) {
+            const int kk = k <= hx ? k : mx - k;
+            double2 Av = make_double2(0.0, 0.0), Bv = make_double2(0.0, 0.0);
+            if (kk < nxh) {
+                Av = qa[kk];
+                if (g < NF) Bv = qb[kk];
+            }
+            if (k == 0 || k == hx) { Av.y = 0.0; Bv.y = 0.0; }
+            a[k] = k <= hx ? make_double2(Av.x - Bv.y, Av.y + Bv.x) : make_double2(Av.x + Bv.y, -Av.y + Bv.x);
+        }
+        __syncwarp();
+        const double2 *res = fft_warp(P, a, b, +1);
+        for (int x = lane; x < mx; x += 32) {
+            const double2 v = res[x];
+            ph[(size_t)f * mx + x] = v.x;
+            if (g < NF) ph[(size_t)g * mx + x] = v.y;
+        }
+        __syncwarp();
+    }
+    for (int x = lane; x < mx; x += 32) {
+        const size_t g3 = ((size_t)y * mz + z) * mx + x;
+#define PH(m) ph[(size_t)(m) * mx + x]
+        if (MODE == 5) {
+            o0[g3] = swirl_point(PH(0), PH(1), PH(2), PH(3), PH(4), PH(5), PH(6), PH(7), PH(8));
+        } else {
+            o0[g3] = -q_point(PH(0), PH(1), PH(2), PH(3), PH(4), PH(5), PH(6), PH(7), PH(8));
+            o1[g3] = exp(-alpha_poly * fabs(PH(9)));
+        }
+#undef PH
+    }
+}
+
+// the largest value of a non-negative field (its bit pattern orders like the value): red[0]
+__global__ void k_target_max(const double *__restrict__ f, size_t n, unsigned long long *red) {
+    double m = 0.0;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        m = fmax(m, f[e]);
+    for (int off = 16; off; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+    if ((threadIdx.x & 31) == 0) atomicMax(red, (unsigned long long)__double_as_longlong(m));
+}
+
+// f <- f / fmax in place, and per block the partial volume integral of f Lx Ly Lz (Ly the Chebyshev
+// node's half-spacings, helpers.f90:1198-1210) into part[blockIdx.x]; blocks span whole y-planes
+// in turn so the sum of the partials in block order is deterministic
+#define TG_SUM_THREADS 256
+__global__ void __launch_bounds__(TG_SUM_THREADS) k_target_norm(double *__restrict__ f, const double *__restrict__ red,
+                                                                const double *__restrict__ yc, double *__restrict__ part,
+                                                                int nyp, size_t nplane, double lxlz) {
+    __shared__ double sh[TG_SUM_THREADS / 32];
+    const double fmax_ = red[0];
+    const int ny = nyp - 1;
+    double acc = 0.0;
+    const size_t n = (size_t)nyp * nplane;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e / nplane);
+        double ly;
+        if (i == 0) ly = fabs(yc[1] - yc[0]) / 2.0;
+        else if (i == nyp - 1) ly = fabs(yc[nyp - 1] - yc[ny - 1]) / 2.0;
+        else ly = fabs(yc[i + 1] - yc[i]) / 2.0 + fabs(yc[i] - yc[i - 1]) / 2.0;
+        const double v = f[e] / fmax_;
+        f[e] = v;
+        acc += v * (lxlz * ly);
+    }
+    for (int off = 16; off; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < TG_SUM_THREADS / 32; ++w) t += sh[w];
+        part[blockIdx.x] = t;
+    }
+}
+
+// f <- f * spts / sum(part) (var1, helpers.f90:1213-1220)
+__global__ void k_target_scale(double *__restrict__ f, const double *__restrict__ part, int nparts, size_t n,
+                               double spts) {
+    __shared__ double var1;
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int b = 0; b < nparts; ++b) t += part[b];
+        var1 = spts / t;
+    }
+    __syncthreads();
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        f[e] = f[e] * var1;
+}
+
+// a candidate of findmaxQ: its place in the reference's loop order (x outer, z, y inner over the
+// interior points), -Q and beta there
+struct TgCand {
+    long long order;
+    double q, beta;
+};
+
+// interior grid points (1-based y 2..ny, z 2..mz-1, x 2..mx-1) whose -Q is negative and below all
+// six neighbours: appended to the list (capacity cap; *cnt counts them all)
+__global__ void k_target_minima(const double *__restrict__ nq, const double *__restrict__ beta, TgCand *__restrict__ list,
+                                unsigned *__restrict__ cnt, size_t cap, int nyp, int mz, int mx) {
+    const size_t nplane = (size_t)mz * mx, n = (size_t)nyp * nplane;
+    const int ny = nyp - 1;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e / nplane), r = (int)(e - (size_t)i * nplane), j = r / mx, k = r - j * mx;   // 0-based
+        if (i < 1 || i > ny - 1 || j < 1 || j > mz - 2 || k < 1 || k > mx - 2) continue;
+        const double v = nq[e];
+        if (!(v < 0.0)) continue;
+        if (v < nq[e + nplane] && v < nq[e - nplane] && v < nq[e + mx] && v < nq[e - mx] && v < nq[e + 1] &&
+            v < nq[e - 1]) {
+            const unsigned s = atomicAdd(cnt, 1u);
+            if (s < cap) {
+                TgCand c;
+                c.order = ((long long)(k - 1) * (mz - 2) + (j - 1)) * (long long)(ny - 1) + (i - 1);
+                c.q = v;
+                c.beta = beta[e];
+                list[s] = c;
+            }
+        }
+    }
+}
+
+// the source of the placed targets: per point, every target's Gaussian in placement order with the
+// reference's cut-offs (solvers.f90:2177-2200), so each point's sum has the reference's order
+__global__ void k_target_deposit(double *__restrict__ sc, const double *__restrict__ tc, int nt,
+                                 const double *__restrict__ ycoord, int nyp, int mz, int mx, double delxm, double delzm,
+                                 double sx, double sy, double sz, double dT) {
+    const size_t nplane = (size_t)mz * mx, n = (size_t)nyp * nplane;
+    const double ax = 2.0 * sx * sx, ay = 2.0 * sy * sy, az = 2.0 * sz * sz;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e / nplane), r = (int)(e - (size_t)i * nplane), j = r / mx, k = r - j * mx;
+        const double xk = (double)k * delxm, zj = (double)j * delzm, yi = ycoord[i];
+        double acc = 0.0;
+        for (int t = 0; t < nt; ++t) {
+            const double dx = xk - tc[3 * t], betax = dx * dx / ax;
+            if (!(betax < 18.0)) continue;
+            const double dz = zj - tc[3 * t + 2], betaz = dz * dz / az;
+            if (!(betax + betaz < 18.0)) continue;
+            const double dy = yi - tc[3 * t + 1], betay = dy * dy / ay;
+            if (betax + betay + betaz < 18.0) acc += dT * exp(-(betax + betay + betaz));
+        }
+        sc[e] = acc;
+    }
+}
+
+// Shell_Sort of findmaxQ's list (helpers.f90:1557-1594): the reference's increments (n / 2, then
+// * 5 / 11, 2 -> 1), which decide the order of equal values; b, c, d, e follow a's moves
+static void tg_shell_sort(double *a, int *b, int *c, int *d, double *e, int n) {
+    int inc = n / 2;
+    while (inc > 0) {
+        for (int i = inc; i < n; ++i) {
+            int j = i;
+            const double t1 = a[i], t5 = e[i];
+            const int t2 = b[i], t3 = c[i], t4 = d[i];
+            while (j >= inc && a[j - inc] > t1) {
+                a[j] = a[j - inc]; b[j] = b[j - inc]; c[j] = c[j - inc]; d[j] = d[j - inc]; e[j] = e[j - inc];
+                j -= inc;
+            }
+            a[j] = t1; b[j] = t2; c[j] = t3; d[j] = t4; e[j] = t5;
+        }
+        inc = inc == 2 ? 1 : inc * 5 / 11;
+    }
+}
+
+// the scalar source of scl_flag 4 or 5 into ctx->scsource (the caller zeroes it outside the
+// source window); the nine gradients U11..U33 are current
+int kmm_target_source(kmm_ctx *ctx) {
+    const int flag = ctx->p.scl_flag;
+    const int nyp = ctx->nyp, nz = ctx->nz, nxh = ctx->nxh, mz = ctx->mz, mx = ctx->mx;
+    const int ncols = nz * nxh, nf = flag == 4 ? 10 : 9;
+    const size_t nphys = ctx->nphys, nplane = (size_t)mz * mx;
+    FieldPtrs in;
+    for (int m = 0; m < 9; ++m) {
+        in.p[m] = SPEC(ctx, KMM_U11 + m);
+        if (!in.p[m]) return KMM_ERR_NOMEM;
+    }
+    if (flag == 4) {
+        in.p[9] = SPEC(ctx, KMM_SCALAR);
+        if (!in.p[9]) return KMM_ERR_NOMEM;
+    }
+    RET(kmm_ensure_plane_buffers(ctx, nf, 0));
+    if (!ctx->d_tgtred) CK(cudaMalloc(&ctx->d_tgtred, sizeof(double) * 2048));
+    const size_t sm_dct = sizeof(double2) * 2 * (size_t)fb_len(DCT_CB, 2 * ctx->ny);
+    const size_t sm_z = sizeof(double2) * 2 * (size_t)fb_len(ZKB, mz);
+    const size_t sm_s = sizeof(double2) * (size_t)SW_WARPS * 7 * mx;
+    RET(kmm_smem_attr(ctx, (const void *)k_dct_fwd<double2>, sm_dct));
+    RET(kmm_smem_attr(ctx, (const void *)k_zfft_bwd<double2>, sm_z));
+    k_dct_fwd<double2><<<dim3((ncols + DCT_CB - 1) / DCT_CB, nf), 256, sm_dct, ctx->stream>>>(in, ctx->pl_in, ctx->py2,
+                                                                                                ctx->py2.tw, nyp, nz,
+                                                                                                nxh, ncols);
+    CKL();
+    ZRecipe zr;
+    for (int m = 0; m < nf; ++m) {
+        zr.base[m] = (unsigned char)m;
+        zr.mult[m] = 0;
+    }
+    k_zfft_bwd<double2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nf), 256, sm_z, ctx->stream>>>(
+        ctx->pl_in, ctx->q_in, ctx->pmz, ctx->pmz.tw, nyp, nz, nxh, mz, zr, ctx->d_wavx, ctx->d_wavz);
+    CKL();
+    const dim3 gx((mz + SW_WARPS - 1) / SW_WARPS, nyp);
+    const int nb = (int)((nphys + 255) / 256 < 2048 ? (nphys + 255) / 256 : 2048);
+    if (flag == 5) {
+        RET(kmm_smem_attr(ctx, (const void *)k_target_x<5>, sm_s));
+        k_target_x<5><<<gx, SW_WARPS * 32, sm_s, ctx->stream>>>(ctx->q_in, ctx->scsource, NULL, ctx->wmx, 0.0, nyp, mz,
+                                                               mx, nxh);
+        CKL();
+        CK(cudaMemsetAsync(ctx->d_tgtred, 0, sizeof(double), ctx->stream));
+        k_target_max<<<nb, 256, 0, ctx->stream>>>(ctx->scsource, nphys, (unsigned long long *)ctx->d_tgtred);
+        CKL();
+        const int npart = nb < 2047 ? nb : 2047;
+        k_target_norm<<<npart, TG_SUM_THREADS, 0, ctx->stream>>>(ctx->scsource, ctx->d_tgtred, ctx->d_ycoord,
+                                                                 ctx->d_tgtred + 1, nyp, nplane,
+                                                                 (ctx->xl / (double)mx) * (ctx->zl / (double)mz));
+        CKL();
+        k_target_scale<<<nb, 256, 0, ctx->stream>>>(ctx->scsource, ctx->d_tgtred + 1, npart, nphys, ctx->p.spts);
+        CKL();
+        return KMM_OK;
+    }
+    // scl_flag = 4: -Q into d_tgtq, beta into the source array (overwritten by the deposit below)
+    if (!ctx->d_tgtq) CK(cudaMalloc(&ctx->d_tgtq, sizeof(double) * nphys));
+    if (!ctx->d_tgtcnt) CK(cudaMalloc(&ctx->d_tgtcnt, sizeof(unsigned)));
+    if (!ctx->d_tgtc) CK(cudaMalloc(&ctx->d_tgtc, sizeof(double) * 3 * TG_NTARG));
+    if (!ctx->h_targ) {
+        ctx->h_targ = (int *)calloc(3 * TG_NTARG, sizeof(int));
+        if (!ctx->h_targ) return KMM_ERR_NOMEM;
+    }
+    if (!ctx->d_tgtlist) {
+        const size_t cap = nphys < ((size_t)1 << 22) ? nphys : ((size_t)1 << 22);
+        CK(cudaMalloc(&ctx->d_tgtlist, sizeof(TgCand) * cap));
+        CK(cudaMallocHost(&ctx->h_tgtlist, sizeof(TgCand) * cap));
+        ctx->tgt_cap = cap;
+    }
+    RET(kmm_smem_attr(ctx, (const void *)k_target_x<4>, sm_s));
+    k_target_x<4><<<gx, SW_WARPS * 32, sm_s, ctx->stream>>>(ctx->q_in, ctx->d_tgtq, ctx->scsource, ctx->wmx,
+                                                           ctx->p.alpha_poly, nyp, mz, mx, nxh);
+    CKL();
+    CK(cudaMemsetAsync(ctx->d_tgtcnt, 0, sizeof(unsigned), ctx->stream));
+    k_target_minima<<<nb, 256, 0, ctx->stream>>>(ctx->d_tgtq, ctx->scsource, (TgCand *)ctx->d_tgtlist, ctx->d_tgtcnt,
+                                                 ctx->tgt_cap, nyp, mz, mx);
+    CKL();
+    unsigned *hcnt = (unsigned *)kmm_h_pin_status(ctx);   // the pinned status word, free until the x stage
+    CK(cudaMemcpyAsync(hcnt, ctx->d_tgtcnt, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const size_t found = *hcnt;
+    if (found > ctx->tgt_cap) {
+        kmm_set_error(ctx, "scl_flag = 4: %zu candidate minima exceed the list capacity %zu", found, ctx->tgt_cap);
+        return KMM_ERR_UNSUPPORTED;
+    }
+    TgCand *hl = (TgCand *)ctx->h_tgtlist;
+    if (found) {
+        CK(cudaMemcpyAsync(hl, ctx->d_tgtlist, sizeof(TgCand) * found, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    // the first qn minima in the reference's loop order, then its sort of the qn-long list
+    std::sort(hl, hl + found, [](const TgCand &a, const TgCand &b) { return a.order < b.order; });
+    const int nkeep = found < TG_QN ? (int)found : TG_QN;
+    std::vector<double> qv(TG_QN, 0.0), bv(TG_QN, 0.0);
+    std::vector<int> qx(TG_QN, 0), qy(TG_QN, 0), qz(TG_QN, 0);
+    const int ny = ctx->ny;
+    for (int c = 0; c < nkeep; ++c) {
+        const long long o = hl[c].order;
+        const int i = (int)(o % (ny - 1)), jk = (int)(o / (ny - 1)), j = jk % (mz - 2), k = jk / (mz - 2);
+        qv[c] = hl[c].q;
+        bv[c] = hl[c].beta;
+        qx[c] = k + 2;   // 1-based x, y, z indices (the reference's Qx, Qy, Qz)
+        qy[c] = i + 2;
+        qz[c] = j + 2;
+    }
+    tg_shell_sort(qv.data(), qx.data(), qy.data(), qz.data(), bv.data(), TG_QN);
+    double *hc = (double *)malloc(sizeof(double) * 3 * TG_NTARG);
+    if (!hc) return KMM_ERR_NOMEM;
+    const double delxm = ctx->xl / (double)mx, delzm = ctx->zl / (double)mz;
+    int nt = 0;
+    for (int n = 0; n < TG_QN && nt < TG_NTARG; ++n) {
+        if (qx[n] == 0) break;   // the end of the found minima
+        if (!(bv[n] > 0.8)) continue;
+        hc[3 * nt] = delxm * (double)(qx[n] - 1);
+        hc[3 * nt + 1] = ctx->h_ycoord[qy[n] - 1];
+        hc[3 * nt + 2] = delzm * (double)(qz[n] - 1);
+        ctx->h_targ[3 * nt] = qx[n];
+        ctx->h_targ[3 * nt + 1] = qy[n];
+        ctx->h_targ[3 * nt + 2] = qz[n];
+        ++nt;
+    }
+    ctx->ntarg = nt;
+    cudaError_t e = nt ? cudaMemcpyAsync(ctx->d_tgtc, hc, sizeof(double) * 3 * nt, cudaMemcpyHostToDevice, ctx->stream)
+                       : cudaSuccess;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);   // hc is pageable and freed next
+    free(hc);
+    CK(e);
+    k_target_deposit<<<nb, 256, 0, ctx->stream>>>(ctx->scsource, ctx->d_tgtc, nt, ctx->d_ycoord, nyp, mz, mx, delxm,
+                                                  delzm, ctx->p.sigmax, ctx->p.sigmay, ctx->p.sigmaz, ctx->p.deltat);
+    CKL();
+    return KMM_OK;
+}
+
+extern "C" int kmm_target_list(kmm_ctx *ctx, int *ijk, int n) {
+    if (!ctx || n < 0 || (n > 0 && !ijk)) return -KMM_ERR_ARG;
+    for (int m = 0; m < 3 * ctx->ntarg && m < n; ++m) ijk[m] = ctx->h_targ[m];
+    return ctx->ntarg;
 }
 
 // ---------------------------------------------------------------------------

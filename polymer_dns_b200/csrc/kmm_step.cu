@@ -304,9 +304,11 @@ extern "C" int kmm_initial(kmm_ctx *ctx) {
 
 // vcw3dp inside the routine step forms the x and z derivatives among its inputs in its z inverse
 // (KMM_OPT_DERIVED_INPUTS, default 1), except where inertial particles need the materialised
-// velocity gradient and Laplacian on the 3/2 grid
+// velocity gradient and Laplacian on the 3/2 grid, or the targeted scalar sources the spectral
+// velocity gradient U11..U33
 bool kmm_derived_inputs(const kmm_ctx *ctx) {
-    return ctx->use_derived && !(ctx->p.particle_flag > 0 && ctx->p.npart > 0);
+    return ctx->use_derived && !(ctx->p.particle_flag > 0 && ctx->p.npart > 0) &&
+           !(ctx->p.scalar_on && (ctx->p.scl_flag == 4 || ctx->p.scl_flag == 5));
 }
 
 // ---------------------------------------------------------------------------
@@ -423,8 +425,10 @@ extern "C" int kmm_step(kmm_ctx *ctx) {
             RET(norm_ids(ctx, l, 3));
         }
     }
-    if (ctx->p.polymer_on || ctx->p.particle_flag > 0) {
-        // the velocity gradient / Laplacian feed only the polymer terms and inertial particles
+    const bool targeted = ctx->p.scalar_on && (ctx->p.scl_flag == 4 || ctx->p.scl_flag == 5);
+    if (ctx->p.polymer_on || ctx->p.particle_flag > 0 || targeted) {
+        // the velocity gradient / Laplacian feed only the polymer terms, inertial particles and the
+        // targeted scalar sources (the reference computes them every step, main_dns.f90:544)
         if (derived) {
             RET(want_dy(KMM_U, KMM_U12));
             RET(want_dy(KMM_V, KMM_U22));

@@ -79,6 +79,8 @@ def lib():
         L.kmm_tracer_cells.restype = ctypes.c_int
         L.kmm_wait_selftest.argtypes = [vp, ctypes.c_double]
         L.kmm_wait_selftest.restype = ctypes.c_int
+        L.kmm_target_list.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        L.kmm_target_list.restype = ctypes.c_int
         for name, sig in _ROUTINES.items():
             f = getattr(L, "kmm_" + name)
             f.argtypes = [vp] + [_CT[c] for c in sig]
@@ -92,7 +94,8 @@ def exported_symbols():
     base = ["kmm_ctx_create", "kmm_ctx_destroy", "kmm_last_error", "kmm_abi_version", "kmm_field_size",
             "kmm_upload", "kmm_download", "kmm_get_stats", "kmm_set_timing", "kmm_get_stage_times",
             "kmm_launch_count", "kmm_event_record", "kmm_event_elapsed", "kmm_xyzfft_noalloc", "kmm_flowstats",
-            "kmm_ensemble_step", "kmm_ensemble_run", "kmm_tracer_cells", "kmm_wait_selftest"]
+            "kmm_ensemble_step", "kmm_ensemble_run", "kmm_tracer_cells", "kmm_wait_selftest",
+            "kmm_target_list"]
     return base + ["kmm_" + n for n in _ROUTINES]
 
 
@@ -218,6 +221,15 @@ class KmmContext:
         self._check(self.L.kmm_tracer_cells(self.h, cells.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), cells.size),
                     "kmm_tracer_cells")
         return cells.reshape(3, self.npart)
+
+    def target_list(self):
+        """kmm_target_list: (n, 3) int32 1-based (x, y, z) grid indices of the last scl_flag = 4
+        source's targets, in placement order."""
+        buf = np.zeros(3 * 1023, np.int32)
+        n = int(self.L.kmm_target_list(self.h, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), buf.size))
+        if n < 0:
+            raise KmmError(-n, "kmm_target_list")
+        return buf[:3 * n].reshape(n, 3)
 
     def wait_selftest(self, limit_ms):
         """kmm_wait_selftest: status of a bounded wait on a barrier nothing arrives on

@@ -580,14 +580,6 @@ def test_particle_scalar_source_matches_oracle(rt, oracle_mod):
     for name in ["SCALAR", "SCN", "SCNM1", "V", "XPART", "ZPART"]:
         _cmp(g, o, name, RUN_TOL)
     assert np.abs(g.download("SCALAR")).max() > 1e-3   # the source did act
-    # the targeted sources are not built: both report it instead of running without them
-    q = kc.cfg_small(16, 32, 16, scalar_on=1, diff=1.0, scl_flag=4)
-    g2, o2 = _pair(rt, oracle_mod, q)
-    f2 = kc.initial_fields(q, amp=0.05, seed=1)
-    for c in (g2, o2):
-        kc.load_initial(c, q, f2, np.zeros_like(f2[0]))
-    assert o2.initial() == abi.ERR_UNSUPPORTED
-    assert g2.call("initial", allow=(abi.ERR_UNSUPPORTED,)) == abi.ERR_UNSUPPORTED
 
 
 @pytest.mark.parametrize("variant", ["polymer_ib", "inertial", "routine_plain"])
