@@ -12,19 +12,35 @@
 #define KMM_CB_MINB 3
 #endif
 #define CB_MINB KMM_CB_MINB   // blocks per SM the register budget is sized for
-// blocks per SM for kernels that spill at CB_MINB's register budget: FP64 scalar and u/w kernels
-// and the back kernel run faster with two blocks and no (or little) spilling; the FP32 forms of
-// the scalar and u/w kernels keep three
+// blocks per SM for the FP64 kernels that spill at CB_MINB's register budget: the scalar and u/w
+// kernels and the back kernel run faster with two blocks and no (or little) spilling
 #ifndef KMM_CB_MINB_FWD
 #define KMM_CB_MINB_FWD 2
 #endif
 #ifndef KMM_CB_MINB_BWD
 #define KMM_CB_MINB_BWD 2
 #endif
-// the FP32 back kernel runs faster with three blocks per SM, the FP64 one with two
+// blocks per SM each kernel's register budget is sized for, as measured per kernel: FP64 scalar,
+// u/w and back kernels two, v and omega_y three; in FP32 the scalar, u/w and omega_y kernels
+// four, v and the back kernel three
 template <typename C> struct CbMinB {
-    static constexpr int fwd = sizeof(C) == 16 ? KMM_CB_MINB_FWD : CB_MINB;
-    static constexpr int bwd = sizeof(C) == 16 ? KMM_CB_MINB_BWD : 3;
+    static constexpr bool f64 = sizeof(C) == 16;
+    static constexpr int fwd = f64 ? KMM_CB_MINB_FWD : 4;   // k_bcol_scl, k_bcol_uw
+    static constexpr int omy = f64 ? CB_MINB : 4;
+    static constexpr int v = CB_MINB;
+    static constexpr int bwd = f64 ? KMM_CB_MINB_BWD : 3;
+};
+
+// shared memory of one warp: region A holds the bload_s / bstore_s scratch (2 (NY + 8) double2)
+// and bdct_store / bload_dct's natural-order column pair (2 (NY + 8) elements of C, within the
+// swizzled rows); region B the DCT passes' transpose buffer (2 N = 4 NY elements of C).  A's size
+// is a multiple of 128 bytes, so B's swizzled rows keep their bank alignment.
+template <int K, typename C>
+struct CbSmem {
+    static constexpr size_t a_bytes = 2 * (16 * K + 8) * sizeof(double2);
+    static constexpr size_t b_bytes = 4 * 16 * K * sizeof(C);
+    static constexpr size_t warp_bytes = a_bytes + b_bytes;
+    static_assert(a_bytes % 128 == 0, "region B starts on a 128-byte boundary");
 };
 
 // phirhs on one column (solvers.f90:633-675)
@@ -89,11 +105,12 @@ __device__ __forceinline__ bool bpair(BPair &P, int nz, int nzh, int nxh, const 
 template <int K, typename C>
 __global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::fwd) k_bcol_scl(ColFwdArgs A, FusedTabs T, const double *__restrict__ rj,
                                                             const C *__restrict__ tw) {
-    constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
+    constexpr int NY = 16 * K, NYP = NY + 1;
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ double2 sm[];
-    C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
-    double2 *wsm = sm + (size_t)(threadIdx.x >> 5) * 4 * L;   // bload_s / bstore_s scratch (fa's space)
+    char *wreg = reinterpret_cast<char *>(sm) + (size_t)(threadIdx.x >> 5) * CbSmem<K, C>::warp_bytes;
+    C *fa = reinterpret_cast<C *>(wreg), *fb = reinterpret_cast<C *>(wreg + CbSmem<K, C>::a_bytes);
+    double2 *wsm = reinterpret_cast<double2 *>(wreg);   // bload_s / bstore_s scratch (fa's space)
     BPair P;
     if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;   // whole warps: no block barrier below
     const size_t fstride = (size_t)A.nz * A.nxh * col_ld<C>(NYP), yoff = (size_t)P.col * col_ld<C>(NYP);
@@ -119,13 +136,14 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::fwd) k_bcol_scl(ColF
 // normal vorticity (main_dns.f90:411-422, 479-484, 500-502, 520-526): phirhs, Robin solve, zero
 // on the mean column, norm, store; y-physical omega_y
 template <int K, typename C>
-__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_omy(ColFwdArgs A, FusedTabs T, const double *__restrict__ rj,
+__global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::omy) k_bcol_omy(ColFwdArgs A, FusedTabs T, const double *__restrict__ rj,
                                                             const C *__restrict__ tw) {
-    constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
+    constexpr int NY = 16 * K, NYP = NY + 1;
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ double2 sm[];
-    C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
-    double2 *wsm = sm + (size_t)(threadIdx.x >> 5) * 4 * L;   // bload_s / bstore_s scratch (fa's space)
+    char *wreg = reinterpret_cast<char *>(sm) + (size_t)(threadIdx.x >> 5) * CbSmem<K, C>::warp_bytes;
+    C *fa = reinterpret_cast<C *>(wreg), *fb = reinterpret_cast<C *>(wreg + CbSmem<K, C>::a_bytes);
+    double2 *wsm = reinterpret_cast<double2 *>(wreg);   // bload_s / bstore_s scratch (fa's space)
     BPair P;
     if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;
     const size_t fstride = (size_t)A.nz * A.nxh * col_ld<C>(NYP), yoff = (size_t)P.col * col_ld<C>(NYP);
@@ -153,13 +171,14 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_omy(ColFwdArgs 
 // wall-normal velocity (main_dns.f90:363-407, 426-466, 489-502, 520): phi, phirhs, Helmholtz and
 // Poisson solves, influence-matrix correction, uzero for the mean modes, norm, store; y-physical v
 template <int K, typename C>
-__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_v(ColFwdArgs A, FusedTabs T, const double *__restrict__ rj,
+__global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::v) k_bcol_v(ColFwdArgs A, FusedTabs T, const double *__restrict__ rj,
                                                           const C *__restrict__ tw) {
-    constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
+    constexpr int NY = 16 * K, NYP = NY + 1;
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ double2 sm[];
-    C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
-    double2 *wsm = sm + (size_t)(threadIdx.x >> 5) * 4 * L;   // bload_s / bstore_s scratch (fa's space)
+    char *wreg = reinterpret_cast<char *>(sm) + (size_t)(threadIdx.x >> 5) * CbSmem<K, C>::warp_bytes;
+    C *fa = reinterpret_cast<C *>(wreg), *fb = reinterpret_cast<C *>(wreg + CbSmem<K, C>::a_bytes);
+    double2 *wsm = reinterpret_cast<double2 *>(wreg);   // bload_s / bstore_s scratch (fa's space)
     const int lane = threadIdx.x & 31, h = lane >> 4;
     BPair P;
     if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;
@@ -268,11 +287,12 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB) k_bcol_v(ColFwdArgs A,
 // veloc (solvers.f90:1576-1659) from the new v and omega_y; y-physical u, du/dy, w, dw/dy
 template <int K, typename C>
 __global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::fwd) k_bcol_uw(ColFwdArgs A, const C *__restrict__ tw) {
-    constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
+    constexpr int NY = 16 * K, NYP = NY + 1;
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ double2 sm[];
-    C *fa = reinterpret_cast<C *>(sm + (size_t)(threadIdx.x >> 5) * 4 * L), *fb = fa + 2 * L;
-    double2 *wsm = sm + (size_t)(threadIdx.x >> 5) * 4 * L;   // bload_s / bstore_s scratch (fa's space)
+    char *wreg = reinterpret_cast<char *>(sm) + (size_t)(threadIdx.x >> 5) * CbSmem<K, C>::warp_bytes;
+    C *fa = reinterpret_cast<C *>(wreg), *fb = reinterpret_cast<C *>(wreg + CbSmem<K, C>::a_bytes);
+    double2 *wsm = reinterpret_cast<double2 *>(wreg);   // bload_s / bstore_s scratch (fa's space)
     BPair P;
     if (!bpair<K>(P, A.nz, A.nzh, A.nxh, A.wavx, A.wavz)) return;
     const size_t fstride = (size_t)A.nz * A.nxh * col_ld<C>(NYP), yoff = (size_t)P.col * col_ld<C>(NYP);
@@ -331,12 +351,13 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::fwd) k_bcol_uw(ColFw
 
 template <int K, typename C>
 __global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::bwd) k_bcol_bwd(ColBwdArgs A, const C *__restrict__ tw) {
-    constexpr int NY = 16 * K, L = 2 * NY, NYP = NY + 1;
+    constexpr int NY = 16 * K, NYP = NY + 1;
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ double2 sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, h = lane >> 4;
-    C *fa = reinterpret_cast<C *>(sm + (size_t)warp * 4 * L), *fb = fa + 2 * L;
-    double2 *wsm = sm + (size_t)warp * 4 * L;   // bload_s / bstore_s scratch (fa's space)
+    char *wreg = reinterpret_cast<char *>(sm) + (size_t)warp * CbSmem<K, C>::warp_bytes;
+    C *fa = reinterpret_cast<C *>(wreg), *fb = reinterpret_cast<C *>(wreg + CbSmem<K, C>::a_bytes);
+    double2 *wsm = reinterpret_cast<double2 *>(wreg);   // bload_s / bstore_s scratch (fa's space)
     const int npair = A.nz / 2;
     const int pr = blockIdx.x * CB_WARPS + warp;
     if (pr >= A.nxh * npair) return;
@@ -495,7 +516,6 @@ int kmm_colblk_fwd(kmm_ctx *ctx, const ColFwdArgs &A, const FusedTabs &T, const 
     if (!K) return KMM_ERR_UNSUPPORTED;
     const int npairs = ctx->nxh * (ctx->nz / 2);
     const int nblk = (npairs + CB_WARPS - 1) / CB_WARPS;
-    const size_t smem = sizeof(double2) * (size_t)CB_WARPS * 4 * (2 * ctx->ny);
     // scalar and omega_y (independent of v and of each other) on the two side streams, v on the
     // main stream, so each kernel's last partial wave overlaps the others; u, w after all three
     cudaStream_t s_scl = ctx->side, s_omy = ctx->side2;
@@ -505,6 +525,7 @@ int kmm_colblk_fwd(kmm_ctx *ctx, const ColFwdArgs &A, const FusedTabs &T, const 
 #define BF(KK, CC)                                                                                    \
     do {                                                                                              \
         const CC *twc = (const CC *)tw;                                                               \
+        const size_t smem = (size_t)CB_WARPS * CbSmem<KK, CC>::warp_bytes;                            \
         if (A.scalar) {                                                                               \
             RET(kmm_smem_attr(ctx, (const void *)k_bcol_scl<KK, CC>, smem));                          \
             k_bcol_scl<KK, CC><<<nblk, CB_WARPS * 32, smem, s_scl>>>(A, T, rj, twc);                   \
@@ -626,9 +647,9 @@ int kmm_colblk_bwd(kmm_ctx *ctx, const ColBwdArgs &B, const void *tw, bool fp32)
     if (!K) return KMM_ERR_UNSUPPORTED;
     const int npairs = ctx->nxh * (ctx->nz / 2);
     const int nblk = (npairs + CB_WARPS - 1) / CB_WARPS;
-    const size_t smem = sizeof(double2) * (size_t)CB_WARPS * 4 * (2 * ctx->ny);
 #define BB(KK, CC)                                                                                    \
     do {                                                                                              \
+        const size_t smem = (size_t)CB_WARPS * CbSmem<KK, CC>::warp_bytes;                            \
         RET(kmm_smem_attr(ctx, (const void *)k_bcol_bwd<KK, CC>, smem));                              \
         k_bcol_bwd<KK, CC><<<nblk, CB_WARPS * 32, smem, ctx->stream>>>(B, (const CC *)tw);             \
         CKL();                                                                                        \

@@ -578,34 +578,3 @@ __device__ __forceinline__ void bload_dct(BCol<K> &x, const C *__restrict__ src,
     __syncwarp();
 }
 
-// DCT-I of the warp's two columns through the specialised FFT of length 2 NY (even extension):
-//   to_phys: scale by c(i)/2 first (solvers.f90:2241-2546);  !to_phys: /ny, halve the ends (3279-3416)
-// a, b: the warp's two smem buffers of 2 * 2 NY complex each.
-template <int K>
-__device__ __forceinline__ void bdct(BCol<K> &x, double2 *a, double2 *b, const double2 *tw, bool to_phys) {
-    constexpr int NY = 16 * K, L = 2 * NY;
-    const int t = bl_t(), h = (threadIdx.x >> 4) & 1;
-    const int base = h * L;
-#pragma unroll
-    for (int m = 0; m <= K; ++m) {
-        if (m == K && t != 15) continue;
-        const int i = bidx<K>(m);
-        double2 v = x.v[m];
-        if (to_phys && i > 0 && i < NY) v = make_double2(v.x * 0.5, v.y * 0.5);
-        a[swz<double2>(base + i)] = v;
-        if (i > 0 && i < NY) a[swz<double2>(base + L - i)] = v;
-    }
-    __syncwarp();
-    const double2 *r = fft_warp_ct<double2, L, -1, 2, true>(a, b, tw);
-#pragma unroll
-    for (int m = 0; m <= K; ++m) {
-        const int i = bidx<K>(m);
-        double2 v = r[swz<double2>(base + i)];
-        if (!to_phys) {
-            v = make_double2(v.x / (double)NY, v.y / (double)NY);
-            if (i == 0 || i == NY) v = make_double2(v.x / 2.0, v.y / 2.0);
-        }
-        x.v[m] = v;
-    }
-    __syncwarp();
-}
