@@ -296,7 +296,10 @@ int  kmm_flowstats(kmm_ctx *ctx, double *prof, double *scal);
  * processes, LO_multi_run/setup.py:93-101) ----------------------------------------------
  * Advance n independent contexts (any grids, any devices) by one step each.  Every member's
  * step is enqueued on its own stream before any is waited on, so the members overlap on the
- * GPU; members that need the routine path (polymer, IB) step synchronously.  status[m] receives
+ * GPU; members that need the routine path (polymer, IB) step synchronously.  When every member
+ * is on one device, takes the fused step with graph replay and KMM_OPT_ENSEMBLE_GRAPH = 1, the
+ * whole ensemble step is one CUDA graph whose child graphs are the members' captured steps
+ * (cached per member set; one launch per ensemble step).  status[m] receives
  * each member's kmm_step status; the return value is the first nonzero one (KMM_OK if none).
  * The members must be distinct contexts; a context must not be used from another host thread
  * during the call.                                                                          */
@@ -330,7 +333,7 @@ enum kmm_option {
                            transforms as 3xTF32 GEMMs of the cosine matrix on the tcgen05 tensor
                            cores (ny = 32, 64, 96, 128); 0 (default) as FP32 FFTs of the even
                            extension                                                          */
-    KMM_OPT_DERIVED_INPUTS = 8 /* 1 (default): inside the routine step, vcw3dp forms the x and z derivatives
+    KMM_OPT_DERIVED_INPUTS = 8, /* 1 (default): inside the routine step, vcw3dp forms the x and z derivatives
                            of its inputs (i kx, i kz times the y-transformed field, in the z
                            inverse) instead of transforming them as separate spectral fields,
                            and the step computes only the y derivatives; 0: every input
@@ -338,6 +341,9 @@ enum kmm_option {
                            with inertial particles, which read the gradient on the 3/2 grid.
                            The U11 .. DC333 mirrors then hold only their y-derivative members
                            after a step (kmm_gradv / kmm_derivscji recompute them)          */
+    KMM_OPT_ENSEMBLE_GRAPH = 9 /* 1 (default): kmm_ensemble_step replays the members' step graphs as
+                           one parent graph where it can (see above); 0: one graph launch per
+                           member on its own stream.  Read from every member (all must be 1). */
 };
 int  kmm_set_option(kmm_ctx *ctx, int option, int value);
 

@@ -9,6 +9,7 @@ import ctypes
 KMM_ABI_VERSION = 1
 
 # options (enum kmm_option)
+OPT_ENSEMBLE_GRAPH = 9
 OPT_FUSED, OPT_COLUMN_BLOCKED, OPT_GRAPH, OPT_ZTMA, OPT_WAIT_LIMIT_MS, OPT_XBIG, OPT_TC_DCT, OPT_DERIVED_INPUTS = (
     1, 2, 3, 4, 5, 6, 7, 8)
 

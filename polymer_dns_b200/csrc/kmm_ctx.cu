@@ -279,6 +279,7 @@ extern "C" int kmm_ctx_create(const kmm_params *p, int device, kmm_ctx **out) {
     c->use_graph = 1;
     c->use_ztma = 1;
     c->use_derived = 1;
+    c->use_ens_graph = 1;
 #define DUP(dst, src, n)                                                        \
     do {                                                                        \
         CK(cudaMalloc(&(dst), sizeof(double) * (size_t)(n)));                   \
@@ -332,6 +333,7 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
         for (int e = 0; e < 2 * KMM_TIMER_RECORDS; ++e) cudaEventDestroy(ctx->tm_ev[e]);
     for (int e = 0; e < 16; ++e)
         if (ctx->user_ev[e]) cudaEventDestroy(ctx->user_ev[e]);
+    kmm_ensemble_forget(ctx);   // cached ensemble graphs replay this context's buffers
     kmm_graph_release(ctx);
     kmm_fused_release(ctx);
     kmm_ztma_release(ctx);
@@ -353,6 +355,7 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
     for (int s = 0; s < 5; ++s)
         if (ctx->tw_store[s]) cudaFree(ctx->tw_store[s]);
     if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+    if (ctx->ens_ev) cudaEventDestroy(ctx->ens_ev);
     if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
     if (ctx->cfork_ev) cudaEventDestroy(ctx->cfork_ev);
     for (int e = 0; e < 2; ++e)
@@ -476,6 +479,7 @@ extern "C" int kmm_set_option(kmm_ctx *ctx, int option, int value) {
     case KMM_OPT_XBIG: ctx->force_xbig = value ? 1 : 0; return KMM_OK;
     case KMM_OPT_TC_DCT: ctx->use_tcdct = value ? 1 : 0; return KMM_OK;
     case KMM_OPT_DERIVED_INPUTS: ctx->use_derived = value ? 1 : 0; return KMM_OK;
+    case KMM_OPT_ENSEMBLE_GRAPH: ctx->use_ens_graph = value ? 1 : 0; return KMM_OK;
     case KMM_OPT_WAIT_LIMIT_MS: {
         if (value < 100 || value > 60000) {
             kmm_set_error(ctx, "wait limit %d ms outside 100 .. 60000", value);

@@ -992,10 +992,14 @@ int kmm_fused_step(kmm_ctx *ctx) {
 void kmm_graph_release(kmm_ctx *ctx) {
     if (!ctx->graph_ready) return;
     cudaStreamSynchronize(ctx->stream);
-    for (int p = 0; p < 2; ++p)
+    for (int p = 0; p < 2; ++p) {
         if (ctx->gexec[p]) cudaGraphExecDestroy(ctx->gexec[p]);
-    ctx->gexec[0] = ctx->gexec[1] = NULL;
+        if (ctx->ggraph[p]) cudaGraphDestroy(ctx->ggraph[p]);
+        ctx->gexec[p] = NULL;
+        ctx->ggraph[p] = NULL;
+    }
     ctx->graph_ready = 0;
+    ctx->ggen = kmm_graph_generation();
 }
 
 static void swap_history(kmm_ctx *ctx) {
@@ -1023,12 +1027,14 @@ static int capture_graphs(kmm_ctx *ctx) {
         ctx->gkernels[p] = ctx->launches - l0;
         ctx->launches = l0;
         if (e == cudaSuccess && st == KMM_OK) e = cudaGraphInstantiate(&ctx->gexec[p], g, 0);
-        if (g) cudaGraphDestroy(g);
+        ctx->ggraph[p] = g;   // kept: an ensemble step adds it to its parent graph as a child
         if (e != cudaSuccess || st != KMM_OK) {
             for (int h = 0; h < 6; ++h) ctx->f[hist[h]] = saved[h];
             ctx->it = it0;
-            for (int q = 0; q < 2; ++q)
+            for (int q = 0; q < 2; ++q) {
                 if (ctx->gexec[q]) { cudaGraphExecDestroy(ctx->gexec[q]); ctx->gexec[q] = NULL; }
+                if (ctx->ggraph[q]) { cudaGraphDestroy(ctx->ggraph[q]); ctx->ggraph[q] = NULL; }
+            }
             cudaGetLastError();
             kmm_set_error(ctx, "graph capture of the fused step failed (%s)", cudaGetErrorString(e));
             return st != KMM_OK ? st : KMM_ERR_CUDA;
@@ -1036,7 +1042,26 @@ static int capture_graphs(kmm_ctx *ctx) {
     }
     ctx->it = it0;          // captured, not executed
     ctx->graph_ready = 1;   // the two captured swaps restored arrangement 0
+    ctx->ggen = kmm_graph_generation();
     return KMM_OK;
+}
+
+// the graph a replayed fused step of this context would launch now (capturing it first), or -1
+// when the step is not replayed from a graph; *parity receives the arrangement
+int kmm_fused_graph_for_step(kmm_ctx *ctx, int *parity) {
+    const bool graphable = ctx->use_fused && kmm_fused_applicable(ctx) && ctx->use_graph && !ctx->timing_on &&
+                           ctx->fused != NULL && ctx->it >= ctx->p.irstrt;
+    if (!graphable) return -1;
+    if (!ctx->graph_ready) RET(capture_graphs(ctx));
+    *parity = ctx->f[KMM_FN] == ctx->g_fn0 ? 0 : 1;
+    return KMM_OK;
+}
+
+// after an ensemble graph replayed this member's step: the host side of kmm_fused_enqueue
+void kmm_fused_replayed(kmm_ctx *ctx, int parity) {
+    ctx->launches += ctx->gkernels[parity];
+    swap_history(ctx);
+    ctx->it += 1;
 }
 
 int kmm_fused_enqueue(kmm_ctx *ctx) {

@@ -117,6 +117,10 @@ struct kmm_ctx {
     int use_graph, graph_ready;
     cudaGraphExec_t gexec[2];
     long long gkernels[2];   // kernels in each graph (added to the launch count per replay)
+    cudaGraph_t ggraph[2];   // the captured graphs (child graphs of an ensemble step)
+    unsigned long long ggen;  // incremented whenever the graphs are captured or released
+    int use_ens_graph;        // KMM_OPT_ENSEMBLE_GRAPH
+    cudaEvent_t ens_ev;       // an ensemble graph's completion, waited on by this member's stream
     void *g_fn0;      // the FN buffer of parity 0
     int use_ztma;     // FP64 inverse z transform through TMA tile copies (default 1)
     void *ztma;       // its cached tensor maps (kmm_ztma.cu)
@@ -132,6 +136,10 @@ int kmm_fused_step(kmm_ctx *ctx);
 // and evaluate (kmm_fused_step = launch + finish; the ensemble launches all members first)
 int kmm_fused_launch(kmm_ctx *ctx);
 int kmm_fused_finish(kmm_ctx *ctx);
+int kmm_fused_graph_for_step(kmm_ctx *ctx, int *parity);
+unsigned long long kmm_graph_generation();   // a process-wide counter: every capture / release gets a new value
+void kmm_ensemble_forget(kmm_ctx *ctx);      // drop the cached ensemble graphs that hold ctx
+void kmm_fused_replayed(kmm_ctx *ctx, int parity);
 // one fused step enqueued on ctx->stream: through the captured graphs when enabled and ready
 // (captured on first use), else kernel by kernel
 int kmm_fused_enqueue(kmm_ctx *ctx);

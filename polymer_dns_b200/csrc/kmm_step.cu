@@ -2,6 +2,9 @@
 // Green's functions (gfcn, solvers.f90:5-172), initial (main_dns.f90:1602-2231) and the body
 // of the time loop (main_dns.f90:198-811).  Every device call goes through the routine entry
 // points of the other translation units, in the reference's order.
+#include <atomic>
+#include <mutex>
+
 #include <math.h>
 
 #include "kmm_internal.cuh"
@@ -507,15 +510,139 @@ extern "C" int kmm_polynl(kmm_ctx *ctx) {
 // before any member is waited on, so the members' kernels overlap on the GPU
 // ---------------------------------------------------------------------------
 static int ensemble_step_all(kmm_ctx **ctxs, int n, int *status);
+static int ensemble_step_graph(kmm_ctx **ctxs, int n, int *status);
 
 // the caller's current device is restored before returning
 extern "C" int kmm_ensemble_step(kmm_ctx **ctxs, int n, int *status) {
     if (!ctxs || n <= 0 || n > KMM_MAX_ENSEMBLE || !status) return KMM_ERR_ARG;
     int dev0 = 0;
     if (cudaGetDevice(&dev0) != cudaSuccess) return KMM_ERR_CUDA;
-    const int st = ensemble_step_all(ctxs, n, status);
+    int st = ensemble_step_graph(ctxs, n, status);
+    if (st == KMM_ERR_UNSUPPORTED) st = ensemble_step_all(ctxs, n, status);
     cudaSetDevice(dev0);
     return st;
+}
+
+// ---- the whole ensemble step as one CUDA graph -----------------------------------------
+// A parent graph holds every member's captured step (the graph of its current history
+// arrangement) as an independent child graph.  Parent graphs are cached per member set, the
+// members' arrangements and their graphs' generations; the generations come from one
+// process-wide counter, so a graph captured anew (or a context created at a freed one's
+// address) never matches a cached entry, and destroying a context drops the entries holding it.
+#define ENS_CACHE 4
+struct EnsGraph {
+    int n;
+    kmm_ctx *m[KMM_MAX_ENSEMBLE];
+    unsigned long long gen[KMM_MAX_ENSEMBLE];
+    unsigned char par[KMM_MAX_ENSEMBLE];
+    cudaGraphExec_t exec;
+    int device;
+};
+static EnsGraph g_ens[ENS_CACHE];
+static int g_ens_next = 0;
+static std::mutex g_ens_mu;
+static std::atomic<unsigned long long> g_graph_gen{0};
+
+unsigned long long kmm_graph_generation() { return ++g_graph_gen; }
+
+static void ens_drop(EnsGraph &e) {
+    if (e.exec) {
+        int d0 = 0;
+        cudaGetDevice(&d0);
+        cudaSetDevice(e.device);
+        cudaGraphExecDestroy(e.exec);
+        cudaSetDevice(d0);
+    }
+    e.exec = NULL;
+    e.n = 0;
+}
+
+void kmm_ensemble_forget(kmm_ctx *ctx) {
+    std::lock_guard<std::mutex> lk(g_ens_mu);
+    for (int c = 0; c < ENS_CACHE; ++c)
+        for (int i = 0; i < g_ens[c].n; ++i)
+            if (g_ens[c].m[i] == ctx) {
+                ens_drop(g_ens[c]);
+                break;
+            }
+}
+
+// KMM_ERR_UNSUPPORTED: the members cannot run as one graph this step (the caller falls back)
+static int ensemble_step_graph(kmm_ctx **ctxs, int n, int *status) {
+    if (n < 2) return KMM_ERR_UNSUPPORTED;
+    const int dev = ctxs[0] ? ctxs[0]->device : -1;
+    for (int m = 0; m < n; ++m) {
+        kmm_ctx *c = ctxs[m];
+        if (!c || c->device != dev || !c->use_ens_graph) return KMM_ERR_UNSUPPORTED;
+        for (int q = 0; q < m; ++q)
+            if (ctxs[q] == c) return KMM_ERR_UNSUPPORTED;
+    }
+    if (cudaSetDevice(dev) != cudaSuccess) return KMM_ERR_UNSUPPORTED;
+    unsigned char par[KMM_MAX_ENSEMBLE];
+    for (int m = 0; m < n; ++m) {
+        int p = 0;
+        const int st = kmm_fused_graph_for_step(ctxs[m], &p);
+        if (st != KMM_OK) return st < 0 ? KMM_ERR_UNSUPPORTED : st;
+        par[m] = (unsigned char)p;
+    }
+    std::lock_guard<std::mutex> lk(g_ens_mu);
+    EnsGraph *hit = NULL;
+    for (int c = 0; c < ENS_CACHE && !hit; ++c) {
+        EnsGraph &e = g_ens[c];
+        if (e.n != n || !e.exec || e.device != dev) continue;
+        bool same = true;
+        for (int m = 0; m < n && same; ++m)
+            same = e.m[m] == ctxs[m] && e.gen[m] == ctxs[m]->ggen && e.par[m] == par[m];
+        if (same) hit = &e;
+    }
+    if (!hit) {
+        EnsGraph &e = g_ens[g_ens_next];
+        g_ens_next = (g_ens_next + 1) % ENS_CACHE;
+        ens_drop(e);
+        cudaGraph_t parent = NULL;
+        cudaError_t err = cudaGraphCreate(&parent, 0);
+        for (int m = 0; m < n && err == cudaSuccess; ++m) {
+            cudaGraphNode_t node;
+            err = cudaGraphAddChildGraphNode(&node, parent, NULL, 0, ctxs[m]->ggraph[par[m]]);
+        }
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&e.exec, parent, 0);
+        if (parent) cudaGraphDestroy(parent);
+        if (err != cudaSuccess) {
+            cudaGetLastError();
+            e.exec = NULL;
+            return KMM_ERR_UNSUPPORTED;
+        }
+        e.n = n;
+        e.device = dev;
+        for (int m = 0; m < n; ++m) {
+            e.m[m] = ctxs[m];
+            e.gen[m] = ctxs[m]->ggen;
+            e.par[m] = par[m];
+        }
+        hit = &e;
+    }
+    // order the graph after every member's earlier work and every member's later work after it
+    // (CUDA errors are reported on member 0)
+    kmm_ctx *ctx = ctxs[0];
+    cudaStream_t s0 = ctx->stream;
+    for (int m = 0; m < n; ++m) {
+        kmm_ctx *c = ctxs[m];
+        if (!c->ens_ev) CK(cudaEventCreateWithFlags(&c->ens_ev, cudaEventDisableTiming));
+        if (m > 0) {
+            CK(cudaEventRecord(c->ens_ev, c->stream));
+            CK(cudaStreamWaitEvent(s0, c->ens_ev, 0));
+        }
+    }
+    CK(cudaGraphLaunch(hit->exec, s0));
+    CK(cudaEventRecord(ctxs[0]->ens_ev, s0));
+    for (int m = 1; m < n; ++m) CK(cudaStreamWaitEvent(ctxs[m]->stream, ctxs[0]->ens_ev, 0));
+    int first = KMM_OK;
+    for (int m = 0; m < n; ++m) {
+        kmm_fused_replayed(ctxs[m], par[m]);
+        status[m] = kmm_fused_finish(ctxs[m]);
+        if (first == KMM_OK && status[m] != KMM_OK) first = status[m];
+    }
+    return first;
 }
 
 static int ensemble_step_all(kmm_ctx **ctxs, int n, int *status) {

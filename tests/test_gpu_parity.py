@@ -502,6 +502,56 @@ def test_ensemble_matches_independent_runs(rt):
             assert np.array_equal(a.download(name), b.download(name)), name
 
 
+def test_ensemble_graph_matches_independent_runs(rt):
+    """Every member on the fused step: kmm_ensemble_step replays the whole ensemble step as one
+    parent graph of the members' step graphs (KMM_OPT_ENSEMBLE_GRAPH = 1).  Each member ends in
+    exactly the state of the same run stepped alone, and of the ensemble with the option off;
+    after a member is destroyed and a new one takes its place, the cached parent graph is not
+    reused (the new member is also exact)."""
+    specs = [dict(grid=(32, 32, 32)),
+             dict(grid=(16, 32, 12), scalar_on=1, diff=1.0, npart=64, tracer_scheme=1),
+             dict(grid=(32, 64, 32), precision=1, scalar_on=1, diff=1.0),
+             dict(grid=(48, 32, 32), scalar_on=1, diff=1.0, npart=32)]
+
+    def make(spec, graph=1):
+        kw = {k: v for k, v in spec.items() if k != "grid"}
+        p = kc.cfg_small(*spec["grid"], **kw)
+        fields = kc.initial_fields(p, amp=0.1, seed=12)
+        g = rt.KmmContext(p)
+        g.call("set_option", abi.OPT_ENSEMBLE_GRAPH, graph)
+        kc.load_initial(g, p, fields, np.zeros_like(fields[0]) if p.scalar_on else None)
+        if p.npart:
+            for name, arr in zip(("XPART", "YPART", "ZPART"), inputs.uniform_particles(p.npart, p.xl, p.yl, p.zl, p.ap, 4)):
+                g.upload(name, arr)
+        assert g.initial() == 0
+        return g
+
+    names = ["V", "OMY", "FN", "GN", "U0", "W0"]
+    ens = [make(s) for s in specs]
+    off = [make(s, graph=0) for s in specs]
+    alone = [make(s) for s in specs]
+    assert rt.ensemble_run(ens, 6) == [0] * len(specs)
+    assert rt.ensemble_run(off, 6) == [0] * len(specs)
+    for g in alone:
+        for _ in range(6):
+            assert g.step() == 0
+    for a, b, c in zip(ens, off, alone):
+        for name in names:
+            assert np.array_equal(a.download(name), c.download(name)), name
+            assert np.array_equal(b.download(name), c.download(name)), name
+    # replace member 1: the parent graph cached for the old member set must not be replayed
+    ens[1].close()
+    ens[1] = make(specs[1])
+    lone = make(specs[1])
+    assert rt.ensemble_run(ens, 3) == [0] * len(specs)
+    for _ in range(3):
+        assert lone.step() == 0
+    for name in names:
+        assert np.array_equal(ens[1].download(name), lone.download(name)), name
+    for g in ens + off + alone + [lone]:
+        g.close()
+
+
 def test_graph_replay_matches_kernel_launches(rt):
     """The fused step replayed from its two captured CUDA graphs (KMM_OPT_GRAPH) against the same
     step launched kernel by kernel: identical fields, particles and CFL after 7 steps (scalar,
