@@ -259,6 +259,13 @@ struct ZRecipe {
     unsigned char base[MAXIO], mult[MAXIO];
 };
 
+// the rows the x stage reads for each pair of inputs (2 p, 2 p + 1): the z-inverse outputs qa and
+// qb, or (xd = 1) the one row qa, the pair's second input being i kx times the first, formed in
+// the x stage (qb = 255: the pair has one input)
+struct XRecipe {
+    unsigned char qa[MAXIO / 2], qb[MAXIO / 2], xd[MAXIO / 2];
+};
+
 template <typename C>
 __global__ void __launch_bounds__(256, 4) k_zfft_bwd(const C *__restrict__ pl, C *__restrict__ q, const __grid_constant__ DevPlan P,
                                                   const C *__restrict__ tw, int nyp, int nz, int nxh, int mz,
@@ -553,7 +560,9 @@ __global__ void __launch_bounds__(256) k_xinv_big(const double2 *__restrict__ q,
 #define XBW 4   // rows (warps) per block of k_xinv_big2
 template <int MX, typename C>
 __global__ void __launch_bounds__(XBW * 32) k_xinv_big2(const C *__restrict__ q, typename kct::Real<C>::T *__restrict__ pb,
-                                                        const C *__restrict__ tw, int nin, int nyp, int mz) {
+                                                        const C *__restrict__ tw, int nin, int nyp, int mz,
+                                                        const __grid_constant__ XRecipe X,
+                                                        const double *__restrict__ wavx) {
     typedef typename kct::Real<C>::T T;
     constexpr int NXH = MX / 3;
     extern __shared__ double2 smd[];
@@ -561,12 +570,18 @@ __global__ void __launch_bounds__(XBW * 32) k_xinv_big2(const C *__restrict__ q,
     const int z = blockIdx.x * XBW + warp, y = blockIdx.y, f = 2 * blockIdx.z, g = f + 1 < nin ? f + 1 : -1;
     if (z >= mz) return;   // whole warps: no block barrier below
     C *a = reinterpret_cast<C *>(smd) + (size_t)warp * 2 * MX, *b = a + MX;
-    const C *qa = q + (((size_t)f * nyp + y) * mz + z) * NXH;
-    const C *qb = q + (((size_t)(g >= 0 ? g : f) * nyp + y) * mz + z) * NXH;
+    const int pr = blockIdx.z;
+    const bool xd = X.xd[pr];
+    const C *qa = q + (((size_t)X.qa[pr] * nyp + y) * mz + z) * NXH;
+    const C *qb = q + (((size_t)((g >= 0 && !xd) ? X.qb[pr] : X.qa[pr]) * nyp + y) * mz + z) * NXH;
     const C zc = kct::mk<C>((T)0, (T)0);
     for (int k = NXH + lane; k <= MX - NXH; k += 32) a[swz<C>(k)] = zc;
     for (int kk = lane; kk < NXH; kk += 32) {
         C A_ = qa[kk], B_ = g >= 0 ? qb[kk] : zc;
+        if (xd) {   // the pair's second input is i kx times the first
+            const T kx = (T)wavx[kk];
+            B_ = kct::mk<C>(-kx * A_.y, kx * A_.x);
+        }
         if (kk == 0) { A_.y = (T)0; B_.y = (T)0; }   // c2r ignores Im of the mean mode
         a[swz<C>(kk)] = kct::mk<C>(A_.x - B_.y, A_.y + B_.x);
         if (kk > 0) a[swz<C>(MX - kk)] = kct::mk<C>(A_.x + B_.y, -A_.y + B_.x);
@@ -647,7 +662,8 @@ __global__ void __launch_bounds__(XpW<C>::n * 32) k_xphys2(const C *__restrict__
                                                     const double *__restrict__ scsource,
                                                     const double *__restrict__ seght, double *__restrict__ cfl,
                                                     double *__restrict__ umax, const C *__restrict__ tw,
-                                                    PhysArgs A, Save3D sv, int nyp, int mz, int *status) {
+                                                    PhysArgs A, Save3D sv, int nyp, int mz, int *status,
+                                                    const __grid_constant__ XRecipe X, const double *__restrict__ wavx) {
     typedef typename kct::Real<C>::T T;
     constexpr int XPW = XpW<C>::n;
     constexpr int NXH = MX / 3;
@@ -669,10 +685,13 @@ __global__ void __launch_bounds__(XpW<C>::n * 32) k_xphys2(const C *__restrict__
         kasync::mbar_init_fence();
         for (int pr = 0; pr < npairs; ++pr) {
             const int f = 2 * pr, g = f + 1 < A.nin ? f + 1 : -1;
-            kasync::mbar_expect_tx(&xbar[pr], g >= 0 ? 2 * ROWB : ROWB);
-            kasync::bulk_g2s(phys + (size_t)f * MX, q + (((size_t)f * nyp + y) * mz + z) * NXH, ROWB, &xbar[pr]);
-            if (g >= 0)
-                kasync::bulk_g2s(phys + (size_t)g * MX, q + (((size_t)g * nyp + y) * mz + z) * NXH, ROWB, &xbar[pr]);
+            const bool two = g >= 0 && !X.xd[pr];
+            kasync::mbar_expect_tx(&xbar[pr], two ? 2 * ROWB : ROWB);
+            kasync::bulk_g2s(phys + (size_t)f * MX, q + (((size_t)X.qa[pr] * nyp + y) * mz + z) * NXH, ROWB,
+                             &xbar[pr]);
+            if (two)
+                kasync::bulk_g2s(phys + (size_t)g * MX, q + (((size_t)X.qb[pr] * nyp + y) * mz + z) * NXH, ROWB,
+                                 &xbar[pr]);
         }
     }
     __syncthreads();
@@ -685,14 +704,20 @@ __global__ void __launch_bounds__(XpW<C>::n * 32) k_xphys2(const C *__restrict__
             ok = false;
             continue;
         }
+        const bool xd = X.xd[pr];
         const C *qa = reinterpret_cast<const C *>(phys + (size_t)f * MX);
-        const C *qb = g >= 0 ? reinterpret_cast<const C *>(phys + (size_t)g * MX) : qa;
+        const C *qb = (g >= 0 && !xd) ? reinterpret_cast<const C *>(phys + (size_t)g * MX) : qa;
         // Hermitian extension: Z_k = A_k + i B_k for k < nxh, conj(A) + i conj(B) at mx - k, and the
-        // modes nxh .. mx - nxh (the Nyquist mode mx / 2 among them) not carried
+        // modes nxh .. mx - nxh (the Nyquist mode mx / 2 among them) not carried; B = i kx A for an
+        // x-derivative pair
         const C zc = kct::mk<C>((T)0, (T)0);
         for (int k = NXH + lane; k <= MX - NXH; k += 32) a[swz<C>(k)] = zc;
         for (int kk = lane; kk < NXH; kk += 32) {
             C A_ = qa[kk], B_ = g >= 0 ? qb[kk] : zc;
+            if (xd) {
+                const T kx = (T)wavx[kk];
+                B_ = kct::mk<C>(-kx * A_.y, kx * A_.x);
+            }
             if (kk == 0) { A_.y = (T)0; B_.y = (T)0; }   // c2r ignores Im of the mean mode
             a[swz<C>(kk)] = kct::mk<C>(A_.x - B_.y, A_.y + B_.x);
             if (kk > 0) a[swz<C>(MX - kk)] = kct::mk<C>(A_.x + B_.y, -A_.y + B_.x);
@@ -1280,6 +1305,64 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         static const int qq[6] = {KMM_QP11, KMM_QP12, KMM_QP13, KMM_QP22, KMM_QP23, KMM_QP33};
         for (int m = 0; m < 6; ++m) RET(add_out(O_QP11 + m, qq[m]));
     }
+    // x derivatives formed in the x stage (with polymer, derived inputs and a compiled x stage:
+    // k_xphys2 or the two-pass k_xinv_big2): every input i kx f whose f is also an input moves
+    // right after it, an odd place, and the x stage builds their pair from the one row of f; the
+    // z inverse produces the other nq inputs only
+    bool xform[MAXIO];
+    for (int i = 0; i < MAXIO; ++i) xform[i] = false;
+    const bool x_compiled = ((mx == 48 || mx == 96 || mx == 144 || mx == 192) &&
+                             !(ctx->force_xbig && ctx->p.precision == 0)) ||
+                            mx == 576;
+    if (derived && poly && x_compiled) {
+        int slot_at[MAXIO];
+        for (int i = 0; i < nin; ++i) slot_at[i] = -1;
+        for (int sl = 0; sl < S_NSLOT; ++sl)
+            if (A.slot_of_in[sl] >= 0) slot_at[A.slot_of_in[sl]] = sl;
+        int order[MAXIO], no = 0;
+        bool used[MAXIO], odd_x[MAXIO];
+        for (int i = 0; i < nin; ++i) used[i] = odd_x[i] = false;
+        for (int d = 0; d < nin; ++d) {
+            if (zr.mult[d] != 1) continue;
+            int f = -1;
+            for (int c = 0; c < nin && f < 0; ++c)
+                if (!used[c] && zr.mult[c] == 0 && zr.base[c] == zr.base[d]) f = c;
+            if (f < 0) continue;
+            used[f] = used[d] = true;
+            order[no++] = f;
+            odd_x[no] = true;
+            order[no++] = d;
+        }
+        for (int c = 0; c < nin; ++c)
+            if (!used[c]) order[no++] = c;
+        ZRecipe z2;
+        for (int pos = 0; pos < nin; ++pos) {
+            const int old = order[pos];
+            z2.base[pos] = zr.base[old];
+            z2.mult[pos] = zr.mult[old];
+            if (slot_at[old] >= 0) A.slot_of_in[slot_at[old]] = pos;
+            xform[pos] = odd_x[pos];
+        }
+        zr = z2;
+    }
+    // the z inverse's outputs (the inputs not formed in the x stage, compacted) and the x stage's rows
+    int nq = 0;
+    unsigned char qidx[MAXIO];
+    ZRecipe zq;
+    for (int i = 0; i < nin; ++i) {
+        if (xform[i]) continue;
+        qidx[i] = (unsigned char)nq;
+        zq.base[nq] = zr.base[i];
+        zq.mult[nq] = zr.mult[i];
+        ++nq;
+    }
+    XRecipe xr;
+    for (int pr = 0; pr < (nin + 1) / 2; ++pr) {
+        const int f = 2 * pr, g = f + 1;
+        xr.qa[pr] = qidx[f];
+        xr.xd[pr] = (unsigned char)(g < nin && xform[g]);
+        xr.qb[pr] = g >= nin ? (unsigned char)255 : (xform[g] ? qidx[f] : qidx[g]);
+    }
     A.nin = nin;
     A.nout = nout;
     A.scalar = scal;
@@ -1409,11 +1492,11 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     kmm_toc(ctx, KMM_STAGE_DCT_FWD);
     kmm_tic(ctx);
     if (f32)
-        k_zfft_bwd<float2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nin), 256, sm_z, ctx->stream>>>(
-            pl_in32, q_in32, ctx->pmz, tw_mz, nyp, nz, nxh, mz, zr, ctx->d_wavx, ctx->d_wavz);
+        k_zfft_bwd<float2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nq), 256, sm_z, ctx->stream>>>(
+            pl_in32, q_in32, ctx->pmz, tw_mz, nyp, nz, nxh, mz, zq, ctx->d_wavx, ctx->d_wavz);
     else
-        k_zfft_bwd<double2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nin), 256, sm_z, ctx->stream>>>(
-            ctx->pl_in, ctx->q_in, ctx->pmz, ctx->pmz.tw, nyp, nz, nxh, mz, zr, ctx->d_wavx, ctx->d_wavz);
+        k_zfft_bwd<double2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nq), 256, sm_z, ctx->stream>>>(
+            ctx->pl_in, ctx->q_in, ctx->pmz, ctx->pmz.tw, nyp, nz, nxh, mz, zq, ctx->d_wavx, ctx->d_wavz);
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_BWD);
     bool fast_done = false, xstat = false;
@@ -1440,7 +1523,7 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         RET(kmm_smem_attr(ctx, (const void *)k_xphys2<MM, CC>, sm_x2));                                          \
         k_xphys2<MM, CC><<<dim3(mz, nyp), XpW<CC>::n * 32, sm_x2, ctx->stream>>>(                                         \
             QQ, PO, ctx->drag, up3, vp3, wp3, im, fxi, fyi, fzi, ctx->scsource, ctx->d_seght, ctx->d_cfl,          \
-            ctx->d_umax, TW, A, sv, nyp, mz, ctx->d_status);                                                     \
+            ctx->d_umax, TW, A, sv, nyp, mz, ctx->d_status, xr, ctx->d_wavx);                                   \
     } while (0)
 #define XP2S(MM)                                                                                                 \
     do {                                                                                                         \
@@ -1463,11 +1546,11 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
                 if (mx == 576 && f32) {
                     RET(kmm_smem_attr(ctx, (const void *)k_xinv_big2<576, float2>, sm_b2));
                     k_xinv_big2<576, float2><<<g1, XBW * 32, sm_b2, ctx->stream>>>(q_in32, (float *)ctx->xbig, tw_mx,
-                                                                                    nin, nyp, mz);
+                                                                                    nin, nyp, mz, xr, ctx->d_wavx);
                 } else if (mx == 576) {
                     RET(kmm_smem_attr(ctx, (const void *)k_xinv_big2<576, double2>, sm_b2));
                     k_xinv_big2<576, double2><<<g1, XBW * 32, sm_b2, ctx->stream>>>(ctx->q_in, ctx->xbig, ctx->wmx.tw,
-                                                                                     nin, nyp, mz);
+                                                                                     nin, nyp, mz, xr, ctx->d_wavx);
                 } else {
                     k_xinv_big<<<dim3((mz + XZB - 1) / XZB, nyp, (nin + 1) / 2), 256, sm_xf, ctx->stream>>>(
                         ctx->q_in, ctx->xbig, ctx->pmx, nin, nyp, mz, mx, nxh);
