@@ -314,6 +314,18 @@ bool kmm_derived_inputs(const kmm_ctx *ctx) {
            !(ctx->p.scalar_on && (ctx->p.scl_flag == 4 || ctx->p.scl_flag == 5));
 }
 
+// the routine step's history copies (c11nm1 = c11n ..., scnm1 = scn, fnm1 = fn, gnm1 = gn;
+// main_dns.f90:268-275, 335, 386, 418)
+// as an exchange of the two fields' buffers: the n field is next written whole by vcw3dp, and
+// nothing reads it in between, so after the exchange both fields hold what the copy would leave
+static int swap_fields(kmm_ctx *ctx, int nm1, int n) {
+    if (!kmm_field_ptr(ctx, nm1) || !kmm_field_ptr(ctx, n)) return KMM_ERR_NOMEM;
+    void *t = ctx->f[nm1];
+    ctx->f[nm1] = ctx->f[n];
+    ctx->f[n] = t;
+    return KMM_OK;
+}
+
 // ---------------------------------------------------------------------------
 // one iteration of the time loop, main_dns.f90:198-811
 // ---------------------------------------------------------------------------
@@ -361,8 +373,8 @@ extern "C" int kmm_step(kmm_ctx *ctx) {
             }
             RET(kmm_internal_phirhs_many(ctx, cm, nlc, nl2c, 6, ctx->p.diffpoly, wc, w1));
             for (int m = 0; m < 6; ++m) {
-                RET(kmm_copy(ctx, KMM_C11NM1 + m, KMM_C11N + m));
-                RET(kmm_copy(ctx, KMM_STR11NM1 + m, KMM_STR11N + m));
+                RET(swap_fields(ctx, KMM_C11NM1 + m, KMM_C11N + m));
+                RET(swap_fields(ctx, KMM_STR11NM1 + m, KMM_STR11N + m));
             }
             const double g = (re * ctx->p.diffpoly) / (dt * th);
             RET(kmm_zero(ctx, KMM_BCTOP));
@@ -376,7 +388,7 @@ extern "C" int kmm_step(kmm_ctx *ctx) {
     }
     if (ctx->p.scalar_on) {
         RET(kmm_phirhs(ctx, KMM_SCALAR, KMM_SCN, KMM_SCNM1, ctx->p.diff));
-        RET(kmm_copy(ctx, KMM_SCNM1, KMM_SCN));
+        RET(swap_fields(ctx, KMM_SCNM1, KMM_SCN));
         const double g = (re * ctx->p.diff) / (dt * th);
         RET(kmm_zero(ctx, KMM_BCTOP));   // bcscltop = bcsclbot = 0 (main_dns.f90:39)
         RET(kmm_zero(ctx, KMM_BCBOT));
@@ -385,11 +397,11 @@ extern "C" int kmm_step(kmm_ctx *ctx) {
     }
     RET(kmm_phi_from_v(ctx));
     RET(kmm_phirhs(ctx, KMM_V, KMM_FN, KMM_FNM1, 1.0));
-    RET(kmm_copy(ctx, KMM_FNM1, KMM_FN));
+    RET(swap_fields(ctx, KMM_FNM1, KMM_FN));
     RET(kmm_solve(ctx, KMM_V, re / (dt * th), 0));
     RET(kmm_solve(ctx, KMM_V, 0.0, 0));
     RET(kmm_phirhs(ctx, KMM_OMY, KMM_GN, KMM_GNM1, 1.0));
-    RET(kmm_copy(ctx, KMM_GNM1, KMM_GN));
+    RET(swap_fields(ctx, KMM_GNM1, KMM_GN));
     RET(kmm_influence(ctx));
     RET(kmm_penta(ctx, KMM_OMY, re / (dt * th), 0, ctx->atu, ctx->btu, ctx->abu, ctx->bbu));
     RET(kmm_uzero(ctx, 1));
