@@ -976,7 +976,10 @@ __global__ void k_phirhs_a(PhiList L, const double *__restrict__ wavx, const dou
     const double a = -re * var / (dt * th), b = re * var / (2.0 * th);
     GRID_LOOP(n) {
         DECOMP();
-        double2 vv = v[idx], f = fn[idx], fm = fnm1[idx];
+        double2 vv = v[idx], f = fn[idx];
+        // fnm1 = NULL: the n-1 term is 2 fn (the polymer components' call, main_dns.f90:250-260),
+        // formed here exactly instead of read
+        const double2 fm = fnm1 ? fnm1[idx] : make_double2(2.0 * f.x, 2.0 * f.y);
         double2 w;
         w.x = a * vv.x - b * (3.0 * f.x - fm.x);
         w.y = a * vv.y - b * (3.0 * f.y - fm.y);
@@ -1428,17 +1431,6 @@ extern "C" int kmm_subforce(kmm_ctx *ctx) {
     k_subforce<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(SPEC(ctx, KMM_GN), SPEC(ctx, KMM_FN),
                                                                      SPEC(ctx, KMM_OMZ), SPEC(ctx, KMM_T1),
                                                                      SPEC(ctx, KMM_T2), SPEC(ctx, KMM_T3), ctx->nspec);
-    CKL();
-    return KMM_OK;
-}
-
-// y <- a*x  (the 2.0*cNL argument of main_dns.f90:248-261)
-__global__ void k_scale_copy(double2 *y, const double2 *x, double a, size_t n) {
-    GRID_LOOP(n) { y[idx] = make_double2(a * x[idx].x, a * x[idx].y); }
-}
-
-int kmm_internal_axpy_spec(kmm_ctx *ctx, double2 *y, const double2 *x, double a) {
-    k_scale_copy<<<kmm_blocks(ctx->nspec, 256), 256, 0, ctx->stream>>>(y, x, a, ctx->nspec);
     CKL();
     return KMM_OK;
 }

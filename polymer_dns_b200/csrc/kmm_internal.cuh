@@ -195,7 +195,8 @@ int kmm_colblk_solve_many(kmm_ctx *ctx, double2 *const *u, int nf, double g, int
 // penta (ib = 0) of nf distinct fields of one configuration
 int kmm_internal_penta_many(kmm_ctx *ctx, double2 *const *u, int nf, double g, double at, double bt, double ab,
                             double bb, const double2 *gt, const double2 *gb);
-// phirhs of nf independent fields (at most KMM_PHI_BATCH), each with its own two scratch fields
+// phirhs of nf independent fields (at most KMM_PHI_BATCH), each with its own two scratch fields;
+// FM[m] = NULL takes 2 F[m] as the n-1 term (the polymer components' call)
 #define KMM_PHI_BATCH 8
 int kmm_internal_phirhs_many(kmm_ctx *ctx, double2 *const *V, const double2 *const *F, const double2 *const *FM,
                              int nf, double var, double2 *const *wrkc, double2 *const *wrk1);
@@ -207,7 +208,6 @@ void kmm_tau_release(kmm_ctx *ctx);
 int kmm_routine_tw32(kmm_ctx *ctx, const float2 **y2, const float2 **mz, const float2 **mx);
 int kmm_internal_penta(kmm_ctx *ctx, double2 *u, double g, int ib, double at, double bt, double ab, double bb,
                        const double2 *gt, const double2 *gb);
-int kmm_internal_axpy_spec(kmm_ctx *ctx, double2 *y, const double2 *x, double a);
 int kmm_internal_set_constant_mode(kmm_ctx *ctx, double2 *a, double value);
 int kmm_plan_init(kmm_ctx *ctx, DevPlan *p, int n, int slot);
 void kmm_plan_r8(const DevPlan *src, DevPlan *dst);

@@ -357,19 +357,17 @@ extern "C" int kmm_step(kmm_ctx *ctx) {
                 if (!nl[m]) return KMM_ERR_NOMEM;
             }
             RET(kmm_internal_polynl(ctx, nl));
-            // the six components' phirhs in batched launches, each component with its own 2 nl,
-            // wrkc and wrk1 (scratch ids 6 .. 23)
-            double2 *nl2[6], *wc[6], *w1[6], *cm[6];
+            // the six components' phirhs in batched launches, each component with its own wrkc
+            // and wrk1 (scratch ids 12 .. 23); its n-1 term 2 nl is formed in the kernel (NULL)
+            double2 *wc[6], *w1[6], *cm[6];
             const double2 *nlc[6], *nl2c[6];
             for (int m = 0; m < 6; ++m) {
-                nl2[m] = poly_scratch(ctx, 6 + m);
                 wc[m] = poly_scratch(ctx, 12 + m);
                 w1[m] = poly_scratch(ctx, 18 + m);
                 cm[m] = SPEC(ctx, kPolyComp[m]);
-                if (!nl2[m] || !wc[m] || !w1[m] || !cm[m]) return KMM_ERR_NOMEM;
+                if (!wc[m] || !w1[m] || !cm[m]) return KMM_ERR_NOMEM;
                 nlc[m] = nl[m];
-                nl2c[m] = nl2[m];
-                RET(kmm_internal_axpy_spec(ctx, nl2[m], nl[m], 2.0));
+                nl2c[m] = NULL;
             }
             RET(kmm_internal_phirhs_many(ctx, cm, nlc, nl2c, 6, ctx->p.diffpoly, wc, w1));
             for (int m = 0; m < 6; ++m) {
