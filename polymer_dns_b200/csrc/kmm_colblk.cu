@@ -21,12 +21,12 @@
 #define KMM_CB_MINB_BWD 2
 #endif
 // blocks per SM each kernel's register budget is sized for, as measured per kernel: FP64 scalar,
-// u/w and back kernels two, v and omega_y three; in FP32 the scalar, u/w and omega_y kernels
+// u/w and back kernels two, v three, omega_y four; in FP32 the scalar, u/w and omega_y kernels
 // four, v and the back kernel three
 template <typename C> struct CbMinB {
     static constexpr bool f64 = sizeof(C) == 16;
     static constexpr int fwd = f64 ? KMM_CB_MINB_FWD : 4;   // k_bcol_scl, k_bcol_uw
-    static constexpr int omy = f64 ? CB_MINB : 4;
+    static constexpr int omy = 4;   // with bphirhs_g (its histories staged in shared memory)
     static constexpr int v = CB_MINB;
     static constexpr int bwd = f64 ? KMM_CB_MINB_BWD : 3;
 };
@@ -34,16 +34,18 @@ template <typename C> struct CbMinB {
 // shared memory of one warp: region A holds the bload_s / bstore_s scratch (2 (NY + 8) double2)
 // and bdct_store / bload_dct's natural-order column pair (2 (NY + 8) elements of C, within the
 // swizzled rows); region B the DCT passes' transpose buffer (2 N = 4 NY elements of C).  A's size
-// is a multiple of 128 bytes, so B's swizzled rows keep their bank alignment.
+// is a multiple of 128 bytes, so B's swizzled rows keep their bank alignment.  bphirhs_g's two
+// staged columns (4 (NY + 8) double2) span both regions, which the FP32 forms widen to hold.
 template <int K, typename C>
 struct CbSmem {
     static constexpr size_t a_bytes = 2 * (16 * K + 8) * sizeof(double2);
     static constexpr size_t b_bytes = 4 * 16 * K * sizeof(C);
-    static constexpr size_t warp_bytes = a_bytes + b_bytes;
+    static constexpr size_t stage_bytes = 4 * (16 * K + 8) * sizeof(double2);
+    static constexpr size_t warp_bytes = a_bytes + b_bytes > stage_bytes ? a_bytes + b_bytes : stage_bytes;
     static_assert(a_bytes % 128 == 0, "region B starts on a 128-byte boundary");
 };
 
-// phirhs on one column (solvers.f90:633-675)
+// phirhs on one column pair (solvers.f90:633-675), the n and n-1 terms in registers
 template <int K>
 __device__ __forceinline__ void bphirhs(BCol<K> &x, const BCol<K> &fn, const BCol<K> &fnm1, double re, double var,
                                         double dt, double th, double w2, double dyde, unsigned mask) {
@@ -66,6 +68,81 @@ __device__ __forceinline__ void bphirhs(BCol<K> &x, const BCol<K> &fn, const BCo
 #pragma unroll
     for (int m = 0; m <= K; ++m)
         x.v[m] = make_double2(w.v[m].x - (1.0 - th) * d2.v[m].x / th, w.v[m].y - (1.0 - th) * d2.v[m].y / th);
+}
+
+// The same with the n and n-1 terms read from global memory
+// (fn, fnm1 at the pair's columns) through the warp's scratch buf (4 (16 K + 8) double2): both are
+// staged with coalesced loads and read slot by slot, and for th <= 0.99 the derivatives are formed
+// first, so that at most three column variables are live; per coefficient the arithmetic is
+// w = a x - b (3 fn - fnm1) + (1 - th) k^2 x / th, x <- w - (1 - th) x'' / th.
+template <int K>
+__device__ __forceinline__ void bphirhs_g(BCol<K> &x, const double2 *__restrict__ fn, const double2 *__restrict__ fnm1,
+                                          double2 *buf, double re, double var, double dt, double th, double w2,
+                                          double dyde, unsigned mask) {
+    const double a = -re * var / (dt * th), b = re * var / (2.0 * th);
+    const double c = (1.0 - th) * w2;
+    const int t = bl_t(), h = (threadIdx.x >> 4) & 1;
+    double2 *b0 = buf + h * (16 * K + 8), *b1 = buf + 2 * (16 * K + 8) + h * (16 * K + 8);
+    {
+        double2 r0[K], r1[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            r0[j] = fn[t + 16 * j];
+            r1[j] = fnm1[t + 16 * j];
+        }
+        const double2 top0 = fn[16 * K], top1 = fnm1[16 * K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            b0[swz<double2>(t + 16 * j)] = r0[j];
+            b1[swz<double2>(t + 16 * j)] = r1[j];
+        }
+        if (t == 15) {
+            b0[swz<double2>(16 * K)] = top0;
+            b1[swz<double2>(16 * K)] = top1;
+        }
+    }
+    __syncwarp();
+    if (th > 0.99) {   // x takes the right-hand side before its derivatives are formed
+        BCol<K> w;
+#pragma unroll
+        for (int m = 0; m <= K; ++m) {
+            const int i = bidx<K>(m);
+            const double2 f = b0[swz<double2>(i)], fm = b1[swz<double2>(i)];
+            double2 r;
+            r.x = a * x.v[m].x - b * (3.0 * f.x - fm.x);
+            r.y = a * x.v[m].y - b * (3.0 * f.y - fm.y);
+            x.v[m] = r;
+            r.x = r.x + c * x.v[m].x / th;
+            r.y = r.y + c * x.v[m].y / th;
+            w.v[m] = r;
+        }
+        __syncwarp();
+        BCol<K> d1, d2;
+        bcderiv<K>(d1, x, dyde, mask);
+        bcderiv<K>(d2, d1, dyde, mask);
+#pragma unroll
+        for (int m = 0; m <= K; ++m)
+            x.v[m] = make_double2(w.v[m].x - (1.0 - th) * d2.v[m].x / th, w.v[m].y - (1.0 - th) * d2.v[m].y / th);
+        return;
+    }
+    BCol<K> d2;
+    {
+        BCol<K> d1;
+        bcderiv<K>(d1, x, dyde, mask);
+        bcderiv<K>(d2, d1, dyde, mask);
+    }
+#pragma unroll
+    for (int m = 0; m <= K; ++m) {
+        const int i = bidx<K>(m);
+        const double2 f = b0[swz<double2>(i)], fm = b1[swz<double2>(i)];
+        double2 r;
+        r.x = a * x.v[m].x - b * (3.0 * f.x - fm.x);
+        r.y = a * x.v[m].y - b * (3.0 * f.y - fm.y);
+        r.x = r.x + c * x.v[m].x / th;
+        r.y = r.y + c * x.v[m].y / th;
+        x.v[m] = make_double2(r.x - (1.0 - th) * d2.v[m].x / th, r.y - (1.0 - th) * d2.v[m].y / th);
+    }
+    __syncwarp();
 }
 
 // the column pair of the calling warp
@@ -151,12 +228,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::omy) k_bcol_omy(ColF
     const double2 zero = make_double2(0.0, 0.0);
     BCol<K> om;
     bload_s<K>(om, A.omy + P.off, wsm);
-    {
-        BCol<K> g1c, g0c;
-        bload_s<K>(g1c, A.gn + P.off, wsm);
-        bload_s<K>(g0c, A.gnm1 + P.off, wsm);
-        bphirhs<K>(om, g1c, g0c, A.re, 1.0, A.dt, A.th, P.w2, A.dyde, FULL);
-    }
+    bphirhs_g<K>(om, A.gn + P.off, A.gnm1 + P.off, wsm, A.re, 1.0, A.dt, A.th, P.w2, A.dyde, FULL);
     const TauTab to = tab_at(T, TB_OMY, P.tcol, NYP);
     bsolve_robin<K>(om, to, zero, zero, P.w2 + g1, A.c0, rj, FULL);
     if (P.mean) {
@@ -195,11 +267,13 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CbMinB<C>::v) k_bcol_v(ColFwdAr
 #pragma unroll
         for (int m = 0; m <= K; ++m) v.v[m] = make_double2(d2.v[m].x - w2 * v.v[m].x, d2.v[m].y - w2 * v.v[m].y);
     }
-    {
+    if constexpr (sizeof(C) == 16) {   // FP64: the register form (measured faster at this budget)
         BCol<K> f1, f0;
         bload_s<K>(f1, A.fn + P.off, wsm);
         bload_s<K>(f0, A.fnm1 + P.off, wsm);
         bphirhs<K>(v, f1, f0, A.re, 1.0, A.dt, A.th, w2, A.dyde, FULL);
+    } else {
+        bphirhs_g<K>(v, A.fn + P.off, A.fnm1 + P.off, wsm, A.re, 1.0, A.dt, A.th, w2, A.dyde, FULL);
     }
     {
         const TauTab tp = tab_at(T, TB_PHI, P.tcol, NYP);
