@@ -11,7 +11,9 @@ L2 flush is inserted between steps.
 
 --impl kmm (default): value = steps/s of the device-resident run (CUDA events on the library's
     stream, max over ranks); e2e = the same steps through the C ABI with the restart state held on
-    the host: every step uploads the prognostic state from pinned memory, steps, and downloads it.
+    the host (kmm_bind_host + kmm_run_host): every step uploads the prognostic state from pinned
+    memory, steps, and downloads it, one step's downloads overlapping the next step's uploads;
+    e2e.single_calls = the same copies as kmm_upload / kmm_step / kmm_download calls.
 --impl reference: the CPU restatement of the reference (oracle/, OpenMP over all host cores) on a
     bounded sample of the same workload (rank 0 only).
 Multi-GPU: replicas only (the reference's ensemble is independent runs); each rank runs its own
@@ -287,6 +289,11 @@ def run_kmm(a, rank, world, local_rank):
         state += ["SCALAR", "SCN", "SCNM1"]
     if p.npart:
         state += ["XPART", "YPART", "ZPART", "UPART", "VPART", "WPART"]
+    if p.polymer_on:   # the c-restart records (restart.py)
+        comp = ["11", "12", "13", "22", "23", "33"]
+        state += ["C11", "C12", "C13", "C21", "C22", "C23", "C31", "C32", "C33"]
+        state += ["C%sN" % c for c in comp] + ["C%sNM1" % c for c in comp]
+        state += ["STR%sN" % c for c in comp] + ["STR%sNM1" % c for c in comp]
     host = {}
     for n in state:
         arr = ctx.download(n)
@@ -295,6 +302,17 @@ def run_kmm(a, rank, world, local_rank):
         host[n] = buf
     nbytes = sum(int(b.numel()) for b in host.values())
     e2e_steps = max(2, min(a.steps, 10))
+    # (1) kmm_run_host: the state bound to the host arrays; every step uploads all of it, steps and
+    # downloads all of it, one step's downloads overlapping the next step's uploads
+    for n, b in host.items():
+        ctx.bind_host(n, b.data_ptr(), int(b.numel()))
+    barrier()
+    ctx.event_record(2)
+    ctx.run_host(e2e_steps)
+    ctx.event_record(3)
+    e2e_ms = ctx.event_elapsed(2, 3)
+    ctx.unbind_host()
+    # (2) the same copies as single calls: kmm_upload per field, kmm_step, kmm_download per field
     barrier()
     ctx.event_record(2)
     for _ in range(e2e_steps):
@@ -304,9 +322,10 @@ def run_kmm(a, rank, world, local_rank):
         for n, b in host.items():
             ctx.download_ptr(n, b.data_ptr(), int(b.numel()))
     ctx.event_record(3)
-    e2e_ms = ctx.event_elapsed(2, 3)
+    calls_ms = ctx.event_elapsed(2, 3)
     barrier()
     e2e_ms, e2e_value = replicas.job_throughput(dist, e2e_ms, e2e_steps, world, "cuda")
+    calls_ms, calls_value = replicas.job_throughput(dist, calls_ms, e2e_steps, world, "cuda")
 
     result = None
     if rank == 0:
@@ -354,7 +373,9 @@ def run_kmm(a, rank, world, local_rank):
                        "stage_share": {k: round(v[0] / total_stage_ms, 4) for k, v in stages.items()} if total_stage_ms else {}},
             "roofline": roof,
             "e2e": {"value": round(e2e_value, 3), "unit": "timesteps/s", "h2d_bytes_per_step": nbytes,
-                    "d2h_bytes_per_step": nbytes, "steps": e2e_steps},
+                    "d2h_bytes_per_step": nbytes, "steps": e2e_steps, "call": "kmm_bind_host + kmm_run_host",
+                    "single_calls": {"value": round(calls_value, 3), "unit": "timesteps/s",
+                                     "call": "kmm_upload per field, kmm_step, kmm_download per field"}},
             "gpu_launches": int(launches),
             "clocks": dict(clk.summary(), **({"ms_per_step_x_median_mhz": round(ms_per_step * clk.summary()["sm_mhz"], 2)}
                                              if clk.summary().get("sm_mhz") else {})),

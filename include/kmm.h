@@ -261,6 +261,21 @@ int  kmm_step(kmm_ctx *ctx);
 /* `n` iterations (stops early with the status of a failing step) */
 int  kmm_run(kmm_ctx *ctx, int n);
 
+/* ---- state held in host arrays ---------------------------------------------
+ * The reference's time loop works on host arrays (main_dns.f90:198-811).  kmm_bind_host makes
+ * `host` (bytes = the field's size, reference layout) the home of a spectral, mean-mode, wall or
+ * particle field; host = NULL unbinds it, and field < 0 with host = NULL unbinds all.  Page-locked
+ * memory (cudaHostAlloc / cudaHostRegister) lets the copies run asynchronously; pageable memory
+ * works but serialises them.
+ * kmm_run_host runs `n` iterations as a host loop around the solver would: before every step each
+ * bound field is copied host -> device, after every step device -> host, so the host arrays hold
+ * each step's result (also that of a step that returns a stop status such as KMM_ERR_CFL, after
+ * which it returns).  A step's downloads and the next step's uploads run together on two copy
+ * streams, chunk by chunk.  The host arrays must not be touched during the call.  Without
+ * bindings it is kmm_run.                                                                      */
+int  kmm_bind_host(kmm_ctx *ctx, int field, void *host, size_t bytes);
+int  kmm_run_host(kmm_ctx *ctx, int n);
+
 /* ---- particles (part_track.f90) ----------------------------------------- */
 /* tracer_update(u,v,w), part_track.f90:360-433, from KMM_UP3D/VP3D/WP3D */
 int  kmm_tracer_update(kmm_ctx *ctx);

@@ -23,7 +23,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE
 # per-file flags: the Chebyshev recurrences and tau eliminations keep separate multiply / add
 # rounding like the reference's operation sequence
 PER_FILE = {"kmm_column.cu": ["-fmad=false"]}
-SOURCES = ["kmm_ctx.cu", "kmm_column.cu", "kmm_plane.cu", "kmm_fast.cu", "kmm_fused.cu", "kmm_colblk.cu", "kmm_tracer.cu", "kmm_step.cu", "kmm_noalloc.cu", "kmm_ztma.cu", "kmm_tcdct.cu"]
+SOURCES = ["kmm_ctx.cu", "kmm_column.cu", "kmm_plane.cu", "kmm_fast.cu", "kmm_fused.cu", "kmm_colblk.cu", "kmm_tracer.cu", "kmm_step.cu", "kmm_noalloc.cu", "kmm_ztma.cu", "kmm_tcdct.cu", "kmm_hoststate.cu"]
 HEADERS = ["kmm_internal.cuh", "kmm_warpcol.cuh", "kmm_fft.cuh", "kmm_fused.cuh", "kmm_colblk.cuh", "kmm_async.cuh"]
 
 

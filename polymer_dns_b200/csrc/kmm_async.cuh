@@ -32,25 +32,34 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
 // includes this header has its own copy, set through kasync_set_wait_limit from that unit.
 static __device__ unsigned long long kasync_wait_ns = 2000000000ull;
 
-// wait for phase `phase` of a barrier, at most `limit_ns` of %globaltimer; false if the limit ran out
+// one test of phase `phase` of a barrier (the hardware may hold the thread for a while first)
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, unsigned phase) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(sm_addr(bar)), "r"(phase)
+        : "memory");
+    return done != 0;
+}
+
+// wait for phase `phase` of a barrier, at most `limit_ns` of %globaltimer; false if the limit ran
+// out.  The first test comes before the timer is read, so a barrier that has already completed
+// costs one instruction.
 __device__ __forceinline__ bool mbar_wait_for(uint64_t *bar, unsigned phase, unsigned long long limit_ns) {
+    if (mbar_try(bar, phase)) return true;
     const unsigned long long t0 = gtimer();
     for (;;) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(sm_addr(bar)), "r"(phase)
-            : "memory");
-        if (done) return true;
+        if (mbar_try(bar, phase)) return true;
         if (gtimer() - t0 > limit_ns) return false;
     }
 }
 
-// the same with the unit's current limit (kasync_wait_ns)
+// the same with the unit's current limit (kasync_wait_ns, read only when the first test fails)
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase) {
+    if (mbar_try(bar, phase)) return true;
     return mbar_wait_for(bar, phase, kasync_wait_ns);
 }
 

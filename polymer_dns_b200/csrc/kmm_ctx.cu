@@ -334,6 +334,7 @@ extern "C" int kmm_ctx_destroy(kmm_ctx *ctx) {
     for (int e = 0; e < 16; ++e)
         if (ctx->user_ev[e]) cudaEventDestroy(ctx->user_ev[e]);
     kmm_ensemble_forget(ctx);   // cached ensemble graphs replay this context's buffers
+    kmm_hoststate_release(ctx);
     kmm_graph_release(ctx);
     kmm_fused_release(ctx);
     kmm_ztma_release(ctx);

@@ -128,8 +128,10 @@ struct kmm_ctx {
     float2 *rtw32[3]; // FP32 twiddles of 2 ny, mz, mx for the routine path's mixed form (kmm_fused.cu)
     double *d_frate;  // constant flow rate: W, G, the last correction, scratch (kmm_column.cu)
     int frate_ready;
+    void *hoststate;  // host arrays bound by kmm_bind_host, their copy streams and events (kmm_hoststate.cu)
 };
 
+void kmm_hoststate_release(kmm_ctx *ctx);
 void kmm_fused_release(kmm_ctx *ctx);
 int kmm_fused_step(kmm_ctx *ctx);
 // the fused step in two halves: enqueue every kernel and the read-back of CFL / status, then wait

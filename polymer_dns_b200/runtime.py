@@ -81,6 +81,10 @@ def lib():
         L.kmm_wait_selftest.restype = ctypes.c_int
         L.kmm_target_list.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
         L.kmm_target_list.restype = ctypes.c_int
+        L.kmm_bind_host.argtypes = [vp, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]
+        L.kmm_bind_host.restype = ctypes.c_int
+        L.kmm_run_host.argtypes = [vp, ctypes.c_int]
+        L.kmm_run_host.restype = ctypes.c_int
         for name, sig in _ROUTINES.items():
             f = getattr(L, "kmm_" + name)
             f.argtypes = [vp] + [_CT[c] for c in sig]
@@ -95,7 +99,7 @@ def exported_symbols():
             "kmm_upload", "kmm_download", "kmm_get_stats", "kmm_set_timing", "kmm_get_stage_times",
             "kmm_launch_count", "kmm_event_record", "kmm_event_elapsed", "kmm_xyzfft_noalloc", "kmm_flowstats",
             "kmm_ensemble_step", "kmm_ensemble_run", "kmm_tracer_cells", "kmm_wait_selftest",
-            "kmm_target_list"]
+            "kmm_target_list", "kmm_bind_host", "kmm_run_host"]
     return base + ["kmm_" + n for n in _ROUTINES]
 
 
@@ -213,6 +217,21 @@ class KmmContext:
     def download_ptr(self, f, ptr, nbytes):
         fid = self._id(f)
         self._check(self.L.kmm_download(self.h, fid, ctypes.c_void_p(ptr), nbytes), "kmm_download(%s)" % f)
+
+    def bind_host(self, f, ptr, nbytes):
+        """kmm_bind_host: make the host array at `ptr` (reference layout, page-locked for
+        asynchronous copies) the home of field `f` for run_host; ptr = 0 unbinds."""
+        fid = self._id(f)
+        self._check(self.L.kmm_bind_host(self.h, fid, ctypes.c_void_p(ptr) if ptr else None, int(nbytes)),
+                    "kmm_bind_host(%s)" % f)
+
+    def unbind_host(self):
+        self._check(self.L.kmm_bind_host(self.h, -1, None, 0), "kmm_bind_host")
+
+    def run_host(self, n, allow=()):
+        """kmm_run_host: n steps with the bound fields uploaded before and downloaded after every
+        step.  Returns the status (statuses in `allow` are returned, others raise)."""
+        return self._check(self.L.kmm_run_host(self.h, int(n)), "kmm_run_host", allow)
 
     def tracer_cells(self):
         """kmm_tracer_cells: the 1-based interpolation cell (imin, jmin, kmax) of every particle,
