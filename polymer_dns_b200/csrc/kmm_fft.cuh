@@ -233,6 +233,56 @@ struct Step<C, N, F, S, NQ, SWZ, TWS, false> {
         return Step<C, N, F + 1, S, NQ, SWZ, TWS, (F + 1 >= nfac(N))>::go(dst, src, tw, lane);
     }
 };
+
+// stage F of one sequence with its inputs from ld(x) and its outputs to st(x, value): the same
+// butterflies, twiddles and operation order as stage()
+template <typename C, int N, int F, int S, int TWS, typename LD, typename ST>
+__device__ __forceinline__ void stage_io(LD &ld, ST &st, const C *__restrict__ tw, int lane) {
+    constexpr int R = fac(N, F);
+    constexpr int NS = stride(N, F);
+    constexpr int NR = N / R;
+    constexpr int TSTEP = N / (NS * R);
+    constexpr int IT = (NR + 31) / 32;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int j = lane + 32 * it;
+        if (NR % 32 == 0 || j < NR) {
+            const int k = j % NS;
+            C v[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                C x = ld(j + r * NR);
+                if (NS > 1 && r > 0 && k) {
+                    C w = __ldg(&tw[r * k * TSTEP * TWS]);
+                    if (S > 0) w.y = -w.y;
+                    x = mul(x, w);
+                }
+                v[r] = x;
+            }
+            Dft<C, R, S>::run(v);
+            const int idxD = (j - k) * R + k;
+#pragma unroll
+            for (int q = 0; q < R; ++q) st(idxD + q * NS, v[q]);
+        }
+    }
+}
+
+// the stages between the first and the last, ping-ponging between two swizzled buffers; returns
+// the buffer holding the output of the last of them
+template <typename C, int N, int F, int S, int TWS, bool END>
+struct MidSteps;
+template <typename C, int N, int F, int S, int TWS>
+struct MidSteps<C, N, F, S, TWS, true> {
+    static __device__ __forceinline__ C *go(C *src, C *, const C *, int) { return src; }
+};
+template <typename C, int N, int F, int S, int TWS>
+struct MidSteps<C, N, F, S, TWS, false> {
+    static __device__ __forceinline__ C *go(C *src, C *dst, const C *tw, int lane) {
+        stage<C, N, F, S, 1, true, TWS>(src, dst, tw, lane);
+        __syncwarp();
+        return MidSteps<C, N, F + 1, S, TWS, (F + 2 >= nfac(N))>::go(dst, src, tw, lane);
+    }
+};
 }   // namespace kct
 
 // S = -1: exp(-2 pi i jk/N) (FFTW_FORWARD), +1: exp(+...) (FFTW_BACKWARD).  NQ sequences of
@@ -244,6 +294,27 @@ template <typename C, int N, int S, int NQ = 1, bool SWZ = false, int TWS = 1>
 __device__ __forceinline__ C *fft_warp_ct(C *a, C *b, const C *tw) {
     static_assert(kct::nfac(N) > 0, "transform length must be 2^a 3^b 5^c");
     return kct::Step<C, N, 0, S, NQ, SWZ, TWS, false>::go(a, b, tw, threadIdx.x & 31);
+}
+
+// fft_warp_ct of one sequence whose first stage reads its input through ld(x) (element x of the
+// sequence) and whose last stage writes its output through st(x, value), natural order, so that
+// neither needs a copy pass through shared memory; the stages in between use the swizzled
+// buffers a and b (private to the warp).  pre() runs between the second-last and the last stage
+// in every thread of the warp (a block-wide barrier there must be reached by every warp).  Same
+// arithmetic as fft_warp_ct.  The last stage reads buffer a when nfac(N) is even, else b; st may
+// write the other one.
+template <typename C, int N, int S, int TWS = 1, typename LD, typename ST, typename PRE>
+__device__ __forceinline__ void fft_warp_ct_io(LD ld, ST st, PRE pre, C *a, C *b, const C *tw) {
+    constexpr int L = kct::nfac(N);
+    static_assert(L >= 2, "fft_warp_ct_io needs at least two stages");
+    const int lane = threadIdx.x & 31;
+    auto to_a = [&](int x, C v) { a[swz<C>(x)] = v; };
+    kct::stage_io<C, N, 0, S, TWS>(ld, to_a, tw, lane);
+    __syncwarp();
+    const C *src = kct::MidSteps<C, N, 1, S, TWS, (2 >= L)>::go(a, b, tw, lane);
+    pre();
+    auto from_src = [&](int x) { return src[swz<C>(x)]; };
+    kct::stage_io<C, N, L - 1, S, TWS>(from_src, st, tw, lane);
 }
 
 // the transform lengths with compiled instances (3/2-rule grids of nx, nz = 32, 64, 96, 128, 384

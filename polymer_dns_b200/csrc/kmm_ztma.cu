@@ -8,13 +8,14 @@
 // mz (modes j > nz/2 move to mz - nz + j), inverse c2c along z, and store Q[g][y][z][kx].
 //
 // Data movement: one CTA per (kx, 4 consecutive y).  Its thread 0 issues one tiled TMA load per
-// base field (box: 4 y x all nz kz of one kx, 64 B rows, 64-byte swizzle) at the start, each on
-// its own mbarrier, so the whole 8 x 8 KB input tile is in flight at once and the first FFTs
-// start as soon as u has landed.  Four warps each transform one y column per output field (the
-// warp-private compile-time FFT of kmm_fft.cuh), the results go to a [y][z] staging tile, and a
-// tiled TMA store (box: 1 kx x mz z x 4 y) writes it out while the next field is transformed.
-// 101 KB of shared memory per CTA at mz = 192, so two CTAs share an SM and one's copies overlap
-// the other's FFTs.
+// base field (box: 4 y x all nz kz of one kx, 64 B rows, 64-byte swizzle), each on its own
+// mbarrier, into a ring of three tile slots (below).  Four warps each form one y column per output
+// field from the tiles and transform it (the warp-private compile-time FFT of kmm_fft.cuh); the
+// results go to a [y][z] staging tile, which a tiled TMA store (box: 1 kx x mz z x 4 y) writes out
+// while the next field is transformed.  62.5 KB of shared memory per CTA at mz = 192, so three
+// CTAs share an SM.  (Forming the inputs inside the FFT's first stage and writing the staging tile
+// from its last, as the FP32 form and the forward transforms do, made this kernel 11 % slower:
+// the staging tile's barrier then falls between two FFT stages.)
 //
 // Every wait on an mbarrier is bounded (KMM_OPT_WAIT_LIMIT_MS, default 2 s of %globaltimer); a wait
 // that runs out records KMM_ERR_TIMEOUT in the step's status word and the CTA finishes without the
@@ -192,8 +193,9 @@ __global__ void __launch_bounds__(ZTM_WARPS * 32, 3)
 // layout Yo[o][kx][kz][y].  One CTA per (kx, 4 consecutive y): one TMA load per field (box 1 kx x
 // mz z x 4 y, rows of 16 B), one warp per y column, and a TMA store per field of the [kz][4 y]
 // result tile (64 B rows, 64-byte swizzle: the layout of the inverse transform's input tiles).
-// The output tiles pass through two shared-memory slots: fields 0 and 1 are loaded at the start,
-// field o + 2 into slot o mod 2 once field o has been read, so three CTAs share an SM.
+// The input tiles pass through two shared-memory slots: fields 0 and 1 are loaded at the start,
+// field o + 2 into slot o mod 2 once field o has been read, so three CTAs share an SM.  The first
+// FFT stage reads its column straight from the tile.
 #define ZF_SLOTS 2
 template <int MZ>
 __global__ void __launch_bounds__(ZTM_WARPS * 32, 3)
@@ -231,9 +233,13 @@ __global__ void __launch_bounds__(ZTM_WARPS * 32, 3)
         ok = mbar_wait(&bar[o], 0) && ok;
         ready |= 1u << o;
         const double2 *t = tiles + (size_t)(o % ZF_SLOTS) * TIN + (size_t)y * MZ;
-        for (int z = lane; z < MZ; z += 32) a[swz<double2>(z)] = ok ? t[z] : make_double2(0.0, 0.0);
+        // the first FFT stage reads the tile row, the last writes the scratch buffer it does not read
+        auto ld = [&](int z) { return ok ? t[z] : make_double2(0.0, 0.0); };
+        double2 *r = kct::nfac(MZ) % 2 == 0 ? b : a;
+        auto st = [&](int z, double2 v) { r[swz<double2>(z)] = v; };
+        auto pre = [] {};
+        fft_warp_ct_io<double2, MZ, -1>(ld, st, pre, a, b, tw);
         __syncwarp();
-        const double2 *r = fft_warp_ct<double2, MZ, -1, 1, true>(a, b, tw);
         if (threadIdx.x == 0) tma_store_wait_read();   // the previous field's store has read the stage
         __syncthreads();
         for (int kz = lane; kz < NZ; kz += 32) {
@@ -321,7 +327,7 @@ __global__ void __launch_bounds__(ZT32_WARPS * 32, 2)
         if (f1 >= 0) need(f1);
         const float2 *t0 = tiles + ((size_t)f0 * ZT32_KX + kl) * TILE;
         const float2 *t1 = f1 >= 0 ? tiles + ((size_t)f1 * ZT32_KX + kl) * TILE : t0;
-        for (int z = lane; z < MZ; z += 32) {
+        auto ld = [&](int z) {
             float2 val = make_float2(0.f, 0.f);
             if (z < NZH || z >= MZ - NZH) {
                 const int kz = z < NZH ? z : z - (MZ - NZ);
@@ -345,13 +351,14 @@ __global__ void __launch_bounds__(ZT32_WARPS * 32, 2)
                 default: val = p; break;
                 }
             }
-            a[swz<float2>(z)] = val;
-        }
-        __syncwarp();
-        const float2 *r = fft_warp_ct<float2, MZ, +1, 1, true>(a, b, tw);
-        if (threadIdx.x == 0) tma_store_wait_read();
-        __syncthreads();
-        for (int z = lane; z < MZ; z += 32) stage[((size_t)y * MZ + z) * ZT32_KX + kl] = r[swz<float2>(z)];
+            return val;
+        };
+        auto pre = [&]() {
+            if (threadIdx.x == 0) tma_store_wait_read();
+            __syncthreads();
+        };
+        auto st = [&](int z, float2 v) { stage[((size_t)y * MZ + z) * ZT32_KX + kl] = v; };
+        fft_warp_ct_io<float2, MZ, +1>(ld, st, pre, a, b, tw);
         fence_async_smem();
         __syncthreads();
         if (threadIdx.x == 0) tma_store4(&tout, 2 * kx0, 0, y0, g, stage);
@@ -390,10 +397,12 @@ __global__ void __launch_bounds__(ZT32_WARPS * 32, 2)
     for (int o = 0; o < nout; ++o) {
         ok = mbar_wait(&bar[o], 0) && ok;
         const float2 *t = tiles + (size_t)o * TIN;
-        for (int z = lane; z < MZ; z += 32)
-            a[swz<float2>(z)] = ok ? t[((size_t)y * MZ + z) * ZT32_KX + kl] : make_float2(0.f, 0.f);
+        auto ld = [&](int z) { return ok ? t[((size_t)y * MZ + z) * ZT32_KX + kl] : make_float2(0.f, 0.f); };
+        float2 *r = kct::nfac(MZ) % 2 == 0 ? b : a;
+        auto st = [&](int z, float2 v) { r[swz<float2>(z)] = v; };
+        auto pre = [] {};
+        fft_warp_ct_io<float2, MZ, -1>(ld, st, pre, a, b, tw);
         __syncwarp();
-        const float2 *r = fft_warp_ct<float2, MZ, -1, 1, true>(a, b, tw);
         if (threadIdx.x == 0) tma_store_wait_read();
         __syncthreads();
         for (int kz = lane; kz < NZ; kz += 32) {
