@@ -716,6 +716,117 @@ int kmm_colblk_solve(kmm_ctx *ctx, double2 *u, double g, int robin, double at, d
     return kmm_colblk_solve_many(ctx, &u, 1, g, robin, at, bt, ab, bb, gt, gb);
 }
 
+// ---------------------------------------------------------------------------
+// The routine step's phirhs followed by its solve(s), in one pass over each column pair: [phi =
+// v'' - k^2 v (main_dns.f90:363-375),] phirhs (solvers.f90:555-676) with the nonlinear terms fn,
+// fnm1 (fnm1 = NULL: the n-1 term is 2 fn), then one or two tau solves with zero boundary values
+// (solve, solvers.f90:174-553, or penta, 680-1061; ib = 0).  The same arithmetic as k_phirhs_a /
+// cderiv / k_phirhs_b followed by k_bsolve, without the intermediate fields.
+// ---------------------------------------------------------------------------
+struct PhiSolveJobs {
+    double2 *x[KMM_SOLVE_BATCH];
+    const double2 *fn[KMM_SOLVE_BATCH];
+    const double2 *fnm1[KMM_SOLVE_BATCH];
+};
+
+struct PhiSolveCfg {   // the cached tables of one solve's configuration, its g, Robin (1) or Dirichlet (0)
+    const double *tab[5];
+    double g;
+    int robin;
+};
+
+template <int K>
+__device__ __forceinline__ void bsolve_cfg(BCol<K> &x, const PhiSolveCfg &S, const BPair &P, double c0,
+                                           const double *rj) {
+    constexpr int NYP = 16 * K + 1;
+    constexpr unsigned FULL = 0xffffffffu;
+    const double2 zero = make_double2(0.0, 0.0);
+    TauTab T;
+    T.td = S.tab[0] + (size_t)P.tcol * NYP;
+    T.te = S.tab[1] + (size_t)P.tcol * NYP;
+    T.tb1 = S.tab[2] + (size_t)P.tcol * NYP;
+    T.tb2 = S.tab[3] + (size_t)P.tcol * NYP;
+    T.tf = S.tab[4] + (size_t)P.tcol * 4;
+    if (S.robin) bsolve_robin<K>(x, T, zero, zero, P.w2 + S.g, c0, rj, FULL);
+    else bsolve_dirichlet<K>(x, T, zero, zero, P.w2 + S.g, c0, rj, FULL);
+}
+
+template <int K>
+__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB)
+    k_bphirhs_solve(PhiSolveJobs J, PhiSolveCfg S0, PhiSolveCfg S1, int nsolve, int phi,
+                    const double *__restrict__ rj, const double *__restrict__ wavx, const double *__restrict__ wavz,
+                    int nz, int nzh, int nxh, double re, double var, double dt, double th, double dyde, double c0) {
+    constexpr unsigned FULL = 0xffffffffu;
+    __shared__ double2 sbuf[CB_WARPS][2 * (16 * K + 8)];
+    double2 *wsm = sbuf[threadIdx.x >> 5];   // bload_s / bstore_s scratch
+    double2 *X = J.x[blockIdx.y];
+    const double2 *F = J.fn[blockIdx.y], *FM = J.fnm1[blockIdx.y];
+    BPair P;
+    if (!bpair<K>(P, nz, nzh, nxh, wavx, wavz)) return;
+    BCol<K> x;
+    bload_s<K>(x, X + P.off, wsm);
+    if (phi) {
+        BCol<K> d1, d2;
+        bcderiv<K>(d1, x, dyde, FULL);
+        bcderiv<K>(d2, d1, dyde, FULL);
+#pragma unroll
+        for (int m = 0; m <= K; ++m)
+            x.v[m] = make_double2(d2.v[m].x - P.w2 * x.v[m].x, d2.v[m].y - P.w2 * x.v[m].y);
+    }
+    {
+        BCol<K> f1, f0;
+        bload_s<K>(f1, F + P.off, wsm);
+        if (FM) {
+            bload_s<K>(f0, FM + P.off, wsm);
+        } else {
+#pragma unroll
+            for (int m = 0; m <= K; ++m) f0.v[m] = make_double2(2.0 * f1.v[m].x, 2.0 * f1.v[m].y);
+        }
+        bphirhs<K>(x, f1, f0, re, var, dt, th, P.w2, dyde, FULL);
+    }
+    bsolve_cfg<K>(x, S0, P, c0, rj);
+    if (nsolve > 1) bsolve_cfg<K>(x, S1, P, c0, rj);
+    bstore_s<K>(X + P.off, x, wsm);
+}
+
+int kmm_colblk_phirhs_solve(kmm_ctx *ctx, double2 *const *x, const double2 *const *fn, const double2 *const *fnm1,
+                            int nf, double var, int phi, int nsolve, const KmmSolveSpec *spec) {
+    const int K = colblk_k(ctx);
+    if (!K || K > 8 || !ctx->use_colblk) return KMM_ERR_UNSUPPORTED;
+    if (nf < 1 || nf > KMM_SOLVE_BATCH || nsolve < 1 || nsolve > 2) return KMM_ERR_ARG;
+    PhiSolveCfg S[2];
+    const double *rj = NULL;
+    for (int k = 0; k < 2; ++k) {
+        const KmmSolveSpec &q = spec[k < nsolve ? k : 0];
+        const int st = kmm_tau_tabset(ctx, q.g, q.robin, q.at, q.bt, q.ab, q.bb, S[k].tab, &rj);
+        if (st != KMM_OK) return st;
+        S[k].g = q.g;
+        S[k].robin = q.robin;
+    }
+    PhiSolveJobs J;
+    for (int m = 0; m < nf; ++m) {
+        J.x[m] = x[m];
+        J.fn[m] = fn[m];
+        J.fnm1[m] = fnm1[m];
+    }
+    const int npairs = ctx->nxh * (ctx->nz / 2);
+    const dim3 grid((npairs + CB_WARPS - 1) / CB_WARPS, nf);
+#define PS(KK)                                                                                                    \
+    k_bphirhs_solve<KK><<<grid, CB_WARPS * 32, 0, ctx->stream>>>(J, S[0], S[1], nsolve, phi, rj, ctx->d_wavx,   \
+                                                                ctx->d_wavz, ctx->nz, ctx->nzh, ctx->nxh, ctx->re, \
+                                                                var, ctx->dt, ctx->theta, ctx->dyde, ctx->h_c[0])
+    switch (K) {
+    case 2: PS(2); break;
+    case 4: PS(4); break;
+    case 6: PS(6); break;
+    case 8: PS(8); break;
+    default: return KMM_ERR_UNSUPPORTED;
+    }
+#undef PS
+    CKL();
+    return KMM_OK;
+}
+
 int kmm_colblk_bwd(kmm_ctx *ctx, const ColBwdArgs &B, const void *tw, bool fp32) {
     const int K = colblk_k(ctx);
     if (!K) return KMM_ERR_UNSUPPORTED;

@@ -194,6 +194,16 @@ int kmm_colblk_solve(kmm_ctx *ctx, double2 *u, double g, int robin, double at, d
 #define KMM_SOLVE_BATCH 8
 int kmm_colblk_solve_many(kmm_ctx *ctx, double2 *const *u, int nf, double g, int robin, double at, double bt,
                           double ab, double bb, const double2 *gt, const double2 *gb);
+// the routine step's phirhs followed by one or two tau solves with zero boundary values, fused per
+// column pair (blocked kernels, ny = 32 .. 128): x[m] <- solve(phirhs([phi of] x[m]; fn[m], fnm1[m],
+// var)), fnm1[m] = NULL taking 2 fn[m]; KMM_ERR_UNSUPPORTED where the blocked kernels do not apply
+struct KmmSolveSpec {
+    double g;
+    int robin;   // 1: penta (Robin coefficients at, bt, ab, bb), 0: solve (Dirichlet)
+    double at, bt, ab, bb;
+};
+int kmm_colblk_phirhs_solve(kmm_ctx *ctx, double2 *const *x, const double2 *const *fn, const double2 *const *fnm1,
+                            int nf, double var, int phi, int nsolve, const KmmSolveSpec *spec);
 // penta (ib = 0) of nf distinct fields of one configuration
 int kmm_internal_penta_many(kmm_ctx *ctx, double2 *const *u, int nf, double g, double at, double bt, double ab,
                             double bb, const double2 *gt, const double2 *gb);

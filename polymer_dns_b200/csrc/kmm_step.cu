@@ -357,51 +357,93 @@ extern "C" int kmm_step(kmm_ctx *ctx) {
                 if (!nl[m]) return KMM_ERR_NOMEM;
             }
             RET(kmm_internal_polynl(ctx, nl));
-            // the six components' phirhs in batched launches, each component with its own wrkc
-            // and wrk1 (scratch ids 12 .. 23); its n-1 term 2 nl is formed in the kernel (NULL)
-            double2 *wc[6], *w1[6], *cm[6];
+            // the six components' phirhs and penta: its n-1 term 2 nl is formed in the kernel (NULL)
+            double2 *cm[6];
             const double2 *nlc[6], *nl2c[6];
             for (int m = 0; m < 6; ++m) {
-                wc[m] = poly_scratch(ctx, 12 + m);
-                w1[m] = poly_scratch(ctx, 18 + m);
                 cm[m] = SPEC(ctx, kPolyComp[m]);
-                if (!wc[m] || !w1[m] || !cm[m]) return KMM_ERR_NOMEM;
+                if (!cm[m]) return KMM_ERR_NOMEM;
                 nlc[m] = nl[m];
                 nl2c[m] = NULL;
             }
-            RET(kmm_internal_phirhs_many(ctx, cm, nlc, nl2c, 6, ctx->p.diffpoly, wc, w1));
+            const double g = (re * ctx->p.diffpoly) / (dt * th);
+            const KmmSolveSpec sp = {g, 1, 0.0, 1.0, 0.0, 1.0};
+            RET(kmm_zero(ctx, KMM_BCTOP));
+            RET(kmm_zero(ctx, KMM_BCBOT));
+            int pst = kmm_colblk_phirhs_solve(ctx, cm, nlc, nl2c, 6, ctx->p.diffpoly, 0, 1, &sp);
+            if (pst == KMM_ERR_UNSUPPORTED) {
+                // batched launches, each component with its own wrkc and wrk1 (scratch ids 12 .. 23)
+                double2 *wc[6], *w1[6];
+                for (int m = 0; m < 6; ++m) {
+                    wc[m] = poly_scratch(ctx, 12 + m);
+                    w1[m] = poly_scratch(ctx, 18 + m);
+                    if (!wc[m] || !w1[m]) return KMM_ERR_NOMEM;
+                }
+                RET(kmm_internal_phirhs_many(ctx, cm, nlc, nl2c, 6, ctx->p.diffpoly, wc, w1));
+                pst = kmm_internal_penta_many(ctx, cm, 6, g, 0.0, 1.0, 0.0, 1.0, SPEC(ctx, KMM_BCTOP),
+                                              SPEC(ctx, KMM_BCBOT));
+            }
+            RET(pst);
             for (int m = 0; m < 6; ++m) {
                 RET(swap_fields(ctx, KMM_C11NM1 + m, KMM_C11N + m));
                 RET(swap_fields(ctx, KMM_STR11NM1 + m, KMM_STR11N + m));
             }
-            const double g = (re * ctx->p.diffpoly) / (dt * th);
-            RET(kmm_zero(ctx, KMM_BCTOP));
-            RET(kmm_zero(ctx, KMM_BCBOT));
-            RET(kmm_internal_penta_many(ctx, cm, 6, g, 0.0, 1.0, 0.0, 1.0, SPEC(ctx, KMM_BCTOP), SPEC(ctx, KMM_BCBOT)));
             RET(norm_ids(ctx, kPolyComp, 6));
             RET(kmm_copy(ctx, KMM_C21, KMM_C12));
             RET(kmm_copy(ctx, KMM_C31, KMM_C13));
             RET(kmm_copy(ctx, KMM_C32, KMM_C23));
         }
     }
+    // phirhs and its solves in one blocked kernel per field where compiled (every boundary value
+    // is zero: phirhs zeroes bctop / bcbot, main_dns.f90:39, solvers.f90:670-671), else routine by
+    // routine
+    auto phi_solve = [&](int x, int fn, int fnm1, double var, int phi, int nsolve, const KmmSolveSpec *sp) -> int {
+        double2 *xp = SPEC(ctx, x);
+        const double2 *fp = SPEC(ctx, fn), *fmp = SPEC(ctx, fnm1);
+        if (!xp || !fp || !fmp) return KMM_ERR_NOMEM;
+        return kmm_colblk_phirhs_solve(ctx, &xp, &fp, &fmp, 1, var, phi, nsolve, sp);
+    };
     if (ctx->p.scalar_on) {
-        RET(kmm_phirhs(ctx, KMM_SCALAR, KMM_SCN, KMM_SCNM1, ctx->p.diff));
-        RET(swap_fields(ctx, KMM_SCNM1, KMM_SCN));
         const double g = (re * ctx->p.diff) / (dt * th);
+        const KmmSolveSpec sp = ctx->p.scalar_bc == 1 ? KmmSolveSpec{g, 1, 1.0, 0.0, 1.0, 0.0}
+                                                      : KmmSolveSpec{g, 1, 0.0, 1.0, 0.0, 1.0};
         RET(kmm_zero(ctx, KMM_BCTOP));   // bcscltop = bcsclbot = 0 (main_dns.f90:39)
         RET(kmm_zero(ctx, KMM_BCBOT));
-        if (ctx->p.scalar_bc == 1) RET(kmm_penta(ctx, KMM_SCALAR, g, 0, 1.0, 0.0, 1.0, 0.0));
-        else RET(kmm_penta(ctx, KMM_SCALAR, g, 0, 0.0, 1.0, 0.0, 1.0));
+        int st = phi_solve(KMM_SCALAR, KMM_SCN, KMM_SCNM1, ctx->p.diff, 0, 1, &sp);
+        if (st == KMM_ERR_UNSUPPORTED) {
+            RET(kmm_phirhs(ctx, KMM_SCALAR, KMM_SCN, KMM_SCNM1, ctx->p.diff));
+            st = kmm_penta(ctx, KMM_SCALAR, g, 0, sp.at, sp.bt, sp.ab, sp.bb);
+        }
+        RET(st);
+        RET(swap_fields(ctx, KMM_SCNM1, KMM_SCN));
     }
-    RET(kmm_phi_from_v(ctx));
-    RET(kmm_phirhs(ctx, KMM_V, KMM_FN, KMM_FNM1, 1.0));
-    RET(swap_fields(ctx, KMM_FNM1, KMM_FN));
-    RET(kmm_solve(ctx, KMM_V, re / (dt * th), 0));
-    RET(kmm_solve(ctx, KMM_V, 0.0, 0));
-    RET(kmm_phirhs(ctx, KMM_OMY, KMM_GN, KMM_GNM1, 1.0));
-    RET(swap_fields(ctx, KMM_GNM1, KMM_GN));
-    RET(kmm_influence(ctx));
-    RET(kmm_penta(ctx, KMM_OMY, re / (dt * th), 0, ctx->atu, ctx->btu, ctx->abu, ctx->bbu));
+    {
+        const KmmSolveSpec sv[2] = {{re / (dt * th), 0, 0.0, 0.0, 0.0, 0.0}, {0.0, 0, 0.0, 0.0, 0.0, 0.0}};
+        int st = phi_solve(KMM_V, KMM_FN, KMM_FNM1, 1.0, 1, 2, sv);
+        if (st == KMM_ERR_UNSUPPORTED) {
+            RET(kmm_phi_from_v(ctx));
+            RET(kmm_phirhs(ctx, KMM_V, KMM_FN, KMM_FNM1, 1.0));
+            RET(kmm_solve(ctx, KMM_V, sv[0].g, 0));
+            st = kmm_solve(ctx, KMM_V, sv[1].g, 0);
+        }
+        RET(st);
+        RET(swap_fields(ctx, KMM_FNM1, KMM_FN));
+    }
+    {
+        const KmmSolveSpec so = {re / (dt * th), 1, ctx->atu, ctx->btu, ctx->abu, ctx->bbu};
+        int st = phi_solve(KMM_OMY, KMM_GN, KMM_GNM1, 1.0, 0, 1, &so);
+        if (st == KMM_ERR_UNSUPPORTED) {
+            RET(kmm_phirhs(ctx, KMM_OMY, KMM_GN, KMM_GNM1, 1.0));
+            RET(kmm_influence(ctx));
+            st = kmm_penta(ctx, KMM_OMY, so.g, 0, so.at, so.bt, so.ab, so.bb);
+        } else if (st == KMM_OK) {
+            st = kmm_influence(ctx);   // v only: omega_y's solve does not depend on it
+        }
+        RET(st);
+        RET(swap_fields(ctx, KMM_GNM1, KMM_GN));
+    }
+    RET(kmm_zero(ctx, KMM_BCTOP));   // as phirhs leaves them
+    RET(kmm_zero(ctx, KMM_BCBOT));
     RET(kmm_uzero(ctx, 1));
     RET(kmm_flowrate_apply(ctx, ctx->stream));
     RET(kmm_uzero(ctx, 3));
