@@ -723,20 +723,34 @@ __global__ void __launch_bounds__(XpW<C>::n * 32) k_xphys2(const C *__restrict__
             if (kk > 0) a[swz<C>(MX - kk)] = kct::mk<C>(A_.x + B_.y, -A_.y + B_.x);
         }
         __syncwarp();
-        const C *r = fft_warp_ct<C, MX, +1, 1, true>(a, b, tw);
-        // the result may sit in the pair's own rows: read it all before writing the real rows
-        constexpr int E = (MX + 31) / 32;
-        C rv[E];
+        if constexpr (kct::nfac(MX) % 2 == 1) {
+            // an odd number of FFT stages: the first writes the pair's rows (as one complex
+            // buffer), the second reads them back into a, and the last reads a and writes the
+            // two real rows straight into the rows it no longer needs
+            T *pf = phys + (size_t)f * MX, *pg = phys + (size_t)(g >= 0 ? g : f) * MX;
+            auto ld = [&](int x) { return a[swz<C>(x)]; };
+            auto st = [&](int x, C v) {
+                pf[x] = v.x;
+                if (g >= 0) pg[x] = v.y;
+            };
+            auto pre = [] {};
+            fft_warp_ct_io<C, MX, +1>(ld, st, pre, b, a, tw);
+        } else {
+            const C *r = fft_warp_ct<C, MX, +1, 1, true>(a, b, tw);
+            // the result may sit in the pair's own rows: read it all before writing the real rows
+            constexpr int E = (MX + 31) / 32;
+            C rv[E];
 #pragma unroll
-        for (int e = 0; e < E; ++e)
-            if (lane + 32 * e < MX) rv[e] = r[swz<C>(lane + 32 * e)];
-        __syncwarp();
+            for (int e = 0; e < E; ++e)
+                if (lane + 32 * e < MX) rv[e] = r[swz<C>(lane + 32 * e)];
+            __syncwarp();
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int x = lane + 32 * e;
-            if (x < MX) {
-                phys[(size_t)f * MX + x] = rv[e].x;
-                if (g >= 0) phys[(size_t)g * MX + x] = rv[e].y;
+            for (int e = 0; e < E; ++e) {
+                const int x = lane + 32 * e;
+                if (x < MX) {
+                    phys[(size_t)f * MX + x] = rv[e].x;
+                    if (g >= 0) phys[(size_t)g * MX + x] = rv[e].y;
+                }
             }
         }
         __syncwarp();
@@ -789,10 +803,15 @@ __global__ void __launch_bounds__(XW * 32) k_xfwd2(const typename kct::Real<C>::
     const size_t n3 = (size_t)nyp * mz * MX, g3 = ((size_t)y * mz + z) * MX;
     for (int pr = warp; pr < (nout + 1) / 2; pr += XW) {
         const int o = 2 * pr, g = o + 1 < nout ? o + 1 : -1;
-        for (int x = lane; x < MX; x += 32)
-            a[swz<C>(x)] = kct::mk<C>(po[(size_t)o * n3 + g3 + x], g >= 0 ? po[(size_t)g * n3 + g3 + x] : (T)0);
+        // the FFT's first stage reads the two real rows straight from global memory, its last
+        // writes the scratch buffer the stage does not read
+        const T *ro = po + (size_t)o * n3 + g3, *rg = po + (size_t)(g >= 0 ? g : o) * n3 + g3;
+        auto ld = [&](int x) { return kct::mk<C>(ro[x], g >= 0 ? rg[x] : (T)0); };
+        C *r = kct::nfac(MX) % 2 == 0 ? b : a;
+        auto st = [&](int x, C v) { r[swz<C>(x)] = v; };
+        auto pre = [] {};
+        fft_warp_ct_io<C, MX, -1>(ld, st, pre, a, b, tw);
         __syncwarp();
-        const C *r = fft_warp_ct<C, MX, -1, 1, true>(a, b, tw);
         for (int k = lane; k < NXH; k += 32) {
             const C Z = r[swz<C>(k)];
             C Zc = r[swz<C>(k == 0 ? 0 : MX - k)];
