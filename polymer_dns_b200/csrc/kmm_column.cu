@@ -837,8 +837,7 @@ __global__ void __launch_bounds__(128) k_uzero(double *u0g, const double *h1g, c
 #undef UZ_ROW
 }
 
-extern "C" int kmm_uzero(kmm_ctx *ctx, int uflag) {
-    if (!ctx || (uflag != 1 && uflag != 3)) return KMM_ERR_ARG;
+int kmm_internal_uzero(kmm_ctx *ctx, int uflag, cudaStream_t st) {
     double *u0 = REAL(ctx, uflag == 1 ? KMM_U0 : KMM_W0);
     double *h1 = REAL(ctx, uflag == 1 ? KMM_H1N : KMM_H3N);
     double *h1l = REAL(ctx, uflag == 1 ? KMM_H1NM1 : KMM_H3NM1);
@@ -847,13 +846,18 @@ extern "C" int kmm_uzero(kmm_ctx *ctx, int uflag) {
     RET(kmm_smem_attr(ctx, (const void *)k_uzero, sm));
     // uflag 3 passes btu, as the reference does (solvers.f90:1173)
     if (uflag == 1)
-        k_uzero<<<1, 128, sm, ctx->stream>>>(u0, h1, h1l, ctx->nyp, ctx->re, ctx->dt, ctx->theta, ctx->dyde, ctx->atu,
-                                             ctx->btu, ctx->gtu, ctx->abu, ctx->bbu, ctx->gbu, ctx->h_c[0], ctx->h_wavz[0]);
+        k_uzero<<<1, 128, sm, st>>>(u0, h1, h1l, ctx->nyp, ctx->re, ctx->dt, ctx->theta, ctx->dyde, ctx->atu,
+                                    ctx->btu, ctx->gtu, ctx->abu, ctx->bbu, ctx->gbu, ctx->h_c[0], ctx->h_wavz[0]);
     else
-        k_uzero<<<1, 128, sm, ctx->stream>>>(u0, h1, h1l, ctx->nyp, ctx->re, ctx->dt, ctx->theta, ctx->dyde, ctx->atw,
-                                             ctx->btu, ctx->gtw, ctx->abw, ctx->bbw, ctx->gbw, ctx->h_c[0], ctx->h_wavz[0]);
+        k_uzero<<<1, 128, sm, st>>>(u0, h1, h1l, ctx->nyp, ctx->re, ctx->dt, ctx->theta, ctx->dyde, ctx->atw,
+                                    ctx->btu, ctx->gtw, ctx->abw, ctx->bbw, ctx->gbw, ctx->h_c[0], ctx->h_wavz[0]);
     CKL();
     return KMM_OK;
+}
+
+extern "C" int kmm_uzero(kmm_ctx *ctx, int uflag) {
+    if (!ctx || (uflag != 1 && uflag != 3)) return KMM_ERR_ARG;
+    return kmm_internal_uzero(ctx, uflag, ctx->stream);
 }
 
 // ---------------------------------------------------------------------------

@@ -185,6 +185,8 @@ int kmm_internal_norm(kmm_ctx *ctx, double2 *a);
 int kmm_internal_norm_many(kmm_ctx *ctx, double2 *const *a, int nf);
 int kmm_internal_wallderiv(kmm_ctx *ctx, const double2 *f, int order, int wall, double2 *out, int iy);
 int kmm_internal_solve(kmm_ctx *ctx, double2 *u, double g, int ib, const double2 *bct, const double2 *bcb);
+// uzero for u0 (uflag 1) or w0 (3) on stream st (one block, the (0,0) mode)
+int kmm_internal_uzero(kmm_ctx *ctx, int uflag, cudaStream_t st);
 // the routine solve / penta with the blocked column kernels (ny = 32, 64, 96, 128; ib = 0);
 // KMM_ERR_UNSUPPORTED where they do not apply (kmm_colblk.cu)
 int kmm_colblk_solve(kmm_ctx *ctx, double2 *u, double g, int robin, double at, double bt, double ab, double bb,

@@ -444,9 +444,14 @@ extern "C" int kmm_step(kmm_ctx *ctx) {
     }
     RET(kmm_zero(ctx, KMM_BCTOP));   // as phirhs leaves them
     RET(kmm_zero(ctx, KMM_BCBOT));
-    RET(kmm_uzero(ctx, 1));
+    // the u0 and w0 solves (each one block) side by side: w0's on the side stream
+    CK(cudaEventRecord(ctx->fork_ev, ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
+    RET(kmm_internal_uzero(ctx, 3, ctx->side));
+    RET(kmm_internal_uzero(ctx, 1, ctx->stream));
     RET(kmm_flowrate_apply(ctx, ctx->stream));
-    RET(kmm_uzero(ctx, 3));
+    CK(cudaEventRecord(ctx->join_ev, ctx->side));
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0));
     k_zero_mean<<<1, 256, 0, ctx->stream>>>(SPEC(ctx, KMM_OMY), ctx->nyp);
     CKL();
     RET(kmm_copy(ctx, KMM_H1NM1, KMM_H1N));
