@@ -266,6 +266,42 @@ struct XRecipe {
     unsigned char qa[MAXIO / 2], qb[MAXIO / 2], xd[MAXIO / 2];
 };
 
+// the z inverse at a compiled length N: warp c transforms column c of the block, its FFT's first
+// stage reading the column's nz modes straight from global memory (zero-padded to N, times i kx or
+// i kz where the recipe asks), its last stage writing the block buffer in the fb_at layout;
+// returns that buffer, visible to the whole block
+template <typename C, int N>
+__device__ __forceinline__ C *zbwd_io(const C *__restrict__ src, C *a, C *b, const C *__restrict__ tw, int nk, int nz,
+                                      int kx0, int mult, const double *__restrict__ wavx,
+                                      const double *__restrict__ wavz) {
+    typedef typename kct::Real<C>::T T;
+    static_assert(ZKB == 8, "one column per warp");
+    C *res = kct::nfac(N) % 2 == 1 ? a : b;
+    const int c = threadIdx.x >> 5;
+    if (c < nk) {
+        const size_t w = (size_t)c * (N + FB_PAD);
+        const C *col = src + (size_t)c * nz;
+        const int nzh = nz / 2, hi = N - nz + nzh;
+        auto ld = [&](int z) {
+            C v = kct::mk<C>((T)0, (T)0);
+            if (z < nzh || z >= hi) {
+                const int j = z < nzh ? z : z - (N - nz);
+                v = col[j];
+                if (mult) {   // i k v
+                    const T k = (T)(mult == 1 ? wavx[kx0 + c] : wavz[j]);
+                    v = kct::mk<C>(-k * v.y, k * v.x);
+                }
+            }
+            return v;
+        };
+        auto st = [&](int x, C v) { res[w + swz<C>(x)] = v; };
+        auto pre = [] {};
+        fft_warp_ct_io<C, N, +1>(ld, st, pre, a + w, b + w, tw);
+    }
+    __syncthreads();
+    return res;
+}
+
 template <typename C>
 __global__ void __launch_bounds__(256, 4) k_zfft_bwd(const C *__restrict__ pl, C *__restrict__ q, const __grid_constant__ DevPlan P,
                                                   const C *__restrict__ tw, int nyp, int nz, int nxh, int mz,
@@ -280,30 +316,44 @@ __global__ void __launch_bounds__(256, 4) k_zfft_bwd(const C *__restrict__ pl, C
     const int nzh = nz / 2;
     C *a = sm, *b = sm + fb_len(ZKB, mz);
     const bool ct = fb_compiled(mz);
-    for (int e = threadIdx.x; e < fb_len(ZKB, mz); e += blockDim.x) a[e] = kct::mk<C>((T)0, (T)0);
-    __syncthreads();
     const C *src = pl + (((size_t)fb * nyp + y) * nxh + kx0) * nz;
-    for (int e0 = threadIdx.x; e0 < nk * nz; e0 += LDG * 256) {
-        C wv[LDG];
-#pragma unroll
-        for (int u = 0; u < LDG; ++u)
-            if (e0 + 256 * u < nk * nz) wv[u] = src[e0 + 256 * u];
-#pragma unroll
-        for (int u = 0; u < LDG; ++u) {
-            const int e = e0 + 256 * u;
-            if (e >= nk * nz) break;
-            const int c = e / nz, j = e - c * nz;
-            const int jj = (j < nzh) ? j : (mz - nz) + j;
-            C v = wv[u];
-            if (mult) {   // i k v
-                const T k = (T)(mult == 1 ? wavx[kx0 + c] : wavz[j]);
-                v = kct::mk<C>(-k * v.y, k * v.x);
-            }
-            a[fb_at<C, ZKB>(c, jj, mz, ct)] = v;
-        }
+    C *r = NULL;
+    switch (mz) {
+    case 48: r = zbwd_io<C, 48>(src, a, b, tw, nk, nz, kx0, mult, wavx, wavz); break;
+    case 64: r = zbwd_io<C, 64>(src, a, b, tw, nk, nz, kx0, mult, wavx, wavz); break;
+    case 96: r = zbwd_io<C, 96>(src, a, b, tw, nk, nz, kx0, mult, wavx, wavz); break;
+    case 128: r = zbwd_io<C, 128>(src, a, b, tw, nk, nz, kx0, mult, wavx, wavz); break;
+    case 144: r = zbwd_io<C, 144>(src, a, b, tw, nk, nz, kx0, mult, wavx, wavz); break;
+    case 192: r = zbwd_io<C, 192>(src, a, b, tw, nk, nz, kx0, mult, wavx, wavz); break;
+    case 256: r = zbwd_io<C, 256>(src, a, b, tw, nk, nz, kx0, mult, wavx, wavz); break;
+    case 576: r = zbwd_io<C, 576>(src, a, b, tw, nk, nz, kx0, mult, wavx, wavz); break;
+    default: break;
     }
-    __syncthreads();
-    C *r = fft_block<C, +1, ZKB>(P, a, b, tw, mz);
+    if (!r) {   // the runtime block FFT: stage the zero-padded columns, then transform
+        for (int e = threadIdx.x; e < fb_len(ZKB, mz); e += blockDim.x) a[e] = kct::mk<C>((T)0, (T)0);
+        __syncthreads();
+        for (int e0 = threadIdx.x; e0 < nk * nz; e0 += LDG * 256) {
+            C wv[LDG];
+#pragma unroll
+            for (int u = 0; u < LDG; ++u)
+                if (e0 + 256 * u < nk * nz) wv[u] = src[e0 + 256 * u];
+#pragma unroll
+            for (int u = 0; u < LDG; ++u) {
+                const int e = e0 + 256 * u;
+                if (e >= nk * nz) break;
+                const int c = e / nz, j = e - c * nz;
+                const int jj = (j < nzh) ? j : (mz - nz) + j;
+                C v = wv[u];
+                if (mult) {   // i k v
+                    const T k = (T)(mult == 1 ? wavx[kx0 + c] : wavz[j]);
+                    v = kct::mk<C>(-k * v.y, k * v.x);
+                }
+                a[fb_at<C, ZKB>(c, jj, mz, ct)] = v;
+            }
+        }
+        __syncthreads();
+        r = fft_block<C, +1, ZKB>(P, a, b, tw, mz);
+    }
     C *dst = q + (((size_t)f * nyp + y) * mz) * nxh;
     for (int e = threadIdx.x; e < nk * mz; e += blockDim.x) {
         const int z = e / nk, c = e - z * nk;
