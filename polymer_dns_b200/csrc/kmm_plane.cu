@@ -693,15 +693,17 @@ __global__ void __launch_bounds__(256) k_xpoint(const T *__restrict__ pb, T *__r
 // compile-time warp FFT into the row's physical table in shared memory; then the block evaluates
 // the pointwise terms.  The two physical rows of a pair are one buffer of MX complex values, which
 // serves as the FFT's second (ping-pong) buffer once the pair's input has been read out of it, so
-// a warp needs only one private buffer and two 8-warp blocks fit on an SM even with 55 fields.
+// a warp needs only one private buffer and two 7-warp blocks fit on an SM even with 55 fields.
 // The generic k_xphys tiles two rows per block and transforms them with the runtime block FFT.
 #define XW 4    // warps of k_xfwd2
-// warps of k_xphys2: 8 in FP64 (two blocks per SM, held by shared memory and registers); 4 in
-// FP32, whose halved row buffer already lets four blocks share an SM, where 8-warp blocks would
-// be held to two by registers with more idle threads in the pointwise pass
+// warps of k_xphys2: 7 in FP64 (two blocks per SM, held by shared memory and registers; the 28
+// field pairs of the polymer + scalar inputs then take four full rounds, where 8 warps left half
+// of them idle in the last round before the block barrier: 3.8 % faster at 128^3); 4 in FP32,
+// whose halved row buffer already lets four blocks share an SM, where 8-warp blocks would be held
+// to two by registers with more idle threads in the pointwise pass
 template <typename C>
 struct XpW {
-    static constexpr int n = sizeof(C) == 16 ? 8 : 4;
+    static constexpr int n = sizeof(C) == 16 ? 7 : 4;
 };
 template <int MX, typename C>
 __global__ void __launch_bounds__(XpW<C>::n * 32) k_xphys2(const C *__restrict__ q, typename kct::Real<C>::T *__restrict__ po,
