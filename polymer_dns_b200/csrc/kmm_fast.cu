@@ -209,15 +209,28 @@ __global__ void __launch_bounds__(FX_WARPS * 32, Fx2MinB<C>::v) k_fx2(const C *_
         }
         __syncwarp();
     };
+    // the last FFT stage of MX = 96, 192, 576 leaves output x = lane + 32 e in lane `lane` (its
+    // stride is a multiple of 32): it writes the lane's registers directly
+    constexpr bool REG_OUT = kct::stride(MX, kct::nfac(MX) - 1) % 32 == 0;
     auto run_inv = [&](T *ra, T *rb) {
-        const C *res = fft_warp_ct<C, MX, +1, 1, true>(a, b, tw);
+        if constexpr (REG_OUT) {
+            auto ld = [&](int x) { return a[swz<C>(x)]; };
+            auto st = [&](int x, C v) {
+                ra[x >> 5] = v.x;
+                rb[x >> 5] = v.y;
+            };
+            auto pre = [] {};
+            fft_warp_ct_io<C, MX, +1>(ld, st, pre, b, a, tw);
+        } else {
+            const C *res = fft_warp_ct<C, MX, +1, 1, true>(a, b, tw);
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int x = lane + 32 * e;
-            if (x < MX) {
-                const C v = res[swz<C>(x)];
-                ra[e] = v.x;
-                rb[e] = v.y;
+            for (int e = 0; e < E; ++e) {
+                const int x = lane + 32 * e;
+                if (x < MX) {
+                    const C v = res[swz<C>(x)];
+                    ra[e] = v.x;
+                    rb[e] = v.y;
+                }
             }
         }
         __syncwarp();
