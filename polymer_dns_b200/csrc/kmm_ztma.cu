@@ -14,8 +14,9 @@
 // results go to a [y][z] staging tile, which a tiled TMA store (box: 1 kx x mz z x 4 y) writes out
 // while the next field is transformed.  62.5 KB of shared memory per CTA at mz = 192, so three
 // CTAs share an SM.  (Forming the inputs inside the FFT's first stage and writing the staging tile
-// from its last, as the FP32 form and the forward transforms do, made this kernel 11 % slower:
-// the staging tile's barrier then falls between two FFT stages.)
+// from its last, as the FP32 form and the forward transforms do, made this kernel 11 % slower: the
+// staging tile's barrier then falls between two FFT stages.  Keeping the FFT's output in registers
+// across the barrier, as the forward transforms do, made it 8 % slower.)
 //
 // Every wait on an mbarrier is bounded (KMM_OPT_WAIT_LIMIT_MS, default 2 s of %globaltimer); a wait
 // that runs out records KMM_ERR_TIMEOUT in the step's status word and the CTA finishes without the
@@ -73,6 +74,11 @@ __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.a
 // tile element (kz, y) of one base field: 64-byte rows (4 y values of 16 B), 64-byte swizzle
 // (16-byte chunk index XOR bits 7-8 of the byte offset)
 __device__ __forceinline__ int ztile_idx(int kz, int y) { return kz * ZTM_YT + (y ^ ((kz >> 1) & 3)); }
+
+// the z lengths whose FFT's last stage leaves output z = lane + 32 e in lane `lane` (its stride is
+// a multiple of 32), so that the stage can write the lane's registers
+template <int MZ>
+constexpr bool ZREG = MZ % 32 == 0 && kct::stride(MZ, kct::nfac(MZ) - 1) % 32 == 0;
 
 // The base-field tiles pass through a ring of ZB_SLOTS shared-memory slots: the q fields are formed
 // in the order ZB_ORDER (each needs at most two base fields live), every base field is loaded into
@@ -235,16 +241,34 @@ __global__ void __launch_bounds__(ZTM_WARPS * 32, 3)
         const double2 *t = tiles + (size_t)(o % ZF_SLOTS) * TIN + (size_t)y * MZ;
         // the first FFT stage reads the tile row, the last writes the scratch buffer it does not read
         auto ld = [&](int z) { return ok ? t[z] : make_double2(0.0, 0.0); };
-        double2 *r = kct::nfac(MZ) % 2 == 0 ? b : a;
-        auto st = [&](int z, double2 v) { r[swz<double2>(z)] = v; };
         auto pre = [] {};
-        fft_warp_ct_io<double2, MZ, -1>(ld, st, pre, a, b, tw);
-        __syncwarp();
-        if (threadIdx.x == 0) tma_store_wait_read();   // the previous field's store has read the stage
-        __syncthreads();
-        for (int kz = lane; kz < NZ; kz += 32) {
-            const double2 v = r[swz<double2>(kz < NZH ? kz : (MZ - NZ) + kz)];
-            stage[ztile_idx(kz, y)] = make_double2(v.x / scale, v.y / scale);   // the reference's /(mx mz)
+        if constexpr (ZREG<MZ>) {
+            // the last stage leaves output z = lane + 32 e in lane `lane`: registers, truncated
+            // into the staging tile once the previous field's store has read it
+            double2 rv[MZ / 32];
+            auto st = [&](int z, double2 v) { rv[z >> 5] = v; };
+            fft_warp_ct_io<double2, MZ, -1>(ld, st, pre, a, b, tw);
+            if (threadIdx.x == 0) tma_store_wait_read();   // the previous field's store has read the stage
+            __syncthreads();
+#pragma unroll
+            for (int e = 0; e < MZ / 32; ++e) {
+                const int z = lane + 32 * e;
+                if (z < NZH || z >= MZ - NZH) {
+                    const int kz = z < NZH ? z : z - (MZ - NZ);
+                    stage[ztile_idx(kz, y)] = make_double2(rv[e].x / scale, rv[e].y / scale);   // the reference's /(mx mz)
+                }
+            }
+        } else {
+            double2 *r = kct::nfac(MZ) % 2 == 0 ? b : a;
+            auto st = [&](int z, double2 v) { r[swz<double2>(z)] = v; };
+            fft_warp_ct_io<double2, MZ, -1>(ld, st, pre, a, b, tw);
+            __syncwarp();
+            if (threadIdx.x == 0) tma_store_wait_read();   // the previous field's store has read the stage
+            __syncthreads();
+            for (int kz = lane; kz < NZ; kz += 32) {
+                const double2 v = r[swz<double2>(kz < NZH ? kz : (MZ - NZ) + kz)];
+                stage[ztile_idx(kz, y)] = make_double2(v.x / scale, v.y / scale);   // the reference's /(mx mz)
+            }
         }
         fence_async_smem();   // also orders this field's tile reads before the next load into the slot
         __syncthreads();
@@ -398,16 +422,32 @@ __global__ void __launch_bounds__(ZT32_WARPS * 32, 2)
         ok = mbar_wait(&bar[o], 0) && ok;
         const float2 *t = tiles + (size_t)o * TIN;
         auto ld = [&](int z) { return ok ? t[((size_t)y * MZ + z) * ZT32_KX + kl] : make_float2(0.f, 0.f); };
-        float2 *r = kct::nfac(MZ) % 2 == 0 ? b : a;
-        auto st = [&](int z, float2 v) { r[swz<float2>(z)] = v; };
         auto pre = [] {};
-        fft_warp_ct_io<float2, MZ, -1>(ld, st, pre, a, b, tw);
-        __syncwarp();
-        if (threadIdx.x == 0) tma_store_wait_read();
-        __syncthreads();
-        for (int kz = lane; kz < NZ; kz += 32) {
-            const float2 v = r[swz<float2>(kz < NZH ? kz : (MZ - NZ) + kz)];
-            stage[(size_t)kl * TOUT + ztile32_idx(kz, y)] = make_float2(v.x * rscale, v.y * rscale);
+        if constexpr (ZREG<MZ>) {
+            float2 rv[MZ / 32];
+            auto st = [&](int z, float2 v) { rv[z >> 5] = v; };
+            fft_warp_ct_io<float2, MZ, -1>(ld, st, pre, a, b, tw);
+            if (threadIdx.x == 0) tma_store_wait_read();
+            __syncthreads();
+#pragma unroll
+            for (int e = 0; e < MZ / 32; ++e) {
+                const int z = lane + 32 * e;
+                if (z < NZH || z >= MZ - NZH) {
+                    const int kz = z < NZH ? z : z - (MZ - NZ);
+                    stage[(size_t)kl * TOUT + ztile32_idx(kz, y)] = make_float2(rv[e].x * rscale, rv[e].y * rscale);
+                }
+            }
+        } else {
+            float2 *r = kct::nfac(MZ) % 2 == 0 ? b : a;
+            auto st = [&](int z, float2 v) { r[swz<float2>(z)] = v; };
+            fft_warp_ct_io<float2, MZ, -1>(ld, st, pre, a, b, tw);
+            __syncwarp();
+            if (threadIdx.x == 0) tma_store_wait_read();
+            __syncthreads();
+            for (int kz = lane; kz < NZ; kz += 32) {
+                const float2 v = r[swz<float2>(kz < NZH ? kz : (MZ - NZ) + kz)];
+                stage[(size_t)kl * TOUT + ztile32_idx(kz, y)] = make_float2(v.x * rscale, v.y * rscale);
+            }
         }
         fence_async_smem();
         __syncthreads();
