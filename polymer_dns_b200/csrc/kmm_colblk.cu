@@ -751,8 +751,9 @@ __device__ __forceinline__ void bsolve_cfg(BCol<K> &x, const PhiSolveCfg &S, con
     else bsolve_dirichlet<K>(x, T, zero, zero, P.w2 + S.g, c0, rj, FULL);
 }
 
+// (ny = 256: the 17 coefficients per lane of each column need the 2-block register budget)
 template <int K>
-__global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB)
+__global__ void __launch_bounds__(CB_WARPS * 32, K > 8 ? 2 : CB_MINB)
     k_bphirhs_solve(PhiSolveJobs J, PhiSolveCfg S0, PhiSolveCfg S1, int nsolve, int phi,
                     const double *__restrict__ rj, const double *__restrict__ wavx, const double *__restrict__ wavz,
                     int nz, int nzh, int nxh, double re, double var, double dt, double th, double dyde, double c0) {
@@ -792,7 +793,7 @@ __global__ void __launch_bounds__(CB_WARPS * 32, CB_MINB)
 int kmm_colblk_phirhs_solve(kmm_ctx *ctx, double2 *const *x, const double2 *const *fn, const double2 *const *fnm1,
                             int nf, double var, int phi, int nsolve, const KmmSolveSpec *spec) {
     const int K = colblk_k(ctx);
-    if (!K || K > 8 || !ctx->use_colblk) return KMM_ERR_UNSUPPORTED;
+    if (!K || !ctx->use_colblk) return KMM_ERR_UNSUPPORTED;
     if (nf < 1 || nf > KMM_SOLVE_BATCH || nsolve < 1 || nsolve > 2) return KMM_ERR_ARG;
     PhiSolveCfg S[2];
     const double *rj = NULL;
@@ -820,6 +821,7 @@ int kmm_colblk_phirhs_solve(kmm_ctx *ctx, double2 *const *x, const double2 *cons
     case 4: PS(4); break;
     case 6: PS(6); break;
     case 8: PS(8); break;
+    case 16: PS(16); break;
     default: return KMM_ERR_UNSUPPORTED;
     }
 #undef PS

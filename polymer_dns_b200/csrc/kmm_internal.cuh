@@ -197,7 +197,7 @@ int kmm_colblk_solve(kmm_ctx *ctx, double2 *u, double g, int robin, double at, d
 int kmm_colblk_solve_many(kmm_ctx *ctx, double2 *const *u, int nf, double g, int robin, double at, double bt,
                           double ab, double bb, const double2 *gt, const double2 *gb);
 // the routine step's phirhs followed by one or two tau solves with zero boundary values, fused per
-// column pair (blocked kernels, ny = 32 .. 128): x[m] <- solve(phirhs([phi of] x[m]; fn[m], fnm1[m],
+// column pair (blocked kernels, ny = 32 .. 128 and 256): x[m] <- solve(phirhs([phi of] x[m]; fn[m], fnm1[m],
 // var)), fnm1[m] = NULL taking 2 fn[m]; KMM_ERR_UNSUPPORTED where the blocked kernels do not apply
 struct KmmSolveSpec {
     double g;
