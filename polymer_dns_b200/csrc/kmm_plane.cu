@@ -637,13 +637,17 @@ __global__ void __launch_bounds__(XBW * 32) k_xinv_big2(const C *__restrict__ q,
         if (kk > 0) a[swz<C>(MX - kk)] = kct::mk<C>(A_.x + B_.y, -A_.y + B_.x);
     }
     __syncwarp();
-    const C *r = fft_warp_ct<C, MX, +1, 1, true>(a, b, tw);
     const size_t nphys = (size_t)nyp * mz * MX, g3 = ((size_t)y * mz + z) * MX;
-    for (int x = lane; x < MX; x += 32) {
-        const C v = r[swz<C>(x)];
-        pb[(size_t)f * nphys + g3 + x] = v.x;
-        if (g >= 0) pb[(size_t)g * nphys + g3 + x] = v.y;
-    }
+    // the FFT's last stage stores the two real rows straight to the physical buffer (consecutive
+    // lanes, consecutive x)
+    T *pf = pb + (size_t)f * nphys + g3, *pg = pb + (size_t)(g >= 0 ? g : f) * nphys + g3;
+    auto ld = [&](int x) { return a[swz<C>(x)]; };
+    auto st = [&](int x, C v) {
+        pf[x] = v.x;
+        if (g >= 0) pg[x] = v.y;
+    };
+    auto pre = [] {};
+    fft_warp_ct_io<C, MX, +1>(ld, st, pre, b, a, tw);
 }
 
 // pass 2: the pointwise terms from the physical buffer (precision T) into po (precision T)
