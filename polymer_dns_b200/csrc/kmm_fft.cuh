@@ -267,6 +267,62 @@ __device__ __forceinline__ void stage_io(LD &ld, ST &st, const C *__restrict__ t
     }
 }
 
+// stage F of one sequence in place in the swizzled buffer x: every lane reads and transforms all
+// its butterflies' inputs before the warp writes any output (the same arithmetic as stage())
+template <typename C, int N, int F, int S, int TWS>
+__device__ __forceinline__ void stage_ip(C *x, const C *__restrict__ tw, int lane) {
+    constexpr int R = fac(N, F);
+    constexpr int NS = stride(N, F);
+    constexpr int NR = N / R;
+    constexpr int TSTEP = N / (NS * R);
+    constexpr int IT = (NR + 31) / 32;
+    C v[IT][R];
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int j = lane + 32 * it;
+        if (NR % 32 == 0 || j < NR) {
+            const int k = j % NS;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                C u = x[swz<C>(j + r * NR)];
+                if (NS > 1 && r > 0 && k) {
+                    C w = __ldg(&tw[r * k * TSTEP * TWS]);
+                    if (S > 0) w.y = -w.y;
+                    u = mul(u, w);
+                }
+                v[it][r] = u;
+            }
+            Dft<C, R, S>::run(v[it]);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int j = lane + 32 * it;
+        if (NR % 32 == 0 || j < NR) {
+            const int k = j % NS;
+            const int idxD = (j - k) * R + k;
+#pragma unroll
+            for (int q = 0; q < R; ++q) x[swz<C>(idxD + q * NS)] = v[it][q];
+        }
+    }
+    __syncwarp();
+}
+
+template <typename C, int N, int F, int S, int TWS, bool END>
+struct IpSteps;
+template <typename C, int N, int F, int S, int TWS>
+struct IpSteps<C, N, F, S, TWS, true> {
+    static __device__ __forceinline__ void go(C *, const C *, int) {}
+};
+template <typename C, int N, int F, int S, int TWS>
+struct IpSteps<C, N, F, S, TWS, false> {
+    static __device__ __forceinline__ void go(C *x, const C *tw, int lane) {
+        stage_ip<C, N, F, S, TWS>(x, tw, lane);
+        IpSteps<C, N, F + 1, S, TWS, (F + 2 >= nfac(N))>::go(x, tw, lane);
+    }
+};
+
 // the stages between the first and the last, ping-ponging between two swizzled buffers; returns
 // the buffer holding the output of the last of them
 template <typename C, int N, int F, int S, int TWS, bool END>
@@ -315,6 +371,20 @@ __device__ __forceinline__ void fft_warp_ct_io(LD ld, ST st, PRE pre, C *a, C *b
     pre();
     auto from_src = [&](int x) { return src[swz<C>(x)]; };
     kct::stage_io<C, N, L - 1, S, TWS>(from_src, st, tw, lane);
+}
+
+// fft_warp_ct of one sequence held in one swizzled buffer a (the input visible to the whole warp):
+// every stage but the last runs in place (stage_ip), and the last reads a and writes its output
+// through st(x, value), so a warp needs one buffer of N elements instead of two.  Same arithmetic
+// as fft_warp_ct.
+template <typename C, int N, int S, int TWS = 1, typename ST>
+__device__ __forceinline__ void fft_warp_ct_ip(C *a, ST st, const C *tw) {
+    constexpr int L = kct::nfac(N);
+    static_assert(L >= 1, "transform length must be 2^a 3^b 5^c");
+    const int lane = threadIdx.x & 31;
+    kct::IpSteps<C, N, 0, S, TWS, (1 >= L)>::go(a, tw, lane);
+    auto from_a = [&](int x) { return a[swz<C>(x)]; };
+    kct::stage_io<C, N, L - 1, S, TWS>(from_a, st, tw, lane);
 }
 
 // the transform lengths with compiled instances (3/2-rule grids of nx, nz = 32, 64, 96, 128, 384

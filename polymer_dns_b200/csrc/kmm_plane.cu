@@ -606,10 +606,12 @@ __global__ void __launch_bounds__(256) k_xinv_big(const double2 *__restrict__ q,
 
 // pass 1 at the compiled lengths (MX = 576: nx = 384), in either precision: one warp per (y, z)
 // row and field pair, the Hermitian extension of A + iB (as in k_xphys2) through the compile-time
-// warp FFT, the two real rows stored to the physical buffer in precision C
+// warp FFT (FP64: run in place in one buffer, fft_warp_ct_ip, so four blocks of four warps share an
+// SM instead of three), the two real rows stored to the physical buffer in precision C by its last
+// stage
 #define XBW 4   // rows (warps) per block of k_xinv_big2
 template <int MX, typename C>
-__global__ void __launch_bounds__(XBW * 32) k_xinv_big2(const C *__restrict__ q, typename kct::Real<C>::T *__restrict__ pb,
+__global__ void __launch_bounds__(XBW * 32, sizeof(C) == 16 ? 4 : 6) k_xinv_big2(const C *__restrict__ q, typename kct::Real<C>::T *__restrict__ pb,
                                                         const C *__restrict__ tw, int nin, int nyp, int mz,
                                                         const __grid_constant__ XRecipe X,
                                                         const double *__restrict__ wavx) {
@@ -619,7 +621,9 @@ __global__ void __launch_bounds__(XBW * 32) k_xinv_big2(const C *__restrict__ q,
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int z = blockIdx.x * XBW + warp, y = blockIdx.y, f = 2 * blockIdx.z, g = f + 1 < nin ? f + 1 : -1;
     if (z >= mz) return;   // whole warps: no block barrier below
-    C *a = reinterpret_cast<C *>(smd) + (size_t)warp * 2 * MX, *b = a + MX;
+    // FP64: one buffer per warp, the FFT in place; FP32: two (its registers allow six blocks per SM)
+    constexpr int NBUF = sizeof(C) == 16 ? 1 : 2;
+    C *a = reinterpret_cast<C *>(smd) + (size_t)warp * NBUF * MX;
     const int pr = blockIdx.z;
     const bool xd = X.xd[pr];
     const C *qa = q + (((size_t)X.qa[pr] * nyp + y) * mz + z) * NXH;
@@ -641,13 +645,17 @@ __global__ void __launch_bounds__(XBW * 32) k_xinv_big2(const C *__restrict__ q,
     // the FFT's last stage stores the two real rows straight to the physical buffer (consecutive
     // lanes, consecutive x)
     T *pf = pb + (size_t)f * nphys + g3, *pg = pb + (size_t)(g >= 0 ? g : f) * nphys + g3;
-    auto ld = [&](int x) { return a[swz<C>(x)]; };
     auto st = [&](int x, C v) {
         pf[x] = v.x;
         if (g >= 0) pg[x] = v.y;
     };
-    auto pre = [] {};
-    fft_warp_ct_io<C, MX, +1>(ld, st, pre, b, a, tw);
+    if constexpr (NBUF == 1) {
+        fft_warp_ct_ip<C, MX, +1>(a, st, tw);
+    } else {
+        auto ld = [&](int x) { return a[swz<C>(x)]; };
+        auto pre = [] {};
+        fft_warp_ct_io<C, MX, +1>(ld, st, pre, a + MX, a, tw);
+    }
 }
 
 // pass 2: the pointwise terms from the physical buffer (precision T) into po (precision T)
@@ -1617,7 +1625,7 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
                     ctx->d_cfl, ctx->d_umax, ctx->pmx, A, sv, nyp, mz, mx, nxh);
             } else {
                 const dim3 g1((mz + XBW - 1) / XBW, nyp, (nin + 1) / 2);
-                const size_t sm_b2 = 2 * eb * 2 * XBW * (size_t)mx;
+                const size_t sm_b2 = 2 * eb * (f32 ? 2 : 1) * XBW * (size_t)mx;   // complex rows per warp
                 if (mx == 576 && f32) {
                     RET(kmm_smem_attr(ctx, (const void *)k_xinv_big2<576, float2>, sm_b2));
                     k_xinv_big2<576, float2><<<g1, XBW * 32, sm_b2, ctx->stream>>>(q_in32, (float *)ctx->xbig, tw_mx,
