@@ -387,6 +387,15 @@ __device__ __forceinline__ void fft_warp_ct_ip(C *a, ST st, const C *tw) {
     kct::stage_io<C, N, L - 1, S, TWS>(from_a, st, tw, lane);
 }
 
+// the same with every stage in place: the result is left in a (natural order, swizzled)
+template <typename C, int N, int S, int TWS = 1>
+__device__ __forceinline__ void fft_warp_ct_inplace(C *a, const C *tw) {
+    constexpr int L = kct::nfac(N);
+    const int lane = threadIdx.x & 31;
+    kct::IpSteps<C, N, 0, S, TWS, (1 >= L)>::go(a, tw, lane);
+    kct::stage_ip<C, N, L - 1, S, TWS>(a, tw, lane);
+}
+
 // the transform lengths with compiled instances (3/2-rule grids of nx, nz = 32, 64, 96, 128, 384
 // and the Chebyshev extensions 2 ny = 64, 128, 192, 256, 512)
 #define KMM_CT_LEN_LIST(X) X(48) X(64) X(96) X(128) X(144) X(192) X(256) X(512) X(576)

@@ -302,8 +302,10 @@ __device__ __forceinline__ C *zbwd_io(const C *__restrict__ src, C *a, C *b, con
     return res;
 }
 
-template <typename C>
-__global__ void __launch_bounds__(256, 4) k_zfft_bwd(const C *__restrict__ pl, C *__restrict__ q, const __grid_constant__ DevPlan P,
+// BIG (mz = 576 only): one buffer per block, each warp's FFT in place (fft_warp_ct_inplace), so two
+// blocks share an SM where the two 74 KB buffers held it to one
+template <typename C, bool BIG = false>
+__global__ void __launch_bounds__(256, BIG ? 2 : 4) k_zfft_bwd(const C *__restrict__ pl, C *__restrict__ q, const __grid_constant__ DevPlan P,
                                                   const C *__restrict__ tw, int nyp, int nz, int nxh, int mz,
                                                   const __grid_constant__ ZRecipe R, const double *__restrict__ wavx,
                                                   const double *__restrict__ wavz) {
@@ -318,7 +320,7 @@ __global__ void __launch_bounds__(256, 4) k_zfft_bwd(const C *__restrict__ pl, C
     const bool ct = fb_compiled(mz);
     const C *src = pl + (((size_t)fb * nyp + y) * nxh + kx0) * nz;
     C *r = NULL;
-    switch (mz) {
+    if constexpr (!BIG) switch (mz) {
     case 48: r = zbwd_io<C, 48>(src, a, b, tw, nk, nz, kx0, mult, wavx, wavz); break;
     case 64: r = zbwd_io<C, 64>(src, a, b, tw, nk, nz, kx0, mult, wavx, wavz); break;
     case 96: r = zbwd_io<C, 96>(src, a, b, tw, nk, nz, kx0, mult, wavx, wavz); break;
@@ -352,7 +354,14 @@ __global__ void __launch_bounds__(256, 4) k_zfft_bwd(const C *__restrict__ pl, C
             }
         }
         __syncthreads();
-        r = fft_block<C, +1, ZKB>(P, a, b, tw, mz);
+        if constexpr (BIG) {
+            const int w = threadIdx.x >> 5;
+            if (w < nk) fft_warp_ct_inplace<C, 576, +1>(a + (size_t)w * (576 + FB_PAD), tw);
+            __syncthreads();
+            r = a;
+        } else {
+            r = fft_block<C, +1, ZKB>(P, a, b, tw, mz);
+        }
     }
     C *dst = q + (((size_t)f * nyp + y) * mz) * nxh;
     for (int e = threadIdx.x; e < nk * mz; e += blockDim.x) {
@@ -978,8 +987,9 @@ __global__ void __launch_bounds__(256) k_xfwd(const double *__restrict__ po, dou
 // ---------------------------------------------------------------------------
 // 6. z: forward c2c, truncate to nz, /(mx*mz)
 // ---------------------------------------------------------------------------
-template <typename C>
-__global__ void __launch_bounds__(256, 4) k_zfft_fwd(const C *__restrict__ q, C *__restrict__ pl, const __grid_constant__ DevPlan P,
+// BIG (mz = 576 only): one buffer, each warp's FFT in place, as in k_zfft_bwd
+template <typename C, bool BIG = false>
+__global__ void __launch_bounds__(256, BIG ? 2 : 4) k_zfft_fwd(const C *__restrict__ q, C *__restrict__ pl, const __grid_constant__ DevPlan P,
                                                   const C *__restrict__ tw, int nyp, int nz, int nxh, int mz,
                                                   double scale) {
     typedef typename kct::Real<C>::T T;
@@ -1009,7 +1019,15 @@ __global__ void __launch_bounds__(256, 4) k_zfft_fwd(const C *__restrict__ q, C 
         }
     }
     __syncthreads();
-    C *r = fft_block<C, -1, ZKB>(P, a, b, tw, mz);
+    C *r;
+    if constexpr (BIG) {
+        const int w = threadIdx.x >> 5;
+        if (w < nk) fft_warp_ct_inplace<C, 576, -1>(a + (size_t)w * (576 + FB_PAD), tw);
+        __syncthreads();
+        r = a;
+    } else {
+        r = fft_block<C, -1, ZKB>(P, a, b, tw, mz);
+    }
     C *dst = pl + (((size_t)f * nyp + y) * nxh + kx0) * nz;
     for (int e = threadIdx.x; e < nk * nz; e += blockDim.x) {
         const int c = e / nz, j = e - c * nz;
@@ -1517,6 +1535,15 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     RET(kmm_smem_attr(ctx, (const void *)k_dct_bwd<float2>, sm_dct));
     RET(kmm_smem_attr(ctx, (const void *)k_zfft_bwd<float2>, sm_z));
     RET(kmm_smem_attr(ctx, (const void *)k_zfft_fwd<float2>, sm_z));
+    // mz = 576: the one-buffer forms (in-place warp FFTs, two blocks per SM)
+    const bool zbig = mz == 576;
+    const size_t sm_zb = sizeof(double2) * (size_t)fb_len(ZKB, mz);
+    if (zbig) {
+        RET(kmm_smem_attr(ctx, (const void *)k_zfft_bwd<double2, true>, sm_zb));
+        RET(kmm_smem_attr(ctx, (const void *)k_zfft_fwd<double2, true>, sm_zb));
+        RET(kmm_smem_attr(ctx, (const void *)k_zfft_bwd<float2, true>, sm_zb));
+        RET(kmm_smem_attr(ctx, (const void *)k_zfft_fwd<float2, true>, sm_zb));
+    }
     // rows of every input field in shared memory (k_xphys) unless that exceeds the 227 KB limit:
     // then the two-pass x stage through an HBM buffer of the physical inputs (k_xinv_big, k_xpoint)
     // (always at mx = 576, whose compiled transforms serve the two-pass form in both precisions)
@@ -1574,12 +1601,21 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
     }
     kmm_toc(ctx, KMM_STAGE_DCT_FWD);
     kmm_tic(ctx);
-    if (f32)
-        k_zfft_bwd<float2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nq), 256, sm_z, ctx->stream>>>(
-            pl_in32, q_in32, ctx->pmz, tw_mz, nyp, nz, nxh, mz, zq, ctx->d_wavx, ctx->d_wavz);
-    else
-        k_zfft_bwd<double2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nq), 256, sm_z, ctx->stream>>>(
-            ctx->pl_in, ctx->q_in, ctx->pmz, ctx->pmz.tw, nyp, nz, nxh, mz, zq, ctx->d_wavx, ctx->d_wavz);
+    {
+        const dim3 gz((nxh + ZKB - 1) / ZKB, nyp, nq);
+        if (f32 && zbig)
+            k_zfft_bwd<float2, true><<<gz, 256, sm_zb, ctx->stream>>>(pl_in32, q_in32, ctx->pmz, tw_mz, nyp, nz, nxh, mz,
+                                                                      zq, ctx->d_wavx, ctx->d_wavz);
+        else if (f32)
+            k_zfft_bwd<float2><<<gz, 256, sm_z, ctx->stream>>>(pl_in32, q_in32, ctx->pmz, tw_mz, nyp, nz, nxh, mz, zq,
+                                                              ctx->d_wavx, ctx->d_wavz);
+        else if (zbig)
+            k_zfft_bwd<double2, true><<<gz, 256, sm_zb, ctx->stream>>>(ctx->pl_in, ctx->q_in, ctx->pmz, ctx->pmz.tw, nyp,
+                                                                       nz, nxh, mz, zq, ctx->d_wavx, ctx->d_wavz);
+        else
+            k_zfft_bwd<double2><<<gz, 256, sm_z, ctx->stream>>>(ctx->pl_in, ctx->q_in, ctx->pmz, ctx->pmz.tw, nyp, nz,
+                                                               nxh, mz, zq, ctx->d_wavx, ctx->d_wavz);
+    }
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_BWD);
     bool fast_done = false, xstat = false;
@@ -1706,12 +1742,21 @@ extern "C" int kmm_vcw3dp(kmm_ctx *ctx) {
         kmm_toc(ctx, KMM_STAGE_XFWD);
     }
     kmm_tic(ctx);
-    if (f32)
-        k_zfft_fwd<float2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nout), 256, sm_z, ctx->stream>>>(
-            q_out32, pl_out32, ctx->pmz, tw_mz, nyp, nz, nxh, mz, (double)mx * (double)mz);
-    else
-        k_zfft_fwd<double2><<<dim3((nxh + ZKB - 1) / ZKB, nyp, nout), 256, sm_z, ctx->stream>>>(
-            ctx->q_out, ctx->pl_out, ctx->pmz, ctx->pmz.tw, nyp, nz, nxh, mz, (double)mx * (double)mz);
+    {
+        const dim3 gz((nxh + ZKB - 1) / ZKB, nyp, nout);
+        const double zs = (double)mx * (double)mz;
+        if (f32 && zbig)
+            k_zfft_fwd<float2, true><<<gz, 256, sm_zb, ctx->stream>>>(q_out32, pl_out32, ctx->pmz, tw_mz, nyp, nz, nxh,
+                                                                      mz, zs);
+        else if (f32)
+            k_zfft_fwd<float2><<<gz, 256, sm_z, ctx->stream>>>(q_out32, pl_out32, ctx->pmz, tw_mz, nyp, nz, nxh, mz, zs);
+        else if (zbig)
+            k_zfft_fwd<double2, true><<<gz, 256, sm_zb, ctx->stream>>>(ctx->q_out, ctx->pl_out, ctx->pmz, ctx->pmz.tw,
+                                                                       nyp, nz, nxh, mz, zs);
+        else
+            k_zfft_fwd<double2><<<gz, 256, sm_z, ctx->stream>>>(ctx->q_out, ctx->pl_out, ctx->pmz, ctx->pmz.tw, nyp, nz,
+                                                               nxh, mz, zs);
+    }
     CKL();
     kmm_toc(ctx, KMM_STAGE_ZFFT_FWD);
     kmm_tic(ctx);
