@@ -163,7 +163,14 @@ __device__ __forceinline__ void dct1_half(C *x, C *a, C *b, const C *__restrict_
     for (int o = 16; o; o >>= 1)
         seed = kct::add(seed, kct::mk<C>(__shfl_xor_sync(0xffffffffu, seed.x, o), __shfl_xor_sync(0xffffffffu, seed.y, o)));
     __syncwarp();
-    const C *Y = fft_warp_ct<C, N, -1, 1, true, 2>(a, b, tw);
+    // N = 256: the FFT in place in a (one buffer per warp: three blocks per SM instead of two)
+    const C *Y;
+    if constexpr (N == 256) {
+        fft_warp_ct_inplace<C, N, -1, 2>(a, tw);
+        Y = a;
+    } else {
+        Y = fft_warp_ct<C, N, -1, 1, true, 2>(a, b, tw);
+    }
     // odd outputs: X_{2m+1} = seed + sum_{t=1}^{m} d_t, d_t = -i (Y_t - Y_{N-t}); lane holds m = lane Q .. lane Q + Q - 1
     C d[Q];
     C tot = kct::mk<C>((T)0, (T)0);
@@ -1137,7 +1144,8 @@ __global__ void __launch_bounds__(256) k_dct_bwd_h(const C *__restrict__ pl, con
 template <typename C>
 static int dct_h_fwd(kmm_ctx *ctx, int nf, const FieldPtrs &in, C *pl, const C *tw, int nz, int nxh, int ncols) {
     const int ny = ctx->nyp - 1;
-    const size_t sm = sizeof(C) * ((size_t)DCT_CB * (ny + 1) + 2 * (size_t)fb_len(DCT_CB, ny));
+    const size_t nbuf = ny == 256 ? 1 : 2;   // dct1_half's FFT runs in place at ny = 256
+    const size_t sm = sizeof(C) * ((size_t)DCT_CB * (ny + 1) + nbuf * (size_t)fb_len(DCT_CB, ny));
     const dim3 grid((ncols + DCT_CB - 1) / DCT_CB, nf);
 #define DH(NN)                                                                                            \
     do {                                                                                                  \
@@ -1160,7 +1168,8 @@ static int dct_h_fwd(kmm_ctx *ctx, int nf, const FieldPtrs &in, C *pl, const C *
 template <typename C>
 static int dct_h_bwd(kmm_ctx *ctx, int nf, const C *pl, const FieldPtrsW &out, const C *tw, int nz, int nxh, int ncols) {
     const int ny = ctx->nyp - 1;
-    const size_t sm = sizeof(C) * ((size_t)DCT_CB * (ny + 1) + 2 * (size_t)fb_len(DCT_CB, ny));
+    const size_t nbuf = ny == 256 ? 1 : 2;   // dct1_half's FFT runs in place at ny = 256
+    const size_t sm = sizeof(C) * ((size_t)DCT_CB * (ny + 1) + nbuf * (size_t)fb_len(DCT_CB, ny));
     const dim3 grid((ncols + DCT_CB - 1) / DCT_CB, nf);
 #define DH(NN)                                                                                            \
     do {                                                                                                  \
