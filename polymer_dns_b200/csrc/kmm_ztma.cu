@@ -16,7 +16,8 @@
 // CTAs share an SM.  (Forming the inputs inside the FFT's first stage and writing the staging tile
 // from its last, as the FP32 form and the forward transforms do, made this kernel 11 % slower: the
 // staging tile's barrier then falls between two FFT stages.  Keeping the FFT's output in registers
-// across the barrier, as the forward transforms do, made it 8 % slower.)
+// across the barrier, as the forward transforms do, made it 8 % slower, and so did one FFT buffer
+// per warp (the transform in place) with four CTAs per SM.)
 //
 // Every wait on an mbarrier is bounded (KMM_OPT_WAIT_LIMIT_MS, default 2 s of %globaltimer); a wait
 // that runs out records KMM_ERR_TIMEOUT in the step's status word and the CTA finishes without the
