@@ -194,11 +194,12 @@ def test_two_pass_x_stage_matches_shared_memory_form(rt):
         g.close()
 
 
-@pytest.mark.parametrize("grid", [(384, 32, 16), (16, 256, 12)])
+@pytest.mark.parametrize("grid", [(384, 32, 16), (16, 256, 12), (16, 32, 384)])
 def test_cfg5_lengths_match_oracle(rt, oracle_mod, grid):
     """The transform lengths of the 384 x 257 x 384 workload on small grids the oracle runs in
-    seconds: mx = 576 (the two-pass x stage with 55 polymer inputs) and ny = 256 (2 ny = 512 DCTs,
-    the one-thread-per-column solves), polymer + scalar + IB cylinder + tracers, 3 steps."""
+    seconds: mx = 576 (the two-pass x stage with 55 polymer inputs), ny = 256 (2 ny = 512 DCTs,
+    the one-thread-per-column solves) and mz = 576 (the one-buffer z transforms with in-place warp
+    FFTs), polymer + scalar + IB cylinder + tracers, 3 steps."""
     nx, ny, nz = grid
     p, init, _ = configs.make("cfg5", nx=nx, ny=ny, nz=nz, npart=2000, dt=0.002)
     f, extra = configs.build_inputs(p, init, "cfg5")
