@@ -271,7 +271,8 @@ int  kmm_run(kmm_ctx *ctx, int n);
  * bound field is copied host -> device, after every step device -> host, so the host arrays hold
  * each step's result (also that of a step that returns a stop status such as KMM_ERR_CFL, after
  * which it returns).  A step's downloads and the next step's uploads run together on two copy
- * streams, chunk by chunk.  The host arrays must not be touched during the call.  Without
+ * streams, chunk by chunk; the history fields' downloads (FNM1, GNM1, SCNM1, the polymer n-1
+ * records) run during the step.  The host arrays must not be touched during the call.  Without
  * bindings it is kmm_run.                                                                      */
 int  kmm_bind_host(kmm_ctx *ctx, int field, void *host, size_t bytes);
 int  kmm_run_host(kmm_ctx *ctx, int n);

@@ -10,6 +10,8 @@
 // HS_CHUNK bytes.  After a step, its downloads (device -> host) and the next step's uploads
 // (host -> device) proceed together: each chunk's upload waits only for the download of the same
 // chunk, so the two copy engines work at once and the next step waits for the last upload only.
+// The history fields' downloads (fn^{n-1} and the like, whose new value is the buffer the step
+// takes over from fn) start before the step and run during it.
 #include <new>
 #include <vector>
 
@@ -36,6 +38,7 @@ struct Chunk {
 struct KmmHostState {
     std::vector<HostBind> binds;
     std::vector<Chunk> chunks;
+    std::vector<const void *> early_src;   // per binding: the buffer its early download read (or NULL)
     std::vector<cudaEvent_t> down_ev;   // one per chunk: its download has finished
     cudaStream_t h2d = NULL, d2h = NULL;
     cudaEvent_t entry_ev = NULL, up_ev = NULL, step_ev = NULL;
@@ -92,12 +95,49 @@ int enqueue_uploads(kmm_ctx *ctx, KmmHostState *S, bool after_down) {
     return KMM_OK;
 }
 
-// every bound field device -> host on d2h, after the work enqueued so far on the context's stream
+// the n field whose buffer a history field n-1 takes over in a step (the step exchanges the two
+// buffers and writes only the new n: fn^{n-1} = fn^n, main_dns.f90:268-275, 335, 386, 418), or -1
+int hist_partner(int f) {
+    if (f == KMM_FNM1) return KMM_FN;
+    if (f == KMM_GNM1) return KMM_GN;
+    if (f == KMM_SCNM1) return KMM_SCN;
+    if (f >= KMM_C11NM1 && f <= KMM_C33NM1) return KMM_C11N + (f - KMM_C11NM1);
+    if (f >= KMM_STR11NM1 && f <= KMM_STR33NM1) return KMM_STR11N + (f - KMM_STR11NM1);
+    return -1;
+}
+
+// before a step: the bound history fields' results are the n fields' current buffers, which the
+// step reads but does not write, so their downloads start now and run during the step (after this
+// step's uploads have read the host arrays)
+int enqueue_early_downloads(kmm_ctx *ctx, KmmHostState *S) {
+    S->early_src.assign(S->binds.size(), NULL);
+    bool any = false;
+    for (size_t i = 0; i < S->chunks.size(); ++i) {
+        const Chunk &c = S->chunks[i];
+        const int n = hist_partner(S->binds[c.bind].field);
+        if (n < 0) continue;
+        const char *d = (const char *)kmm_field_ptr(ctx, n);
+        if (!d) return KMM_ERR_NOMEM;
+        if (!any) CK(cudaStreamWaitEvent(S->d2h, S->up_ev, 0));
+        any = true;
+        S->early_src[c.bind] = d;
+        CK(cudaMemcpyAsync((char *)S->binds[c.bind].host + c.off, d + c.off, c.n, cudaMemcpyDeviceToHost, S->d2h));
+        CK(cudaEventRecord(S->down_ev[i], S->d2h));
+    }
+    return KMM_OK;
+}
+
+// every bound field device -> host on d2h, after the work enqueued so far on the context's stream;
+// a history field downloaded early is skipped if the step made that buffer its own (else, e.g. when
+// the step stopped before its exchanges, it is downloaded again here)
 int enqueue_downloads(kmm_ctx *ctx, KmmHostState *S) {
     CK(cudaEventRecord(S->step_ev, ctx->stream));
     CK(cudaStreamWaitEvent(S->d2h, S->step_ev, 0));
     for (size_t i = 0; i < S->chunks.size(); ++i) {
         const Chunk &c = S->chunks[i];
+        if (c.bind < (int)S->early_src.size() && S->early_src[c.bind] &&
+            kmm_field_ptr(ctx, S->binds[c.bind].field) == S->early_src[c.bind])
+            continue;
         const char *d = chunk_dev(ctx, S, c);
         if (!d) return KMM_ERR_NOMEM;
         CK(cudaMemcpyAsync((char *)S->binds[c.bind].host + c.off, d, c.n, cudaMemcpyDeviceToHost, S->d2h));
@@ -164,6 +204,8 @@ extern "C" int kmm_run_host(kmm_ctx *ctx, int n) {
     RET(enqueue_uploads(ctx, S, false));
     int st = KMM_OK;
     for (int s = 0; s < n; ++s) {
+        st = enqueue_early_downloads(ctx, S);
+        if (st) break;
         st = kmm_step(ctx);
         if (st == KMM_ERR_CUDA || st == KMM_ERR_NOMEM || st == KMM_ERR_ARG) break;
         // the host arrays receive this step's result even when the step reports a stop status

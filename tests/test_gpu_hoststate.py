@@ -125,3 +125,30 @@ def test_bind_host_arguments(rt):
     assert L.kmm_bind_host(h, -1, None, 0) == 0                                # unbind all
     assert L.kmm_run_host(h, -1) == abi.ERR_ARG
     g.close()
+
+
+def test_run_host_polymer_routine_path(rt):
+    """The routine path with FENE-P polymer and the IB cylinder (the c-restart records bound too:
+    their n-1 histories are downloaded during the step, from the buffers the step takes over)."""
+    from polymer_dns_b200 import configs
+    p, init, _ = configs.make("cfg3", 0, grid=32)
+    f, extra = configs.build_inputs(p, init, "cfg3")
+    ctxs = []
+    for _ in range(2):
+        c = rt.KmmContext(p)
+        configs.load(f, extra, c.upload)
+        assert c.initial() == 0
+        ctxs.append(c)
+    g, r = ctxs
+    comp = ["11", "12", "13", "22", "23", "33"]
+    names = [n for n in STATE] + ["C11", "C12", "C13", "C21", "C22", "C23", "C31", "C32", "C33"]
+    names += ["C%sN" % c for c in comp] + ["C%sNM1" % c for c in comp]
+    names += ["STR%sN" % c for c in comp] + ["STR%sNM1" % c for c in comp]
+    if not p.npart:
+        names = [n for n in names if not n.endswith("PART")]
+    host = _bind_names(g, names)
+    assert g.run_host(4) == 0
+    for _ in range(4):
+        assert r.step() == 0
+    _same(host, r, names)
+    _same(host, g, names)
