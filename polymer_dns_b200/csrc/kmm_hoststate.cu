@@ -81,15 +81,24 @@ char *chunk_dev(kmm_ctx *ctx, const KmmHostState *S, const Chunk &c) {
     return d ? d + c.off : NULL;
 }
 
-// every bound field host -> device on h2d; the chunk waits for its own download when `after_down`
+// a chunk whose download ran during the step (its field took over the buffer that download read)
+bool downloaded_early(kmm_ctx *ctx, const KmmHostState *S, const Chunk &c) {
+    return c.bind < (int)S->early_src.size() && S->early_src[c.bind] &&
+           kmm_field_ptr(ctx, S->binds[c.bind].field) == S->early_src[c.bind];
+}
+
+// every bound field host -> device on h2d; the chunk waits for its own download when `after_down`,
+// and the chunks downloaded during the step go first (their downloads have finished or will soon)
 int enqueue_uploads(kmm_ctx *ctx, KmmHostState *S, bool after_down) {
-    for (size_t i = 0; i < S->chunks.size(); ++i) {
-        const Chunk &c = S->chunks[i];
-        char *d = chunk_dev(ctx, S, c);
-        if (!d) return KMM_ERR_NOMEM;
-        if (after_down) CK(cudaStreamWaitEvent(S->h2d, S->down_ev[i], 0));
-        CK(cudaMemcpyAsync(d, (const char *)S->binds[c.bind].host + c.off, c.n, cudaMemcpyHostToDevice, S->h2d));
-    }
+    for (int pass = after_down ? 0 : 1; pass < 2; ++pass)
+        for (size_t i = 0; i < S->chunks.size(); ++i) {
+            const Chunk &c = S->chunks[i];
+            if (after_down && downloaded_early(ctx, S, c) != (pass == 0)) continue;
+            char *d = chunk_dev(ctx, S, c);
+            if (!d) return KMM_ERR_NOMEM;
+            if (after_down) CK(cudaStreamWaitEvent(S->h2d, S->down_ev[i], 0));
+            CK(cudaMemcpyAsync(d, (const char *)S->binds[c.bind].host + c.off, c.n, cudaMemcpyHostToDevice, S->h2d));
+        }
     CK(cudaEventRecord(S->up_ev, S->h2d));
     CK(cudaStreamWaitEvent(ctx->stream, S->up_ev, 0));   // the step reads what has landed
     return KMM_OK;
@@ -135,9 +144,7 @@ int enqueue_downloads(kmm_ctx *ctx, KmmHostState *S) {
     CK(cudaStreamWaitEvent(S->d2h, S->step_ev, 0));
     for (size_t i = 0; i < S->chunks.size(); ++i) {
         const Chunk &c = S->chunks[i];
-        if (c.bind < (int)S->early_src.size() && S->early_src[c.bind] &&
-            kmm_field_ptr(ctx, S->binds[c.bind].field) == S->early_src[c.bind])
-            continue;
+        if (downloaded_early(ctx, S, c)) continue;
         const char *d = chunk_dev(ctx, S, c);
         if (!d) return KMM_ERR_NOMEM;
         CK(cudaMemcpyAsync((char *)S->binds[c.bind].host + c.off, d, c.n, cudaMemcpyDeviceToHost, S->d2h));
